@@ -1,0 +1,644 @@
+"""Python binding of libmufflon_core.so (ctypes), mirroring Mufflon's
+src/pythonbinding/bindings.py: ``DllInterface`` wraps the C API one call per
+method (same method names), ``RenderActions`` is the convenience layer
+(enable a renderer by name, iterate, read targets). ``load_scene_spec`` builds
+a procedural :class:`mufflon_b200.scenes.SceneSpec` through the same C API
+calls that Mufflon's scene loader issues.
+
+There is no CPU fallback: constructing a ``DllInterface`` without the built
+library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, Union, byref, c_bool, c_char_p, c_float, c_int, c_int32, c_size_t,
+                    c_uint8, c_uint16, c_uint32, c_uint64, c_ulonglong, c_void_p)
+from enum import IntEnum
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_LIB = os.path.join(_HERE, "lib", "libmufflon_core.so")
+
+
+class ProcessTime(Structure):
+    _fields_ = [("cycles", c_ulonglong), ("microseconds", c_ulonglong)]
+
+
+class Vec2(Structure):
+    _fields_ = [("u", c_float), ("v", c_float)]
+
+
+class Vec3(Structure):
+    _fields_ = [("x", c_float), ("y", c_float), ("z", c_float)]
+
+
+class UVec3(Structure):
+    _fields_ = [("x", c_uint32), ("y", c_uint32), ("z", c_uint32)]
+
+
+class UVec4(Structure):
+    _fields_ = [("x", c_uint32), ("y", c_uint32), ("z", c_uint32), ("w", c_uint32)]
+
+
+class Mat3x4(Structure):
+    _fields_ = [("v", c_float * 12)]
+
+
+class AABB(Structure):
+    _fields_ = [("min", Vec3), ("max", Vec3)]
+
+
+class NormalDistFunction(IntEnum):
+    BECKMANN = 0
+    GGX = 1
+    COSINE = 2
+
+
+class ShadowingModel(IntEnum):
+    VCAVITY = 0
+    SMITH = 1
+
+
+class MaterialParamType(IntEnum):
+    EMISSIVE = 0
+    LAMBERT = 1
+    ORENNAYAR = 2
+    TORRANCE = 3
+    WALTER = 4
+    BLEND = 5
+    FRESNEL = 6
+    MICROFACET = 7
+
+
+class LightType(IntEnum):
+    POINT = 0
+    SPOT = 1
+    DIRECTIONAL = 2
+    ENVMAP = 3
+
+
+class BackgroundType(IntEnum):
+    MONOCHROME = 0
+    ENVMAP = 1
+    SKY_HOSEK = 2
+
+
+class Device(IntEnum):
+    CPU = 1
+    CUDA = 2
+    OPENGL = 4
+
+
+class LogLevel(IntEnum):
+    PEDANTIC = 0
+    INFO = 1
+    WARNING = 2
+    ERROR = 3
+    FATAL_ERROR = 4
+
+
+class Medium(Structure):
+    _fields_ = [("refractionIndex", Vec2), ("absorption", Vec3)]
+
+
+class LambertParams(Structure):
+    _fields_ = [("albedo", c_void_p)]
+
+
+class TorranceParams(Structure):
+    _fields_ = [("roughness", c_void_p), ("shadowingModel", c_int), ("ndf", c_int), ("albedo", c_void_p)]
+
+
+class WalterParams(Structure):
+    _fields_ = [("roughness", c_void_p), ("shadowingModel", c_int), ("ndf", c_int), ("absorption", Vec3),
+                ("refractionIndex", c_float)]
+
+
+class EmissiveParams(Structure):
+    _fields_ = [("radiance", c_void_p), ("scale", Vec3)]
+
+
+class OrennayarParams(Structure):
+    _fields_ = [("albedo", c_void_p), ("roughness", c_float)]
+
+
+class BlendLayer(Structure):
+    _fields_ = [("factor", c_float), ("mat", c_void_p)]
+
+
+class BlendParams(Structure):
+    _fields_ = [("a", BlendLayer), ("b", BlendLayer)]
+
+
+class FresnelParams(Structure):
+    _fields_ = [("refractionIndex", Vec2), ("a", c_void_p), ("b", c_void_p)]
+
+
+class MaterialParamsDisplacement(Structure):
+    _fields_ = [("map", c_void_p), ("maxMips", c_void_p), ("bias", c_float), ("scale", c_float)]
+
+
+class _MaterialInner(Union):
+    _fields_ = [("lambert", LambertParams), ("torrance", TorranceParams), ("walter", WalterParams),
+                ("emissive", EmissiveParams), ("orennayar", OrennayarParams), ("blend", BlendParams),
+                ("fresnel", FresnelParams)]
+
+
+class MaterialParams(Structure):
+    _fields_ = [("outerMedium", Medium), ("innerType", c_int), ("alpha", c_void_p),
+                ("displacement", MaterialParamsDisplacement), ("inner", _MaterialInner)]
+
+
+class LightHdl(Structure):
+    _fields_ = [("type", c_uint32, 3), ("index", c_uint32, 29)]
+
+
+class _BulkDescriptor(Union):
+    _fields_ = [("file", c_void_p), ("bytes", c_void_p)]
+
+
+class BulkLoader(Structure):
+    _fields_ = [("type", c_int), ("descriptor", _BulkDescriptor)]
+
+
+class MufflonRenderStats(Structure):
+    _fields_ = [("rays", c_uint64), ("shadowRays", c_uint64), ("nodeVisits", c_uint64), ("primTests", c_uint64),
+                ("instanceVisits", c_uint64), ("errors", c_uint32), ("kernelMs", c_float)]
+
+
+def _bulk(a: np.ndarray) -> BulkLoader:
+    b = BulkLoader()
+    b.type = 1  # BULK_ARRAY
+    b.descriptor.bytes = a.ctypes.data
+    return b
+
+
+def _ptr(a):
+    return a.ctypes.data_as(c_void_p) if a is not None and a.size else None
+
+
+class DllHolder:
+    """Loads the library and declares the C signatures."""
+
+    def __init__(self, binary_path=None):
+        path = binary_path or os.environ.get("MUFFLON_CORE_LIB", DEFAULT_LIB)
+        if not os.path.exists(path):
+            raise RuntimeError(f"libmufflon_core.so not built ({path}); run mufflon_b200.build.build()")
+        self.path = path
+        self.core = ctypes.CDLL(path)
+        c = self.core
+        sig = {
+            "core_get_dll_error": (c_char_p, []),
+            "core_set_log_level": (c_uint32, [c_int32]),
+            "mufflon_initialize": (c_void_p, []),
+            "mufflon_destroy": (None, [c_void_p]),
+            "mufflon_is_cuda_available": (c_uint32, []),
+            "mufflon_get_cuda_device_index": (c_int32, []),
+            "mufflon_get_target_image": (c_uint32, [c_void_p, c_char_p, c_uint32, POINTER(POINTER(c_float))]),
+            "mufflon_get_target_image_num_channels": (c_uint32, [c_void_p, POINTER(c_int)]),
+            "world_clear_all": (None, [c_void_p]),
+            "world_create_object": (c_void_p, [c_void_p, c_char_p, c_int]),
+            "object_add_lod": (c_void_p, [c_void_p, c_uint32, c_uint32]),
+            "polygon_add_vertex": (c_int32, [c_void_p, Vec3, Vec3, Vec2]),
+            "polygon_add_triangle_material": (c_int32, [c_void_p, UVec3, c_uint16]),
+            "polygon_add_quad_material": (c_int32, [c_void_p, UVec4, c_uint16]),
+            "polygon_add_vertex_bulk": (c_int32, [c_void_p, c_size_t, POINTER(BulkLoader), POINTER(BulkLoader),
+                                                  POINTER(BulkLoader), c_void_p, POINTER(c_size_t),
+                                                  POINTER(c_size_t), POINTER(c_size_t)]),
+            "polygon_add_triangle_bulk": (c_int32, [c_void_p, c_size_t, c_void_p, c_void_p]),
+            "polygon_add_quad_bulk": (c_int32, [c_void_p, c_size_t, c_void_p, c_void_p]),
+            "spheres_add_sphere_bulk": (c_int32, [c_void_p, c_size_t, POINTER(BulkLoader), c_void_p, POINTER(c_size_t)]),
+            "spheres_set_material_idx_bulk": (c_size_t, [c_void_p, c_int32, c_size_t, POINTER(BulkLoader)]),
+            "world_create_instance": (c_void_p, [c_void_p, c_void_p, c_uint32]),
+            "instance_set_transformation_matrix": (c_uint32, [c_void_p, c_void_p, POINTER(Mat3x4), c_uint32]),
+            "world_add_material": (c_void_p, [c_void_p, c_char_p, POINTER(MaterialParams)]),
+            "world_add_texture_value": (c_void_p, [c_void_p, POINTER(c_float), c_int, c_int]),
+            "world_add_texture_rgba32f": (c_void_p, [c_void_p, c_char_p, c_uint32, c_uint32, c_void_p, c_int]),
+            "world_add_pinhole_camera": (c_void_p, [c_void_p, c_char_p, POINTER(Vec3), POINTER(Vec3), POINTER(Vec3),
+                                                    c_uint32, c_float, c_float, c_float]),
+            "world_get_camera": (c_void_p, [c_void_p, c_char_p]),
+            "world_create_scenario": (c_void_p, [c_void_p, c_char_p]),
+            "world_find_scenario": (c_void_p, [c_void_p, c_char_p]),
+            "world_get_current_scenario": (c_void_p, [c_void_p]),
+            "world_finalize_scenario": (c_uint32, [c_void_p, c_void_p, POINTER(c_char_p)]),
+            "world_load_scenario": (c_void_p, [c_void_p, c_void_p]),
+            "scenario_set_resolution": (c_uint32, [c_void_p, c_uint32, c_uint32]),
+            "scenario_set_camera": (c_uint32, [c_void_p, c_void_p, c_void_p]),
+            "scenario_mask_instance": (c_uint32, [c_void_p, c_void_p]),
+            "scenario_add_light": (c_uint32, [c_void_p, c_void_p, LightHdl]),
+            "scenario_declare_material_slot": (c_uint16, [c_void_p, c_char_p, c_size_t]),
+            "scenario_assign_material": (c_uint32, [c_void_p, c_uint16, c_void_p]),
+            "world_add_light": (LightHdl, [c_void_p, c_char_p, c_int, c_uint32]),
+            "world_add_background_light": (LightHdl, [c_void_p, c_char_p, c_int]),
+            "world_set_point_light_position": (c_uint32, [c_void_p, LightHdl, Vec3, c_uint32]),
+            "world_set_point_light_intensity": (c_uint32, [c_void_p, LightHdl, Vec3, c_uint32]),
+            "world_set_env_light_color": (c_uint32, [c_void_p, LightHdl, Vec3]),
+            "world_set_env_light_scale": (c_uint32, [c_void_p, LightHdl, Vec3]),
+            "render_get_renderer_count": (c_uint32, [c_void_p]),
+            "render_get_renderer_variations": (c_uint32, [c_void_p, c_uint32]),
+            "render_get_renderer_name": (c_char_p, [c_void_p, c_uint32]),
+            "render_get_renderer_short_name": (c_char_p, [c_void_p, c_uint32]),
+            "render_get_renderer_devices": (c_uint32, [c_void_p, c_uint32, c_uint32]),
+            "render_enable_renderer": (c_uint32, [c_void_p, c_uint32, c_uint32]),
+            "render_iterate": (c_uint32, [c_void_p, POINTER(ProcessTime), POINTER(ProcessTime), POINTER(ProcessTime)]),
+            "render_get_current_iteration": (c_uint32, [c_void_p]),
+            "render_reset": (c_uint32, [c_void_p]),
+            "render_save_screenshot": (c_uint32, [c_void_p, c_char_p, c_char_p, c_uint32]),
+            "render_get_render_target_count": (c_uint32, [c_void_p]),
+            "render_get_render_target_name": (c_char_p, [c_void_p, c_uint32]),
+            "render_enable_render_target": (c_uint32, [c_void_p, c_char_p, c_uint32]),
+            "render_disable_render_target": (c_uint32, [c_void_p, c_char_p, c_uint32]),
+            "render_is_render_target_enabled": (c_uint32, [c_void_p, c_char_p, c_uint32]),
+            "renderer_get_num_parameters": (c_uint32, [c_void_p]),
+            "renderer_get_parameter_desc": (c_char_p, [c_void_p, c_uint32, POINTER(c_int)]),
+            "renderer_set_parameter_int": (c_uint32, [c_void_p, c_char_p, c_int32]),
+            "renderer_get_parameter_int": (c_uint32, [c_void_p, c_char_p, POINTER(c_int32)]),
+            "renderer_set_parameter_float": (c_uint32, [c_void_p, c_char_p, c_float]),
+            "renderer_set_parameter_bool": (c_uint32, [c_void_p, c_char_p, c_uint32]),
+            "renderer_set_parameter_enum": (c_uint32, [c_void_p, c_char_p, c_int32]),
+            "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
+            "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
+                                              c_void_p, c_void_p]),
+            "mufflon_trace_occlusion": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+            "mufflon_get_bvh": (c_uint32, [c_void_p, c_int32, POINTER(c_int32), POINTER(c_int32), c_void_p, c_void_p]),
+            "mufflon_lbvh_build": (c_uint32, [c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32,
+                                              c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int32), c_void_p]),
+            "mufflon_lbvh_build_device": (c_uint32, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32,
+                                                     c_void_p, POINTER(c_int32), POINTER(c_float), c_void_p]),
+            "mufflon_sort_pairs": (c_uint32, [c_void_p, c_void_p, c_uint32]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(c, name)
+            f.restype = res
+            f.argtypes = args
+
+
+class MufflonError(RuntimeError):
+    pass
+
+
+class DllInterface:
+    """One method per C function (names as in Mufflon's bindings.py)."""
+
+    def __init__(self, binary_path=None, useLoader=False):
+        self.dllHolder = DllHolder(binary_path)
+        self.core = self.dllHolder.core
+        if not self.core.mufflon_is_cuda_available():
+            raise MufflonError("no CUDA device available; the B200 core has no CPU fallback")
+        self.muffInst = self.core.mufflon_initialize()
+        if not self.muffInst:
+            raise MufflonError("mufflon_initialize failed: " + self.core_get_dll_error())
+
+    def __del__(self):
+        try:
+            if getattr(self, "muffInst", None):
+                self.core.mufflon_destroy(self.muffInst)
+                self.muffInst = None
+        except Exception:
+            pass
+
+    def close(self):
+        self.__del__()
+
+    def _check(self, ok, what):
+        if not ok:
+            raise MufflonError(f"{what} failed: {self.core_get_dll_error()}")
+        return ok
+
+    def core_get_dll_error(self):
+        e = self.core.core_get_dll_error()
+        return e.decode() if e else ""
+
+    def core_set_log_level(self, logLevel):
+        return self.core.core_set_log_level(int(logLevel)) != 0
+
+    def world_clear_all(self):
+        self.core.world_clear_all(self.muffInst)
+
+    def renderer_set_parameter_bool(self, parameterName, value):
+        return self.core.renderer_set_parameter_bool(self.muffInst, parameterName.encode(), 1 if value else 0) != 0
+
+    def renderer_set_parameter_float(self, parameterName, value):
+        return self.core.renderer_set_parameter_float(self.muffInst, parameterName.encode(), value) != 0
+
+    def renderer_set_parameter_int(self, parameterName, value):
+        return self.core.renderer_set_parameter_int(self.muffInst, parameterName.encode(), int(value)) != 0
+
+    def renderer_get_parameter_int(self, parameterName):
+        v = c_int32(0)
+        self._check(self.core.renderer_get_parameter_int(self.muffInst, parameterName.encode(), byref(v)), "renderer_get_parameter_int")
+        return v.value
+
+    def renderer_set_parameter_enum(self, parameterName, value):
+        return self.core.renderer_set_parameter_enum(self.muffInst, parameterName.encode(), int(value)) != 0
+
+    def render_iterate(self):
+        iterateTime, preTime, postTime = ProcessTime(0, 0), ProcessTime(0, 0), ProcessTime(0, 0)
+        self._check(self.core.render_iterate(self.muffInst, byref(iterateTime), byref(preTime), byref(postTime)),
+                    "render_iterate")
+        return iterateTime, preTime, postTime
+
+    def render_reset(self):
+        return self.core.render_reset(self.muffInst) != 0
+
+    def render_get_current_iteration(self):
+        return self.core.render_get_current_iteration(self.muffInst)
+
+    def render_save_screenshot(self, fileName, targetName, variance):
+        return self.core.render_save_screenshot(self.muffInst, fileName.encode(), targetName.encode(), int(variance)) != 0
+
+    def render_get_render_target_count(self):
+        return self.core.render_get_render_target_count(self.muffInst)
+
+    def render_get_render_target_name(self, index):
+        return self.core.render_get_render_target_name(self.muffInst, index).decode()
+
+    def render_is_render_target_enabled(self, targetName, variance):
+        return self.core.render_is_render_target_enabled(self.muffInst, targetName.encode(), int(variance)) != 0
+
+    def render_enable_render_target(self, targetName, variance):
+        return self.core.render_enable_render_target(self.muffInst, targetName.encode(), int(variance)) != 0
+
+    def render_disable_render_target(self, targetName, variance):
+        return self.core.render_disable_render_target(self.muffInst, targetName.encode(), int(variance)) != 0
+
+    def render_enable_renderer(self, rendererIndex, variation):
+        return self.core.render_enable_renderer(self.muffInst, rendererIndex, variation) != 0
+
+    def render_get_renderer_count(self):
+        return self.core.render_get_renderer_count(self.muffInst)
+
+    def render_get_renderer_variations(self, index):
+        return self.core.render_get_renderer_variations(self.muffInst, index)
+
+    def render_get_renderer_name(self, rendererIndex):
+        return self.core.render_get_renderer_name(self.muffInst, rendererIndex).decode()
+
+    def render_get_renderer_short_name(self, rendererIndex):
+        return self.core.render_get_renderer_short_name(self.muffInst, rendererIndex).decode()
+
+    def render_get_renderer_devices(self, rendererIndex, variation):
+        return self.core.render_get_renderer_devices(self.muffInst, rendererIndex, variation)
+
+    def world_find_scenario(self, name):
+        return self.core.world_find_scenario(self.muffInst, name.encode())
+
+    def world_load_scenario(self, hdl):
+        return self.core.world_load_scenario(self.muffInst, hdl)
+
+    def world_get_current_scenario(self):
+        return self.core.world_get_current_scenario(self.muffInst)
+
+    def world_get_camera(self, name):
+        return self.core.world_get_camera(self.muffInst, name.encode())
+
+    def scenario_set_camera(self, scenario, cam):
+        return self.core.scenario_set_camera(self.muffInst, scenario, cam) != 0
+
+    def instance_set_transformation_matrix(self, instHdl, mat, isWorldToInst):
+        return self.core.instance_set_transformation_matrix(self.muffInst, instHdl, byref(mat), int(isWorldToInst)) != 0
+
+    # -- image readback
+    def get_target_image(self, targetName: str) -> np.ndarray:
+        """Cumulative mean of a target as (height, width, channels) float32, y = 0 first."""
+        p = POINTER(c_float)()
+        self._check(self.core.mufflon_get_target_image(self.muffInst, targetName.encode(), 0, byref(p)),
+                    "mufflon_get_target_image")
+        ch = c_int(0)
+        self.core.mufflon_get_target_image_num_channels(self.muffInst, byref(ch))
+        if not p:
+            return None
+        w, h = self.resolution
+        return np.ctypeslib.as_array(p, shape=(h * w * ch.value,)).reshape(h, w, ch.value).copy()
+
+    # -- extensions
+    def render_stats(self):
+        s = MufflonRenderStats()
+        self._check(self.core.mufflon_get_render_stats(self.muffInst, byref(s)), "mufflon_get_render_stats")
+        return {k: getattr(s, k) for k, _ in MufflonRenderStats._fields_}
+
+    def trace_rays(self, rays, tmax=1048576.0, geo_normals=None):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        t = np.zeros(n, np.float32)
+        inst = np.zeros(n, np.int32)
+        prim = np.zeros(n, np.int32)
+        sp = np.zeros((n, 2), np.float32)
+        g = None if geo_normals is None else np.ascontiguousarray(geo_normals, np.float32)
+        self._check(self.core.mufflon_trace_rays(self.muffInst, _ptr(rays), _ptr(g), tmax, n, _ptr(t), _ptr(inst),
+                                                 _ptr(prim), _ptr(sp)), "mufflon_trace_rays")
+        return t, inst, prim, sp
+
+    def trace_occlusion(self, a, b):
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        occ = np.zeros(len(a), np.uint8)
+        self._check(self.core.mufflon_trace_occlusion(self.muffInst, _ptr(a), _ptr(b), len(a), _ptr(occ)),
+                    "mufflon_trace_occlusion")
+        return occ.astype(bool)
+
+    def get_bvh(self, which: int):
+        n, ni = c_int32(0), c_int32(0)
+        self._check(self.core.mufflon_get_bvh(self.muffInst, which, byref(n), byref(ni), None, None), "mufflon_get_bvh")
+        nodes = np.zeros((2 * ni.value, 8), np.float32)
+        prim = np.zeros(n.value, np.int32)
+        self._check(self.core.mufflon_get_bvh(self.muffInst, which, byref(n), byref(ni), _ptr(nodes), _ptr(prim)),
+                    "mufflon_get_bvh")
+        return nodes, prim, ni.value
+
+
+def lbvh_build(dll: DllInterface, lod):
+    """GPU LBVH build of one LodSpec: (morton_sorted, parents, nodes, prim_ids, num_internal, stage_ms)."""
+    idx = np.concatenate([lod.triangles.reshape(-1), lod.quads.reshape(-1)]).astype(np.uint32)
+    v = np.ascontiguousarray(lod.vertices, np.float32)
+    s = np.ascontiguousarray(lod.spheres, np.float32)
+    n = lod.num_prims
+    morton = np.zeros(max(n, 1), np.uint64)
+    parents = np.zeros(max(2 * n - 1, 1), np.int32)
+    nodes = np.zeros((max(2 * (n - 1), 1), 8), np.float32)
+    prim = np.zeros(max(n, 1), np.int32)
+    ni = c_int32(0)
+    ms = np.zeros(8, np.float32)
+    ok = dll.core.mufflon_lbvh_build(_ptr(v), len(v), _ptr(idx), len(lod.triangles), len(lod.quads), _ptr(s), len(s),
+                                     _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim), byref(ni), _ptr(ms))
+    dll._check(ok, "mufflon_lbvh_build")
+    return morton[:n], parents[:max(2 * n - 1, 0)], nodes[:2 * ni.value], prim[:n], ni.value, ms
+
+
+def sort_pairs(dll: DllInterface, keys: np.ndarray, values: np.ndarray):
+    k = np.ascontiguousarray(keys, np.uint64).copy()
+    v = np.ascontiguousarray(values, np.int32).copy()
+    dll._check(dll.core.mufflon_sort_pairs(_ptr(k), _ptr(v), len(k)), "mufflon_sort_pairs")
+    return k, v
+
+
+def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
+    """Builds a SceneSpec through the world-building C API and loads it."""
+    core, I = dll.core, dll.muffInst
+    keep = []
+    sc = core.world_create_scenario(I, (scenario_name or spec.name).encode())
+    dll._check(sc, "world_create_scenario")
+
+    def tex_value(vals):
+        arr = (c_float * len(vals))(*[float(x) for x in vals])
+        t = core.world_add_texture_value(I, arr, len(vals), 0)
+        dll._check(t, "world_add_texture_value")
+        return t
+
+    textures = []
+    for k, tex in enumerate(spec.textures):
+        a = np.ascontiguousarray(tex, np.float32)
+        keep.append(a)
+        t = core.world_add_texture_rgba32f(I, f"texture{k}".encode(), a.shape[1], a.shape[0], _ptr(a), 0)
+        dll._check(t, "world_add_texture_rgba32f")
+        textures.append(t)
+    for i, m in enumerate(spec.materials):
+        name = f"mat{i}".encode()
+        slot = core.scenario_declare_material_slot(sc, name, len(name))
+        p = MaterialParams()
+        p.outerMedium.refractionIndex.u = 1.0
+        if m.type == 0:
+            p.innerType = MaterialParamType.LAMBERT
+            p.inner.lambert.albedo = textures[m.albedo_texture] if m.albedo_texture >= 0 else tex_value(m.albedo)
+        elif m.type == 1:
+            p.innerType = MaterialParamType.TORRANCE
+            p.inner.torrance.albedo = textures[m.albedo_texture] if m.albedo_texture >= 0 else tex_value(m.albedo)
+            p.inner.torrance.roughness = tex_value(m.roughness)
+            p.inner.torrance.shadowingModel = ShadowingModel.SMITH
+            p.inner.torrance.ndf = NormalDistFunction.GGX
+        else:
+            p.innerType = MaterialParamType.EMISSIVE
+            p.inner.emissive.radiance = tex_value(m.radiance)
+            p.inner.emissive.scale = Vec3(*m.scale)
+        mh = core.world_add_material(I, name, byref(p))
+        dll._check(mh, "world_add_material")
+        dll._check(core.scenario_assign_material(sc, slot, mh), "scenario_assign_material")
+    objs = []
+    for li, lod in enumerate(spec.lods):
+        obj = core.world_create_object(I, lod.name.encode(), 0)
+        dll._check(obj, "world_create_object")
+        lh = core.object_add_lod(obj, 0, 0)
+        dll._check(lh, "object_add_lod")
+        nv = len(lod.vertices)
+        if nv:
+            pts = np.ascontiguousarray(lod.vertices, np.float32)
+            nrm = np.ascontiguousarray(lod.normals, np.float32)
+            uvs = np.ascontiguousarray(lod.uvs, np.float32)
+            keep += [pts, nrm, uvs]
+            bp, bn, bu = _bulk(pts), _bulk(nrm), _bulk(uvs)
+            r = core.polygon_add_vertex_bulk(lh, nv, byref(bp), byref(bn), byref(bu), None, None, None, None)
+            dll._check(r >= 0, "polygon_add_vertex_bulk")
+        fm = np.ascontiguousarray(lod.face_materials, np.uint16)
+        nt, nq = len(lod.triangles), len(lod.quads)
+        if nt:
+            t = np.ascontiguousarray(lod.triangles, np.uint32)
+            dll._check(core.polygon_add_triangle_bulk(lh, nt, _ptr(t), _ptr(fm[:nt].copy())) >= 0, "polygon_add_triangle_bulk")
+        if nq:
+            q = np.ascontiguousarray(lod.quads, np.uint32)
+            dll._check(core.polygon_add_quad_bulk(lh, nq, _ptr(q), _ptr(fm[nt:].copy())) >= 0, "polygon_add_quad_bulk")
+        ns = len(lod.spheres)
+        if ns:
+            sph = np.ascontiguousarray(lod.spheres, np.float32)
+            sm = np.ascontiguousarray(lod.sphere_materials, np.uint16)
+            keep += [sph, sm]
+            bs = _bulk(sph)
+            dll._check(core.spheres_add_sphere_bulk(lh, ns, byref(bs), None, None) >= 0, "spheres_add_sphere_bulk")
+            bm = _bulk(sm)
+            dll._check(core.spheres_set_material_idx_bulk(lh, 0, ns, byref(bm)) == ns, "spheres_set_material_idx_bulk")
+        objs.append(obj)
+    for i in range(len(spec.instance_lod)):
+        li = int(spec.instance_lod[i])
+        masked = li == 0xFFFFFFFF
+        ih = core.world_create_instance(I, objs[0 if masked else li], 0)
+        dll._check(ih, "world_create_instance")
+        m = Mat3x4()
+        m.v[:] = [float(x) for x in spec.world_to_instance[i]]
+        dll._check(core.instance_set_transformation_matrix(I, ih, byref(m), 1), "instance_set_transformation_matrix")
+        if masked:
+            core.scenario_mask_instance(sc, ih)
+    cam = core.world_add_pinhole_camera(I, b"camera", byref(Vec3(*spec.cam_pos)), byref(Vec3(*spec.cam_dir)),
+                                        byref(Vec3(*spec.cam_up)), 1, 1e-4, 1e10, spec.vfov)
+    dll._check(cam, "world_add_pinhole_camera")
+    dll._check(core.scenario_set_camera(I, sc, cam), "scenario_set_camera")
+    dll._check(core.scenario_set_resolution(sc, spec.width, spec.height), "scenario_set_resolution")
+    for k, pl in enumerate(spec.point_lights):
+        h = core.world_add_light(I, f"point{k}".encode(), LightType.POINT, 1)
+        core.world_set_point_light_position(I, h, Vec3(*pl[:3]), 0)
+        core.world_set_point_light_intensity(I, h, Vec3(*pl[3:]), 0)
+        dll._check(core.scenario_add_light(I, sc, h), "scenario_add_light")
+    if spec.background is not None:
+        h = core.world_add_background_light(I, b"background", BackgroundType.MONOCHROME)
+        core.world_set_env_light_color(I, h, Vec3(*spec.background[0]))
+        core.world_set_env_light_scale(I, h, Vec3(*spec.background[1]))
+        dll._check(core.scenario_add_light(I, sc, h), "scenario_add_light")
+    msg = c_char_p()
+    dll._check(core.world_finalize_scenario(I, sc, byref(msg)), "world_finalize_scenario")
+    dll._check(core.world_load_scenario(I, sc), "world_load_scenario")
+    dll.resolution = (spec.width, spec.height)
+    return sc
+
+
+class RenderActions:
+    """Convenience layer with the method names of Mufflon's RenderActions."""
+
+    def __init__(self, binary_path=None, useLoader=False):
+        self.dllInterface = DllInterface(binary_path)
+        self.activeRendererName = ""
+        self.sceneName = ""
+
+    def load_spec(self, spec, defaultRenderTarget="Radiance"):
+        self.sceneName = spec.name
+        load_scene_spec(self.dllInterface, spec)
+        self.enable_render_target(defaultRenderTarget, False)
+
+    def enable_renderer(self, rendererName, devices):
+        d = self.dllInterface
+        for i in range(d.render_get_renderer_count()):
+            name = d.render_get_renderer_name(i)
+            short = d.render_get_renderer_short_name(i)
+            if name.lower() == rendererName.lower() or short.lower() == rendererName.lower():
+                for v in range(d.render_get_renderer_variations(i)):
+                    if int(devices) == d.render_get_renderer_devices(i, v):
+                        self.activeRendererName = rendererName
+                        d.render_enable_renderer(i, v)
+                        return
+        raise MufflonError(f"Could not find renderer '{rendererName}' for the devices {devices}")
+
+    def load_scenario(self, scenarioName):
+        d = self.dllInterface
+        hdl = d.world_find_scenario(scenarioName)
+        if not hdl:
+            raise MufflonError(f"Failed to find scenario '{scenarioName}'")
+        if not d.world_load_scenario(hdl):
+            raise MufflonError(f"Failed to load scenario '{scenarioName}'")
+
+    def enable_render_target(self, targetName, variance):
+        if not self.dllInterface.render_enable_render_target(targetName, variance):
+            raise MufflonError(f"Failed to enable render target {targetName} (variance: {variance})")
+
+    def disable_render_target(self, targetName, variance):
+        if not self.dllInterface.render_disable_render_target(targetName, variance):
+            raise MufflonError(f"Failed to disable render target {targetName} (variance: {variance})")
+
+    def renderer_set_parameter_int(self, parameterName, value):
+        return self.dllInterface.renderer_set_parameter_int(parameterName, value)
+
+    def renderer_set_parameter_bool(self, parameterName, value):
+        return self.dllInterface.renderer_set_parameter_bool(parameterName, value)
+
+    def render_reset(self):
+        self.dllInterface.render_reset()
+
+    def render_for_iterations(self, iterationCount, printProgress=False, progressSteps=1, takeScreenshot=False):
+        acc = ProcessTime(0, 0)
+        for i in range(iterationCount):
+            if printProgress and (i % progressSteps == 0):
+                print("--- ", (i + 1), " of ", iterationCount, " ---", flush=True)
+            it, _, _ = self.dllInterface.render_iterate()
+            acc.microseconds += it.microseconds
+        return acc
+
+    def get_target(self, targetName="Radiance"):
+        return self.dllInterface.get_target_image(targetName)

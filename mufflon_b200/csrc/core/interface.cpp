@@ -1,0 +1,1107 @@
+// C API of the B200 path-tracer core: the subset of
+// src/core/export/interface.cpp that builds a world, runs the "Pathtracer"
+// renderer and reads its targets back. Every function catches all
+// exceptions, logs, stores the message for core_get_dll_error() and returns
+// false / nullptr / INVALID_INDEX, as interface.cpp:53-83 does.
+#include "../../../include/mufflon_core.h"
+#include "world.hpp"
+#include "../trace/pt_api.hpp"
+
+#include <chrono>
+#include <cstdarg>
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace mb;
+
+namespace {
+
+thread_local std::string s_lastError;
+void (*s_logger)(const char*, int) = nullptr;
+int s_logLevel = LOG_INFO;
+
+void log_msg(int level, const std::string& msg) {
+	if(level < s_logLevel) return;
+	if(s_logger) s_logger(msg.c_str(), level);
+}
+
+struct ApiError : std::runtime_error { using std::runtime_error::runtime_error; };
+
+#define TRY try {
+#define CATCH_ALL(ret) } catch(const std::exception& ex) { s_lastError = std::string(__func__) + ": " + ex.what(); log_msg(LOG_ERROR, s_lastError); return ret; } \
+	catch(...) { s_lastError = std::string(__func__) + ": unknown error"; log_msg(LOG_ERROR, s_lastError); return ret; }
+#define CHECK(cond, msg) do { if(!(cond)) throw ApiError(msg); } while(0)
+#define CHECK_CUDA(expr) do { cudaError_t e_ = (expr); if(e_ != cudaSuccess) throw ApiError(std::string("CUDA: ") + cudaGetErrorString(e_)); } while(0)
+
+MufflonInstance& minst(void* h) {
+	if(!h) throw ApiError("invalid mufflon instance");
+	return *static_cast<MufflonInstance*>(h);
+}
+HostLod& mlod(void* h) {
+	if(!h) throw ApiError("invalid LoD handle");
+	return *static_cast<HostLod*>(h);
+}
+
+// Parameters of the path tracer (pt_params.hpp:8-14, parameter.hpp:327-365)
+// plus two extensions.
+struct ParamDesc { const char* name; ParameterType type; };
+const ParamDesc PT_PARAMS[] = {
+	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
+	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
+	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT },
+};
+// Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
+// implements Radiance and Hit ID; the others are recognised names.
+const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
+
+int32_t* param_ptr(RendererState& r, const char* name) {
+	if(!std::strcmp(name, "Seed")) return &r.params.seed;
+	if(!std::strcmp(name, "Min. path length")) return &r.params.minPathLength;
+	if(!std::strcmp(name, "Max. path length")) return &r.params.maxPathLength;
+	if(!std::strcmp(name, "NEE count")) return &r.params.neeCount;
+	if(!std::strcmp(name, "RR start depth")) return &r.params.rrStartDepth;
+	if(!std::strcmp(name, "Blocks per SM")) return &r.blocksPerSm;
+	return nullptr;
+}
+
+size_t read_bulk(const BulkLoader* b, void* dst, size_t bytes) {
+	if(!b) return 0;
+	if(b->type == BULK_ARRAY) { std::memcpy(dst, b->descriptor.bytes, bytes); return bytes; }
+	return std::fread(dst, 1, bytes, b->descriptor.file);
+}
+
+void ensure_render_buffers(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	HostScenario* sc = I.current;
+	CHECK(sc != nullptr, "no scenario loaded");
+	if(r.width == sc->width && r.height == sc->height && r.rng) return;
+	r.release();
+	r.width = sc->width; r.height = sc->height;
+	const size_t n = size_t(r.width) * r.height;
+	CHECK_CUDA(cudaMalloc(&r.rng, n * sizeof(uint64_t)));
+	CHECK_CUDA(cudaMalloc(&r.radiance, n * 3 * sizeof(float)));
+	CHECK_CUDA(cudaMalloc(&r.hitId, n * 2 * sizeof(float)));
+	CHECK_CUDA(cudaMalloc(&r.workCounter, sizeof(unsigned int)));
+	CHECK_CUDA(cudaMalloc(&r.counters, sizeof(TraceCounters)));
+	CHECK_CUDA(cudaEventCreate(&r.evStart));
+	CHECK_CUDA(cudaEventCreate(&r.evStop));
+	r.needsReset = true;
+}
+
+void load_scene_if_needed(MufflonInstance& I) {
+	if(!I.sceneDirty && I.scene.valid) return;
+	std::string err;
+	if(!build_device_scene(I, err)) throw ApiError(err);
+	I.sceneDirty = false;
+	I.renderer.needsReset = true;
+}
+
+} // namespace
+
+namespace mb {
+void RendererState::release() {
+	cudaFree(rng); cudaFree(radiance); cudaFree(hitId); cudaFree(workCounter); cudaFree(counters);
+	if(evStart) cudaEventDestroy(evStart);
+	if(evStop) cudaEventDestroy(evStop);
+	rng = nullptr; radiance = nullptr; hitId = nullptr; workCounter = nullptr; counters = nullptr;
+	evStart = evStop = nullptr;
+	width = height = 0;
+}
+MufflonInstance::~MufflonInstance() {
+	renderer.release();
+	scene.release();
+	if(stream) cudaStreamDestroy(stream);
+}
+} // namespace mb
+
+extern "C" {
+
+const char* core_get_dll_error(void) { return s_lastError.c_str(); }
+Boolean core_set_logger(void (*cb)(const char*, int)) { s_logger = cb; return true; }
+Boolean core_set_log_level(LogLevel level) { s_logLevel = int(level); return true; }
+
+// interface.cpp:4295-4414: pick the CUDA device with the highest compute capability.
+MufflonInstanceHdl mufflon_initialize(void) {
+	TRY
+	int count = 0;
+	CHECK_CUDA(cudaGetDeviceCount(&count));
+	CHECK(count > 0, "no CUDA device");
+	int best = 0, bestCc = -1;
+	for(int d = 0; d < count; ++d) {
+		cudaDeviceProp p;
+		CHECK_CUDA(cudaGetDeviceProperties(&p, d));
+		const int cc = p.major * 100 + p.minor;
+		if(p.unifiedAddressing && cc > bestCc) { best = d; bestCc = cc; }
+	}
+	CHECK_CUDA(cudaSetDevice(best));
+	auto* I = new MufflonInstance();
+	I->device = best;
+	CHECK_CUDA(cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking));
+	return I;
+	CATCH_ALL(nullptr)
+}
+
+void mufflon_destroy(MufflonInstanceHdl h) {
+	TRY
+	delete static_cast<MufflonInstance*>(h);
+	CATCH_ALL()
+}
+
+int32_t mufflon_get_cuda_device_index(void) {
+	int d = -1;
+	if(cudaGetDevice(&d) != cudaSuccess) return -1;
+	return d;
+}
+Boolean mufflon_is_cuda_available(void) {
+	int count = 0;
+	return cudaGetDeviceCount(&count) == cudaSuccess && count > 0;
+}
+
+// interface.cpp:241-262: a library-owned copy of the cumulative target
+Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean variance, const float** ptr) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(I.renderer.enabled, "no renderer enabled");
+	CHECK(name != nullptr, "target name is null");
+	CHECK(!variance, "variance targets are not recorded by this renderer");
+	RendererState& r = I.renderer;
+	if(!r.rng || r.iteration < 0) { if(ptr) *ptr = nullptr; return true; }
+	const size_t n = size_t(r.width) * r.height;
+	if(!std::strcmp(name, "Radiance")) {
+		CHECK(r.targetRadiance, "target 'Radiance' is not enabled");
+		r.screen.resize(n * 3);
+		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		r.screenChannels = 3;
+	} else if(!std::strcmp(name, "Hit ID")) {
+		CHECK(r.targetHitId, "target 'Hit ID' is not enabled");
+		r.screen.resize(n * 2);
+		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		r.screenChannels = 2;
+	} else {
+		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA path tracer");
+	}
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	if(ptr) *ptr = r.screen.data();
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_get_target_image_num_channels(MufflonInstanceHdl h, int* numChannels) {
+	TRY
+	MufflonInstance& I = minst(h);
+	if(numChannels) *numChannels = I.renderer.screenChannels;
+	return true;
+	CATCH_ALL(false)
+}
+
+void world_clear_all(MufflonInstanceHdl h) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	I.scene.release();
+	I.objects.clear(); I.instances.clear(); I.materials.clear(); I.textures.clear(); I.cameras.clear();
+	I.pointLights.clear(); I.backgrounds.clear(); I.scenarios.clear(); I.current = nullptr;
+	I.sceneDirty = true;
+	I.renderer.needsReset = true;
+	CATCH_ALL()
+}
+
+Boolean world_finalize(MufflonInstanceHdl h, const Vec3, const Vec3, const char** msg) {
+	TRY
+	MufflonInstance& I = minst(h);
+	if(msg) *msg = "";
+	CHECK(!I.cameras.empty(), "world has no camera");
+	return true;
+	CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- polygons
+Boolean polygon_reserve(LodHdl l, size_t v, size_t t, size_t q) {
+	TRY
+	HostLod& L = mlod(l);
+	L.vertices.reserve(3 * v); L.normals.reserve(3 * v); L.uvs.reserve(2 * v);
+	L.triIdx.reserve(3 * t); L.triMat.reserve(t); L.quadIdx.reserve(4 * q); L.quadMat.reserve(q);
+	return true;
+	CATCH_ALL(false)
+}
+
+VertexHdl polygon_add_vertex(LodHdl l, Vec3 p, Vec3 n, Vec2 uv) {
+	TRY
+	HostLod& L = mlod(l);
+	const VertexHdl idx = VertexHdl(L.num_vertices());
+	L.vertices.insert(L.vertices.end(), { p.x, p.y, p.z });
+	L.normals.insert(L.normals.end(), { n.x, n.y, n.z });
+	L.uvs.insert(L.uvs.end(), { uv.x, uv.y });
+	return idx;
+	CATCH_ALL(INVALID_INDEX)
+}
+
+static FaceHdl add_tri(HostLod& L, UVec3 v, MatIdx m) {
+	const uint32_t nv = L.num_vertices();
+	CHECK(v.x < nv && v.y < nv && v.z < nv, "triangle index out of range");
+	CHECK(L.quadMat.empty(), "triangles must be added before quads");
+	L.triIdx.insert(L.triIdx.end(), { v.x, v.y, v.z });
+	L.triMat.push_back(m);
+	return FaceHdl(L.num_triangles() - 1);
+}
+static FaceHdl add_quad(HostLod& L, UVec4 v, MatIdx m) {
+	const uint32_t nv = L.num_vertices();
+	CHECK(v.x < nv && v.y < nv && v.z < nv && v.w < nv, "quad index out of range");
+	L.quadIdx.insert(L.quadIdx.end(), { v.x, v.y, v.z, v.w });
+	L.quadMat.push_back(m);
+	return FaceHdl(L.num_triangles() + L.num_quads() - 1);
+}
+
+FaceHdl polygon_add_triangle(LodHdl l, UVec3 v) { TRY return add_tri(mlod(l), v, 0); CATCH_ALL(INVALID_INDEX) }
+FaceHdl polygon_add_triangle_material(LodHdl l, UVec3 v, MatIdx m) { TRY return add_tri(mlod(l), v, m); CATCH_ALL(INVALID_INDEX) }
+FaceHdl polygon_add_quad(LodHdl l, UVec4 v) { TRY return add_quad(mlod(l), v, 0); CATCH_ALL(INVALID_INDEX) }
+FaceHdl polygon_add_quad_material(LodHdl l, UVec4 v, MatIdx m) { TRY return add_quad(mlod(l), v, m); CATCH_ALL(INVALID_INDEX) }
+
+FaceHdl polygon_add_triangle_bulk(LodHdl l, size_t count, const UVec3* v, const MatIdx* m) {
+	TRY
+	HostLod& L = mlod(l);
+	CHECK(L.quadMat.empty(), "triangles must be added before quads");
+	const uint32_t nv = L.num_vertices();
+	const FaceHdl first = FaceHdl(L.num_triangles());
+	L.triIdx.reserve(L.triIdx.size() + 3 * count);
+	L.triMat.reserve(L.triMat.size() + count);
+	for(size_t i = 0; i < count; ++i) {
+		CHECK(v[i].x < nv && v[i].y < nv && v[i].z < nv, "triangle index out of range");
+		L.triIdx.insert(L.triIdx.end(), { v[i].x, v[i].y, v[i].z });
+		L.triMat.push_back(m ? m[i] : MatIdx(0));
+	}
+	return first;
+	CATCH_ALL(INVALID_INDEX)
+}
+
+FaceHdl polygon_add_quad_bulk(LodHdl l, size_t count, const UVec4* v, const MatIdx* m) {
+	TRY
+	HostLod& L = mlod(l);
+	const uint32_t nv = L.num_vertices();
+	const FaceHdl first = FaceHdl(L.num_triangles() + L.num_quads());
+	for(size_t i = 0; i < count; ++i) {
+		CHECK(v[i].x < nv && v[i].y < nv && v[i].z < nv && v[i].w < nv, "quad index out of range");
+		L.quadIdx.insert(L.quadIdx.end(), { v[i].x, v[i].y, v[i].z, v[i].w });
+		L.quadMat.push_back(m ? m[i] : MatIdx(0));
+	}
+	return first;
+	CATCH_ALL(INVALID_INDEX)
+}
+
+VertexHdl polygon_add_vertex_bulk(LodHdl l, size_t count, const BulkLoader* points, const BulkLoader* normals,
+                                  const BulkLoader* uvs, const AABB*, size_t* pr, size_t* nr, size_t* ur) {
+	TRY
+	HostLod& L = mlod(l);
+	CHECK(points != nullptr, "points stream is required");
+	const VertexHdl first = VertexHdl(L.num_vertices());
+	const size_t v0 = L.vertices.size(), n0 = L.normals.size(), u0 = L.uvs.size();
+	L.vertices.resize(v0 + 3 * count);
+	L.normals.resize(n0 + 3 * count, 0.0f);
+	L.uvs.resize(u0 + 2 * count, 0.0f);
+	const size_t a = read_bulk(points, L.vertices.data() + v0, 12 * count) / 12;
+	const size_t b = normals ? read_bulk(normals, L.normals.data() + n0, 12 * count) / 12 : 0;
+	const size_t c = uvs ? read_bulk(uvs, L.uvs.data() + u0, 8 * count) / 8 : 0;
+	if(pr) *pr = a;
+	if(nr) *nr = b;
+	if(ur) *ur = c;
+	CHECK(a == count, "short read of vertex positions");
+	return first;
+	CATCH_ALL(INVALID_INDEX)
+}
+
+Boolean polygon_set_material_idx(LodHdl l, FaceHdl f, MatIdx m) {
+	TRY
+	HostLod& L = mlod(l);
+	CHECK(f >= 0 && uint32_t(f) < L.num_triangles() + L.num_quads(), "face index out of range");
+	if(uint32_t(f) < L.num_triangles()) L.triMat[f] = m; else L.quadMat[f - L.num_triangles()] = m;
+	return true;
+	CATCH_ALL(false)
+}
+
+size_t polygon_set_material_idx_bulk(LodHdl l, FaceHdl start, size_t count, const BulkLoader* stream) {
+	TRY
+	HostLod& L = mlod(l);
+	std::vector<MatIdx> buf(count);
+	const size_t got = read_bulk(stream, buf.data(), count * sizeof(MatIdx)) / sizeof(MatIdx);
+	for(size_t i = 0; i < got; ++i) {
+		const size_t f = size_t(start) + i;
+		CHECK(f < L.num_triangles() + L.num_quads(), "face index out of range");
+		if(f < L.num_triangles()) L.triMat[f] = buf[i]; else L.quadMat[f - L.num_triangles()] = buf[i];
+	}
+	return got;
+	CATCH_ALL(size_t(-1))
+}
+
+size_t polygon_get_vertex_count(LodHdl l) { TRY return mlod(l).num_vertices(); CATCH_ALL(0) }
+size_t polygon_get_face_count(LodHdl l) { TRY return mlod(l).num_triangles() + mlod(l).num_quads(); CATCH_ALL(0) }
+size_t polygon_get_triangle_count(LodHdl l) { TRY return mlod(l).num_triangles(); CATCH_ALL(0) }
+size_t polygon_get_quad_count(LodHdl l) { TRY return mlod(l).num_quads(); CATCH_ALL(0) }
+Boolean polygon_get_bounding_box(LodHdl l, Vec3* mn, Vec3* mx) {
+	TRY
+	float a[3], b[3];
+	mlod(l).bounds(a, b);
+	if(mn) *mn = { a[0], a[1], a[2] };
+	if(mx) *mx = { b[0], b[1], b[2] };
+	return true;
+	CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- spheres
+Boolean spheres_reserve(LodHdl l, size_t c) { TRY mlod(l).spheres.reserve(4 * c); mlod(l).sphereMat.reserve(c); return true; CATCH_ALL(false) }
+SphereHdl spheres_add_sphere(LodHdl l, Vec3 p, float r) { return spheres_add_sphere_material(l, p, r, 0); }
+SphereHdl spheres_add_sphere_material(LodHdl l, Vec3 p, float r, MatIdx m) {
+	TRY
+	HostLod& L = mlod(l);
+	CHECK(r > 0.0f, "sphere radius must be positive");
+	L.spheres.insert(L.spheres.end(), { p.x, p.y, p.z, r });
+	L.sphereMat.push_back(m);
+	return SphereHdl(L.num_spheres() - 1);
+	CATCH_ALL(INVALID_INDEX)
+}
+SphereHdl spheres_add_sphere_bulk(LodHdl l, size_t count, const BulkLoader* stream, const AABB*, size_t* read) {
+	TRY
+	HostLod& L = mlod(l);
+	const SphereHdl first = SphereHdl(L.num_spheres());
+	const size_t s0 = L.spheres.size();
+	L.spheres.resize(s0 + 4 * count);
+	const size_t got = read_bulk(stream, L.spheres.data() + s0, 16 * count) / 16;
+	L.spheres.resize(s0 + 4 * got);
+	L.sphereMat.resize(L.sphereMat.size() + got, 0);
+	if(read) *read = got;
+	return first;
+	CATCH_ALL(INVALID_INDEX)
+}
+Boolean spheres_set_material_idx(LodHdl l, SphereHdl s, MatIdx m) {
+	TRY
+	HostLod& L = mlod(l);
+	CHECK(s >= 0 && uint32_t(s) < L.num_spheres(), "sphere index out of range");
+	L.sphereMat[s] = m;
+	return true;
+	CATCH_ALL(false)
+}
+size_t spheres_set_material_idx_bulk(LodHdl l, SphereHdl start, size_t count, const BulkLoader* stream) {
+	TRY
+	HostLod& L = mlod(l);
+	std::vector<MatIdx> buf(count);
+	const size_t got = read_bulk(stream, buf.data(), count * sizeof(MatIdx)) / sizeof(MatIdx);
+	for(size_t i = 0; i < got; ++i) {
+		CHECK(size_t(start) + i < L.num_spheres(), "sphere index out of range");
+		L.sphereMat[size_t(start) + i] = buf[i];
+	}
+	return got;
+	CATCH_ALL(size_t(-1))
+}
+size_t spheres_get_sphere_count(LodHdl l) { TRY return mlod(l).num_spheres(); CATCH_ALL(0) }
+Boolean spheres_get_bounding_box(LodHdl l, Vec3* mn, Vec3* mx) { return polygon_get_bounding_box(l, mn, mx); }
+
+// ---------------------------------------------------------------- objects / instances
+ObjectHdl world_create_object(MufflonInstanceHdl h, const char* name, ObjectFlags flags) {
+	TRY
+	MufflonInstance& I = minst(h);
+	auto o = std::make_unique<HostObject>();
+	o->name = name ? name : "";
+	o->flags = uint32_t(flags);
+	I.objects.push_back(std::move(o));
+	I.sceneDirty = true;
+	return I.objects.back().get();
+	CATCH_ALL(nullptr)
+}
+ObjectHdl world_get_object(MufflonInstanceHdl h, const char* name) {
+	TRY
+	for(auto& o : minst(h).objects) if(name && o->name == name) return o.get();
+	throw ApiError("object not found");
+	CATCH_ALL(nullptr)
+}
+const char* world_get_object_name(ObjectHdl o) { TRY CHECK(o, "invalid object"); return static_cast<HostObject*>(o)->name.c_str(); CATCH_ALL(nullptr) }
+Boolean object_has_lod(ConstObjectHdl o, LodLevel level) {
+	TRY CHECK(o, "invalid object"); return static_cast<const HostObject*>(o)->lods.count(level) > 0; CATCH_ALL(false)
+}
+LodHdl object_add_lod(ObjectHdl o, LodLevel level, Boolean) {
+	TRY
+	CHECK(o, "invalid object");
+	auto& slot = static_cast<HostObject*>(o)->lods[level];
+	if(!slot) slot = std::make_unique<HostLod>();
+	return slot.get();
+	CATCH_ALL(nullptr)
+}
+void world_reserve_objects_instances(MufflonInstanceHdl h, const uint32_t o, const uint32_t i) {
+	TRY minst(h).objects.reserve(o); minst(h).instances.reserve(i); CATCH_ALL()
+}
+InstanceHdl world_create_instance(MufflonInstanceHdl h, ObjectHdl obj, const uint32_t) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(obj, "invalid object");
+	auto inst = std::make_unique<HostInstance>();
+	inst->object = static_cast<HostObject*>(obj);
+	inst->index = uint32_t(I.instances.size());
+	I.instances.push_back(std::move(inst));
+	I.sceneDirty = true;
+	return I.instances.back().get();
+	CATCH_ALL(nullptr)
+}
+uint32_t world_get_instance_count(MufflonInstanceHdl h, const uint32_t) { TRY return uint32_t(minst(h).instances.size()); CATCH_ALL(0) }
+
+// instance_set_transformation_matrix: the stored matrix is world-to-instance;
+// an instance-to-world input is inverted exactly like
+// InstanceData::compute_instance_to_world_transformation (the inverse of an
+// affine 3x4 is the same formula in both directions).
+Boolean instance_set_transformation_matrix(MufflonInstanceHdl h, InstanceHdl inst, const Mat3x4* mat, const Boolean isWorldToInst) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(inst && mat, "invalid instance or matrix");
+	HostInstance& in = *static_cast<HostInstance*>(inst);
+	if(isWorldToInst) std::memcpy(in.worldToInstance, mat->v, sizeof(in.worldToInstance));
+	else {
+		const float* r = mat->v;
+		const float m00 = r[5] * r[10] - r[9] * r[6], m01 = r[9] * r[2] - r[1] * r[10], m02 = r[1] * r[6] - r[5] * r[2];
+		const float m10 = r[8] * r[6] - r[4] * r[10], m11 = r[0] * r[10] - r[8] * r[2], m12 = r[4] * r[2] - r[0] * r[6];
+		const float m20 = r[4] * r[9] - r[8] * r[5], m21 = r[8] * r[1] - r[0] * r[9], m22 = r[0] * r[5] - r[4] * r[1];
+		const float det = r[0] * m00 + r[1] * m10 + r[2] * m20;
+		CHECK(det != 0.0f, "singular transformation");
+		const float id = 1.0f / det;
+		float* o = in.worldToInstance;
+		const float i[9] = { id * m00, id * m01, id * m02, id * m10, id * m11, id * m12, id * m20, id * m21, id * m22 };
+		for(int row = 0; row < 3; ++row) {
+			o[4 * row] = i[3 * row]; o[4 * row + 1] = i[3 * row + 1]; o[4 * row + 2] = i[3 * row + 2];
+			o[4 * row + 3] = -(i[3 * row] * r[3] + i[3 * row + 1] * r[7] + i[3 * row + 2] * r[11]);
+		}
+	}
+	I.sceneDirty = true;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean instance_get_transformation_matrix(MufflonInstanceHdl h, InstanceHdl inst, Mat3x4* mat) {
+	TRY
+	(void)minst(h);
+	CHECK(inst && mat, "invalid instance or matrix");
+	std::memcpy(mat->v, static_cast<HostInstance*>(inst)->worldToInstance, sizeof(mat->v));
+	return true;
+	CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- materials / textures
+MaterialHdl world_add_material(MufflonInstanceHdl h, const char* name, const MaterialParams* p) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(p, "material parameters are null");
+	auto m = std::make_unique<HostMaterial>();
+	m->name = name ? name : "";
+	switch(p->innerType) {
+		case MATERIAL_LAMBERT:
+			m->type = MAT_LAMBERT;
+			m->albedo = static_cast<HostTexture*>(p->inner.lambert.albedo);
+			break;
+		case MATERIAL_TORRANCE:
+			CHECK(p->inner.torrance.ndf == NDF_GGX && p->inner.torrance.shadowingModel == SHADOWING_SMITH,
+			      "the CUDA path tracer implements Torrance with GGX and Smith shadowing");
+			m->type = MAT_TORRANCE;
+			m->albedo = static_cast<HostTexture*>(p->inner.torrance.albedo);
+			m->roughness = static_cast<HostTexture*>(p->inner.torrance.roughness);
+			break;
+		case MATERIAL_EMISSIVE:
+			m->type = MAT_EMISSIVE;
+			m->radiance = static_cast<HostTexture*>(p->inner.emissive.radiance);
+			m->scale[0] = p->inner.emissive.scale.x; m->scale[1] = p->inner.emissive.scale.y; m->scale[2] = p->inner.emissive.scale.z;
+			break;
+		default:
+			throw ApiError("material type not implemented by the CUDA path tracer");
+	}
+	I.materials.push_back(std::move(m));
+	I.sceneDirty = true;
+	return I.materials.back().get();
+	CATCH_ALL(nullptr)
+}
+IndexType world_get_material_count(MufflonInstanceHdl h) { TRY return IndexType(minst(h).materials.size()); CATCH_ALL(INVALID_INDEX) }
+
+TextureHdl world_add_texture_value(MufflonInstanceHdl h, const float* value, int num, TextureSampling) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(value && num >= 1 && num <= 4, "texture value needs 1 to 4 channels");
+	auto t = std::make_unique<HostTexture>();
+	t->width = t->height = 1;
+	t->channels = uint32_t(num);
+	t->texels.assign(4, 0.0f);
+	for(int i = 0; i < num; ++i) t->texels[i] = value[i];
+	I.textures.push_back(std::move(t));
+	return I.textures.back().get();
+	CATCH_ALL(nullptr)
+}
+
+TextureHdl world_add_texture_rgba32f(MufflonInstanceHdl h, const char* name, uint32_t w, uint32_t hh, const float* texels, TextureSampling) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(texels && w > 0 && hh > 0, "invalid texture");
+	auto t = std::make_unique<HostTexture>();
+	t->name = name ? name : "";
+	t->width = w; t->height = hh; t->channels = 4;
+	t->texels.assign(texels, texels + size_t(w) * hh * 4);
+	I.textures.push_back(std::move(t));
+	I.sceneDirty = true;
+	return I.textures.back().get();
+	CATCH_ALL(nullptr)
+}
+
+// ---------------------------------------------------------------- cameras
+CameraHdl world_add_pinhole_camera(MufflonInstanceHdl h, const char* name, const Vec3* pos, const Vec3* dir,
+                                   const Vec3* up, const uint32_t pathCount, float nearP, float farP, float vFov) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(pos && dir && up && pathCount >= 1, "invalid camera description");
+	auto c = std::make_unique<HostCamera>();
+	c->name = name ? name : "";
+	c->position[0] = pos->x; c->position[1] = pos->y; c->position[2] = pos->z;
+	c->dir[0] = dir->x; c->dir[1] = dir->y; c->dir[2] = dir->z;
+	c->up[0] = up->x; c->up[1] = up->y; c->up[2] = up->z;
+	c->nearPlane = nearP; c->farPlane = farP; c->vFov = vFov;
+	I.cameras.push_back(std::move(c));
+	return I.cameras.back().get();
+	CATCH_ALL(nullptr)
+}
+CameraHdl world_get_camera(MufflonInstanceHdl h, const char* name) {
+	TRY
+	for(auto& c : minst(h).cameras) if(name && c->name == name) return c.get();
+	throw ApiError("camera not found");
+	CATCH_ALL(nullptr)
+}
+Boolean world_set_camera_position(CameraHdl cam, Vec3 p, const uint32_t) {
+	TRY CHECK(cam, "invalid camera"); auto* c = static_cast<HostCamera*>(cam);
+	c->position[0] = p.x; c->position[1] = p.y; c->position[2] = p.z; return true; CATCH_ALL(false)
+}
+Boolean world_set_camera_direction(CameraHdl cam, Vec3 d, Vec3 u, const uint32_t) {
+	TRY CHECK(cam, "invalid camera"); auto* c = static_cast<HostCamera*>(cam);
+	c->dir[0] = d.x; c->dir[1] = d.y; c->dir[2] = d.z; c->up[0] = u.x; c->up[1] = u.y; c->up[2] = u.z; return true; CATCH_ALL(false)
+}
+Boolean world_set_pinhole_camera_fov(CameraHdl cam, float vFov) {
+	TRY CHECK(cam, "invalid camera"); static_cast<HostCamera*>(cam)->vFov = vFov; return true; CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- scenarios
+ScenarioHdl world_create_scenario(MufflonInstanceHdl h, const char* name) {
+	TRY
+	MufflonInstance& I = minst(h);
+	auto s = std::make_unique<HostScenario>();
+	s->name = name ? name : "";
+	I.scenarios.push_back(std::move(s));
+	return I.scenarios.back().get();
+	CATCH_ALL(nullptr)
+}
+ScenarioHdl world_find_scenario(MufflonInstanceHdl h, const char* name) {
+	TRY
+	for(auto& s : minst(h).scenarios) if(name && s->name == name) return s.get();
+	throw ApiError("scenario not found");
+	CATCH_ALL(nullptr)
+}
+ConstScenarioHdl world_get_current_scenario(MufflonInstanceHdl h) { TRY return minst(h).current; CATCH_ALL(nullptr) }
+Boolean world_finalize_scenario(MufflonInstanceHdl h, ScenarioHdl s, const char** msg) {
+	TRY
+	(void)minst(h);
+	CHECK(s, "invalid scenario");
+	if(msg) *msg = "";
+	CHECK(static_cast<HostScenario*>(s)->camera != nullptr, "scenario has no camera");
+	return true;
+	CATCH_ALL(false)
+}
+SceneHdl world_load_scenario(MufflonInstanceHdl h, ScenarioHdl s) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(s, "invalid scenario");
+	I.current = static_cast<HostScenario*>(s);
+	I.sceneDirty = true;
+	load_scene_if_needed(I);
+	return &I.scene;
+	CATCH_ALL(nullptr)
+}
+const char* scenario_get_name(ScenarioHdl s) { TRY CHECK(s, "invalid scenario"); return static_cast<HostScenario*>(s)->name.c_str(); CATCH_ALL(nullptr) }
+Boolean scenario_get_resolution(ScenarioHdl s, uint32_t* w, uint32_t* h) {
+	TRY CHECK(s, "invalid scenario"); auto* sc = static_cast<HostScenario*>(s); if(w) *w = sc->width; if(h) *h = sc->height; return true; CATCH_ALL(false)
+}
+Boolean scenario_set_resolution(ScenarioHdl s, uint32_t w, uint32_t h) {
+	TRY CHECK(s, "invalid scenario"); CHECK(w > 0 && h > 0 && w <= 65535 && h <= 65535, "resolution out of range");
+	auto* sc = static_cast<HostScenario*>(s); sc->width = w; sc->height = h; return true; CATCH_ALL(false)
+}
+CameraHdl scenario_get_camera(ScenarioHdl s) { TRY CHECK(s, "invalid scenario"); return static_cast<HostScenario*>(s)->camera; CATCH_ALL(nullptr) }
+Boolean scenario_set_camera(MufflonInstanceHdl h, ScenarioHdl s, CameraHdl cam) {
+	TRY (void)minst(h); CHECK(s && cam, "invalid scenario or camera"); static_cast<HostScenario*>(s)->camera = static_cast<HostCamera*>(cam); return true; CATCH_ALL(false)
+}
+Boolean scenario_mask_instance(ScenarioHdl s, InstanceHdl inst) {
+	TRY CHECK(s && inst, "invalid scenario or instance");
+	static_cast<HostScenario*>(s)->maskedInstances.push_back(static_cast<HostInstance*>(inst)->index); return true; CATCH_ALL(false)
+}
+Boolean scenario_add_light(MufflonInstanceHdl h, ScenarioHdl s, LightHdl hdl) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(s, "invalid scenario");
+	auto* sc = static_cast<HostScenario*>(s);
+	if(hdl.type == LIGHT_POINT) {
+		CHECK(hdl.index < I.pointLights.size(), "invalid point light");
+		sc->pointLights.push_back(hdl.index);
+	} else if(hdl.type == LIGHT_ENVMAP) {
+		CHECK(hdl.index < I.backgrounds.size(), "invalid background light");
+		sc->background = int32_t(hdl.index);
+	} else {
+		throw ApiError("light type not implemented by the CUDA path tracer");
+	}
+	I.sceneDirty = true;
+	return true;
+	CATCH_ALL(false)
+}
+MatIdx scenario_declare_material_slot(ScenarioHdl s, const char* name, size_t len) {
+	TRY
+	CHECK(s, "invalid scenario");
+	auto* sc = static_cast<HostScenario*>(s);
+	const std::string n(name ? name : "", name ? len : 0);
+	for(size_t i = 0; i < sc->slotNames.size(); ++i) if(sc->slotNames[i] == n) return MatIdx(i);
+	sc->slotNames.push_back(n);
+	sc->slotMaterials.push_back(nullptr);
+	return MatIdx(sc->slotNames.size() - 1);
+	CATCH_ALL(MatIdx(0xFFFF))
+}
+MatIdx scenario_get_material_slot(ScenarioHdl s, const char* name, size_t len) {
+	TRY
+	CHECK(s, "invalid scenario");
+	auto* sc = static_cast<HostScenario*>(s);
+	const std::string n(name ? name : "", name ? len : 0);
+	for(size_t i = 0; i < sc->slotNames.size(); ++i) if(sc->slotNames[i] == n) return MatIdx(i);
+	throw ApiError("material slot not found");
+	CATCH_ALL(MatIdx(0xFFFF))
+}
+Boolean scenario_assign_material(ScenarioHdl s, MatIdx idx, MaterialHdl m) {
+	TRY
+	CHECK(s && m, "invalid scenario or material");
+	auto* sc = static_cast<HostScenario*>(s);
+	CHECK(idx < sc->slotMaterials.size(), "material slot out of range");
+	sc->slotMaterials[idx] = static_cast<HostMaterial*>(m);
+	return true;
+	CATCH_ALL(false)
+}
+SceneHdl world_get_current_scene(MufflonInstanceHdl h) { TRY MufflonInstance& I = minst(h); return I.scene.valid ? &I.scene : nullptr; CATCH_ALL(nullptr) }
+Boolean scene_get_bounding_box(SceneHdl s, Vec3* mn, Vec3* mx) {
+	TRY CHECK(s, "invalid scene"); auto* d = static_cast<DeviceScene*>(s);
+	if(mn) *mn = { d->aabb[0], d->aabb[1], d->aabb[2] }; if(mx) *mx = { d->aabb[3], d->aabb[4], d->aabb[5] }; return true; CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- lights
+LightHdl world_add_light(MufflonInstanceHdl h, const char* name, LightType type, const uint32_t) {
+	LightHdl bad; bad.type = 7; bad.index = 0x1FFFFFFF;
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(type == LIGHT_POINT, "the CUDA path tracer implements point, area and environment lights");
+	HostPointLight l;
+	l.name = name ? name : "";
+	I.pointLights.push_back(l);
+	LightHdl r; r.type = LIGHT_POINT; r.index = uint32_t(I.pointLights.size() - 1);
+	return r;
+	CATCH_ALL(bad)
+}
+LightHdl world_add_background_light(MufflonInstanceHdl h, const char* name, BackgroundType type) {
+	LightHdl bad; bad.type = 7; bad.index = 0x1FFFFFFF;
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(type == BACKGROUND_MONOCHROME, "the CUDA path tracer implements monochrome backgrounds");
+	HostBackground b;
+	b.name = name ? name : "";
+	I.backgrounds.push_back(b);
+	LightHdl r; r.type = LIGHT_ENVMAP; r.index = uint32_t(I.backgrounds.size() - 1);
+	return r;
+	CATCH_ALL(bad)
+}
+Boolean world_set_point_light_position(MufflonInstanceHdl h, LightHdl l, Vec3 p, const uint32_t) {
+	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_POINT && l.index < I.pointLights.size(), "invalid point light");
+	auto& L = I.pointLights[l.index]; L.position[0] = p.x; L.position[1] = p.y; L.position[2] = p.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+}
+Boolean world_set_point_light_intensity(MufflonInstanceHdl h, LightHdl l, Vec3 v, const uint32_t) {
+	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_POINT && l.index < I.pointLights.size(), "invalid point light");
+	auto& L = I.pointLights[l.index]; L.intensity[0] = v.x; L.intensity[1] = v.y; L.intensity[2] = v.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+}
+Boolean world_set_env_light_color(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
+	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_ENVMAP && l.index < I.backgrounds.size(), "invalid background light");
+	auto& B = I.backgrounds[l.index]; B.color[0] = c.x; B.color[1] = c.y; B.color[2] = c.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+}
+Boolean world_set_env_light_scale(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
+	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_ENVMAP && l.index < I.backgrounds.size(), "invalid background light");
+	auto& B = I.backgrounds[l.index]; B.scale[0] = c.x; B.scale[1] = c.y; B.scale[2] = c.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- renderers
+uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 1u; CATCH_ALL(0u) }
+uint32_t render_get_renderer_variations(MufflonInstanceHdl h, uint32_t index) {
+	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
+}
+const char* render_get_renderer_name(MufflonInstanceHdl h, uint32_t index) {
+	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return "Pathtracer"; CATCH_ALL(nullptr)
+}
+const char* render_get_renderer_short_name(MufflonInstanceHdl h, uint32_t index) {
+	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return "PT"; CATCH_ALL(nullptr)
+}
+RenderDevice render_get_renderer_devices(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
+	TRY (void)minst(h); CHECK(index == 0 && variation == 0, "renderer index out of bounds"); return DEVICE_CUDA; CATCH_ALL(DEVICE_NONE)
+}
+Boolean render_enable_renderer(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(index == 0 && variation == 0, "renderer index out of bounds");
+	I.renderer.enabled = true;
+	I.renderer.needsReset = true;
+	return true;
+	CATCH_ALL(false)
+}
+
+// interface.cpp:3611-3685: one iteration = one sample per pixel
+Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime* preTime, ProcessTime* postTime) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(I.renderer.enabled, "No renderer is currently set");
+	CHECK(I.current != nullptr, "Failed to load scenario");
+	using clk = std::chrono::steady_clock;
+	auto t0 = clk::now();
+	load_scene_if_needed(I);
+	ensure_render_buffers(I);
+	RendererState& r = I.renderer;
+	const uint32_t n = r.width * r.height;
+	if(r.needsReset) {
+		CHECK_CUDA(launch_seed_rng(r.rng, n, r.params.seed, I.stream));
+		CHECK_CUDA(cudaMemsetAsync(r.radiance, 0, size_t(n) * 3 * sizeof(float), I.stream));
+		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
+		r.iteration = 0;
+		r.needsReset = false;
+	} else {
+		++r.iteration;
+	}
+	auto t1 = clk::now();
+	RenderState rs{};
+	rs.rngState = r.rng;
+	rs.radiance = r.targetRadiance ? r.radiance : nullptr;
+	rs.hitId = r.targetHitId ? r.hitId : nullptr;
+	rs.width = r.width; rs.height = r.height;
+	rs.iteration = r.iteration;
+	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, sizeof(TraceCounters), I.stream));
+	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
+	CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
+	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(&r.lastCounters, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	CHECK_CUDA(cudaEventElapsedTime(&r.lastKernelMs, r.evStart, r.evStop));
+	auto t2 = clk::now();
+	auto us = [](clk::duration d) { return uint64_t(std::chrono::duration_cast<std::chrono::microseconds>(d).count()); };
+	if(preTime) { preTime->cycles = 0; preTime->microseconds = us(t1 - t0); }
+	if(iterTime) { iterTime->cycles = 0; iterTime->microseconds = us(t2 - t1); }
+	if(postTime) { postTime->cycles = 0; postTime->microseconds = 0; }
+	if(r.lastCounters.errors) log_msg(LOG_WARNING, "traversal stack overflow in " + std::to_string(r.lastCounters.errors) + " rays");
+	return true;
+	CATCH_ALL(false)
+}
+
+uint32_t render_get_current_iteration(ConstMufflonInstanceHdl h) {
+	if(!h) return 0;
+	const MufflonInstance& I = *static_cast<const MufflonInstance*>(h);
+	return uint32_t(I.renderer.iteration + 1);
+}
+Boolean render_reset(MufflonInstanceHdl h) {
+	TRY MufflonInstance& I = minst(h); std::lock_guard<std::recursive_mutex> lock(I.iterationMutex); I.renderer.needsReset = true; return true; CATCH_ALL(false)
+}
+
+// PFM screenshot of a target (render_save_screenshot, interface.cpp:3704)
+Boolean render_save_screenshot(MufflonInstanceHdl h, const char* filename, const char* target, Boolean variance) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(filename && target, "filename and target are required");
+	const float* px = nullptr;
+	CHECK(mufflon_get_target_image(h, target, variance, &px), s_lastError);
+	CHECK(px != nullptr, "no image yet");
+	const int ch = I.renderer.screenChannels;
+	FILE* f = std::fopen(filename, "wb");
+	CHECK(f != nullptr, "cannot open output file");
+	std::fprintf(f, "PF\n%u %u\n-1.0\n", I.renderer.width, I.renderer.height);
+	for(size_t p = 0; p < size_t(I.renderer.width) * I.renderer.height; ++p) {
+		float rgb[3] = { 0, 0, 0 };
+		for(int c = 0; c < ch && c < 3; ++c) rgb[c] = px[p * ch + c];
+		std::fwrite(rgb, sizeof(float), 3, f);
+	}
+	std::fclose(f);
+	return true;
+	CATCH_ALL(false)
+}
+
+uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 8u; CATCH_ALL(0u) }
+const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) {
+	TRY (void)minst(h); CHECK(index < 8, "render target index out of bounds"); return TARGETS[index]; CATCH_ALL(nullptr)
+}
+Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(target, "target name is null");
+	CHECK(!variance, "variance targets are not recorded by this renderer");
+	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = true;
+	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = true;
+	else throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA path tracer");
+	I.renderer.needsReset = true;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, Boolean) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(target, "target name is null");
+	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = false;
+	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = false;
+	I.renderer.needsReset = true;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean render_is_render_target_enabled(MufflonInstanceHdl h, const char* name, Boolean variance) {
+	TRY
+	MufflonInstance& I = minst(h);
+	if(variance || !name) return false;
+	if(!std::strcmp(name, "Radiance")) return I.renderer.targetRadiance;
+	if(!std::strcmp(name, "Hit ID")) return I.renderer.targetHitId;
+	return false;
+	CATCH_ALL(false)
+}
+
+uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) { TRY (void)minst(h); return uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0])); CATCH_ALL(0u) }
+const char* renderer_get_parameter_desc(MufflonInstanceHdl h, uint32_t idx, ParameterType* type) {
+	TRY
+	(void)minst(h);
+	CHECK(idx < sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]), "parameter index out of bounds");
+	if(type) *type = PT_PARAMS[idx].type;
+	return PT_PARAMS[idx].name;
+	CATCH_ALL(nullptr)
+}
+Boolean renderer_set_parameter_int(MufflonInstanceHdl h, const char* name, int32_t value) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(name, "parameter name is null");
+	int32_t* p = param_ptr(I.renderer, name);
+	CHECK(p != nullptr, std::string("unknown parameter '") + name + "'");
+	if(!std::strcmp(name, "NEE count")) CHECK(value >= 0, "NEE count must be non-negative");
+	if(!std::strcmp(name, "Max. path length")) CHECK(value >= 1, "Max. path length must be at least 1");
+	*p = value;
+	I.renderer.needsReset = true; // ResetEvent::PARAMETER (renderer.hpp:19-48)
+	return true;
+	CATCH_ALL(false)
+}
+Boolean renderer_get_parameter_int(MufflonInstanceHdl h, const char* name, int32_t* value) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(name && value, "invalid arguments");
+	int32_t* p = param_ptr(I.renderer, name);
+	CHECK(p != nullptr, std::string("unknown parameter '") + name + "'");
+	*value = *p;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean renderer_set_parameter_float(MufflonInstanceHdl h, const char* name, float) {
+	TRY (void)minst(h); throw ApiError(std::string("unknown float parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+}
+Boolean renderer_get_parameter_float(MufflonInstanceHdl h, const char* name, float*) {
+	TRY (void)minst(h); throw ApiError(std::string("unknown float parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+}
+Boolean renderer_set_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean value) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(name && !std::strcmp(name, "NEE position guide"), std::string("unknown bool parameter '") + (name ? name : "") + "'");
+	CHECK(!value, "NEE position guide is not implemented by the CUDA path tracer");
+	return true;
+	CATCH_ALL(false)
+}
+Boolean renderer_get_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean* value) {
+	TRY
+	(void)minst(h);
+	CHECK(name && !std::strcmp(name, "NEE position guide") && value, "unknown bool parameter");
+	*value = 0;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean renderer_set_parameter_enum(MufflonInstanceHdl h, const char* name, int) {
+	TRY (void)minst(h); throw ApiError(std::string("unknown enum parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+}
+Boolean renderer_get_parameter_enum(MufflonInstanceHdl h, const char* name, int*) {
+	TRY (void)minst(h); throw ApiError(std::string("unknown enum parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- extensions
+Boolean mufflon_get_render_stats(MufflonInstanceHdl h, MufflonRenderStats* s) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(s, "stats pointer is null");
+	const TraceCounters& c = I.renderer.lastCounters;
+	s->rays = c.rays; s->shadowRays = c.shadowRays; s->nodeVisits = c.nodeVisits; s->primTests = c.primTests;
+	s->instanceVisits = c.instanceVisits; s->errors = c.errors; s->kernelMs = I.renderer.lastKernelMs;
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_trace_rays(MufflonInstanceHdl h, const float* rays, const float* geo, float tmax, uint32_t n,
+                           float* t, int32_t* inst, int32_t* prim, float* sp) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(rays && t && inst && prim, "invalid arguments");
+	load_scene_if_needed(I);
+	if(n == 0) return true;
+	float *dr = nullptr, *dg = nullptr, *dt = nullptr, *dsp = nullptr;
+	int32_t *di = nullptr, *dp = nullptr;
+	CHECK_CUDA(cudaMalloc(&dr, size_t(n) * 24));
+	CHECK_CUDA(cudaMalloc(&dt, size_t(n) * 4));
+	CHECK_CUDA(cudaMalloc(&di, size_t(n) * 4));
+	CHECK_CUDA(cudaMalloc(&dp, size_t(n) * 4));
+	CHECK_CUDA(cudaMalloc(&dsp, size_t(n) * 8));
+	if(geo) CHECK_CUDA(cudaMalloc(&dg, size_t(n) * 12));
+	CHECK_CUDA(cudaMemcpyAsync(dr, rays, size_t(n) * 24, cudaMemcpyHostToDevice, I.stream));
+	if(geo) CHECK_CUDA(cudaMemcpyAsync(dg, geo, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
+	CHECK_CUDA(launch_trace_rays(I.scene.desc, dr, dg, tmax, n, dt, di, dp, dsp, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(t, dt, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(inst, di, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(prim, dp, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
+	if(sp) CHECK_CUDA(cudaMemcpyAsync(sp, dsp, size_t(n) * 8, cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	cudaFree(dr); cudaFree(dg); cudaFree(dt); cudaFree(di); cudaFree(dp); cudaFree(dsp);
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_trace_occlusion(MufflonInstanceHdl h, const float* a, const float* b, uint32_t n, uint8_t* occ) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(a && b && occ, "invalid arguments");
+	load_scene_if_needed(I);
+	if(n == 0) return true;
+	float *da = nullptr, *db = nullptr;
+	uint8_t* dout = nullptr;
+	CHECK_CUDA(cudaMalloc(&da, size_t(n) * 12));
+	CHECK_CUDA(cudaMalloc(&db, size_t(n) * 12));
+	CHECK_CUDA(cudaMalloc(&dout, n));
+	CHECK_CUDA(cudaMemcpyAsync(da, a, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(db, b, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
+	CHECK_CUDA(launch_occlusion(I.scene.desc, da, db, n, dout, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(occ, dout, n, cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	cudaFree(da); cudaFree(db); cudaFree(dout);
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_get_bvh(MufflonInstanceHdl h, int32_t which, int32_t* numPrims, int32_t* numInternal, void* nodes, int32_t* primIds) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	load_scene_if_needed(I);
+	const BvhBuffers* b = nullptr;
+	if(which < 0) b = &I.scene.tlas;
+	else { CHECK(size_t(which) < I.scene.lods.size(), "LoD index out of range"); b = &I.scene.lods[which].bvh; }
+	if(numPrims) *numPrims = b->numPrims;
+	if(numInternal) *numInternal = b->numInternal;
+	if(nodes && b->numInternal > 0) CHECK_CUDA(cudaMemcpy(nodes, b->nodes, sizeof(BvhNode) * 2 * size_t(b->numInternal), cudaMemcpyDeviceToHost));
+	if(primIds && b->numPrims > 0) CHECK_CUDA(cudaMemcpy(primIds, b->primIds, sizeof(int32_t) * size_t(b->numPrims), cudaMemcpyDeviceToHost));
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_lbvh_build(const float* vertices, uint32_t numVertices, const uint32_t* indices, uint32_t numTriangles,
+                           uint32_t numQuads, const float* spheres, uint32_t numSpheres, uint64_t* mortonSorted,
+                           int32_t* parents, void* nodes, int32_t* primIds, int32_t* numInternal, float* stageMs) {
+	TRY
+	CHECK(mufflon_is_cuda_available(), "no CUDA device");
+	HostLod L;
+	L.vertices.assign(vertices, vertices + 3 * size_t(numVertices));
+	L.triIdx.assign(indices, indices + 3 * size_t(numTriangles));
+	L.quadIdx.assign(indices + 3 * size_t(numTriangles), indices + 3 * size_t(numTriangles) + 4 * size_t(numQuads));
+	L.triMat.assign(numTriangles, 0); L.quadMat.assign(numQuads, 0);
+	if(numSpheres) L.spheres.assign(spheres, spheres + 4 * size_t(numSpheres));
+	L.sphereMat.assign(numSpheres, 0);
+	const uint32_t n = numTriangles + numQuads + numSpheres;
+	float *dv = nullptr; uint32_t* di = nullptr; float4* ds = nullptr;
+	CHECK_CUDA(cudaMalloc(&dv, std::max<size_t>(1, L.vertices.size()) * 4));
+	CHECK_CUDA(cudaMalloc(&di, std::max<size_t>(1, 3 * size_t(numTriangles) + 4 * size_t(numQuads)) * 4));
+	CHECK_CUDA(cudaMalloc(&ds, std::max<size_t>(1, numSpheres) * 16));
+	if(!L.vertices.empty()) CHECK_CUDA(cudaMemcpy(dv, L.vertices.data(), L.vertices.size() * 4, cudaMemcpyHostToDevice));
+	if(numTriangles + numQuads) CHECK_CUDA(cudaMemcpy(di, indices, (3 * size_t(numTriangles) + 4 * size_t(numQuads)) * 4, cudaMemcpyHostToDevice));
+	if(numSpheres) CHECK_CUDA(cudaMemcpy(ds, spheres, size_t(numSpheres) * 16, cudaMemcpyHostToDevice));
+	LodBuildInput in{};
+	in.numTriangles = numTriangles; in.numQuads = numQuads; in.numSpheres = numSpheres;
+	in.vertices = dv; in.indices = di; in.spheres = ds;
+	L.bounds(in.aabbMin, in.aabbMax);
+	LbvhBuilder builder;
+	builder.enable_timing(stageMs != nullptr);
+	BvhBuffers out;
+	cudaStream_t s;
+	CHECK_CUDA(cudaStreamCreate(&s));
+	const cudaError_t e = builder.build_lod(in, out, s);
+	if(e == cudaSuccess && n > 1) {
+		if(mortonSorted) cudaMemcpy(mortonSorted, builder.sorted_keys(), sizeof(uint64_t) * n, cudaMemcpyDeviceToHost);
+		if(parents) cudaMemcpy(parents, builder.parents(), sizeof(int32_t) * (2 * size_t(n) - 1), cudaMemcpyDeviceToHost);
+	}
+	if(e == cudaSuccess) {
+		if(nodes && out.numInternal > 0) cudaMemcpy(nodes, out.nodes, sizeof(BvhNode) * 2 * size_t(out.numInternal), cudaMemcpyDeviceToHost);
+		if(primIds && n > 0) cudaMemcpy(primIds, out.primIds, sizeof(int32_t) * n, cudaMemcpyDeviceToHost);
+		if(numInternal) *numInternal = out.numInternal;
+		if(stageMs) { const StageTimes t = builder.last_times(); const float v[8] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup }; std::memcpy(stageMs, v, sizeof(v)); }
+	}
+	out.release();
+	cudaStreamDestroy(s);
+	cudaFree(dv); cudaFree(di); cudaFree(ds);
+	CHECK_CUDA(e);
+	CHECK_CUDA(cudaGetLastError());
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_lbvh_build_device(const float* dVertices, const uint32_t* dIndices, uint32_t numTriangles, uint32_t numQuads,
+                                  const float* dSpheres, uint32_t numSpheres, const float* aabb6, int32_t* numInternal,
+                                  float* buildMs, float* stageMs) {
+	TRY
+	CHECK(aabb6, "aabb is required");
+	LodBuildInput in{};
+	in.numTriangles = numTriangles; in.numQuads = numQuads; in.numSpheres = numSpheres;
+	in.vertices = dVertices; in.indices = dIndices; in.spheres = reinterpret_cast<const float4*>(dSpheres);
+	std::memcpy(in.aabbMin, aabb6, 12); std::memcpy(in.aabbMax, aabb6 + 3, 12);
+	static LbvhBuilder* builder = new LbvhBuilder();
+	static BvhBuffers* out = new BvhBuffers();
+	builder->enable_timing(stageMs != nullptr);
+	cudaEvent_t a, b;
+	CHECK_CUDA(cudaEventCreate(&a)); CHECK_CUDA(cudaEventCreate(&b));
+	CHECK_CUDA(cudaEventRecord(a, 0));
+	CHECK_CUDA(builder->build_lod(in, *out, 0));
+	CHECK_CUDA(cudaEventRecord(b, 0));
+	CHECK_CUDA(cudaEventSynchronize(b));
+	float ms = 0.0f;
+	cudaEventElapsedTime(&ms, a, b);
+	cudaEventDestroy(a); cudaEventDestroy(b);
+	if(buildMs) *buildMs = ms;
+	if(numInternal) *numInternal = out->numInternal;
+	if(stageMs) { const StageTimes t = builder->last_times(); const float v[8] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup }; std::memcpy(stageMs, v, sizeof(v)); }
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint32_t n) {
+	TRY
+	CHECK(keys && values, "invalid arguments");
+	if(n == 0) return true;
+	LbvhBuilder builder;
+	uint64_t* dk = nullptr; int32_t* dv = nullptr;
+	CHECK_CUDA(cudaMalloc(&dk, size_t(n) * 8));
+	CHECK_CUDA(cudaMalloc(&dv, size_t(n) * 4));
+	CHECK_CUDA(cudaMemcpy(dk, keys, size_t(n) * 8, cudaMemcpyHostToDevice));
+	CHECK_CUDA(cudaMemcpy(dv, values, size_t(n) * 4, cudaMemcpyHostToDevice));
+	CHECK_CUDA(builder.sort_pairs(dk, dv, n, 0));
+	CHECK_CUDA(cudaDeviceSynchronize());
+	CHECK_CUDA(cudaMemcpy(keys, dk, size_t(n) * 8, cudaMemcpyDeviceToHost));
+	CHECK_CUDA(cudaMemcpy(values, dv, size_t(n) * 4, cudaMemcpyDeviceToHost));
+	cudaFree(dk); cudaFree(dv);
+	return true;
+	CATCH_ALL(false)
+}
+
+} // extern "C"

@@ -1,0 +1,171 @@
+// Host-side world model of the C API: objects, LoDs, instances, materials,
+// textures, cameras, lights and scenarios (the parts of
+// src/core/scene/world_container.hpp, object.hpp, lod.hpp, scenario.hpp that
+// the path tracer consumes), plus the device-resident scene they are
+// flattened into.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../trace/scene_types.hpp"
+#include "../lbvh/lbvh.hpp"
+
+namespace mb {
+
+struct HostLod {
+	std::vector<float> vertices, normals, uvs; // 3, 3, 2 per vertex
+	std::vector<uint32_t> triIdx, quadIdx;     // 3 per triangle, 4 per quad
+	std::vector<uint16_t> triMat, quadMat;
+	std::vector<float> spheres;                // 4 per sphere
+	std::vector<uint16_t> sphereMat;
+	uint32_t num_vertices() const { return uint32_t(vertices.size() / 3); }
+	uint32_t num_triangles() const { return uint32_t(triMat.size()); }
+	uint32_t num_quads() const { return uint32_t(quadMat.size()); }
+	uint32_t num_spheres() const { return uint32_t(sphereMat.size()); }
+	uint32_t num_prims() const { return num_triangles() + num_quads() + num_spheres(); }
+	bool bounds(float mn[3], float mx[3]) const;
+};
+
+struct HostObject {
+	std::string name;
+	uint32_t flags = 0;
+	std::map<uint32_t, std::unique_ptr<HostLod>> lods;
+};
+
+struct HostInstance {
+	HostObject* object = nullptr;
+	uint32_t index = 0;
+	float worldToInstance[12] = { 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0 };
+};
+
+struct HostTexture {
+	std::string name;
+	uint32_t width = 1, height = 1, channels = 4;
+	std::vector<float> texels; // 4 per texel
+};
+
+struct HostMaterial {
+	std::string name;
+	int32_t type = MAT_LAMBERT;
+	HostTexture* albedo = nullptr;
+	HostTexture* roughness = nullptr;
+	HostTexture* radiance = nullptr;
+	float scale[3] = { 1, 1, 1 };
+	int32_t shadowing = 1, ndf = 1;
+	bool supported = true;
+};
+
+struct HostCamera {
+	std::string name;
+	float position[3] = { 0, 0, 0 };
+	float dir[3] = { 0, 0, -1 };
+	float up[3] = { 0, 1, 0 };
+	float vFov = 0.7853982f;
+	float nearPlane = 1e-4f, farPlane = 1e10f;
+};
+
+struct HostPointLight { std::string name; float position[3] = { 0, 0, 0 }; float intensity[3] = { 1, 1, 1 }; };
+struct HostBackground { std::string name; int32_t type = 0; float color[3] = { 0, 0, 0 }; float scale[3] = { 1, 1, 1 }; };
+
+struct HostScenario {
+	std::string name;
+	uint32_t width = 800, height = 600;
+	HostCamera* camera = nullptr;
+	std::vector<uint32_t> pointLights;
+	int32_t background = -1;
+	std::vector<std::string> slotNames;
+	std::vector<HostMaterial*> slotMaterials;
+	std::vector<uint32_t> maskedInstances;
+};
+
+// Device buffers of one LoD.
+struct DeviceLod {
+	float* vertices = nullptr;
+	float* normals = nullptr;
+	float* uvs = nullptr;
+	uint32_t* indices = nullptr;
+	uint16_t* faceMat = nullptr;
+	float4* spheres = nullptr;
+	uint16_t* sphereMat = nullptr;
+	BvhBuffers bvh;
+	DLod desc{};
+	void release();
+};
+
+// The flattened scene resident in HBM (see scene_types.hpp).
+struct DeviceScene {
+	std::vector<DeviceLod> lods;
+	std::vector<const HostLod*> lodSources;
+	DLod* dLods = nullptr;
+	float4* dW2I = nullptr;
+	uint32_t* dInstLod = nullptr;
+	float* dInstBoxes = nullptr;
+	float* dInstCentroids = nullptr;
+	BvhBuffers tlas;
+	DMaterial* dMaterials = nullptr;
+	std::vector<float4*> textureBuffers;
+	DTexture* dTextures = nullptr;
+	DLight* dLights = nullptr;
+	DLightNode* dLightNodes = nullptr;
+	uint64_t* dLightKeys = nullptr;
+	uint32_t* dLightCodes = nullptr;
+	DScene desc{};
+	float aabb[6] = { 0, 0, 0, 0, 0, 0 };
+	bool valid = false;
+	void release();
+};
+
+struct MufflonInstance;
+// Builds (or rebuilds) the device scene of the current scenario.
+bool build_device_scene(MufflonInstance& inst, std::string& error);
+
+struct RendererState {
+	bool enabled = false;
+	PtParams params{ 0, 0, 16, 1, 0 };
+	int32_t blocksPerSm = 8;
+	bool targetRadiance = true;
+	bool targetHitId = false;
+	bool needsReset = true;
+	int32_t iteration = -1;
+	uint32_t width = 0, height = 0;
+	uint64_t* rng = nullptr;
+	float* radiance = nullptr;
+	float* hitId = nullptr;
+	unsigned int* workCounter = nullptr;
+	TraceCounters* counters = nullptr;
+	cudaEvent_t evStart = nullptr, evStop = nullptr;
+	TraceCounters lastCounters{};
+	float lastKernelMs = 0.0f;
+	std::vector<float> screen;
+	int screenChannels = 0;
+	void release();
+};
+
+struct MufflonInstance {
+	std::recursive_mutex iterationMutex;
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::vector<std::unique_ptr<HostObject>> objects;
+	std::vector<std::unique_ptr<HostInstance>> instances;
+	std::vector<std::unique_ptr<HostMaterial>> materials;
+	std::vector<std::unique_ptr<HostTexture>> textures;
+	std::vector<std::unique_ptr<HostCamera>> cameras;
+	std::vector<HostPointLight> pointLights;
+	std::vector<HostBackground> backgrounds;
+	std::vector<std::unique_ptr<HostScenario>> scenarios;
+	HostScenario* current = nullptr;
+	bool sceneDirty = true;
+	DeviceScene scene;
+	LbvhBuilder builder;
+	RendererState renderer;
+	~MufflonInstance();
+};
+
+} // namespace mb

@@ -1,0 +1,2097 @@
+// CPU oracle for the Mufflon path-tracer hot path: TEST INFRASTRUCTURE ONLY.
+//
+// A single-translation-unit restatement of the reference renderer's CPU path:
+//   LBVH build ........ src/core/scene/accel_structs/build_lbvh.cu:59-780,
+//                       src/core/math/sfcurves.hpp:26-46,
+//                       src/core/scene/accel_structs/accel_structs_commons.hpp:56-109
+//   traversal ......... src/core/scene/accel_structs/intersection.cu:16-753,
+//                       src/core/scene/accel_structs/tangent_space.hpp:10-66
+//   path tracer ....... src/core/renderer/pt/pt_common.hpp:75-156,
+//                       src/core/renderer/random_walk.hpp:38-113,
+//                       src/core/renderer/path_util.hpp:130-665
+//   camera ............ src/core/cameras/pinhole.hpp:53-81, camera.hpp:81-96
+//   materials ......... src/core/scene/materials/{material_sampling,lambert,
+//                       microfacet_base,microfacet_specular,emissive}.hpp
+//   lights ............ src/core/scene/lights/{light_tree_sampling,light_sampling,
+//                       lights}.hpp, light_tree.cpp:120-330, lights.cpp:10-91,
+//                       background.cpp:125-135
+//   rng / sampling .... src/core/math/rng.hpp:126-207, sampling.hpp:23-199
+//   pixel loop ........ src/core/renderer/pt/cpu_pt.cpp:18-45
+//   accumulation ...... src/core/renderer/targets/output_handler_variance.hpp:7-31
+//
+// Pinned deviations from the reference (each needed because the reference is
+// either order-dependent or relies on the missing "epsilon" library):
+//   1. exact count-leading-zeros (the Linux host path uses log2f);
+//   2. stable (key, index) sort of Morton codes;
+//   3. SAH merge order fixed to "right child is the arriving thread", which is
+//      what a sequential run of the reference CPU loop produces;
+//   4. first hits are ordered by (world t, instance, primitive), so the result
+//      does not depend on traversal order; box culling uses tmax * (1 + 2^-16)
+//      so that it stays conservative;
+//   5. the slab test clamps cmin at 0 on both sides (the reference GPU form,
+//      with the FMA the GPU compiler forms: fma(min, invDir, -oDivDir));
+//   6. watertight triangle test (Woop, Benthin, Wald, JCGT 2013);
+//   7. sphere test from the quadratic with a stable root, solveSquarePoly and
+//      the vector helpers (surface, bilerp, sgn, box transform) written from
+//      their mathematical definitions;
+//   8. sin/cos/atan2/acos from mufflon_b200/csrc/common/fmath.hpp, the only
+//      file shared with the product, so that host and device round alike;
+//   9. no FP contraction (-ffp-contract=off), explicit fmaf where the GPU
+//      uses an FMA;
+//  10. sphere primitives are indexed from the sphere offset (the reference's
+//      intersection.cu:270 and descriptors.hpp:198 index the sphere arrays
+//      with the global primitive id, which only works for sphere-only LoDs).
+#include "oracle.h"
+#include "../mufflon_b200/csrc/common/fmath.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <utility>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+using u16 = uint16_t;
+using u32 = uint32_t;
+using u64 = uint64_t;
+using i32 = int32_t;
+
+constexpr float PI = 3.14159265358979f;
+constexpr float MAX_SCENE_SIZE = 1048576.0f;
+constexpr float SCENE_SCALE_EPS = 1e-4f;
+constexpr float INF_PDF = 4294967296.0f;
+constexpr float BOX_SLACK = 1.0f + 1.0f / 65536.0f;
+constexpr float DISTANCESQ_EPSILON = 1e-10f;
+constexpr float SHADING_NORMAL_EPS = 1e-3f;
+constexpr i32 TREE_HEAD = 0x10000000;
+
+// ---------------------------------------------------------------- vectors
+struct V2 { float x, y; };
+struct V3 {
+	float x, y, z;
+	float operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+inline V3 operator+(V3 a, V3 b) { return { a.x + b.x, a.y + b.y, a.z + b.z }; }
+inline V3 operator-(V3 a, V3 b) { return { a.x - b.x, a.y - b.y, a.z - b.z }; }
+inline V3 operator-(V3 a) { return { -a.x, -a.y, -a.z }; }
+inline V3 operator*(V3 a, V3 b) { return { a.x * b.x, a.y * b.y, a.z * b.z }; }
+inline V3 operator*(V3 a, float s) { return { a.x * s, a.y * s, a.z * s }; }
+inline V3 operator*(float s, V3 a) { return { s * a.x, s * a.y, s * a.z }; }
+inline V3 operator/(V3 a, float s) { return { a.x / s, a.y / s, a.z / s }; }
+inline V3 operator/(V3 a, V3 b) { return { a.x / b.x, a.y / b.y, a.z / b.z }; }
+inline V2 operator+(V2 a, V2 b) { return { a.x + b.x, a.y + b.y }; }
+inline V2 operator-(V2 a, V2 b) { return { a.x - b.x, a.y - b.y }; }
+inline V2 operator*(V2 a, float s) { return { a.x * s, a.y * s }; }
+inline V2 operator*(float s, V2 a) { return { s * a.x, s * a.y }; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+	return { a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x };
+}
+inline float lensq(V3 a) { return dot(a, a); }
+inline float len(V3 a) { return mbmath::sqrt(lensq(a)); }
+inline V3 normalize(V3 a) { return a / len(a); }
+inline float fmin_(float a, float b) { return std::fmin(a, b); }
+inline float fmax_(float a, float b) { return std::fmax(a, b); }
+// Box merges use an explicit select so that signed zeros resolve the same
+// way on host and device: min(a, b) = b < a ? b : a.
+inline float bmin(float a, float b) { return b < a ? b : a; }
+inline float bmax(float a, float b) { return a < b ? b : a; }
+inline V3 vmin(V3 a, V3 b) { return { bmin(a.x, b.x), bmin(a.y, b.y), bmin(a.z, b.z) }; }
+inline V3 vmax(V3 a, V3 b) { return { bmax(a.x, b.x), bmax(a.y, b.y), bmax(a.z, b.z) }; }
+inline float maxc(V3 a) { return fmax_(fmax_(a.x, a.y), a.z); }
+inline float sgn(float x) { return x < 0.0f ? -1.0f : 1.0f; }
+inline float sdiv(float x, float d) { return x / (d + 1e-20f * sgn(d)); }
+inline V3 sdiv(V3 x, V3 d) { return { sdiv(x.x, d.x), sdiv(x.y, d.y), sdiv(x.z, d.z) }; }
+inline bool any_pos(V3 a) { return a.x > 0.0f || a.y > 0.0f || a.z > 0.0f; }
+inline bool nonzero(V3 a) { return a.x != 0.0f || a.y != 0.0f || a.z != 0.0f; }
+
+struct Box { V3 mn, mx; };
+inline Box empty_box() { return { { FLT_MAX, FLT_MAX, FLT_MAX }, { -FLT_MAX, -FLT_MAX, -FLT_MAX } }; }
+inline Box merge(Box a, Box b) { return { vmin(a.mn, b.mn), vmax(a.mx, b.mx) }; }
+inline float surface(Box b) {
+	V3 d = b.mx - b.mn;
+	return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
+}
+inline V3 center(Box b) { return (b.mn + b.mx) * 0.5f; }
+
+struct Mat34 { float m[12]; };
+inline V3 xform_point(const Mat34& M, V3 p) {
+	const float* m = M.m;
+	return { m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3],
+	         m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+	         m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11] };
+}
+inline V3 xform_dir(const Mat34& M, V3 d) {
+	const float* m = M.m;
+	return { m[0] * d.x + m[1] * d.y + m[2] * d.z,
+	         m[4] * d.x + m[5] * d.y + m[6] * d.z,
+	         m[8] * d.x + m[9] * d.y + m[10] * d.z };
+}
+// transpose(Mat3x3(M)) * n
+inline V3 xform_transposed(const Mat34& M, V3 n) {
+	const float* m = M.m;
+	return { m[0] * n.x + m[4] * n.y + m[8] * n.z,
+	         m[1] * n.x + m[5] * n.y + m[9] * n.z,
+	         m[2] * n.x + m[6] * n.y + m[10] * n.z };
+}
+// descriptors.hpp:108-129
+Mat34 instance_to_world(const Mat34& W) {
+	const float* r = W.m;
+	const float r00 = r[0], r01 = r[1], r02 = r[2], r10 = r[4], r11 = r[5], r12 = r[6],
+	            r20 = r[8], r21 = r[9], r22 = r[10];
+	const float m00 = r11 * r22 - r21 * r12;
+	const float m01 = r21 * r02 - r01 * r22;
+	const float m02 = r01 * r12 - r11 * r02;
+	const float m10 = r20 * r12 - r10 * r22;
+	const float m11 = r00 * r22 - r20 * r02;
+	const float m12 = r10 * r02 - r00 * r12;
+	const float m20 = r10 * r21 - r20 * r11;
+	const float m21 = r20 * r01 - r00 * r21;
+	const float m22 = r00 * r11 - r10 * r01;
+	const float det = r00 * m00 + r01 * m10 + r02 * m20;
+	const float id = 1.0f / det;
+	const float i00 = id * m00, i01 = id * m01, i02 = id * m02, i10 = id * m10, i11 = id * m11,
+	            i12 = id * m12, i20 = id * m20, i21 = id * m21, i22 = id * m22;
+	const float tx = r[3], ty = r[7], tz = r[11];
+	Mat34 o;
+	o.m[0] = i00; o.m[1] = i01; o.m[2] = i02; o.m[3] = -(i00 * tx + i01 * ty + i02 * tz);
+	o.m[4] = i10; o.m[5] = i11; o.m[6] = i12; o.m[7] = -(i10 * tx + i11 * ty + i12 * tz);
+	o.m[8] = i20; o.m[9] = i21; o.m[10] = i22; o.m[11] = -(i20 * tx + i21 * ty + i22 * tz);
+	return o;
+}
+Box xform_box(const Mat34& M, Box b) {
+	Box o = empty_box();
+	for(int c = 0; c < 8; ++c) {
+		V3 p = { (c & 1) ? b.mx.x : b.mn.x, (c & 2) ? b.mx.y : b.mn.y, (c & 4) ? b.mx.z : b.mn.z };
+		V3 q = xform_point(M, p);
+		o.mn = vmin(o.mn, q);
+		o.mx = vmax(o.mx, q);
+	}
+	return o;
+}
+
+// ---------------------------------------------------------------- rng
+// rng.hpp:126-131
+inline u64 scramble_seed(u32 x) {
+	u64 z = u64(x) + 0x9e3779b97f4a7c15ull;
+	z = (z ^ (z >> 30u)) * 0xbf58476d1ce4e5b9ull;
+	z = (z ^ (z >> 27u)) * 0x94d049bb133111ebull;
+	return z ^ (z >> 31u);
+}
+// rng.hpp:184-207
+struct Pcg64 {
+	u64 state;
+	u64 next() {
+		u64 x = state;
+		const u64 count = state >> 59ull;
+		state = state * 6364136223846793005ull + 1442695040888963407ull;
+		x ^= x >> (5 + count);
+		x *= 12605985483714917081ull;
+		return x ^ (x >> 43);
+	}
+	static Pcg64 seeded(u32 seed) {
+		Pcg64 r;
+		r.state = scramble_seed(seed);
+		r.next();
+		r.state += seed;
+		r.next();
+		return r;
+	}
+};
+// sampling.hpp:23-29
+inline float sample_uniform(u32 u) { return float(u) / 4294967810.0f; }
+// sampling.hpp:39-46
+inline u64 percentage_of(u64 num, float p) {
+	u64 pfix = u64(p * 2147483648.0f);
+	return ((pfix * (num & 0x7fffffff)) >> 31) + (pfix * (num >> 31));
+}
+
+// ---------------------------------------------------------------- morton
+// sfcurves.hpp:35-44
+inline u64 part_by_two21(u32 x) {
+	u64 r = x;
+	r = (r | (r << 32)) & 0x001f00000000ffffull;
+	r = (r | (r << 16)) & 0x001f0000ff0000ffull;
+	r = (r | (r << 8)) & 0x100f00f00f00f00full;
+	r = (r | (r << 4)) & 0x10c30c30c30c30c3ull;
+	r = (r | (r << 2)) & 0x1249249249249249ull;
+	return r;
+}
+inline int clz64(u64 v) { return v == 0 ? 64 : __builtin_clzll(v); }
+inline int clz32(u32 v) { return v == 0 ? 32 : __builtin_clz(v); }
+
+// build_lbvh.cu:71-85
+inline u64 morton63(V3 p, Box bb) {
+	V3 span = bb.mx - bb.mn;
+	V3 n = sdiv(p - bb.mn, span);
+	auto disc = [](float v) {
+		float x = v * 2097152.0f;
+		x = std::fmin(std::fmax(x, 0.0f), 2097151.0f);
+		return u32(x);
+	};
+	return part_by_two21(disc(n.x)) * 4 + part_by_two21(disc(n.y)) * 2 + part_by_two21(disc(n.z));
+}
+
+// ---------------------------------------------------------------- scene
+struct Lod {
+	u32 nV = 0, nT = 0, nQ = 0, nS = 0;
+	std::vector<V3> verts, normals;
+	std::vector<V2> uvs;
+	std::vector<u32> idx;
+	std::vector<u16> faceMat;
+	std::vector<float> spheres; // 4 per sphere
+	std::vector<u16> sphereMat;
+	i32 numPrims = 0;
+	Box aabb = empty_box();
+};
+
+struct BvhNode { V3 mn, mx; i32 index, primCount; };
+
+struct Bvh {
+	i32 numPrims = 0;
+	i32 numInternal = 0; // after collapse
+	std::vector<u64> mortonSorted;
+	std::vector<i32> parents;
+	std::vector<BvhNode> nodes; // 2 per internal node
+	std::vector<i32> primIds;
+};
+
+struct Material {
+	i32 type;
+	V3 albedo;
+	V2 roughness;
+	i32 shadowing, ndf;
+	V3 radiance, scale;
+	i32 albedoTex;
+};
+
+struct Texture { u32 w, h; std::vector<float> texels; };
+
+enum LightType : u16 { LT_POINT = 0, LT_SPOT = 1, LT_TRI = 2, LT_QUAD = 3, LT_SPHERE = 4, LT_DIR = 5, LT_ENV = 6 };
+constexpr u16 INTERNAL_NODE = 0xFFFF;
+
+struct PosLight {
+	u16 type;
+	// point
+	V3 position, intensity;
+	// area quad (light.hpp:107-124 precomputed vectors)
+	V3 posV[4];
+	V2 uvV[4];
+	u16 material;
+	i32 primInst = -1, primId = -1;
+};
+
+struct LightNodeRef { float flux; i32 index; u16 type; }; // index: light index or node index
+struct LightNode { LightNodeRef left, right; V3 center; };
+
+struct LightTree {
+	std::vector<PosLight> lights;
+	std::vector<LightNode> nodes;
+	float rootFlux = 0.0f;
+	u16 rootType = INTERNAL_NODE;
+	i32 rootIndex = 0;
+	V3 bgFlux = { 0, 0, 0 };
+	bool hasBackground = false;
+	V3 bgColor = { 0, 0, 0 }, bgScale = { 0, 0, 0 };
+	std::map<std::pair<i32, i32>, u32> primToNodePath;
+	float dirFlux = 0.0f;
+};
+
+struct Camera {
+	V3 position, viewDir, up;
+	float tanVFov, nearP, farP;
+	u16 resX, resY;
+};
+
+struct Counters {
+	u64 rays = 0, shadowRays = 0, nodeVisits = 0, instanceVisits = 0, tri = 0, quad = 0, sphere = 0;
+	void add(const Counters& o) {
+		rays += o.rays; shadowRays += o.shadowRays; nodeVisits += o.nodeVisits;
+		instanceVisits += o.instanceVisits; tri += o.tri; quad += o.quad; sphere += o.sphere;
+	}
+};
+
+struct Scene {
+	std::vector<Lod> lods;
+	std::vector<Bvh> lodBvh;
+	std::vector<Mat34> w2i;
+	std::vector<u32> instLod;
+	i32 activeInstances = 0;
+	u32 validInstance = 0;
+	Bvh tlas;
+	std::vector<Material> materials;
+	std::vector<Texture> textures;
+	LightTree lightTree;
+	Camera cam;
+	Box aabb = empty_box();
+	u32 width = 0, height = 0;
+};
+
+// -------------------------------------------------------- primitive access
+inline V3 sphere_center(const Lod& l, i32 s) { return { l.spheres[4 * s], l.spheres[4 * s + 1], l.spheres[4 * s + 2] }; }
+inline float sphere_radius(const Lod& l, i32 s) { return l.spheres[4 * s + 3]; }
+
+// accel_structs_commons.hpp:56-80
+V3 lod_centroid(const Lod& l, i32 p) {
+	const i32 sphOff = i32(l.nT + l.nQ);
+	if(p >= sphOff) return sphere_center(l, p - sphOff);
+	if(p >= i32(l.nT)) {
+		const u32 q = u32(p - i32(l.nT)) * 4 + l.nT * 3;
+		return (((l.verts[l.idx[q]] + l.verts[l.idx[q + 1]]) + l.verts[l.idx[q + 2]]) + l.verts[l.idx[q + 3]]) / 4.0f;
+	}
+	const u32 t = u32(p) * 3;
+	return ((l.verts[l.idx[t]] + l.verts[l.idx[t + 1]]) + l.verts[l.idx[t + 2]]) / 3.0f;
+}
+// accel_structs_commons.hpp:85-103
+Box lod_box(const Lod& l, i32 p) {
+	const i32 sphOff = i32(l.nT + l.nQ);
+	if(p >= sphOff) {
+		V3 c = sphere_center(l, p - sphOff);
+		float r = sphere_radius(l, p - sphOff);
+		return { c - V3{ r, r, r }, c + V3{ r, r, r } };
+	}
+	Box b = empty_box();
+	if(p >= i32(l.nT)) {
+		const u32 q = u32(p - i32(l.nT)) * 4 + l.nT * 3;
+		for(int k = 0; k < 4; ++k) { b.mn = vmin(b.mn, l.verts[l.idx[q + k]]); b.mx = vmax(b.mx, l.verts[l.idx[q + k]]); }
+		return b;
+	}
+	const u32 t = u32(p) * 3;
+	for(int k = 0; k < 3; ++k) { b.mn = vmin(b.mn, l.verts[l.idx[t + k]]); b.mx = vmax(b.mx, l.verts[l.idx[t + k]]); }
+	return b;
+}
+
+// ---------------------------------------------------------------- LBVH
+// Build-time descriptor abstraction over LoDs (3 primitive types, clamped
+// 10-bit counts) and scenes (instances).
+struct BuildDesc {
+	bool isScene;
+	const Scene* scene;
+	const Lod* lod;
+	i32 numPrims;
+	Box bb;
+	std::vector<Box> instBoxes; // scene only
+	std::vector<V3> instCentroids;
+};
+
+struct Counts { i32 c[3]; };
+inline Counts prim_count(const BuildDesc& d, i32 p) {
+	if(d.isScene) return { { 1, 0, 0 } };
+	const Lod& l = *d.lod;
+	if(p >= i32(l.nT + l.nQ)) return { { 0, 0, 1 } };
+	if(p >= i32(l.nT)) return { { 0, 1, 0 } };
+	return { { 1, 0, 0 } };
+}
+inline Counts add(Counts a, Counts b) { return { { a.c[0] + b.c[0], a.c[1] + b.c[1], a.c[2] + b.c[2] } }; }
+inline Counts clamp_counts(const BuildDesc& d, Counts a) {
+	if(d.isScene) return a;
+	return { { std::min(a.c[0], 0x3FF), std::min(a.c[1], 0x3FF), std::min(a.c[2], 0x3FF) } };
+}
+// build_lbvh.cu:319-324 with the constants of build_lbvh.cu:35-48
+inline float get_cost(const BuildDesc& d, Counts c) {
+	if(d.isScene) return 1.0f + float(c.c[0]) * 8.5f;
+	return 2.0f + ((float(c.c[0]) * 1.2f + float(c.c[1]) * 4.0f) + float(c.c[2]) * 1.0f);
+}
+inline bool count_limit(const BuildDesc& d, Counts c) {
+	if(d.isScene) return c.c[0] >= 1023;
+	return c.c[0] >= 1023 || c.c[1] >= 1023 || c.c[2] >= 1023;
+}
+
+// build_lbvh.cu:164-178
+inline i32 lcp(const std::vector<u64>& k, i32 n, i32 i1, i32 i2, u64 key1) {
+	if(i2 < 0 || i2 >= n) return -1;
+	const u64 key2 = k[i2];
+	if(key1 == key2) return 64 + clz32(u32(i1 ^ i2));
+	return clz64(key1 ^ key2);
+}
+
+// build_lbvh.cu:180-245
+void karras_node(const std::vector<u64>& keys, i32 n, std::vector<i32>& parents, i32 idx) {
+	const u64 key1 = keys[idx];
+	const i32 lcp1 = lcp(keys, n, idx, idx + 1, key1);
+	const i32 lcp2 = lcp(keys, n, idx, idx - 1, key1);
+	const i32 direction = (lcp1 - lcp2) < 0 ? -1 : 1;
+	const i32 minLcp = lcp(keys, n, idx, idx - direction, key1);
+	i32 lMax = 2;
+	while(lcp(keys, n, idx, idx + lMax * direction, key1) > minLcp) lMax *= 2;
+	i32 l = 0;
+	for(i32 t = lMax; t > 1;) {
+		t = t / 2;
+		if(lcp(keys, n, idx, idx + (l + t) * direction, key1) > minLcp) l += t;
+	}
+	const i32 j = idx + l * direction;
+	const i32 nodeLcp = lcp(keys, n, idx, j, key1);
+	i32 s = 0;
+	const i32 maxDivisor = 1 << (32 - clz32(u32(l)));
+	for(i32 divisor = 2; divisor <= maxDivisor; divisor *= 2) {
+		const i32 t = (l + divisor - 1) / divisor;
+		if(lcp(keys, n, idx, idx + (s + t) * direction, key1) > nodeLcp) s += t;
+	}
+	const i32 split = idx + s * direction + std::min(direction, 0);
+	const i32 leftIndex = (std::min(idx, j) == split) ? split + n - 1 : split;
+	const i32 rightIndex = (std::max(idx, j) == split + 1) ? split + n : split + 1;
+	parents[leftIndex] = ~idx;
+	parents[rightIndex] = idx;
+	if(idx == 0) parents[0] = TREE_HEAD;
+}
+
+void build_lbvh(const BuildDesc& d, i32 numPrimitives, i32 actualPrimCount, Bvh& out) {
+	out = Bvh{};
+	out.numPrims = numPrimitives;
+	if(numPrimitives <= 0) return;
+	// build_lbvh.cu:595-602: a single primitive needs no hierarchy
+	if(actualPrimCount == 1) {
+		out.primIds = { 0 };
+		out.numInternal = 0;
+		// The mask (if any) still determines which instance is the valid one;
+		// the traversal goes through the single-instance shortcut instead.
+		return;
+	}
+	const i32 used = actualPrimCount != 0 ? actualPrimCount : numPrimitives;
+	const i32 numInternal = used - 1;
+	const i32 numNodes = numInternal + used;
+
+	// Morton codes (build_lbvh.cu:96-108)
+	std::vector<std::pair<u64, i32>> kv(numPrimitives);
+	for(i32 i = 0; i < numPrimitives; ++i) {
+		u64 code;
+		if(d.isScene) {
+			if(d.scene->instLod[i] == 0xFFFFFFFFu) code = ~0ull;
+			else code = morton63(d.instCentroids[i], d.bb);
+		} else {
+			code = morton63(lod_centroid(*d.lod, i), d.bb);
+		}
+		kv[i] = { code, i };
+	}
+	std::stable_sort(kv.begin(), kv.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+	out.mortonSorted.resize(numPrimitives);
+	out.primIds.resize(numPrimitives);
+	for(i32 i = 0; i < numPrimitives; ++i) { out.mortonSorted[i] = kv[i].first; out.primIds[i] = kv[i].second; }
+
+	// Karras hierarchy
+	out.parents.assign(numNodes, 0);
+	for(i32 i = 0; i < numInternal; ++i) karras_node(out.mortonSorted, used, out.parents, i);
+
+	// Children from the parent links (root: node 0)
+	std::vector<i32> leftChild(numInternal, -1), rightChild(numInternal, -1);
+	for(i32 nd = 1; nd < numNodes; ++nd) {
+		i32 p = out.parents[nd];
+		if(p < 0) leftChild[~p] = nd; else rightChild[p] = nd;
+	}
+
+	// Bottom-up boxes, SAH cost and counts (build_lbvh.cu:326-411), sequential
+	// order: the right child's thread is the arriving one.
+	std::vector<Box> box(numNodes);
+	std::vector<Counts> cnt(numNodes);
+	std::vector<float> cost(numNodes);
+	for(i32 i = 0; i < used; ++i) {
+		const i32 prim = out.primIds[i];
+		const i32 leaf = numInternal + i;
+		box[leaf] = d.isScene ? d.instBoxes[prim] : lod_box(*d.lod, prim);
+		cnt[leaf] = prim_count(d, prim);
+		cost[leaf] = get_cost(d, cnt[leaf]);
+	}
+	// post-order over internal nodes
+	{
+		std::vector<std::pair<i32, bool>> st;
+		st.push_back({ 0, false });
+		while(!st.empty()) {
+			auto [nd, expanded] = st.back();
+			st.pop_back();
+			if(nd >= numInternal) continue;
+			if(!expanded) {
+				st.push_back({ nd, true });
+				st.push_back({ rightChild[nd], false });
+				st.push_back({ leftChild[nd], false });
+				continue;
+			}
+			const i32 L = leftChild[nd], R = rightChild[nd];
+			const float currentSA = surface(box[R]);
+			Box b = { vmin(box[R].mn, box[L].mn), vmax(box[R].mx, box[L].mx) };
+			const float newSA = surface(b);
+			const float otherSA = surface(box[L]);
+			const float nodeCost = d.isScene ? 1.0f : 2.0f;
+			cost[nd] = (nodeCost + (currentSA / newSA) * get_cost(d, clamp_counts(d, cnt[R])))
+				+ (otherSA / newSA) * get_cost(d, clamp_counts(d, cnt[L]));
+			cnt[nd] = add(cnt[R], cnt[L]);
+			box[nd] = b;
+		}
+	}
+	// Marks (build_lbvh.cu:417-463)
+	std::vector<i32> marks(numInternal, 1);
+	for(i32 i = 0; i < used; ++i) {
+		const i32 leaf = numInternal + i;
+		i32 collapseNode = -1;
+		i32 cur = out.parents[leaf];
+		if(cur < 0) cur = ~cur;
+		while(cur != 0) {
+			const Counts c = clamp_counts(d, cnt[cur]);
+			if(count_limit(d, c)) break;
+			if(get_cost(d, c) < cost[cur]) collapseNode = cur;
+			cur = out.parents[cur];
+			if(cur < 0) cur = ~cur;
+		}
+		if(collapseNode != -1) {
+			cur = out.parents[leaf];
+			if(cur < 0) cur = ~cur;
+			while(cur != collapseNode) {
+				marks[cur] = 0;
+				cur = out.parents[cur];
+				if(cur < 0) cur = ~cur;
+			}
+			marks[cur] = 0;
+		}
+	}
+	// Inclusive scan
+	std::vector<i32> offsets(numInternal);
+	i32 acc = 0;
+	for(i32 i = 0; i < numInternal; ++i) { acc += marks[i]; offsets[i] = acc; }
+	const i32 after = offsets[numInternal - 1];
+	out.numInternal = after;
+	out.nodes.assign(size_t(after) * 2, BvhNode{ { 0, 0, 0 }, { 0, 0, 0 }, 0, 0 });
+	auto is_collapsed = [&](i32 nd) {
+		if(nd > 0 && nd < numInternal) return (offsets[nd] - offsets[nd - 1]) == 0;
+		return false;
+	};
+	// build_lbvh.cu:511-566
+	for(i32 nd = 1; nd < numNodes; ++nd) {
+		if(is_collapsed(nd)) continue;
+		i32 parent = out.parents[nd];
+		i32 offset;
+		if(parent < 0) { offset = 0; parent = ~parent; } else offset = 1;
+		i32 finalNode = nd;
+		bool skip = false;
+		if(finalNode >= numInternal) {
+			while(is_collapsed(parent)) {
+				if(offset == 1) { skip = true; break; }
+				finalNode = parent;
+				parent = out.parents[parent];
+				if(parent < 0) { offset = 0; parent = ~parent; } else offset = 1;
+			}
+		}
+		if(skip) continue;
+		const Counts c = clamp_counts(d, cnt[finalNode]);
+		const i32 primCount = d.isScene ? c.c[0] : (c.c[0] + c.c[1] + c.c[2]);
+		const i32 outIdx = (offsets[parent] - 1) * 2;
+		const i32 outNode = (nd >= numInternal) ? nd - numInternal + after : offsets[nd] - 1;
+		const Box b = box[finalNode];
+		const V3 ctr = (b.mn + b.mx) * 0.5f;
+		BvhNode node;
+		node.mn = (b.mn - ctr) * 1.0001f + ctr;
+		node.mx = (b.mx - ctr) * 1.0001f + ctr;
+		node.index = outNode;
+		node.primCount = primCount;
+		out.nodes[outIdx + offset] = node;
+	}
+}
+
+// ---------------------------------------------------------------- rays
+struct FastRay {
+	V3 o, d, inv, oDiv;
+	// watertight test precomputation
+	int kx, ky, kz;
+	float Sx, Sy, Sz;
+};
+FastRay make_ray(V3 o, V3 d) {
+	FastRay r;
+	r.o = o; r.d = d;
+	r.inv = { 1.0f / d.x, 1.0f / d.y, 1.0f / d.z };
+	r.oDiv = o * r.inv;
+	const float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+	int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+	int kx = kz + 1 == 3 ? 0 : kz + 1;
+	int ky = kx + 1 == 3 ? 0 : kx + 1;
+	if(d[kz] < 0.0f) std::swap(kx, ky);
+	r.kx = kx; r.ky = ky; r.kz = kz;
+	r.Sx = d[kx] / d[kz];
+	r.Sy = d[ky] / d[kz];
+	r.Sz = 1.0f / d[kz];
+	return r;
+}
+
+// intersection.cu:47-77 (GPU form)
+inline bool box_test(const V3& mn, const V3& mx, const FastRay& r, float tmax, float& cmin) {
+	const float lox = mbmath::fma_(mn.x, r.inv.x, -r.oDiv.x);
+	const float loy = mbmath::fma_(mn.y, r.inv.y, -r.oDiv.y);
+	const float loz = mbmath::fma_(mn.z, r.inv.z, -r.oDiv.z);
+	const float hix = mbmath::fma_(mx.x, r.inv.x, -r.oDiv.x);
+	const float hiy = mbmath::fma_(mx.y, r.inv.y, -r.oDiv.y);
+	const float hiz = mbmath::fma_(mx.z, r.inv.z, -r.oDiv.z);
+	cmin = fmax_(fmax_(fmin_(lox, hix), fmin_(loy, hiy)), fmax_(fmin_(loz, hiz), 0.0f));
+	const float cmax = fmin_(fmin_(fmax_(lox, hix), fmax_(loy, hiy)), fmin_(fmax_(loz, hiz), tmax));
+	return cmin <= cmax;
+}
+
+// Watertight ray/triangle test; returns t and the barycentric weights of v0, v1.
+inline bool tri_test(const FastRay& r, V3 v0, V3 v1, V3 v2, float& t, V2& bary) {
+	const V3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+	const float Ax = A[r.kx] - r.Sx * A[r.kz];
+	const float Ay = A[r.ky] - r.Sy * A[r.kz];
+	const float Bx = B[r.kx] - r.Sx * B[r.kz];
+	const float By = B[r.ky] - r.Sy * B[r.kz];
+	const float Cx = C[r.kx] - r.Sx * C[r.kz];
+	const float Cy = C[r.ky] - r.Sy * C[r.kz];
+	float U = Cx * By - Cy * Bx;
+	float V = Ax * Cy - Ay * Cx;
+	float W = Bx * Ay - By * Ax;
+	if(U == 0.0f || V == 0.0f || W == 0.0f) {
+		U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+		V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+		W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+	}
+	if((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+	const float det = U + V + W;
+	if(det == 0.0f) return false;
+	const float Az = r.Sz * A[r.kz];
+	const float Bz = r.Sz * B[r.kz];
+	const float Cz = r.Sz * C[r.kz];
+	const float T = U * Az + V * Bz + W * Cz;
+	t = T / det;
+	bary = { U / det, V / det };
+	return true;
+}
+
+// a x^2 + b x + c = 0 (real roots, x0 <= x1)
+inline bool solve_square(float a, float b, float c, float& x0, float& x1) {
+	if(a == 0.0f) {
+		if(b == 0.0f) return false;
+		x0 = x1 = -c / b;
+		return true;
+	}
+	const float disc = b * b - 4.0f * a * c;
+	if(disc < 0.0f) return false;
+	const float q = -0.5f * (b + sgn(b) * mbmath::sqrt(disc));
+	if(q == 0.0f) { x0 = x1 = 0.0f; return true; }
+	float r0 = q / a, r1 = c / q;
+	if(r0 > r1) std::swap(r0, r1);
+	x0 = r0; x1 = r1;
+	return true;
+}
+
+inline float pabs(float x) { return x < 0.0f ? -x : x; }
+
+// intersection.cu:85-94
+inline float computeU(float v, float A1, float A2, float B1, float B2, float C1, float C2, float D1, float D2) {
+	const float a = v * A2 + B2;
+	const float b = v * (A2 - A1) + B2 - B1;
+	if(std::fabs(b) >= std::fabs(a)) return (v * (C1 - C2) + D1 - D2) / b;
+	return (-v * C2 - D2) / a;
+}
+
+// intersection.cu:99-179 (Ramsey et al. 2004 bilinear patch)
+bool quad_test(V3 p00, V3 p10, V3 p11, V3 p01, const FastRay& ray, float& resT1, float& resT2, V2& uv1, V2& uv2) {
+	int d0 = 0, d1 = 1, d2 = 2;
+	if(pabs(ray.d.x) < pabs(ray.d.y) || pabs(ray.d.x) < pabs(ray.d.z)) {
+		if(pabs(ray.d.y) >= pabs(ray.d.z)) { d0 = 1; d1 = 0; d2 = 2; }
+		else { d0 = 2; d1 = 1; d2 = 0; }
+	}
+	const V3 a = ((p11 - p10) - p01) + p00;
+	const V3 b = p10 - p00;
+	const V3 c = p01 - p00;
+	const V3 d = p00 - ray.o;
+	const float A1 = a[d1] * ray.d[d0] - a[d0] * ray.d[d1];
+	const float A2 = a[d2] * ray.d[d0] - a[d0] * ray.d[d2];
+	const float B1 = b[d1] * ray.d[d0] - b[d0] * ray.d[d1];
+	const float B2 = b[d2] * ray.d[d0] - b[d0] * ray.d[d2];
+	const float C1 = c[d1] * ray.d[d0] - c[d0] * ray.d[d1];
+	const float C2 = c[d2] * ray.d[d0] - c[d0] * ray.d[d2];
+	const float D1 = d[d1] * ray.d[d0] - d[d0] * ray.d[d1];
+	const float D2 = d[d2] * ray.d[d0] - d[d0] * ray.d[d2];
+	float v0 = 0.0f, v1 = 0.0f;
+	if(solve_square(A2 * C1 - A1 * C2, ((A2 * D1 - A1 * D2) + B2 * C1) - B1 * C2, B2 * D1 - B1 * D2, v0, v1)) {
+		float u0 = 0.0f, u1 = 0.0f;
+		float t0 = -1.0f, t1 = -1.0f;
+		if(v0 >= 0.0f && v0 <= 1.0f) {
+			u0 = computeU(v0, A1, A2, B1, B2, C1, C2, D1, D2);
+			if(u0 >= 0.0f && u0 <= 1.0f)
+				t0 = ((((u0 * v0) * a[d0] + u0 * b[d0]) + v0 * c[d0]) + d[d0]) * ray.inv[d0];
+		}
+		if(v1 == v0) {
+			uv1 = { u0, v0 };
+			resT1 = t0;
+			resT2 = -1.0f;
+		} else {
+			if(v1 >= 0.0f && v1 <= 1.0f) {
+				u1 = computeU(v1, A1, A2, B1, B2, C1, C2, D1, D2);
+				if(u1 >= 0.0f && u1 <= 1.0f)
+					t1 = ((((u1 * v1) * a[d0] + u1 * b[d0]) + v1 * c[d0]) + d[d0]) * ray.inv[d0];
+			}
+			if(t0 > 0.0f) {
+				if(t1 > 0.0f && t1 < t0) { uv1 = { u1, v1 }; uv2 = { u0, v0 }; resT1 = t1; resT2 = t0; }
+				else { uv2 = { u1, v1 }; uv1 = { u0, v0 }; resT2 = t1; resT1 = t0; }
+			} else {
+				uv1 = { u1, v1 }; uv2 = { u0, v0 }; resT1 = t1; resT2 = t0;
+			}
+		}
+		return resT1 > 0.0f;
+	}
+	return false;
+}
+
+// Ray/sphere: nearest root with t > 0.
+inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t) {
+	const V3 oc = r.o - c;
+	const float b = dot(oc, r.d);
+	const float cc = dot(oc, oc) - rad * rad;
+	const float disc = b * b - cc;
+	if(disc < 0.0f) return false;
+	const float q = -(b + sgn(b) * mbmath::sqrt(disc));
+	float x0, x1;
+	if(q == 0.0f) { x0 = x1 = 0.0f; }
+	else { x0 = q; x1 = cc / q; if(x0 > x1) std::swap(x0, x1); }
+	if(x0 > 0.0f) { t = x0; return true; }
+	if(x1 > 0.0f) { t = x1; return true; }
+	return false;
+}
+
+// Primitive test in object space: returns the object-space t (> 0) and the
+// surface parametrisation. intersection.cu:181-316 without the alpha test.
+inline bool prim_test(const Lod& l, const FastRay& r, i32 p, float& t, V2& sp, Counters& cnt) {
+	if(p < i32(l.nT)) {
+		++cnt.tri;
+		const u32 o = u32(p) * 3;
+		if(tri_test(r, l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], t, sp)) return t > 0.0f;
+		return false;
+	}
+	if(p < i32(l.nT + l.nQ)) {
+		++cnt.quad;
+		const u32 o = u32(p - i32(l.nT)) * 4 + l.nT * 3;
+		float t1, t2; V2 b1, b2;
+		if(quad_test(l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], l.verts[l.idx[o + 3]], r, t1, t2, b1, b2)) {
+			t = t1; sp = b1;
+			return true;
+		}
+		return false;
+	}
+	++cnt.sphere;
+	const i32 s = p - i32(l.nT + l.nQ);
+	if(sphere_test(r, sphere_center(l, s), sphere_radius(l, s), t)) { sp = { 0, 0 }; return true; }
+	return false;
+}
+
+inline void add_epsilon(V3& o, V3 dir, V3 n) {
+	const V3 off = n * SCENE_SCALE_EPS;
+	if(dot(n, dir) >= 0.0f) o = o + off; else o = o - off;
+}
+
+struct InstRay { FastRay ray; float scale; };
+// intersection.cu:322-348
+inline InstRay instance_ray(const Scene& S, u32 inst, V3 o, V3 d) {
+	const Mat34& W = S.w2i[inst];
+	const V3 dirO = xform_dir(W, d);
+	const float scale = len(dirO);
+	InstRay ir;
+	ir.ray = make_ray(xform_point(W, o), dirO / scale);
+	ir.scale = scale;
+	return ir;
+}
+
+struct HitRec {
+	float t;
+	i32 inst, prim;
+	V2 sp;
+	bool has;
+};
+
+inline bool better(float tw, i32 inst, i32 prim, const HitRec& h) {
+	if(tw < h.t) return true;
+	if(h.has && tw == h.t) return inst < h.inst || (inst == h.inst && prim < h.prim);
+	return false;
+}
+
+// BVH traversal inside one instance (closest hit). The stack discipline is
+// the reference's (near child first, far child pushed); the result is order
+// independent because of the (t, inst, prim) ordering.
+void blas_closest(const Scene& S, u32 inst, const InstRay& ir, HitRec& best, Counters& cnt) {
+	const Lod& l = S.lods[S.instLod[inst]];
+	const Bvh& bvh = S.lodBvh[S.instLod[inst]];
+	auto consider = [&](i32 p) {
+		float t; V2 sp;
+		if(prim_test(l, ir.ray, p, t, sp, cnt)) {
+			const float tw = t / ir.scale;
+			if(better(tw, i32(inst), p, best)) best = { tw, i32(inst), p, sp, true };
+		}
+	};
+	if(l.numPrims <= 0) return;
+	if(l.numPrims == 1) { consider(0); return; }
+	const i32 nInt = bvh.numInternal;
+	i32 stack[192];
+	i32 sp = 0;
+	i32 node = 0;
+	for(;;) {
+		// node < nInt: internal
+		if(node < nInt) {
+			++cnt.nodeVisits;
+			const BvhNode& L = bvh.nodes[2 * node];
+			const BvhNode& R = bvh.nodes[2 * node + 1];
+			const float tmaxBox = best.t * ir.scale * BOX_SLACK;
+			float c0, c1;
+			const bool h0 = box_test(L.mn, L.mx, ir.ray, tmaxBox, c0);
+			const bool h1 = box_test(R.mn, R.mx, ir.ray, tmaxBox, c1);
+			if(!h0) c0 = 1e38f;
+			if(!h1) c1 = 1e38f;
+			if(h0 && h1) {
+				const BvhNode& far = (c1 < c0) ? L : R;
+				stack[sp++] = far.index;
+				stack[sp++] = far.primCount;
+			}
+			if(h0 || h1) {
+				const BvhNode& nearN = (c0 <= c1) ? L : R;
+				if(nearN.index < nInt) { node = nearN.index; continue; }
+				const i32 first = nearN.index - nInt;
+				for(i32 k = 0; k < nearN.primCount; ++k) consider(bvh.primIds[first + k]);
+			}
+		} else {
+			// unreachable: leaves are handled at their parent
+		}
+		// pop
+		bool found = false;
+		while(sp > 0) {
+			const i32 pc = stack[--sp];
+			const i32 idx = stack[--sp];
+			if(idx < nInt) { node = idx; found = true; break; }
+			const i32 first = idx - nInt;
+			for(i32 k = 0; k < pc; ++k) consider(bvh.primIds[first + k]);
+		}
+		if(!found) break;
+	}
+}
+
+bool blas_any(const Scene& S, u32 inst, const InstRay& ir, float tmaxObj, Counters& cnt) {
+	const Lod& l = S.lods[S.instLod[inst]];
+	const Bvh& bvh = S.lodBvh[S.instLod[inst]];
+	auto hits = [&](i32 p) {
+		float t; V2 sp;
+		return prim_test(l, ir.ray, p, t, sp, cnt) && t < tmaxObj;
+	};
+	if(l.numPrims <= 0) return false;
+	if(l.numPrims == 1) return hits(0);
+	const i32 nInt = bvh.numInternal;
+	const float tmaxBox = tmaxObj * BOX_SLACK;
+	i32 stack[192];
+	i32 sp = 0;
+	i32 node = 0;
+	for(;;) {
+		++cnt.nodeVisits;
+		const BvhNode& L = bvh.nodes[2 * node];
+		const BvhNode& R = bvh.nodes[2 * node + 1];
+		float c0, c1;
+		const bool h0 = box_test(L.mn, L.mx, ir.ray, tmaxBox, c0);
+		const bool h1 = box_test(R.mn, R.mx, ir.ray, tmaxBox, c1);
+		if(!h0) c0 = 1e38f;
+		if(!h1) c1 = 1e38f;
+		if(h0 && h1) {
+			const BvhNode& far = (c1 < c0) ? L : R;
+			stack[sp++] = far.index;
+			stack[sp++] = far.primCount;
+		}
+		if(h0 || h1) {
+			const BvhNode& nearN = (c0 <= c1) ? L : R;
+			if(nearN.index < nInt) { node = nearN.index; continue; }
+			const i32 first = nearN.index - nInt;
+			for(i32 k = 0; k < nearN.primCount; ++k) if(hits(bvh.primIds[first + k])) return true;
+		}
+		bool found = false;
+		while(sp > 0) {
+			const i32 pc = stack[--sp];
+			const i32 idx = stack[--sp];
+			if(idx < nInt) { node = idx; found = true; break; }
+			const i32 first = idx - nInt;
+			for(i32 k = 0; k < pc; ++k) if(hits(bvh.primIds[first + k])) return true;
+		}
+		if(!found) return false;
+	}
+}
+
+// Instance entry: object AABB test (intersection.cu:335-346)
+inline bool enter_instance(const Scene& S, u32 inst, V3 o, V3 d, float tmaxWorld, InstRay& ir, Counters& cnt) {
+	++cnt.instanceVisits;
+	ir = instance_ray(S, inst, o, d);
+	const Box& ob = S.lods[S.instLod[inst]].aabb;
+	float c;
+	return box_test(ob.mn, ob.mx, ir.ray, tmaxWorld * ir.scale * BOX_SLACK, c);
+}
+
+template < class F >
+void tlas_visit(const Scene& S, const FastRay& wr, const float* tmaxWorld, F&& onInstance, Counters& cnt, bool& stop) {
+	stop = false;
+	if(S.activeInstances <= 0) return;
+	if(S.activeInstances == 1) { onInstance(S.validInstance); return; }
+	const Bvh& bvh = S.tlas;
+	const i32 nInt = bvh.numInternal;
+	i32 stack[192];
+	i32 sp = 0;
+	i32 node = 0;
+	for(;;) {
+		++cnt.nodeVisits;
+		const BvhNode& L = bvh.nodes[2 * node];
+		const BvhNode& R = bvh.nodes[2 * node + 1];
+		const float tmaxBox = *tmaxWorld * BOX_SLACK;
+		float c0, c1;
+		const bool h0 = box_test(L.mn, L.mx, wr, tmaxBox, c0);
+		const bool h1 = box_test(R.mn, R.mx, wr, tmaxBox, c1);
+		if(!h0) c0 = 1e38f;
+		if(!h1) c1 = 1e38f;
+		if(h0 && h1) {
+			const BvhNode& far = (c1 < c0) ? L : R;
+			stack[sp++] = far.index;
+			stack[sp++] = far.primCount;
+		}
+		if(h0 || h1) {
+			const BvhNode& nearN = (c0 <= c1) ? L : R;
+			if(nearN.index < nInt) { node = nearN.index; continue; }
+			const i32 first = nearN.index - nInt;
+			for(i32 k = 0; k < nearN.primCount && !stop; ++k) onInstance(u32(bvh.primIds[first + k]));
+			if(stop) return;
+		}
+		bool found = false;
+		while(sp > 0) {
+			const i32 pc = stack[--sp];
+			const i32 idx = stack[--sp];
+			if(idx < nInt) { node = idx; found = true; break; }
+			const i32 first = idx - nInt;
+			for(i32 k = 0; k < pc && !stop; ++k) onInstance(u32(bvh.primIds[first + k]));
+			if(stop) return;
+		}
+		if(!found) return;
+	}
+}
+
+struct Intersection {
+	float distance;
+	i32 inst, prim;
+	V3 normal, tangentX;
+	V2 uv;
+	V2 sp;
+};
+
+inline V2 bilerp2(V2 x00, V2 x10, V2 x01, V2 x11, float s, float t) {
+	const V2 a = (1.0f - s) * x00 + s * x10;
+	const V2 b = (1.0f - s) * x01 + s * x11;
+	return (1.0f - t) * a + t * b;
+}
+inline V3 bilerp3(V3 x00, V3 x10, V3 x01, V3 x11, float s, float t) {
+	const V3 a = (1.0f - s) * x00 + s * x10;
+	const V3 b = (1.0f - s) * x01 + s * x11;
+	return (1.0f - t) * a + t * b;
+}
+
+// intersection.cu:366-621
+Intersection first_intersection(const Scene& S, V3& origin, V3 dir, V3 geoN, float tmax, Counters& cnt) {
+	add_epsilon(origin, dir, geoN);
+	++cnt.rays;
+	const FastRay wr = make_ray(origin, dir);
+	HitRec best = { tmax, -1, -1, { 0, 0 }, false };
+	bool stop;
+	tlas_visit(S, wr, &best.t, [&](u32 inst) {
+		InstRay ir;
+		if(enter_instance(S, inst, origin, dir, best.t, ir, cnt)) blas_closest(S, inst, ir, best, cnt);
+	}, cnt, stop);
+	Intersection res;
+	res.distance = best.t;
+	res.inst = best.has ? best.inst : -1;
+	res.prim = best.has ? best.prim : -1;
+	res.sp = best.sp;
+	res.uv = { 0, 0 };
+	res.normal = { 0, 0, 0 };
+	res.tangentX = { 0, 0, 0 };
+	if(!best.has) return res;
+	const Lod& l = S.lods[S.instLod[best.inst]];
+	const Mat34& W = S.w2i[best.inst];
+	V3 geoNormal, tangentX;
+	V2 uv;
+	const i32 p = best.prim;
+	const i32 sphOff = i32(l.nT + l.nQ);
+	if(p >= sphOff) {
+		const i32 s = p - sphOff;
+		const V3 hitPoint = origin + best.t * dir;
+		const V3 local = xform_point(W, hitPoint);
+		geoNormal = normalize(local - sphere_center(l, s));
+		if(geoNormal.x == 0.0f && geoNormal.y == 0.0f) tangentX = { 1, 0, 0 };
+		else {
+			const float ll = mbmath::sqrt(geoNormal.y * geoNormal.y + (-geoNormal.x) * (-geoNormal.x));
+			tangentX = { geoNormal.y / ll, -geoNormal.x / ll, 0.0f };
+		}
+		uv.x = mbmath::atan2(geoNormal.z, geoNormal.x) / (2.0f * PI) + 0.5f;
+		uv.y = mbmath::acos(-geoNormal.y) / PI;
+		res.sp = uv;
+	} else if(p < i32(l.nT)) {
+		const u32 o = u32(p) * 3;
+		const u32 i0 = l.idx[o], i1 = l.idx[o + 1], i2 = l.idx[o + 2];
+		const V3 dx0 = l.verts[i1] - l.verts[i0];
+		const V3 dx1 = l.verts[i2] - l.verts[i0];
+		const V2 du0 = l.uvs[i1] - l.uvs[i0];
+		const V2 du1 = l.uvs[i2] - l.uvs[i0];
+		const float det = du0.x * du1.y - du0.y * du1.x;
+		if(det >= 1e-5f || det <= -1e5f) tangentX = (dx0 * du1.y - dx1 * du0.y) / det;
+		else tangentX = dx0;
+		geoNormal = cross(dx0, dx1);
+		uv = (l.uvs[i0] * best.sp.x + l.uvs[i1] * best.sp.y) + l.uvs[i2] * ((1.0f - best.sp.x) - best.sp.y);
+	} else {
+		const u32 o = u32(p - i32(l.nT)) * 4 + l.nT * 3;
+		const V3 v0 = l.verts[l.idx[o]], v1 = l.verts[l.idx[o + 1]], v2 = l.verts[l.idx[o + 2]], v3 = l.verts[l.idx[o + 3]];
+		const V2 t0 = l.uvs[l.idx[o]], t1 = l.uvs[l.idx[o + 1]], t2 = l.uvs[l.idx[o + 2]], t3 = l.uvs[l.idx[o + 3]];
+		const float bu = best.sp.x, bv = best.sp.y;
+		const V3 dxds = (1.0f - bu) * (v3 - v0) + bu * (v2 - v1);
+		const V3 dxdt = (1.0f - bv) * (v1 - v0) + bv * (v2 - v3);
+		const V2 duds = (1.0f - bu) * (t3 - t0) + bu * (t2 - t1);
+		const V2 dudt = (1.0f - bv) * (t1 - t0) + bv * (t2 - t3);
+		const float detD = duds.x * dudt.y - dudt.x * duds.y;
+		if(detD >= 1e-9f || detD <= -1e-9f) {
+			const float a = dudt.y / detD, b = -duds.y / detD;
+			tangentX = { dxds.x * a + dxdt.x * b, dxds.y * a + dxdt.y * b, dxds.z * a + dxdt.z * b };
+		} else tangentX = dxds;
+		geoNormal = cross(dxdt, dxds);
+		uv = bilerp2(t0, t1, t3, t2, bu, bv);
+	}
+	res.normal = normalize(xform_transposed(W, geoNormal));
+	res.tangentX = normalize(xform_transposed(W, tangentX));
+	if(p < sphOff) res.uv = uv; else res.uv = res.sp;
+	return res;
+}
+
+// intersection.cu:624-753
+bool any_intersection(const Scene& S, V3 a, V3 b, V3 geoA, V3 geoB, V3 dirAB, Counters& cnt) {
+	add_epsilon(a, dirAB, geoA);
+	add_epsilon(b, -dirAB, geoB);
+	++cnt.rays; ++cnt.shadowRays;
+	const V3 corrected = b - a;
+	const float tmax = len(corrected);
+	const V3 dir = corrected / tmax;
+	const FastRay wr = make_ray(a, dir);
+	bool occluded = false;
+	bool stop = false;
+	float tm = tmax;
+	tlas_visit(S, wr, &tm, [&](u32 inst) {
+		InstRay ir;
+		if(enter_instance(S, inst, a, dir, tmax, ir, cnt) && blas_any(S, inst, ir, tmax * ir.scale, cnt)) {
+			occluded = true;
+			stop = true;
+		}
+	}, cnt, stop);
+	return occluded;
+}
+
+struct TangentSpace { V3 shadingN, geoN, shadingTX, shadingTY; };
+
+// tangent_space.hpp:10-66
+TangentSpace tangent_space(const Scene& S, const Intersection& h) {
+	const Lod& l = S.lods[S.instLod[h.inst]];
+	const Mat34& W = S.w2i[h.inst];
+	if(u32(h.prim) >= l.nT + l.nQ) return { h.normal, h.normal, h.tangentX, cross(h.normal, h.tangentX) };
+	V3 sn;
+	if(u32(h.prim) < l.nT) {
+		const u32 o = 3u * u32(h.prim);
+		sn = (h.sp.x * l.normals[l.idx[o]] + h.sp.y * l.normals[l.idx[o + 1]])
+			+ (1.0f - (h.sp.x + h.sp.y)) * l.normals[l.idx[o + 2]];
+	} else {
+		const u32 o = 4u * u32(h.prim - i32(l.nT)) + 3u * l.nT;
+		sn = bilerp3(l.normals[l.idx[o]], l.normals[l.idx[o + 1]], l.normals[l.idx[o + 3]], l.normals[l.idx[o + 2]], h.sp.x, h.sp.y);
+	}
+	sn = normalize(xform_transposed(W, sn));
+	const V3 tx = normalize(h.tangentX - sn * dot(h.tangentX, sn));
+	const V3 ty = cross(sn, tx);
+	return { sn, h.normal, tx, ty };
+}
+
+// ---------------------------------------------------------------- materials
+struct Params { i32 type; V3 albedo; V2 roughness; V3 radiance; };
+
+inline V3 sample_texture(const Texture& t, V2 uv) {
+	// nearest sampling with wrap-around
+	float fx = uv.x - std::floor(uv.x), fy = uv.y - std::floor(uv.y);
+	i32 x = i32(fx * float(t.w)), y = i32(fy * float(t.h));
+	if(x >= i32(t.w)) x = i32(t.w) - 1;
+	if(y >= i32(t.h)) y = i32(t.h) - 1;
+	const float* p = &t.texels[(size_t(y) * t.w + x) * 4];
+	return { p[0], p[1], p[2] };
+}
+
+inline Params fetch_material(const Scene& S, u16 matIdx, V2 uv) {
+	const Material& m = S.materials[matIdx];
+	Params p;
+	p.type = m.type;
+	p.albedo = (m.albedoTex >= 0) ? sample_texture(S.textures[m.albedoTex], uv) : m.albedo;
+	p.roughness = m.roughness;
+	p.radiance = m.radiance * m.scale;
+	return p;
+}
+
+inline u16 material_index(const Scene& S, i32 inst, i32 prim) {
+	const Lod& l = S.lods[S.instLod[inst]];
+	const u32 faces = l.nT + l.nQ;
+	if(u32(prim) < faces) return l.faceMat[prim];
+	return l.sphereMat[u32(prim) - faces];
+}
+
+struct PathSample { V3 throughput; bool valid; V3 excident; float pdfF, pdfB; };
+struct EvalValue { V3 value; float cosOut; float pdfF, pdfB; };
+
+// sampling.hpp:175-181
+inline V3 sample_dir_cosine(float u0, float u1, float& cosTheta) {
+	cosTheta = mbmath::sqrt(u0);
+	const float sinTheta = mbmath::sqrt(1.0f - u0);
+	const float phi = u1 * 2.0f * PI;
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	return { sinTheta * s, sinTheta * c, cosTheta };
+}
+// sampling.hpp:184-192
+inline V3 sample_dir_sphere_uniform(float u0, float u1) {
+	const float cosTheta = u0 * 2.0f - 1.0f;
+	const float sinTheta = mbmath::sqrt((1.0f - cosTheta) * (1.0f + cosTheta));
+	const float phi = u1 * 2.0f * PI;
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	return { sinTheta * s, sinTheta * c, cosTheta };
+}
+inline float projected_area(V3 dir, Box b) {
+	const V3 sides = b.mx - b.mn;
+	const float ax = sides.y * sides.z * std::fabs(dir.x);
+	const float ay = sides.x * sides.z * std::fabs(dir.y);
+	const float az = sides.x * sides.y * std::fabs(dir.z);
+	return ax + ay + az;
+}
+
+// microfacet_base.hpp:85-112 (GGX branch)
+inline float geo_smith(float wDotH, V3 w, V2 r) {
+	if(wDotH * w.z <= 0.0f) return 0.0f;
+	const float a = w.x * r.x, b = w.y * r.y;
+	const float oneOverASq = sdiv(a * a + b * b, w.z * w.z);
+	return 2.0f / (1.0f + mbmath::sqrt(1.0f + oneOverASq));
+}
+// microfacet_base.hpp:296-308
+inline float eval_ggx(V2 r, V3 h) {
+	const float norm = fmax_(PI * r.x * r.y, 1e-30f);
+	const float cosThetaSq = h.z * h.z;
+	const float rx = sdiv(h.x, r.x), ry = sdiv(h.y, r.y);
+	const float tmp = rx * rx + ry * ry + cosThetaSq;
+	return sdiv(1.0f, norm * tmp * tmp);
+}
+// microfacet_base.hpp:227-259
+inline V2 sample_slopes_ggx(float tanTheta, float u0, float u1, u64& rnd2) {
+	// The reference compares against the double 0.0001; for a float x,
+	// x < 0.0001 (double) <=> x <= 0.0001f.
+	if(tanTheta <= 0.0001f) {
+		const float r = mbmath::sqrt(sdiv(u0, 1.0f - u0));
+		const float phi = 6.28318530718f * u1;
+		float s, c;
+		mbmath::sincos(phi, s, c);
+		return { r * c, r * s };
+	}
+	const float a1 = 1.0f / tanTheta;
+	const float g1 = 2.0f / (1.0f + mbmath::sqrt(1.0f + 1.0f / (a1 * a1)));
+	const float a = 2.0f * u0 / g1 - 1.0f;
+	const float tmp = sdiv(1.0f, a * a - 1.0f);
+	const float d = tmp * mbmath::sqrt(tanTheta * tanTheta - (a * a - tanTheta * tanTheta) / tmp);
+	const float sx1 = tanTheta * tmp - d;
+	const float sx2 = tanTheta * tmp + d;
+	const float slopeX = (a < 0.0f || sx2 > 1.0f / tanTheta) ? sx1 : sx2;
+	float s;
+	if(rnd2 & (1ull << 63)) { rnd2 *= 2; s = 1.0f; } else { rnd2 *= 2; s = -1.0f; }
+	const float z = sdiv(u1 * (u1 * (u1 * 0.27385f - 0.73369f) + 0.46341f),
+	                     u1 * (u1 * (u1 * 0.093073f + 0.309420f) - 1.000000f) + 0.597999f);
+	const float slopeY = s * z * mbmath::sqrt(1.0f + slopeX * slopeX);
+	return { slopeX, slopeY };
+}
+// microfacet_base.hpp:262-293
+inline V3 sample_visible_normal_smith(V3 inc, V2 r, float u0, float u1, u64& rnd2) {
+	V3 st = normalize(inc * V3{ r.x, r.y, 1.0f });
+	if(inc.z < 0.0f) st = -st;
+	const float sinTheta = mbmath::sqrt((1.0f - st.z) * (1.0f + st.z));
+	const float tanTheta = sinTheta / st.z;
+	const float cosPhi = sinTheta > 1e-5f ? st.x / sinTheta : 0.0f;
+	const float sinPhi = sinTheta > 1e-5f ? st.y / sinTheta : 0.0f;
+	V2 sl = sample_slopes_ggx(tanTheta, u0, u1, rnd2);
+	const float tmp = cosPhi * sl.x - sinPhi * sl.y;
+	sl.y = sinPhi * sl.x + cosPhi * sl.y;
+	sl.x = tmp;
+	sl.x *= r.x;
+	sl.y *= r.y;
+	return normalize(V3{ -sl.x, -sl.y, 1.0f });
+}
+
+// half vector for vacuum on both sides (microfacet_base.hpp:15-27)
+inline V3 half_vector(V3 inTS, V3 exTS) {
+	const V3 h = 1.0f * inTS + 1.0f * exTS;
+	const float l = len(h) * sgn(h.z);
+	return { sdiv(h.x, l), sdiv(h.y, l), sdiv(h.z, l) };
+}
+
+// material_sampling.hpp:77-141 with the Lambert / Torrance(Smith, GGX) / Emissive samplers
+PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident, float u0, float u1, u64 i0) {
+	PathSample none = { { 0, 0, 0 }, false, { 0, 0, 0 }, 0, 0 };
+	const float iDotG = -dot(incident, ts.geoN);
+	const float iDotN = -dot(incident, ts.shadingN);
+	if(iDotG * iDotN <= 0.0f) return none;
+	const V3 inTS = { -dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN };
+	PathSample res = none;
+	if(p.type == OR_MAT_LAMBERT) {
+		float cosT;
+		const V3 e = sample_dir_cosine(u0, u1, cosT);
+		res = { p.albedo, true, e * sgn(inTS.z), e.z / PI, std::fabs(inTS.z) / PI };
+	} else if(p.type == OR_MAT_TORRANCE) {
+		u64 rnd = i0;
+		const V3 h = sample_visible_normal_smith(inTS, p.roughness, u0, u1, rnd);
+		float cavityPdf = eval_ggx(p.roughness, h);
+		cavityPdf *= h.z;
+		const float iDotH = dot(inTS, h);
+		const V3 exTS = (2.0f * iDotH) * h - inTS;
+		const float ge = geo_smith(iDotH, exTS, p.roughness);
+		const float gi = geo_smith(iDotH, inTS, p.roughness);
+		const float g = gi * ge;
+		if(ge == 0.0f || gi == 0.0f) return none;
+		res = { p.albedo * sdiv(g, gi), true, exTS,
+		        cavityPdf * sdiv(gi, std::fabs(4.0f * inTS.z * h.z)),
+		        cavityPdf * sdiv(ge, std::fabs(4.0f * exTS.z * h.z)) };
+	} else {
+		return none;
+	}
+	if(!nonzero(res.throughput)) return none;
+	V3 g = (res.excident.x * ts.shadingTX + res.excident.y * ts.shadingTY) + res.excident.z * ts.shadingN;
+	g = normalize(g);
+	const float eDotG = dot(g, ts.geoN);
+	const float eDotN = res.excident.z;
+	if(eDotG * eDotN <= 0.0f) return none;
+	res.excident = g;
+	res.pdfF = fmin_(res.pdfF, 1e9f);
+	res.pdfB = fmin_(res.pdfB, 1e9f);
+	return res;
+}
+
+// material_sampling.hpp:156-237 (adjoint = false, no merge normal)
+EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident, V3 excident) {
+	EvalValue none = { { 0, 0, 0 }, 0, 0, 0 };
+	const float iDotN = -dot(incident, ts.shadingN);
+	const float eDotN = dot(excident, ts.shadingN);
+	if(p.type == OR_MAT_EMISSIVE) {
+		// Emissive materials are neither reflective nor refractive
+		if(iDotN * eDotN > 0.0f) return none;
+		if(iDotN * eDotN < 0.0f) return none;
+	} else {
+		if(iDotN * eDotN < 0.0f) return none; // not refractive
+	}
+	const float iDotG = -dot(incident, ts.geoN);
+	const float eDotG = dot(excident, ts.geoN);
+	if(eDotG * eDotN <= 0.0f || iDotG * iDotN <= 0.0f) return none;
+	const V3 inTS = { -dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN };
+	const V3 exTS = { dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN };
+	V3 value; float pf, pb;
+	if(p.type == OR_MAT_LAMBERT) {
+		if(inTS.z * exTS.z < 0.0f) return none;
+		value = p.albedo / PI;
+		pf = std::fabs(exTS.z) / PI;
+		pb = std::fabs(inTS.z) / PI;
+	} else if(p.type == OR_MAT_TORRANCE) {
+		const V3 h = half_vector(inTS, exTS);
+		if(inTS.z * exTS.z < 0.0f) return none;
+		const float iDotH = dot(inTS, h);
+		const float ge = geo_smith(iDotH, exTS, p.roughness);
+		const float gi = geo_smith(iDotH, inTS, p.roughness);
+		const float g = gi * ge;
+		if(ge == 0.0f || gi == 0.0f) return none;
+		const float dd = eval_ggx(p.roughness, h);
+		value = p.albedo * sdiv(g * dd, std::fabs(4.0f * inTS.z * exTS.z));
+		pf = sdiv(gi * dd, std::fabs(4.0f * inTS.z));
+		pb = sdiv(ge * dd, std::fabs(4.0f * exTS.z));
+	} else {
+		return none;
+	}
+	if(!nonzero(value)) return none;
+	return { value, std::fabs(eDotN), fmin_(pf, 1e9f), fmin_(pb, 1e9f) };
+}
+
+// ---------------------------------------------------------------- lights
+inline V3 quad_light_center(const PosLight& l) {
+	return (l.posV[0] + (l.posV[1] + l.posV[2]) * 0.5f) + l.posV[3] * 0.25f;
+}
+inline V3 light_center(const PosLight& l) {
+	if(l.type == LT_QUAD) return quad_light_center(l);
+	return l.position;
+}
+inline float light_flux(const Scene& S, const PosLight& l) {
+	if(l.type == LT_POINT) {
+		const V3 f = l.intensity * 4.0f * PI;
+		return (f.x + f.y) + f.z;
+	}
+	// lights.cpp:43-62: for constant emission textures every one of the 128
+	// samples adds the same value; the per-sample area is the local
+	// parallelogram area at a low-discrepancy sample point.
+	const Material& m = S.materials[l.material];
+	const V3 rad = m.radiance * m.scale;
+	// GoldenRatio2D seeded from the light's address in the reference; here
+	// seeded from its index in the light list (deterministic).
+	u64 state = scramble_seed(u32(l.primId) * 2654435761u + u32(l.primInst));
+	V3 sum = { 0, 0, 0 };
+	for(int i = 0; i < 128; ++i) {
+		u64 s = state;
+		state += 11400714819323198485ull;
+		s = s ^ (s >> 1);
+		s = ((s >> 1) & 0x2222222222222222ull) | ((s << 1) & 0x4444444444444444ull) | (s & 0x9999999999999999ull);
+		s = ((s >> 2) & 0x0c0c0c0c0c0c0c0cull) | ((s << 2) & 0x3030303030303030ull) | (s & 0xc3c3c3c3c3c3c3c3ull);
+		s = ((s >> 4) & 0x00f000f000f000f0ull) | ((s << 4) & 0x0f000f000f000f00ull) | (s & 0xf00ff00ff00ff00full);
+		s = ((s >> 8) & 0x0000ff000000ff00ull) | ((s << 8) & 0x00ff000000ff0000ull) | (s & 0xff0000ffff0000ffull);
+		s = ((s >> 16) & 0x00000000ffff0000ull) | ((s << 16) & 0x0000ffff00000000ull) | (s & 0xffff00000000ffffull);
+		const float ux = sample_uniform(u32(s & 0xffffffffull));
+		const float uy = sample_uniform(u32(s >> 32ull));
+		const V3 tx = l.posV[1] + ux * l.posV[3];
+		const V3 ty = l.posV[2] + uy * l.posV[3];
+		const float area = len(cross(ty, tx));
+		sum = sum + area * rad;
+	}
+	sum = sum / 128.0f;
+	const V3 f = sum * 2.0f * PI;
+	return (f.x + f.y) + f.z;
+}
+
+// light_tree.cpp:120-330 (positional sub-tree) and fill_map
+void build_pos_tree(const Scene& S, LightTree& T) {
+	auto& lights = T.lights;
+	const size_t n = lights.size();
+	T.nodes.clear();
+	T.primToNodePath.clear();
+	if(n == 0) { T.rootFlux = 0.0f; T.rootType = INTERNAL_NODE; return; }
+	std::vector<float> flux(n);
+	for(size_t i = 0; i < n; ++i) flux[i] = light_flux(S, lights[i]);
+	if(n == 1) {
+		T.rootType = lights[0].type;
+		T.rootIndex = 0;
+		T.rootFlux = flux[0];
+		if(lights[0].primInst != -1) T.primToNodePath[{ lights[0].primInst, lights[0].primId }] = 0u;
+		return;
+	}
+	size_t height = 0;
+	while((size_t(1) << (height + 1)) <= n) ++height;
+	const size_t extra = n - (size_t(1) << height);
+	const size_t internalCount = ((size_t(1) << height) - 1) + extra;
+	T.nodes.assign(internalCount, LightNode{});
+	auto lightRef = [&](size_t i) { return LightNodeRef{ flux[i], i32(i), lights[i].type }; };
+	auto nodeRef = [&](size_t i) {
+		const LightNode& nd = T.nodes[i];
+		return LightNodeRef{ nd.left.flux + nd.right.flux, i32(i), INTERNAL_NODE };
+	};
+	auto refCenter = [&](const LightNodeRef& r) {
+		if(r.type == INTERNAL_NODE) return T.nodes[r.index].center;
+		return light_center(lights[r.index]);
+	};
+	auto makeNode = [&](size_t at, LightNodeRef l, LightNodeRef r) {
+		LightNode nd;
+		nd.left = l;
+		nd.right = r;
+		nd.center = (refCenter(l) + refCenter(r)) / 2.0f;
+		T.nodes[at] = nd;
+	};
+	if(extra > 0) {
+		const size_t startNode = (size_t(1) << height) - 1;
+		const size_t startLight = n - 2 * extra;
+		for(size_t i = 0; i < extra; ++i) makeNode(startNode + i, lightRef(startLight + 2 * i), lightRef(startLight + 2 * i + 1));
+		const size_t startInner = (size_t(1) << (height - 1)) - 1;
+		for(size_t i = 0; i < extra / 2; ++i) makeNode(startInner + i, nodeRef(startNode + 2 * i), nodeRef(startNode + 2 * i + 1));
+		if(extra % 2 != 0) makeNode(startInner + extra / 2, nodeRef(startNode + extra - 1), lightRef(0));
+	}
+	const size_t startLight = (extra % 2 == 0) ? 0 : 1;
+	const size_t levelNodeCount = n - 2 * extra - startLight;
+	const size_t nodeCount = levelNodeCount / 2;
+	const size_t startNodeIndex = (size_t(1) << height) - nodeCount - 1;
+	for(size_t i = 0; i < nodeCount; ++i) makeNode(startNodeIndex + i, lightRef(startLight + 2 * i), lightRef(startLight + 2 * i + 1));
+	if(height > 1) {
+		for(size_t level = height - 1; level >= 1; --level) {
+			const size_t nodes = size_t(1) << level;
+			const size_t inner = nodes / 2 - 1;
+			for(size_t i = 0; i < nodes / 2; ++i) makeNode(inner + i, nodeRef(nodes - 1 + 2 * i), nodeRef(nodes - 1 + 2 * i + 1));
+		}
+	}
+	T.rootType = INTERNAL_NODE;
+	T.rootIndex = 0;
+	T.rootFlux = T.nodes[0].left.flux + T.nodes[0].right.flux;
+	// fill_map
+	int h = int(height);
+	const u32 lowerLightCount = u32(1u << h) - u32(extra);
+	u32 i = 0;
+	if(extra > 0) {
+		for(; i < lowerLightCount; ++i) {
+			if(lights[i].primInst != -1) {
+				u32 code = ((1u << h) - 1) - (lowerLightCount - i - 1);
+				code <<= (32 - h);
+				T.primToNodePath[{ lights[i].primInst, lights[i].primId }] = code;
+			}
+		}
+		h += 1;
+	}
+	for(; i < n; ++i) {
+		if(lights[i].primInst != -1) {
+			const u32 code = (i - lowerLightCount) << (32 - h);
+			T.primToNodePath[{ lights[i].primInst, lights[i].primId }] = code;
+		}
+	}
+}
+
+struct Nee {
+	V3 position;
+	float creationPdf;
+	V3 dir;
+	float dirPdf;
+	float cosOut;
+	V3 diffIrradiance;
+	float dist;
+	V3 geoNormal;
+	float distSq;
+	bool valid;
+};
+
+// light_sampling.hpp:143-171 + 369-390
+Nee connect_quad(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
+	const V3 tx = l.posV[1] + u0 * l.posV[3];
+	const V3 ty = l.posV[2] + u1 * l.posV[3];
+	V3 normal = cross(ty, tx);
+	const float area = len(normal);
+	normal = normal / area;
+	const V3 position = (l.posV[0] + tx * u1) + l.posV[2] * u0;
+	const V2 uv = ((l.uvV[0] + l.uvV[1] * u1) + l.uvV[2] * u0) + l.uvV[3] * (u0 * u1);
+	(void)uv;
+	const Material& m = S.materials[l.material];
+	const V3 radiance = m.type == OR_MAT_EMISSIVE ? m.radiance * m.scale : V3{ 0, 0, 0 };
+	const V3 intensity = radiance * area;
+	const float pdf = 1.0f / area;
+	V3 direction = position - pos;
+	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
+	const float dist = mbmath::sqrt(distSq);
+	direction = direction / dist;
+	// evaluate_area(-direction, intensity, normal)
+	const float cosOut = dot(normal, -direction);
+	V3 value = { 0, 0, 0 }; float vcos = 0.0f, vpdf = 0.0f;
+	if(cosOut > 0.0f) { value = intensity; vcos = cosOut; vpdf = cosOut / PI; }
+	const V3 diff = value / distSq;
+	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true };
+}
+
+// light_sampling.hpp:308-325
+Nee connect_point(const PosLight& l, V3 pos) {
+	V3 direction = l.position - pos;
+	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
+	const float dist = mbmath::sqrt(distSq);
+	direction = direction / dist;
+	const V3 diff = l.intensity / distSq;
+	return { l.position, INF_PDF, direction, 1.0f / (4.0f * PI), 0.0f, diff, dist, { 0, 0, 0 }, distSq, true };
+}
+
+// light_sampling.hpp:447-462
+Nee connect_background(const LightTree& T, V3 pos, Box bounds, float u0, float u1) {
+	const V3 dir = sample_dir_sphere_uniform(u0, u1);
+	const float dirPdf = 1.0f / (4.0f * PI);
+	const V3 radiance = T.bgColor * T.bgScale;
+	const float posPdf = 1.0f / projected_area(dir, bounds);
+	const V3 diff = radiance / dirPdf;
+	const float creation = dirPdf * std::fabs(1.0f) / (MAX_SCENE_SIZE * MAX_SCENE_SIZE);
+	return { pos + dir * len(bounds.mx - bounds.mn), creation, dir, posPdf, 1.0f, diff,
+	         MAX_SCENE_SIZE, { 0, 0, 0 }, MAX_SCENE_SIZE * MAX_SCENE_SIZE, true };
+}
+
+inline Nee adjust(Nee n, float chance) {
+	n.creationPdf *= chance;
+	n.diffIrradiance = n.diffIrradiance / chance;
+	return n;
+}
+
+Nee connect_pos_light(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
+	if(l.type == LT_QUAD) return connect_quad(S, l, pos, u0, u1);
+	return connect_point(l, pos);
+}
+
+// light_tree_sampling.hpp:278-329 and 195-259
+Nee lights_connect(const Scene& S, u64 index, u64 numIndices, u64 seed, V3 position, float u0, float u1) {
+	const LightTree& T = S.lightTree;
+	u64 rndChoice = numIndices > 0 ? seed + index * (~0ull / numIndices) : seed;
+	if(rndChoice == ~0ull) --rndChoice;
+	const float bgSum = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+	const float fluxSum = (bgSum + T.dirFlux) + T.rootFlux;
+	Nee none{};
+	none.valid = false;
+	if(!(fluxSum > 0.0f)) return none;
+	const float envProb = bgSum / fluxSum;
+	const float dirProb = T.dirFlux / fluxSum;
+	const float posProb = T.rootFlux / fluxSum;
+	const u64 rightEnv = percentage_of(~0ull, envProb);
+	if(rndChoice < rightEnv) return adjust(connect_background(T, position, S.aabb, u0, u1), envProb);
+	u64 right = percentage_of(~0ull, envProb + dirProb);
+	u64 left = rightEnv;
+	float p = dirProb;
+	if(rndChoice < right) {
+		return none; // no directional lights are supported
+	}
+	left = right;
+	right = ~0ull;
+	p = posProb;
+	// traverse the positional tree
+	u16 type = T.rootType;
+	i32 index2 = T.rootIndex;
+	u64 iL = left, iR = right;
+	float lightProb = p;
+	i32 nodeIdx = 0;
+	while(type == INTERNAL_NODE) {
+		const LightNode& nd = T.nodes[nodeIdx];
+		const float probLeft = nd.left.flux / (nd.left.flux + nd.right.flux);
+		const u64 boundary = iL + percentage_of(iR - iL, probLeft);
+		if(rndChoice < boundary) {
+			type = nd.left.type; index2 = nd.left.index; iR = boundary; lightProb *= probLeft;
+		} else {
+			type = nd.right.type; index2 = nd.right.index; iL = boundary; lightProb *= (1.0f - probLeft);
+		}
+		nodeIdx = index2;
+	}
+	return adjust(connect_pos_light(S, T.lights[index2], position, u0, u1), lightProb);
+}
+
+// light_tree_sampling.hpp:340-412 (quad area lights)
+float light_connect_pdf(const Scene& S, i32 inst, i32 prim, V2 sp) {
+	const LightTree& T = S.lightTree;
+	const float bgSum = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+	float p = T.rootFlux / ((T.dirFlux + T.rootFlux) + bgSum);
+	auto it = T.primToNodePath.find({ inst, prim });
+	if(it == T.primToNodePath.end()) return 0.0f;
+	u32 code = it->second;
+	u16 type = T.rootType;
+	i32 idx = T.rootIndex;
+	i32 nodeIdx = 0;
+	while(type == INTERNAL_NODE) {
+		const LightNode& nd = T.nodes[nodeIdx];
+		const float pLeft = nd.left.flux / (nd.left.flux + nd.right.flux);
+		if(code & 0x80000000u) { p *= (1.0f - pLeft); type = nd.right.type; idx = nd.right.index; }
+		else { p *= pLeft; type = nd.left.type; idx = nd.left.index; }
+		nodeIdx = idx;
+		code <<= 1;
+	}
+	const PosLight& l = T.lights[idx];
+	if(l.type == LT_QUAD) {
+		const V3 tx = l.posV[1] + sp.x * l.posV[3];
+		const V3 ty = l.posV[2] + sp.y * l.posV[3];
+		return p / len(cross(ty, tx));
+	}
+	return 0.0f;
+}
+
+// ---------------------------------------------------------------- path tracer
+enum VType { V_CAMERA, V_SURFACE, V_VOID };
+
+struct Vertex {
+	VType type;
+	V3 position;
+	V3 incidentEncoded;
+	i32 pathLen;
+	float incidentPdf;
+	TangentSpace ts;
+	i32 inst, prim;
+	V2 surfaceParams;
+	Params mat;
+};
+
+// render_target.hpp:64-75: a NaN channel of a contribution is replaced by 0
+inline float nan_to_zero(float x) { return std::isnan(x) ? 0.0f : x; }
+inline V3 contribute(V3 acc, V3 c) { return { acc.x + nan_to_zero(c.x), acc.y + nan_to_zero(c.y), acc.z + nan_to_zero(c.z) }; }
+
+inline V3 incident_direction(const Vertex& v) {
+	const V3 e = v.incidentEncoded;
+	float t = 1.0f - e.x * e.x - e.y * e.y;
+	t = std::fmin(std::fmax(t, 0.0f), 1.0f);
+	return { e.x, e.y, sgn(e.z) * mbmath::sqrt(t) };
+}
+
+struct PtState {
+	const Scene* scene;
+	OrPtParams params;
+	std::vector<Pcg64> rngs;
+	std::vector<float> radiance, hitId;   // cumulative
+	i32 iteration = -1;
+	Counters stats;
+};
+
+// pinhole.hpp:58-81
+inline V3 pinhole_ray(const Camera& c, i32 px, i32 py, float u0, float u1, float& pdf) {
+	const V2 sub = { float(px) + u0, float(py) + u1 };
+	V2 cp = { sub.x / float(c.resX), sub.y / float(c.resY) };
+	cp = { cp.x * 2.0f - 1.0f, cp.y * 2.0f - 1.0f };
+	cp = { cp.x * c.tanVFov, cp.y * c.tanVFov };
+	const float aspect = float(c.resX) / float(c.resY);
+	const V3 nPos = { cp.x * aspect, cp.y, 1.0f };
+	const V3 xAxis = cross(c.viewDir, c.up);
+	const V3 dir = normalize((xAxis * nPos.x + c.up * nPos.y) + c.viewDir * nPos.z);
+	const float t2 = 2.0f * c.tanVFov;
+	const float pixelArea = (t2 * t2) * aspect;
+	const float cosOut = dot(c.viewDir, dir);
+	pdf = 1.0f / (((pixelArea * cosOut) * cosOut) * cosOut);
+	return dir;
+}
+
+// pt_common.hpp:75-156
+void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hitOut, Counters& cnt) {
+	const Scene& S = *st.scene;
+	const OrPtParams& P = st.params;
+	V3 throughput = { 1, 1, 1 };
+	V3 radiance = { 0, 0, 0 };
+	V2 hitAcc = { 0, 0 };
+	Vertex v{};
+	v.type = V_CAMERA;
+	v.position = S.cam.position;
+	v.incidentEncoded = { float(px), float(py), 0.0f };
+	v.pathLen = 0;
+	v.incidentPdf = 1.0f;
+	v.inst = v.prim = -1;
+	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
+	int pathLen = 0;
+	do {
+		if(pathLen > 0 && pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
+			const u64 neeSeed = rng.next();
+			for(int i = 0; i < P.neeCount; ++i) {
+				const u64 r = rng.next();
+				const float nu0 = sample_uniform(u32(r)), nu1 = sample_uniform(u32(r >> 32));
+				Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, v.position, nu0, nu1);
+				if(!nee.valid) continue;
+				EvalValue val = material_evaluate(v.ts, v.mat, incident_direction(v), nee.dir);
+				if(nee.cosOut != 0.0f) val.cosOut *= nee.cosOut;
+				const V3 rad = val.value * nee.diffIrradiance;
+				if(any_pos(rad) && val.cosOut > 0.0f) {
+					const bool occ = any_intersection(S, v.position, nee.position, v.ts.geoN, nee.geoNormal, nee.dir, cnt);
+					if(!occ) {
+						const float hitPdf = val.pdfF * std::fabs(nee.cosOut) / nee.distSq;
+						const float mis = 1.0f / (float(P.neeCount) + hitPdf / nee.creationPdf);
+						radiance = contribute(radiance, ((throughput * val.cosOut) * rad) * mis);
+					}
+				}
+			}
+		}
+		// walk (random_walk.hpp:38-113)
+		const V3 lastPosition = (v.type == V_VOID) ? V3{ 0, 0, 0 } : v.position;
+		const u64 x0 = rng.next(), x1 = rng.next();
+		const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
+		const float rr = sample_uniform(u32(rng.next()));
+		V3 origin, excident;
+		V3 sThroughput;
+		float pdfF;
+		if(v.type == V_CAMERA) {
+			excident = pinhole_ray(S.cam, px, py, ru0, ru1, pdfF);
+			sThroughput = { 1, 1, 1 };
+			origin = v.position;
+		} else {
+			PathSample s = material_sample(v.ts, v.mat, incident_direction(v), ru0, ru1, x1);
+			if(!s.valid) break;
+			excident = s.excident;
+			sThroughput = s.throughput;
+			pdfF = s.pdfF;
+			origin = v.position;
+		}
+		throughput = throughput * sThroughput;
+		if(pathLen >= P.rrStartDepth) {
+			const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
+			if(rr >= cp) break;
+			throughput = throughput / cp;
+		}
+		const V3 geoN = (v.type == V_SURFACE) ? v.ts.geoN : V3{ 0, 0, 0 };
+		Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt);
+		if(hit.inst < 0) {
+			v.type = V_VOID;
+			v.incidentEncoded = excident;
+			v.position = { 0, 0, 0 };
+			v.incidentPdf = pdfF * 1.0f;
+		} else {
+			const V3 position = origin + excident * hit.distance;
+			const TangentSpace ts = tangent_space(S, hit);
+			v.type = V_SURFACE;
+			v.position = position;
+			v.incidentEncoded = { excident.x, excident.y, hit.distance * sgn(excident.z) };
+			v.ts = ts;
+			v.inst = hit.inst;
+			v.prim = hit.prim;
+			v.surfaceParams = hit.sp;
+			v.mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+			const float inCosAbs = std::fabs(dot(excident, ts.shadingN));
+			v.incidentPdf = pdfF * std::fabs(inCosAbs) / (hit.distance * hit.distance);
+		}
+		if(pathLen == 0) hitAcc = { float(v.type == V_SURFACE ? v.inst : -1), float(v.type == V_SURFACE ? v.prim : -1) };
+		++pathLen;
+		if(pathLen >= P.minPathLength) {
+			V3 emission = { 0, 0, 0 };
+			float connectPdf = 0.0f;
+			if(v.type == V_VOID) {
+				if(S.lightTree.hasBackground) {
+					emission = S.lightTree.bgColor * S.lightTree.bgScale;
+					if(nonzero(emission)) {
+						const LightTree& T = S.lightTree;
+						const float bgFlux = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+						const float p = bgFlux / ((T.dirFlux + T.rootFlux) + bgFlux);
+						connectPdf = (1.0f / (4.0f * PI)) * p;
+					}
+				}
+			} else if(v.mat.type == OR_MAT_EMISSIVE) {
+				const V3 ex = -incident_direction(v);
+				const float cosOut = dot(v.ts.geoN, ex);
+				if(cosOut > 0.0f) {
+					emission = v.mat.radiance;
+					if(nonzero(emission)) connectPdf = light_connect_pdf(S, v.inst, v.prim, v.surfaceParams);
+				}
+			}
+			if(nonzero(emission) && pathLen > 1) {
+				const float misWeight = 1.0f / (1.0f + float(P.neeCount) * (connectPdf / v.incidentPdf));
+				emission = emission * misWeight;
+			}
+			radiance = contribute(radiance, throughput * emission);
+		}
+		if(v.type != V_SURFACE) break;
+	} while(pathLen < P.maxPathLength);
+	radianceOut = radiance;
+	hitOut = hitAcc;
+}
+
+void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
+	const Scene& S = *st.scene;
+	const i32 W = i32(S.width), H = i32(S.height);
+	if(accumulate) ++st.iteration;
+	const float it = float(st.iteration);
+	const i32 p0 = i32(y0) * W, p1 = i32(y1) * W;
+	(void)H;
+	Counters total;
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(static, 1000)
+		for(i32 pixel = p0; pixel < p1; ++pixel) {
+			V3 rad; V2 hid;
+			pt_sample(st, pixel % W, pixel / W, st.rngs[pixel], rad, hid, local);
+			if(accumulate) {
+				// output_handler_variance.hpp:7-31 (mean only)
+				const float iter[5] = { rad.x, rad.y, rad.z, hid.x, hid.y };
+				float* cr = &st.radiance[size_t(pixel) * 3];
+				float* ch = &st.hitId[size_t(pixel) * 2];
+				const float den = std::fmax(1.0f, it + 1.0f);
+				for(int c = 0; c < 3; ++c) { const float diff = iter[c] - cr[c]; cr[c] += diff / den; }
+				for(int c = 0; c < 2; ++c) { const float diff = iter[3 + c] - ch[c]; ch[c] += diff / den; }
+			}
+		}
+#pragma omp critical
+		total.add(local);
+	}
+	st.stats.add(total);
+}
+
+// ---------------------------------------------------------------- scene setup
+Scene* create_scene(const OrSceneDesc* d) {
+	auto S = std::make_unique<Scene>();
+	S->width = d->width; S->height = d->height;
+	for(u32 i = 0; i < d->numMaterials; ++i) {
+		const OrMaterial& m = d->materials[i];
+		Material mm;
+		mm.type = m.type;
+		mm.albedo = { m.albedo[0], m.albedo[1], m.albedo[2] };
+		mm.roughness = { m.roughness[0], m.roughness[1] };
+		mm.shadowing = m.shadowing; mm.ndf = m.ndf;
+		mm.radiance = { m.radiance[0], m.radiance[1], m.radiance[2] };
+		mm.scale = { m.scale[0], m.scale[1], m.scale[2] };
+		mm.albedoTex = m.albedoTexture;
+		S->materials.push_back(mm);
+	}
+	for(u32 i = 0; i < d->numTextures; ++i) {
+		Texture t;
+		t.w = d->textures[i].width; t.h = d->textures[i].height;
+		t.texels.assign(d->textures[i].texels, d->textures[i].texels + size_t(t.w) * t.h * 4);
+		S->textures.push_back(std::move(t));
+	}
+	S->lods.resize(d->numLods);
+	for(u32 i = 0; i < d->numLods; ++i) {
+		const OrLod& s = d->lods[i];
+		Lod& l = S->lods[i];
+		l.nV = s.numVertices; l.nT = s.numTriangles; l.nQ = s.numQuads; l.nS = s.numSpheres;
+		l.verts.resize(l.nV); l.normals.resize(l.nV); l.uvs.resize(l.nV);
+		for(u32 v = 0; v < l.nV; ++v) {
+			l.verts[v] = { s.vertices[3 * v], s.vertices[3 * v + 1], s.vertices[3 * v + 2] };
+			l.normals[v] = s.normals ? V3{ s.normals[3 * v], s.normals[3 * v + 1], s.normals[3 * v + 2] } : V3{ 0, 0, 0 };
+			l.uvs[v] = s.uvs ? V2{ s.uvs[2 * v], s.uvs[2 * v + 1] } : V2{ 0, 0 };
+		}
+		l.idx.assign(s.indices, s.indices + (size_t(l.nT) * 3 + size_t(l.nQ) * 4));
+		l.faceMat.assign(s.faceMaterials, s.faceMaterials + (l.nT + l.nQ));
+		l.spheres.assign(s.spheres, s.spheres + size_t(l.nS) * 4);
+		l.sphereMat.assign(s.sphereMaterials, s.sphereMaterials + l.nS);
+		l.numPrims = i32(l.nT + l.nQ + l.nS);
+		Box b = empty_box();
+		for(u32 v = 0; v < l.nV; ++v) { b.mn = vmin(b.mn, l.verts[v]); b.mx = vmax(b.mx, l.verts[v]); }
+		for(u32 k = 0; k < l.nS; ++k) {
+			const V3 c = sphere_center(l, k); const float r = sphere_radius(l, k);
+			b.mn = vmin(b.mn, c - V3{ r, r, r }); b.mx = vmax(b.mx, c + V3{ r, r, r });
+		}
+		l.aabb = b;
+	}
+	// LoD BVHs (lod.cpp:16-38)
+	S->lodBvh.resize(d->numLods);
+	for(u32 i = 0; i < d->numLods; ++i) {
+		BuildDesc bd;
+		bd.isScene = false; bd.scene = S.get(); bd.lod = &S->lods[i];
+		bd.numPrims = S->lods[i].numPrims; bd.bb = S->lods[i].aabb;
+		build_lbvh(bd, bd.numPrims, bd.numPrims, S->lodBvh[i]);
+	}
+	// Instances (scene.cpp:111-419)
+	S->w2i.resize(d->numInstances);
+	S->instLod.assign(d->instanceLod, d->instanceLod + d->numInstances);
+	std::vector<Box> instBoxes(d->numInstances, empty_box());
+	std::vector<V3> instCentroids(d->numInstances, V3{ 0, 0, 0 });
+	S->activeInstances = 0;
+	S->validInstance = 0xFFFFFFFFu;
+	Box sceneBox = empty_box();
+	for(u32 i = 0; i < d->numInstances; ++i) {
+		std::memcpy(S->w2i[i].m, d->worldToInstance + 12 * i, sizeof(float) * 12);
+		if(S->instLod[i] == 0xFFFFFFFFu) continue;
+		++S->activeInstances;
+		if(S->validInstance == 0xFFFFFFFFu) S->validInstance = i;
+		const Mat34 i2w = instance_to_world(S->w2i[i]);
+		const Box lb = S->lods[S->instLod[i]].aabb;
+		instBoxes[i] = xform_box(i2w, lb);
+		instCentroids[i] = xform_point(i2w, center(lb));
+		sceneBox = merge(sceneBox, instBoxes[i]);
+	}
+	S->aabb = sceneBox;
+	{
+		BuildDesc bd;
+		bd.isScene = true; bd.scene = S.get(); bd.lod = nullptr;
+		bd.numPrims = i32(d->numInstances); bd.bb = sceneBox;
+		bd.instBoxes = instBoxes; bd.instCentroids = instCentroids;
+		build_lbvh(bd, i32(d->numInstances), S->activeInstances, S->tlas);
+	}
+	// Camera (camera.hpp:81-96, pinhole.hpp:22)
+	{
+		V3 dir = { d->camDir[0], d->camDir[1], d->camDir[2] };
+		V3 up = { d->camUp[0], d->camUp[1], d->camUp[2] };
+		dir = normalize(dir);
+		up = normalize(up);
+		const float zDotY = dot(dir, up);
+		up = normalize(up - zDotY * dir);
+		S->cam.position = { d->camPos[0], d->camPos[1], d->camPos[2] };
+		S->cam.viewDir = dir;
+		S->cam.up = up;
+		S->cam.tanVFov = std::tan(d->vFov / 2.0f);
+		S->cam.nearP = d->nearPlane; S->cam.farP = d->farPlane;
+		S->cam.resX = u16(d->width); S->cam.resY = u16(d->height);
+	}
+	// Lights (world_container.cpp:869-990, light_tree.cpp:340-447)
+	LightTree& T = S->lightTree;
+	for(u32 inst = 0; inst < d->numInstances; ++inst) {
+		if(S->instLod[inst] == 0xFFFFFFFFu) continue;
+		const Lod& l = S->lods[S->instLod[inst]];
+		const Mat34 i2w = instance_to_world(S->w2i[inst]);
+		const float* m = i2w.m;
+		const float det3 = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[1] * (m[4] * m[10] - m[8] * m[6]) + m[2] * (m[4] * m[9] - m[8] * m[5]);
+		const bool mirroring = det3 < 0.0f;
+		for(u32 q = 0; q < l.nQ; ++q) {
+			const u16 mi = l.faceMat[l.nT + q];
+			if(S->materials[mi].type != OR_MAT_EMISSIVE) continue;
+			V3 pts[4]; V2 uvs[4];
+			const u32 o = l.nT * 3 + q * 4;
+			for(int k = 0; k < 4; ++k) { pts[k] = xform_point(i2w, l.verts[l.idx[o + k]]); uvs[k] = l.uvs[l.idx[o + k]]; }
+			if(mirroring) { std::swap(pts[1], pts[3]); std::swap(uvs[1], uvs[3]); }
+			PosLight pl{};
+			pl.type = LT_QUAD;
+			pl.posV[0] = pts[0];
+			pl.posV[1] = pts[3] - pts[0];
+			pl.posV[2] = pts[1] - pts[0];
+			pl.posV[3] = (pts[2] - pts[3]) - pl.posV[2];
+			pl.uvV[0] = uvs[0];
+			pl.uvV[1] = uvs[3] - uvs[0];
+			pl.uvV[2] = uvs[1] - uvs[0];
+			pl.uvV[3] = (uvs[2] - uvs[3]) - pl.uvV[2];
+			pl.material = mi;
+			pl.primInst = i32(inst);
+			pl.primId = i32(l.nT + q);
+			T.lights.push_back(pl);
+		}
+	}
+	for(u32 i = 0; i < d->numPointLights; ++i) {
+		PosLight pl{};
+		pl.type = LT_POINT;
+		pl.position = { d->pointLights[6 * i], d->pointLights[6 * i + 1], d->pointLights[6 * i + 2] };
+		pl.intensity = { d->pointLights[6 * i + 3], d->pointLights[6 * i + 4], d->pointLights[6 * i + 5] };
+		T.lights.push_back(pl);
+	}
+	if(T.lights.size() > 1) {
+		const V3 scale = sceneBox.mx - sceneBox.mn;
+		auto conv = [](float v) { return v <= 0.0f ? 0u : (v >= 4294967040.0f ? 0xFFFFFF00u : u32(v)); };
+		auto p16 = [](u32 x) {
+			u64 r = x & 0xFFFF;
+			r = (r | (r << 16)) & 0x0000ff0000ffull;
+			r = (r | (r << 8)) & 0x00f00f00f00full;
+			r = (r | (r << 4)) & 0x0c30c30c30c3ull;
+			r = (r | (r << 2)) & 0x249249249249ull;
+			return r;
+		};
+		auto hilbert = [&](u32 a, u32 b, u32 c) {
+			u64 num = p16(a) | (p16(b) << 1u) | (p16(c) << 2u);
+			num = num ^ (num >> 32); num = num ^ (num >> 16); num = num ^ (num >> 8);
+			num = num ^ (num >> 4); num = num ^ (num >> 2); num = num ^ (num >> 1);
+			return num;
+		};
+		std::stable_sort(T.lights.begin(), T.lights.end(), [&](const PosLight& a, const PosLight& b) {
+			const V3 ca = light_center(a) * scale, cb = light_center(b) * scale;
+			const u32 ax = conv(ca.x), ay = conv(ca.y), az = conv(ca.z);
+			const u32 bx = conv(cb.x), by = conv(cb.y), bz = conv(cb.z);
+			u64 A = hilbert(ax >> 16, ay >> 16, az >> 16), B = hilbert(bx >> 16, by >> 16, bz >> 16);
+			if(A == B) { A = hilbert(ax & 0xffff, ay & 0xffff, az & 0xffff); B = hilbert(bx & 0xffff, by & 0xffff, bz & 0xffff); }
+			return A < B;
+		});
+	}
+	build_pos_tree(*S, T);
+	T.hasBackground = d->hasBackground != 0;
+	if(T.hasBackground) {
+		T.bgColor = { d->backgroundColor[0], d->backgroundColor[1], d->backgroundColor[2] };
+		T.bgScale = { d->backgroundScale[0], d->backgroundScale[1], d->backgroundScale[2] };
+		// background.cpp:125-135
+		const V3 diag = sceneBox.mx - sceneBox.mn;
+		const float solidAngle = 4.0f * PI;
+		const float area = 2.0f * PI * ((diag.x * diag.y + diag.x * diag.z) + diag.y * diag.z);
+		const float f = solidAngle * area;
+		T.bgFlux = T.bgColor * f;
+	}
+	return S.release();
+}
+
+} // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+void* oracle_scene_create(const OrSceneDesc* desc) {
+	if(!desc) return nullptr;
+	return create_scene(desc);
+}
+
+void oracle_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+static const Bvh* pick_bvh(Scene* S, int32_t which) {
+	if(which < 0) return &S->tlas;
+	if(u32(which) >= S->lodBvh.size()) return nullptr;
+	return &S->lodBvh[which];
+}
+
+int oracle_bvh_info(void* s, int32_t which, int32_t* numPrims, int32_t* numInternal) {
+	const Bvh* b = pick_bvh(static_cast<Scene*>(s), which);
+	if(!b) return 0;
+	if(numPrims) *numPrims = b->numPrims;
+	if(numInternal) *numInternal = b->numInternal;
+	return 1;
+}
+
+int oracle_bvh_get(void* s, int32_t which, uint64_t* morton, int32_t* parents, float* nodes, int32_t* primIds) {
+	const Bvh* b = pick_bvh(static_cast<Scene*>(s), which);
+	if(!b) return 0;
+	if(morton && !b->mortonSorted.empty()) std::memcpy(morton, b->mortonSorted.data(), b->mortonSorted.size() * 8);
+	if(parents && !b->parents.empty()) std::memcpy(parents, b->parents.data(), b->parents.size() * 4);
+	if(nodes && !b->nodes.empty()) std::memcpy(nodes, b->nodes.data(), b->nodes.size() * sizeof(BvhNode));
+	if(primIds && !b->primIds.empty()) std::memcpy(primIds, b->primIds.data(), b->primIds.size() * 4);
+	return 1;
+}
+
+int oracle_scene_aabb(void* s, float* a) {
+	Scene* S = static_cast<Scene*>(s);
+	a[0] = S->aabb.mn.x; a[1] = S->aabb.mn.y; a[2] = S->aabb.mn.z;
+	a[3] = S->aabb.mx.x; a[4] = S->aabb.mx.y; a[5] = S->aabb.mx.z;
+	return 1;
+}
+
+int oracle_trace_first(void* s, const float* rays, const float* geoNormals, float tmax, uint32_t n,
+                       float* tOut, int32_t* instOut, int32_t* primOut, float* spOut) {
+	Scene* S = static_cast<Scene*>(s);
+#pragma omp parallel for schedule(static, 256)
+	for(int64_t i = 0; i < int64_t(n); ++i) {
+		Counters c;
+		V3 o = { rays[6 * i], rays[6 * i + 1], rays[6 * i + 2] };
+		const V3 d = { rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5] };
+		const V3 g = geoNormals ? V3{ geoNormals[3 * i], geoNormals[3 * i + 1], geoNormals[3 * i + 2] } : V3{ 0, 0, 0 };
+		const Intersection h = first_intersection(*S, o, d, g, tmax, c);
+		tOut[i] = h.distance; instOut[i] = h.inst; primOut[i] = h.prim;
+		if(spOut) { spOut[2 * i] = h.sp.x; spOut[2 * i + 1] = h.sp.y; }
+	}
+	return 1;
+}
+
+int oracle_trace_any(void* s, const float* a, const float* b, uint32_t n, uint8_t* occ) {
+	Scene* S = static_cast<Scene*>(s);
+#pragma omp parallel for schedule(static, 256)
+	for(int64_t i = 0; i < int64_t(n); ++i) {
+		Counters c;
+		const V3 pa = { a[3 * i], a[3 * i + 1], a[3 * i + 2] };
+		const V3 pb = { b[3 * i], b[3 * i + 1], b[3 * i + 2] };
+		const V3 dv = pb - pa;
+		const V3 dir = dv / len(dv);
+		occ[i] = any_intersection(*S, pa, pb, { 0, 0, 0 }, { 0, 0, 0 }, dir, c) ? 1 : 0;
+	}
+	return 1;
+}
+
+void* oracle_pt_create(void* s, const OrPtParams* params) {
+	Scene* S = static_cast<Scene*>(s);
+	auto* st = new PtState();
+	st->scene = S;
+	st->params = *params;
+	const i32 num = i32(S->width * S->height);
+	st->rngs.resize(num);
+	// cpu_pt.cpp:40-45
+	const i32 seed = i32(u32(params->seed) * u32(num + 1));
+	for(i32 i = 0; i < num; ++i) st->rngs[i] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
+	st->radiance.assign(size_t(num) * 3, 0.0f);
+	st->hitId.assign(size_t(num) * 2, 0.0f);
+	return st;
+}
+
+void oracle_pt_destroy(void* p) { delete static_cast<PtState*>(p); }
+
+int oracle_pt_iterate(void* p, int32_t nt) {
+	PtState* st = static_cast<PtState*>(p);
+	pt_iterate(*st, nt > 0 ? nt : 1, 0, st->scene->height, true);
+	return 1;
+}
+
+int oracle_pt_iterate_rows(void* p, int32_t nt, uint32_t y0, uint32_t y1) {
+	PtState* st = static_cast<PtState*>(p);
+	if(y1 > st->scene->height) y1 = st->scene->height;
+	if(y0 >= y1) return 0;
+	pt_iterate(*st, nt > 0 ? nt : 1, y0, y1, false);
+	return 1;
+}
+
+int oracle_pt_get_target(void* p, int32_t target, float* out) {
+	PtState* st = static_cast<PtState*>(p);
+	if(target == 0) std::memcpy(out, st->radiance.data(), st->radiance.size() * 4);
+	else if(target == 1) std::memcpy(out, st->hitId.data(), st->hitId.size() * 4);
+	else return 0;
+	return 1;
+}
+
+int oracle_pt_stats(void* p, OrStats* o) {
+	PtState* st = static_cast<PtState*>(p);
+	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
+	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
+	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
+	return 1;
+}
+
+int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents) {
+	if(n < 2) return 0;
+	std::vector<u64> k(keys, keys + n);
+	std::vector<i32> p(size_t(2 * n - 1), 0);
+	for(i32 i = 0; i < n - 1; ++i) karras_node(k, n, p, i);
+	std::memcpy(parents, p.data(), p.size() * 4);
+	return 1;
+}
+
+uint64_t oracle_pcg64_seed(uint32_t seed) { return Pcg64::seeded(seed).state; }
+uint64_t oracle_pcg64_next(uint64_t* state) { Pcg64 r; r.state = *state; u64 v = r.next(); *state = r.state; return v; }
+uint64_t oracle_part_by_two21(uint32_t x) { return part_by_two21(x); }
+void oracle_sincos(float x, float* s, float* c) { mbmath::sincos(x, *s, *c); }
+float oracle_atan2(float y, float x) { return mbmath::atan2(y, x); }
+float oracle_acos(float x) { return mbmath::acos(x); }
+
+} // extern "C"

@@ -1,0 +1,135 @@
+/*
+ * CPU oracle for the Mufflon path-tracer hot path: TEST INFRASTRUCTURE ONLY.
+ *
+ * This library is a CPU restatement of the reference renderer's CPU path
+ * (LBVH build, two-level traversal, pt_sample), written to check the CUDA
+ * implementation in mufflon_b200/ bit for bit. Only tests/, the smoke()
+ * entry point and bench.py's CPU-baseline leg load it. The product library
+ * never links, loads or calls it.
+ *
+ * Parity status: the reference cannot be built here (its math library
+ * "epsilon" and its cub dependency are missing), so there are no reference
+ * outputs to pin against. The restatement is checked against hand-derived
+ * known answers (Morton codes, PCG64 streams, Karras hierarchies, ray tests)
+ * in tests/test_oracle_*.py; beyond those, parity is unpinned.
+ */
+#ifndef MUFFLON_ORACLE_H
+#define MUFFLON_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+	uint32_t numVertices;
+	uint32_t numTriangles;
+	uint32_t numQuads;
+	uint32_t numSpheres;
+	const float* vertices;       /* 3 * numVertices */
+	const float* normals;        /* 3 * numVertices */
+	const float* uvs;            /* 2 * numVertices */
+	const uint32_t* indices;     /* 3 * numTriangles, then 4 * numQuads */
+	const uint16_t* faceMaterials; /* numTriangles + numQuads */
+	const float* spheres;        /* 4 * numSpheres: center xyz, radius */
+	const uint16_t* sphereMaterials; /* numSpheres */
+} OrLod;
+
+enum { OR_MAT_LAMBERT = 0, OR_MAT_TORRANCE = 1, OR_MAT_EMISSIVE = 2 };
+
+typedef struct {
+	int32_t type;
+	float albedo[3];
+	float roughness[2];
+	int32_t shadowing;    /* 0 v-cavity, 1 smith */
+	int32_t ndf;          /* 0 ggx (only GGX is supported) */
+	float radiance[3];
+	float scale[3];
+	int32_t albedoTexture; /* index into the texture table or -1 */
+} OrMaterial;
+
+typedef struct {
+	uint32_t width, height;
+	const float* texels; /* width*height*4, row-major, y = 0 first */
+} OrTexture;
+
+typedef struct {
+	uint32_t numLods;
+	const OrLod* lods;
+	uint32_t numInstances;
+	const float* worldToInstance; /* 12 floats per instance, row-major 3x4 */
+	const uint32_t* instanceLod;  /* UINT32_MAX marks a masked instance */
+	uint32_t numMaterials;
+	const OrMaterial* materials;
+	uint32_t numTextures;
+	const OrTexture* textures;
+	uint32_t numPointLights;
+	const float* pointLights;     /* 6 floats: position, intensity */
+	int32_t hasBackground;
+	float backgroundColor[3];
+	float backgroundScale[3];
+	float camPos[3], camDir[3], camUp[3];
+	float vFov, nearPlane, farPlane;
+	uint32_t width, height;
+} OrSceneDesc;
+
+typedef struct {
+	int32_t seed;
+	int32_t minPathLength;
+	int32_t maxPathLength;
+	int32_t neeCount;
+	int32_t neePositionGuide;
+	int32_t rrStartDepth;   /* extension: Russian roulette from this path length (0 = always, as the reference) */
+} OrPtParams;
+
+typedef struct {
+	uint64_t rays;          /* extension + shadow rays traced */
+	uint64_t shadowRays;
+	uint64_t nodeVisits;    /* binary BVH nodes (64 B each) fetched */
+	uint64_t instanceVisits;
+	uint64_t triTests, quadTests, sphereTests;
+} OrStats;
+
+void* oracle_scene_create(const OrSceneDesc* desc);
+void oracle_scene_destroy(void* scene);
+
+/* BVH inspection. which = -1 selects the instance-level BVH, otherwise a LoD.
+ * Returns the number of build primitives and internal nodes after collapse. */
+int oracle_bvh_info(void* scene, int32_t which, int32_t* numPrims, int32_t* numInternal);
+int oracle_bvh_get(void* scene, int32_t which, uint64_t* mortonSorted, int32_t* parents,
+                   float* nodes /* 8 words per node: min3 max3 index primCount (as int bits) */,
+                   int32_t* primIds);
+int oracle_scene_aabb(void* scene, float* aabb6);
+
+/* Ray queries. rays: 6 floats per ray (origin, direction). */
+int oracle_trace_first(void* scene, const float* rays, const float* geoNormals, float tmax,
+                       uint32_t n, float* tOut, int32_t* instOut, int32_t* primOut,
+                       float* surfParamsOut);
+int oracle_trace_any(void* scene, const float* pointsA, const float* pointsB, uint32_t n,
+                     uint8_t* occludedOut);
+
+/* Path tracer (CpuPathTracer equivalent). */
+void* oracle_pt_create(void* scene, const OrPtParams* params);
+void oracle_pt_destroy(void* pt);
+int oracle_pt_iterate(void* pt, int32_t numThreads);
+/* Cumulative target: 0 radiance (3 ch), 1 hit id (2 ch) */
+int oracle_pt_get_target(void* pt, int32_t target, float* out);
+int oracle_pt_stats(void* pt, OrStats* stats);
+/* One iteration restricted to rows [y0, y1) (for bounded CPU baselines). */
+int oracle_pt_iterate_rows(void* pt, int32_t numThreads, uint32_t y0, uint32_t y1);
+
+/* Building blocks exposed for known-answer tests. */
+int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
+uint64_t oracle_pcg64_next(uint64_t* state);
+uint64_t oracle_pcg64_seed(uint32_t seed);
+uint64_t oracle_part_by_two21(uint32_t x);
+void oracle_sincos(float x, float* s, float* c);
+float oracle_atan2(float y, float x);
+float oracle_acos(float x);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

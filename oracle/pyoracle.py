@@ -1,0 +1,255 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so): TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as a checker. The product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+class OrLod(C.Structure):
+    _fields_ = [("numVertices", C.c_uint32), ("numTriangles", C.c_uint32), ("numQuads", C.c_uint32),
+                ("numSpheres", C.c_uint32), ("vertices", C.c_void_p), ("normals", C.c_void_p),
+                ("uvs", C.c_void_p), ("indices", C.c_void_p), ("faceMaterials", C.c_void_p),
+                ("spheres", C.c_void_p), ("sphereMaterials", C.c_void_p)]
+
+
+class OrMaterial(C.Structure):
+    _fields_ = [("type", C.c_int32), ("albedo", C.c_float * 3), ("roughness", C.c_float * 2),
+                ("shadowing", C.c_int32), ("ndf", C.c_int32), ("radiance", C.c_float * 3),
+                ("scale", C.c_float * 3), ("albedoTexture", C.c_int32)]
+
+
+class OrTexture(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("texels", C.c_void_p)]
+
+
+class OrSceneDesc(C.Structure):
+    _fields_ = [("numLods", C.c_uint32), ("lods", C.POINTER(OrLod)), ("numInstances", C.c_uint32),
+                ("worldToInstance", C.c_void_p), ("instanceLod", C.c_void_p), ("numMaterials", C.c_uint32),
+                ("materials", C.POINTER(OrMaterial)), ("numTextures", C.c_uint32),
+                ("textures", C.POINTER(OrTexture)), ("numPointLights", C.c_uint32),
+                ("pointLights", C.c_void_p), ("hasBackground", C.c_int32), ("backgroundColor", C.c_float * 3),
+                ("backgroundScale", C.c_float * 3), ("camPos", C.c_float * 3), ("camDir", C.c_float * 3),
+                ("camUp", C.c_float * 3), ("vFov", C.c_float), ("nearPlane", C.c_float), ("farPlane", C.c_float),
+                ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class OrPtParams(C.Structure):
+    _fields_ = [("seed", C.c_int32), ("minPathLength", C.c_int32), ("maxPathLength", C.c_int32),
+                ("neeCount", C.c_int32), ("neePositionGuide", C.c_int32), ("rrStartDepth", C.c_int32)]
+
+
+class OrStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("shadowRays", C.c_uint64), ("nodeVisits", C.c_uint64),
+                ("instanceVisits", C.c_uint64), ("triTests", C.c_uint64), ("quadTests", C.c_uint64),
+                ("sphereTests", C.c_uint64)]
+
+
+def build():
+    """Compile liboracle.so with the recipe in oracle/Makefile."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        L = _lib
+        L.oracle_scene_create.restype = C.c_void_p
+        L.oracle_scene_create.argtypes = [C.POINTER(OrSceneDesc)]
+        L.oracle_scene_destroy.argtypes = [C.c_void_p]
+        L.oracle_bvh_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.oracle_bvh_get.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_scene_aabb.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_trace_first.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_uint32,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_trace_any.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.oracle_pt_create.restype = C.c_void_p
+        L.oracle_pt_create.argtypes = [C.c_void_p, C.POINTER(OrPtParams)]
+        L.oracle_pt_destroy.argtypes = [C.c_void_p]
+        L.oracle_pt_iterate.argtypes = [C.c_void_p, C.c_int32]
+        L.oracle_pt_iterate_rows.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32]
+        L.oracle_pt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.oracle_pt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_pcg64_seed.restype = C.c_uint64
+        L.oracle_pcg64_seed.argtypes = [C.c_uint32]
+        L.oracle_pcg64_next.restype = C.c_uint64
+        L.oracle_pcg64_next.argtypes = [C.POINTER(C.c_uint64)]
+        L.oracle_part_by_two21.restype = C.c_uint64
+        L.oracle_part_by_two21.argtypes = [C.c_uint32]
+        L.oracle_karras.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.oracle_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.oracle_atan2.restype = C.c_float
+        L.oracle_atan2.argtypes = [C.c_float, C.c_float]
+        L.oracle_acos.restype = C.c_float
+        L.oracle_acos.argtypes = [C.c_float]
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+class OracleScene:
+    """Owns the numpy buffers referenced by the descriptor while the scene is built."""
+
+    def __init__(self, spec):
+        L = lib()
+        self.spec = spec
+        keep = []
+        lods = (OrLod * max(1, len(spec.lods)))()
+        for i, l in enumerate(spec.lods):
+            idx = np.concatenate([l.triangles.reshape(-1), l.quads.reshape(-1)]).astype(np.uint32)
+            arrs = [np.ascontiguousarray(l.vertices, np.float32), np.ascontiguousarray(l.normals, np.float32),
+                    np.ascontiguousarray(l.uvs, np.float32), np.ascontiguousarray(idx),
+                    np.ascontiguousarray(l.face_materials, np.uint16), np.ascontiguousarray(l.spheres, np.float32),
+                    np.ascontiguousarray(l.sphere_materials, np.uint16)]
+            keep += arrs
+            lods[i] = OrLod(len(l.vertices), len(l.triangles), len(l.quads), len(l.spheres),
+                            *[_ptr(a) for a in arrs])
+        mats = (OrMaterial * max(1, len(spec.materials)))()
+        for i, m in enumerate(spec.materials):
+            mats[i] = OrMaterial(m.type, (C.c_float * 3)(*m.albedo), (C.c_float * 2)(*m.roughness), 1, 0,
+                                 (C.c_float * 3)(*m.radiance), (C.c_float * 3)(*m.scale), m.albedo_texture)
+        texs = (OrTexture * max(1, len(spec.textures)))()
+        for i, t in enumerate(spec.textures):
+            a = np.ascontiguousarray(t, np.float32)
+            keep.append(a)
+            texs[i] = OrTexture(a.shape[1], a.shape[0], _ptr(a))
+        w2i = np.ascontiguousarray(spec.world_to_instance, np.float32)
+        il = np.ascontiguousarray(spec.instance_lod, np.uint32)
+        pl = np.ascontiguousarray(spec.point_lights, np.float32)
+        keep += [w2i, il, pl]
+        d = OrSceneDesc()
+        d.numLods = len(spec.lods)
+        d.lods = lods
+        d.numInstances = len(il)
+        d.worldToInstance = _ptr(w2i)
+        d.instanceLod = _ptr(il)
+        d.numMaterials = len(spec.materials)
+        d.materials = mats
+        d.numTextures = len(spec.textures)
+        d.textures = texs
+        d.numPointLights = len(pl)
+        d.pointLights = _ptr(pl)
+        d.hasBackground = 1 if spec.background is not None else 0
+        if spec.background is not None:
+            d.backgroundColor = (C.c_float * 3)(*spec.background[0])
+            d.backgroundScale = (C.c_float * 3)(*spec.background[1])
+        d.camPos = (C.c_float * 3)(*spec.cam_pos)
+        d.camDir = (C.c_float * 3)(*spec.cam_dir)
+        d.camUp = (C.c_float * 3)(*spec.cam_up)
+        d.vFov = spec.vfov
+        d.nearPlane = 1e-4
+        d.farPlane = 1e10
+        d.width = spec.width
+        d.height = spec.height
+        self.handle = L.oracle_scene_create(C.byref(d))
+        if not self.handle:
+            raise RuntimeError("oracle_scene_create failed")
+
+    def close(self):
+        if self.handle:
+            lib().oracle_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bvh(self, which: int):
+        """(morton_sorted, parents, nodes (n,8) float32 view, prim_ids, num_internal); which=-1 is the TLAS."""
+        L = lib()
+        np_, ni = C.c_int32(), C.c_int32()
+        if not L.oracle_bvh_info(self.handle, which, C.byref(np_), C.byref(ni)):
+            raise IndexError(which)
+        n = np_.value
+        morton = np.zeros(max(n, 0), np.uint64)
+        parents = np.zeros(max(2 * n - 1, 0), np.int32)
+        nodes = np.zeros((2 * ni.value, 8), np.float32)
+        prim = np.zeros(max(n, 0), np.int32)
+        L.oracle_bvh_get(self.handle, which, _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim))
+        return morton, parents, nodes, prim, ni.value
+
+    def aabb(self):
+        a = np.zeros(6, np.float32)
+        lib().oracle_scene_aabb(self.handle, _ptr(a))
+        return a
+
+    def trace_first(self, rays: np.ndarray, tmax: float = 1048576.0, geo_normals=None):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        t = np.zeros(n, np.float32)
+        inst = np.zeros(n, np.int32)
+        prim = np.zeros(n, np.int32)
+        sp = np.zeros((n, 2), np.float32)
+        g = None if geo_normals is None else np.ascontiguousarray(geo_normals, np.float32)
+        lib().oracle_trace_first(self.handle, _ptr(rays), _ptr(g), tmax, n, _ptr(t), _ptr(inst), _ptr(prim), _ptr(sp))
+        return t, inst, prim, sp
+
+    def trace_any(self, a: np.ndarray, b: np.ndarray):
+        a = np.ascontiguousarray(a, np.float32)
+        b = np.ascontiguousarray(b, np.float32)
+        occ = np.zeros(len(a), np.uint8)
+        lib().oracle_trace_any(self.handle, _ptr(a), _ptr(b), len(a), _ptr(occ))
+        return occ.astype(bool)
+
+
+class OraclePathTracer:
+    def __init__(self, scene: OracleScene, seed=0, min_path=0, max_path=16, nee_count=1, rr_start=0):
+        self.scene = scene
+        p = OrPtParams(seed, min_path, max_path, nee_count, 0, rr_start)
+        self.handle = lib().oracle_pt_create(scene.handle, C.byref(p))
+
+    def iterate(self, threads: int = 0):
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        lib().oracle_pt_iterate(self.handle, threads)
+
+    def iterate_rows(self, y0: int, y1: int, threads: int = 0):
+        """One untallied pass over rows [y0, y1) (CPU baseline timing)."""
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        lib().oracle_pt_iterate_rows(self.handle, threads, y0, y1)
+
+    def target(self, name: str):
+        w, h = self.scene.spec.width, self.scene.spec.height
+        if name == "Radiance":
+            out = np.zeros((h, w, 3), np.float32)
+            lib().oracle_pt_get_target(self.handle, 0, _ptr(out))
+        elif name == "Hit ID":
+            out = np.zeros((h, w, 2), np.float32)
+            lib().oracle_pt_get_target(self.handle, 1, _ptr(out))
+        else:
+            raise KeyError(name)
+        return out
+
+    def stats(self):
+        s = OrStats()
+        lib().oracle_pt_stats(self.handle, C.byref(s))
+        return {k: getattr(s, k) for k, _ in OrStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().oracle_pt_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
