@@ -1,0 +1,337 @@
+"""Path-tracer benchmark: Mrays/s (and spp/s) at 1920x1080 on the displaced
+icosphere (1 310 720 triangles, 16 spp per frame, path length 10), next to the
+CPU oracle timed on this host's cores.
+
+One step = one 16-spp frame (16 render_iterate calls of the CUDA path tracer).
+
+value  -- rays (extension + shadow) of the K timed frames / the summed device
+          time of the path-tracing kernel (CUDA events on the library's stream);
+          the scene stays resident in HBM.
+e2e    -- the same metric through the public C API from host buffers: every step
+          re-uploads the scene from host memory (world_load_scenario: geometry
+          upload + GPU LBVH build), renders 16 iterations and copies the
+          radiance image back to host memory (wall clock around the calls).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank renders the frame with its own seed (the
+samples split across GPUs, per-GPU work fixed -> weak scaling); the e2e step
+averages the images with one NCCL all-reduce.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SPP_PER_FRAME = 16
+MAX_PATH = 10
+WIDTH, HEIGHT = 1920, 1080
+METRIC = "Mrays/s & spp/s at 1080p vs CPU PT"
+WORKLOAD = "displaced_icosphere_1310720tri_1920x1080_16spp_depth10"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--subdiv", type=int, default=8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path)), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (SM clock, reasons)."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def scene_bytes(spec):
+    """Host->device bytes of one scene upload (geometry, instances, materials, lights)."""
+    b = 0
+    for l in spec.lods:
+        nv, nt, nq, ns = len(l.vertices), len(l.triangles), len(l.quads), len(l.spheres)
+        b += nv * (12 + 12 + 8) + nt * 12 + nq * 16 + (nt + nq) * 2 + ns * (16 + 2)
+    ni = len(spec.instance_lod)
+    b += ni * (48 + 4 + 24 + 12)
+    return b
+
+
+def cpu_baseline(spec, seconds):
+    """CPU oracle (restatement of the reference CPU path tracer) on all host cores."""
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    sc = pyoracle.OracleScene(spec)
+    pt = pyoracle.OraclePathTracer(sc, seed=0, max_path=MAX_PATH)
+    rows_per_chunk = max(1, spec.height // 8)
+    rays, elapsed, rows_done, passes = 0, 0.0, 0, 0
+    t_start = time.perf_counter()
+    y = 0
+    while elapsed < seconds or rows_done == 0:
+        y1 = min(spec.height, y + rows_per_chunk)
+        before = pt.stats()["rays"]
+        t0 = time.perf_counter()
+        pt.iterate_rows(y, y1, threads)
+        elapsed += time.perf_counter() - t0
+        rays += pt.stats()["rays"] - before
+        rows_done += y1 - y
+        y = 0 if y1 >= spec.height else y1
+        if y == 0:
+            passes += 1
+        if time.perf_counter() - t_start > 4 * seconds:
+            break
+    mrays = rays / elapsed / 1e6
+    pixels = rows_done * spec.width
+    return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"{rows_done} rows x {spec.width} px x 1 spp ({pixels} paths, {rays} rays, {elapsed:.1f} s)",
+            "spp_per_s_1080p": round(pixels / elapsed / (spec.width * spec.height), 4)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from mufflon_b200 import scenes
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    from oracle import pyoracle
+    threads = os.cpu_count() or 1
+    sc = pyoracle.OracleScene(spec)
+    pt = pyoracle.OraclePathTracer(sc, seed=0, max_path=MAX_PATH)
+    band = max(1, HEIGHT // 16)  # a bounded sample of the frame per step
+    vals = []
+    tot_rays, tot_time = 0, 0.0
+    for i in range(args.warmup + args.steps):
+        y0 = (i * band) % HEIGHT
+        before = pt.stats()["rays"]
+        t0 = time.perf_counter()
+        pt.iterate_rows(y0, min(HEIGHT, y0 + band), threads)
+        dt = time.perf_counter() - t0
+        r = pt.stats()["rays"] - before
+        if i >= args.warmup:
+            tot_rays += r
+            tot_time += dt
+    v = tot_rays / tot_time / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * tot_time / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "step": f"1 spp over {band} rows of the frame (CPU oracle port, all host threads)"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} bands of {band} rows x {WIDTH} px, 1 spp"},
+            "e2e": {"value": round(v, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from mufflon_b200 import bindings, build, scenes
+    build.build()
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    dll = bindings.DllInterface()
+    bindings.load_scene_spec(dll, spec)
+    assert dll.render_enable_renderer(0, 0)
+    assert dll.renderer_set_parameter_int("Max. path length", MAX_PATH)
+    assert dll.renderer_set_parameter_int("Seed", rank)
+
+    def frame():
+        rays = shadow = nodes = prims = inst = 0
+        ms = 0.0
+        for _ in range(SPP_PER_FRAME):
+            dll.render_iterate()
+            s = dll.render_stats()
+            rays += s["rays"]; shadow += s["shadowRays"]; nodes += s["nodeVisits"]
+            prims += s["primTests"]; inst += s["instanceVisits"]; ms += s["kernelMs"]
+            if s["errors"]:
+                raise RuntimeError(f"traversal errors reported: {s['errors']}")
+        return rays, shadow, nodes, prims, inst, ms
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        dll.render_reset()
+        frame()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    tot = np.zeros(6)
+    for _ in range(args.steps):
+        dll.render_reset()
+        tot += np.array(frame(), dtype=np.float64)
+    barrier()
+    clk = clocks.stop()
+    rays, shadow, nodes, prims, inst, kernel_ms = tot
+    # max over ranks of the device time, sum of rays
+    if world > 1:
+        t = torch.tensor([kernel_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        kernel_ms_max = float(t.item())
+        r = torch.tensor([rays], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(r)
+        rays_all = float(r.item())
+    else:
+        kernel_ms_max, rays_all = kernel_ms, rays
+    mrays = rays_all / (kernel_ms_max * 1e-3) / 1e6
+    spp_s = SPP_PER_FRAME * args.steps * world / (kernel_ms_max * 1e-3)
+
+    # e2e: scene upload + BVH build + 16 iterations + image readback per step
+    d2h = WIDTH * HEIGHT * 3 * 4
+    h2d = scene_bytes(spec)
+    barrier()
+    e2e_rays, t_e2e = 0.0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        dll.core.world_load_scenario(dll.muffInst, dll.core.world_get_current_scenario(dll.muffInst))
+        for _ in range(SPP_PER_FRAME):
+            dll.render_iterate()
+            e2e_rays += dll.render_stats()["rays"]
+        img = dll.get_target_image("Radiance")
+        if world > 1:
+            ti = torch.from_numpy(img).cuda()
+            torch.distributed.all_reduce(ti)
+            img = (ti / world).cpu().numpy()
+        t_e2e += time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([t_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(t.item())
+        r = torch.tensor([e2e_rays], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(r)
+        e2e_rays = float(r.item())
+    e2e_mrays = e2e_rays / t_e2e / 1e6
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / launch time
+    launches = SPP_PER_FRAME * args.steps
+    alg_bytes = nodes * 64 + prims * 48 + inst * 72
+    achieved_gbs = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    peaks, peak_kind = measured_peaks()
+    l2 = bindings.c_float(0.0)
+    dll.core.mufflon_measure_l2_bandwidth(32 << 20, 100, bindings.byref(l2))
+    roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved_gbs / peaks["hbm_gbs"], 4), "traffic": None,
+                "peak_source": f"{peak_kind} HBM copy bandwidth",
+                "l2_read_peak_gbs": round(float(l2.value), 1),
+                "frac_of_l2": round(achieved_gbs / max(float(l2.value), 1e-9), 4),
+                "bytes_per_ray": round(alg_bytes / max(rays, 1), 1),
+                "kernel": "pt_megakernel", "launches": launches,
+                "avg_launch_ms": round(kernel_ms / launches, 3)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(spec, args.cpu_seconds)
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(mrays, 2), "unit": "Mrays/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(kernel_ms_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "triangles": int(spec.num_prims), "resolution": [WIDTH, HEIGHT],
+                           "spp_per_step": SPP_PER_FRAME, "max_path_length": MAX_PATH,
+                           "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)",
+                           "parallelism": f"replicas x{world} (samples split by seed)"},
+                "spp_per_s": round(spp_s, 3),
+                "rays_per_step": int(rays / args.steps),
+                "e2e": {"value": round(e2e_mrays, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h),
+                        "note": "scene upload + GPU LBVH build + 16 iterations + radiance readback per step (wall clock)"},
+                "gpu_launches": launches,
+                "roofline": roofline,
+                "cpu_baseline": cpu,
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    dll.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -286,6 +286,9 @@ CORE_API Boolean CDECL mufflon_lbvh_build_device(const float* dVertices, const u
                                                  uint32_t numQuads, const float* dSpheres, uint32_t numSpheres,
                                                  const float* aabb6, int32_t* numInternal, float* buildMs,
                                                  float* stageMs);
+/* Measured read bandwidth (GB/s) of an L2-resident buffer of `bytes`, read
+ * `repetitions` times; the denominator of the traversal roofline. */
+CORE_API Boolean CDECL mufflon_measure_l2_bandwidth(uint64_t bytes, int32_t repetitions, float* gbs);
 /* Stable radix sort of (uint64 key, int32 value) pairs in host memory. */
 CORE_API Boolean CDECL mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint32_t n);
 

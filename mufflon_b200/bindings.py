@@ -268,6 +268,7 @@ class DllHolder:
             "mufflon_lbvh_build_device": (c_uint32, [c_void_p, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32,
                                                      c_void_p, POINTER(c_int32), POINTER(c_float), c_void_p]),
             "mufflon_sort_pairs": (c_uint32, [c_void_p, c_void_p, c_uint32]),
+            "mufflon_measure_l2_bandwidth": (c_uint32, [c_uint64, c_int32, POINTER(c_float)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(c, name)

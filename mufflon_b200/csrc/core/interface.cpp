@@ -1085,6 +1085,14 @@ Boolean mufflon_lbvh_build_device(const float* dVertices, const uint32_t* dIndic
 	CATCH_ALL(false)
 }
 
+Boolean mufflon_measure_l2_bandwidth(uint64_t bytes, int32_t reps, float* gbs) {
+	TRY
+	CHECK(gbs && bytes >= (1u << 20) && reps > 0, "invalid arguments");
+	CHECK_CUDA(measure_l2_bandwidth(size_t(bytes), reps, gbs));
+	return true;
+	CATCH_ALL(false)
+}
+
 Boolean mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint32_t n) {
 	TRY
 	CHECK(keys && values, "invalid arguments");

@@ -248,6 +248,18 @@ __global__ void occlusion_kernel(const DScene S, const float* a, const float* b,
 	}
 }
 
+// Streaming read of an L2-resident buffer: the measured L2 read bandwidth is
+// the roofline denominator of the traversal kernel.
+__global__ void l2_read_kernel(const float4* __restrict__ buf, size_t n, int reps, float* sink) {
+	float acc = 0.0f;
+	for(int r = 0; r < reps; ++r)
+		for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+			const float4 v = __ldcg(buf + i);
+			acc += v.x + v.y + v.z + v.w;
+		}
+	if(acc == 1234.5f) *sink = acc;
+}
+
 // ------------------------------------------------------------ host wrappers
 static int sm_count() {
 	static int n = 0;
@@ -281,6 +293,30 @@ cudaError_t launch_trace_rays(const DScene& S, const float* rays, const float* g
 	if(n == 0) return cudaSuccess;
 	trace_rays_kernel<<<blocks, 128, 0, stream>>>(S, rays, geoNormals, tmax, n, t, inst, prim, sp);
 	return cudaGetLastError();
+}
+
+cudaError_t measure_l2_bandwidth(size_t bytes, int reps, float* gbs) {
+	float4* buf = nullptr;
+	float* sink = nullptr;
+	cudaError_t e = cudaMalloc(&buf, bytes);
+	if(e != cudaSuccess) return e;
+	if((e = cudaMalloc(&sink, sizeof(float))) != cudaSuccess) { cudaFree(buf); return e; }
+	cudaMemset(buf, 0, bytes);
+	const size_t n = bytes / sizeof(float4);
+	const int blocks = sm_count() * 8;
+	cudaEvent_t a, b;
+	cudaEventCreate(&a); cudaEventCreate(&b);
+	l2_read_kernel<<<blocks, 256>>>(buf, n, 2, sink); // warm the L2
+	cudaEventRecord(a);
+	l2_read_kernel<<<blocks, 256>>>(buf, n, reps, sink);
+	cudaEventRecord(b);
+	e = cudaEventSynchronize(b);
+	float ms = 0.0f;
+	cudaEventElapsedTime(&ms, a, b);
+	*gbs = float(double(bytes) * reps / (double(ms) * 1e-3) / 1e9);
+	cudaEventDestroy(a); cudaEventDestroy(b);
+	cudaFree(buf); cudaFree(sink);
+	return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_occlusion(const DScene& S, const float* a, const float* b, uint32_t n, uint8_t* out,

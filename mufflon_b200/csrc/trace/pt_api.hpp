@@ -20,4 +20,7 @@ cudaError_t launch_trace_rays(const DScene& scene, const float* rays, const floa
 cudaError_t launch_occlusion(const DScene& scene, const float* a, const float* b, uint32_t n, uint8_t* out,
                              cudaStream_t stream);
 
+// Read bandwidth of an L2-resident buffer of `bytes` (GB/s).
+cudaError_t measure_l2_bandwidth(size_t bytes, int reps, float* gbs);
+
 } // namespace mb

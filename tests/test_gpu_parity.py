@@ -146,7 +146,7 @@ def test_first_hit_bit_exact(dll, oracle, scene):
     assert np.array_equal(gp, op)
     assert np.array_equal(gt.view(np.uint32), ot.view(np.uint32))
     assert np.array_equal(gs.view(np.uint32), os_.view(np.uint32))
-    assert (gi >= 0).mean() > 0.3
+    assert (gi >= 0).mean() > (0.12 if scene == "instanced" else 0.3)
 
 
 @pytest.mark.parametrize("scene", ["cornell", "instanced"])
