@@ -292,6 +292,22 @@ CORE_API Boolean CDECL mufflon_measure_l2_bandwidth(uint64_t bytes, int32_t repe
 /* Stable radix sort of (uint64 key, int32 value) pairs in host memory. */
 CORE_API Boolean CDECL mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint32_t n);
 
+/* EXTENSION with no counterpart in the reference: the same stable sort of n
+ * device-resident pairs, in place, without allocating any device memory.
+ * For callers that cannot call cudaMalloc: an engine that has reserved all
+ * device memory for its own allocator, or a frame loop that must not stall in
+ * cudaMalloc/cudaFree (they may synchronise the device). The scratch space is
+ * a fixed array of about 12.3 MiB inside the library, held by every GPU that
+ * loads the library until the process exits; n above
+ * MUFFLON_SORT_NOALLOC_MAX_PAIRS is rejected with an error. The first call on
+ * a device looks up the array's address on that device (make it before any
+ * stream capture). All calls share the array, so calls that overlap on the
+ * GPU race. keys/values are device pointers owned by the caller; stream is a
+ * cudaStream_t (NULL: default stream); the call returns after the pairs are
+ * sorted. */
+#define MUFFLON_SORT_NOALLOC_MAX_PAIRS (1u << 20)
+CORE_API Boolean CDECL mufflon_sort_pairs_device_noalloc(uint64_t* keys, int32_t* values, uint32_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

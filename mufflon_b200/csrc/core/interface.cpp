@@ -6,6 +6,7 @@
 #include "../../../include/mufflon_core.h"
 #include "world.hpp"
 #include "../trace/pt_api.hpp"
+#include "../lbvh/sort_noalloc.hpp"
 
 #include <chrono>
 #include <cstdarg>
@@ -1089,6 +1090,20 @@ Boolean mufflon_measure_l2_bandwidth(uint64_t bytes, int32_t reps, float* gbs) {
 	TRY
 	CHECK(gbs && bytes >= (1u << 20) && reps > 0, "invalid arguments");
 	CHECK_CUDA(measure_l2_bandwidth(size_t(bytes), reps, gbs));
+	return true;
+	CATCH_ALL(false)
+}
+
+// Allocation-free sort: launches and memsets only (sort_noalloc.cu).
+Boolean mufflon_sort_pairs_device_noalloc(uint64_t* keys, int32_t* values, uint32_t n, void* stream) {
+	TRY
+	CHECK(n <= NOALLOC_MAX_PAIRS, "n = " + std::to_string(n) + " exceeds the maximum of " +
+	      std::to_string(NOALLOC_MAX_PAIRS) + " pairs of the allocation-free sort");
+	CHECK(n == 0 || (keys && values), "keys and values must be device pointers");
+	bool expired = false;
+	const cudaError_t e = sort_pairs_noalloc(keys, values, n, static_cast<cudaStream_t>(stream), &expired);
+	CHECK(!expired, "a bounded wait of the sort expired; the result is incomplete");
+	CHECK_CUDA(e);
 	return true;
 	CATCH_ALL(false)
 }
