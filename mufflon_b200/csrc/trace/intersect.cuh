@@ -387,15 +387,12 @@ MBD f3 bilerp3(f3 x00, f3 x10, f3 x01, f3 x11, float s, float t) {
 MBD f2 uvat(const DLod& l, uint32_t i) { return ldg2(l.uvs + 2 * size_t(i)); }
 MBD f3 nrmat(const DLod& l, uint32_t i) { return ldg3(l.normals + 3 * size_t(i)); }
 
-// Closest hit for a world-space ray (intersection.cu:366-621). `origin` is
-// offset by add_epsilon in place, as the reference's ray is.
-MBD Intersection first_intersection(const DScene& S, f3& origin, f3 dir, f3 geoN, float tmax,
-                                    LocalCounters& cnt, int2* bstack, int2* tstack) {
-	add_epsilon(origin, dir, geoN);
+// Closest hit of a world-space ray whose origin is already offset
+// (intersection.cu:366-492): returns (t, instance, primitive, surface params).
+MBD HitRec closest_hit(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, int2* bstack, int2* tstack) {
 	++cnt.rays;
 	HitRec best;
 	best.t = tmax; best.inst = -1; best.prim = -1; best.sp = make2(0.0f, 0.0f); best.has = false;
-	const f3 o = origin;
 	if(S.activeInstances == 1) {
 		blas_closest(S, S.validInstance, o, dir, best, cnt, bstack);
 	} else if(S.activeInstances > 1) {
@@ -408,6 +405,11 @@ MBD Intersection first_intersection(const DScene& S, f3& origin, f3 dir, f3 geoN
 			},
 			tstack, TLAS_STACK, cnt);
 	}
+	return best;
+}
+
+// Hit attribute synthesis for a closest hit (intersection.cu:511-620).
+MBD Intersection hit_attributes(const DScene& S, f3 origin, f3 dir, const HitRec& best) {
 	Intersection res;
 	res.distance = best.t;
 	res.inst = best.has ? best.inst : -1;
@@ -474,29 +476,52 @@ MBD Intersection first_intersection(const DScene& S, f3& origin, f3 dir, f3 geoN
 	return res;
 }
 
-// Shadow ray between two surface points (intersection.cu:624-753).
-MBD bool any_intersection(const DScene& S, f3 a, f3 b, f3 geoA, f3 geoB, f3 dirAB,
-                          LocalCounters& cnt, int2* bstack, int2* tstack) {
-	add_epsilon(a, dirAB, geoA);
-	add_epsilon(b, -dirAB, geoB);
+// Closest hit for a world-space ray (intersection.cu:366-621). `origin` is
+// offset by add_epsilon in place, as the reference's ray is.
+MBD Intersection first_intersection(const DScene& S, f3& origin, f3 dir, f3 geoN, float tmax,
+                                    LocalCounters& cnt, int2* bstack, int2* tstack) {
+	add_epsilon(origin, dir, geoN);
+	const HitRec best = closest_hit(S, origin, dir, tmax, cnt, bstack, tstack);
+	return hit_attributes(S, origin, dir, best);
+}
+
+// Occlusion test of a prepared shadow ray (origin already offset, unit
+// direction, world-space length tmax).
+MBD bool occluded(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, int2* bstack, int2* tstack) {
 	++cnt.rays; ++cnt.shadow;
-	const f3 corrected = b - a;
-	const float tmax = len(corrected);
-	const f3 dir = corrected / tmax;
 	if(S.activeInstances == 1) return blas_any(S, S.validInstance, a, dir, tmax, cnt, bstack);
 	if(S.activeInstances <= 0) return false;
 	const FastRay wr = make_ray(a, dir);
-	bool occluded = false;
+	bool occ = false;
 	const float tmaxBox = tmax * BOX_SLACK;
 	traverse(S.tlasNodes, S.tlasNumInternal, wr,
 		[&]() { return tmaxBox; },
 		[&](int first, int count) {
 			for(int k = 0; k < count; ++k)
-				if(blas_any(S, uint32_t(__ldg(S.tlasPrimIds + first + k)), a, dir, tmax, cnt, bstack)) { occluded = true; return false; }
+				if(blas_any(S, uint32_t(__ldg(S.tlasPrimIds + first + k)), a, dir, tmax, cnt, bstack)) { occ = true; return false; }
 			return true;
 		},
 		tstack, TLAS_STACK, cnt);
-	return occluded;
+	return occ;
+}
+
+// Shadow-ray set-up of intersection.cu:624-637: both end points are offset
+// along their geometric normals; returns the origin, direction and length.
+MBD void shadow_ray(f3 a, f3 b, f3 geoA, f3 geoB, f3 dirAB, f3& o, f3& dir, float& tmax) {
+	add_epsilon(a, dirAB, geoA);
+	add_epsilon(b, -dirAB, geoB);
+	const f3 corrected = b - a;
+	tmax = len(corrected);
+	dir = corrected / tmax;
+	o = a;
+}
+
+// Shadow ray between two surface points (intersection.cu:624-753).
+MBD bool any_intersection(const DScene& S, f3 a, f3 b, f3 geoA, f3 geoB, f3 dirAB,
+                          LocalCounters& cnt, int2* bstack, int2* tstack) {
+	f3 o, dir; float tmax;
+	shadow_ray(a, b, geoA, geoB, dirAB, o, dir, tmax);
+	return occluded(S, o, dir, tmax, cnt, bstack, tstack);
 }
 
 struct TangentSpace { f3 shadingN, geoN, shadingTX, shadingTY; };
