@@ -52,7 +52,7 @@ struct ParamDesc { const char* name; ParameterType type; };
 const ParamDesc PT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
-	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT },
+	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
 };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
@@ -65,6 +65,7 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "NEE count")) return &r.params.neeCount;
 	if(!std::strcmp(name, "RR start depth")) return &r.params.rrStartDepth;
 	if(!std::strcmp(name, "Blocks per SM")) return &r.blocksPerSm;
+	if(!std::strcmp(name, "Megakernel")) return &r.megakernel;
 	return nullptr;
 }
 
@@ -92,6 +93,43 @@ void ensure_render_buffers(MufflonInstance& I) {
 	r.needsReset = true;
 }
 
+// Wavefront state for the current resolution and NEE count (one slab).
+void ensure_wavefront_buffers(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	const size_t n = size_t(r.width) * r.height;
+	const int nee = r.params.neeCount > 0 ? r.params.neeCount : 1;
+	static const size_t ALIGN = 256;
+	auto al = [](size_t b) { return (b + ALIGN - 1) / ALIGN * ALIGN; };
+	const size_t need = al(n * 16) * 2 + al(n * 8) + 2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) +
+	                    al(n * nee * 4) + 3 * al(n * nee * 16) + al(WF_COUNTERS * 4);
+	if(r.wfMemory && r.wfNee == nee && r.wfPixels == n) return;
+	if(r.wfMemory) cudaFree(r.wfMemory);
+	r.wfMemory = nullptr;
+	r.wfNee = 0;
+	r.wfPixels = 0;
+	CHECK_CUDA(cudaMalloc(&r.wfMemory, need));
+	char* m = static_cast<char*>(r.wfMemory);
+	auto take = [&](size_t b) { char* p = m; m += al(b); return p; };
+	WfState& W = r.wf;
+	W.thrPdf = reinterpret_cast<float4*>(take(n * 16));
+	W.rad = reinterpret_cast<float4*>(take(n * 16));
+	W.hit0 = reinterpret_cast<float2*>(take(n * 8));
+	for(int q = 0; q < 2; ++q) {
+		W.qPath[q] = reinterpret_cast<int*>(take(n * 4));
+		W.qOrg[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qDir[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHit[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHitSpy[q] = reinterpret_cast<float*>(take(n * 4));
+	}
+	W.sPath = reinterpret_cast<int*>(take(n * nee * 4));
+	W.sOrg = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.sDir = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.sContrib = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.counters = reinterpret_cast<unsigned*>(take(WF_COUNTERS * 4));
+	r.wfNee = nee;
+	r.wfPixels = n;
+}
+
 void load_scene_if_needed(MufflonInstance& I) {
 	if(!I.sceneDirty && I.scene.valid) return;
 	std::string err;
@@ -104,6 +142,9 @@ void load_scene_if_needed(MufflonInstance& I) {
 
 namespace mb {
 void RendererState::release() {
+	if(wfMemory) cudaFree(wfMemory);
+	wfMemory = nullptr;
+	wf = WfState{};
 	cudaFree(rng); cudaFree(radiance); cudaFree(hitId); cudaFree(workCounter); cudaFree(counters);
 	if(evStart) cudaEventDestroy(evStart);
 	if(evStop) cudaEventDestroy(evStop);
@@ -783,8 +824,10 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	rs.width = r.width; rs.height = r.height;
 	rs.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, sizeof(TraceCounters), I.stream));
+	if(!r.megakernel) ensure_wavefront_buffers(I);
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
-	CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
+	if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
+	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(&r.lastCounters, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));

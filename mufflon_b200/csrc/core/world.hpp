@@ -16,6 +16,7 @@
 
 #include "../trace/scene_types.hpp"
 #include "../lbvh/lbvh.hpp"
+#include "../trace/wavefront.hpp"
 
 namespace mb {
 
@@ -130,6 +131,11 @@ struct RendererState {
 	bool enabled = false;
 	PtParams params{ 0, 0, 16, 1, 0 };
 	int32_t blocksPerSm = 8;
+	int32_t megakernel = 0;       // 0: wavefront stages (default), 1: single megakernel
+	WfState wf{};
+	void* wfMemory = nullptr;
+	int32_t wfNee = 0;
+	size_t wfPixels = 0;
 	bool targetRadiance = true;
 	bool targetHitId = false;
 	bool needsReset = true;

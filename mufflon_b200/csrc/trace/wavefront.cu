@@ -1,0 +1,345 @@
+// Wavefront path tracer: pt_sample (src/core/renderer/pt/pt_common.hpp:75-156)
+// split into stage kernels that run once per bounce over queues in HBM.
+//
+//   camera   one thread per pixel: consume the camera's and the first walk's
+//            random numbers, write the primary ray into queue 0;
+//   extend   persistent warps pull 32 rays at a time from the current queue
+//            (one atomic per warp) and run closest-hit traversal only;
+//   shadow   persistent warps pull shadow-ray groups, run any-hit traversal
+//            and add the visible next-event contributions to the path's sum;
+//   shade    one thread per queued path: hit attributes, emission with MIS,
+//            then (if the path continues) next-event estimation, which
+//            appends shadow rays, and the BSDF sample, Russian roulette and
+//            the next ray, appended to the other queue;
+//   finalize one thread per pixel: running mean of the iteration's result.
+//
+// Each kernel is small and does one kind of work, so it keeps its lanes
+// converged, stays in the instruction cache and needs few registers. The
+// per-path order of random numbers and of radiance additions is the one of
+// pt_sample: the shadow kernel of bounce k runs after shade k and before
+// shade k+1, so a next-event contribution is added between the emission terms
+// that surround it, exactly as the sequential loop adds them.
+#include "shading.cuh"
+#include "wavefront.hpp"
+
+#include <cooperative_groups.h>
+
+namespace mb {
+namespace {
+
+enum { C_QUEUE0 = 0, C_QUEUE1 = 1, C_SHADOW = 2, C_WORK = 3 };
+
+MBD float nan_to_zero(float x) { return isnan(x) ? 0.0f : x; }
+MBD f3 contribute(f3 acc, f3 c) {
+	return make3(acc.x + nan_to_zero(c.x), acc.y + nan_to_zero(c.y), acc.z + nan_to_zero(c.z));
+}
+MBD f3 incident_direction(f3 e) {
+	float t = 1.0f - e.x * e.x - e.y * e.y;
+	t = fminf(fmaxf(t, 0.0f), 1.0f);
+	return make3(e.x, e.y, sgn(e.z) * sqrt_(t));
+}
+MBD float4 pack(f3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+// One atomic per group of converged lanes that each ask for `want` items.
+MBD unsigned warp_reserve(unsigned* counter, unsigned want) {
+	namespace cg = cooperative_groups;
+	cg::coalesced_group g = cg::coalesced_threads();
+	unsigned base = 0;
+	if(g.thread_rank() == 0) base = atomicAdd(counter, g.size() * want);
+	base = g.shfl(base, 0);
+	return base + g.thread_rank() * want;
+}
+
+MBD void flush_counters(const LocalCounters& cnt, TraceCounters* out) {
+	unsigned long long rays = cnt.rays, shadow = cnt.shadow, nodes = cnt.nodes, prims = cnt.prims, inst = cnt.instances;
+	unsigned errs = cnt.errors;
+	for(int o = 16; o > 0; o >>= 1) {
+		rays += __shfl_down_sync(0xffffffffu, rays, o);
+		shadow += __shfl_down_sync(0xffffffffu, shadow, o);
+		nodes += __shfl_down_sync(0xffffffffu, nodes, o);
+		prims += __shfl_down_sync(0xffffffffu, prims, o);
+		inst += __shfl_down_sync(0xffffffffu, inst, o);
+		errs += __shfl_down_sync(0xffffffffu, errs, o);
+	}
+	if((threadIdx.x & 31u) == 0) {
+		if(rays) atomicAdd(&out->rays, rays);
+		if(shadow) atomicAdd(&out->shadowRays, shadow);
+		if(nodes) atomicAdd(&out->nodeVisits, nodes);
+		if(prims) atomicAdd(&out->primTests, prims);
+		if(inst) atomicAdd(&out->instanceVisits, inst);
+		if(errs) atomicAdd(&out->errors, errs);
+	}
+}
+
+__global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t numPixels, uint32_t width) {
+	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(p >= numPixels) return;
+	u64 rng = W.rng[p];
+	(void)pcg_next(rng); // create_camera
+	const u64 x0 = pcg_next(rng);
+	(void)pcg_next(rng);
+	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
+	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
+	float pdfF;
+	const f3 dir = pinhole_ray(S.camera, int(p % width), int(p / width), ru0, ru1, pdfF);
+	f3 thr = make3(1.0f, 1.0f, 1.0f);
+	bool alive = true;
+	if(0 >= P.rrStartDepth) {
+		const float cp = fmin_(maxc(thr) + 0.1f, 1.0f);
+		if(rr >= cp) alive = false;
+		else thr = thr / cp;
+	}
+	W.rng[p] = rng;
+	W.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	W.hit0[p] = make_float2(-1.0f, -1.0f);
+	W.thrPdf[p] = pack(thr, pdfF);
+	if(!alive) return;
+	f3 o = lv(S.camera.position);
+	add_epsilon(o, dir, make3(0.0f, 0.0f, 0.0f));
+	const unsigned slot = warp_reserve(W.counters + C_QUEUE0, 1u);
+	W.qPath[0][slot] = int(p);
+	W.qOrg[0][slot] = pack(o, 0.0f);
+	W.qDir[0][slot] = pack(dir, 0.0f);
+}
+
+__global__ void __launch_bounds__(128) k_extend(const DScene S, WfState W, int q, int workIdx, TraceCounters* counters) {
+	int2 bstack[BLAS_STACK];
+	int2 tstack[TLAS_STACK];
+	LocalCounters cnt;
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	const unsigned lane = threadIdx.x & 31u;
+	for(;;) {
+		unsigned base = 0;
+		if(lane == 0) base = atomicAdd(W.counters + C_WORK + workIdx, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if(base >= count) break;
+		const unsigned slot = base + lane;
+		if(slot < count) {
+			const float4 o = W.qOrg[q][slot], d = W.qDir[q][slot];
+			const HitRec h = closest_hit(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, cnt, bstack, tstack);
+			W.qHit[q][slot] = make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x);
+			W.qHitSpy[q][slot] = h.sp.y;
+		}
+	}
+	flush_counters(cnt, counters);
+}
+
+__global__ void __launch_bounds__(128) k_shadow(const DScene S, WfState W, int neeCount, int workIdx, TraceCounters* counters) {
+	int2 bstack[BLAS_STACK];
+	int2 tstack[TLAS_STACK];
+	LocalCounters cnt;
+	const unsigned groups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW) / unsigned(neeCount);
+	const unsigned lane = threadIdx.x & 31u;
+	for(;;) {
+		unsigned base = 0;
+		if(lane == 0) base = atomicAdd(W.counters + C_WORK + workIdx, 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if(base >= groups) break;
+		const unsigned g = base + lane;
+		if(g < groups) {
+			const int p = W.sPath[g * neeCount];
+			float4 acc = W.rad[p];
+			f3 radiance = f4to3(acc);
+			for(int i = 0; i < neeCount; ++i) {
+				const unsigned slot = g * neeCount + i;
+				const float4 o = W.sOrg[slot];
+				if(!(o.w > 0.0f)) continue; // no contribution in this slot
+				const float4 d = W.sDir[slot];
+				if(!occluded(S, f4to3(o), f4to3(d), o.w, cnt, bstack, tstack))
+					radiance = contribute(radiance, f4to3(W.sContrib[slot]));
+			}
+			W.rad[p] = pack(radiance, acc.w);
+		}
+	}
+	flush_counters(cnt, counters);
+}
+
+__global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P, WfState W, int q, int bounce) {
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
+	if(slot >= count) return;
+	const int p = W.qPath[q][slot];
+	const f3 origin = f4to3(W.qOrg[q][slot]);
+	const f3 dir = f4to3(W.qDir[q][slot]);
+	const float4 hh = W.qHit[q][slot];
+	HitRec hr;
+	hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
+	hr.sp = make2(hh.w, W.qHitSpy[q][slot]);
+	hr.has = hr.inst >= 0;
+	const float4 tp = W.thrPdf[p];
+	f3 throughput = f4to3(tp);
+	const float pdfF = tp.w;
+	const float4 ra = W.rad[p];
+	f3 radiance = f4to3(ra);
+	// -- the new vertex (random_walk.hpp:88-111)
+	bool surface = false;
+	f3 position = make3(0.0f, 0.0f, 0.0f), incidentEncoded;
+	float incidentPdf;
+	TangentSpace ts;
+	Params mat;
+	const Intersection hit = hit_attributes(S, origin, dir, hr);
+	if(hit.inst < 0) {
+		incidentEncoded = dir;
+		incidentPdf = pdfF * 1.0f;
+	} else {
+		surface = true;
+		position = origin + dir * hit.distance;
+		ts = tangent_space(S, hit);
+		incidentEncoded = make3(dir.x, dir.y, hit.distance * sgn(dir.z));
+		mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+		const float inCosAbs = fabsf(dot(dir, ts.shadingN));
+		incidentPdf = __fdiv_rn(pdfF * fabsf(inCosAbs), hit.distance * hit.distance);
+	}
+	if(bounce == 0) W.hit0[p] = make_float2(float(surface ? hit.inst : -1), float(surface ? hit.prim : -1));
+	const int pathLen = bounce + 1;
+	// -- emission (pt_common.hpp:139-153)
+	if(pathLen >= P.minPathLength) {
+		f3 emission = make3(0.0f, 0.0f, 0.0f);
+		float connectPdf = 0.0f;
+		if(!surface) {
+			if(S.hasBackground) {
+				emission = lv(S.bgColor) * lv(S.bgScale);
+				if(nonzero(emission)) {
+					const float bgFlux = (S.bgFlux[0] + S.bgFlux[1]) + S.bgFlux[2];
+					const float pb = __fdiv_rn(bgFlux, (S.dirFlux + S.rootFlux) + bgFlux);
+					connectPdf = __fdiv_rn(1.0f, 4.0f * PI) * pb;
+				}
+			}
+		} else if(mat.type == MAT_EMISSIVE) {
+			const f3 ex = -incident_direction(incidentEncoded);
+			const float cosOut = dot(ts.geoN, ex);
+			if(cosOut > 0.0f) {
+				emission = mat.radiance;
+				if(nonzero(emission)) connectPdf = light_connect_pdf(S, hit.inst, hit.prim, hit.sp);
+			}
+		}
+		if(nonzero(emission) && pathLen > 1) {
+			const float misWeight = __fdiv_rn(1.0f, 1.0f + float(P.neeCount) * __fdiv_rn(connectPdf, incidentPdf));
+			emission = emission * misWeight;
+		}
+		radiance = contribute(radiance, throughput * emission);
+	}
+	W.rad[p] = pack(radiance, ra.w);
+	if(!surface || !(pathLen < P.maxPathLength)) return;
+	// -- next loop iteration of pt_sample: next-event estimation
+	u64 rng = W.rng[p];
+	const f3 incident = incident_direction(incidentEncoded);
+	if(pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
+		const u64 neeSeed = pcg_next(rng);
+		unsigned base = 0xFFFFFFFFu;
+		for(int i = 0; i < P.neeCount; ++i) {
+			const u64 r = pcg_next(rng);
+			const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
+			const Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, position, nu0, nu1);
+			if(!nee.valid) continue;
+			EvalValue val = material_evaluate(ts, mat, incident, nee.dir);
+			if(nee.cosOut != 0.0f) val.cosOut *= nee.cosOut;
+			const f3 rad = val.value * nee.diffIrradiance;
+			if(any_pos(rad) && val.cosOut > 0.0f) {
+				const float hitPdf = __fdiv_rn(val.pdfF * fabsf(nee.cosOut), nee.distSq);
+				const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
+				const f3 c = ((throughput * val.cosOut) * rad) * mis;
+				f3 so, sd; float stmax;
+				shadow_ray(position, nee.position, ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
+				if(base == 0xFFFFFFFFu) {
+					base = atomicAdd(W.counters + C_SHADOW, unsigned(P.neeCount));
+					for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
+				}
+				W.sOrg[base + i] = pack(so, stmax);
+				W.sDir[base + i] = pack(sd, 0.0f);
+				W.sContrib[base + i] = pack(c, 0.0f);
+			}
+		}
+	}
+	// -- walk (random_walk.hpp:38-86)
+	const u64 x0 = pcg_next(rng), x1 = pcg_next(rng);
+	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
+	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
+	W.rng[p] = rng;
+	const PathSample s = material_sample(ts, mat, incident, ru0, ru1, x1);
+	if(!s.valid) return;
+	throughput = throughput * s.throughput;
+	if(pathLen >= P.rrStartDepth) {
+		const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
+		if(rr >= cp) return;
+		throughput = throughput / cp;
+	}
+	W.thrPdf[p] = pack(throughput, s.pdfF);
+	f3 o = position;
+	add_epsilon(o, s.excident, ts.geoN);
+	const int out = q ^ 1;
+	const unsigned nslot = warp_reserve(W.counters + out, 1u);
+	W.qPath[out][nslot] = p;
+	W.qOrg[out][nslot] = pack(o, 0.0f);
+	W.qDir[out][nslot] = pack(s.excident, 0.0f);
+}
+
+__global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
+	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(p >= numPixels) return;
+	const float den = fmaxf(1.0f, float(R.iteration) + 1.0f);
+	const float4 rad = W.rad[p];
+	if(R.radiance) {
+		float* cr = R.radiance + 3 * size_t(p);
+		const float it[3] = { rad.x, rad.y, rad.z };
+		for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+	}
+	if(R.hitId) {
+		const float2 h = W.hit0[p];
+		float* ch = R.hitId + 2 * size_t(p);
+		const float it[2] = { h.x, h.y };
+		for(int c = 0; c < 2; ++c) { const float diff = it[c] - ch[c]; ch[c] += __fdiv_rn(diff, den); }
+	}
+	if(R.iterRadiance) {
+		float* o = R.iterRadiance + 3 * size_t(p);
+		o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
+	}
+}
+
+int persistent_blocks(const void* fn, int threads) {
+	int dev = 0, sms = 148, perSm = 4;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, threads, 0);
+	return sms * (perSm > 0 ? perSm : 1);
+}
+
+} // namespace
+
+cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const RenderState& R, WfState W,
+                                TraceCounters* counters, cudaStream_t stream) {
+	const uint32_t n = R.width * R.height;
+	if(n == 0) return cudaSuccess;
+	static int extendBlocks = 0, shadowBlocks = 0;
+	if(!extendBlocks) {
+		extendBlocks = persistent_blocks(reinterpret_cast<const void*>(k_extend), 128);
+		shadowBlocks = persistent_blocks(reinterpret_cast<const void*>(k_shadow), 128);
+	}
+	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
+	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;
+	const unsigned workSlots = WF_COUNTERS - C_WORK;
+	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
+	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);
+	if(e != cudaSuccess) return e;
+	W.rng = R.rngState;
+	const unsigned grid = (n + 127) / 128;
+	k_camera<<<grid, 128, 0, stream>>>(S, P, W, n, R.width);
+	unsigned work = 0;
+	for(int b = 0; b < maxBounces; ++b) {
+		const int q = b & 1;
+		if(work + 2 > workSlots) { // very long paths: recycle the work counters (stream ordered)
+			cudaMemsetAsync(W.counters + C_WORK, 0, sizeof(unsigned) * workSlots, stream);
+			work = 0;
+		}
+		k_extend<<<extendBlocks, 128, 0, stream>>>(S, W, q, int(work++), counters);
+		if(b > 0) k_shadow<<<shadowBlocks, 128, 0, stream>>>(S, W, neeCount, int(work++), counters);
+		// the shade of this bounce appends to the other queue and to the shadow queue
+		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);
+		cudaMemsetAsync(W.counters + C_SHADOW, 0, sizeof(unsigned), stream);
+		k_shade<<<grid, 128, 0, stream>>>(S, P, W, q, b);
+	}
+	k_finalize<<<grid, 128, 0, stream>>>(W, R, n);
+	return cudaGetLastError();
+}
+
+} // namespace mb

@@ -1,0 +1,35 @@
+// Device state of the wavefront path tracer (see wavefront.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "scene_types.hpp"
+
+namespace mb {
+
+// All arrays are sized for one path per pixel; queues are indexed by slot.
+struct WfState {
+	uint64_t* rng;        // per pixel (the renderer's generator state)
+	float4* thrPdf;       // per path: throughput xyz, pdf of the sampled direction
+	float4* rad;          // per path: radiance of this iteration
+	float2* hit0;         // per path: first hit (instance, primitive)
+	int* qPath[2];        // extension queues (double buffered)
+	float4* qOrg[2];      // ray origin (epsilon offset applied)
+	float4* qDir[2];      // ray direction
+	float4* qHit[2];      // t, instance bits, primitive bits, surface u
+	float* qHitSpy[2];    // surface v
+	int* sPath;           // shadow rays: neeCount consecutive slots per path
+	float4* sOrg;         // origin, length (<= 0: empty slot)
+	float4* sDir;         // direction
+	float4* sContrib;     // contribution if unoccluded
+	unsigned* counters;   // queue sizes and per-launch work counters (WF_COUNTERS)
+};
+
+// Size of WfState::counters: 3 queue sizes plus one work counter per
+// persistent launch (two per bounce); longer paths recycle the work counters.
+constexpr unsigned WF_COUNTERS = 4096;
+
+// One iteration (one sample per pixel) of the wavefront path tracer.
+cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
+                                TraceCounters* counters, cudaStream_t stream);
+
+} // namespace mb

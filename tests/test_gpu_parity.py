@@ -92,10 +92,16 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
     _compare_bvh(dll, oracle, spec.lods[0])
 
 
+DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
+                  "RR start depth": 0, "Megakernel": 0}
+
+
 def _load(dll, spec):
     dll.world_clear_all()
     bindings.load_scene_spec(dll, spec)
     assert dll.render_enable_renderer(0, 0)
+    for name, value in DEFAULT_PARAMS.items():  # the library instance is shared by all tests
+        assert dll.renderer_set_parameter_int(name, value)
 
 
 def _camera_rays(spec, n, seed):
@@ -161,15 +167,22 @@ def test_occlusion_matches_oracle(dll, oracle, scene):
     assert np.array_equal(dll.trace_occlusion(a, b), sc.trace_any(a, b))
 
 
-def _render_pair(dll, oracle, spec, spp, max_path, seed=0, rr_start=0):
+KERNELS = {"wavefront": 0, "megakernel": 1}
+
+
+def _render_pair(dll, oracle, spec, spp, max_path, seed=0, rr_start=0, kernel="wavefront", nee=1, min_path=0):
     _load(dll, spec)
     dll.render_enable_render_target("Radiance", False)
     dll.render_enable_render_target("Hit ID", False)
+    assert dll.renderer_set_parameter_int("Megakernel", KERNELS[kernel])
     assert dll.renderer_set_parameter_int("Seed", seed)
     assert dll.renderer_set_parameter_int("Max. path length", max_path)
+    assert dll.renderer_set_parameter_int("Min. path length", min_path)
+    assert dll.renderer_set_parameter_int("NEE count", nee)
     assert dll.renderer_set_parameter_int("RR start depth", rr_start)
     sc = oracle.OracleScene(spec)
-    pt = oracle.OraclePathTracer(sc, seed=seed, max_path=max_path, rr_start=rr_start)
+    pt = oracle.OraclePathTracer(sc, seed=seed, min_path=min_path, max_path=max_path, nee_count=nee,
+                                 rr_start=rr_start)
     dll.render_iterate()
     pt.iterate()
     first_hits = (dll.get_target_image("Hit ID"), pt.target("Hit ID"))
@@ -180,28 +193,67 @@ def _render_pair(dll, oracle, spec, spp, max_path, seed=0, rr_start=0):
     return first_hits, (dll.get_target_image("Radiance"), pt.target("Radiance"))
 
 
-def test_pt_cornell_parity(dll, oracle):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_pt_cornell_parity(dll, oracle, kernel):
     """Config 0: Cornell box 256x256, 4 spp, path length 8."""
     spec = scenes.cornell_box(0)
-    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 4, 8)
+    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 4, 8, kernel=kernel)
     assert np.array_equal(gh, oh), "first-hit ids differ"
     err = rel_rmse(gr, orad)
     assert err <= RMSE_TOL, err
     assert orad.mean() > 0.05
 
 
-def test_pt_icosphere_parity(dll, oracle):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_pt_icosphere_parity(dll, oracle, kernel):
     spec = scenes.displaced_icosphere(0, subdiv=6, width=160, height=90)
-    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 2, 10)
+    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 2, 10, kernel=kernel)
     assert np.array_equal(gh, oh)
     assert rel_rmse(gr, orad) <= RMSE_TOL
 
 
-def test_pt_instanced_parity(dll, oracle):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_pt_instanced_parity(dll, oracle, kernel):
     spec = _small_instanced(1)
-    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 2, 12, rr_start=3)
+    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 2, 12, rr_start=3, kernel=kernel)
     assert np.array_equal(gh, oh)
     assert rel_rmse(gr, orad) <= RMSE_TOL
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
+def test_pt_multi_nee_min_path_parity(dll, oracle, kernel):
+    """Several next-event samples per vertex (shadow-ray groups) and a minimum path length."""
+    spec = scenes.cornell_box(2, 96, 96)
+    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 2, 6, nee=3, min_path=2, rr_start=2, kernel=kernel)
+    assert np.array_equal(gh, oh)
+    assert rel_rmse(gr, orad) <= RMSE_TOL
+    assert orad.mean() > 0.01
+
+
+def test_pt_long_paths_parity(dll, oracle):
+    """Path length beyond the usual limit keeps the wavefront stages in step with the sequential loop."""
+    spec = scenes.cornell_box(3, 48, 48)
+    (gh, oh), (gr, orad) = _render_pair(dll, oracle, spec, 1, 40, rr_start=30)
+    assert np.array_equal(gh, oh)
+    assert rel_rmse(gr, orad) <= RMSE_TOL
+
+
+def test_wavefront_equals_megakernel(dll):
+    """The two kernel schedules produce the same bits."""
+    spec = scenes.cornell_box(4, 128, 128)
+    out = []
+    for kernel in KERNELS.values():
+        _load(dll, spec)
+        dll.render_enable_render_target("Radiance", False)
+        dll.render_enable_render_target("Hit ID", False)
+        assert dll.renderer_set_parameter_int("Megakernel", kernel)
+        assert dll.renderer_set_parameter_int("NEE count", 2)
+        assert dll.renderer_set_parameter_int("Max. path length", 12)
+        for _ in range(3):
+            dll.render_iterate()
+        out.append((dll.get_target_image("Radiance").copy(), dll.get_target_image("Hit ID").copy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
 
 
 def test_gpu_matches_golden_fixture(dll):
