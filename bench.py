@@ -217,14 +217,28 @@ def run_b200(args):
     def frame():
         rays = shadow = nodes = prims = inst = 0
         ms = 0.0
+        launches = 1  # the generator seeding after render_reset
         for _ in range(SPP_PER_FRAME):
             dll.render_iterate()
             s = dll.render_stats()
             rays += s["rays"]; shadow += s["shadowRays"]; nodes += s["nodeVisits"]
             prims += s["primTests"]; inst += s["instanceVisits"]; ms += s["kernelMs"]
+            launches += dll.stage_stats()["launches"]
             if s["errors"]:
                 raise RuntimeError(f"traversal errors reported: {s['errors']}")
-        return rays, shadow, nodes, prims, inst, ms
+        return rays, shadow, nodes, prims, inst, ms, launches
+
+    def stage_frame():
+        """One untimed frame with events around every stage launch."""
+        assert dll.renderer_set_parameter_int("Stage timing", 1)
+        dll.render_reset()
+        acc = {}
+        for _ in range(SPP_PER_FRAME):
+            dll.render_iterate()
+            for k, v in dll.stage_stats().items():
+                acc[k] = acc.get(k, 0) + v
+        assert dll.renderer_set_parameter_int("Stage timing", 0)
+        return acc
 
     def barrier():
         torch.cuda.synchronize()
@@ -237,13 +251,13 @@ def run_b200(args):
     clocks = ClockSampler(local)
     clocks.start()
     barrier()
-    tot = np.zeros(6)
+    tot = np.zeros(7)
     for _ in range(args.steps):
         dll.render_reset()
         tot += np.array(frame(), dtype=np.float64)
     barrier()
     clk = clocks.stop()
-    rays, shadow, nodes, prims, inst, kernel_ms = tot
+    rays, shadow, nodes, prims, inst, kernel_ms, gpu_launches = tot
     # max over ranks of the device time, sum of rays
     if world > 1:
         t = torch.tensor([kernel_ms], device="cuda")
@@ -283,10 +297,16 @@ def run_b200(args):
         e2e_rays = float(r.item())
     e2e_mrays = e2e_rays / t_e2e / 1e6
 
-    # roofline of the dominant kernel: algorithmic bytes per launch / launch time
-    launches = SPP_PER_FRAME * args.steps
-    alg_bytes = nodes * 64 + prims * 48 + inst * 72
-    achieved_gbs = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    # roofline of the dominant kernel (closest-hit traversal): algorithmic
+    # bytes per launch / its average launch time (events on the library's
+    # stream). Per unit: an 8-wide node 80 B, a primitive-soup slot 48 B, an
+    # instance entry 56 B (world-to-instance rows 48 B + LoD index 4 B + the
+    # LoD's hierarchy pointers); the queue entry of the ray 32 B in, 20 B out.
+    st = stage_frame()
+    extend_launches = SPP_PER_FRAME * MAX_PATH
+    alg_bytes = (st["extendNodeVisits"] * 80 + st["extendPrimTests"] * 48 + st["extendInstanceVisits"] * 56
+                 + st["extensionRays"] * (32 + 20))
+    achieved_gbs = alg_bytes / (st["extendMs"] * 1e-3) / 1e9
     peaks, peak_kind = measured_peaks()
     l2 = bindings.c_float(0.0)
     dll.core.mufflon_measure_l2_bandwidth(32 << 20, 100, bindings.byref(l2))
@@ -295,9 +315,14 @@ def run_b200(args):
                 "peak_source": f"{peak_kind} HBM copy bandwidth",
                 "l2_read_peak_gbs": round(float(l2.value), 1),
                 "frac_of_l2": round(achieved_gbs / max(float(l2.value), 1e-9), 4),
-                "bytes_per_ray": round(alg_bytes / max(rays, 1), 1),
-                "kernel": "pt_megakernel", "launches": launches,
-                "avg_launch_ms": round(kernel_ms / launches, 3)}
+                "bytes_per_ray": round(alg_bytes / max(st["extensionRays"], 1), 1),
+                "kernel": "k_extend", "launches": extend_launches,
+                "avg_launch_ms": round(st["extendMs"] / extend_launches, 4)}
+    stage_ms = {k[:-2]: round(v, 3) for k, v in st.items() if k.endswith("Ms")}
+    per_ray = {"extend_nodes": round(st["extendNodeVisits"] / max(st["extensionRays"], 1), 2),
+               "extend_prims": round(st["extendPrimTests"] / max(st["extensionRays"], 1), 2),
+               "shadow_nodes": round(st["shadowNodeVisits"] / max(st["shadowRays"], 1), 2),
+               "shadow_prims": round(st["shadowPrimTests"] / max(st["shadowRays"], 1), 2)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(spec, args.cpu_seconds)
@@ -315,8 +340,10 @@ def run_b200(args):
                 "e2e": {"value": round(e2e_mrays, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h),
                         "note": "scene upload + GPU LBVH build + 16 iterations + radiance readback per step (wall clock)"},
-                "gpu_launches": launches,
+                "gpu_launches": int(gpu_launches),
                 "roofline": roofline,
+                "stage_ms_per_frame": stage_ms,
+                "traversal_per_ray": per_ray,
                 "cpu_baseline": cpu,
                 "clocks": clk}
         print(json.dumps(line), flush=True)

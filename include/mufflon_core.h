@@ -257,6 +257,20 @@ typedef struct {
 } MufflonRenderStats;
 CORE_API Boolean CDECL mufflon_get_render_stats(MufflonInstanceHdl instHdl, MufflonRenderStats* stats);
 
+/* Per-stage view of the last render_iterate. With the wavefront schedule the
+ * traversal counters are split into extension rays (closest hit) and shadow
+ * rays (any hit); with the megakernel all of them are in the extension
+ * fields. The stage times are filled only while the integer renderer
+ * parameter "Stage timing" is non-zero (events around every stage launch). */
+typedef struct {
+	uint64_t extensionRays, extendNodeVisits, extendPrimTests, extendInstanceVisits;
+	uint64_t shadowRays, shadowNodeVisits, shadowPrimTests, shadowInstanceVisits;
+	float cameraMs, extendMs, shadowMs, shadeMs, finalizeMs;
+	uint32_t launches;  /* kernel launches of the iteration */
+	uint32_t wavefront; /* 1: wavefront stages, 0: megakernel */
+} MufflonStageStats;
+CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
+
 /* Closest hits of n rays (6 floats: origin, direction) against the loaded
  * scene, with the path tracer's epsilon offset along geoNormals (may be NULL). */
 CORE_API Boolean CDECL mufflon_trace_rays(MufflonInstanceHdl instHdl, const float* rays, const float* geoNormals,
@@ -274,14 +288,16 @@ CORE_API Boolean CDECL mufflon_get_bvh(MufflonInstanceHdl instHdl, int32_t which
 /* Standalone LBVH build of one LoD from host arrays (no instance needed).
  * Outputs: sorted Morton codes (numPrims), Karras parents (2*numPrims-1),
  * nodes (2*(numPrims-1) capacity), primIds (numPrims), the internal-node
- * count after collapse, and per-stage device times in ms (8 floats: morton,
- * sort, emit, merge, mark, scan, compact, soup; may be NULL). */
+ * count after collapse, and per-stage device times in ms (9 floats: morton,
+ * sort, emit, merge, mark, scan, compact, soup, and the conversion into the
+ * compressed 8-wide traversal hierarchy; may be NULL). */
 CORE_API Boolean CDECL mufflon_lbvh_build(const float* vertices, uint32_t numVertices, const uint32_t* indices,
                                           uint32_t numTriangles, uint32_t numQuads, const float* spheres,
                                           uint32_t numSpheres, uint64_t* mortonSorted, int32_t* parents,
                                           void* nodes, int32_t* primIds, int32_t* numInternal, float* stageMs);
 /* Same build on device-resident inputs; outputs stay on the device. Times
- * the whole build with CUDA events (ms). Returns the node count after collapse. */
+ * the whole build with CUDA events (ms), 8-wide conversion included. Returns
+ * the node count after collapse; stageMs as above (9 floats). */
 CORE_API Boolean CDECL mufflon_lbvh_build_device(const float* dVertices, const uint32_t* dIndices, uint32_t numTriangles,
                                                  uint32_t numQuads, const float* dSpheres, uint32_t numSpheres,
                                                  const float* aabb6, int32_t* numInternal, float* buildMs,

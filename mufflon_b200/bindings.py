@@ -168,6 +168,14 @@ class MufflonRenderStats(Structure):
                 ("instanceVisits", c_uint64), ("errors", c_uint32), ("kernelMs", c_float)]
 
 
+class MufflonStageStats(Structure):
+    _fields_ = [("extensionRays", c_uint64), ("extendNodeVisits", c_uint64), ("extendPrimTests", c_uint64),
+                ("extendInstanceVisits", c_uint64), ("shadowRays", c_uint64), ("shadowNodeVisits", c_uint64),
+                ("shadowPrimTests", c_uint64), ("shadowInstanceVisits", c_uint64), ("cameraMs", c_float),
+                ("extendMs", c_float), ("shadowMs", c_float), ("shadeMs", c_float), ("finalizeMs", c_float),
+                ("launches", c_uint32), ("wavefront", c_uint32)]
+
+
 def _bulk(a: np.ndarray) -> BulkLoader:
     b = BulkLoader()
     b.type = 1  # BULK_ARRAY
@@ -259,6 +267,7 @@ class DllHolder:
             "renderer_set_parameter_bool": (c_uint32, [c_void_p, c_char_p, c_uint32]),
             "renderer_set_parameter_enum": (c_uint32, [c_void_p, c_char_p, c_int32]),
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
+            "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
             "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
                                               c_void_p, c_void_p]),
             "mufflon_trace_occlusion": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
@@ -420,6 +429,11 @@ class DllInterface:
         self._check(self.core.mufflon_get_render_stats(self.muffInst, byref(s)), "mufflon_get_render_stats")
         return {k: getattr(s, k) for k, _ in MufflonRenderStats._fields_}
 
+    def stage_stats(self):
+        s = MufflonStageStats()
+        self._check(self.core.mufflon_get_stage_stats(self.muffInst, byref(s)), "mufflon_get_stage_stats")
+        return {k: getattr(s, k) for k, _ in MufflonStageStats._fields_}
+
     def trace_rays(self, rays, tmax=1048576.0, geo_normals=None):
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
@@ -461,7 +475,7 @@ def lbvh_build(dll: DllInterface, lod):
     nodes = np.zeros((max(2 * (n - 1), 1), 8), np.float32)
     prim = np.zeros(max(n, 1), np.int32)
     ni = c_int32(0)
-    ms = np.zeros(8, np.float32)
+    ms = np.zeros(9, np.float32)
     ok = dll.core.mufflon_lbvh_build(_ptr(v), len(v), _ptr(idx), len(lod.triangles), len(lod.quads), _ptr(s), len(s),
                                      _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim), byref(ni), _ptr(ms))
     dll._check(ok, "mufflon_lbvh_build")

@@ -25,11 +25,11 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
-CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu"]
+CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/wide.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu"]
 CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
 HEADERS = ["common/fmath.hpp", "trace/dmath.cuh", "trace/intersect.cuh", "trace/shading.cuh",
            "trace/scene_types.hpp", "trace/pt_api.hpp", "lbvh/lbvh.hpp", "lbvh/radix_sort.cuh",
-           "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "core/world.hpp"]
+           "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "trace/wide_traverse.cuh", "lbvh/wide.hpp", "core/world.hpp"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-Xptxas", "-v",

@@ -8,6 +8,7 @@
 #include "../trace/pt_api.hpp"
 #include "../lbvh/sort_noalloc.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstring>
@@ -53,6 +54,7 @@ const ParamDesc PT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
+	{ "Stage timing", PARAM_INT },
 };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
@@ -66,6 +68,7 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "RR start depth")) return &r.params.rrStartDepth;
 	if(!std::strcmp(name, "Blocks per SM")) return &r.blocksPerSm;
 	if(!std::strcmp(name, "Megakernel")) return &r.megakernel;
+	if(!std::strcmp(name, "Stage timing")) return &r.stageTiming;
 	return nullptr;
 }
 
@@ -87,7 +90,7 @@ void ensure_render_buffers(MufflonInstance& I) {
 	CHECK_CUDA(cudaMalloc(&r.radiance, n * 3 * sizeof(float)));
 	CHECK_CUDA(cudaMalloc(&r.hitId, n * 2 * sizeof(float)));
 	CHECK_CUDA(cudaMalloc(&r.workCounter, sizeof(unsigned int)));
-	CHECK_CUDA(cudaMalloc(&r.counters, sizeof(TraceCounters)));
+	CHECK_CUDA(cudaMalloc(&r.counters, 2 * sizeof(TraceCounters)));
 	CHECK_CUDA(cudaEventCreate(&r.evStart));
 	CHECK_CUDA(cudaEventCreate(&r.evStop));
 	r.needsReset = true;
@@ -145,6 +148,8 @@ void RendererState::release() {
 	if(wfMemory) cudaFree(wfMemory);
 	wfMemory = nullptr;
 	wf = WfState{};
+	for(cudaEvent_t e : stageEvents) cudaEventDestroy(e);
+	stageEvents.clear();
 	cudaFree(rng); cudaFree(radiance); cudaFree(hitId); cudaFree(workCounter); cudaFree(counters);
 	if(evStart) cudaEventDestroy(evStart);
 	if(evStop) cudaEventDestroy(evStop);
@@ -823,15 +828,44 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	rs.hitId = r.targetHitId ? r.hitId : nullptr;
 	rs.width = r.width; rs.height = r.height;
 	rs.iteration = r.iteration;
-	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, sizeof(TraceCounters), I.stream));
-	if(!r.megakernel) ensure_wavefront_buffers(I);
+	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
+	WfLaunchInfo info;
+	if(!r.megakernel) {
+		ensure_wavefront_buffers(I);
+		if(r.stageTiming) {
+			const int pairs = 3 * std::max(1, r.params.maxPathLength) + 2;
+			while(int(r.stageEvents.size()) < 2 * pairs) {
+				cudaEvent_t e;
+				CHECK_CUDA(cudaEventCreate(&e));
+				r.stageEvents.push_back(e);
+			}
+			r.stageKinds.resize(pairs);
+			info.events = r.stageEvents.data();
+			info.kinds = r.stageKinds.data();
+			info.eventPairs = pairs;
+		}
+	}
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
 	if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
-	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream));
+	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
-	CHECK_CUDA(cudaMemcpyAsync(&r.lastCounters, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
+	TraceCounters both[2];
+	CHECK_CUDA(cudaMemcpyAsync(both, r.counters, 2 * sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	CHECK_CUDA(cudaEventElapsedTime(&r.lastKernelMs, r.evStart, r.evStop));
+	r.lastExtend = both[0];
+	r.lastShadow = both[1];
+	r.lastCounters = both[0];
+	r.lastCounters.rays += both[1].rays; r.lastCounters.shadowRays += both[1].shadowRays;
+	r.lastCounters.nodeVisits += both[1].nodeVisits; r.lastCounters.primTests += both[1].primTests;
+	r.lastCounters.instanceVisits += both[1].instanceVisits; r.lastCounters.errors += both[1].errors;
+	r.lastLaunches = r.megakernel ? 1 : info.launches;
+	for(float& m : r.stageMs) m = 0.0f;
+	for(int i = 0; i < info.pairsUsed; ++i) {
+		float ms = 0.0f;
+		CHECK_CUDA(cudaEventElapsedTime(&ms, info.events[2 * i], info.events[2 * i + 1]));
+		r.stageMs[info.kinds[i]] += ms;
+	}
 	auto t2 = clk::now();
 	auto us = [](clk::duration d) { return uint64_t(std::chrono::duration_cast<std::chrono::microseconds>(d).count()); };
 	if(preTime) { preTime->cycles = 0; preTime->microseconds = us(t1 - t0); }
@@ -985,6 +1019,24 @@ Boolean mufflon_get_render_stats(MufflonInstanceHdl h, MufflonRenderStats* s) {
 	CATCH_ALL(false)
 }
 
+Boolean mufflon_get_stage_stats(MufflonInstanceHdl h, MufflonStageStats* s) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(s, "stats pointer is null");
+	const RendererState& r = I.renderer;
+	const TraceCounters &e = r.lastExtend, &sh = r.lastShadow;
+	s->extensionRays = e.rays; s->extendNodeVisits = e.nodeVisits; s->extendPrimTests = e.primTests;
+	s->extendInstanceVisits = e.instanceVisits;
+	s->shadowRays = sh.rays; s->shadowNodeVisits = sh.nodeVisits; s->shadowPrimTests = sh.primTests;
+	s->shadowInstanceVisits = sh.instanceVisits;
+	s->cameraMs = r.stageMs[WF_CAMERA]; s->extendMs = r.stageMs[WF_EXTEND]; s->shadowMs = r.stageMs[WF_SHADOW];
+	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE];
+	s->launches = uint32_t(r.lastLaunches);
+	s->wavefront = r.megakernel ? 0u : 1u;
+	return true;
+	CATCH_ALL(false)
+}
+
 Boolean mufflon_trace_rays(MufflonInstanceHdl h, const float* rays, const float* geo, float tmax, uint32_t n,
                            float* t, int32_t* inst, int32_t* prim, float* sp) {
 	TRY
@@ -1003,7 +1055,8 @@ Boolean mufflon_trace_rays(MufflonInstanceHdl h, const float* rays, const float*
 	if(geo) CHECK_CUDA(cudaMalloc(&dg, size_t(n) * 12));
 	CHECK_CUDA(cudaMemcpyAsync(dr, rays, size_t(n) * 24, cudaMemcpyHostToDevice, I.stream));
 	if(geo) CHECK_CUDA(cudaMemcpyAsync(dg, geo, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
-	CHECK_CUDA(launch_trace_rays(I.scene.desc, dr, dg, tmax, n, dt, di, dp, dsp, I.stream));
+	if(I.renderer.megakernel) CHECK_CUDA(launch_trace_rays(I.scene.desc, dr, dg, tmax, n, dt, di, dp, dsp, I.stream));
+	else CHECK_CUDA(launch_trace_rays_wide(I.scene.desc, dr, dg, tmax, n, dt, di, dp, dsp, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(t, dt, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(inst, di, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(prim, dp, size_t(n) * 4, cudaMemcpyDeviceToHost, I.stream));
@@ -1028,7 +1081,8 @@ Boolean mufflon_trace_occlusion(MufflonInstanceHdl h, const float* a, const floa
 	CHECK_CUDA(cudaMalloc(&dout, n));
 	CHECK_CUDA(cudaMemcpyAsync(da, a, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(db, b, size_t(n) * 12, cudaMemcpyHostToDevice, I.stream));
-	CHECK_CUDA(launch_occlusion(I.scene.desc, da, db, n, dout, I.stream));
+	if(I.renderer.megakernel) CHECK_CUDA(launch_occlusion(I.scene.desc, da, db, n, dout, I.stream));
+	else CHECK_CUDA(launch_occlusion_wide(I.scene.desc, da, db, n, dout, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(occ, dout, n, cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	cudaFree(da); cudaFree(db); cudaFree(dout);
@@ -1090,7 +1144,7 @@ Boolean mufflon_lbvh_build(const float* vertices, uint32_t numVertices, const ui
 		if(nodes && out.numInternal > 0) cudaMemcpy(nodes, out.nodes, sizeof(BvhNode) * 2 * size_t(out.numInternal), cudaMemcpyDeviceToHost);
 		if(primIds && n > 0) cudaMemcpy(primIds, out.primIds, sizeof(int32_t) * n, cudaMemcpyDeviceToHost);
 		if(numInternal) *numInternal = out.numInternal;
-		if(stageMs) { const StageTimes t = builder.last_times(); const float v[8] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup }; std::memcpy(stageMs, v, sizeof(v)); }
+		if(stageMs) { const StageTimes t = builder.last_times(); const float v[9] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup, t.wide }; std::memcpy(stageMs, v, sizeof(v)); }
 	}
 	out.release();
 	cudaStreamDestroy(s);
@@ -1124,7 +1178,7 @@ Boolean mufflon_lbvh_build_device(const float* dVertices, const uint32_t* dIndic
 	cudaEventDestroy(a); cudaEventDestroy(b);
 	if(buildMs) *buildMs = ms;
 	if(numInternal) *numInternal = out->numInternal;
-	if(stageMs) { const StageTimes t = builder->last_times(); const float v[8] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup }; std::memcpy(stageMs, v, sizeof(v)); }
+	if(stageMs) { const StageTimes t = builder->last_times(); const float v[9] = { t.morton, t.sort, t.emit, t.merge, t.mark, t.scan, t.compact, t.soup, t.wide }; std::memcpy(stageMs, v, sizeof(v)); }
 	return true;
 	CATCH_ALL(false)
 }

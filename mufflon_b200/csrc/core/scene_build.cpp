@@ -361,6 +361,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		d.numPrims = int32_t(h.num_prims());
 		d.numInternal = g.bvh.numInternal;
 		d.nodes = g.bvh.nodes; d.primIds = g.bvh.primIds; d.triSoup = g.bvh.triSoup;
+		d.wnodes = g.bvh.wnodes; d.wprims = g.bvh.wprims; d.wsoup = g.bvh.wsoup; d.numWide = g.bvh.numWide;
 		d.vertices = g.vertices; d.normals = g.normals; d.uvs = g.uvs; d.indices = g.indices;
 		d.faceMaterials = g.faceMat; d.spheres = g.spheres; d.sphereMaterials = g.sphereMat;
 		std::memcpy(d.aabbMin, in.aabbMin, sizeof(d.aabbMin));
@@ -516,6 +517,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	S.worldToInstance = D.dW2I; S.instanceLod = D.dInstLod; S.numInstances = numInst;
 	S.activeInstances = active; S.validInstance = valid;
 	S.tlasNodes = D.tlas.nodes; S.tlasPrimIds = D.tlas.primIds; S.tlasNumInternal = D.tlas.numInternal;
+	S.tlasWide = D.tlas.wnodes; S.tlasWidePrims = D.tlas.wprims; S.tlasNumWide = D.tlas.numWide;
 	S.materials = D.dMaterials; S.textures = D.dTextures;
 	S.lights = D.dLights; S.lightNodes = D.dLightNodes; S.lightPrimKeys = D.dLightKeys; S.lightPrimCodes = D.dLightCodes;
 	S.numLightPrims = uint32_t(keys.size());

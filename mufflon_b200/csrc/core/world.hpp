@@ -136,6 +136,12 @@ struct RendererState {
 	void* wfMemory = nullptr;
 	int32_t wfNee = 0;
 	size_t wfPixels = 0;
+	int32_t stageTiming = 0;      // record device time per stage kernel
+	std::vector<cudaEvent_t> stageEvents;
+	std::vector<unsigned char> stageKinds;
+	float stageMs[WF_STAGES] = {};
+	int32_t lastLaunches = 0;
+	TraceCounters lastExtend{}, lastShadow{};
 	bool targetRadiance = true;
 	bool targetHitId = false;
 	bool needsReset = true;
@@ -145,7 +151,7 @@ struct RendererState {
 	float* radiance = nullptr;
 	float* hitId = nullptr;
 	unsigned int* workCounter = nullptr;
-	TraceCounters* counters = nullptr;
+	TraceCounters* counters = nullptr; // [0] extension rays, [1] shadow rays
 	cudaEvent_t evStart = nullptr, evStop = nullptr;
 	TraceCounters lastCounters{};
 	float lastKernelMs = 0.0f;

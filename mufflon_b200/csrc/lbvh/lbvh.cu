@@ -14,6 +14,7 @@
 #include "lbvh.hpp"
 #include "../trace/dmath.cuh"
 #include "radix_sort.cuh"
+#include "wide.hpp"
 
 #include <algorithm>
 #include <cfloat>
@@ -144,7 +145,8 @@ MBD int lcp(const u64* keys, int n, int i1, int i2, u64 key1) {
 }
 
 // build_lbvh.cu:180-245 (plus explicit child links and mark initialisation)
-__global__ void k_karras(int n, const u64* __restrict__ keys, int32_t* parents, int32_t* children, int32_t* marks) {
+__global__ void k_karras(int n, const u64* __restrict__ keys, int32_t* parents, int32_t* children, int32_t* marks,
+                         int2* ranges) {
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if(idx >= n - 1) return;
 	const u64 key1 = keys[idx];
@@ -176,6 +178,7 @@ __global__ void k_karras(int n, const u64* __restrict__ keys, int32_t* parents, 
 	children[2 * idx] = leftIndex;
 	children[2 * idx + 1] = rightIndex;
 	marks[idx] = 1;
+	ranges[idx] = make_int2(min(idx, j), max(idx, j));
 }
 
 // ---------------------------------------------------------------- merge
@@ -379,6 +382,26 @@ __global__ void k_soup(LodBuildInput in, int n, const int32_t* __restrict__ prim
 	}
 }
 
+// Soup of the wide hierarchy's primitive order: slot k holds primitive
+// wprims[k]; for triangles the three vertices, and the primitive id in the
+// w component of the first float4 for every primitive type.
+__global__ void k_wsoup(LodBuildInput in, int n, const int32_t* __restrict__ wprims, float4* soup) {
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if(k >= n) return;
+	const int p = wprims[k];
+	float4 a = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(p)), b = make_float4(0, 0, 0, 0), c = b;
+	if(p < int(in.numTriangles)) {
+		const uint32_t t = uint32_t(p) * 3;
+		const f3 v0 = v3(in.vertices, in.indices[t]), v1 = v3(in.vertices, in.indices[t + 1]), v2 = v3(in.vertices, in.indices[t + 2]);
+		a = make_float4(v0.x, v0.y, v0.z, __int_as_float(p));
+		b = make_float4(v1.x, v1.y, v1.z, 0.0f);
+		c = make_float4(v2.x, v2.y, v2.z, 0.0f);
+	}
+	soup[3 * size_t(k)] = a;
+	soup[3 * size_t(k) + 1] = b;
+	soup[3 * size_t(k) + 2] = c;
+}
+
 inline unsigned blocks_for(size_t n, unsigned threads) { return unsigned((n + threads - 1) / threads); }
 
 template < class T >
@@ -394,8 +417,14 @@ void BvhBuffers::release() {
 	if(nodes) cudaFree(nodes);
 	if(primIds) cudaFree(primIds);
 	if(triSoup) cudaFree(triSoup);
+	if(wnodes) cudaFree(wnodes);
+	if(wprims) cudaFree(wprims);
+	if(wsoup) cudaFree(wsoup);
 	nodes = nullptr; primIds = nullptr; triSoup = nullptr;
+	wnodes = nullptr; wprims = nullptr; wsoup = nullptr;
 	nodeCapacity = primCapacity = soupCapacity = 0;
+	wideCapacity = wprimCapacity = wsoupCapacity = 0;
+	numWide = 0;
 }
 
 LbvhBuilder::~LbvhBuilder() {
@@ -403,6 +432,7 @@ LbvhBuilder::~LbvhBuilder() {
 	cudaFree(m_parents); cudaFree(m_children); cudaFree(m_nodeData); cudaFree(m_flags);
 	cudaFree(m_marks); cudaFree(m_blockSums); cudaFree(m_hist); cudaFree(m_status);
 	cudaFree(m_tileCounter); cudaFree(m_error);
+	cudaFree(m_ranges); cudaFree(m_wideCounters); cudaFree(m_wideQueueA); cudaFree(m_wideQueueB);
 	if(m_hostCount) cudaFreeHost(m_hostCount);
 	for(auto& e : m_ev) if(e) cudaEventDestroy(e);
 }
@@ -413,6 +443,7 @@ cudaError_t LbvhBuilder::reserve(uint32_t n) {
 		if((e = cudaMalloc(&m_hist, 8 * 256 * sizeof(uint32_t))) != cudaSuccess) return e;
 		if((e = cudaMalloc(&m_tileCounter, 8 * sizeof(unsigned int))) != cudaSuccess) return e;
 		if((e = cudaMalloc(&m_error, sizeof(unsigned int))) != cudaSuccess) return e;
+		if((e = cudaMalloc(&m_wideCounters, WIDE_COUNTERS * sizeof(uint32_t))) != cudaSuccess) return e;
 		if((e = cudaMallocHost(&m_hostCount, sizeof(int32_t))) != cudaSuccess) return e;
 		if((e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SORT_SMEM))) != cudaSuccess) return e;
 		for(auto& ev : m_ev) if((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
@@ -428,6 +459,10 @@ cudaError_t LbvhBuilder::reserve(uint32_t n) {
 	if((e = grow(m_nodeData, 4 * N)) != cudaSuccess) return e;
 	if((e = grow(m_flags, N)) != cudaSuccess) return e;
 	if((e = grow(m_marks, N)) != cudaSuccess) return e;
+	if((e = grow(m_ranges, N)) != cudaSuccess) return e;
+	m_wideQueueCapacity = uint32_t(wide_node_capacity(N, 1));
+	if((e = grow(m_wideQueueA, size_t(m_wideQueueCapacity))) != cudaSuccess) return e;
+	if((e = grow(m_wideQueueB, size_t(m_wideQueueCapacity))) != cudaSuccess) return e;
 	if((e = grow(m_blockSums, N / SCAN_TILE + 2)) != cudaSuccess) return e;
 	const uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
 	if((e = grow(m_status, size_t(tiles) * 256)) != cudaSuccess) return e;
@@ -487,11 +522,36 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 		out.soupCapacity = 3 * size_t(numPrimitives);
 	}
 	if((e = reserve(numPrimitives)) != cudaSuccess) return e;
+	const bool wide = withSoup || mode == MODE_SCENE;
+	if(wide) {
+		const size_t wcap = wide_node_capacity(std::max<uint32_t>(used, 2u), mode == MODE_SCENE ? WIDE_TLAS_LEAF_MAX : WIDE_LEAF_MAX);
+		if(out.wideCapacity < wcap) {
+			if(out.wnodes) cudaFree(out.wnodes);
+			out.wnodes = nullptr;
+			if((e = cudaMalloc(&out.wnodes, sizeof(WideNode) * wcap)) != cudaSuccess) return e;
+			out.wideCapacity = wcap;
+		}
+		if(out.wprimCapacity < numPrimitives) {
+			if(out.wprims) cudaFree(out.wprims);
+			out.wprims = nullptr;
+			if((e = cudaMalloc(&out.wprims, sizeof(int32_t) * numPrimitives)) != cudaSuccess) return e;
+			out.wprimCapacity = numPrimitives;
+		}
+		if(mode == MODE_LOD && out.wsoupCapacity < 3 * size_t(numPrimitives)) {
+			if(out.wsoup) cudaFree(out.wsoup);
+			out.wsoup = nullptr;
+			if((e = cudaMalloc(&out.wsoup, sizeof(float4) * 3 * size_t(numPrimitives))) != cudaSuccess) return e;
+			out.wsoupCapacity = 3 * size_t(numPrimitives);
+		}
+	}
+	out.numWide = 0;
 	if(used <= 1) {
 		// build_lbvh.cu:595-602: one primitive needs no hierarchy
 		cudaMemsetAsync(out.primIds, 0, sizeof(int32_t), stream);
 		out.numInternal = 0;
 		if(mode == MODE_LOD && withSoup) k_soup<<<1, 32, 0, stream>>>(*lod, 1, out.primIds, out.triSoup);
+		if(wide) cudaMemsetAsync(out.wprims, 0, sizeof(int32_t), stream);
+		if(mode == MODE_LOD && wide) k_wsoup<<<1, 32, 0, stream>>>(*lod, 1, out.wprims, out.wsoup);
 		return cudaGetLastError();
 	}
 	const int n = int(used);
@@ -504,7 +564,7 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	if((e = sort_pairs(m_keysA, m_valsA, numPrimitives, stream)) != cudaSuccess) return e;
 	if(m_timing) cudaEventRecord(m_ev[2], stream);
 	cudaMemsetAsync(m_parents, 0, sizeof(int32_t) * numNodes, stream);
-	k_karras<<<blocks_for(numInternal, 256), 256, 0, stream>>>(n, m_keysA, m_parents, m_children, m_marks);
+	k_karras<<<blocks_for(numInternal, 256), 256, 0, stream>>>(n, m_keysA, m_parents, m_children, m_marks, m_ranges);
 	if(m_timing) cudaEventRecord(m_ev[3], stream);
 	cudaMemsetAsync(m_flags, 0, sizeof(unsigned int) * numInternal, stream);
 	const LodBuildInput lodIn = lod ? *lod : LodBuildInput{};
@@ -528,6 +588,28 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	if(mode == MODE_LOD && withSoup)
 		k_soup<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*lod, int(numPrimitives), out.primIds, out.triSoup);
 	if(m_timing) cudaEventRecord(m_ev[8], stream);
+	if(wide) {
+		WideBuildArgs wa{};
+		wa.n = n;
+		wa.numInternal = numInternal;
+		wa.leafMax = mode == MODE_SCENE ? WIDE_TLAS_LEAF_MAX : WIDE_LEAF_MAX;
+		wa.children = m_children;
+		wa.ranges = m_ranges;
+		wa.nodeData = m_nodeData;
+		wa.sortedIds = m_valsA;
+		wa.nodes = out.wnodes;
+		wa.prims = out.wprims;
+		wa.nodeCapacity = uint32_t(std::min<size_t>(out.wideCapacity, m_wideQueueCapacity));
+		wa.counters = m_wideCounters;
+		wa.queueA = m_wideQueueA;
+		wa.queueB = m_wideQueueB;
+		int32_t numWide = 0;
+		if((e = build_wide(wa, &numWide, stream)) != cudaSuccess) return e;
+		out.numWide = numWide;
+		if(mode == MODE_LOD)
+			k_wsoup<<<blocks_for(n, 256), 256, 0, stream>>>(*lod, n, out.wprims, out.wsoup);
+	}
+	if(m_timing) cudaEventRecord(m_ev[9], stream);
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	if((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
 	unsigned int err = 0;
@@ -535,9 +617,9 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	if(err) return cudaErrorLaunchTimeout;
 	out.numInternal = *m_hostCount;
 	if(m_timing) {
-		float t[8];
-		for(int k = 0; k < 8; ++k) cudaEventElapsedTime(&t[k], m_ev[k], m_ev[k + 1]);
-		m_times = { t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7] };
+		float t[9];
+		for(int k = 0; k < 9; ++k) cudaEventElapsedTime(&t[k], m_ev[k], m_ev[k + 1]);
+		m_times = { t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8] };
 	}
 	return cudaSuccess;
 }

@@ -11,13 +11,16 @@
 //   4. bottom-up AABB / SAH / primitive-count merge with atomic arrival flags,
 //   5. SAH collapse marks, inclusive scan, compaction into the reference's
 //      32-byte BvhNode pair layout (lbvh.hpp:14-44),
-//   6. for LoDs: a leaf-ordered triangle soup (3 x float4 per leaf slot).
+//   6. for LoDs: a leaf-ordered triangle soup (3 x float4 per leaf slot),
+//   7. conversion of the binary hierarchy into the compressed 8-wide one used
+//      for traversal (wide.hpp), with its own primitive order and soup.
 // All temporary storage is owned by the builder and reused across builds.
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "../trace/scene_types.hpp"
+#include "wide.hpp"
 
 namespace mb {
 
@@ -47,10 +50,18 @@ struct BvhBuffers {
 	size_t nodeCapacity = 0;
 	size_t primCapacity = 0;
 	size_t soupCapacity = 0;
+	// compressed 8-wide hierarchy used for traversal (wide.hpp)
+	WideNode* wnodes = nullptr;    // device, numWide nodes
+	int32_t* wprims = nullptr;     // device, n: wide leaf slot -> primitive id
+	float4* wsoup = nullptr;       // device, 3 * n (LoDs only)
+	int32_t numWide = 0;
+	size_t wideCapacity = 0;
+	size_t wprimCapacity = 0;
+	size_t wsoupCapacity = 0;
 	void release();
 };
 
-struct StageTimes { float morton, sort, emit, merge, mark, scan, compact, soup; };
+struct StageTimes { float morton, sort, emit, merge, mark, scan, compact, soup, wide; };
 
 class LbvhBuilder {
 public:
@@ -95,6 +106,11 @@ private:
 	float4* m_nodeData = nullptr;     // 2 (2n - 1)
 	unsigned int* m_flags = nullptr;  // n - 1
 	int32_t* m_marks = nullptr;       // n - 1 (scanned in place)
+	int2* m_ranges = nullptr;         // n - 1: sorted leaf range per internal node
+	uint32_t* m_wideCounters = nullptr;
+	int2* m_wideQueueA = nullptr;
+	int2* m_wideQueueB = nullptr;
+	uint32_t m_wideQueueCapacity = 0;
 	int32_t* m_blockSums = nullptr;
 	uint32_t* m_hist = nullptr;       // 8 * 256
 	uint32_t* m_status = nullptr;     // tiles * 256
@@ -105,7 +121,7 @@ private:
 	int32_t m_lastN = 0;
 	bool m_timing = false;
 	StageTimes m_times{};
-	cudaEvent_t m_ev[9] = {};
+	cudaEvent_t m_ev[10] = {};
 };
 
 } // namespace mb

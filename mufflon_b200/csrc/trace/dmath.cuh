@@ -25,7 +25,8 @@ constexpr float SCENE_SCALE_EPS = 1e-4f;
 constexpr float INF_PDF = 4294967296.0f;
 // Box culling uses tmax * (1 + 2^-16) so that it never culls a primitive the
 // exact (t, instance, primitive) ordering would accept.
-constexpr float BOX_SLACK = 1.0f + 1.0f / 65536.0f;
+constexpr float BOX_SLACK = 1.0f + 1.0f / 4096.0f;      // tmax culling slack
+constexpr float BOX_FAR_SLACK = 1.0f + 1.0f / 1048576.0f; // slab interval tolerance
 constexpr float DISTANCESQ_EPSILON = 1e-10f;
 
 #define MBD __device__ __forceinline__

@@ -23,7 +23,7 @@ constexpr int TLAS_STACK = 64;
 constexpr int MAX_TRAVERSAL_STEPS = 1 << 22;
 
 struct FastRay {
-	f3 o, d, inv, oDiv;
+	f3 o, d, inv;
 	int kx, ky, kz;
 	float Sx, Sy, Sz;
 };
@@ -33,7 +33,6 @@ MBD FastRay make_ray(f3 o, f3 d) {
 	r.o = o;
 	r.d = d;
 	r.inv = make3(__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z));
-	r.oDiv = o * r.inv;
 	const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
 	int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
 	int kx = kz + 1 == 3 ? 0 : kz + 1;
@@ -46,18 +45,24 @@ MBD FastRay make_ray(f3 o, f3 d) {
 	return r;
 }
 
-// Slab test, GPU form of intersection.cu:47-55 (cmin clamped at 0).
+// Slab test of intersection.cu:47-55 in a robust form: per axis
+// t = (bound - origin) * invDir, which has a relative error of a few ulp and
+// the exact sign (the reference's fma(bound, invDir, -origin * invDir) errs
+// relative to the origin's magnitude); the entry is clamped at 0 and the
+// interval is accepted up to far * (1 + 2^-20). A box that contains a
+// primitive's hit point is therefore never culled, and every hierarchy over
+// the same primitives yields the same closest hit.
 MBD bool box_test(float mnx, float mny, float mnz, float mxx, float mxy, float mxz,
                   const FastRay& r, float tmax, float& cmin) {
-	const float lox = __fmaf_rn(mnx, r.inv.x, -r.oDiv.x);
-	const float loy = __fmaf_rn(mny, r.inv.y, -r.oDiv.y);
-	const float loz = __fmaf_rn(mnz, r.inv.z, -r.oDiv.z);
-	const float hix = __fmaf_rn(mxx, r.inv.x, -r.oDiv.x);
-	const float hiy = __fmaf_rn(mxy, r.inv.y, -r.oDiv.y);
-	const float hiz = __fmaf_rn(mxz, r.inv.z, -r.oDiv.z);
+	const float lox = __fmul_rn(__fsub_rn(mnx, r.o.x), r.inv.x);
+	const float loy = __fmul_rn(__fsub_rn(mny, r.o.y), r.inv.y);
+	const float loz = __fmul_rn(__fsub_rn(mnz, r.o.z), r.inv.z);
+	const float hix = __fmul_rn(__fsub_rn(mxx, r.o.x), r.inv.x);
+	const float hiy = __fmul_rn(__fsub_rn(mxy, r.o.y), r.inv.y);
+	const float hiz = __fmul_rn(__fsub_rn(mxz, r.o.z), r.inv.z);
 	cmin = fmax_(fmax_(fmin_(lox, hix), fmin_(loy, hiy)), fmax_(fmin_(loz, hiz), 0.0f));
-	const float cmax = fmin_(fmin_(fmax_(lox, hix), fmax_(loy, hiy)), fmin_(fmax_(loz, hiz), tmax));
-	return cmin <= cmax;
+	const float cfar = fmin_(fmin_(fmax_(lox, hix), fmax_(loy, hiy)), fmax_(loz, hiz));
+	return cmin <= tmax && cmin <= cfar * BOX_FAR_SLACK;
 }
 
 // Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013).

@@ -12,6 +12,8 @@
 
 namespace mb {
 
+struct WideNode; // lbvh/wide.hpp
+
 enum : int32_t { MAT_LAMBERT = 0, MAT_TORRANCE = 1, MAT_EMISSIVE = 2 };
 enum : uint16_t { LT_POINT = 0, LT_QUAD = 3, LT_INTERNAL = 0xFFFF };
 
@@ -40,6 +42,11 @@ struct DLod {
 	const float4* spheres;        // center, radius
 	const uint16_t* sphereMaterials;
 	float aabbMin[3], aabbMax[3];
+	// compressed 8-wide hierarchy used for traversal (lbvh/wide.hpp)
+	const WideNode* wnodes;
+	const int32_t* wprims;        // wide leaf slot -> primitive id
+	const float4* wsoup;          // 3 float4 per wide leaf slot, primitive id in the first .w
+	int32_t numWide;
 };
 
 struct DMaterial {
@@ -89,6 +96,9 @@ struct DScene {
 	const BvhNode* tlasNodes;
 	const int32_t* tlasPrimIds;
 	int32_t tlasNumInternal;
+	const WideNode* tlasWide;
+	const int32_t* tlasWidePrims; // wide leaf slot -> instance id
+	int32_t tlasNumWide;
 	const DMaterial* materials;
 	const DTexture* textures;
 	// light tree (src/core/scene/lights/light_tree.hpp)

@@ -20,8 +20,10 @@
 // shade k+1, so a next-event contribution is added between the emission terms
 // that surround it, exactly as the sequential loop adds them.
 #include "shading.cuh"
+#include "wide_traverse.cuh"
 #include "wavefront.hpp"
 
+#include <algorithm>
 #include <cooperative_groups.h>
 
 namespace mb {
@@ -103,8 +105,7 @@ __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t n
 }
 
 __global__ void __launch_bounds__(128) k_extend(const DScene S, WfState W, int q, int workIdx, TraceCounters* counters) {
-	int2 bstack[BLAS_STACK];
-	int2 tstack[TLAS_STACK];
+	uint2 stack[WIDE_STACK];
 	LocalCounters cnt;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	const unsigned lane = threadIdx.x & 31u;
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(128) k_extend(const DScene S, WfState W, int q
 		const unsigned slot = base + lane;
 		if(slot < count) {
 			const float4 o = W.qOrg[q][slot], d = W.qDir[q][slot];
-			const HitRec h = closest_hit(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, cnt, bstack, tstack);
+			const HitRec h = closest_hit_wide(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, cnt, stack);
 			W.qHit[q][slot] = make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x);
 			W.qHitSpy[q][slot] = h.sp.y;
 		}
@@ -125,8 +126,7 @@ __global__ void __launch_bounds__(128) k_extend(const DScene S, WfState W, int q
 }
 
 __global__ void __launch_bounds__(128) k_shadow(const DScene S, WfState W, int neeCount, int workIdx, TraceCounters* counters) {
-	int2 bstack[BLAS_STACK];
-	int2 tstack[TLAS_STACK];
+	uint2 stack[WIDE_STACK];
 	LocalCounters cnt;
 	const unsigned groups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW) / unsigned(neeCount);
 	const unsigned lane = threadIdx.x & 31u;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128) k_shadow(const DScene S, WfState W, int n
 				const float4 o = W.sOrg[slot];
 				if(!(o.w > 0.0f)) continue; // no contribution in this slot
 				const float4 d = W.sDir[slot];
-				if(!occluded(S, f4to3(o), f4to3(d), o.w, cnt, bstack, tstack))
+				if(!occluded_wide(S, f4to3(o), f4to3(d), o.w, cnt, stack))
 					radiance = contribute(radiance, f4to3(W.sContrib[slot]));
 			}
 			W.rad[p] = pack(radiance, acc.w);
@@ -296,6 +296,39 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	}
 }
 
+// Closest hits / shadow-ray tests of caller-provided rays over the wide
+// hierarchies (the parity and measurement entry points).
+__global__ void k_trace_rays_wide(const DScene S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
+                                  float* tOut, int32_t* instOut, int32_t* primOut, float* spOut) {
+	uint2 stack[WIDE_STACK];
+	LocalCounters cnt;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		f3 o = make3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+		const f3 d = make3(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+		const f3 g = geoNormals ? make3(geoNormals[3 * i], geoNormals[3 * i + 1], geoNormals[3 * i + 2]) : make3(0, 0, 0);
+		add_epsilon(o, d, g);
+		const HitRec hr = closest_hit_wide(S, o, d, tmax, cnt, stack);
+		const Intersection h = hit_attributes(S, o, d, hr);
+		tOut[i] = h.distance; instOut[i] = h.inst; primOut[i] = h.prim;
+		if(spOut) { spOut[2 * i] = h.sp.x; spOut[2 * i + 1] = h.sp.y; }
+	}
+}
+
+__global__ void k_occlusion_wide(const DScene S, const float* a, const float* b, uint32_t n, uint8_t* out) {
+	uint2 stack[WIDE_STACK];
+	LocalCounters cnt;
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		const f3 pa = make3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+		const f3 pb = make3(b[3 * i], b[3 * i + 1], b[3 * i + 2]);
+		const f3 dv = pb - pa;
+		const f3 dir = dv / len(dv);
+		f3 so, sd;
+		float stmax;
+		shadow_ray(pa, pb, make3(0, 0, 0), make3(0, 0, 0), dir, so, sd, stmax);
+		out[i] = occluded_wide(S, so, sd, stmax, cnt, stack) ? 1 : 0;
+	}
+}
+
 int persistent_blocks(const void* fn, int threads) {
 	int dev = 0, sms = 148, perSm = 4;
 	cudaGetDevice(&dev);
@@ -306,8 +339,38 @@ int persistent_blocks(const void* fn, int threads) {
 
 } // namespace
 
+cudaError_t launch_trace_rays_wide(const DScene& S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
+                                  float* t, int32_t* inst, int32_t* prim, float* sp, cudaStream_t stream) {
+	if(n == 0) return cudaSuccess;
+	const unsigned blocks = unsigned(std::min<uint32_t>((n + 127) / 128, 148u * 16u));
+	k_trace_rays_wide<<<blocks, 128, 0, stream>>>(S, rays, geoNormals, tmax, n, t, inst, prim, sp);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_occlusion_wide(const DScene& S, const float* a, const float* b, uint32_t n, uint8_t* out,
+                                 cudaStream_t stream) {
+	if(n == 0) return cudaSuccess;
+	const unsigned blocks = unsigned(std::min<uint32_t>((n + 127) / 128, 148u * 16u));
+	k_occlusion_wide<<<blocks, 128, 0, stream>>>(S, a, b, n, out);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const RenderState& R, WfState W,
-                                TraceCounters* counters, cudaStream_t stream) {
+                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info) {
+	WfLaunchInfo none;
+	WfLaunchInfo& L = info ? *info : none;
+	L.pairsUsed = 0;
+	L.launches = 0;
+	auto begin = [&](WfStage k) {
+		++L.launches;
+		if(L.events && L.pairsUsed < L.eventPairs) {
+			L.kinds[L.pairsUsed] = (unsigned char)k;
+			cudaEventRecord(L.events[2 * L.pairsUsed], stream);
+		}
+	};
+	auto end = [&]() {
+		if(L.events && L.pairsUsed < L.eventPairs) cudaEventRecord(L.events[2 * L.pairsUsed++ + 1], stream);
+	};
 	const uint32_t n = R.width * R.height;
 	if(n == 0) return cudaSuccess;
 	static int extendBlocks = 0, shadowBlocks = 0;
@@ -323,7 +386,9 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 	if(e != cudaSuccess) return e;
 	W.rng = R.rngState;
 	const unsigned grid = (n + 127) / 128;
+	begin(WF_CAMERA);
 	k_camera<<<grid, 128, 0, stream>>>(S, P, W, n, R.width);
+	end();
 	unsigned work = 0;
 	for(int b = 0; b < maxBounces; ++b) {
 		const int q = b & 1;
@@ -331,14 +396,24 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 			cudaMemsetAsync(W.counters + C_WORK, 0, sizeof(unsigned) * workSlots, stream);
 			work = 0;
 		}
+		begin(WF_EXTEND);
 		k_extend<<<extendBlocks, 128, 0, stream>>>(S, W, q, int(work++), counters);
-		if(b > 0) k_shadow<<<shadowBlocks, 128, 0, stream>>>(S, W, neeCount, int(work++), counters);
+		end();
+		if(b > 0) {
+			begin(WF_SHADOW);
+			k_shadow<<<shadowBlocks, 128, 0, stream>>>(S, W, neeCount, int(work++), counters + 1);
+			end();
+		}
 		// the shade of this bounce appends to the other queue and to the shadow queue
 		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);
 		cudaMemsetAsync(W.counters + C_SHADOW, 0, sizeof(unsigned), stream);
+		begin(WF_SHADE);
 		k_shade<<<grid, 128, 0, stream>>>(S, P, W, q, b);
+		end();
 	}
+	begin(WF_FINALIZE);
 	k_finalize<<<grid, 128, 0, stream>>>(W, R, n);
+	end();
 	return cudaGetLastError();
 }
 

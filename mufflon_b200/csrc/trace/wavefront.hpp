@@ -28,8 +28,30 @@ struct WfState {
 // persistent launch (two per bounce); longer paths recycle the work counters.
 constexpr unsigned WF_COUNTERS = 4096;
 
+enum WfStage { WF_CAMERA = 0, WF_EXTEND = 1, WF_SHADOW = 2, WF_SHADE = 3, WF_FINALIZE = 4, WF_STAGES = 5 };
+
+// Host-side launch record of one iteration. With `events` set, a pair of
+// events is recorded around each stage launch (while capacity lasts) and
+// `kinds` receives the stage of each pair.
+struct WfLaunchInfo {
+	cudaEvent_t* events = nullptr;
+	unsigned char* kinds = nullptr;
+	int eventPairs = 0;     // capacity in pairs
+	int pairsUsed = 0;
+	int launches = 0;       // kernel launches of the iteration
+};
+
 // One iteration (one sample per pixel) of the wavefront path tracer.
+// counters[0] receives the extension rays' traversal counts, counters[1] the
+// shadow rays'.
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
-                                TraceCounters* counters, cudaStream_t stream);
+                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info);
+
+// Closest hits and shadow-ray tests over the compressed 8-wide hierarchies
+// (same arguments as launch_trace_rays / launch_occlusion of pt_api.hpp).
+cudaError_t launch_trace_rays_wide(const DScene& scene, const float* rays, const float* geoNormals, float tmax,
+                                  uint32_t n, float* t, int32_t* inst, int32_t* prim, float* sp, cudaStream_t stream);
+cudaError_t launch_occlusion_wide(const DScene& scene, const float* a, const float* b, uint32_t n, uint8_t* out,
+                                 cudaStream_t stream);
 
 } // namespace mb

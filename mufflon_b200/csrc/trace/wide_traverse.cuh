@@ -1,0 +1,218 @@
+// Traversal of the compressed 8-wide hierarchies (lbvh/wide.hpp) for closest
+// hits and shadow rays; the counterpart of intersection.cu:319-492 and
+// 624-753 of the reference, over a different hierarchy with the same result.
+//
+// One loop runs both levels. The state of a ray is
+//   * a node group: the child base of the last visited node, its internal-slot
+//     mask and the still unvisited hit internal children as bits in
+//     traversal order (bit k = slot k ^ flip, flip chosen from the ray's
+//     direction octant so that bit order is roughly near to far),
+//   * a primitive group: the last visited node's primitive base and one bit
+//     per primitive of its hit leaves,
+//   * a stack of node groups (and, at the instance level, primitive groups of
+//     instances not yet entered).
+// Entering an instance transforms the ray into object space and remembers the
+// stack depth; when the object level's groups are exhausted at that depth the
+// world ray is restored. Every step visits one node (eight box tests that do
+// the same arithmetic in every lane) and then that node's hit primitives.
+//
+// The box test cannot cull a box that contains a hit point (wide.hpp), so the
+// closest hit is the minimum of (world t, instance, primitive) over all
+// primitive hits, exactly as with the binary hierarchy.
+#pragma once
+
+#include "intersect.cuh"
+#include "../lbvh/wide.hpp"
+
+namespace mb {
+
+constexpr int WIDE_STACK = 64;
+constexpr uint32_t PRIM_GROUP = 0x80000000u;
+
+MBD uint32_t octant_flip(f3 d) {
+	return 7u ^ ((d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u));
+}
+
+// Byte b (0..3) of w as an exact float: 0x4B0000bb is the float 2^23 + bb.
+MBD float qbyte(uint32_t w, int b) {
+	return __fsub_rn(__int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(b)))), 8388608.0f);
+}
+
+// Tests the eight child boxes of node `idx`; returns the child's node group
+// and primitive group.
+MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, uint32_t flip, float tmaxBox,
+                        uint32_t& ngBase, uint32_t& ngImask, uint32_t& ngHits, uint32_t& pgBase, uint32_t& pgHits) {
+	const float4* q = reinterpret_cast<const float4*>(nodes + idx);
+	const float4 n0 = __ldg(q), n1 = __ldg(q + 1), n2 = __ldg(q + 2), n3 = __ldg(q + 3), n4 = __ldg(q + 4);
+	const uint32_t eim = __float_as_uint(n0.w);
+	const float sx = __fmul_rn(__uint_as_float((eim & 0xFFu) << 23), r.inv.x);
+	const float sy = __fmul_rn(__uint_as_float(((eim >> 8) & 0xFFu) << 23), r.inv.y);
+	const float sz = __fmul_rn(__uint_as_float(((eim >> 16) & 0xFFu) << 23), r.inv.z);
+	const float ox = __fmul_rn(__fsub_rn(n0.x, r.o.x), r.inv.x);
+	const float oy = __fmul_rn(__fsub_rn(n0.y, r.o.y), r.inv.y);
+	const float oz = __fmul_rn(__fsub_rn(n0.z, r.o.z), r.inv.z);
+	const uint32_t imask = eim >> 24;
+	const bool fx = r.inv.x < 0.0f, fy = r.inv.y < 0.0f, fz = r.inv.z < 0.0f;
+	const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y);
+	const uint32_t ly0 = __float_as_uint(n2.z), ly1 = __float_as_uint(n2.w);
+	const uint32_t lz0 = __float_as_uint(n3.x), lz1 = __float_as_uint(n3.y);
+	const uint32_t hx0 = __float_as_uint(n3.z), hx1 = __float_as_uint(n3.w);
+	const uint32_t hy0 = __float_as_uint(n4.x), hy1 = __float_as_uint(n4.y);
+	const uint32_t hz0 = __float_as_uint(n4.z), hz1 = __float_as_uint(n4.w);
+	const uint32_t nx[2] = { fx ? hx0 : lx0, fx ? hx1 : lx1 }, fxw[2] = { fx ? lx0 : hx0, fx ? lx1 : hx1 };
+	const uint32_t ny[2] = { fy ? hy0 : ly0, fy ? hy1 : ly1 }, fyw[2] = { fy ? ly0 : hy0, fy ? ly1 : hy1 };
+	const uint32_t nz[2] = { fz ? hz0 : lz0, fz ? hz1 : lz1 }, fzw[2] = { fz ? lz0 : hz0, fz ? lz1 : hz1 };
+	const uint32_t meta[2] = { __float_as_uint(n1.z), __float_as_uint(n1.w) };
+	uint32_t nh = 0, ph = 0;
+#pragma unroll
+	for(int i = 0; i < 8; ++i) {
+		const int w = i >> 2, b = i & 3;
+		const float tnx = __fmaf_rn(qbyte(nx[w], b), sx, ox);
+		const float tny = __fmaf_rn(qbyte(ny[w], b), sy, oy);
+		const float tnz = __fmaf_rn(qbyte(nz[w], b), sz, oz);
+		const float tfx = __fmaf_rn(qbyte(fxw[w], b), sx, ox);
+		const float tfy = __fmaf_rn(qbyte(fyw[w], b), sy, oy);
+		const float tfz = __fmaf_rn(qbyte(fzw[w], b), sz, oz);
+		const float tnear = fmax_(fmax_(tnx, tny), fmax_(tnz, 0.0f));
+		const float tfar = fmin_(fmin_(tfx, tfy), tfz);
+		if(tnear <= tmaxBox && tnear <= __fmul_rn(tfar, BOX_FAR_SLACK)) {
+			if(imask & (1u << i)) {
+				nh |= 1u << (uint32_t(i) ^ flip);
+			} else {
+				const uint32_t m = (meta[w] >> (8 * b)) & 0xFFu;
+				ph |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+			}
+		}
+	}
+	ngBase = __float_as_uint(n1.x);
+	ngImask = imask;
+	ngHits = nh;
+	pgBase = __float_as_uint(n1.y);
+	pgHits = ph;
+}
+
+// Closest hit (ANY = false; `best` holds the incoming tmax in best.t) or
+// occlusion test (ANY = true; returns true as soon as a primitive is hit
+// before tmaxW). Returns false on stack overflow or a corrupted hierarchy
+// (counted in cnt.errors).
+template < bool ANY >
+MBD bool wide_trace(const DScene& S, f3 wo, f3 wd, float tmaxW, HitRec& best, LocalCounters& cnt, uint2* stack) {
+	if(S.activeInstances <= 0) return false;
+	FastRay r = make_ray(wo, wd);
+	uint32_t flip = octant_flip(wd);
+	float scale = 1.0f;
+	int inst = -1;
+	const DLod* lod = nullptr;
+	const WideNode* nodes = S.tlasWide;
+	uint32_t ngBase = 0, ngImask = 1, ngHits = 0, pgBase = 0, pgHits = 0;
+	int sp = 0, instSp = -1;
+	const bool single = S.activeInstances == 1;
+
+	auto enter = [&](uint32_t i) {
+		++cnt.instances;
+		inst = int(i);
+		lod = S.lods + __ldg(S.instanceLod + i);
+		const InstRay ir = instance_ray(load_w2i(S, i), wo, wd);
+		r = ir.ray;
+		scale = ir.scale;
+		flip = octant_flip(r.d);
+		nodes = lod->wnodes;
+		const int np = lod->numPrims;
+		ngBase = 0; ngImask = 1; ngHits = 0; pgBase = 0; pgHits = 0;
+		if(np >= 2) ngHits = 1u << flip; // the root, slot 0 of a virtual parent
+		else if(np == 1) pgHits = 1u;
+		instSp = sp;
+	};
+
+	if(single) enter(uint32_t(S.validInstance));
+	else ngHits = S.tlasNumWide > 0 ? (1u << flip) : 0u;
+
+	for(int guard = 0;; ++guard) {
+		if(guard >= MAX_TRAVERSAL_STEPS) { ++cnt.errors; return false; }
+		if(ngHits) {
+			const uint32_t k = uint32_t(__ffs(int(ngHits)) - 1);
+			ngHits &= ngHits - 1u;
+			const uint32_t s = k ^ flip;
+			const uint32_t child = ngBase + uint32_t(__popc(ngImask & ((1u << s) - 1u)));
+			if(ngHits) {
+				if(sp >= WIDE_STACK) { ++cnt.errors; return false; }
+				stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
+			}
+			++cnt.nodes;
+			const float tmaxBox = ANY ? tmaxW * scale * BOX_SLACK : best.t * scale * BOX_SLACK;
+			wide_node_test(nodes, child, r, flip, tmaxBox, ngBase, ngImask, ngHits, pgBase, pgHits);
+		}
+		if(pgHits) {
+			if(instSp >= 0) {
+				const float4* soup = lod->wsoup;
+				const uint32_t ntri = lod->numTriangles;
+				do {
+					const uint32_t j = uint32_t(__ffs(int(pgHits)) - 1);
+					pgHits &= pgHits - 1u;
+					const float4* s4 = soup + 3 * size_t(pgBase + j);
+					const float4 a = __ldg(s4);
+					const int p = __float_as_int(a.w);
+					++cnt.prims;
+					float t;
+					f2 uv;
+					bool hit;
+					if(uint32_t(p) < ntri) {
+						const float4 b = __ldg(s4 + 1), c = __ldg(s4 + 2);
+						hit = tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, uv) && t > 0.0f;
+					} else {
+						hit = prim_test(*lod, r, 0, p, t, uv);
+					}
+					if(hit) {
+						if(ANY) {
+							if(t < tmaxW * scale) return true;
+						} else {
+							const float tw = __fdiv_rn(t, scale);
+							if(better(tw, inst, p, best)) { best.t = tw; best.inst = inst; best.prim = p; best.sp = uv; best.has = true; }
+						}
+					}
+				} while(pgHits);
+			} else {
+				// instance leaves of the top level: enter one, keep the rest
+				const uint32_t j = uint32_t(__ffs(int(pgHits)) - 1);
+				pgHits &= pgHits - 1u;
+				const uint32_t id = uint32_t(__ldg(S.tlasWidePrims + pgBase + j));
+				if(sp + 2 > WIDE_STACK) { ++cnt.errors; return false; }
+				if(ngHits) stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
+				if(pgHits) stack[sp++] = make_uint2(pgBase, pgHits | PRIM_GROUP);
+				enter(id);
+				continue;
+			}
+		}
+		if(!ngHits) {
+			if(instSp >= 0 && sp == instSp) {
+				if(single) break;
+				r = make_ray(wo, wd);
+				flip = octant_flip(wd);
+				scale = 1.0f;
+				nodes = S.tlasWide;
+				instSp = -1;
+			}
+			if(sp == 0) break;
+			const uint2 e = stack[--sp];
+			if(e.y & PRIM_GROUP) { pgBase = e.x; pgHits = e.y & 0xFFFFu; }
+			else { ngBase = e.x; ngImask = e.y & 0xFFu; ngHits = e.y >> 8; }
+		}
+	}
+	return !ANY;
+}
+
+MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
+	++cnt.rays;
+	HitRec best;
+	best.t = tmax; best.inst = -1; best.prim = -1; best.sp = make2(0.0f, 0.0f); best.has = false;
+	wide_trace<false>(S, o, dir, tmax, best, cnt, stack);
+	return best;
+}
+
+MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
+	++cnt.rays; ++cnt.shadow;
+	HitRec unused;
+	return wide_trace<true>(S, a, dir, tmax, unused, cnt, stack);
+}
+
+} // namespace mb

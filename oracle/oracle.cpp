@@ -26,10 +26,15 @@
 //   3. SAH merge order fixed to "right child is the arriving thread", which is
 //      what a sequential run of the reference CPU loop produces;
 //   4. first hits are ordered by (world t, instance, primitive), so the result
-//      does not depend on traversal order; box culling uses tmax * (1 + 2^-16)
+//      does not depend on traversal order; box culling uses tmax * (1 + 2^-12)
 //      so that it stays conservative;
-//   5. the slab test clamps cmin at 0 on both sides (the reference GPU form,
-//      with the FMA the GPU compiler forms: fma(min, invDir, -oDivDir));
+//   5. robust slab test: t = (bound - origin) * invDir per axis (relative
+//      error of a few ulp and the exact sign, where the reference's
+//      fma(bound, invDir, -origin * invDir) has an error relative to the
+//      origin's magnitude), entry clamped at 0, interval accepted up to
+//      far * (1 + 2^-20). A box that contains a primitive's hit point is
+//      never culled, so every bounding hierarchy over the same primitives
+//      yields the same closest hit;
 //   6. watertight triangle test (Woop, Benthin, Wald, JCGT 2013);
 //   7. sphere test from the quadratic with a stable root, solveSquarePoly and
 //      the vector helpers (surface, bilerp, sgn, box transform) written from
@@ -70,7 +75,8 @@ constexpr float PI = 3.14159265358979f;
 constexpr float MAX_SCENE_SIZE = 1048576.0f;
 constexpr float SCENE_SCALE_EPS = 1e-4f;
 constexpr float INF_PDF = 4294967296.0f;
-constexpr float BOX_SLACK = 1.0f + 1.0f / 65536.0f;
+constexpr float BOX_SLACK = 1.0f + 1.0f / 4096.0f;
+constexpr float BOX_FAR_SLACK = 1.0f + 1.0f / 1048576.0f;
 constexpr float DISTANCESQ_EPSILON = 1e-10f;
 constexpr float SHADING_NORMAL_EPS = 1e-3f;
 constexpr i32 TREE_HEAD = 0x10000000;
@@ -597,7 +603,7 @@ void build_lbvh(const BuildDesc& d, i32 numPrimitives, i32 actualPrimCount, Bvh&
 
 // ---------------------------------------------------------------- rays
 struct FastRay {
-	V3 o, d, inv, oDiv;
+	V3 o, d, inv;
 	// watertight test precomputation
 	int kx, ky, kz;
 	float Sx, Sy, Sz;
@@ -606,7 +612,6 @@ FastRay make_ray(V3 o, V3 d) {
 	FastRay r;
 	r.o = o; r.d = d;
 	r.inv = { 1.0f / d.x, 1.0f / d.y, 1.0f / d.z };
-	r.oDiv = o * r.inv;
 	const float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
 	int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
 	int kx = kz + 1 == 3 ? 0 : kz + 1;
@@ -619,17 +624,17 @@ FastRay make_ray(V3 o, V3 d) {
 	return r;
 }
 
-// intersection.cu:47-77 (GPU form)
+// Slab test of intersection.cu:47-77 in its robust form (deviation 5).
 inline bool box_test(const V3& mn, const V3& mx, const FastRay& r, float tmax, float& cmin) {
-	const float lox = mbmath::fma_(mn.x, r.inv.x, -r.oDiv.x);
-	const float loy = mbmath::fma_(mn.y, r.inv.y, -r.oDiv.y);
-	const float loz = mbmath::fma_(mn.z, r.inv.z, -r.oDiv.z);
-	const float hix = mbmath::fma_(mx.x, r.inv.x, -r.oDiv.x);
-	const float hiy = mbmath::fma_(mx.y, r.inv.y, -r.oDiv.y);
-	const float hiz = mbmath::fma_(mx.z, r.inv.z, -r.oDiv.z);
+	const float lox = (mn.x - r.o.x) * r.inv.x;
+	const float loy = (mn.y - r.o.y) * r.inv.y;
+	const float loz = (mn.z - r.o.z) * r.inv.z;
+	const float hix = (mx.x - r.o.x) * r.inv.x;
+	const float hiy = (mx.y - r.o.y) * r.inv.y;
+	const float hiz = (mx.z - r.o.z) * r.inv.z;
 	cmin = fmax_(fmax_(fmin_(lox, hix), fmin_(loy, hiy)), fmax_(fmin_(loz, hiz), 0.0f));
-	const float cmax = fmin_(fmin_(fmax_(lox, hix), fmax_(loy, hiy)), fmin_(fmax_(loz, hiz), tmax));
-	return cmin <= cmax;
+	const float cfar = fmin_(fmin_(fmax_(lox, hix), fmax_(loy, hiy)), fmax_(loz, hiz));
+	return cmin <= tmax && cmin <= cfar * BOX_FAR_SLACK;
 }
 
 // Watertight ray/triangle test; returns t and the barycentric weights of v0, v1.

@@ -71,6 +71,15 @@ def _mixed_lod(seed):
                        sphere_mats=np.zeros(ns, np.uint16))
 
 
+def _single_lod_spec(lod):
+    """One instance of `lod`, a Lambert material, a camera looking down -z."""
+    return scenes.SceneSpec(lods=[lod], world_to_instance=scenes.identity34().reshape(1, 12),
+                            instance_lod=np.zeros(1, np.uint32), materials=[scenes.MaterialSpec(type=0)],
+                            point_lights=np.zeros((0, 6), np.float32), background=None, cam_pos=(0.5, 0.5, 8.0),
+                            cam_dir=(0.0, 0.0, -1.0), cam_up=(0.0, 1.0, 0.0), vfov=0.8, width=64, height=64,
+                            name="mixed")
+
+
 @pytest.mark.parametrize("which", ["walls", "box", "light", "random_2", "random_5000", "mixed", "ico5", "ico7"])
 def test_lbvh_bit_exact(dll, oracle, which):
     if which in ("walls", "box", "light"):
@@ -92,6 +101,9 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
     _compare_bvh(dll, oracle, spec.lods[0])
 
 
+# "wavefront": stage kernels over the 8-wide hierarchies; "megakernel": one
+# kernel over the binary (reference-layout) hierarchies.
+KERNELS = {"wavefront": 0, "megakernel": 1}
 DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
                   "RR start depth": 0, "Megakernel": 0}
 
@@ -128,15 +140,20 @@ def _small_instanced(seed=0):
                                   tri_range=(2000, 8000), width=64, height=48)
 
 
-@pytest.mark.parametrize("scene", ["cornell", "icosphere6", "instanced"])
-def test_first_hit_bit_exact(dll, oracle, scene):
+@pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("scene", ["cornell", "icosphere6", "instanced", "mixed"])
+def test_first_hit_bit_exact(dll, oracle, scene, kernel):
+    """Closest hits over the 8-wide hierarchies ("wavefront") and the binary ones ("megakernel")."""
     if scene == "cornell":
         spec = scenes.cornell_box(3)
     elif scene == "icosphere6":
         spec = scenes.displaced_icosphere(1, subdiv=6, width=64, height=36)
+    elif scene == "mixed":
+        spec = _single_lod_spec(_mixed_lod(7))
     else:
         spec = _small_instanced(2)
     _load(dll, spec)
+    assert dll.renderer_set_parameter_int("Megakernel", KERNELS[kernel])
     sc = oracle.OracleScene(spec)
     rays = np.concatenate([_camera_rays(spec, 20000, 1), _interior_rays(spec, sc, 20000, 2)])
     if scene == "instanced":
@@ -152,22 +169,21 @@ def test_first_hit_bit_exact(dll, oracle, scene):
     assert np.array_equal(gp, op)
     assert np.array_equal(gt.view(np.uint32), ot.view(np.uint32))
     assert np.array_equal(gs.view(np.uint32), os_.view(np.uint32))
-    assert (gi >= 0).mean() > (0.12 if scene == "instanced" else 0.3)
+    assert (gi >= 0).mean() > (0.12 if scene in ("instanced", "mixed") else 0.3)
 
 
+@pytest.mark.parametrize("kernel", list(KERNELS))
 @pytest.mark.parametrize("scene", ["cornell", "instanced"])
-def test_occlusion_matches_oracle(dll, oracle, scene):
+def test_occlusion_matches_oracle(dll, oracle, scene, kernel):
     spec = scenes.cornell_box(4) if scene == "cornell" else _small_instanced(3)
     _load(dll, spec)
+    assert dll.renderer_set_parameter_int("Megakernel", KERNELS[kernel])
     sc = oracle.OracleScene(spec)
     rng = np.random.default_rng(9)
     box = sc.aabb()
     a = rng.uniform(box[:3], box[3:], (20000, 3)).astype(np.float32)
     b = rng.uniform(box[:3], box[3:], (20000, 3)).astype(np.float32)
     assert np.array_equal(dll.trace_occlusion(a, b), sc.trace_any(a, b))
-
-
-KERNELS = {"wavefront": 0, "megakernel": 1}
 
 
 def _render_pair(dll, oracle, spec, spp, max_path, seed=0, rr_start=0, kernel="wavefront", nee=1, min_path=0):
