@@ -276,9 +276,12 @@ def run_b200(args):
     h2d = scene_bytes(spec)
     barrier()
     e2e_rays, t_e2e = 0.0, 0.0
+    load_ms = {}
     for _ in range(args.steps):
         t0 = time.perf_counter()
         dll.core.world_load_scenario(dll.muffInst, dll.core.world_get_current_scenario(dll.muffInst))
+        for k, v in dll.load_stats().items():
+            load_ms[k] = load_ms.get(k, 0.0) + v / args.steps
         for _ in range(SPP_PER_FRAME):
             dll.render_iterate()
             e2e_rays += dll.render_stats()["rays"]
@@ -297,15 +300,19 @@ def run_b200(args):
         e2e_rays = float(r.item())
     e2e_mrays = e2e_rays / t_e2e / 1e6
 
-    # roofline of the dominant kernel (closest-hit traversal): algorithmic
-    # bytes per launch / its average launch time (events on the library's
-    # stream). Per unit: an 8-wide node 80 B, a primitive-soup slot 48 B, an
-    # instance entry 56 B (world-to-instance rows 48 B + LoD index 4 B + the
-    # LoD's hierarchy pointers); the queue entry of the ray 32 B in, 20 B out.
+    # roofline of the dominant kernel (k_trace: closest-hit and shadow-ray
+    # traversal of one bounce): algorithmic bytes per launch / its average
+    # launch time (events on the library's stream). Per unit: an 8-wide node
+    # 80 B, a primitive-soup slot 48 B, an instance entry 56 B (world-to-instance
+    # rows 48 B + LoD index 4 B + the LoD's hierarchy pointers); per extension
+    # ray its queue entry 32 B in and 20 B out, per shadow ray 48 B in.
     st = stage_frame()
-    extend_launches = SPP_PER_FRAME * MAX_PATH
-    alg_bytes = (st["extendNodeVisits"] * 80 + st["extendPrimTests"] * 48 + st["extendInstanceVisits"] * 56
-                 + st["extensionRays"] * (32 + 20))
+    trace_launches = SPP_PER_FRAME * MAX_PATH
+    ext_rays, shd_rays = st["extensionRays"], st["shadowRays"]
+    alg_bytes = ((st["extendNodeVisits"] + st["shadowNodeVisits"]) * 80
+                 + (st["extendPrimTests"] + st["shadowPrimTests"]) * 48
+                 + (st["extendInstanceVisits"] + st["shadowInstanceVisits"]) * 56
+                 + ext_rays * (32 + 20) + shd_rays * 48)
     achieved_gbs = alg_bytes / (st["extendMs"] * 1e-3) / 1e9
     peaks, peak_kind = measured_peaks()
     l2 = bindings.c_float(0.0)
@@ -315,10 +322,11 @@ def run_b200(args):
                 "peak_source": f"{peak_kind} HBM copy bandwidth",
                 "l2_read_peak_gbs": round(float(l2.value), 1),
                 "frac_of_l2": round(achieved_gbs / max(float(l2.value), 1e-9), 4),
-                "bytes_per_ray": round(alg_bytes / max(st["extensionRays"], 1), 1),
-                "kernel": "k_extend", "launches": extend_launches,
-                "avg_launch_ms": round(st["extendMs"] / extend_launches, 4)}
-    stage_ms = {k[:-2]: round(v, 3) for k, v in st.items() if k.endswith("Ms")}
+                "bytes_per_ray": round(alg_bytes / max(ext_rays + shd_rays, 1), 1),
+                "kernel": "k_trace", "launches": trace_launches,
+                "avg_launch_ms": round(st["extendMs"] / trace_launches, 4)}
+    stage_ms = {"camera": round(st["cameraMs"], 3), "trace": round(st["extendMs"], 3),
+                "shade": round(st["shadeMs"], 3), "finalize": round(st["finalizeMs"], 3)}
     per_ray = {"extend_nodes": round(st["extendNodeVisits"] / max(st["extensionRays"], 1), 2),
                "extend_prims": round(st["extendPrimTests"] / max(st["extensionRays"], 1), 2),
                "shadow_nodes": round(st["shadowNodeVisits"] / max(st["shadowRays"], 1), 2),
@@ -339,7 +347,8 @@ def run_b200(args):
                 "rays_per_step": int(rays / args.steps),
                 "e2e": {"value": round(e2e_mrays, 2), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h),
-                        "note": "scene upload + GPU LBVH build + 16 iterations + radiance readback per step (wall clock)"},
+                        "note": "scene upload + GPU LBVH build + 16 iterations + radiance readback per step (wall clock)",
+                        "load_ms": {k: round(v, 3) for k, v in load_ms.items() if k.endswith("Ms")}},
                 "gpu_launches": int(gpu_launches),
                 "roofline": roofline,
                 "stage_ms_per_frame": stage_ms,

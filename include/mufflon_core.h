@@ -261,15 +261,29 @@ CORE_API Boolean CDECL mufflon_get_render_stats(MufflonInstanceHdl instHdl, Muff
  * traversal counters are split into extension rays (closest hit) and shadow
  * rays (any hit); with the megakernel all of them are in the extension
  * fields. The stage times are filled only while the integer renderer
- * parameter "Stage timing" is non-zero (events around every stage launch). */
+ * parameter "Stage timing" is non-zero (events around every stage launch):
+ * camera rays, the trace launches of the wavefront bounces (extension and
+ * shadow rays), the launch that finishes the remaining paths, the shade
+ * launches and the accumulation. */
 typedef struct {
 	uint64_t extensionRays, extendNodeVisits, extendPrimTests, extendInstanceVisits;
 	uint64_t shadowRays, shadowNodeVisits, shadowPrimTests, shadowInstanceVisits;
-	float cameraMs, extendMs, shadowMs, shadeMs, finalizeMs;
+	float cameraMs, extendMs, tailMs, shadeMs, finalizeMs;
 	uint32_t launches;  /* kernel launches of the iteration */
 	uint32_t wavefront; /* 1: wavefront stages, 0: megakernel */
 } MufflonStageStats;
 CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
+
+/* Host-side times (ms) of the last scene load (world_load_scenario or the
+ * implicit load of the first render_iterate): the whole load, the geometry
+ * upload, the object BVH builds (LBVH + 8-wide conversion), the instance BVH,
+ * and lights / materials / textures; plus the geometry bytes copied to the GPU. */
+typedef struct {
+	float totalMs, uploadMs, bvhMs, instanceBvhMs, otherMs;
+	uint32_t pad;
+	uint64_t h2dBytes;
+} MufflonLoadStats;
+CORE_API Boolean CDECL mufflon_get_load_stats(MufflonInstanceHdl instHdl, MufflonLoadStats* stats);
 
 /* Closest hits of n rays (6 floats: origin, direction) against the loaded
  * scene, with the path tracer's epsilon offset along geoNormals (may be NULL). */

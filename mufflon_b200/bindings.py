@@ -172,8 +172,13 @@ class MufflonStageStats(Structure):
     _fields_ = [("extensionRays", c_uint64), ("extendNodeVisits", c_uint64), ("extendPrimTests", c_uint64),
                 ("extendInstanceVisits", c_uint64), ("shadowRays", c_uint64), ("shadowNodeVisits", c_uint64),
                 ("shadowPrimTests", c_uint64), ("shadowInstanceVisits", c_uint64), ("cameraMs", c_float),
-                ("extendMs", c_float), ("shadowMs", c_float), ("shadeMs", c_float), ("finalizeMs", c_float),
+                ("extendMs", c_float), ("tailMs", c_float), ("shadeMs", c_float), ("finalizeMs", c_float),
                 ("launches", c_uint32), ("wavefront", c_uint32)]
+
+
+class MufflonLoadStats(Structure):
+    _fields_ = [("totalMs", c_float), ("uploadMs", c_float), ("bvhMs", c_float), ("instanceBvhMs", c_float),
+                ("otherMs", c_float), ("pad", c_uint32), ("h2dBytes", c_uint64)]
 
 
 def _bulk(a: np.ndarray) -> BulkLoader:
@@ -268,6 +273,7 @@ class DllHolder:
             "renderer_set_parameter_enum": (c_uint32, [c_void_p, c_char_p, c_int32]),
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
+            "mufflon_get_load_stats": (c_uint32, [c_void_p, POINTER(MufflonLoadStats)]),
             "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
                                               c_void_p, c_void_p]),
             "mufflon_trace_occlusion": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
@@ -433,6 +439,11 @@ class DllInterface:
         s = MufflonStageStats()
         self._check(self.core.mufflon_get_stage_stats(self.muffInst, byref(s)), "mufflon_get_stage_stats")
         return {k: getattr(s, k) for k, _ in MufflonStageStats._fields_}
+
+    def load_stats(self):
+        s = MufflonLoadStats()
+        self._check(self.core.mufflon_get_load_stats(self.muffInst, byref(s)), "mufflon_get_load_stats")
+        return {k: getattr(s, k) for k, _ in MufflonLoadStats._fields_ if k != "pad"}
 
     def trace_rays(self, rays, tmax=1048576.0, geo_normals=None):
         rays = np.ascontiguousarray(rays, np.float32)

@@ -54,7 +54,7 @@ const ParamDesc PT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
-	{ "Stage timing", PARAM_INT },
+	{ "Stage timing", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
 };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
@@ -69,6 +69,8 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "Blocks per SM")) return &r.blocksPerSm;
 	if(!std::strcmp(name, "Megakernel")) return &r.megakernel;
 	if(!std::strcmp(name, "Stage timing")) return &r.stageTiming;
+	if(!std::strcmp(name, "Trace blocks per SM")) return &r.traceBlocksPerSm;
+	if(!std::strcmp(name, "Wavefront bounces")) return &r.wavefrontBounces;
 	return nullptr;
 }
 
@@ -729,7 +731,10 @@ Boolean scenario_assign_material(ScenarioHdl s, MatIdx idx, MaterialHdl m) {
 SceneHdl world_get_current_scene(MufflonInstanceHdl h) { TRY MufflonInstance& I = minst(h); return I.scene.valid ? &I.scene : nullptr; CATCH_ALL(nullptr) }
 Boolean scene_get_bounding_box(SceneHdl s, Vec3* mn, Vec3* mx) {
 	TRY CHECK(s, "invalid scene"); auto* d = static_cast<DeviceScene*>(s);
-	if(mn) *mn = { d->aabb[0], d->aabb[1], d->aabb[2] }; if(mx) *mx = { d->aabb[3], d->aabb[4], d->aabb[5] }; return true; CATCH_ALL(false)
+	if(mn) *mn = { d->aabb[0], d->aabb[1], d->aabb[2] };
+	if(mx) *mx = { d->aabb[3], d->aabb[4], d->aabb[5] };
+	return true;
+	CATCH_ALL(false)
 }
 
 // ---------------------------------------------------------------- lights
@@ -847,7 +852,8 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	}
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
 	if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
-	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info));
+	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, r.traceBlocksPerSm,
+	                                    r.wavefrontBounces));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters both[2];
 	CHECK_CUDA(cudaMemcpyAsync(both, r.counters, 2 * sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
@@ -986,7 +992,7 @@ Boolean renderer_get_parameter_float(MufflonInstanceHdl h, const char* name, flo
 }
 Boolean renderer_set_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean value) {
 	TRY
-	MufflonInstance& I = minst(h);
+	(void)minst(h);
 	CHECK(name && !std::strcmp(name, "NEE position guide"), std::string("unknown bool parameter '") + (name ? name : "") + "'");
 	CHECK(!value, "NEE position guide is not implemented by the CUDA path tracer");
 	return true;
@@ -1029,10 +1035,23 @@ Boolean mufflon_get_stage_stats(MufflonInstanceHdl h, MufflonStageStats* s) {
 	s->extendInstanceVisits = e.instanceVisits;
 	s->shadowRays = sh.rays; s->shadowNodeVisits = sh.nodeVisits; s->shadowPrimTests = sh.primTests;
 	s->shadowInstanceVisits = sh.instanceVisits;
-	s->cameraMs = r.stageMs[WF_CAMERA]; s->extendMs = r.stageMs[WF_EXTEND]; s->shadowMs = r.stageMs[WF_SHADOW];
+	s->cameraMs = r.stageMs[WF_CAMERA]; s->extendMs = r.stageMs[WF_EXTEND]; s->tailMs = r.stageMs[WF_TAIL];
 	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE];
 	s->launches = uint32_t(r.lastLaunches);
 	s->wavefront = r.megakernel ? 0u : 1u;
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_get_load_stats(MufflonInstanceHdl h, MufflonLoadStats* s) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(s, "stats pointer is null");
+	const DeviceScene& D = I.scene;
+	s->totalMs = D.loadMs[0]; s->uploadMs = D.loadMs[1]; s->bvhMs = D.loadMs[2];
+	s->instanceBvhMs = D.loadMs[3]; s->otherMs = D.loadMs[4];
+	s->pad = 0;
+	s->h2dBytes = D.loadH2dBytes;
 	return true;
 	CATCH_ALL(false)
 }

@@ -15,6 +15,7 @@
 #include "world.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -224,13 +225,24 @@ LightTreeOut build_pos_tree(const std::vector<HostLight>& lights, const std::vec
 	return T;
 }
 
+// Copies count elements (in up to two parts) into a grow-only device buffer.
 template < class T >
-bool upload(T*& dst, const T* src, size_t count, cudaStream_t s, std::string& err) {
-	if(dst) { cudaFree(dst); dst = nullptr; }
-	if(count == 0) return true;
-	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&dst), sizeof(T) * count);
-	if(e == cudaSuccess) e = cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, s);
+bool upload(T*& dst, size_t& cap, const T* src, size_t count, cudaStream_t s, std::string& err,
+            const T* src2 = nullptr, size_t count2 = 0, uint64_t* bytes = nullptr) {
+	const size_t total = count + count2;
+	if(total == 0) return true;
+	cudaError_t e = cudaSuccess;
+	if(total > cap) {
+		if(dst) cudaFree(dst);
+		dst = nullptr;
+		cap = 0;
+		e = cudaMalloc(reinterpret_cast<void**>(&dst), sizeof(T) * total);
+		if(e == cudaSuccess) cap = total;
+	}
+	if(e == cudaSuccess && count) e = cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, s);
+	if(e == cudaSuccess && count2) e = cudaMemcpyAsync(dst + count, src2, sizeof(T) * count2, cudaMemcpyHostToDevice, s);
 	if(e != cudaSuccess) { err = std::string("device upload failed: ") + cudaGetErrorString(e); return false; }
+	if(bytes) *bytes += sizeof(T) * total;
 	return true;
 }
 
@@ -260,6 +272,7 @@ void DeviceLod::release() {
 	cudaFree(vertices); cudaFree(normals); cudaFree(uvs); cudaFree(indices);
 	cudaFree(faceMat); cudaFree(spheres); cudaFree(sphereMat);
 	vertices = normals = uvs = nullptr; indices = nullptr; faceMat = sphereMat = nullptr; spheres = nullptr;
+	for(size_t& c : cap) c = 0;
 	bvh.release();
 }
 
@@ -276,6 +289,7 @@ void DeviceScene::release() {
 	dLods = nullptr; dW2I = nullptr; dInstLod = nullptr; dInstBoxes = nullptr; dInstCentroids = nullptr;
 	dMaterials = nullptr; dTextures = nullptr; dLights = nullptr; dLightNodes = nullptr;
 	dLightKeys = nullptr; dLightCodes = nullptr;
+	for(size_t& c : cap) c = 0;
 	desc = DScene{};
 	valid = false;
 }
@@ -286,7 +300,17 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	if(!sc->camera) { err = "scenario has no camera"; return false; }
 	cudaStream_t s = inst.stream;
 	DeviceScene& D = inst.scene;
-	D.release();
+	using clk = std::chrono::steady_clock;
+	const auto t0 = clk::now();
+	auto msSince = [](clk::time_point a) { return std::chrono::duration<float, std::milli>(clk::now() - a).count(); };
+	float uploadMs = 0.0f, bvhMs = 0.0f;
+	uint64_t h2d = 0;
+	// keep the device buffers of the previous load (grow-only); textures are re-made
+	D.valid = false;
+	D.desc = DScene{};
+	D.lodSources.clear();
+	for(auto* t : D.textureBuffers) cudaFree(t);
+	D.textureBuffers.clear();
 
 	// --- materials per slot (scene.cpp load_materials)
 	std::vector<DMaterial> mats(std::max<size_t>(sc->slotMaterials.size(), 1));
@@ -334,28 +358,31 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		} else instLod[i] = it->second;
 	}
 	// --- upload LoDs and build their BVHs
+	for(size_t li = D.lodSources.size(); li < D.lods.size(); ++li) D.lods[li].release();
 	D.lods.resize(D.lodSources.size());
 	std::vector<DLod> dl(std::max<size_t>(D.lods.size(), 1));
 	for(size_t li = 0; li < D.lods.size(); ++li) {
 		const HostLod& h = *D.lodSources[li];
 		DeviceLod& g = D.lods[li];
-		std::vector<uint32_t> idx(h.triIdx);
-		idx.insert(idx.end(), h.quadIdx.begin(), h.quadIdx.end());
-		std::vector<uint16_t> fm(h.triMat);
-		fm.insert(fm.end(), h.quadMat.begin(), h.quadMat.end());
-		if(!upload(g.vertices, h.vertices.data(), h.vertices.size(), s, err)) return false;
-		if(!upload(g.normals, h.normals.data(), h.normals.size(), s, err)) return false;
-		if(!upload(g.uvs, h.uvs.data(), h.uvs.size(), s, err)) return false;
-		if(!upload(g.indices, idx.data(), idx.size(), s, err)) return false;
-		if(!upload(g.faceMat, fm.data(), fm.size(), s, err)) return false;
-		if(!upload(g.spheres, reinterpret_cast<const float4*>(h.spheres.data()), h.spheres.size() / 4, s, err)) return false;
-		if(!upload(g.sphereMat, h.sphereMat.data(), h.sphereMat.size(), s, err)) return false;
+		auto tu = clk::now();
+		if(!upload(g.vertices, g.cap[0], h.vertices.data(), h.vertices.size(), s, err, (const float*)nullptr, 0, &h2d)) return false;
+		if(!upload(g.normals, g.cap[1], h.normals.data(), h.normals.size(), s, err, (const float*)nullptr, 0, &h2d)) return false;
+		if(!upload(g.uvs, g.cap[2], h.uvs.data(), h.uvs.size(), s, err, (const float*)nullptr, 0, &h2d)) return false;
+		if(!upload(g.indices, g.cap[3], h.triIdx.data(), h.triIdx.size(), s, err, h.quadIdx.data(), h.quadIdx.size(), &h2d)) return false;
+		if(!upload(g.faceMat, g.cap[4], h.triMat.data(), h.triMat.size(), s, err, h.quadMat.data(), h.quadMat.size(), &h2d)) return false;
+		if(!upload(g.spheres, g.cap[5], reinterpret_cast<const float4*>(h.spheres.data()), h.spheres.size() / 4, s, err,
+		           (const float4*)nullptr, 0, &h2d)) return false;
+		if(!upload(g.sphereMat, g.cap[6], h.sphereMat.data(), h.sphereMat.size(), s, err, (const uint16_t*)nullptr, 0, &h2d)) return false;
 		LodBuildInput in{};
 		in.numTriangles = h.num_triangles(); in.numQuads = h.num_quads(); in.numSpheres = h.num_spheres();
 		in.vertices = g.vertices; in.indices = g.indices; in.spheres = g.spheres;
 		h.bounds(in.aabbMin, in.aabbMax);
+		cudaStreamSynchronize(s);
+		uploadMs += msSince(tu);
+		auto tb = clk::now();
 		cudaError_t e = inst.builder.build_lod(in, g.bvh, s);
 		if(e != cudaSuccess) { err = std::string("LBVH build failed: ") + cudaGetErrorString(e); return false; }
+		bvhMs += msSince(tb);
 		DLod d{};
 		d.numTriangles = in.numTriangles; d.numQuads = in.numQuads; d.numSpheres = in.numSpheres;
 		d.numPrims = int32_t(h.num_prims());
@@ -369,7 +396,8 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		g.desc = d;
 		dl[li] = d;
 	}
-	if(!upload(D.dLods, dl.data(), D.lods.size(), s, err)) return false;
+	const auto tInst = clk::now();
+	if(!upload(D.dLods, D.cap[0], dl.data(), D.lods.size(), s, err)) return false;
 
 	// --- instance transforms, boxes, scene box (scene.cpp:203-303)
 	std::vector<float4> w2i(size_t(std::max<uint32_t>(numInst, 1)) * 3);
@@ -394,10 +422,10 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		st3(&cents[3 * i], c);
 		sceneBox = { vmin(sceneBox.mn, ib.mn), vmax(sceneBox.mx, ib.mx) };
 	}
-	if(!upload(D.dW2I, w2i.data(), size_t(numInst) * 3, s, err)) return false;
-	if(!upload(D.dInstLod, instLod.data(), numInst, s, err)) return false;
-	if(!upload(D.dInstBoxes, boxes.data(), size_t(numInst) * 6, s, err)) return false;
-	if(!upload(D.dInstCentroids, cents.data(), size_t(numInst) * 3, s, err)) return false;
+	if(!upload(D.dW2I, D.cap[1], w2i.data(), size_t(numInst) * 3, s, err)) return false;
+	if(!upload(D.dInstLod, D.cap[2], instLod.data(), numInst, s, err)) return false;
+	if(!upload(D.dInstBoxes, D.cap[3], boxes.data(), size_t(numInst) * 6, s, err)) return false;
+	if(!upload(D.dInstCentroids, D.cap[4], cents.data(), size_t(numInst) * 3, s, err)) return false;
 	if(active > 1) {
 		SceneBuildInput sin{};
 		sin.numInstances = numInst; sin.activeInstances = uint32_t(active);
@@ -407,6 +435,8 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		if(e != cudaSuccess) { err = std::string("instance BVH build failed: ") + cudaGetErrorString(e); return false; }
 	}
 	st3(D.aabb, sceneBox.mn); st3(D.aabb + 3, sceneBox.mx);
+	const float instMs = msSince(tInst);
+	const auto tLights = clk::now();
 
 	// --- lights (world_container.cpp:869-990)
 	std::vector<HostLight> lights;
@@ -495,20 +525,21 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	std::vector<uint64_t> keys;
 	std::vector<uint32_t> codes;
 	for(auto& kc : T.codes) { keys.push_back(kc.first); codes.push_back(kc.second); }
-	if(!upload(D.dLights, dlights.data(), lights.size(), s, err)) return false;
-	if(!upload(D.dLightNodes, T.nodes.data(), T.nodes.size(), s, err)) return false;
-	if(!upload(D.dLightKeys, keys.data(), keys.size(), s, err)) return false;
-	if(!upload(D.dLightCodes, codes.data(), codes.size(), s, err)) return false;
-	if(!upload(D.dMaterials, mats.data(), mats.size(), s, err)) return false;
+	if(!upload(D.dLights, D.cap[5], dlights.data(), lights.size(), s, err)) return false;
+	if(!upload(D.dLightNodes, D.cap[6], T.nodes.data(), T.nodes.size(), s, err)) return false;
+	if(!upload(D.dLightKeys, D.cap[7], keys.data(), keys.size(), s, err)) return false;
+	if(!upload(D.dLightCodes, D.cap[8], codes.data(), codes.size(), s, err)) return false;
+	if(!upload(D.dMaterials, D.cap[9], mats.data(), mats.size(), s, err)) return false;
 	// textures
 	std::vector<DTexture> dtex(std::max<size_t>(texList.size(), 1));
 	for(size_t t = 0; t < texList.size(); ++t) {
 		float4* buf = nullptr;
-		if(!upload(buf, reinterpret_cast<const float4*>(texList[t]->texels.data()), size_t(texList[t]->width) * texList[t]->height, s, err)) return false;
+		size_t bufCap = 0;
+		if(!upload(buf, bufCap, reinterpret_cast<const float4*>(texList[t]->texels.data()), size_t(texList[t]->width) * texList[t]->height, s, err)) return false;
 		D.textureBuffers.push_back(buf);
 		dtex[t] = DTexture{ texList[t]->width, texList[t]->height, buf };
 	}
-	if(!upload(D.dTextures, dtex.data(), texList.size(), s, err)) return false;
+	if(!upload(D.dTextures, D.cap[10], dtex.data(), texList.size(), s, err)) return false;
 
 	// --- scene descriptor
 	DScene& S = D.desc;
@@ -553,6 +584,13 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	}
 	cudaError_t e = cudaStreamSynchronize(s);
 	if(e != cudaSuccess) { err = std::string("scene upload failed: ") + cudaGetErrorString(e); return false; }
+	cudaStreamSynchronize(s);
+	D.loadMs[0] = msSince(t0);
+	D.loadMs[1] = uploadMs;
+	D.loadMs[2] = bvhMs;
+	D.loadMs[3] = instMs;
+	D.loadMs[4] = msSince(tLights);
+	D.loadH2dBytes = h2d;
 	D.valid = true;
 	return true;
 }

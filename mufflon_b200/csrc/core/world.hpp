@@ -5,8 +5,10 @@
 // flattened into.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
+#include <new>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -20,12 +22,30 @@
 
 namespace mb {
 
+// Page-locked host memory for geometry, so that a scene load copies it to
+// the GPU at full link speed without a staging copy.
+template < class T >
+struct PinnedAllocator {
+	using value_type = T;
+	PinnedAllocator() = default;
+	template < class U > PinnedAllocator(const PinnedAllocator<U>&) {}
+	T* allocate(size_t n) {
+		void* p = nullptr;
+		if(cudaMallocHost(&p, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+		return static_cast<T*>(p);
+	}
+	void deallocate(T* p, size_t) { cudaFreeHost(p); }
+	template < class U > bool operator==(const PinnedAllocator<U>&) const { return true; }
+	template < class U > bool operator!=(const PinnedAllocator<U>&) const { return false; }
+};
+template < class T > using pinned_vector = std::vector<T, PinnedAllocator<T>>;
+
 struct HostLod {
-	std::vector<float> vertices, normals, uvs; // 3, 3, 2 per vertex
-	std::vector<uint32_t> triIdx, quadIdx;     // 3 per triangle, 4 per quad
-	std::vector<uint16_t> triMat, quadMat;
-	std::vector<float> spheres;                // 4 per sphere
-	std::vector<uint16_t> sphereMat;
+	pinned_vector<float> vertices, normals, uvs; // 3, 3, 2 per vertex
+	pinned_vector<uint32_t> triIdx, quadIdx;     // 3 per triangle, 4 per quad
+	pinned_vector<uint16_t> triMat, quadMat;
+	pinned_vector<float> spheres;                // 4 per sphere
+	pinned_vector<uint16_t> sphereMat;
 	uint32_t num_vertices() const { return uint32_t(vertices.size() / 3); }
 	uint32_t num_triangles() const { return uint32_t(triMat.size()); }
 	uint32_t num_quads() const { return uint32_t(quadMat.size()); }
@@ -86,7 +106,8 @@ struct HostScenario {
 	std::vector<uint32_t> maskedInstances;
 };
 
-// Device buffers of one LoD.
+// Device buffers of one LoD. Buffers only grow: a reload of the same scene
+// reuses them (capacities in elements).
 struct DeviceLod {
 	float* vertices = nullptr;
 	float* normals = nullptr;
@@ -95,6 +116,7 @@ struct DeviceLod {
 	uint16_t* faceMat = nullptr;
 	float4* spheres = nullptr;
 	uint16_t* sphereMat = nullptr;
+	size_t cap[7] = {};
 	BvhBuffers bvh;
 	DLod desc{};
 	void release();
@@ -120,6 +142,10 @@ struct DeviceScene {
 	DScene desc{};
 	float aabb[6] = { 0, 0, 0, 0, 0, 0 };
 	bool valid = false;
+	size_t cap[12] = {};
+	// host-side times of the last load (ms) and its host-to-device bytes
+	float loadMs[5] = {};          // total, geometry upload, object BVHs, instance BVH, lights/materials
+	uint64_t loadH2dBytes = 0;
 	void release();
 };
 
@@ -137,6 +163,8 @@ struct RendererState {
 	int32_t wfNee = 0;
 	size_t wfPixels = 0;
 	int32_t stageTiming = 0;      // record device time per stage kernel
+	int32_t traceBlocksPerSm = 0; // register budget of the wavefront trace kernel (0: default)
+	int32_t wavefrontBounces = 1; // bounces run as separate stage launches before the tail launch
 	std::vector<cudaEvent_t> stageEvents;
 	std::vector<unsigned char> stageKinds;
 	float stageMs[WF_STAGES] = {};

@@ -65,6 +65,14 @@ MBD bool box_test(float mnx, float mny, float mnz, float mxx, float mxy, float m
 	return cmin <= tmax && cmin <= cfar * BOX_FAR_SLACK;
 }
 
+// Edge functions in double precision, the watertight test's fallback when a
+// single-precision edge function is exactly zero (kept out of line: rare).
+static __device__ __noinline__ float3 edge_functions_double(float Ax, float Ay, float Bx, float By, float Cx, float Cy) {
+	return make_float3(float(__dsub_rn(__dmul_rn(double(Cx), double(By)), __dmul_rn(double(Cy), double(Bx)))),
+	                   float(__dsub_rn(__dmul_rn(double(Ax), double(Cy)), __dmul_rn(double(Ay), double(Cx)))),
+	                   float(__dsub_rn(__dmul_rn(double(Bx), double(Ay)), __dmul_rn(double(By), double(Ax)))));
+}
+
 // Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013).
 MBD bool tri_test(const FastRay& r, f3 v0, f3 v1, f3 v2, float& t, f2& bary) {
 	const f3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
@@ -78,9 +86,8 @@ MBD bool tri_test(const FastRay& r, f3 v0, f3 v1, f3 v2, float& t, f2& bary) {
 	float V = Ax * Cy - Ay * Cx;
 	float W = Bx * Ay - By * Ax;
 	if(U == 0.0f || V == 0.0f || W == 0.0f) {
-		U = float(__dsub_rn(__dmul_rn(double(Cx), double(By)), __dmul_rn(double(Cy), double(Bx))));
-		V = float(__dsub_rn(__dmul_rn(double(Ax), double(Cy)), __dmul_rn(double(Ay), double(Cx))));
-		W = float(__dsub_rn(__dmul_rn(double(Bx), double(Ay)), __dmul_rn(double(By), double(Ax))));
+		const float3 uvw = edge_functions_double(Ax, Ay, Bx, By, Cx, Cy);
+		U = uvw.x; V = uvw.y; W = uvw.z;
 	}
 	if((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
 	const float det = U + V + W;

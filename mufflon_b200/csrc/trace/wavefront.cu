@@ -52,27 +52,6 @@ MBD unsigned warp_reserve(unsigned* counter, unsigned want) {
 	return base + g.thread_rank() * want;
 }
 
-MBD void flush_counters(const LocalCounters& cnt, TraceCounters* out) {
-	unsigned long long rays = cnt.rays, shadow = cnt.shadow, nodes = cnt.nodes, prims = cnt.prims, inst = cnt.instances;
-	unsigned errs = cnt.errors;
-	for(int o = 16; o > 0; o >>= 1) {
-		rays += __shfl_down_sync(0xffffffffu, rays, o);
-		shadow += __shfl_down_sync(0xffffffffu, shadow, o);
-		nodes += __shfl_down_sync(0xffffffffu, nodes, o);
-		prims += __shfl_down_sync(0xffffffffu, prims, o);
-		inst += __shfl_down_sync(0xffffffffu, inst, o);
-		errs += __shfl_down_sync(0xffffffffu, errs, o);
-	}
-	if((threadIdx.x & 31u) == 0) {
-		if(rays) atomicAdd(&out->rays, rays);
-		if(shadow) atomicAdd(&out->shadowRays, shadow);
-		if(nodes) atomicAdd(&out->nodeVisits, nodes);
-		if(prims) atomicAdd(&out->primTests, prims);
-		if(inst) atomicAdd(&out->instanceVisits, inst);
-		if(errs) atomicAdd(&out->errors, errs);
-	}
-}
-
 __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t numPixels, uint32_t width) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= numPixels) return;
@@ -104,74 +83,124 @@ __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t n
 	W.qDir[0][slot] = pack(dir, 0.0f);
 }
 
-__global__ void __launch_bounds__(128) k_extend(const DScene S, WfState W, int q, int workIdx, TraceCounters* counters) {
-	uint2 stack[WIDE_STACK];
-	LocalCounters cnt;
-	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
-	const unsigned lane = threadIdx.x & 31u;
-	for(;;) {
-		unsigned base = 0;
-		if(lane == 0) base = atomicAdd(W.counters + C_WORK + workIdx, 32u);
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if(base >= count) break;
-		const unsigned slot = base + lane;
-		if(slot < count) {
-			const float4 o = W.qOrg[q][slot], d = W.qDir[q][slot];
-			const HitRec h = closest_hit_wide(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, cnt, stack);
-			W.qHit[q][slot] = make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x);
-			W.qHitSpy[q][slot] = h.sp.y;
-		}
-	}
-	flush_counters(cnt, counters);
+// Block-wide traversal statistics in shared memory, one set per ray kind.
+struct BlockStats { unsigned long long v[2][6]; };
+MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
+	if(c.nodes) atomicAdd(&b.v[kind][0], (unsigned long long)c.nodes);
+	if(c.prims) atomicAdd(&b.v[kind][1], (unsigned long long)c.prims);
+	if(c.instances) atomicAdd(&b.v[kind][2], (unsigned long long)c.instances);
+	atomicAdd(&b.v[kind][3], 1ull);
+	if(c.errors) atomicAdd(&b.v[kind][5], (unsigned long long)c.errors);
 }
 
-__global__ void __launch_bounds__(128) k_shadow(const DScene S, WfState W, int neeCount, int workIdx, TraceCounters* counters) {
+// Persistent traversal of one bounce: the extension rays of queue q (closest
+// hit) and the shadow-ray groups written by the previous shade (any hit; one
+// lane runs a path's neeCount rays in order and adds the unoccluded
+// contributions in that order). Work items are fetched one per lane with one
+// atomic per group of idle lanes, and a lane whose ray is finished takes the
+// next item at once, so the lanes of a warp stay busy until the queues are
+// drained. Every loop iteration runs one traversal step in every busy lane.
+// Queue entries are read and written with streaming (evict-first) accesses so
+// that they do not displace the hierarchies from L2.
+template < int MINB >
+__global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, int q, int neeCount, int workIdx,
+                                                     TraceCounters* counters) {
+	namespace cg = cooperative_groups;
+	__shared__ BlockStats stats;
+	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
+	__syncthreads();
 	uint2 stack[WIDE_STACK];
 	LocalCounters cnt;
-	const unsigned groups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW) / unsigned(neeCount);
-	const unsigned lane = threadIdx.x & 31u;
+	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW) / unsigned(neeCount);
+	const unsigned total = nExt + nGroups;
+	WideTracer t;
+	bool active = false, exhausted = false;
+	unsigned item = 0;
+	int path = 0, ray = 0;
+	f3 radiance = make3(0.0f, 0.0f, 0.0f);
+	float radW = 0.0f;
 	for(;;) {
-		unsigned base = 0;
-		if(lane == 0) base = atomicAdd(W.counters + C_WORK + workIdx, 32u);
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if(base >= groups) break;
-		const unsigned g = base + lane;
-		if(g < groups) {
-			const int p = W.sPath[g * neeCount];
-			float4 acc = W.rad[p];
-			f3 radiance = f4to3(acc);
-			for(int i = 0; i < neeCount; ++i) {
-				const unsigned slot = g * neeCount + i;
-				const float4 o = W.sOrg[slot];
-				if(!(o.w > 0.0f)) continue; // no contribution in this slot
-				const float4 d = W.sDir[slot];
-				if(!occluded_wide(S, f4to3(o), f4to3(d), o.w, cnt, stack))
-					radiance = contribute(radiance, f4to3(W.sContrib[slot]));
+		bool seek = false; // look for the next shadow ray of the current group
+		if(!active && !exhausted) {
+			cg::coalesced_group g = cg::coalesced_threads();
+			unsigned base = 0;
+			if(g.thread_rank() == 0) base = atomicAdd(W.counters + C_WORK + workIdx, g.size());
+			item = g.shfl(base, 0) + g.thread_rank();
+			if(item >= total) {
+				exhausted = true;
+			} else if(item < nExt) {
+				const float4 o = __ldcs(W.qOrg[q] + item), d = __ldcs(W.qDir[q] + item);
+				cnt = LocalCounters();
+				t.init(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
+				active = true;
+			} else {
+				path = __ldcs(W.sPath + (item - nExt) * unsigned(neeCount));
+				const float4 acc = W.rad[path];
+				radiance = f4to3(acc);
+				radW = acc.w;
+				ray = 0;
+				seek = true;
 			}
-			W.rad[p] = pack(radiance, acc.w);
+		}
+		if(__all_sync(0xffffffffu, exhausted)) break;
+		if(active && t.step(S, cnt, stack)) {
+			if(item < nExt) {
+				stats_add(stats, 0, cnt);
+				const HitRec& h = t.best;
+				__stcs(W.qHit[q] + item, make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x));
+				__stcs(W.qHitSpy[q] + item, h.sp.y);
+				active = false;
+			} else {
+				stats_add(stats, 1, cnt);
+				const unsigned slot = (item - nExt) * unsigned(neeCount) + unsigned(ray);
+				if(!t.occluded) radiance = contribute(radiance, f4to3(__ldcs(W.sContrib + slot)));
+				++ray;
+				seek = true;
+			}
+		}
+		if(seek) {
+			// next non-empty slot of the group, or write the group's radiance
+			active = false;
+			const unsigned g0 = (item - nExt) * unsigned(neeCount);
+			for(; ray < neeCount; ++ray) {
+				const float4 o = __ldcs(W.sOrg + g0 + unsigned(ray));
+				if(!(o.w > 0.0f)) continue;
+				const float4 d = __ldcs(W.sDir + g0 + unsigned(ray));
+				cnt = LocalCounters();
+				t.init(S, f4to3(o), f4to3(d), o.w, true, cnt);
+				active = true;
+				break;
+			}
+			if(!active) W.rad[path] = pack(radiance, radW);
 		}
 	}
-	flush_counters(cnt, counters);
+	__syncthreads();
+	if(threadIdx.x < 2) {
+		TraceCounters* out = counters + threadIdx.x;
+		const unsigned long long* v = stats.v[threadIdx.x];
+		if(v[3]) {
+			atomicAdd(&out->rays, v[3]);
+			if(threadIdx.x == 1) atomicAdd(&out->shadowRays, v[3]);
+			atomicAdd(&out->nodeVisits, v[0]);
+			atomicAdd(&out->primTests, v[1]);
+			atomicAdd(&out->instanceVisits, v[2]);
+		}
+		if(v[5]) atomicAdd(&out->errors, unsigned(v[5]));
+	}
 }
 
-__global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P, WfState W, int q, int bounce) {
-	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
-	const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
-	if(slot >= count) return;
-	const int p = W.qPath[q][slot];
-	const f3 origin = f4to3(W.qOrg[q][slot]);
-	const f3 dir = f4to3(W.qDir[q][slot]);
-	const float4 hh = W.qHit[q][slot];
-	HitRec hr;
-	hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
-	hr.sp = make2(hh.w, W.qHitSpy[q][slot]);
-	hr.has = hr.inst >= 0;
-	const float4 tp = W.thrPdf[p];
-	f3 throughput = f4to3(tp);
-	const float pdfF = tp.w;
-	const float4 ra = W.rad[p];
-	f3 radiance = f4to3(ra);
-	// -- the new vertex (random_walk.hpp:88-111)
+// One vertex of pt_sample (pt_common.hpp:75-156, random_walk.hpp:38-113):
+// the vertex hit by (origin, dir) at bounce `bounce`, its emission with MIS,
+// then (if the path continues) next-event estimation and the BSDF sample,
+// Russian roulette and the next ray. Next-event samples with a non-zero
+// contribution are handed to shadow(i, origin, dir, length, contribution) in
+// the order i of pt_sample. Returns true and the next ray if the path goes on.
+// The generator `rng` is advanced exactly as pt_sample advances it.
+template < class ShadowFn >
+MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
+                      f3& throughput, float& pdfF, f3& radiance, u64& rng, float2* hit0, f3& nextO, f3& nextD,
+                      ShadowFn&& shadow) {
 	bool surface = false;
 	f3 position = make3(0.0f, 0.0f, 0.0f), incidentEncoded;
 	float incidentPdf;
@@ -190,7 +219,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P,
 		const float inCosAbs = fabsf(dot(dir, ts.shadingN));
 		incidentPdf = __fdiv_rn(pdfF * fabsf(inCosAbs), hit.distance * hit.distance);
 	}
-	if(bounce == 0) W.hit0[p] = make_float2(float(surface ? hit.inst : -1), float(surface ? hit.prim : -1));
+	if(bounce == 0 && hit0) *hit0 = make_float2(float(surface ? hit.inst : -1), float(surface ? hit.prim : -1));
 	const int pathLen = bounce + 1;
 	// -- emission (pt_common.hpp:139-153)
 	if(pathLen >= P.minPathLength) {
@@ -219,14 +248,11 @@ __global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P,
 		}
 		radiance = contribute(radiance, throughput * emission);
 	}
-	W.rad[p] = pack(radiance, ra.w);
-	if(!surface || !(pathLen < P.maxPathLength)) return;
+	if(!surface || !(pathLen < P.maxPathLength)) return false;
 	// -- next loop iteration of pt_sample: next-event estimation
-	u64 rng = W.rng[p];
 	const f3 incident = incident_direction(incidentEncoded);
 	if(pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
 		const u64 neeSeed = pcg_next(rng);
-		unsigned base = 0xFFFFFFFFu;
 		for(int i = 0; i < P.neeCount; ++i) {
 			const u64 r = pcg_next(rng);
 			const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
@@ -241,13 +267,7 @@ __global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P,
 				const f3 c = ((throughput * val.cosOut) * rad) * mis;
 				f3 so, sd; float stmax;
 				shadow_ray(position, nee.position, ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
-				if(base == 0xFFFFFFFFu) {
-					base = atomicAdd(W.counters + C_SHADOW, unsigned(P.neeCount));
-					for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
-				}
-				W.sOrg[base + i] = pack(so, stmax);
-				W.sDir[base + i] = pack(sd, 0.0f);
-				W.sContrib[base + i] = pack(c, 0.0f);
+				shadow(i, so, sd, stmax, c);
 			}
 		}
 	}
@@ -255,23 +275,129 @@ __global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P,
 	const u64 x0 = pcg_next(rng), x1 = pcg_next(rng);
 	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
 	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
-	W.rng[p] = rng;
-	const PathSample s = material_sample(ts, mat, incident, ru0, ru1, x1);
-	if(!s.valid) return;
-	throughput = throughput * s.throughput;
+	const PathSample smp = material_sample(ts, mat, incident, ru0, ru1, x1);
+	if(!smp.valid) return false;
+	throughput = throughput * smp.throughput;
 	if(pathLen >= P.rrStartDepth) {
 		const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
-		if(rr >= cp) return;
+		if(rr >= cp) return false;
 		throughput = throughput / cp;
 	}
-	W.thrPdf[p] = pack(throughput, s.pdfF);
-	f3 o = position;
-	add_epsilon(o, s.excident, ts.geoN);
+	pdfF = smp.pdfF;
+	nextO = position;
+	add_epsilon(nextO, smp.excident, ts.geoN);
+	nextD = smp.excident;
+	return true;
+}
+
+// Shade stage of the wavefront: one thread per queued path. Next-event rays go
+// to the shadow queue (neeCount consecutive slots per path, allocated when
+// the first one is needed), the next ray to the other extension queue.
+__global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P, WfState W, int q, int bounce) {
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
+	if(slot >= count) return;
+	const int p = __ldcs(W.qPath[q] + slot);
+	const f3 origin = f4to3(__ldcs(W.qOrg[q] + slot));
+	const f3 dir = f4to3(__ldcs(W.qDir[q] + slot));
+	const float4 hh = __ldcs(W.qHit[q] + slot);
+	HitRec hr;
+	hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
+	hr.sp = make2(hh.w, __ldcs(W.qHitSpy[q] + slot));
+	hr.has = hr.inst >= 0;
+	const float4 tp = W.thrPdf[p];
+	f3 throughput = f4to3(tp);
+	float pdfF = tp.w;
+	const float4 ra = W.rad[p];
+	f3 radiance = f4to3(ra);
+	u64 rng = W.rng[p];
+	const u64 rng0 = rng;
+	unsigned base = 0xFFFFFFFFu;
+	f3 nextO, nextD;
+	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
+		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c) {
+			if(base == 0xFFFFFFFFu) {
+				base = atomicAdd(W.counters + C_SHADOW, unsigned(P.neeCount));
+				for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
+			}
+			W.sOrg[base + i] = pack(so, stmax);
+			W.sDir[base + i] = pack(sd, 0.0f);
+			W.sContrib[base + i] = pack(c, 0.0f);
+		});
+	W.rad[p] = pack(radiance, ra.w);
+	if(rng != rng0) W.rng[p] = rng;
+	if(!cont) return;
+	W.thrPdf[p] = pack(throughput, pdfF);
 	const int out = q ^ 1;
 	const unsigned nslot = warp_reserve(W.counters + out, 1u);
 	W.qPath[out][nslot] = p;
-	W.qOrg[out][nslot] = pack(o, 0.0f);
-	W.qDir[out][nslot] = pack(s.excident, 0.0f);
+	W.qOrg[out][nslot] = pack(nextO, 0.0f);
+	W.qDir[out][nslot] = pack(nextD, 0.0f);
+}
+
+// Tail of an iteration: persistent threads take the paths of extension queue
+// q (already traced, bounce `bounce`) one at a time and finish each of them in
+// place: shade, trace the next-event rays at once and add their contributions
+// in order, trace the next extension ray, and so on until the path ends. Used
+// once few paths are left, where a separate launch per bounce would be
+// dominated by launch and drain latency.
+template < int MINB >
+__global__ void __launch_bounds__(128, MINB) k_tail(const DScene S, const PtParams P, WfState W, int q, int bounce,
+                                                    int workIdx, TraceCounters* counters) {
+	__shared__ BlockStats stats;
+	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
+	__syncthreads();
+	uint2 stack[WIDE_STACK];
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	for(;;) {
+		const unsigned item = atomicAdd(W.counters + C_WORK + workIdx, 1u);
+		if(item >= count) break;
+		const int p = W.qPath[q][item];
+		f3 origin = f4to3(W.qOrg[q][item]);
+		f3 dir = f4to3(W.qDir[q][item]);
+		const float4 hh = W.qHit[q][item];
+		HitRec hr;
+		hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
+		hr.sp = make2(hh.w, W.qHitSpy[q][item]);
+		hr.has = hr.inst >= 0;
+		const float4 tp = W.thrPdf[p];
+		f3 throughput = f4to3(tp);
+		float pdfF = tp.w;
+		const float4 ra = W.rad[p];
+		f3 radiance = f4to3(ra);
+		u64 rng = W.rng[p];
+		for(int b = bounce;; ++b) {
+			f3 nextO, nextD;
+			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
+				nextO, nextD, [&](int, f3 so, f3 sd, float stmax, f3 c) {
+					LocalCounters cnt;
+					const bool occ = occluded_wide(S, so, sd, stmax, cnt, stack);
+					stats_add(stats, 1, cnt);
+					if(!occ) radiance = contribute(radiance, c);
+				});
+			if(!cont) break;
+			origin = nextO;
+			dir = nextD;
+			LocalCounters cnt;
+			hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
+			stats_add(stats, 0, cnt);
+		}
+		W.rad[p] = pack(radiance, ra.w);
+		W.rng[p] = rng;
+	}
+	__syncthreads();
+	if(threadIdx.x < 2) {
+		TraceCounters* out = counters + threadIdx.x;
+		const unsigned long long* v = stats.v[threadIdx.x];
+		if(v[3]) {
+			atomicAdd(&out->rays, v[3]);
+			if(threadIdx.x == 1) atomicAdd(&out->shadowRays, v[3]);
+			atomicAdd(&out->nodeVisits, v[0]);
+			atomicAdd(&out->primTests, v[1]);
+			atomicAdd(&out->instanceVisits, v[2]);
+		}
+		if(v[5]) atomicAdd(&out->errors, unsigned(v[5]));
+	}
 }
 
 __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
@@ -329,6 +455,31 @@ __global__ void k_occlusion_wide(const DScene S, const float* a, const float* b,
 	}
 }
 
+using TraceFn = void (*)(const DScene, WfState, int, int, int, TraceCounters*);
+struct TraceKernel { TraceFn fn; int blocks; };
+
+int persistent_blocks(const void* fn, int threads);
+
+// The trace kernel compiled for `perSm` resident blocks of 128 threads
+// (register budget 65536 / (128 * perSm)); 0 picks the default.
+TraceKernel trace_kernel(int perSm) {
+	static TraceKernel table[4] = {};
+	static const TraceFn fns[4] = { k_trace<4>, k_trace<5>, k_trace<6>, k_trace<8> };
+	static const int occ[4] = { 4, 5, 6, 8 };
+	int idx = 2;
+	for(int i = 0; i < 4; ++i) if(occ[i] == perSm) idx = i;
+	if(!table[idx].fn) table[idx] = { fns[idx], persistent_blocks(reinterpret_cast<const void*>(fns[idx]), 128) };
+	return table[idx];
+}
+
+using TailFn = void (*)(const DScene, const PtParams, WfState, int, int, int, TraceCounters*);
+struct TailKernel { TailFn fn; int blocks; };
+TailKernel tail_kernel() {
+	static TailKernel k = {};
+	if(!k.fn) k = { k_tail<4>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4>), 128) };
+	return k;
+}
+
 int persistent_blocks(const void* fn, int threads) {
 	int dev = 0, sms = 148, perSm = 4;
 	cudaGetDevice(&dev);
@@ -356,7 +507,8 @@ cudaError_t launch_occlusion_wide(const DScene& S, const float* a, const float* 
 }
 
 cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const RenderState& R, WfState W,
-                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info) {
+                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info, int traceBlocksPerSm,
+                                int wavefrontBounces) {
 	WfLaunchInfo none;
 	WfLaunchInfo& L = info ? *info : none;
 	L.pairsUsed = 0;
@@ -373,15 +525,11 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 	};
 	const uint32_t n = R.width * R.height;
 	if(n == 0) return cudaSuccess;
-	static int extendBlocks = 0, shadowBlocks = 0;
-	if(!extendBlocks) {
-		extendBlocks = persistent_blocks(reinterpret_cast<const void*>(k_extend), 128);
-		shadowBlocks = persistent_blocks(reinterpret_cast<const void*>(k_shadow), 128);
-	}
+	const TraceKernel tk = trace_kernel(traceBlocksPerSm);
 	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
 	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;
 	const unsigned workSlots = WF_COUNTERS - C_WORK;
-	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
+	const unsigned firstClear = unsigned(maxBounces) < workSlots ? unsigned(maxBounces) : workSlots;
 	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);
 	if(e != cudaSuccess) return e;
 	W.rng = R.rngState;
@@ -397,12 +545,15 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 			work = 0;
 		}
 		begin(WF_EXTEND);
-		k_extend<<<extendBlocks, 128, 0, stream>>>(S, W, q, int(work++), counters);
+		tk.fn<<<tk.blocks, 128, 0, stream>>>(S, W, q, neeCount, int(work++), counters);
 		end();
-		if(b > 0) {
-			begin(WF_SHADOW);
-			k_shadow<<<shadowBlocks, 128, 0, stream>>>(S, W, neeCount, int(work++), counters + 1);
+		if(b >= wavefrontBounces && b + 1 < maxBounces) {
+			// few paths are left: finish them in one launch
+			const TailKernel tl = tail_kernel();
+			begin(WF_TAIL);
+			tl.fn<<<tl.blocks, 128, 0, stream>>>(S, P, W, q, b, int(work++), counters);
 			end();
+			break;
 		}
 		// the shade of this bounce appends to the other queue and to the shadow queue
 		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);

@@ -28,7 +28,9 @@ struct WfState {
 // persistent launch (two per bounce); longer paths recycle the work counters.
 constexpr unsigned WF_COUNTERS = 4096;
 
-enum WfStage { WF_CAMERA = 0, WF_EXTEND = 1, WF_SHADOW = 2, WF_SHADE = 3, WF_FINALIZE = 4, WF_STAGES = 5 };
+// WF_EXTEND: the trace launches of the wavefront bounces (extension and
+// shadow rays); WF_TAIL: the launch that finishes the remaining paths.
+enum WfStage { WF_CAMERA = 0, WF_EXTEND = 1, WF_TAIL = 2, WF_SHADE = 3, WF_FINALIZE = 4, WF_STAGES = 5 };
 
 // Host-side launch record of one iteration. With `events` set, a pair of
 // events is recorded around each stage launch (while capacity lasts) and
@@ -43,9 +45,13 @@ struct WfLaunchInfo {
 
 // One iteration (one sample per pixel) of the wavefront path tracer.
 // counters[0] receives the extension rays' traversal counts, counters[1] the
-// shadow rays'.
+// shadow rays'. traceBlocksPerSm selects the register budget of the trace
+// kernel (4, 5, 6 or 8 resident blocks of 128 threads; other values: 6).
+// Bounces 0 .. wavefrontBounces run as separate trace and shade launches;
+// after that one launch finishes every remaining path in place.
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
-                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info);
+                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info,
+                                int traceBlocksPerSm = 0, int wavefrontBounces = 1);
 
 // Closest hits and shadow-ray tests over the compressed 8-wide hierarchies
 // (same arguments as launch_trace_rays / launch_occlusion of pt_api.hpp).

@@ -28,6 +28,8 @@ namespace mb {
 
 constexpr int WIDE_STACK = 64;
 constexpr uint32_t PRIM_GROUP = 0x80000000u;
+// Primitive masks use bits 0..8*leafMax-1; bit 31 tags primitive groups.
+static_assert(8 * WIDE_LEAF_MAX <= 31 && 8 * WIDE_TLAS_LEAF_MAX <= 31, "primitive mask width");
 
 MBD uint32_t octant_flip(f3 d) {
 	return 7u ^ ((d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u));
@@ -36,6 +38,20 @@ MBD uint32_t octant_flip(f3 d) {
 // Byte b (0..3) of w as an exact float: 0x4B0000bb is the float 2^23 + bb.
 MBD float qbyte(uint32_t w, int b) {
 	return __fsub_rn(__int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(b)))), 8388608.0f);
+}
+
+// Out-of-line pieces of the traversal loop that run at most a few times per
+// ray (instance transitions) or rarely (non-triangle primitives); keeping them
+// out of the loop body keeps the loop in the instruction cache.
+static __device__ __noinline__ FastRay make_ray_ool(f3 o, f3 d) { return make_ray(o, d); }
+static __device__ __noinline__ InstRay instance_ray_ool(const DScene& S, uint32_t i, f3 o, f3 d) {
+	return instance_ray(load_w2i(S, i), o, d);
+}
+struct PrimHit { float t; f2 uv; bool hit; };
+static __device__ __noinline__ PrimHit other_prim_test(const DLod* l, FastRay r, int p) {
+	PrimHit h;
+	h.hit = prim_test(*l, r, 0, p, h.t, h.uv);
+	return h;
 }
 
 // Tests the eight child boxes of node `idx`; returns the child's node group
@@ -91,28 +107,49 @@ MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, u
 	pgHits = ph;
 }
 
-// Closest hit (ANY = false; `best` holds the incoming tmax in best.t) or
-// occlusion test (ANY = true; returns true as soon as a primitive is hit
-// before tmaxW). Returns false on stack overflow or a corrupted hierarchy
-// (counted in cnt.errors).
-template < bool ANY >
-MBD bool wide_trace(const DScene& S, f3 wo, f3 wd, float tmaxW, HitRec& best, LocalCounters& cnt, uint2* stack) {
-	if(S.activeInstances <= 0) return false;
-	FastRay r = make_ray(wo, wd);
-	uint32_t flip = octant_flip(wd);
-	float scale = 1.0f;
-	int inst = -1;
-	const DLod* lod = nullptr;
-	const WideNode* nodes = S.tlasWide;
-	uint32_t ngBase = 0, ngImask = 1, ngHits = 0, pgBase = 0, pgHits = 0;
-	int sp = 0, instSp = -1;
-	const bool single = S.activeInstances == 1;
+// Resumable traversal of one ray: init() sets it up, every step() visits at
+// most one node and that node's hit primitives (or enters / leaves an
+// instance), and returns true once the ray is finished. Kernels that refill
+// lanes as soon as their ray finishes call step() from one loop shared by the
+// whole warp.
+struct WideTracer {
+	f3 wo, wd;            // world ray
+	FastRay wr;           // world ray, prepared
+	FastRay r;            // ray of the current level
+	float scale;          // object-space length of a world-space unit
+	float tmaxW;          // shadow rays: world-space segment length
+	HitRec best;          // closest hit so far (best.t holds the incoming tmax)
+	const DLod* lod;
+	const WideNode* nodes;
+	uint32_t flip, ngBase, ngImask, ngHits, pgBase, pgHits;
+	int inst, sp, instSp, steps;
+	bool any, single, occluded, done;
 
-	auto enter = [&](uint32_t i) {
+	MBD void init(const DScene& S, f3 o, f3 d, float tmax, bool anyHit, LocalCounters& cnt) {
+		wo = o; wd = d;
+		tmaxW = tmax;
+		any = anyHit;
+		occluded = false;
+		best.t = tmax; best.inst = -1; best.prim = -1; best.sp = make2(0.0f, 0.0f); best.has = false;
+		sp = 0; instSp = -1; steps = 0; inst = -1; lod = nullptr;
+		scale = 1.0f;
+		ngBase = 0; ngImask = 1; ngHits = 0; pgBase = 0; pgHits = 0;
+		single = S.activeInstances == 1;
+		done = S.activeInstances <= 0;
+		if(done) return;
+		wr = make_ray_ool(o, d);
+		r = wr;
+		flip = octant_flip(d);
+		nodes = S.tlasWide;
+		if(single) enter(S, uint32_t(S.validInstance), cnt);
+		else ngHits = S.tlasNumWide > 0 ? (1u << flip) : 0u;
+	}
+
+	MBD void enter(const DScene& S, uint32_t i, LocalCounters& cnt) {
 		++cnt.instances;
 		inst = int(i);
 		lod = S.lods + __ldg(S.instanceLod + i);
-		const InstRay ir = instance_ray(load_w2i(S, i), wo, wd);
+		const InstRay ir = instance_ray_ool(S, i, wo, wd);
 		r = ir.ray;
 		scale = ir.scale;
 		flip = octant_flip(r.d);
@@ -122,24 +159,22 @@ MBD bool wide_trace(const DScene& S, f3 wo, f3 wd, float tmaxW, HitRec& best, Lo
 		if(np >= 2) ngHits = 1u << flip; // the root, slot 0 of a virtual parent
 		else if(np == 1) pgHits = 1u;
 		instSp = sp;
-	};
+	}
 
-	if(single) enter(uint32_t(S.validInstance));
-	else ngHits = S.tlasNumWide > 0 ? (1u << flip) : 0u;
-
-	for(int guard = 0;; ++guard) {
-		if(guard >= MAX_TRAVERSAL_STEPS) { ++cnt.errors; return false; }
+	MBD bool step(const DScene& S, LocalCounters& cnt, uint2* stack) {
+		if(done) return true;
+		if(++steps > MAX_TRAVERSAL_STEPS) { ++cnt.errors; done = true; return true; }
 		if(ngHits) {
 			const uint32_t k = uint32_t(__ffs(int(ngHits)) - 1);
 			ngHits &= ngHits - 1u;
 			const uint32_t s = k ^ flip;
 			const uint32_t child = ngBase + uint32_t(__popc(ngImask & ((1u << s) - 1u)));
 			if(ngHits) {
-				if(sp >= WIDE_STACK) { ++cnt.errors; return false; }
+				if(sp >= WIDE_STACK) { ++cnt.errors; done = true; return true; }
 				stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
 			}
 			++cnt.nodes;
-			const float tmaxBox = ANY ? tmaxW * scale * BOX_SLACK : best.t * scale * BOX_SLACK;
+			const float tmaxBox = (any ? tmaxW : best.t) * scale * BOX_SLACK;
 			wide_node_test(nodes, child, r, flip, tmaxBox, ngBase, ngImask, ngHits, pgBase, pgHits);
 		}
 		if(pgHits) {
@@ -160,11 +195,12 @@ MBD bool wide_trace(const DScene& S, f3 wo, f3 wd, float tmaxW, HitRec& best, Lo
 						const float4 b = __ldg(s4 + 1), c = __ldg(s4 + 2);
 						hit = tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, uv) && t > 0.0f;
 					} else {
-						hit = prim_test(*lod, r, 0, p, t, uv);
+						const PrimHit ph = other_prim_test(lod, r, p);
+						hit = ph.hit; t = ph.t; uv = ph.uv;
 					}
 					if(hit) {
-						if(ANY) {
-							if(t < tmaxW * scale) return true;
+						if(any) {
+							if(t < tmaxW * scale) { occluded = true; done = true; return true; }
 						} else {
 							const float tw = __fdiv_rn(t, scale);
 							if(better(tw, inst, p, best)) { best.t = tw; best.inst = inst; best.prim = p; best.sp = uv; best.has = true; }
@@ -176,43 +212,47 @@ MBD bool wide_trace(const DScene& S, f3 wo, f3 wd, float tmaxW, HitRec& best, Lo
 				const uint32_t j = uint32_t(__ffs(int(pgHits)) - 1);
 				pgHits &= pgHits - 1u;
 				const uint32_t id = uint32_t(__ldg(S.tlasWidePrims + pgBase + j));
-				if(sp + 2 > WIDE_STACK) { ++cnt.errors; return false; }
+				if(sp + 2 > WIDE_STACK) { ++cnt.errors; done = true; return true; }
 				if(ngHits) stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
 				if(pgHits) stack[sp++] = make_uint2(pgBase, pgHits | PRIM_GROUP);
-				enter(id);
-				continue;
+				enter(S, id, cnt);
+				return false;
 			}
 		}
 		if(!ngHits) {
 			if(instSp >= 0 && sp == instSp) {
-				if(single) break;
-				r = make_ray(wo, wd);
+				if(single) { done = true; return true; }
+				r = wr;
 				flip = octant_flip(wd);
 				scale = 1.0f;
 				nodes = S.tlasWide;
 				instSp = -1;
 			}
-			if(sp == 0) break;
+			if(sp == 0) { done = true; return true; }
 			const uint2 e = stack[--sp];
-			if(e.y & PRIM_GROUP) { pgBase = e.x; pgHits = e.y & 0xFFFFu; }
+			if(e.y & PRIM_GROUP) { pgBase = e.x; pgHits = e.y & ~PRIM_GROUP; }
 			else { ngBase = e.x; ngImask = e.y & 0xFFu; ngHits = e.y >> 8; }
 		}
+		return false;
 	}
-	return !ANY;
-}
+};
 
+// Closest hit of a world-space ray whose origin is already offset.
 MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
 	++cnt.rays;
-	HitRec best;
-	best.t = tmax; best.inst = -1; best.prim = -1; best.sp = make2(0.0f, 0.0f); best.has = false;
-	wide_trace<false>(S, o, dir, tmax, best, cnt, stack);
-	return best;
+	WideTracer t;
+	t.init(S, o, dir, tmax, false, cnt);
+	while(!t.step(S, cnt, stack)) {}
+	return t.best;
 }
 
+// Occlusion of a prepared shadow ray (origin offset, unit direction, length tmax).
 MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
 	++cnt.rays; ++cnt.shadow;
-	HitRec unused;
-	return wide_trace<true>(S, a, dir, tmax, unused, cnt, stack);
+	WideTracer t;
+	t.init(S, a, dir, tmax, true, cnt);
+	while(!t.step(S, cnt, stack)) {}
+	return t.occluded;
 }
 
 } // namespace mb

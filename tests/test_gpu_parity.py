@@ -105,7 +105,7 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
 # kernel over the binary (reference-layout) hierarchies.
 KERNELS = {"wavefront": 0, "megakernel": 1}
 DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
-                  "RR start depth": 0, "Megakernel": 0}
+                  "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 1}
 
 
 def _load(dll, spec):
@@ -244,6 +244,24 @@ def test_pt_multi_nee_min_path_parity(dll, oracle, kernel):
     assert np.array_equal(gh, oh)
     assert rel_rmse(gr, orad) <= RMSE_TOL
     assert orad.mean() > 0.01
+
+
+@pytest.mark.parametrize("wavefront_bounces", [0, 1, 3, 100])
+def test_pt_schedule_parity(dll, oracle, wavefront_bounces):
+    """Any split between per-bounce stage launches and the path-finishing launch gives the oracle's bits."""
+    spec = scenes.cornell_box(5, 80, 80)
+    _load(dll, spec)
+    dll.render_enable_render_target("Radiance", False)
+    dll.render_enable_render_target("Hit ID", False)
+    for name, value in {"Wavefront bounces": wavefront_bounces, "NEE count": 2, "Max. path length": 9,
+                        "RR start depth": 2, "Min. path length": 1}.items():
+        assert dll.renderer_set_parameter_int(name, value)
+    pt = oracle.OraclePathTracer(oracle.OracleScene(spec), seed=0, min_path=1, max_path=9, nee_count=2, rr_start=2)
+    for _ in range(2):
+        dll.render_iterate()
+        pt.iterate()
+    assert np.array_equal(dll.get_target_image("Hit ID"), pt.target("Hit ID"))
+    assert rel_rmse(dll.get_target_image("Radiance"), pt.target("Radiance")) <= RMSE_TOL
 
 
 def test_pt_long_paths_parity(dll, oracle):
