@@ -164,7 +164,7 @@ struct RendererState {
 	size_t wfPixels = 0;
 	int32_t stageTiming = 0;      // record device time per stage kernel
 	int32_t traceBlocksPerSm = 0; // register budget of the wavefront trace kernel (0: default)
-	int32_t wavefrontBounces = 1; // bounces run as separate stage launches before the tail launch
+	int32_t wavefrontBounces = 2; // bounces run as separate stage launches before the tail launch
 	std::vector<cudaEvent_t> stageEvents;
 	std::vector<unsigned char> stageKinds;
 	float stageMs[WF_STAGES] = {};

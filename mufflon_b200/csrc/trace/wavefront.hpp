@@ -51,7 +51,7 @@ struct WfLaunchInfo {
 // after that one launch finishes every remaining path in place.
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
                                 TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info,
-                                int traceBlocksPerSm = 0, int wavefrontBounces = 1);
+                                int traceBlocksPerSm = 0, int wavefrontBounces = 2);
 
 // Closest hits and shadow-ray tests over the compressed 8-wide hierarchies
 // (same arguments as launch_trace_rays / launch_occlusion of pt_api.hpp).

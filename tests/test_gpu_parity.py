@@ -105,7 +105,7 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
 # kernel over the binary (reference-layout) hierarchies.
 KERNELS = {"wavefront": 0, "megakernel": 1}
 DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
-                  "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 1}
+                  "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 2}
 
 
 def _load(dll, spec):
