@@ -55,6 +55,7 @@ const ParamDesc PT_PARAMS[] = {
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
 	{ "Stage timing", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
+	{ "Trace refill lanes", PARAM_INT },
 };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
@@ -71,6 +72,7 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "Stage timing")) return &r.stageTiming;
 	if(!std::strcmp(name, "Trace blocks per SM")) return &r.traceBlocksPerSm;
 	if(!std::strcmp(name, "Wavefront bounces")) return &r.wavefrontBounces;
+	if(!std::strcmp(name, "Trace refill lanes")) return &r.refillLanes;
 	return nullptr;
 }
 
@@ -852,8 +854,13 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	}
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
 	if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
-	else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, r.traceBlocksPerSm,
-	                                    r.wavefrontBounces));
+	else {
+		WfTuning tune;
+		tune.traceBlocksPerSm = r.traceBlocksPerSm;
+		tune.wavefrontBounces = r.wavefrontBounces;
+		tune.refillLanes = r.refillLanes;
+		CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, tune));
+	}
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters both[2];
 	CHECK_CUDA(cudaMemcpyAsync(both, r.counters, 2 * sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));

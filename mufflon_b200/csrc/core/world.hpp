@@ -163,8 +163,9 @@ struct RendererState {
 	int32_t wfNee = 0;
 	size_t wfPixels = 0;
 	int32_t stageTiming = 0;      // record device time per stage kernel
-	int32_t traceBlocksPerSm = 0; // register budget of the wavefront trace kernel (0: default)
+	int32_t traceBlocksPerSm = 6; // register budget of the wavefront trace kernel
 	int32_t wavefrontBounces = 2; // bounces run as separate stage launches before the tail launch
+	int32_t refillLanes = 32;     // idle trace lanes refilled together
 	std::vector<cudaEvent_t> stageEvents;
 	std::vector<unsigned char> stageKinds;
 	float stageMs[WF_STAGES] = {};

@@ -96,16 +96,16 @@ MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
 // Persistent traversal of one bounce: the extension rays of queue q (closest
 // hit) and the shadow-ray groups written by the previous shade (any hit; one
 // lane runs a path's neeCount rays in order and adds the unoccluded
-// contributions in that order). Work items are fetched one per lane with one
-// atomic per group of idle lanes, and a lane whose ray is finished takes the
-// next item at once, so the lanes of a warp stay busy until the queues are
-// drained. Every loop iteration runs one traversal step in every busy lane.
+// contributions in that order). Idle lanes fetch work items with one atomic
+// per warp once at least `refillLanes` of them are idle (or none is busy);
+// with 32 a warp takes 32 new rays whenever all of its rays are finished,
+// which measured fastest: the ray set-up then runs with all lanes at once.
+// Every loop iteration runs one traversal step in every busy lane.
 // Queue entries are read and written with streaming (evict-first) accesses so
 // that they do not displace the hierarchies from L2.
 template < int MINB >
 __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, int q, int neeCount, int workIdx,
-                                                     TraceCounters* counters) {
-	namespace cg = cooperative_groups;
+                                                     TraceCounters* counters, int refillLanes) {
 	__shared__ BlockStats stats;
 	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
 	__syncthreads();
@@ -120,27 +120,34 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, 
 	int path = 0, ray = 0;
 	f3 radiance = make3(0.0f, 0.0f, 0.0f);
 	float radW = 0.0f;
+	const unsigned lane = threadIdx.x & 31u;
 	for(;;) {
 		bool seek = false; // look for the next shadow ray of the current group
-		if(!active && !exhausted) {
-			cg::coalesced_group g = cg::coalesced_threads();
+		// Refill idle lanes together once enough of them are idle (or none is
+		// busy), so that ray set-up runs with many lanes at a time.
+		const unsigned busy = __ballot_sync(0xffffffffu, active);
+		const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+		if(idle && (__popc(idle) >= refillLanes || !busy)) {
 			unsigned base = 0;
-			if(g.thread_rank() == 0) base = atomicAdd(W.counters + C_WORK + workIdx, g.size());
-			item = g.shfl(base, 0) + g.thread_rank();
-			if(item >= total) {
-				exhausted = true;
-			} else if(item < nExt) {
-				const float4 o = __ldcs(W.qOrg[q] + item), d = __ldcs(W.qDir[q] + item);
-				cnt = LocalCounters();
-				t.init(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
-				active = true;
-			} else {
-				path = __ldcs(W.sPath + (item - nExt) * unsigned(neeCount));
-				const float4 acc = W.rad[path];
-				radiance = f4to3(acc);
-				radW = acc.w;
-				ray = 0;
-				seek = true;
+			if(lane == unsigned(__ffs(int(idle)) - 1)) base = atomicAdd(W.counters + C_WORK + workIdx, unsigned(__popc(idle)));
+			base = __shfl_sync(0xffffffffu, base, __ffs(int(idle)) - 1);
+			if(idle & (1u << lane)) {
+				item = base + unsigned(__popc(idle & ((1u << lane) - 1u)));
+				if(item >= total) {
+					exhausted = true;
+				} else if(item < nExt) {
+					const float4 o = __ldcs(W.qOrg[q] + item), d = __ldcs(W.qDir[q] + item);
+					cnt = LocalCounters();
+					t.init(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
+					active = true;
+				} else {
+					path = __ldcs(W.sPath + (item - nExt) * unsigned(neeCount));
+					const float4 acc = W.rad[path];
+					radiance = f4to3(acc);
+					radW = acc.w;
+					ray = 0;
+					seek = true;
+				}
 			}
 		}
 		if(__all_sync(0xffffffffu, exhausted)) break;
@@ -455,7 +462,7 @@ __global__ void k_occlusion_wide(const DScene S, const float* a, const float* b,
 	}
 }
 
-using TraceFn = void (*)(const DScene, WfState, int, int, int, TraceCounters*);
+using TraceFn = void (*)(const DScene, WfState, int, int, int, TraceCounters*, int);
 struct TraceKernel { TraceFn fn; int blocks; };
 
 int persistent_blocks(const void* fn, int threads);
@@ -507,8 +514,9 @@ cudaError_t launch_occlusion_wide(const DScene& S, const float* a, const float* 
 }
 
 cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const RenderState& R, WfState W,
-                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info, int traceBlocksPerSm,
-                                int wavefrontBounces) {
+                                TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info, const WfTuning& tuning) {
+	const int traceBlocksPerSm = tuning.traceBlocksPerSm, wavefrontBounces = tuning.wavefrontBounces;
+	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
 	WfLaunchInfo none;
 	WfLaunchInfo& L = info ? *info : none;
 	L.pairsUsed = 0;
@@ -545,7 +553,7 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 			work = 0;
 		}
 		begin(WF_EXTEND);
-		tk.fn<<<tk.blocks, 128, 0, stream>>>(S, W, q, neeCount, int(work++), counters);
+		tk.fn<<<tk.blocks, 128, 0, stream>>>(S, W, q, neeCount, int(work++), counters, refillLanes);
 		end();
 		if(b >= wavefrontBounces && b + 1 < maxBounces) {
 			// few paths are left: finish them in one launch

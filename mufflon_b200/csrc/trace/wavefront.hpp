@@ -45,13 +45,16 @@ struct WfLaunchInfo {
 
 // One iteration (one sample per pixel) of the wavefront path tracer.
 // counters[0] receives the extension rays' traversal counts, counters[1] the
-// shadow rays'. traceBlocksPerSm selects the register budget of the trace
-// kernel (4, 5, 6 or 8 resident blocks of 128 threads; other values: 6).
-// Bounces 0 .. wavefrontBounces run as separate trace and shade launches;
-// after that one launch finishes every remaining path in place.
+// shadow rays'.
+struct WfTuning {
+	int traceBlocksPerSm = 6;  // register budget of the trace kernel: 4, 5, 6 or 8 resident blocks of 128 threads
+	int wavefrontBounces = 2;  // bounces 0 .. this run as separate trace and shade launches, then one
+	                           // launch finishes every remaining path in place
+	int refillLanes = 32;      // idle lanes of a trace warp are refilled together once this many are idle (1..32)
+};
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
                                 TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info,
-                                int traceBlocksPerSm = 0, int wavefrontBounces = 2);
+                                const WfTuning& tuning = WfTuning());
 
 // Closest hits and shadow-ray tests over the compressed 8-wide hierarchies
 // (same arguments as launch_trace_rays / launch_occlusion of pt_api.hpp).

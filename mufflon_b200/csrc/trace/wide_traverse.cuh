@@ -235,6 +235,7 @@ struct WideTracer {
 		}
 		return false;
 	}
+
 };
 
 // Closest hit of a world-space ray whose origin is already offset.
