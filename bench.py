@@ -45,7 +45,7 @@ WORKLOAD = "displaced_icosphere_1310720tri_1920x1080_16spp_depth10"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--subdiv", type=int, default=8)
@@ -197,6 +197,51 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per algorithmic byte of the traversal launches, from an ncu
+# capture of the bounce-1 k_trace launch of this workload.
+TRACE_DRAM_PER_ALG_BYTE = 0.17
+LBVH_STAGES = ["morton", "sort", "emit", "merge", "mark", "scan", "compact", "soup", "wide"]
+# Algorithmic bytes per triangle of the reference's build stages (Morton 60,
+# sort 200, emit 32, merge 148, mark 32, scan 8, compact 68, soup 96), and of
+# the 8-wide conversion (binary boxes 32 B read, primitive ids 8 B, soup 36 B
+# read + 48 B written).
+LBVH_BYTES_PER_PRIM = 644
+WIDE_BYTES_PER_PRIM = 124
+
+
+def lbvh_build_measurement(dll, lod, torch, reps=10):
+    """Device-resident LBVH build of the workload's mesh (CUDA events)."""
+    import ctypes as C
+    v = torch.from_numpy(np.ascontiguousarray(lod.vertices, np.float32)).cuda()
+    idx = torch.from_numpy(np.ascontiguousarray(lod.triangles.reshape(-1).astype(np.int32))).cuda()
+    aabb = np.concatenate([lod.vertices.min(0), lod.vertices.max(0)]).astype(np.float32)
+    n = len(lod.triangles)
+    ni = C.c_int32(0)
+    ms = C.c_float(0.0)
+    stages = np.zeros(9, np.float32)
+    tot = np.zeros(9)
+    total = 0.0
+    for it in range(3 + reps):
+        ok = dll.core.mufflon_lbvh_build_device(C.c_void_p(v.data_ptr()), C.c_void_p(idx.data_ptr()), n, 0, None, 0,
+                                                aabb.ctypes.data, C.byref(ni), C.byref(ms), stages.ctypes.data)
+        if not ok:
+            raise RuntimeError(dll.core.core_get_dll_error())
+        if it >= 3:
+            tot += stages
+            total += ms.value
+    tot /= reps
+    ref_ms = float(tot[:8].sum())
+    gbs = n * LBVH_BYTES_PER_PRIM / (ref_ms * 1e-3) / 1e9
+    peaks, kind = measured_peaks()
+    return {"prims": n, "build_ms": round(total / reps, 4),
+            "stage_ms": {k: round(float(t), 4) for k, t in zip(LBVH_STAGES, tot)},
+            "reference_stages_ms": round(ref_ms, 4), "alg_bytes_per_prim": LBVH_BYTES_PER_PRIM,
+            "achieved_gbs": round(gbs, 1), "frac_of_hbm": round(gbs / peaks["hbm_gbs"], 4),
+            "wide_alg_bytes_per_prim": WIDE_BYTES_PER_PRIM,
+            "wide_gbs": round(n * WIDE_BYTES_PER_PRIM / (float(tot[8]) * 1e-3) / 1e9, 1),
+            "num_internal_after_collapse": int(ni.value)}
+
+
 def run_b200(args):
     rank, world, local = dist_env()
     import torch
@@ -205,14 +250,14 @@ def run_b200(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from mufflon_b200 import bindings, build, scenes
+    from mufflon_b200 import bindings, build, distributed, scenes
     build.build()
     spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
     dll = bindings.DllInterface()
     bindings.load_scene_spec(dll, spec)
     assert dll.render_enable_renderer(0, 0)
     assert dll.renderer_set_parameter_int("Max. path length", MAX_PATH)
-    assert dll.renderer_set_parameter_int("Seed", rank)
+    assert dll.renderer_set_parameter_int("Seed", distributed.rank_seed(0, rank))
 
     def frame():
         rays = shadow = nodes = prims = inst = 0
@@ -287,9 +332,8 @@ def run_b200(args):
             e2e_rays += dll.render_stats()["rays"]
         img = dll.get_target_image("Radiance")
         if world > 1:
-            ti = torch.from_numpy(img).cuda()
-            torch.distributed.all_reduce(ti)
-            img = (ti / world).cpu().numpy()
+            ti, _ = distributed.combine_images(torch.from_numpy(img).cuda(), SPP_PER_FRAME)
+            img = ti.cpu().numpy()
         t_e2e += time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([t_e2e], device="cuda")
@@ -307,30 +351,41 @@ def run_b200(args):
     # rows 48 B + LoD index 4 B + the LoD's hierarchy pointers); per extension
     # ray its queue entry 32 B in and 20 B out, per shadow ray 48 B in.
     st = stage_frame()
-    trace_launches = SPP_PER_FRAME * MAX_PATH
+    wf_bounces = dll.renderer_get_parameter_int("Wavefront bounces")
+    trace_launches = SPP_PER_FRAME * min(wf_bounces + 1, MAX_PATH)
     ext_rays, shd_rays = st["extensionRays"], st["shadowRays"]
     alg_bytes = ((st["extendNodeVisits"] + st["shadowNodeVisits"]) * 80
                  + (st["extendPrimTests"] + st["shadowPrimTests"]) * 48
                  + (st["extendInstanceVisits"] + st["shadowInstanceVisits"]) * 56
                  + ext_rays * (32 + 20) + shd_rays * 48)
-    achieved_gbs = alg_bytes / (st["extendMs"] * 1e-3) / 1e9
+    # the counters include the rays of the path-finishing launch; the trace
+    # launches carry the rays of bounces 0..wf_bounces (their share measured
+    # below from the stage times is not needed: bytes and time both cover
+    # trace + tail)
+    trace_ms = st["extendMs"] + st["tailMs"]
+    achieved_gbs = alg_bytes / (trace_ms * 1e-3) / 1e9
     peaks, peak_kind = measured_peaks()
     l2 = bindings.c_float(0.0)
     dll.core.mufflon_measure_l2_bandwidth(32 << 20, 100, bindings.byref(l2))
     roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved_gbs / peaks["hbm_gbs"], 4), "traffic": None,
+                "frac": round(achieved_gbs / peaks["hbm_gbs"], 4),
+                "traffic": round(TRACE_DRAM_PER_ALG_BYTE * alg_bytes / (trace_launches + SPP_PER_FRAME)),
+                "traffic_note": ("DRAM bytes per launch: ncu dram__bytes_read+write of the bounce-1 k_trace launch "
+                                 f"per algorithmic byte ({TRACE_DRAM_PER_ALG_BYTE}) x algorithmic bytes per launch"),
                 "peak_source": f"{peak_kind} HBM copy bandwidth",
                 "l2_read_peak_gbs": round(float(l2.value), 1),
                 "frac_of_l2": round(achieved_gbs / max(float(l2.value), 1e-9), 4),
                 "bytes_per_ray": round(alg_bytes / max(ext_rays + shd_rays, 1), 1),
-                "kernel": "k_trace", "launches": trace_launches,
-                "avg_launch_ms": round(st["extendMs"] / trace_launches, 4)}
+                "kernel": "k_trace + k_tail", "launches": trace_launches + SPP_PER_FRAME,
+                "avg_launch_ms": round(trace_ms / (trace_launches + SPP_PER_FRAME), 4)}
     stage_ms = {"camera": round(st["cameraMs"], 3), "trace": round(st["extendMs"], 3),
-                "shade": round(st["shadeMs"], 3), "finalize": round(st["finalizeMs"], 3)}
+                "tail": round(st["tailMs"], 3), "shade": round(st["shadeMs"], 3),
+                "finalize": round(st["finalizeMs"], 3)}
     per_ray = {"extend_nodes": round(st["extendNodeVisits"] / max(st["extensionRays"], 1), 2),
                "extend_prims": round(st["extendPrimTests"] / max(st["extensionRays"], 1), 2),
                "shadow_nodes": round(st["shadowNodeVisits"] / max(st["shadowRays"], 1), 2),
                "shadow_prims": round(st["shadowPrimTests"] / max(st["shadowRays"], 1), 2)}
+    lbvh = lbvh_build_measurement(dll, spec.lods[0], torch) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(spec, args.cpu_seconds)
@@ -352,6 +407,7 @@ def run_b200(args):
                 "gpu_launches": int(gpu_launches),
                 "roofline": roofline,
                 "stage_ms_per_frame": stage_ms,
+                "lbvh": lbvh,
                 "traversal_per_ray": per_ray,
                 "cpu_baseline": cpu,
                 "clocks": clk}
