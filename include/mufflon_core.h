@@ -274,6 +274,35 @@ typedef struct {
 } MufflonStageStats;
 CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
 
+/* EXTENSION with no counterpart in the reference: renders many jobs at once.
+ * A job is the loaded scenario of a library instance (so jobs may use
+ * different scenes), rendered at its own resolution (0 = the scenario's),
+ * sample count and path-tracer parameters. All jobs' paths go through the
+ * same wavefront queues, one iteration (sample) of every unfinished job per
+ * launch sequence; with useGraph the whole batch is captured as one CUDA
+ * graph and launched once. radiance[j] (width*height*3 floats) and hitId[j]
+ * (width*height*2) receive job j's cumulative means; either array or entry may
+ * be NULL. jobDoneMs[j] (may be NULL) receives the device time from the start
+ * of the batch until job j's last sample was accumulated. All jobs must use
+ * the same NEE count; the instances must be on one device. Each job's result
+ * is identical to rendering it alone with render_iterate. */
+typedef struct {
+	MufflonInstanceHdl instance;
+	uint32_t width, height;
+	uint32_t spp;
+	int32_t seed;
+	int32_t minPathLength, maxPathLength, rrStartDepth, neeCount;
+} MufflonBatchJob;
+typedef struct {
+	float deviceMs;     /* device time of the whole batch */
+	uint32_t launches;  /* kernel launches (captured as graph nodes when useGraph) */
+	uint32_t usedGraph;
+	uint32_t pixels;    /* pixels of all jobs */
+} MufflonBatchStats;
+CORE_API Boolean CDECL mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_t useGraph,
+                                            float* const* radiance, float* const* hitId, float* jobDoneMs,
+                                            MufflonBatchStats* stats);
+
 /* Host-side times (ms) of the last scene load (world_load_scenario or the
  * implicit load of the first render_iterate): the whole load, the geometry
  * upload, the object BVH builds (LBVH + 8-wide conversion), the instance BVH,

@@ -181,6 +181,16 @@ class MufflonLoadStats(Structure):
                 ("otherMs", c_float), ("pad", c_uint32), ("h2dBytes", c_uint64)]
 
 
+class MufflonBatchJob(Structure):
+    _fields_ = [("instance", c_void_p), ("width", c_uint32), ("height", c_uint32), ("spp", c_uint32),
+                ("seed", c_int32), ("minPathLength", c_int32), ("maxPathLength", c_int32),
+                ("rrStartDepth", c_int32), ("neeCount", c_int32)]
+
+
+class MufflonBatchStats(Structure):
+    _fields_ = [("deviceMs", c_float), ("launches", c_uint32), ("usedGraph", c_uint32), ("pixels", c_uint32)]
+
+
 def _bulk(a: np.ndarray) -> BulkLoader:
     b = BulkLoader()
     b.type = 1  # BULK_ARRAY
@@ -274,6 +284,8 @@ class DllHolder:
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
             "mufflon_get_load_stats": (c_uint32, [c_void_p, POINTER(MufflonLoadStats)]),
+            "mufflon_render_batch": (c_uint32, [POINTER(MufflonBatchJob), c_uint32, c_int32, c_void_p, c_void_p,
+                                                POINTER(c_float), POINTER(MufflonBatchStats)]),
             "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
                                               c_void_p, c_void_p]),
             "mufflon_trace_occlusion": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
@@ -498,6 +510,37 @@ def sort_pairs(dll: DllInterface, keys: np.ndarray, values: np.ndarray):
     v = np.ascontiguousarray(values, np.int32).copy()
     dll._check(dll.core.mufflon_sort_pairs(_ptr(k), _ptr(v), len(k)), "mufflon_sort_pairs")
     return k, v
+
+
+def render_batch(jobs, use_graph=True, hit_ids=False):
+    """Renders a batch with mufflon_render_batch.
+
+    `jobs` is a list of dicts: instance (a DllInterface with a loaded
+    scenario), width, height (0 = the scenario's), spp, seed, min_path,
+    max_path, rr_start, nee. Returns (radiance images (H, W, 3), hit-id images
+    or None, per-job completion ms, stats dict)."""
+    if not jobs:
+        raise ValueError("empty batch")
+    core = jobs[0]["instance"].core
+    arr = (MufflonBatchJob * len(jobs))()
+    imgs, hits = [], []
+    for j, d in enumerate(jobs):
+        inst = d["instance"]
+        w, h = d.get("width", 0), d.get("height", 0)
+        if not w or not h:
+            w, h = inst.resolution
+        arr[j] = MufflonBatchJob(inst.muffInst, w, h, d["spp"], d.get("seed", 0), d.get("min_path", 0),
+                                 d.get("max_path", 16), d.get("rr_start", 0), d.get("nee", 1))
+        imgs.append(np.zeros((h, w, 3), np.float32))
+        hits.append(np.zeros((h, w, 2), np.float32) if hit_ids else None)
+    rad_ptrs = (c_void_p * len(jobs))(*[im.ctypes.data for im in imgs])
+    hit_ptrs = (c_void_p * len(jobs))(*[(hm.ctypes.data if hm is not None else None) for hm in hits])
+    done = (c_float * len(jobs))()
+    st = MufflonBatchStats()
+    if not core.mufflon_render_batch(arr, len(jobs), 1 if use_graph else 0, rad_ptrs, hit_ptrs if hit_ids else None,
+                                     done, byref(st)):
+        raise MufflonError(f"mufflon_render_batch failed: {core.core_get_dll_error().decode()}")
+    return imgs, (hits if hit_ids else None), list(done), {k: getattr(st, k) for k, _ in MufflonBatchStats._fields_}
 
 
 def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):

@@ -9,6 +9,7 @@
 #include "../lbvh/sort_noalloc.hpp"
 
 #include <algorithm>
+#include <cstdio>
 #include <chrono>
 #include <cstdarg>
 #include <cstring>
@@ -36,7 +37,7 @@ struct ApiError : std::runtime_error { using std::runtime_error::runtime_error; 
 #define CATCH_ALL(ret) } catch(const std::exception& ex) { s_lastError = std::string(__func__) + ": " + ex.what(); log_msg(LOG_ERROR, s_lastError); return ret; } \
 	catch(...) { s_lastError = std::string(__func__) + ": unknown error"; log_msg(LOG_ERROR, s_lastError); return ret; }
 #define CHECK(cond, msg) do { if(!(cond)) throw ApiError(msg); } while(0)
-#define CHECK_CUDA(expr) do { cudaError_t e_ = (expr); if(e_ != cudaSuccess) throw ApiError(std::string("CUDA: ") + cudaGetErrorString(e_)); } while(0)
+#define CHECK_CUDA(expr) do { cudaError_t e_ = (expr); if(e_ != cudaSuccess) throw ApiError(std::string("CUDA: ") + cudaGetErrorString(e_) + " (" #expr ", line " + std::to_string(__LINE__) + ")"); } while(0)
 
 MufflonInstance& minst(void* h) {
 	if(!h) throw ApiError("invalid mufflon instance");
@@ -105,34 +106,13 @@ void ensure_wavefront_buffers(MufflonInstance& I) {
 	RendererState& r = I.renderer;
 	const size_t n = size_t(r.width) * r.height;
 	const int nee = r.params.neeCount > 0 ? r.params.neeCount : 1;
-	static const size_t ALIGN = 256;
-	auto al = [](size_t b) { return (b + ALIGN - 1) / ALIGN * ALIGN; };
-	const size_t need = al(n * 16) * 2 + al(n * 8) + 2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) +
-	                    al(n * nee * 4) + 3 * al(n * nee * 16) + al(WF_COUNTERS * 4);
 	if(r.wfMemory && r.wfNee == nee && r.wfPixels == n) return;
 	if(r.wfMemory) cudaFree(r.wfMemory);
 	r.wfMemory = nullptr;
 	r.wfNee = 0;
 	r.wfPixels = 0;
-	CHECK_CUDA(cudaMalloc(&r.wfMemory, need));
-	char* m = static_cast<char*>(r.wfMemory);
-	auto take = [&](size_t b) { char* p = m; m += al(b); return p; };
-	WfState& W = r.wf;
-	W.thrPdf = reinterpret_cast<float4*>(take(n * 16));
-	W.rad = reinterpret_cast<float4*>(take(n * 16));
-	W.hit0 = reinterpret_cast<float2*>(take(n * 8));
-	for(int q = 0; q < 2; ++q) {
-		W.qPath[q] = reinterpret_cast<int*>(take(n * 4));
-		W.qOrg[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qDir[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qHit[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qHitSpy[q] = reinterpret_cast<float*>(take(n * 4));
-	}
-	W.sPath = reinterpret_cast<int*>(take(n * nee * 4));
-	W.sOrg = reinterpret_cast<float4*>(take(n * nee * 16));
-	W.sDir = reinterpret_cast<float4*>(take(n * nee * 16));
-	W.sContrib = reinterpret_cast<float4*>(take(n * nee * 16));
-	W.counters = reinterpret_cast<unsigned*>(take(WF_COUNTERS * 4));
+	CHECK_CUDA(cudaMalloc(&r.wfMemory, wavefront_bytes(n, nee)));
+	wavefront_carve(r.wfMemory, n, nee, r.wf);
 	r.wfNee = nee;
 	r.wfPixels = n;
 }
@@ -1046,6 +1026,193 @@ Boolean mufflon_get_stage_stats(MufflonInstanceHdl h, MufflonStageStats* s) {
 	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE];
 	s->launches = uint32_t(r.lastLaunches);
 	s->wavefront = r.megakernel ? 0u : 1u;
+	return true;
+	CATCH_ALL(false)
+}
+
+// ---------------------------------------------------------------- batches
+namespace {
+// Grow-only device buffers of mufflon_render_batch (one batch at a time).
+struct BatchState {
+	std::mutex mutex;
+	int device = -1;
+	cudaStream_t stream = nullptr;
+	void* wf = nullptr;
+	size_t wfBytes = 0;
+	void* buf = nullptr;
+	size_t bufBytes = 0;
+	DJob* dJobs = nullptr;
+	size_t jobsCap = 0;
+	std::vector<cudaEvent_t> events;
+};
+BatchState& batch_state() {
+	static BatchState* b = new BatchState(); // lives until process exit
+	return *b;
+}
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+} // namespace
+
+Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_t useGraph, float* const* radiance,
+                             float* const* hitId, float* jobDoneMs, MufflonBatchStats* stats) {
+	TRY
+	CHECK(jobs && count > 0 && count <= 65535, "a batch needs 1 to 65535 jobs");
+	BatchState& B = batch_state();
+	std::lock_guard<std::mutex> batchLock(B.mutex);
+	// every instance used by the batch is locked (in address order) and loaded
+	std::vector<MufflonInstance*> insts;
+	for(uint32_t j = 0; j < count; ++j) insts.push_back(&minst(jobs[j].instance));
+	std::vector<MufflonInstance*> uniq(insts);
+	std::sort(uniq.begin(), uniq.end());
+	uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+	std::vector<std::unique_lock<std::recursive_mutex>> locks;
+	for(MufflonInstance* I : uniq) locks.emplace_back(I->iterationMutex);
+	const int dev = uniq[0]->device;
+	for(MufflonInstance* I : uniq) {
+		CHECK(I->device == dev, "all jobs of a batch must use instances on the same device");
+		CHECK(I->current != nullptr, "a job's instance has no loaded scenario");
+		load_scene_if_needed(*I);
+	}
+	CHECK_CUDA(cudaSetDevice(dev));
+	if(B.device != dev) {
+		CHECK(B.device < 0, "batches on more than one device per process are not supported");
+		CHECK_CUDA(cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking));
+		B.device = dev;
+	}
+	cudaStream_t st = B.stream;
+	// host job table
+	const int nee = jobs[0].neeCount > 0 ? jobs[0].neeCount : 1;
+	std::vector<DJob> hj(count);
+	uint64_t pixels = 0;
+	int maxSpp = 0, maxBounces = 1;
+	for(uint32_t j = 0; j < count; ++j) {
+		const MufflonBatchJob& in = jobs[j];
+		const MufflonInstance& I = *insts[j];
+		const uint32_t w = in.width ? in.width : I.current->width;
+		const uint32_t h = in.height ? in.height : I.current->height;
+		CHECK(w > 0 && h > 0 && w <= 65535 && h <= 65535, "job resolution out of range");
+		CHECK(in.spp >= 1, "a job needs at least one sample");
+		CHECK(in.maxPathLength >= 1, "Max. path length must be at least 1");
+		CHECK((in.neeCount > 0 ? in.neeCount : 1) == nee, "all jobs of a batch must use the same NEE count");
+		DJob& d = hj[j];
+		d.scene = I.scene.desc;
+		d.scene.camera.resX = uint16_t(w);
+		d.scene.camera.resY = uint16_t(h);
+		d.params = PtParams{ in.seed, in.minPathLength, in.maxPathLength, nee, in.rrStartDepth };
+		d.width = w; d.height = h; d.spp = in.spp;
+		d.pixelOffset = uint32_t(pixels);
+		pixels += uint64_t(w) * h;
+		maxSpp = std::max(maxSpp, int(in.spp));
+		maxBounces = std::max(maxBounces, int(in.maxPathLength));
+	}
+	CHECK(pixels < (1ull << 31), "a batch holds at most 2^31 - 1 pixels");
+	const size_t n = size_t(pixels);
+	// device buffers (grow-only)
+	const size_t need = align256(n * 8) + align256(n * 2) + align256(n * 12) + align256(n * 8) + align256(2 * sizeof(TraceCounters));
+	if(B.bufBytes < need) {
+		if(B.buf) cudaFree(B.buf);
+		B.buf = nullptr; B.bufBytes = 0;
+		CHECK_CUDA(cudaMalloc(&B.buf, need));
+		B.bufBytes = need;
+	}
+	const size_t wfNeed = wavefront_bytes(n, nee);
+	if(B.wfBytes < wfNeed) {
+		if(B.wf) cudaFree(B.wf);
+		B.wf = nullptr; B.wfBytes = 0;
+		CHECK_CUDA(cudaMalloc(&B.wf, wfNeed));
+		B.wfBytes = wfNeed;
+	}
+	if(B.jobsCap < count) {
+		if(B.dJobs) cudaFree(B.dJobs);
+		B.dJobs = nullptr; B.jobsCap = 0;
+		CHECK_CUDA(cudaMalloc(&B.dJobs, sizeof(DJob) * count));
+		B.jobsCap = count;
+	}
+	char* m = static_cast<char*>(B.buf);
+	auto take = [&](size_t b) { char* p = m; m += align256(b); return p; };
+	uint64_t* rng = reinterpret_cast<uint64_t*>(take(n * 8));
+	uint16_t* pathJob = reinterpret_cast<uint16_t*>(take(n * 2));
+	float* rad = reinterpret_cast<float*>(take(n * 12));
+	float* hit = reinterpret_cast<float*>(take(n * 8));
+	TraceCounters* counters = reinterpret_cast<TraceCounters*>(take(2 * sizeof(TraceCounters)));
+	WfState W{};
+	wavefront_carve(B.wf, n, nee, W);
+	W.rng = rng;
+	std::vector<uint16_t> pj(n);
+	for(uint32_t j = 0; j < count; ++j) {
+		std::fill(pj.begin() + hj[j].pixelOffset, pj.begin() + hj[j].pixelOffset + size_t(hj[j].width) * hj[j].height, uint16_t(j));
+		hj[j].radiance = rad + 3 * size_t(hj[j].pixelOffset);
+		hj[j].hitId = hit + 2 * size_t(hj[j].pixelOffset);
+	}
+	CHECK_CUDA(cudaMemcpyAsync(pathJob, pj.data(), n * 2, cudaMemcpyHostToDevice, st));
+	CHECK_CUDA(cudaMemcpyAsync(B.dJobs, hj.data(), sizeof(DJob) * count, cudaMemcpyHostToDevice, st));
+	CHECK_CUDA(cudaMemsetAsync(rad, 0, n * 12, st));
+	CHECK_CUDA(cudaMemsetAsync(hit, 0, n * 8, st));
+	CHECK_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(TraceCounters), st));
+	for(uint32_t j = 0; j < count; ++j)
+		CHECK_CUDA(launch_seed_rng(rng + hj[j].pixelOffset, hj[j].width * hj[j].height, hj[j].params.seed, st));
+	const RendererState& r0 = uniq[0]->renderer;
+	WfTuning tune;
+	tune.traceBlocksPerSm = r0.traceBlocksPerSm;
+	tune.wavefrontBounces = r0.wavefrontBounces;
+	tune.refillLanes = r0.refillLanes;
+	prepare_batch_kernels(tune);
+	while(B.events.size() < size_t(maxSpp) + 1) {
+		cudaEvent_t e;
+		CHECK_CUDA(cudaEventCreate(&e));
+		B.events.push_back(e);
+	}
+	CHECK_CUDA(cudaStreamSynchronize(st));
+	uint32_t launches = 0;
+	auto body = [&]() -> cudaError_t {
+		for(int it = 0; it < maxSpp; ++it) {
+			WfLaunchInfo info;
+			const cudaError_t e = launch_pt_batch(B.dJobs, pathJob, uint32_t(n), it, maxBounces, nee, W, counters, st, tune, &info);
+			if(e != cudaSuccess) return e;
+			launches += uint32_t(info.launches);
+			// inside a capture only an "external" record becomes a timing record of the graph
+			const cudaError_t er = useGraph ? cudaEventRecordWithFlags(B.events[size_t(it) + 1], st, cudaEventRecordExternal)
+			                                : cudaEventRecord(B.events[size_t(it) + 1], st);
+			if(er != cudaSuccess) return er;
+		}
+		return cudaSuccess;
+	};
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	if(useGraph) {
+		CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		const cudaError_t e = body();
+		const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+		CHECK_CUDA(e);
+		CHECK_CUDA(e2);
+		CHECK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+		CHECK_CUDA(cudaEventRecord(B.events[0], st));
+		CHECK_CUDA(cudaGraphLaunch(exec, st));
+	} else {
+		CHECK_CUDA(cudaEventRecord(B.events[0], st));
+		CHECK_CUDA(body());
+	}
+	const cudaError_t se = cudaStreamSynchronize(st);
+	if(exec) cudaGraphExecDestroy(exec);
+	if(graph) cudaGraphDestroy(graph);
+	CHECK_CUDA(se);
+	CHECK_CUDA(cudaGetLastError());
+	if(jobDoneMs)
+		for(uint32_t j = 0; j < count; ++j) {
+			float ms = 0.0f;
+			CHECK_CUDA(cudaEventElapsedTime(&ms, B.events[0], B.events[hj[j].spp]));
+			jobDoneMs[j] = ms;
+		}
+	if(stats) {
+		CHECK_CUDA(cudaEventElapsedTime(&stats->deviceMs, B.events[0], B.events[size_t(maxSpp)]));
+		stats->launches = launches;
+		stats->usedGraph = useGraph ? 1u : 0u;
+		stats->pixels = uint32_t(n);
+	}
+	for(uint32_t j = 0; j < count; ++j) {
+		const size_t np = size_t(hj[j].width) * hj[j].height;
+		if(radiance && radiance[j]) CHECK_CUDA(cudaMemcpy(radiance[j], hj[j].radiance, np * 12, cudaMemcpyDeviceToHost));
+		if(hitId && hitId[j]) CHECK_CUDA(cudaMemcpy(hitId[j], hj[j].hitId, np * 8, cudaMemcpyDeviceToHost));
+	}
 	return true;
 	CATCH_ALL(false)
 }

@@ -52,9 +52,25 @@ MBD unsigned warp_reserve(unsigned* counter, unsigned want) {
 	return base + g.thread_rank() * want;
 }
 
-__global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t numPixels, uint32_t width) {
-	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-	if(p >= numPixels) return;
+// Where a path's scene and path-tracer parameters come from: the kernel
+// argument for a plain render, or the device job table of a batch, whose jobs
+// share the queues (path p belongs to job pathJob[p]).
+struct OneScene {
+	DScene S;
+	PtParams P;
+	MBD const DScene& scene(int) const { return S; }
+	MBD const PtParams& params(int) const { return P; }
+};
+struct JobScenes {
+	const DJob* jobs;
+	const uint16_t* pathJob;
+	MBD const DScene& scene(int p) const { return jobs[pathJob[p]].scene; }
+	MBD const PtParams& params(int p) const { return jobs[pathJob[p]].params; }
+};
+
+// Primary ray of one path (pinhole_ray, the camera's and the first walk's
+// random numbers, Russian roulette at path length 0).
+MBD void camera_path(const DScene& S, const PtParams& P, WfState& W, uint32_t p, int px, int py) {
 	u64 rng = W.rng[p];
 	(void)pcg_next(rng); // create_camera
 	const u64 x0 = pcg_next(rng);
@@ -62,7 +78,7 @@ __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t n
 	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
 	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
 	float pdfF;
-	const f3 dir = pinhole_ray(S.camera, int(p % width), int(p / width), ru0, ru1, pdfF);
+	const f3 dir = pinhole_ray(S.camera, px, py, ru0, ru1, pdfF);
 	f3 thr = make3(1.0f, 1.0f, 1.0f);
 	bool alive = true;
 	if(0 >= P.rrStartDepth) {
@@ -81,6 +97,23 @@ __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t n
 	W.qPath[0][slot] = int(p);
 	W.qOrg[0][slot] = pack(o, 0.0f);
 	W.qDir[0][slot] = pack(dir, 0.0f);
+}
+
+// Camera stage of a batch: global pixel g of job pathJob[g]; pixels of jobs
+// whose samples are all taken stay idle.
+__global__ void k_camera_batch(const DJob* jobs, WfState W, const uint16_t* pathJob, uint32_t numPixels, int iteration) {
+	const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+	if(g >= numPixels) return;
+	const DJob& J = jobs[pathJob[g]];
+	if(iteration >= int(J.spp)) return;
+	const uint32_t local = g - J.pixelOffset;
+	camera_path(J.scene, J.params, W, g, int(local % J.width), int(local / J.width));
+}
+
+__global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t numPixels, uint32_t width) {
+	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(p >= numPixels) return;
+	camera_path(S, P, W, p, int(p % width), int(p / width));
 }
 
 // Block-wide traversal statistics in shared memory, one set per ray kind.
@@ -103,8 +136,8 @@ MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
 // Every loop iteration runs one traversal step in every busy lane.
 // Queue entries are read and written with streaming (evict-first) accesses so
 // that they do not displace the hierarchies from L2.
-template < int MINB >
-__global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, int q, int neeCount, int workIdx,
+template < int MINB, class SP >
+__global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int q, int neeCount, int workIdx,
                                                      TraceCounters* counters, int refillLanes) {
 	__shared__ BlockStats stats;
 	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
@@ -117,7 +150,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, 
 	WideTracer t;
 	bool active = false, exhausted = false;
 	unsigned item = 0;
-	int path = 0, ray = 0;
+	int path = 0, ray = 0; // path of the current item
 	f3 radiance = make3(0.0f, 0.0f, 0.0f);
 	float radW = 0.0f;
 	const unsigned lane = threadIdx.x & 31u;
@@ -137,8 +170,9 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, 
 					exhausted = true;
 				} else if(item < nExt) {
 					const float4 o = __ldcs(W.qOrg[q] + item), d = __ldcs(W.qDir[q] + item);
+					path = W.qPath[q][item];
 					cnt = LocalCounters();
-					t.init(S, f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
+					t.init(sp.scene(path), f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
 					active = true;
 				} else {
 					path = __ldcs(W.sPath + (item - nExt) * unsigned(neeCount));
@@ -151,7 +185,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, 
 			}
 		}
 		if(__all_sync(0xffffffffu, exhausted)) break;
-		if(active && t.step(S, cnt, stack)) {
+		if(active && t.step(sp.scene(path), cnt, stack)) {
 			if(item < nExt) {
 				stats_add(stats, 0, cnt);
 				const HitRec& h = t.best;
@@ -175,7 +209,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const DScene S, WfState W, 
 				if(!(o.w > 0.0f)) continue;
 				const float4 d = __ldcs(W.sDir + g0 + unsigned(ray));
 				cnt = LocalCounters();
-				t.init(S, f4to3(o), f4to3(d), o.w, true, cnt);
+				t.init(sp.scene(path), f4to3(o), f4to3(d), o.w, true, cnt);
 				active = true;
 				break;
 			}
@@ -300,11 +334,14 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 // Shade stage of the wavefront: one thread per queued path. Next-event rays go
 // to the shadow queue (neeCount consecutive slots per path, allocated when
 // the first one is needed), the next ray to the other extension queue.
-__global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P, WfState W, int q, int bounce) {
+template < class SP >
+__global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, int bounce) {
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
 	if(slot >= count) return;
 	const int p = __ldcs(W.qPath[q] + slot);
+	const DScene& S = sp.scene(p);
+	const PtParams& P = sp.params(p);
 	const f3 origin = f4to3(__ldcs(W.qOrg[q] + slot));
 	const f3 dir = f4to3(__ldcs(W.qDir[q] + slot));
 	const float4 hh = __ldcs(W.qHit[q] + slot);
@@ -348,8 +385,8 @@ __global__ void __launch_bounds__(128) k_shade(const DScene S, const PtParams P,
 // in order, trace the next extension ray, and so on until the path ends. Used
 // once few paths are left, where a separate launch per bounce would be
 // dominated by launch and drain latency.
-template < int MINB >
-__global__ void __launch_bounds__(128, MINB) k_tail(const DScene S, const PtParams P, WfState W, int q, int bounce,
+template < int MINB, class SP >
+__global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int q, int bounce,
                                                     int workIdx, TraceCounters* counters) {
 	__shared__ BlockStats stats;
 	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
@@ -360,6 +397,8 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const DScene S, const PtPara
 		const unsigned item = atomicAdd(W.counters + C_WORK + workIdx, 1u);
 		if(item >= count) break;
 		const int p = W.qPath[q][item];
+		const DScene& S = sp.scene(p);
+		const PtParams& P = sp.params(p);
 		f3 origin = f4to3(W.qOrg[q][item]);
 		f3 dir = f4to3(W.qDir[q][item]);
 		const float4 hh = W.qHit[q][item];
@@ -429,6 +468,27 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	}
 }
 
+// Accumulation of a batch iteration into each job's image (jobs whose
+// samples are all taken are left alone).
+__global__ void k_finalize_batch(const DJob* jobs, WfState W, const uint16_t* pathJob, uint32_t numPixels, int iteration) {
+	const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+	if(g >= numPixels) return;
+	const DJob& J = jobs[pathJob[g]];
+	if(iteration >= int(J.spp)) return;
+	const size_t local = g - J.pixelOffset;
+	const float den = fmaxf(1.0f, float(iteration) + 1.0f);
+	const float4 rad = W.rad[g];
+	float* cr = J.radiance + 3 * local;
+	const float it[3] = { rad.x, rad.y, rad.z };
+	for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+	if(J.hitId) {
+		const float2 h = W.hit0[g];
+		float* ch = J.hitId + 2 * local;
+		const float ih[2] = { h.x, h.y };
+		for(int c = 0; c < 2; ++c) { const float diff = ih[c] - ch[c]; ch[c] += __fdiv_rn(diff, den); }
+	}
+}
+
 // Closest hits / shadow-ray tests of caller-provided rays over the wide
 // hierarchies (the parity and measurement entry points).
 __global__ void k_trace_rays_wide(const DScene S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
@@ -462,16 +522,18 @@ __global__ void k_occlusion_wide(const DScene S, const float* a, const float* b,
 	}
 }
 
-using TraceFn = void (*)(const DScene, WfState, int, int, int, TraceCounters*, int);
-struct TraceKernel { TraceFn fn; int blocks; };
-
 int persistent_blocks(const void* fn, int threads);
 
+template < class SP > struct TraceKernel {
+	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*, int);
+	Fn fn;
+	int blocks;
+};
 // The trace kernel compiled for `perSm` resident blocks of 128 threads
-// (register budget 65536 / (128 * perSm)); 0 picks the default.
-TraceKernel trace_kernel(int perSm) {
-	static TraceKernel table[4] = {};
-	static const TraceFn fns[4] = { k_trace<4>, k_trace<5>, k_trace<6>, k_trace<8> };
+// (register budget 65536 / (128 * perSm)); other values pick 6.
+template < class SP > TraceKernel<SP> trace_kernel(int perSm) {
+	static TraceKernel<SP> table[4] = {};
+	static const typename TraceKernel<SP>::Fn fns[4] = { k_trace<4, SP>, k_trace<5, SP>, k_trace<6, SP>, k_trace<8, SP> };
 	static const int occ[4] = { 4, 5, 6, 8 };
 	int idx = 2;
 	for(int i = 0; i < 4; ++i) if(occ[i] == perSm) idx = i;
@@ -479,12 +541,68 @@ TraceKernel trace_kernel(int perSm) {
 	return table[idx];
 }
 
-using TailFn = void (*)(const DScene, const PtParams, WfState, int, int, int, TraceCounters*);
-struct TailKernel { TailFn fn; int blocks; };
-TailKernel tail_kernel() {
-	static TailKernel k = {};
-	if(!k.fn) k = { k_tail<4>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4>), 128) };
+template < class SP > struct TailKernel {
+	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*);
+	Fn fn;
+	int blocks;
+};
+template < class SP > TailKernel<SP> tail_kernel() {
+	static TailKernel<SP> k = {};
+	if(!k.fn) k = { k_tail<4, SP>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4, SP>), 128) };
 	return k;
+}
+
+// Stage timing and launch counting of one iteration.
+struct LaunchLog {
+	WfLaunchInfo& L;
+	cudaStream_t stream;
+	void begin(WfStage k) {
+		++L.launches;
+		if(L.events && L.pairsUsed < L.eventPairs) {
+			L.kinds[L.pairsUsed] = (unsigned char)k;
+			cudaEventRecord(L.events[2 * L.pairsUsed], stream);
+		}
+	}
+	void end() {
+		if(L.events && L.pairsUsed < L.eventPairs) cudaEventRecord(L.events[2 * L.pairsUsed++ + 1], stream);
+	}
+};
+
+// The bounces of one iteration after the camera stage: per-bounce trace and
+// shade launches for bounces 0 .. wavefrontBounces, then one launch that
+// finishes the remaining paths. `numPaths` bounds the queue lengths.
+template < class SP >
+void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numPaths, int maxBounces, int neeCount,
+                 const WfTuning& tuning, LaunchLog& log, cudaStream_t stream) {
+	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
+	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm);
+	const unsigned workSlots = WF_COUNTERS - C_WORK;
+	const unsigned grid = (numPaths + 127) / 128;
+	unsigned work = 0;
+	for(int b = 0; b < maxBounces; ++b) {
+		const int q = b & 1;
+		if(work + 2 > workSlots) { // very long paths: recycle the work counters (stream ordered)
+			cudaMemsetAsync(W.counters + C_WORK, 0, sizeof(unsigned) * workSlots, stream);
+			work = 0;
+		}
+		log.begin(WF_EXTEND);
+		tk.fn<<<tk.blocks, 128, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes);
+		log.end();
+		if(b >= tuning.wavefrontBounces && b + 1 < maxBounces) {
+			// few paths are left: finish them in one launch
+			const TailKernel<SP> tl = tail_kernel<SP>();
+			log.begin(WF_TAIL);
+			tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters);
+			log.end();
+			break;
+		}
+		// the shade of this bounce appends to the other queue and to the shadow queue
+		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);
+		cudaMemsetAsync(W.counters + C_SHADOW, 0, sizeof(unsigned), stream);
+		log.begin(WF_SHADE);
+		k_shade<SP><<<grid, 128, 0, stream>>>(sp, W, q, b);
+		log.end();
+	}
 }
 
 int persistent_blocks(const void* fn, int threads) {
@@ -496,6 +614,45 @@ int persistent_blocks(const void* fn, int threads) {
 }
 
 } // namespace
+
+namespace {
+constexpr size_t WF_ALIGN = 256;
+size_t wf_align(size_t b) { return (b + WF_ALIGN - 1) / WF_ALIGN * WF_ALIGN; }
+} // namespace
+
+size_t wavefront_bytes(size_t n, int nee) {
+	if(nee < 1) nee = 1;
+	return wf_align(n * 16) * 2 + wf_align(n * 8) + 2 * (wf_align(n * 4) + 3 * wf_align(n * 16) + wf_align(n * 4)) +
+	       wf_align(n * nee * 4) + 3 * wf_align(n * nee * 16) + wf_align(WF_COUNTERS * 4);
+}
+
+void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
+	if(nee < 1) nee = 1;
+	char* m = static_cast<char*>(memory);
+	auto take = [&](size_t b) { char* p = m; m += wf_align(b); return p; };
+	W.thrPdf = reinterpret_cast<float4*>(take(n * 16));
+	W.rad = reinterpret_cast<float4*>(take(n * 16));
+	W.hit0 = reinterpret_cast<float2*>(take(n * 8));
+	for(int q = 0; q < 2; ++q) {
+		W.qPath[q] = reinterpret_cast<int*>(take(n * 4));
+		W.qOrg[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qDir[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHit[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHitSpy[q] = reinterpret_cast<float*>(take(n * 4));
+	}
+	W.sPath = reinterpret_cast<int*>(take(n * nee * 4));
+	W.sOrg = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.sDir = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.sContrib = reinterpret_cast<float4*>(take(n * nee * 16));
+	W.counters = reinterpret_cast<unsigned*>(take(WF_COUNTERS * 4));
+}
+
+void prepare_batch_kernels(const WfTuning& tuning) {
+	(void)trace_kernel<JobScenes>(tuning.traceBlocksPerSm);
+	(void)tail_kernel<JobScenes>();
+	(void)trace_kernel<OneScene>(tuning.traceBlocksPerSm);
+	(void)tail_kernel<OneScene>();
+}
 
 cudaError_t launch_trace_rays_wide(const DScene& S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
                                   float* t, int32_t* inst, int32_t* prim, float* sp, cudaStream_t stream) {
@@ -515,25 +672,13 @@ cudaError_t launch_occlusion_wide(const DScene& S, const float* a, const float* 
 
 cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const RenderState& R, WfState W,
                                 TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info, const WfTuning& tuning) {
-	const int traceBlocksPerSm = tuning.traceBlocksPerSm, wavefrontBounces = tuning.wavefrontBounces;
-	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
 	WfLaunchInfo none;
 	WfLaunchInfo& L = info ? *info : none;
 	L.pairsUsed = 0;
 	L.launches = 0;
-	auto begin = [&](WfStage k) {
-		++L.launches;
-		if(L.events && L.pairsUsed < L.eventPairs) {
-			L.kinds[L.pairsUsed] = (unsigned char)k;
-			cudaEventRecord(L.events[2 * L.pairsUsed], stream);
-		}
-	};
-	auto end = [&]() {
-		if(L.events && L.pairsUsed < L.eventPairs) cudaEventRecord(L.events[2 * L.pairsUsed++ + 1], stream);
-	};
+	LaunchLog log{ L, stream };
 	const uint32_t n = R.width * R.height;
 	if(n == 0) return cudaSuccess;
-	const TraceKernel tk = trace_kernel(traceBlocksPerSm);
 	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
 	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;
 	const unsigned workSlots = WF_COUNTERS - C_WORK;
@@ -542,37 +687,45 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 	if(e != cudaSuccess) return e;
 	W.rng = R.rngState;
 	const unsigned grid = (n + 127) / 128;
-	begin(WF_CAMERA);
+	log.begin(WF_CAMERA);
 	k_camera<<<grid, 128, 0, stream>>>(S, P, W, n, R.width);
-	end();
-	unsigned work = 0;
-	for(int b = 0; b < maxBounces; ++b) {
-		const int q = b & 1;
-		if(work + 2 > workSlots) { // very long paths: recycle the work counters (stream ordered)
-			cudaMemsetAsync(W.counters + C_WORK, 0, sizeof(unsigned) * workSlots, stream);
-			work = 0;
-		}
-		begin(WF_EXTEND);
-		tk.fn<<<tk.blocks, 128, 0, stream>>>(S, W, q, neeCount, int(work++), counters, refillLanes);
-		end();
-		if(b >= wavefrontBounces && b + 1 < maxBounces) {
-			// few paths are left: finish them in one launch
-			const TailKernel tl = tail_kernel();
-			begin(WF_TAIL);
-			tl.fn<<<tl.blocks, 128, 0, stream>>>(S, P, W, q, b, int(work++), counters);
-			end();
-			break;
-		}
-		// the shade of this bounce appends to the other queue and to the shadow queue
-		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);
-		cudaMemsetAsync(W.counters + C_SHADOW, 0, sizeof(unsigned), stream);
-		begin(WF_SHADE);
-		k_shade<<<grid, 128, 0, stream>>>(S, P, W, q, b);
-		end();
-	}
-	begin(WF_FINALIZE);
+	log.end();
+	OneScene one;
+	one.S = S;
+	one.P = P;
+	run_bounces(one, W, counters, n, maxBounces, neeCount, tuning, log, stream);
+	log.begin(WF_FINALIZE);
 	k_finalize<<<grid, 128, 0, stream>>>(W, R, n);
-	end();
+	log.end();
+	return cudaGetLastError();
+}
+
+cudaError_t launch_pt_batch(const DJob* jobs, const uint16_t* pathJob, uint32_t numPixels, int iteration,
+                            int maxBounces, int neeCount, WfState W, TraceCounters* counters, cudaStream_t stream,
+                            const WfTuning& tuning, WfLaunchInfo* info) {
+	WfLaunchInfo none;
+	WfLaunchInfo& L = info ? *info : none;
+	L.pairsUsed = 0;
+	L.launches = 0;
+	LaunchLog log{ L, stream };
+	if(numPixels == 0) return cudaSuccess;
+	if(neeCount < 1) neeCount = 1;
+	if(maxBounces < 1) maxBounces = 1;
+	const unsigned workSlots = WF_COUNTERS - C_WORK;
+	const unsigned firstClear = unsigned(maxBounces) < workSlots ? unsigned(maxBounces) : workSlots;
+	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);
+	if(e != cudaSuccess) return e;
+	const unsigned grid = (numPixels + 127) / 128;
+	log.begin(WF_CAMERA);
+	k_camera_batch<<<grid, 128, 0, stream>>>(jobs, W, pathJob, numPixels, iteration);
+	log.end();
+	JobScenes js;
+	js.jobs = jobs;
+	js.pathJob = pathJob;
+	run_bounces(js, W, counters, numPixels, maxBounces, neeCount, tuning, log, stream);
+	log.begin(WF_FINALIZE);
+	k_finalize_batch<<<grid, 128, 0, stream>>>(jobs, W, pathJob, numPixels, iteration);
+	log.end();
 	return cudaGetLastError();
 }
 

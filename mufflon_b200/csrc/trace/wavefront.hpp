@@ -63,4 +63,32 @@ cudaError_t launch_trace_rays_wide(const DScene& scene, const float* rays, const
 cudaError_t launch_occlusion_wide(const DScene& scene, const float* a, const float* b, uint32_t n, uint8_t* out,
                                  cudaStream_t stream);
 
+// Device memory of the wavefront state for n paths and nee shadow rays per
+// path, and the carving of one allocation of that size into WfState.
+size_t wavefront_bytes(size_t n, int nee);
+void wavefront_carve(void* memory, size_t n, int nee, WfState& W);
+
+// Resolves the trace and tail kernels' launch shapes (occupancy queries), so
+// that a later stream capture does not have to.
+void prepare_batch_kernels(const WfTuning& tuning);
+
+// One job of a batch: its scene (a loaded scene of some library instance),
+// path-tracer parameters, resolution, sample count, its pixels' place in the
+// batch's global pixel range, and its cumulative images.
+struct DJob {
+	DScene scene;
+	PtParams params;
+	uint32_t width, height, pixelOffset, spp;
+	float* radiance;  // width * height * 3, cumulative mean
+	float* hitId;     // width * height * 2, or null
+};
+
+// One iteration (sample) of every job with spp > iteration, all jobs' paths
+// in the same queues. pathJob[g] is the job of global pixel g; W.rng holds
+// every global pixel's generator. neeCount must be the same for all jobs;
+// maxBounces is the largest max path length of the batch.
+cudaError_t launch_pt_batch(const DJob* jobs, const uint16_t* pathJob, uint32_t numPixels, int iteration,
+                            int maxBounces, int neeCount, WfState W, TraceCounters* counters, cudaStream_t stream,
+                            const WfTuning& tuning, WfLaunchInfo* info);
+
 } // namespace mb
