@@ -51,6 +51,9 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--workload", default="frame", choices=["frame", "batch"],
+                   help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one")
+    p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
 
@@ -417,8 +420,92 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
+def batch_jobs(n_jobs, seed=7):
+    """The mixed-job workload: scene in {Cornell box, 1.3 M-triangle icosphere,
+    4096 instances of 10 meshes + 20 000 spheres, 100 K-triangle displaced
+    plane}, square side log-uniform in [128, 1024], spp uniform in 1..64, max
+    path length uniform in 4..12 (seeded)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(n_jobs):
+        side = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
+        jobs.append(dict(scene=int(rng.integers(0, 4)), width=side, height=side, spp=int(rng.integers(1, 65)),
+                         max_path=int(rng.integers(4, 13)), seed=j))
+    return jobs
+
+
+def run_batch(args):
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import autotune, bindings, build, scenes
+    build.build()
+    specs = [scenes.cornell_box(0), scenes.displaced_icosphere(0, subdiv=8, width=512, height=512),
+             scenes.instanced_scene(0), scenes.displaced_plane(0)]
+    worlds = []
+    for spec in specs:
+        d = bindings.DllInterface()
+        bindings.load_scene_spec(d, spec)
+        assert d.render_enable_renderer(0, 0)
+        worlds.append(d)
+    tuned = autotune.autotune(worlds[1], iterations=2, warmup=1)  # tuning of the largest mesh, used by the batch
+    jobs = batch_jobs(args.jobs)
+    req = [dict(instance=worlds[j["scene"]], width=j["width"], height=j["height"], spp=j["spp"],
+                max_path=j["max_path"], seed=j["seed"]) for j in jobs]
+    bindings.render_batch(req[:4], use_graph=False)  # warm-up of the batch buffers and kernels
+    res = {}
+    for graph in (True, False):
+        t0 = time.perf_counter()
+        _, _, done, st = bindings.render_batch(req, use_graph=graph)
+        wall = time.perf_counter() - t0
+        res[graph] = (done, st, wall)
+    seq_done, seq_total, seq_wall = [], 0.0, 0.0
+    per_scene = {}
+    for j, r in zip(jobs, req):
+        t0 = time.perf_counter()
+        _, _, done, st = bindings.render_batch([r], use_graph=False)
+        seq_wall += time.perf_counter() - t0
+        seq_total += st["deviceMs"]
+        seq_done.append(seq_total)
+        ps = per_scene.setdefault(j["scene"], [0, 0.0, 0])
+        ps[0] += j["width"] * j["height"] * j["spp"]
+        ps[1] += st["deviceMs"]
+        ps[2] += 1
+    done_g, st_g, wall_g = res[True]
+    pct = lambda v, q: float(np.percentile(np.asarray(v), q))
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    line = {"metric": "batched jobs/s (64 mixed jobs: 4 scenes, 128-1024 px, 1-64 spp, depth 4-12)",
+            "value": round(len(jobs) / (st_g["deviceMs"] * 1e-3), 3), "unit": "jobs/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "batch_64_mixed_jobs", "jobs": len(jobs), "pixels": st_g["pixels"],
+                       "samples": int(samples), "scenes": ["cornell_box", "displaced_icosphere_1310720tri",
+                                                           "instanced_4096x10meshes_20000spheres",
+                                                           "displaced_plane_100k"]},
+            "batched": {"device_ms": round(st_g["deviceMs"], 3), "wall_ms": round(wall_g * 1e3, 3),
+                        "launches": st_g["launches"], "graph": True,
+                        "p50_ms": round(pct(done_g, 50), 3), "p99_ms": round(pct(done_g, 99), 3),
+                        "msamples_per_s": round(samples / (st_g["deviceMs"] * 1e-3) / 1e6, 1)},
+            "batched_no_graph": {"device_ms": round(res[False][1]["deviceMs"], 3),
+                                 "wall_ms": round(res[False][2] * 1e3, 3),
+                                 "p50_ms": round(pct(res[False][0], 50), 3), "p99_ms": round(pct(res[False][0], 99), 3)},
+            "sequential": {"device_ms": round(seq_total, 3), "wall_ms": round(seq_wall * 1e3, 3),
+                           "jobs_per_s": round(len(jobs) / (seq_total * 1e-3), 3),
+                           "p50_ms": round(pct(seq_done, 50), 3), "p99_ms": round(pct(seq_done, 99), 3)},
+            "speedup_vs_sequential": round(seq_total / st_g["deviceMs"], 3),
+            "sequential_per_scene": {["cornell", "icosphere", "instanced", "plane"][k]:
+                                     {"jobs": v[2], "device_ms": round(v[1], 1),
+                                      "msamples_per_s": round(v[0] / (v[1] * 1e-3) / 1e6, 1)}
+                                     for k, v in sorted(per_scene.items())},
+            "autotune": tuned["best"]}
+    print(json.dumps(line), flush=True)
+    for d in worlds:
+        d.close()
+
+
 def main():
     args = parse()
+    if args.workload == "batch":
+        run_batch(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -56,7 +56,8 @@ const ParamDesc PT_PARAMS[] = {
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
 	{ "Stage timing", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
-	{ "Trace refill lanes", PARAM_INT },
+	{ "Trace refill lanes", PARAM_INT }, { "Tail paths", PARAM_INT }, { "Iteration graph", PARAM_INT },
+	{ "Planned tail", PARAM_INT },
 };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
@@ -74,6 +75,9 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "Trace blocks per SM")) return &r.traceBlocksPerSm;
 	if(!std::strcmp(name, "Wavefront bounces")) return &r.wavefrontBounces;
 	if(!std::strcmp(name, "Trace refill lanes")) return &r.refillLanes;
+	if(!std::strcmp(name, "Tail paths")) return &r.tailPaths;
+	if(!std::strcmp(name, "Iteration graph")) return &r.iterationGraph;
+	if(!std::strcmp(name, "Planned tail")) return &r.planTail;
 	return nullptr;
 }
 
@@ -129,6 +133,12 @@ void load_scene_if_needed(MufflonInstance& I) {
 
 namespace mb {
 void RendererState::release() {
+	if(graphExec) cudaGraphExecDestroy(graphExec);
+	graphExec = nullptr;
+	graphKey.clear();
+	if(dIteration) cudaFree(dIteration);
+	if(hIteration) cudaFreeHost(hIteration);
+	dIteration = nullptr; hIteration = nullptr;
 	if(wfMemory) cudaFree(wfMemory);
 	wfMemory = nullptr;
 	wf = WfState{};
@@ -832,19 +842,82 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 			info.eventPairs = pairs;
 		}
 	}
-	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
-	if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
-	else {
-		WfTuning tune;
-		tune.traceBlocksPerSm = r.traceBlocksPerSm;
-		tune.wavefrontBounces = r.wavefrontBounces;
-		tune.refillLanes = r.refillLanes;
-		CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, tune));
+	WfTuning tune;
+	tune.traceBlocksPerSm = r.traceBlocksPerSm;
+	tune.wavefrontBounces = r.wavefrontBounces;
+	tune.refillLanes = r.refillLanes;
+	tune.tailPaths = r.tailPaths;
+	// The schedule is planned from the previous iteration's queue lengths
+	// when it ran with the same scene and parameters (every schedule renders
+	// the same bits; only the launch count differs).
+	std::vector<unsigned char> planKey;
+	{
+		auto addp = [&](const void* p, size_t b) { const unsigned char* c = static_cast<const unsigned char*>(p); planKey.insert(planKey.end(), c, c + b); };
+		addp(&I.scene.desc, sizeof(DScene)); addp(&r.params, sizeof(PtParams));
+		addp(&r.wavefrontBounces, sizeof(int32_t)); addp(&r.tailPaths, sizeof(int32_t));
+		addp(&r.width, sizeof(r.width)); addp(&r.height, sizeof(r.height));
+	}
+	if(!r.megakernel && r.planTail && planKey == r.planKey) tune.tailBounce = r.plannedTail;
+	const bool graph = !r.megakernel && !r.stageTiming && r.iterationGraph;
+	if(graph) {
+		// The launch sequence of an iteration is the same every iteration
+		// (the iteration number is read from device memory), so it is
+		// captured once and replayed; it is captured again when anything it
+		// was built from changes.
+		if(!r.dIteration) {
+			CHECK_CUDA(cudaMalloc(&r.dIteration, sizeof(int32_t)));
+			CHECK_CUDA(cudaMallocHost(&r.hIteration, sizeof(int32_t)));
+		}
+		rs.dIteration = r.dIteration;
+		rs.iteration = 0; // read from dIteration: not part of the captured launches
+		std::vector<unsigned char> key;
+		auto add = [&](const void* p, size_t b) { const unsigned char* c = static_cast<const unsigned char*>(p); key.insert(key.end(), c, c + b); };
+		add(&I.scene.desc, sizeof(DScene)); add(&r.params, sizeof(PtParams)); add(&tune, sizeof(WfTuning));
+		add(&rs, sizeof(RenderState)); add(&r.wf, sizeof(WfState)); add(&r.counters, sizeof(r.counters));
+		if(!r.graphExec || key != r.graphKey) {
+			if(r.graphExec) cudaGraphExecDestroy(r.graphExec);
+			r.graphExec = nullptr;
+			r.graphKey.clear();
+			prepare_batch_kernels(tune);
+			cudaGraph_t g = nullptr;
+			CHECK_CUDA(cudaStreamBeginCapture(I.stream, cudaStreamCaptureModeThreadLocal));
+			const cudaError_t e = launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, tune);
+			const cudaError_t e2 = cudaStreamEndCapture(I.stream, &g);
+			if(e != cudaSuccess || e2 != cudaSuccess) { if(g) cudaGraphDestroy(g); CHECK_CUDA(e); CHECK_CUDA(e2); }
+			const cudaError_t e3 = cudaGraphInstantiate(&r.graphExec, g, 0);
+			cudaGraphDestroy(g);
+			CHECK_CUDA(e3);
+			r.graphKey = key;
+			r.graphLaunches = info.launches;
+		}
+		*r.hIteration = r.iteration;
+		CHECK_CUDA(cudaMemcpyAsync(r.dIteration, r.hIteration, sizeof(int32_t), cudaMemcpyHostToDevice, I.stream));
+		CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
+		CHECK_CUDA(cudaGraphLaunch(r.graphExec, I.stream));
+		info.launches = r.graphLaunches;
+	} else {
+		CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
+		if(r.megakernel) CHECK_CUDA(launch_pt(I.scene.desc, r.params, rs, r.workCounter, r.counters, 0u, n, r.blocksPerSm, I.stream));
+		else CHECK_CUDA(launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, tune));
 	}
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters both[2];
 	CHECK_CUDA(cudaMemcpyAsync(both, r.counters, 2 * sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
+	unsigned bounceQueue[WF_BOUNCE_STATS] = {};
+	if(!r.megakernel)
+		CHECK_CUDA(cudaMemcpyAsync(bounceQueue, r.wf.counters + WF_COUNTERS - WF_BOUNCE_STATS, sizeof(bounceQueue),
+		                           cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	if(!r.megakernel) {
+		// next iteration's plan: the first bounce >= wavefrontBounces whose
+		// extension queue held at most tailPaths paths (none: no tail)
+		const int maxB = std::max(1, r.params.maxPathLength);
+		int plan = maxB;
+		for(int b = std::max(0, r.wavefrontBounces); b + 1 < maxB && b < int(WF_BOUNCE_STATS); ++b)
+			if(bounceQueue[b] <= unsigned(std::max(0, r.tailPaths))) { plan = b; break; }
+		r.plannedTail = plan;
+		r.planKey = planKey;
+	}
 	CHECK_CUDA(cudaEventElapsedTime(&r.lastKernelMs, r.evStart, r.evStop));
 	r.lastExtend = both[0];
 	r.lastShadow = both[1];
@@ -1155,6 +1228,7 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	tune.traceBlocksPerSm = r0.traceBlocksPerSm;
 	tune.wavefrontBounces = r0.wavefrontBounces;
 	tune.refillLanes = r0.refillLanes;
+	tune.tailPaths = r0.tailPaths;
 	prepare_batch_kernels(tune);
 	while(B.events.size() < size_t(maxSpp) + 1) {
 		cudaEvent_t e;

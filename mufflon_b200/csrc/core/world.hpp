@@ -166,6 +166,16 @@ struct RendererState {
 	int32_t traceBlocksPerSm = 6; // register budget of the wavefront trace kernel
 	int32_t wavefrontBounces = 2; // bounces run as separate stage launches before the tail launch
 	int32_t refillLanes = 32;     // idle trace lanes refilled together
+	int32_t tailPaths = 98304;    // queue length at or below which the tail launch takes over
+	int32_t iterationGraph = 1;   // replay the wavefront launches of an iteration as one CUDA graph
+	int32_t planTail = 1;         // plan the tail bounce from the previous iteration's queue lengths
+	std::vector<unsigned char> planKey;
+	int32_t plannedTail = -1;
+	cudaGraphExec_t graphExec = nullptr;
+	std::vector<unsigned char> graphKey;
+	int32_t graphLaunches = 0;
+	int32_t* dIteration = nullptr; // device copy of the iteration number read by the graph
+	int32_t* hIteration = nullptr; // page-locked staging of it
 	std::vector<cudaEvent_t> stageEvents;
 	std::vector<unsigned char> stageKinds;
 	float stageMs[WF_STAGES] = {};

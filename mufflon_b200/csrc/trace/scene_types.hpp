@@ -134,6 +134,7 @@ struct RenderState {
 	float* iterRadiance;    // optional per-iteration radiance (may be null)
 	uint32_t width, height;
 	int32_t iteration;      // 0 for the first iteration after a reset
+	const int32_t* dIteration; // if set: the iteration number is read here (a replayed CUDA graph)
 };
 
 // Counters accumulated by the kernels (one atomic per thread at exit).

@@ -29,7 +29,13 @@
 namespace mb {
 namespace {
 
-enum { C_QUEUE0 = 0, C_QUEUE1 = 1, C_SHADOW = 2, C_WORK = 3 };
+// counters: queue sizes, the shadow-slot count, the "paths handed to the tail"
+// flag, then one work counter per persistent launch
+enum { C_QUEUE0 = 0, C_QUEUE1 = 1, C_SHADOW0 = 2, C_SHADOW1 = 3, C_TAILED = 4, C_WORK = 5 };
+// Shade of bounce b appends its next rays to queue (b + 1) & 1 and its shadow
+// rays to shadow counter C_SHADOW0 + (b & 1); the trace launch of bounce b
+// reads queue b & 1 and shadow counter C_SHADOW0 + ((b - 1) & 1) and resets
+// the two counters that the following shade fills.
 
 MBD float nan_to_zero(float x) { return isnan(x) ? 0.0f : x; }
 MBD f3 contribute(f3 acc, f3 c) {
@@ -138,14 +144,20 @@ MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
 // that they do not displace the hierarchies from L2.
 template < int MINB, class SP >
 __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int q, int neeCount, int workIdx,
-                                                     TraceCounters* counters, int refillLanes) {
+                                                     TraceCounters* counters, int refillLanes, int bounce) {
 	__shared__ BlockStats stats;
 	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
 	__syncthreads();
+	if(*reinterpret_cast<volatile unsigned*>(W.counters + C_TAILED)) return; // the tail launch finished the paths
+	if(blockIdx.x == 0 && threadIdx.x == 0) {
+		W.counters[q ^ 1] = 0u;           // filled by this bounce's shade
+		W.counters[C_SHADOW0 + q] = 0u;
+		if(bounce < int(WF_BOUNCE_STATS)) W.counters[WF_COUNTERS - WF_BOUNCE_STATS + bounce] = W.counters[q];
+	}
 	uint2 stack[WIDE_STACK];
 	LocalCounters cnt;
 	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + q);
-	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW) / unsigned(neeCount);
+	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW0 + (q ^ 1)) / unsigned(neeCount);
 	const unsigned total = nExt + nGroups;
 	WideTracer t;
 	bool active = false, exhausted = false;
@@ -335,10 +347,7 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 // to the shadow queue (neeCount consecutive slots per path, allocated when
 // the first one is needed), the next ray to the other extension queue.
 template < class SP >
-__global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, int bounce) {
-	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
-	const unsigned slot = blockIdx.x * blockDim.x + threadIdx.x;
-	if(slot >= count) return;
+MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) {
 	const int p = __ldcs(W.qPath[q] + slot);
 	const DScene& S = sp.scene(p);
 	const PtParams& P = sp.params(p);
@@ -361,7 +370,7 @@ __global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, in
 	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
 		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c) {
 			if(base == 0xFFFFFFFFu) {
-				base = atomicAdd(W.counters + C_SHADOW, unsigned(P.neeCount));
+				base = atomicAdd(W.counters + C_SHADOW0 + q, unsigned(P.neeCount));
 				for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
 			}
 			W.sOrg[base + i] = pack(so, stmax);
@@ -379,6 +388,21 @@ __global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, in
 	W.qDir[out][nslot] = pack(nextD, 0.0f);
 }
 
+// Shade stage of the wavefront over queue q, grid-stride over its entries
+// (a fixed grid, so that a launch over a short or empty queue costs little).
+template < class SP >
+__global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, int bounce, unsigned tailMax, int tailAllowed) {
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	if(*reinterpret_cast<volatile unsigned*>(W.counters + C_TAILED)) return;
+	if(tailAllowed && count <= tailMax) {
+		// the tail launch of this bounce took the paths; later launches skip
+		if(blockIdx.x == 0 && threadIdx.x == 0) W.counters[C_TAILED] = 1u;
+		return;
+	}
+	for(unsigned slot = blockIdx.x * blockDim.x + threadIdx.x; slot < count; slot += gridDim.x * blockDim.x)
+		shade_slot(sp, W, q, bounce, slot);
+}
+
 // Tail of an iteration: persistent threads take the paths of extension queue
 // q (already traced, bounce `bounce`) one at a time and finish each of them in
 // place: shade, trace the next-event rays at once and add their contributions
@@ -387,12 +411,14 @@ __global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, in
 // dominated by launch and drain latency.
 template < int MINB, class SP >
 __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int q, int bounce,
-                                                    int workIdx, TraceCounters* counters) {
+                                                    int workIdx, TraceCounters* counters, unsigned tailMax) {
 	__shared__ BlockStats stats;
 	if(threadIdx.x < 12) (&stats.v[0][0])[threadIdx.x] = 0ull;
 	__syncthreads();
-	uint2 stack[WIDE_STACK];
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
+	// takes over only the first bounce whose queue holds at most tailMax paths
+	if(*reinterpret_cast<volatile unsigned*>(W.counters + C_TAILED) || count > tailMax) return;
+	uint2 stack[WIDE_STACK];
 	for(;;) {
 		const unsigned item = atomicAdd(W.counters + C_WORK + workIdx, 1u);
 		if(item >= count) break;
@@ -449,7 +475,8 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= numPixels) return;
-	const float den = fmaxf(1.0f, float(R.iteration) + 1.0f);
+	const int iteration = R.dIteration ? *R.dIteration : R.iteration;
+	const float den = fmaxf(1.0f, float(iteration) + 1.0f);
 	const float4 rad = W.rad[p];
 	if(R.radiance) {
 		float* cr = R.radiance + 3 * size_t(p);
@@ -525,7 +552,7 @@ __global__ void k_occlusion_wide(const DScene S, const float* a, const float* b,
 int persistent_blocks(const void* fn, int threads);
 
 template < class SP > struct TraceKernel {
-	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*, int);
+	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*, int, int);
 	Fn fn;
 	int blocks;
 };
@@ -542,7 +569,7 @@ template < class SP > TraceKernel<SP> trace_kernel(int perSm) {
 }
 
 template < class SP > struct TailKernel {
-	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*);
+	using Fn = void (*)(const SP, WfState, int, int, int, TraceCounters*, unsigned);
 	Fn fn;
 	int blocks;
 };
@@ -576,8 +603,11 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
                  const WfTuning& tuning, LaunchLog& log, cudaStream_t stream) {
 	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
 	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm);
-	const unsigned workSlots = WF_COUNTERS - C_WORK;
-	const unsigned grid = (numPaths + 127) / 128;
+	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
+	static int sms = 0;
+	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
+	const unsigned shadeGrid = std::max(1u, std::min((numPaths + 127) / 128, unsigned(sms) * 16u));
+	const unsigned tailMax = unsigned(tuning.tailPaths < 0 ? 0 : tuning.tailPaths);
 	unsigned work = 0;
 	for(int b = 0; b < maxBounces; ++b) {
 		const int q = b & 1;
@@ -586,21 +616,36 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 			work = 0;
 		}
 		log.begin(WF_EXTEND);
-		tk.fn<<<tk.blocks, 128, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes);
+		tk.fn<<<tk.blocks, 128, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes, b);
 		log.end();
-		if(b >= tuning.wavefrontBounces && b + 1 < maxBounces) {
-			// few paths are left: finish them in one launch
+		if(tuning.tailBounce >= 0) {
+			// planned schedule: the tail takes over at tailBounce, nothing follows
+			if(b == tuning.tailBounce && b + 1 < maxBounces) {
+				const TailKernel<SP> tl = tail_kernel<SP>();
+				log.begin(WF_TAIL);
+				tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters, 0xFFFFFFFFu);
+				log.end();
+				break;
+			}
+			log.begin(WF_SHADE);
+			k_shade<SP><<<(numPaths + 127) / 128, 128, 0, stream>>>(sp, W, q, b, 0u, 0); // one thread per entry
+			log.end();
+			continue;
+		}
+		// From bounce wavefrontBounces on, the first bounce whose queue holds
+		// at most tailMax paths is finished by one launch (decided on the
+		// device from the queue length); the later launches return at once.
+		const bool tailAllowed = b >= tuning.wavefrontBounces && b + 1 < maxBounces;
+		if(tailAllowed) {
 			const TailKernel<SP> tl = tail_kernel<SP>();
 			log.begin(WF_TAIL);
-			tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters);
+			tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters, tailMax);
 			log.end();
-			break;
 		}
-		// the shade of this bounce appends to the other queue and to the shadow queue
-		cudaMemsetAsync(W.counters + (q ^ 1), 0, sizeof(unsigned), stream);
-		cudaMemsetAsync(W.counters + C_SHADOW, 0, sizeof(unsigned), stream);
+		// the shade of this bounce appends to the other queue and to the shadow
+		// queue (the trace launch above reset both counters)
 		log.begin(WF_SHADE);
-		k_shade<SP><<<grid, 128, 0, stream>>>(sp, W, q, b);
+		k_shade<SP><<<shadeGrid, 128, 0, stream>>>(sp, W, q, b, tailMax, tailAllowed ? 1 : 0);
 		log.end();
 	}
 }
@@ -681,9 +726,11 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 	if(n == 0) return cudaSuccess;
 	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
 	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;
-	const unsigned workSlots = WF_COUNTERS - C_WORK;
-	const unsigned firstClear = unsigned(maxBounces) < workSlots ? unsigned(maxBounces) : workSlots;
+	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
+	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
 	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);
+	if(e == cudaSuccess)
+		e = cudaMemsetAsync(W.counters + WF_COUNTERS - WF_BOUNCE_STATS, 0, sizeof(unsigned) * WF_BOUNCE_STATS, stream);
 	if(e != cudaSuccess) return e;
 	W.rng = R.rngState;
 	const unsigned grid = (n + 127) / 128;
@@ -711,9 +758,11 @@ cudaError_t launch_pt_batch(const DJob* jobs, const uint16_t* pathJob, uint32_t 
 	if(numPixels == 0) return cudaSuccess;
 	if(neeCount < 1) neeCount = 1;
 	if(maxBounces < 1) maxBounces = 1;
-	const unsigned workSlots = WF_COUNTERS - C_WORK;
-	const unsigned firstClear = unsigned(maxBounces) < workSlots ? unsigned(maxBounces) : workSlots;
+	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
+	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
 	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);
+	if(e == cudaSuccess)
+		e = cudaMemsetAsync(W.counters + WF_COUNTERS - WF_BOUNCE_STATS, 0, sizeof(unsigned) * WF_BOUNCE_STATS, stream);
 	if(e != cudaSuccess) return e;
 	const unsigned grid = (numPixels + 127) / 128;
 	log.begin(WF_CAMERA);

@@ -24,9 +24,11 @@ struct WfState {
 	unsigned* counters;   // queue sizes and per-launch work counters (WF_COUNTERS)
 };
 
-// Size of WfState::counters: 3 queue sizes plus one work counter per
-// persistent launch (two per bounce); longer paths recycle the work counters.
+// Size of WfState::counters: queue sizes, flags and one work counter per
+// persistent launch (two per bounce; longer paths recycle them), then the
+// extension-queue length of each bounce (WF_BOUNCE_STATS entries at the end).
 constexpr unsigned WF_COUNTERS = 4096;
+constexpr unsigned WF_BOUNCE_STATS = 64;
 
 // WF_EXTEND: the trace launches of the wavefront bounces (extension and
 // shadow rays); WF_TAIL: the launch that finishes the remaining paths.
@@ -48,8 +50,12 @@ struct WfLaunchInfo {
 // shadow rays'.
 struct WfTuning {
 	int traceBlocksPerSm = 6;  // register budget of the trace kernel: 4, 5, 6 or 8 resident blocks of 128 threads
-	int wavefrontBounces = 2;  // bounces 0 .. this run as separate trace and shade launches, then one
-	                           // launch finishes every remaining path in place
+	int wavefrontBounces = 2;  // bounces 0 .. this-1 always run as separate trace and shade launches; from
+	                           // bounce this on, the first bounce with at most tailPaths queued paths
+	                           // is finished by one launch that runs every remaining path in place
+	int tailPaths = 98304;
+	int tailBounce = -1;       // >= 0: planned schedule, the tail launch takes over at this bounce and
+	                           // nothing is launched after it; -1: decided on the device per bounce
 	int refillLanes = 32;      // idle lanes of a trace warp are refilled together once this many are idle (1..32)
 };
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,

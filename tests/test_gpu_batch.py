@@ -93,3 +93,26 @@ def test_batch_rejects_bad_jobs(worlds):
         bindings.render_batch([dict(instance=d, spp=0, max_path=4)])
     with pytest.raises(bindings.MufflonError):
         bindings.render_batch([dict(instance=d, spp=1, max_path=4, nee=1), dict(instance=d, spp=1, max_path=4, nee=2)])
+
+
+def test_autotune_keeps_the_image(worlds):
+    """Tuning picks one of the candidates and does not change the rendered bits."""
+    from mufflon_b200 import autotune
+    d, _ = worlds["ico"]
+    d.render_enable_render_target("Radiance", False)
+    for name, v in {"Seed": 0, "Max. path length": 8, "Min. path length": 0, "NEE count": 1, "RR start depth": 0,
+                    "Megakernel": 0, "Wavefront bounces": 2, "Trace blocks per SM": 6, "Trace refill lanes": 32}.items():
+        assert d.renderer_set_parameter_int(name, v)
+    d.render_reset()
+    for _ in range(2):
+        d.render_iterate()
+    before = d.get_target_image("Radiance").copy()
+    cands = [dict(megakernel=0, trace_blocks=4, wavefront_bounces=1, refill_lanes=16),
+             dict(megakernel=0, trace_blocks=6, wavefront_bounces=3, refill_lanes=32), dict(megakernel=1)]
+    res = autotune.autotune(d, iterations=1, warmup=0, candidates=cands)
+    assert res["best"] in cands and len(res["table"]) == 3
+    for k, v in res["best"].items():
+        assert d.renderer_get_parameter_int(autotune.PARAMS[k]) == v
+    for _ in range(2):
+        d.render_iterate()
+    assert np.array_equal(d.get_target_image("Radiance"), before)

@@ -105,7 +105,8 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
 # kernel over the binary (reference-layout) hierarchies.
 KERNELS = {"wavefront": 0, "megakernel": 1}
 DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
-                  "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 2}
+                  "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 2, "Tail paths": 98304, "Iteration graph": 1,
+                  "Planned tail": 1}
 
 
 def _load(dll, spec):
@@ -246,15 +247,17 @@ def test_pt_multi_nee_min_path_parity(dll, oracle, kernel):
     assert orad.mean() > 0.01
 
 
-@pytest.mark.parametrize("wavefront_bounces", [0, 1, 3, 100])
-def test_pt_schedule_parity(dll, oracle, wavefront_bounces):
-    """Any split between per-bounce stage launches and the path-finishing launch gives the oracle's bits."""
+@pytest.mark.parametrize("wavefront_bounces,tail_paths", [(0, 98304), (1, 98304), (3, 98304), (100, 98304),
+                                                           (1, 0), (1, 2500)])
+def test_pt_schedule_parity(dll, oracle, wavefront_bounces, tail_paths):
+    """Any split between per-bounce stage launches and the path-finishing launch gives the oracle's bits
+    (tail_paths 2500 hands over in the middle of the paths, 0 never before the queues are empty)."""
     spec = scenes.cornell_box(5, 80, 80)
     _load(dll, spec)
     dll.render_enable_render_target("Radiance", False)
     dll.render_enable_render_target("Hit ID", False)
-    for name, value in {"Wavefront bounces": wavefront_bounces, "NEE count": 2, "Max. path length": 9,
-                        "RR start depth": 2, "Min. path length": 1}.items():
+    for name, value in {"Wavefront bounces": wavefront_bounces, "Tail paths": tail_paths, "NEE count": 2,
+                        "Max. path length": 9, "RR start depth": 2, "Min. path length": 1}.items():
         assert dll.renderer_set_parameter_int(name, value)
     pt = oracle.OraclePathTracer(oracle.OracleScene(spec), seed=0, min_path=1, max_path=9, nee_count=2, rr_start=2)
     for _ in range(2):
@@ -262,6 +265,26 @@ def test_pt_schedule_parity(dll, oracle, wavefront_bounces):
         pt.iterate()
     assert np.array_equal(dll.get_target_image("Hit ID"), pt.target("Hit ID"))
     assert rel_rmse(dll.get_target_image("Radiance"), pt.target("Radiance")) <= RMSE_TOL
+
+
+def test_graph_replay_equals_plain_launches(dll):
+    """An iteration replayed from its captured CUDA graph gives the same bits as plain launches,
+    also across a parameter change that forces a new capture."""
+    spec = scenes.cornell_box(7, 96, 64)
+    out = []
+    for graph in (1, 0):
+        _load(dll, spec)
+        dll.render_enable_render_target("Radiance", False)
+        dll.render_enable_render_target("Hit ID", False)
+        assert dll.renderer_set_parameter_int("Iteration graph", graph)
+        assert dll.renderer_set_parameter_int("Max. path length", 9)
+        for _ in range(3):
+            dll.render_iterate()
+        assert dll.renderer_set_parameter_int("Max. path length", 5)  # resets and re-captures
+        for _ in range(2):
+            dll.render_iterate()
+        out.append((dll.get_target_image("Radiance").copy(), dll.get_target_image("Hit ID").copy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
 def test_pt_long_paths_parity(dll, oracle):
