@@ -303,6 +303,23 @@ CORE_API Boolean CDECL mufflon_render_batch(const MufflonBatchJob* jobs, uint32_
                                             float* const* radiance, float* const* hitId, float* jobDoneMs,
                                             MufflonBatchStats* stats);
 
+/* EXTENSIONS for differentiable rendering, with no counterpart in the
+ * reference.
+ * mufflon_texture_update replaces the texels (width*height*4 floats, RGBA)
+ * of a texture created by the world API, also on the GPU if the loaded scene
+ * uses it, without reloading the scene; the accumulation is reset.
+ * mufflon_albedo_gradient computes the gradient of a loss with respect to an
+ * albedo texture by path replay: given imageGrad = dLoss/dImage (W*H*3 floats
+ * for the scenario's resolution, image = mean of spp samples as rendered by
+ * spp render_iterate calls after a reset), it writes dLoss/dTexel to
+ * textureGrad (width*height*3 floats, RGB) for the Lambert materials that
+ * use the texture as albedo (nearest-texel lookup). It uses the renderer's
+ * parameters and requires Russian roulette off (RR start depth >= Max. path
+ * length, at most 32). deviceMs (may be NULL) receives the kernels' time. */
+CORE_API Boolean CDECL mufflon_texture_update(MufflonInstanceHdl instHdl, TextureHdl texture, const float* rgba);
+CORE_API Boolean CDECL mufflon_albedo_gradient(MufflonInstanceHdl instHdl, TextureHdl texture, uint32_t spp,
+                                               const float* imageGrad, float* textureGrad, float* deviceMs);
+
 /* Host-side times (ms) of the last scene load (world_load_scenario or the
  * implicit load of the first render_iterate): the whole load, the geometry
  * upload, the object BVH builds (LBVH + 8-wide conversion), the instance BVH,

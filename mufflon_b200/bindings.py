@@ -284,6 +284,8 @@ class DllHolder:
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
             "mufflon_get_load_stats": (c_uint32, [c_void_p, POINTER(MufflonLoadStats)]),
+            "mufflon_texture_update": (c_uint32, [c_void_p, c_void_p, c_void_p]),
+            "mufflon_albedo_gradient": (c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_float)]),
             "mufflon_render_batch": (c_uint32, [POINTER(MufflonBatchJob), c_uint32, c_int32, c_void_p, c_void_p,
                                                 POINTER(c_float), POINTER(MufflonBatchStats)]),
             "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
@@ -457,6 +459,23 @@ class DllInterface:
         self._check(self.core.mufflon_get_load_stats(self.muffInst, byref(s)), "mufflon_get_load_stats")
         return {k: getattr(s, k) for k, _ in MufflonLoadStats._fields_ if k != "pad"}
 
+    def texture_update(self, texture, rgba):
+        """Replaces a texture's texels ((H, W, 4) or (H, W, 3) float32) on host and device; resets the accumulation."""
+        a = np.asarray(rgba, np.float32)
+        if a.ndim == 3 and a.shape[2] == 3:
+            a = np.concatenate([a, np.ones(a.shape[:2] + (1,), np.float32)], axis=2)
+        a = np.ascontiguousarray(a)
+        self._check(self.core.mufflon_texture_update(self.muffInst, texture, a.ctypes.data), "mufflon_texture_update")
+
+    def albedo_gradient(self, texture, spp, image_grad, tex_shape):
+        """dLoss/dTexel (H_t, W_t, 3) for imageGrad = dLoss/dImage (H, W, 3) of the spp-sample image."""
+        g = np.ascontiguousarray(image_grad, np.float32)
+        out = np.zeros((tex_shape[0], tex_shape[1], 3), np.float32)
+        ms = c_float(0.0)
+        self._check(self.core.mufflon_albedo_gradient(self.muffInst, texture, int(spp), g.ctypes.data, out.ctypes.data,
+                                                      byref(ms)), "mufflon_albedo_gradient")
+        return out, ms.value
+
     def trace_rays(self, rays, tmax=1048576.0, geo_normals=None):
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
@@ -563,6 +582,7 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
         t = core.world_add_texture_rgba32f(I, f"texture{k}".encode(), a.shape[1], a.shape[0], _ptr(a), 0)
         dll._check(t, "world_add_texture_rgba32f")
         textures.append(t)
+    dll.textures = textures
     for i, m in enumerate(spec.materials):
         name = f"mat{i}".encode()
         slot = core.scenario_declare_material_slot(sc, name, len(name))

@@ -1291,6 +1291,76 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	CATCH_ALL(false)
 }
 
+// ---------------------------------------------------------------- differentiable rendering
+Boolean mufflon_texture_update(MufflonInstanceHdl h, TextureHdl texHdl, const float* rgba) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(texHdl && rgba, "texture and texel data are required");
+	HostTexture* t = static_cast<HostTexture*>(texHdl);
+	const size_t n = size_t(t->width) * t->height * 4;
+	CHECK(t->texels.size() == n, "texture has no texel storage");
+	std::copy(rgba, rgba + n, t->texels.begin());
+	for(size_t k = 0; k < I.scene.textureSources.size(); ++k)
+		if(I.scene.textureSources[k] == t && I.scene.valid)
+			CHECK_CUDA(cudaMemcpyAsync(I.scene.textureBuffers[k], t->texels.data(), n * sizeof(float), cudaMemcpyHostToDevice, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	I.renderer.needsReset = true;
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_t spp, const float* imageGrad,
+                                float* textureGrad, float* deviceMs) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(texHdl && imageGrad && textureGrad && spp >= 1, "invalid arguments");
+	CHECK(I.current != nullptr, "no scenario loaded");
+	load_scene_if_needed(I);
+	const RendererState& r = I.renderer;
+	CHECK(r.params.rrStartDepth >= r.params.maxPathLength,
+	      "the albedo adjoint needs Russian roulette off: RR start depth >= Max. path length");
+	CHECK(r.params.maxPathLength <= ADJOINT_MAX_PATH, "the albedo adjoint supports paths of at most 32 vertices");
+	const HostTexture* t = static_cast<const HostTexture*>(texHdl);
+	int texIndex = -1;
+	for(size_t k = 0; k < I.scene.textureSources.size(); ++k)
+		if(I.scene.textureSources[k] == t) texIndex = int(k);
+	CHECK(texIndex >= 0, "the texture is not an albedo texture of the loaded scenario");
+	const uint32_t w = I.current->width, hgt = I.current->height;
+	const size_t n = size_t(w) * hgt, nt = size_t(t->width) * t->height;
+	DScene desc = I.scene.desc;
+	desc.camera.resX = uint16_t(w);
+	desc.camera.resY = uint16_t(hgt);
+	uint64_t* rng = nullptr;
+	float *dImg = nullptr, *dGrad = nullptr;
+	cudaEvent_t a = nullptr, b = nullptr;
+	auto cleanup = [&]() { cudaFree(rng); cudaFree(dImg); cudaFree(dGrad); if(a) cudaEventDestroy(a); if(b) cudaEventDestroy(b); };
+	try {
+		CHECK_CUDA(cudaMalloc(&rng, n * 8));
+		CHECK_CUDA(cudaMalloc(&dImg, n * 12));
+		CHECK_CUDA(cudaMalloc(&dGrad, nt * 12));
+		CHECK_CUDA(cudaEventCreate(&a));
+		CHECK_CUDA(cudaEventCreate(&b));
+		CHECK_CUDA(cudaMemcpyAsync(dImg, imageGrad, n * 12, cudaMemcpyHostToDevice, I.stream));
+		CHECK_CUDA(cudaMemsetAsync(dGrad, 0, nt * 12, I.stream));
+		CHECK_CUDA(launch_seed_rng(rng, uint32_t(n), r.params.seed, I.stream));
+		CHECK_CUDA(cudaEventRecord(a, I.stream));
+		for(uint32_t s = 0; s < spp; ++s)
+			CHECK_CUDA(launch_adjoint_albedo(desc, r.params, rng, w, hgt, texIndex, dImg, 1.0f / float(spp), dGrad, I.stream));
+		CHECK_CUDA(cudaEventRecord(b, I.stream));
+		CHECK_CUDA(cudaMemcpyAsync(textureGrad, dGrad, nt * 12, cudaMemcpyDeviceToHost, I.stream));
+		CHECK_CUDA(cudaStreamSynchronize(I.stream));
+		if(deviceMs) CHECK_CUDA(cudaEventElapsedTime(deviceMs, a, b));
+	} catch(...) {
+		cleanup();
+		throw;
+	}
+	cleanup();
+	return true;
+	CATCH_ALL(false)
+}
+
 Boolean mufflon_get_load_stats(MufflonInstanceHdl h, MufflonLoadStats* s) {
 	TRY
 	MufflonInstance& I = minst(h);

@@ -311,6 +311,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	D.lodSources.clear();
 	for(auto* t : D.textureBuffers) cudaFree(t);
 	D.textureBuffers.clear();
+	D.textureSources.clear();
 
 	// --- materials per slot (scene.cpp load_materials)
 	std::vector<DMaterial> mats(std::max<size_t>(sc->slotMaterials.size(), 1));
@@ -537,6 +538,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		size_t bufCap = 0;
 		if(!upload(buf, bufCap, reinterpret_cast<const float4*>(texList[t]->texels.data()), size_t(texList[t]->width) * texList[t]->height, s, err)) return false;
 		D.textureBuffers.push_back(buf);
+		D.textureSources.push_back(texList[t]);
 		dtex[t] = DTexture{ texList[t]->width, texList[t]->height, buf };
 	}
 	if(!upload(D.dTextures, D.cap[10], dtex.data(), texList.size(), s, err)) return false;

@@ -134,6 +134,7 @@ struct DeviceScene {
 	BvhBuffers tlas;
 	DMaterial* dMaterials = nullptr;
 	std::vector<float4*> textureBuffers;
+	std::vector<const HostTexture*> textureSources; // host texture of each device texture
 	DTexture* dTextures = nullptr;
 	DLight* dLights = nullptr;
 	DLightNode* dLightNodes = nullptr;

@@ -250,11 +250,21 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 // contribution are handed to shadow(i, origin, dir, length, contribution) in
 // the order i of pt_sample. Returns true and the next ray if the path goes on.
 // The generator `rng` is advanced exactly as pt_sample advances it.
-template < class ShadowFn >
+// What the adjoint needs to know about a vertex (see onVertex below).
+struct VertexInfo {
+	bool surface;
+	int materialIndex;  // -1 for the background
+	int materialType;
+	f2 uv;
+	f3 albedo;
+};
+
+template < class ShadowFn, class VertexFn >
 MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
                       f3& throughput, float& pdfF, f3& radiance, u64& rng, float2* hit0, f3& nextO, f3& nextD,
-                      ShadowFn&& shadow) {
+                      ShadowFn&& shadow, VertexFn&& onVertex) {
 	bool surface = false;
+	int matIndex = -1;
 	f3 position = make3(0.0f, 0.0f, 0.0f), incidentEncoded;
 	float incidentPdf;
 	TangentSpace ts;
@@ -268,7 +278,8 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 		position = origin + dir * hit.distance;
 		ts = tangent_space(S, hit);
 		incidentEncoded = make3(dir.x, dir.y, hit.distance * sgn(dir.z));
-		mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+		matIndex = material_index(S, hit.inst, hit.prim);
+		mat = fetch_material(S, uint16_t(matIndex), hit.uv);
 		const float inCosAbs = fabsf(dot(dir, ts.shadingN));
 		incidentPdf = __fdiv_rn(pdfF * fabsf(inCosAbs), hit.distance * hit.distance);
 	}
@@ -299,7 +310,13 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 			const float misWeight = __fdiv_rn(1.0f, 1.0f + float(P.neeCount) * __fdiv_rn(connectPdf, incidentPdf));
 			emission = emission * misWeight;
 		}
-		radiance = contribute(radiance, throughput * emission);
+		const f3 eterm = throughput * emission;
+		radiance = contribute(radiance, eterm);
+		onVertex(contribute(make3(0.0f, 0.0f, 0.0f), eterm), VertexInfo{ surface, matIndex, surface ? mat.type : -1, hit.uv,
+		                                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f) });
+	} else {
+		onVertex(make3(0.0f, 0.0f, 0.0f), VertexInfo{ surface, matIndex, surface ? mat.type : -1, hit.uv,
+		                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f) });
 	}
 	if(!surface || !(pathLen < P.maxPathLength)) return false;
 	// -- next loop iteration of pt_sample: next-event estimation
@@ -376,7 +393,7 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 			W.sOrg[base + i] = pack(so, stmax);
 			W.sDir[base + i] = pack(sd, 0.0f);
 			W.sContrib[base + i] = pack(c, 0.0f);
-		});
+		}, [](f3, const VertexInfo&) {});
 	W.rad[p] = pack(radiance, ra.w);
 	if(rng != rng0) W.rng[p] = rng;
 	if(!cont) return;
@@ -446,7 +463,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 					const bool occ = occluded_wide(S, so, sd, stmax, cnt, stack);
 					stats_add(stats, 1, cnt);
 					if(!occ) radiance = contribute(radiance, c);
-				});
+				}, [](f3, const VertexInfo&) {});
 			if(!cont) break;
 			origin = nextO;
 			dir = nextD;
@@ -492,6 +509,90 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	if(R.iterRadiance) {
 		float* o = R.iterRadiance + 3 * size_t(p);
 		o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
+	}
+}
+
+// Path-replay adjoint of the radiance with respect to one albedo texture
+// (no counterpart in the reference). One launch replays one sample of every
+// pixel with the generator state `rng` (seeded as for a reset render, so that
+// sample s replays iteration s of the forward render) through the same code
+// as the forward path tracer. With Russian roulette off (rrStartDepth >=
+// maxPathLength), the sample's radiance is a sum of terms that are products
+// of the Lambert albedos of the vertices before them; each term after vertex
+// k contains vertex k's albedo a_k once, so d(radiance)/d(a_k) = (sum of the
+// terms added after vertex k, its own next-event terms included) / a_k. The
+// suffix sums are kept per textured vertex (no subtraction of running sums),
+// and `scale * imageGrad[p] * suffix / a_k` is added to the gradient of the
+// texel the vertex looked up (nearest texel, as sample_texture).
+constexpr int ADJOINT_MAX_VERTICES = 32;
+
+__global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const PtParams P, uint64_t* rng,
+                                                            uint32_t numPixels, uint32_t width, int texIndex,
+                                                            const float* __restrict__ imageGrad, float scale,
+                                                            float* texGrad) {
+	uint2 stack[WIDE_STACK];
+	const DTexture tex = S.textures[texIndex];
+	for(uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < numPixels; p += gridDim.x * blockDim.x) {
+		u64 r = rng[p];
+		(void)pcg_next(r); // create_camera
+		const u64 x0 = pcg_next(r);
+		(void)pcg_next(r);
+		const float rr = sample_uniform(uint32_t(pcg_next(r)));
+		const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
+		float pdfF;
+		f3 dir = pinhole_ray(S.camera, int(p % width), int(p / width), ru0, ru1, pdfF);
+		f3 throughput = make3(1.0f, 1.0f, 1.0f);
+		bool alive = true;
+		if(0 >= P.rrStartDepth) {
+			const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
+			if(rr >= cp) alive = false;
+			else throughput = throughput / cp;
+		}
+		int texel[ADJOINT_MAX_VERTICES];
+		f3 alb[ADJOINT_MAX_VERTICES], suf[ADJOINT_MAX_VERTICES];
+		int n = 0;
+		f3 radiance = make3(0.0f, 0.0f, 0.0f);
+		f3 origin = lv(S.camera.position);
+		add_epsilon(origin, dir, make3(0.0f, 0.0f, 0.0f));
+		for(int b = 0; alive; ++b) {
+			LocalCounters cnt;
+			const HitRec hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
+			f3 nextO, nextD;
+			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, r, nullptr, nextO, nextD,
+				[&](int, f3 so, f3 sd, float stmax, f3 c) {
+					LocalCounters sc;
+					if(occluded_wide(S, so, sd, stmax, sc, stack)) return;
+					const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
+					radiance = radiance + cc;
+					for(int k = 0; k < n; ++k) suf[k] = suf[k] + cc;
+				},
+				[&](f3 e, const VertexInfo& v) {
+					for(int k = 0; k < n; ++k) suf[k] = suf[k] + e;
+					if(v.surface && v.materialType == MAT_LAMBERT && n < ADJOINT_MAX_VERTICES &&
+					   __ldg(&S.materials[v.materialIndex].albedoTex) == texIndex) {
+						const float fx = v.uv.x - floorf(v.uv.x), fy = v.uv.y - floorf(v.uv.y);
+						int x = int(fx * float(tex.width)), y = int(fy * float(tex.height));
+						if(x >= int(tex.width)) x = int(tex.width) - 1;
+						if(y >= int(tex.height)) y = int(tex.height) - 1;
+						texel[n] = y * int(tex.width) + x;
+						alb[n] = v.albedo;
+						suf[n] = make3(0.0f, 0.0f, 0.0f);
+						++n;
+					}
+				});
+			if(!cont) break;
+			origin = nextO;
+			dir = nextD;
+		}
+		rng[p] = r;
+		const f3 g = make3(imageGrad[3 * size_t(p)] * scale, imageGrad[3 * size_t(p) + 1] * scale,
+		                   imageGrad[3 * size_t(p) + 2] * scale);
+		for(int k = 0; k < n; ++k) {
+			float* t = texGrad + 3 * size_t(texel[k]);
+			if(alb[k].x > 0.0f && suf[k].x != 0.0f) atomicAdd(t, g.x * __fdiv_rn(suf[k].x, alb[k].x));
+			if(alb[k].y > 0.0f && suf[k].y != 0.0f) atomicAdd(t + 1, g.y * __fdiv_rn(suf[k].y, alb[k].y));
+			if(alb[k].z > 0.0f && suf[k].z != 0.0f) atomicAdd(t + 2, g.z * __fdiv_rn(suf[k].z, alb[k].z));
+		}
 	}
 }
 
@@ -690,6 +791,17 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
 	W.sDir = reinterpret_cast<float4*>(take(n * nee * 16));
 	W.sContrib = reinterpret_cast<float4*>(take(n * nee * 16));
 	W.counters = reinterpret_cast<unsigned*>(take(WF_COUNTERS * 4));
+}
+
+cudaError_t launch_adjoint_albedo(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
+                                  int texIndex, const float* imageGrad, float scale, float* texGrad, cudaStream_t stream) {
+	const uint32_t n = width * height;
+	if(n == 0) return cudaSuccess;
+	static int sms = 0;
+	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
+	const unsigned blocks = std::min<unsigned>((n + 127) / 128, unsigned(sms) * 8u);
+	k_adjoint_albedo<<<blocks, 128, 0, stream>>>(S, P, rng, n, width, texIndex, imageGrad, scale, texGrad);
+	return cudaGetLastError();
 }
 
 void prepare_batch_kernels(const WfTuning& tuning) {

@@ -78,6 +78,16 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W);
 // that a later stream capture does not have to.
 void prepare_batch_kernels(const WfTuning& tuning);
 
+// One sample of the path-replay adjoint for every pixel: adds
+// scale * dL/dI(p) * d(sample radiance)/d(texel) to texGrad (w * h * 3 floats)
+// for the albedo texture texIndex of the scene (Lambert vertices). `rng` is
+// the replay's per-pixel generator state, seeded as for a reset render and
+// advanced one sample per launch. Requires Russian roulette off.
+constexpr int ADJOINT_MAX_PATH = 32;
+cudaError_t launch_adjoint_albedo(const DScene& scene, const PtParams& params, uint64_t* rng, uint32_t width,
+                                  uint32_t height, int texIndex, const float* imageGrad, float scale, float* texGrad,
+                                  cudaStream_t stream);
+
 // One job of a batch: its scene (a loaded scene of some library instance),
 // path-tracer parameters, resolution, sample count, its pixels' place in the
 // batch's global pixel range, and its cumulative images.

@@ -186,6 +186,37 @@ def cornell_box(seed: int = 0, width: int = 256, height: int = 256) -> SceneSpec
                      width, height, name="cornell_box")
 
 
+def smooth_noise_texture(seed: int, size: int = 512, lo: float = 0.1, hi: float = 0.9) -> np.ndarray:
+    """(size, size, 4) float32 RGBA texture: seeded Gaussian noise, low-pass
+    filtered (periodic), scaled per channel to [lo, hi]; alpha 1."""
+    rng = np.random.default_rng(seed)
+    f = np.fft.fftfreq(size)
+    fx, fy = np.meshgrid(f, f)
+    lowpass = np.exp(-(fx ** 2 + fy ** 2) / (2 * (4.0 / size) ** 2))
+    out = np.ones((size, size, 4), np.float32)
+    for c in range(3):
+        v = np.real(np.fft.ifft2(np.fft.fft2(rng.normal(size=(size, size))) * lowpass))
+        v = (v - v.min()) / max(v.max() - v.min(), 1e-12)
+        out[..., c] = (lo + (hi - lo) * v).astype(np.float32)
+    return out
+
+
+def cornell_box_textured(seed: int = 0, width: int = 512, height: int = 512, texture=None,
+                         texture_size: int = 512) -> SceneSpec:
+    """The Cornell box with its back wall in its own Lambert material whose
+    albedo is texture 0 ((H, W, 4) float32; default a constant 0.5)."""
+    spec = cornell_box(seed, width, height)
+    tex = np.full((texture_size, texture_size, 4), 0.5, np.float32) if texture is None else np.asarray(texture, np.float32)
+    tex = np.ascontiguousarray(tex)
+    tex[..., 3] = 1.0
+    walls = spec.lods[0]
+    mats = walls.face_materials.copy()
+    mats[2] = len(spec.materials)  # the back wall quad
+    lods = [dataclasses.replace(walls, face_materials=mats)] + spec.lods[1:]
+    materials = spec.materials + [MaterialSpec(MAT_LAMBERT, albedo=(0.5, 0.5, 0.5), albedo_texture=0, name="back_wall")]
+    return dataclasses.replace(spec, lods=lods, materials=materials, textures=[tex], name="cornell_box_textured")
+
+
 # ------------------------------------------------------------------ meshes
 def value_noise3(p: np.ndarray, seed: int, octaves: int = 3) -> np.ndarray:
     """Seeded 3-octave value noise in [-1, 1] (trilinear lattice interpolation)."""

@@ -1637,8 +1637,27 @@ inline V3 pinhole_ray(const Camera& c, i32 px, i32 py, float u0, float u1, float
 	return dir;
 }
 
+// Records, in pt_sample's order, the terms a path sample adds to its radiance
+// and its Lambert vertices that look up albedo texture texIndex, and keeps in
+// double precision, per such vertex, the sum of the terms added after it
+// (its own next-event terms included). With Russian roulette off each of
+// those terms contains the vertex's albedo once, so the derivative of the
+// sample with respect to that albedo is suffix / albedo. This is the CPU
+// reference of the GPU path-replay adjoint (test infrastructure).
+struct AlbedoAdjoint {
+	i32 texIndex = -1;
+	int n = 0;
+	i32 texel[64];
+	double alb[64][3], suf[64][3];
+	void add_all(const V3& c) {
+		for(int k = 0; k < n; ++k) { suf[k][0] += c.x; suf[k][1] += c.y; suf[k][2] += c.z; }
+	}
+	void vertex(const Scene& S, const V3& e, bool surface, i32 type, i32 mat, V2 uv, V3 albedo);
+};
+
 // pt_common.hpp:75-156
-void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hitOut, Counters& cnt) {
+void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hitOut, Counters& cnt,
+               AlbedoAdjoint* adj = nullptr) {
 	const Scene& S = *st.scene;
 	const OrPtParams& P = st.params;
 	V3 throughput = { 1, 1, 1 };
@@ -1670,6 +1689,7 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 						const float hitPdf = val.pdfF * std::fabs(nee.cosOut) / nee.distSq;
 						const float mis = 1.0f / (float(P.neeCount) + hitPdf / nee.creationPdf);
 						radiance = contribute(radiance, ((throughput * val.cosOut) * rad) * mis);
+						if(adj) adj->add_all(contribute(V3{ 0, 0, 0 }, ((throughput * val.cosOut) * rad) * mis));
 					}
 				}
 			}
@@ -1702,6 +1722,8 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 		}
 		const V3 geoN = (v.type == V_SURFACE) ? v.ts.geoN : V3{ 0, 0, 0 };
 		Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt);
+		i32 vMat = -1;
+		const V2 vUv = hit.uv;
 		if(hit.inst < 0) {
 			v.type = V_VOID;
 			v.incidentEncoded = excident;
@@ -1717,7 +1739,8 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 			v.inst = hit.inst;
 			v.prim = hit.prim;
 			v.surfaceParams = hit.sp;
-			v.mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+			vMat = material_index(S, hit.inst, hit.prim);
+			v.mat = fetch_material(S, u16(vMat), hit.uv);
 			const float inCosAbs = std::fabs(dot(excident, ts.shadingN));
 			v.incidentPdf = pdfF * std::fabs(inCosAbs) / (hit.distance * hit.distance);
 		}
@@ -1749,11 +1772,28 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 				emission = emission * misWeight;
 			}
 			radiance = contribute(radiance, throughput * emission);
+			if(adj) adj->vertex(S, contribute(V3{ 0, 0, 0 }, throughput * emission), v.type == V_SURFACE, v.mat.type, vMat, vUv, v.mat.albedo);
+		} else if(adj) {
+			adj->vertex(S, V3{ 0, 0, 0 }, v.type == V_SURFACE, v.mat.type, vMat, vUv, v.mat.albedo);
 		}
 		if(v.type != V_SURFACE) break;
 	} while(pathLen < P.maxPathLength);
 	radianceOut = radiance;
 	hitOut = hitAcc;
+}
+
+void AlbedoAdjoint::vertex(const Scene& S, const V3& e, bool surface, i32 type, i32 mat, V2 uv, V3 albedo) {
+	add_all(e);
+	if(!surface || type != OR_MAT_LAMBERT || n >= 64 || mat < 0 || S.materials[size_t(mat)].albedoTex != texIndex) return;
+	const Texture& t = S.textures[size_t(texIndex)];
+	const float fx = uv.x - std::floor(uv.x), fy = uv.y - std::floor(uv.y);
+	i32 x = i32(fx * float(t.w)), y = i32(fy * float(t.h));
+	if(x >= i32(t.w)) x = i32(t.w) - 1;
+	if(y >= i32(t.h)) y = i32(t.h) - 1;
+	texel[n] = y * i32(t.w) + x;
+	alb[n][0] = albedo.x; alb[n][1] = albedo.y; alb[n][2] = albedo.z;
+	suf[n][0] = suf[n][1] = suf[n][2] = 0.0;
+	++n;
 }
 
 void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
@@ -2052,6 +2092,50 @@ void* oracle_pt_create(void* s, const OrPtParams* params) {
 }
 
 void oracle_pt_destroy(void* p) { delete static_cast<PtState*>(p); }
+
+int oracle_albedo_gradient(void* p, int32_t texIndex, uint32_t spp, const float* imageGrad, double* gradOut, int32_t nt) {
+	PtState& st = *static_cast<PtState*>(p);
+	const Scene& S = *st.scene;
+	if(texIndex < 0 || size_t(texIndex) >= S.textures.size() || spp == 0) return 0;
+	if(st.params.rrStartDepth < st.params.maxPathLength) return 0; // Russian roulette must be off
+	const i32 num = i32(S.width * S.height);
+	const Texture& t = S.textures[size_t(texIndex)];
+	const size_t nt3 = size_t(t.w) * t.h * 3;
+	const i32 seed = i32(u32(st.params.seed) * u32(num + 1));
+	if(nt <= 0) nt = 1;
+	std::vector<std::vector<double>> part(size_t(nt), std::vector<double>(nt3, 0.0));
+#pragma omp parallel num_threads(nt)
+	{
+		int tid = 0;
+#ifdef _OPENMP
+		tid = omp_get_thread_num();
+#endif
+		std::vector<double>& g = part[size_t(tid)];
+		Counters cnt;
+		AlbedoAdjoint adj;
+		adj.texIndex = texIndex;
+#pragma omp for schedule(static, 64)
+		for(i32 pixel = 0; pixel < num; ++pixel) {
+			Pcg64 rng = Pcg64::seeded(u32(i32(u32(pixel) + u32(seed))));
+			const double w[3] = { double(imageGrad[3 * size_t(pixel)]) / spp, double(imageGrad[3 * size_t(pixel) + 1]) / spp,
+			                      double(imageGrad[3 * size_t(pixel) + 2]) / spp };
+			for(u32 s = 0; s < spp; ++s) {
+				adj.n = 0;
+				V3 rad; V2 hid;
+				pt_sample(st, pixel % i32(S.width), pixel / i32(S.width), rng, rad, hid, cnt, &adj);
+				for(int k = 0; k < adj.n; ++k)
+					for(int c = 0; c < 3; ++c)
+						if(adj.alb[k][c] > 0.0) g[3 * size_t(adj.texel[k]) + c] += w[c] * adj.suf[k][c] / adj.alb[k][c];
+			}
+		}
+	}
+	for(size_t i = 0; i < nt3; ++i) {
+		double acc = 0.0;
+		for(auto& g : part) acc += g[i];
+		gradOut[i] = acc;
+	}
+	return 1;
+}
 
 int oracle_pt_iterate(void* p, int32_t nt) {
 	PtState* st = static_cast<PtState*>(p);

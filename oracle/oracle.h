@@ -112,6 +112,13 @@ int oracle_trace_any(void* scene, const float* pointsA, const float* pointsB, ui
 /* Path tracer (CpuPathTracer equivalent). */
 void* oracle_pt_create(void* scene, const OrPtParams* params);
 void oracle_pt_destroy(void* pt);
+/* Gradient of a loss with respect to albedo texture texIndex (Lambert
+ * vertices) by replaying spp samples per pixel from a fresh seed, with the
+ * suffix sums and the gradient in double precision; imageGrad = dLoss/dImage
+ * (W*H*3), gradOut = W_t*H_t*3 doubles. Requires Russian roulette off.
+ * Returns 0 on invalid arguments. */
+int oracle_albedo_gradient(void* pt, int32_t texIndex, uint32_t spp, const float* imageGrad, double* gradOut,
+                           int32_t threads);
 int oracle_pt_iterate(void* pt, int32_t numThreads);
 /* Cumulative target: 0 radiance (3 ch), 1 hit id (2 ch) */
 int oracle_pt_get_target(void* pt, int32_t target, float* out);

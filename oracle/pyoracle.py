@@ -79,6 +79,8 @@ def lib():
         L.oracle_pt_create.restype = C.c_void_p
         L.oracle_pt_create.argtypes = [C.c_void_p, C.POINTER(OrPtParams)]
         L.oracle_pt_destroy.argtypes = [C.c_void_p]
+        L.oracle_albedo_gradient.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int32]
+        L.oracle_albedo_gradient.restype = C.c_int
         L.oracle_pt_iterate.argtypes = [C.c_void_p, C.c_int32]
         L.oracle_pt_iterate_rows.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32]
         L.oracle_pt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
@@ -236,6 +238,18 @@ class OraclePathTracer:
             lib().oracle_pt_get_target(self.handle, 1, _ptr(out))
         else:
             raise KeyError(name)
+        return out
+
+    def albedo_gradient(self, texture_index: int, spp: int, image_grad, threads: int = 0) -> np.ndarray:
+        """dLoss/dTexel (H_t, W_t, 3) in float64 for imageGrad = dLoss/dImage (H, W, 3), replaying spp
+        samples per pixel from the seed (test reference of the GPU adjoint)."""
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        tex = self.scene.spec.textures[texture_index]
+        g = np.ascontiguousarray(image_grad, np.float32)
+        out = np.zeros((tex.shape[0], tex.shape[1], 3), np.float64)
+        if not lib().oracle_albedo_gradient(self.handle, texture_index, spp, _ptr(g), _ptr(out), threads):
+            raise ValueError("oracle_albedo_gradient: invalid arguments (is Russian roulette off?)")
         return out
 
     def stats(self):
