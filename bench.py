@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint"],
                    help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one")
     p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
@@ -501,10 +501,87 @@ def run_batch(args):
         d.close()
 
 
+def run_adjoint(args):
+    """Config 4: gradient of an L2 image loss with respect to a 512^2 RGB albedo
+    texture on the Cornell box's back wall (init 0.5), 512^2 image, 16 spp,
+    depth 6; target rendered with a seeded smoothed-noise texture in
+    [0.1, 0.9]. Reports forward time (16 iterations), adjoint time (replay of
+    the 16 samples) and their ratio, and checks the gradient against the
+    oracle's double-precision gradient and against central differences of GPU
+    renders on 64 texel channels."""
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import bindings, build, scenes
+    from mufflon_b200.adjoint import AlbedoRenderer
+    build.build()
+    spp, depth, res, tsz = 16, 6, 512, 512
+    spec = scenes.cornell_box_textured(0, res, res, texture_size=tsz)
+    d = bindings.DllInterface()
+    bindings.load_scene_spec(d, spec)
+    assert d.render_enable_renderer(0, 0)
+    r = AlbedoRenderer(d, d.textures[0], (tsz, tsz), spp=spp, seed=0, max_path=depth)
+    target_tex = scenes.smooth_noise_texture(1, tsz)[..., :3]
+    target = r.render(target_tex)
+    tex = np.full((tsz, tsz, 3), 0.5, np.float32)
+    fwd, adj = [], []
+    for _ in range(3 + args.steps):
+        img = r.render(tex)
+        dldi = 2.0 * (img - target)
+        g = r.gradient(dldi)
+        fwd.append(r.last_forward_ms)
+        adj.append(r.last_adjoint_ms)
+    fwd_ms, adj_ms = float(np.median(fwd[3:])), float(np.median(adj[3:]))
+    # FD on the 64 texel channels with the largest gradients (central, step 0.1: exact for the polynomial)
+    loss = lambda t: float(np.sum((r.render(t).astype(np.float64) - target) ** 2))
+    idx = np.argsort(-np.abs(g).reshape(-1))[:64]
+    fd_err = []
+    for k in idx:
+        y, x, c = np.unravel_index(k, g.shape)
+        tp, tm = tex.copy(), tex.copy()
+        tp[y, x, c] += 0.1
+        tm[y, x, c] -= 0.1
+        fd = (loss(tp) - loss(tm)) / 0.2
+        fd_err.append(abs(fd - g[y, x, c]) / max(abs(g[y, x, c]), 1e-12))
+    ora = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle import pyoracle
+        pt = pyoracle.OraclePathTracer(pyoracle.OracleScene(dataclasses_replace_texture(spec, tex)), seed=0,
+                                       max_path=depth, rr_start=depth)
+        t0 = time.perf_counter()
+        ref = pt.albedo_gradient(0, spp, dldi)
+        cpu_s = time.perf_counter() - t0
+        scale = np.abs(ref).max()
+        big = np.abs(ref) > 1e-2 * scale
+        ora = {"max_abs_err_over_max": float(np.abs(g - ref).max() / scale),
+               "max_rel_err_significant": float(np.max(np.abs(g[big] - ref[big]) / np.abs(ref[big]))),
+               "cpu_seconds": round(cpu_s, 2), "cpu_cores": os.cpu_count()}
+    line = {"metric": "adjoint/forward time (512^2, 16 spp, depth 6, 512^2 albedo texture)",
+            "value": round(adj_ms / fwd_ms, 3), "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
+            "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "cornell_textured_adjoint", "resolution": [res, res], "spp": spp, "depth": depth,
+                       "texture": [tsz, tsz, 3], "russian_roulette": "off"},
+            "forward_ms": round(fwd_ms, 3), "adjoint_ms": round(adj_ms, 3),
+            "fd_check": {"texels": len(fd_err), "step": 0.1, "max_rel_err": float(np.max(fd_err))},
+            "fp64_oracle_check": ora}
+    print(json.dumps(line), flush=True)
+    d.close()
+
+
+def dataclasses_replace_texture(spec, tex3):
+    import dataclasses
+    t = np.ones(tex3.shape[:2] + (4,), np.float32)
+    t[..., :3] = tex3
+    return dataclasses.replace(spec, textures=[t])
+
+
 def main():
     args = parse()
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     if args.impl == "reference":
         run_reference(args)

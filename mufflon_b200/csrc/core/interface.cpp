@@ -1334,9 +1334,20 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 	desc.camera.resY = uint16_t(hgt);
 	uint64_t* rng = nullptr;
 	float *dImg = nullptr, *dGrad = nullptr;
+	void* adjMem = nullptr;
 	cudaEvent_t a = nullptr, b = nullptr;
-	auto cleanup = [&]() { cudaFree(rng); cudaFree(dImg); cudaFree(dGrad); if(a) cudaEventDestroy(a); if(b) cudaEventDestroy(b); };
+	auto cleanup = [&]() {
+		cudaFree(rng); cudaFree(dImg); cudaFree(dGrad); cudaFree(adjMem);
+		if(a) cudaEventDestroy(a);
+		if(b) cudaEventDestroy(b);
+	};
+	const bool wavefront = !r.megakernel;
+	if(wavefront) {
+		ensure_render_buffers(I);
+		ensure_wavefront_buffers(I);
+	}
 	try {
+		if(wavefront) CHECK_CUDA(cudaMalloc(&adjMem, adjoint_bytes(n, r.params.maxPathLength)));
 		CHECK_CUDA(cudaMalloc(&rng, n * 8));
 		CHECK_CUDA(cudaMalloc(&dImg, n * 12));
 		CHECK_CUDA(cudaMalloc(&dGrad, nt * 12));
@@ -1346,8 +1357,18 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		CHECK_CUDA(cudaMemsetAsync(dGrad, 0, nt * 12, I.stream));
 		CHECK_CUDA(launch_seed_rng(rng, uint32_t(n), r.params.seed, I.stream));
 		CHECK_CUDA(cudaEventRecord(a, I.stream));
-		for(uint32_t s = 0; s < spp; ++s)
-			CHECK_CUDA(launch_adjoint_albedo(desc, r.params, rng, w, hgt, texIndex, dImg, 1.0f / float(spp), dGrad, I.stream));
+		WfTuning tune;
+		tune.traceBlocksPerSm = r.traceBlocksPerSm;
+		tune.wavefrontBounces = r.wavefrontBounces;
+		tune.refillLanes = r.refillLanes;
+		tune.tailPaths = r.tailPaths;
+		for(uint32_t s = 0; s < spp; ++s) {
+			if(wavefront)
+				CHECK_CUDA(launch_adjoint_wavefront(desc, r.params, rng, w, hgt, r.wf, adjMem, r.params.maxPathLength, texIndex,
+				                                    dImg, 1.0f / float(spp), dGrad, r.counters, I.stream, tune));
+			else
+				CHECK_CUDA(launch_adjoint_albedo(desc, r.params, rng, w, hgt, texIndex, dImg, 1.0f / float(spp), dGrad, I.stream));
+		}
 		CHECK_CUDA(cudaEventRecord(b, I.stream));
 		CHECK_CUDA(cudaMemcpyAsync(textureGrad, dGrad, nt * 12, cudaMemcpyDeviceToHost, I.stream));
 		CHECK_CUDA(cudaStreamSynchronize(I.stream));

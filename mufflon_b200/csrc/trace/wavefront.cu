@@ -62,12 +62,50 @@ MBD unsigned warp_reserve(unsigned* counter, unsigned want) {
 // argument for a plain render, or the device job table of a batch, whose jobs
 // share the queues (path p belongs to job pathJob[p]).
 struct OneScene {
+	static constexpr bool adjoint = false;
 	DScene S;
 	PtParams P;
 	MBD const DScene& scene(int) const { return S; }
 	MBD const PtParams& params(int) const { return P; }
 };
+
+// Per-path bookkeeping of the albedo adjoint (path replay through the
+// wavefront kernels): for every Lambert vertex that looked up albedo texture
+// texIndex, its texel and albedo and the sum of the radiance terms added
+// after it. Entry k of path p lives at k * numPaths + p.
+struct AdjointState {
+	int texIndex;
+	uint32_t numPaths, maxEntries;
+	DTexture tex;
+	int* count;        // entries per path
+	float4* entry;     // albedo xyz, texel index bits in w
+	float4* suffix;    // suffix sum xyz
+	const float* imageGrad;
+	float scale;
+	float* texGrad;
+};
+MBD void adjoint_add(const AdjointState& A, int p, f3 c) {
+	const int n = A.count[p];
+	for(int k = 0; k < n; ++k) {
+		float4& s = A.suffix[size_t(k) * A.numPaths + p];
+		s.x += c.x; s.y += c.y; s.z += c.z;
+	}
+}
+struct VertexInfo;
+MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, bool surface, int type, int mat, f2 uv,
+                        f3 albedo);
+
+// A plain render whose paths also keep the adjoint's bookkeeping.
+struct OneSceneAdjoint {
+	static constexpr bool adjoint = true;
+	DScene S;
+	PtParams P;
+	AdjointState A;
+	MBD const DScene& scene(int) const { return S; }
+	MBD const PtParams& params(int) const { return P; }
+};
 struct JobScenes {
+	static constexpr bool adjoint = false;
 	const DJob* jobs;
 	const uint16_t* pathJob;
 	MBD const DScene& scene(int p) const { return jobs[pathJob[p]].scene; }
@@ -207,7 +245,11 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 			} else {
 				stats_add(stats, 1, cnt);
 				const unsigned slot = (item - nExt) * unsigned(neeCount) + unsigned(ray);
-				if(!t.occluded) radiance = contribute(radiance, f4to3(__ldcs(W.sContrib + slot)));
+				if(!t.occluded) {
+					const f3 c = f4to3(__ldcs(W.sContrib + slot));
+					radiance = contribute(radiance, c);
+					if constexpr(SP::adjoint) adjoint_add(sp.A, path, contribute(make3(0.0f, 0.0f, 0.0f), c));
+				}
 				++ray;
 				seek = true;
 			}
@@ -393,7 +435,9 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 			W.sOrg[base + i] = pack(so, stmax);
 			W.sDir[base + i] = pack(sd, 0.0f);
 			W.sContrib[base + i] = pack(c, 0.0f);
-		}, [](f3, const VertexInfo&) {});
+		}, [&](f3 e, const VertexInfo& v) {
+			if constexpr(SP::adjoint) adjoint_vertex(sp.A, S, p, e, v.surface, v.materialType, v.materialIndex, v.uv, v.albedo);
+		});
 	W.rad[p] = pack(radiance, ra.w);
 	if(rng != rng0) W.rng[p] = rng;
 	if(!cont) return;
@@ -462,8 +506,13 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 					LocalCounters cnt;
 					const bool occ = occluded_wide(S, so, sd, stmax, cnt, stack);
 					stats_add(stats, 1, cnt);
-					if(!occ) radiance = contribute(radiance, c);
-				}, [](f3, const VertexInfo&) {});
+					if(!occ) {
+						radiance = contribute(radiance, c);
+						if constexpr(SP::adjoint) adjoint_add(sp.A, p, contribute(make3(0.0f, 0.0f, 0.0f), c));
+					}
+				}, [&](f3 e, const VertexInfo& v) {
+					if constexpr(SP::adjoint) adjoint_vertex(sp.A, S, p, e, v.surface, v.materialType, v.materialIndex, v.uv, v.albedo);
+				});
 			if(!cont) break;
 			origin = nextO;
 			dir = nextD;
@@ -509,6 +558,40 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	if(R.iterRadiance) {
 		float* o = R.iterRadiance + 3 * size_t(p);
 		o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
+	}
+}
+
+MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, bool surface, int type, int mat, f2 uv,
+                        f3 albedo) {
+	adjoint_add(A, p, e);
+	if(!surface || type != MAT_LAMBERT || __ldg(&S.materials[mat].albedoTex) != A.texIndex) return;
+	const int k = A.count[p];
+	if(k >= int(A.maxEntries)) return;
+	const float fx = uv.x - floorf(uv.x), fy = uv.y - floorf(uv.y);
+	int x = int(fx * float(A.tex.width)), y = int(fy * float(A.tex.height));
+	if(x >= int(A.tex.width)) x = int(A.tex.width) - 1;
+	if(y >= int(A.tex.height)) y = int(A.tex.height) - 1;
+	A.entry[size_t(k) * A.numPaths + p] = make_float4(albedo.x, albedo.y, albedo.z, __int_as_float(y * int(A.tex.width) + x));
+	A.suffix[size_t(k) * A.numPaths + p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	A.count[p] = k + 1;
+}
+
+// End of an adjoint sample: d(sample)/d(a_k) = suffix_k / a_k, weighted by
+// scale * dL/dI of the pixel, added to the texel gradient.
+__global__ void k_adjoint_scatter(AdjointState A) {
+	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(p >= A.numPaths) return;
+	const int n = A.count[p];
+	if(n == 0) return;
+	const f3 g = make3(A.imageGrad[3 * size_t(p)] * A.scale, A.imageGrad[3 * size_t(p) + 1] * A.scale,
+	                   A.imageGrad[3 * size_t(p) + 2] * A.scale);
+	for(int k = 0; k < n; ++k) {
+		const float4 a = A.entry[size_t(k) * A.numPaths + p];
+		const float4 sf = A.suffix[size_t(k) * A.numPaths + p];
+		float* t = A.texGrad + 3 * size_t(__float_as_int(a.w));
+		if(a.x > 0.0f && sf.x != 0.0f) atomicAdd(t, g.x * __fdiv_rn(sf.x, a.x));
+		if(a.y > 0.0f && sf.y != 0.0f) atomicAdd(t + 1, g.y * __fdiv_rn(sf.y, a.y));
+		if(a.z > 0.0f && sf.z != 0.0f) atomicAdd(t + 2, g.z * __fdiv_rn(sf.z, a.z));
 	}
 }
 
@@ -801,6 +884,54 @@ cudaError_t launch_adjoint_albedo(const DScene& S, const PtParams& P, uint64_t* 
 	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
 	const unsigned blocks = std::min<unsigned>((n + 127) / 128, unsigned(sms) * 8u);
 	k_adjoint_albedo<<<blocks, 128, 0, stream>>>(S, P, rng, n, width, texIndex, imageGrad, scale, texGrad);
+	return cudaGetLastError();
+}
+
+size_t adjoint_bytes(size_t numPaths, int maxEntries) {
+	return wf_align(numPaths * 4) + 2 * wf_align(numPaths * size_t(maxEntries) * 16);
+}
+
+cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
+                                     WfState W, void* adjointMemory, int maxEntries, int texIndex, const float* imageGrad,
+                                     float scale, float* texGrad, TraceCounters* counters, cudaStream_t stream,
+                                     const WfTuning& tuning) {
+	const uint32_t n = width * height;
+	if(n == 0) return cudaSuccess;
+	AdjointState A;
+	A.texIndex = texIndex;
+	A.numPaths = n;
+	A.maxEntries = uint32_t(maxEntries);
+	char* m = static_cast<char*>(adjointMemory);
+	A.count = reinterpret_cast<int*>(m);
+	m += wf_align(size_t(n) * 4);
+	A.entry = reinterpret_cast<float4*>(m);
+	m += wf_align(size_t(n) * maxEntries * 16);
+	A.suffix = reinterpret_cast<float4*>(m);
+	A.imageGrad = imageGrad;
+	A.scale = scale;
+	A.texGrad = texGrad;
+	cudaError_t e = cudaMemcpyAsync(&A.tex, S.textures + texIndex, sizeof(DTexture), cudaMemcpyDeviceToHost, stream);
+	if(e == cudaSuccess) e = cudaStreamSynchronize(stream);
+	if(e == cudaSuccess) e = cudaMemsetAsync(A.count, 0, size_t(n) * 4, stream);
+	if(e != cudaSuccess) return e;
+	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
+	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;
+	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
+	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
+	if((e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream)) != cudaSuccess) return e;
+	W.rng = rng;
+	const unsigned grid = (n + 127) / 128;
+	k_camera<<<grid, 128, 0, stream>>>(S, P, W, n, width);
+	OneSceneAdjoint one;
+	one.S = S;
+	one.P = P;
+	one.A = A;
+	WfLaunchInfo none;
+	LaunchLog log{ none, stream };
+	WfTuning t = tuning;
+	t.tailBounce = -1;
+	run_bounces(one, W, counters, n, maxBounces, neeCount, t, log, stream);
+	k_adjoint_scatter<<<grid, 128, 0, stream>>>(A);
 	return cudaGetLastError();
 }
 

@@ -88,6 +88,15 @@ cudaError_t launch_adjoint_albedo(const DScene& scene, const PtParams& params, u
                                   uint32_t height, int texIndex, const float* imageGrad, float scale, float* texGrad,
                                   cudaStream_t stream);
 
+// The same adjoint sample through the wavefront kernels (one sample for
+// every pixel per call): `adjointMemory` holds adjoint_bytes(width * height,
+// maxEntries) bytes of per-path bookkeeping, maxEntries >= the max path length.
+size_t adjoint_bytes(size_t numPaths, int maxEntries);
+cudaError_t launch_adjoint_wavefront(const DScene& scene, const PtParams& params, uint64_t* rng, uint32_t width,
+                                     uint32_t height, WfState W, void* adjointMemory, int maxEntries, int texIndex,
+                                     const float* imageGrad, float scale, float* texGrad, TraceCounters* counters,
+                                     cudaStream_t stream, const WfTuning& tuning);
+
 // One job of a batch: its scene (a loaded scene of some library instance),
 // path-tracer parameters, resolution, sample count, its pixels' place in the
 // batch's global pixel range, and its cumulative images.

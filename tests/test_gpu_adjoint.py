@@ -46,8 +46,11 @@ def test_forward_matches_oracle(world, oracle):
     assert np.sqrt(np.mean((img - ref) ** 2)) <= 1e-4 * np.sqrt(np.mean(ref ** 2))
 
 
-def test_gradient_matches_fp64_oracle(world, oracle):
+@pytest.mark.parametrize("megakernel", [0, 1])
+def test_gradient_matches_fp64_oracle(world, oracle, megakernel):
+    """Both adjoint schedules: through the wavefront kernels (default) and one thread per path."""
     d, spec, tex = world
+    assert d.renderer_set_parameter_int("Megakernel", megakernel)
     r = _renderer(d)
     target = _target()
     img = r.render(tex[..., :3])
@@ -60,6 +63,7 @@ def test_gradient_matches_fp64_oracle(world, oracle):
     assert np.abs(g - ref).max() <= 1e-4 * scale
     big = np.abs(ref) > 1e-2 * scale
     assert np.all(np.abs(g[big] - ref[big]) <= 1e-3 * np.abs(ref[big]))
+    assert d.renderer_set_parameter_int("Megakernel", 0)
 
 
 def test_gradient_matches_central_differences(world):
