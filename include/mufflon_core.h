@@ -112,6 +112,15 @@ typedef struct {
 	union { FILE* file; const char* bytes; } descriptor;
 } BulkLoader;
 
+/* core_interface.h:77-83 */
+typedef struct {
+	uint32_t vertices;
+	uint32_t triangles;
+	uint32_t quads;
+	uint32_t edges;
+	uint32_t spheres;
+} LodMetadata;
+
 #define INVALID_INDEX ((int32_t)-1)
 
 /* ---- instance, logging: core_interface.h:345-353 ---- */
@@ -122,6 +131,13 @@ CORE_API MufflonInstanceHdl CDECL mufflon_initialize(void);
 CORE_API void CDECL mufflon_destroy(MufflonInstanceHdl instHdl);
 CORE_API int32_t CDECL mufflon_get_cuda_device_index(void);
 CORE_API Boolean CDECL mufflon_is_cuda_available(void);
+/* core_interface.h:355-357: a scene loader registers these; the core calls
+ * func(userParams, obj, lod, asReduced) when a scenario needs a LoD that the
+ * object does not hold yet (objFunc and metaFunc are kept for the loader's
+ * own use). Passing func = NULL unregisters. */
+CORE_API Boolean CDECL mufflon_set_lod_loader(MufflonInstanceHdl instHdl, Boolean (*func)(void*, ObjectHdl, uint32_t, Boolean),
+                                              Boolean (*objFunc)(void*, uint32_t, uint16_t*, uint32_t*),
+                                              Boolean (*metaFunc)(void*, LodMetadata*, size_t*), void* userParams);
 
 /* ---- image readback: core_interface.h:359-360 ---- */
 CORE_API Boolean CDECL mufflon_get_target_image(MufflonInstanceHdl instHdl, const char* name, Boolean variance, const float** ptr);
@@ -169,12 +185,16 @@ CORE_API ObjectHdl CDECL world_create_object(MufflonInstanceHdl instHdl, const c
 CORE_API ObjectHdl CDECL world_get_object(MufflonInstanceHdl instHdl, const char* name);
 CORE_API const char* CDECL world_get_object_name(ObjectHdl obj);
 CORE_API Boolean CDECL object_has_lod(ConstObjectHdl obj, LodLevel level);
+CORE_API Boolean CDECL object_allocate_lod_slots(ObjectHdl obj, LodLevel slots);
 CORE_API LodHdl CDECL object_add_lod(ObjectHdl obj, LodLevel level, Boolean asReduced);
+CORE_API Boolean CDECL object_get_id(ObjectHdl obj, uint32_t* id);
 CORE_API void CDECL world_reserve_objects_instances(MufflonInstanceHdl instHdl, const uint32_t objects, const uint32_t instances);
 CORE_API InstanceHdl CDECL world_create_instance(MufflonInstanceHdl instHdl, ObjectHdl obj, const uint32_t animationFrame);
 CORE_API uint32_t CDECL world_get_instance_count(MufflonInstanceHdl instHdl, const uint32_t frame);
 CORE_API Boolean CDECL instance_set_transformation_matrix(MufflonInstanceHdl instHdl, InstanceHdl inst, const Mat3x4* mat, const Boolean isWorldToInst);
 CORE_API Boolean CDECL instance_get_transformation_matrix(MufflonInstanceHdl instHdl, InstanceHdl inst, Mat3x4* mat);
+/* core_interface.h:450: the world holds one animation frame (frame 0), so this is 1 */
+CORE_API Boolean CDECL world_get_frame_count(MufflonInstanceHdl instHdl, uint32_t* frameCount);
 
 /* ---- materials and textures: core_interface.h:462-475 ---- */
 CORE_API MaterialHdl CDECL world_add_material(MufflonInstanceHdl instHdl, const char* name, const MaterialParams* mat);
@@ -190,8 +210,11 @@ CORE_API CameraHdl CDECL world_get_camera(MufflonInstanceHdl instHdl, const char
 CORE_API Boolean CDECL world_set_camera_position(CameraHdl cam, Vec3 pos, const uint32_t pathIndex);
 CORE_API Boolean CDECL world_set_camera_direction(CameraHdl cam, Vec3 dir, Vec3 up, const uint32_t pathIndex);
 CORE_API Boolean CDECL world_set_pinhole_camera_fov(CameraHdl cam, float vFov);
+CORE_API Boolean CDECL world_set_camera_near(CameraHdl cam, float near);
+CORE_API Boolean CDECL world_set_camera_far(CameraHdl cam, float far);
 
 /* ---- scenarios: core_interface.h:522-566 ---- */
+CORE_API void CDECL world_reserve_scenarios(MufflonInstanceHdl instHdl, const uint32_t scenarios);
 CORE_API ScenarioHdl CDECL world_create_scenario(MufflonInstanceHdl instHdl, const char* name);
 CORE_API ScenarioHdl CDECL world_find_scenario(MufflonInstanceHdl instHdl, const char* name);
 CORE_API ConstScenarioHdl CDECL world_get_current_scenario(MufflonInstanceHdl instHdl);
@@ -203,6 +226,19 @@ CORE_API Boolean CDECL scenario_set_resolution(ScenarioHdl scenario, uint32_t wi
 CORE_API CameraHdl CDECL scenario_get_camera(ScenarioHdl scenario);
 CORE_API Boolean CDECL scenario_set_camera(MufflonInstanceHdl instHdl, ScenarioHdl scenario, CameraHdl cam);
 CORE_API Boolean CDECL scenario_mask_instance(ScenarioHdl scenario, InstanceHdl inst);
+CORE_API Boolean CDECL scenario_mask_object(ScenarioHdl scenario, ObjectHdl obj);
+CORE_API Boolean CDECL scenario_is_object_masked(ScenarioHdl scenario, ObjectHdl obj);
+/* Level of detail of an instance: its own level if set, else its object's,
+ * else the scenario's global level, clamped to the object's LoD slots
+ * (scenario.cpp:131-154). */
+CORE_API LodLevel CDECL scenario_get_global_lod_level(ScenarioHdl scenario);
+CORE_API Boolean CDECL scenario_set_global_lod_level(ScenarioHdl scenario, LodLevel level);
+CORE_API LodLevel CDECL scenario_get_object_lod(ScenarioHdl scenario, ObjectHdl obj);
+CORE_API Boolean CDECL scenario_set_object_lod(ScenarioHdl scenario, ObjectHdl obj, LodLevel level);
+CORE_API Boolean CDECL scenario_set_instance_lod(ScenarioHdl scenario, InstanceHdl inst, LodLevel level);
+CORE_API void CDECL scenario_reserve_material_slots(ScenarioHdl scenario, size_t count);
+CORE_API void CDECL scenario_reserve_custom_object_properties(ScenarioHdl scenario, size_t objects);
+CORE_API void CDECL scenario_reserve_custom_instance_properties(ScenarioHdl scenario, size_t instances);
 CORE_API Boolean CDECL scenario_add_light(MufflonInstanceHdl instHdl, ScenarioHdl scenario, LightHdl hdl);
 CORE_API MatIdx CDECL scenario_declare_material_slot(ScenarioHdl scenario, const char* name, size_t nameLength);
 CORE_API MatIdx CDECL scenario_get_material_slot(ScenarioHdl scenario, const char* name, size_t nameLength);

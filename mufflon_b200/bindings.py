@@ -20,6 +20,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_LIB = os.path.join(_HERE, "lib", "libmufflon_core.so")
+LOADER_LIB_NAME = "libmufflon_loader.so"
 
 
 class ProcessTime(Structure):
@@ -70,6 +71,17 @@ class MaterialParamType(IntEnum):
     BLEND = 5
     FRESNEL = 6
     MICROFACET = 7
+
+
+class LoaderStatus(IntEnum):
+    SUCCESS = 0
+    ERROR = 1
+    ABORT = 2
+
+
+class LodMetadata(Structure):
+    _fields_ = [("vertices", c_uint32), ("triangles", c_uint32), ("quads", c_uint32), ("edges", c_uint32),
+                ("spheres", c_uint32)]
 
 
 class LightType(IntEnum):
@@ -205,12 +217,33 @@ def _ptr(a):
 class DllHolder:
     """Loads the library and declares the C signatures."""
 
-    def __init__(self, binary_path=None):
+    def __init__(self, binary_path=None, useLoader=False):
         path = binary_path or os.environ.get("MUFFLON_CORE_LIB", DEFAULT_LIB)
         if not os.path.exists(path):
             raise RuntimeError(f"libmufflon_core.so not built ({path}); run mufflon_b200.build.build()")
         self.path = path
-        self.core = ctypes.CDLL(path)
+        self.core = ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL)
+        self.mffLoader = None
+        if useLoader:
+            lpath = os.path.join(os.path.dirname(path), LOADER_LIB_NAME)
+            if not os.path.exists(lpath):
+                raise RuntimeError(f"{LOADER_LIB_NAME} not built ({lpath}); run mufflon_b200.build.build()")
+            self.mffLoader = ctypes.CDLL(lpath, mode=ctypes.RTLD_GLOBAL)
+            for name, (res, args) in {
+                "loader_get_dll_error": (c_char_p, []),
+                "loader_initialize": (c_void_p, [c_void_p]),
+                "loader_destroy": (None, [c_void_p]),
+                "loader_load_json": (c_int, [c_void_p, c_char_p]),
+                "loader_load_lod": (c_uint32, [c_void_p, c_void_p, c_uint32, c_uint32]),
+                "loader_load_object_material_indices": (c_uint32, [c_void_p, c_uint32, c_void_p, POINTER(c_uint32)]),
+                "loader_load_lod_metadatas": (c_uint32, [c_void_p, POINTER(LodMetadata), POINTER(c_size_t)]),
+                "loader_abort": (c_uint32, [c_void_p]),
+                "loader_get_loading_status": (c_char_p, [c_void_p]),
+                "loader_get_warnings": (c_char_p, [c_void_p]),
+            }.items():
+                f = getattr(self.mffLoader, name)
+                f.restype = res
+                f.argtypes = args
         c = self.core
         sig = {
             "core_get_dll_error": (c_char_p, []),
@@ -235,6 +268,18 @@ class DllHolder:
             "spheres_add_sphere_bulk": (c_int32, [c_void_p, c_size_t, POINTER(BulkLoader), c_void_p, POINTER(c_size_t)]),
             "spheres_set_material_idx_bulk": (c_size_t, [c_void_p, c_int32, c_size_t, POINTER(BulkLoader)]),
             "world_create_instance": (c_void_p, [c_void_p, c_void_p, c_uint32]),
+            "world_get_instance_count": (c_uint32, [c_void_p, c_uint32]),
+            "world_get_object": (c_void_p, [c_void_p, c_char_p]),
+            "object_has_lod": (c_uint32, [c_void_p, c_uint32]),
+            "object_get_id": (c_uint32, [c_void_p, POINTER(c_uint32)]),
+            "instance_get_transformation_matrix": (c_uint32, [c_void_p, c_void_p, POINTER(Mat3x4)]),
+            "scenario_get_global_lod_level": (c_uint32, [c_void_p]),
+            "scenario_set_global_lod_level": (c_uint32, [c_void_p, c_uint32]),
+            "scenario_set_object_lod": (c_uint32, [c_void_p, c_void_p, c_uint32]),
+            "scenario_set_instance_lod": (c_uint32, [c_void_p, c_void_p, c_uint32]),
+            "scenario_mask_object": (c_uint32, [c_void_p, c_void_p]),
+            "scenario_get_resolution": (c_uint32, [c_void_p, POINTER(c_uint32), POINTER(c_uint32)]),
+            "scenario_get_name": (c_char_p, [c_void_p]),
             "instance_set_transformation_matrix": (c_uint32, [c_void_p, c_void_p, POINTER(Mat3x4), c_uint32]),
             "world_add_material": (c_void_p, [c_void_p, c_char_p, POINTER(MaterialParams)]),
             "world_add_texture_value": (c_void_p, [c_void_p, POINTER(c_float), c_int, c_int]),
@@ -313,21 +358,64 @@ class DllInterface:
     """One method per C function (names as in Mufflon's bindings.py)."""
 
     def __init__(self, binary_path=None, useLoader=False):
-        self.dllHolder = DllHolder(binary_path)
+        self.dllHolder = DllHolder(binary_path, useLoader)
         self.core = self.dllHolder.core
+        self.loader = self.dllHolder.mffLoader
+        self.muffLoaderInst = None
         if not self.core.mufflon_is_cuda_available():
             raise MufflonError("no CUDA device available; the B200 core has no CPU fallback")
         self.muffInst = self.core.mufflon_initialize()
         if not self.muffInst:
             raise MufflonError("mufflon_initialize failed: " + self.core_get_dll_error())
+        if self.loader is not None:
+            self.muffLoaderInst = self.loader.loader_initialize(self.muffInst)
+            if not self.muffLoaderInst:
+                raise MufflonError("loader_initialize failed: " + self.loader_get_dll_error())
 
     def __del__(self):
         try:
+            # the loader first: destroying it unregisters its LoD callback from the core instance
+            if getattr(self, "muffLoaderInst", None):
+                self.loader.loader_destroy(self.muffLoaderInst)
+                self.muffLoaderInst = None
             if getattr(self, "muffInst", None):
                 self.core.mufflon_destroy(self.muffInst)
                 self.muffInst = None
         except Exception:
             pass
+
+    # -- scene-file loader (libmufflon_loader.so, mff_interface.h)
+    def loader_get_dll_error(self):
+        e = self.loader.loader_get_dll_error()
+        return e.decode() if e else ""
+
+    def loader_load_json(self, sceneJson):
+        return LoaderStatus(self.loader.loader_load_json(self.muffLoaderInst, str(sceneJson).encode("utf-8")))
+
+    def loader_abort(self):
+        return self.loader.loader_abort(self.muffLoaderInst) != 0
+
+    def loader_get_loading_status(self):
+        s = self.loader.loader_get_loading_status(self.muffLoaderInst)
+        return s.decode() if s else ""
+
+    def loader_get_warnings(self):
+        s = self.loader.loader_get_warnings(self.muffLoaderInst)
+        return [w for w in (s.decode() if s else "").split("\n") if w]
+
+    def loader_load_lod_metadatas(self, count):
+        buf = (LodMetadata * max(count, 1))()
+        n = c_size_t(0)
+        if not self.loader.loader_load_lod_metadatas(self.muffLoaderInst, buf, byref(n)):
+            raise MufflonError("loader_load_lod_metadatas failed: " + self.loader_get_dll_error())
+        return [(m.vertices, m.triangles, m.quads, m.edges, m.spheres) for m in buf[:n.value]]
+
+    def loader_load_object_material_indices(self, objId, capacity=65536):
+        buf = (c_uint16 * capacity)()
+        n = c_uint32(0)
+        if not self.loader.loader_load_object_material_indices(self.muffLoaderInst, objId, buf, byref(n)):
+            raise MufflonError("loader_load_object_material_indices failed: " + self.loader_get_dll_error())
+        return list(buf[:n.value])
 
     def close(self):
         self.__del__()
@@ -440,8 +528,17 @@ class DllInterface:
         self.core.mufflon_get_target_image_num_channels(self.muffInst, byref(ch))
         if not p:
             return None
-        w, h = self.resolution
+        w, h = self.current_resolution()
         return np.ctypeslib.as_array(p, shape=(h * w * ch.value,)).reshape(h, w, ch.value).copy()
+
+    def current_resolution(self):
+        """(width, height) of the loaded scenario."""
+        sc = self.core.world_get_current_scenario(self.muffInst)
+        if not sc:
+            return self.resolution
+        w, h = c_uint32(0), c_uint32(0)
+        self._check(self.core.scenario_get_resolution(sc, byref(w), byref(h)), "scenario_get_resolution")
+        return w.value, h.value
 
     # -- extensions
     def render_stats(self):
@@ -669,13 +766,32 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
     return sc
 
 
+def load_scene_file(dll: DllInterface, path: str):
+    """Loads a JSON scene file (and its binary) through loader_load_json; raises on failure."""
+    if dll.loader is None:
+        raise MufflonError("the DllInterface was created without the loader (useLoader=False)")
+    status = dll.loader_load_json(path)
+    if status != LoaderStatus.SUCCESS:
+        raise MufflonError(f"Failed to load scene '{path}' ({status.name}): {dll.loader_get_dll_error()}")
+    sc = dll.core.world_get_current_scenario(dll.muffInst)
+    w, h = c_uint32(0), c_uint32(0)
+    dll.core.scenario_get_resolution(sc, byref(w), byref(h))
+    dll.resolution = (w.value, h.value)
+    return sc
+
+
 class RenderActions:
     """Convenience layer with the method names of Mufflon's RenderActions."""
 
-    def __init__(self, binary_path=None, useLoader=False):
-        self.dllInterface = DllInterface(binary_path)
+    def __init__(self, binary_path=None, useLoader=True):
+        self.dllInterface = DllInterface(binary_path, useLoader)
         self.activeRendererName = ""
         self.sceneName = ""
+
+    def load_json(self, sceneJson, defaultRenderTarget="Radiance"):
+        self.sceneName = os.path.splitext(os.path.basename(sceneJson))[0]
+        load_scene_file(self.dllInterface, sceneJson)
+        self.enable_render_target(defaultRenderTarget, False)
 
     def load_spec(self, spec, defaultRenderTarget="Radiance"):
         self.sceneName = spec.name

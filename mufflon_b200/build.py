@@ -20,6 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmufflon_core.so")
+LOADER_LIB = os.path.join(LIB_DIR, "libmufflon_loader.so")
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
@@ -27,6 +28,9 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/wide.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu"]
 CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
+# the scene-file loader: its own library on top of the core's C API
+LOADER_SOURCES = ["loader/json.cpp", "loader/mff_binary.cpp", "loader/scene_loader.cpp", "loader/interface.cpp"]
+LOADER_HEADERS = ["loader/json.hpp", "loader/mff_binary.hpp", "loader/scene_loader.hpp"]
 HEADERS = ["common/fmath.hpp", "trace/dmath.cuh", "trace/intersect.cuh", "trace/shading.cuh",
            "trace/scene_types.hpp", "trace/pt_api.hpp", "lbvh/lbvh.hpp", "lbvh/radix_sort.cuh",
            "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "trace/wide_traverse.cuh", "lbvh/wide.hpp", "core/world.hpp"]
@@ -48,13 +52,15 @@ def _newer(target, deps):
 def _compile(src, verbose):
     path = os.path.join(CSRC, src)
     obj = os.path.join(BUILD, src.replace("/", "_") + ".o")
-    deps = [path] + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "mufflon_core.h")]
+    deps = [path] + [os.path.join(CSRC, h) for h in HEADERS + LOADER_HEADERS] + \
+        [os.path.join(ROOT, "include", h) for h in ("mufflon_core.h", "mff_interface.h")]
     if not _newer(obj, deps):
         return obj, ""
     if src.endswith(".cu"):
         cmd = [NVCC] + NVCC_FLAGS + ["-c", path, "-o", obj]
     else:
-        cmd = [CXX] + CXX_FLAGS + ["-c", path, "-o", obj]
+        hidden = ["-fvisibility=hidden"] if src.startswith("loader/") else []
+        cmd = [CXX] + CXX_FLAGS + hidden + ["-c", path, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
@@ -79,13 +85,22 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
+        lobjs = [o for o, _ in ex.map(lambda s: _compile(s, verbose), LOADER_SOURCES)]
+    if _newer(LOADER_LIB, lobjs + [LIB]):
+        cmd = [CXX, "-shared", "-o", LOADER_LIB] + lobjs + [f"-L{LIB_DIR}", "-lmufflon_core", "-lz",
+                                                           "-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     return LIB
 
 
 def clean():
     shutil.rmtree(BUILD, ignore_errors=True)
-    if os.path.exists(LIB):
-        os.remove(LIB)
+    for lib in (LIB, LOADER_LIB):
+        if os.path.exists(lib):
+            os.remove(lib)
 
 
 if __name__ == "__main__":

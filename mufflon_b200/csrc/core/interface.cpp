@@ -121,8 +121,29 @@ void ensure_wavefront_buffers(MufflonInstance& I) {
 	r.wfPixels = n;
 }
 
+// Brings in, through the registered LoD loader, every LoD the current
+// scenario shows but its object does not hold yet (world_container.cpp
+// load_scene: missing LoDs are requested from the loader).
+void load_missing_lods(MufflonInstance& I) {
+	HostScenario* sc = I.current;
+	if(!sc || !I.lodLoader.loadLod) return;
+	for(const auto& inst : I.instances) {
+		if(inst->frame != NO_FRAME && inst->frame != 0) continue;
+		HostObject* obj = inst->object;
+		if(!obj) continue;
+		if(std::find(sc->maskedInstances.begin(), sc->maskedInstances.end(), inst->index) != sc->maskedInstances.end()) continue;
+		if(std::find(sc->maskedObjects.begin(), sc->maskedObjects.end(), obj) != sc->maskedObjects.end()) continue;
+		const uint32_t lod = sc->effective_lod(*inst);
+		if(obj->lods.count(lod)) continue;
+		if(!I.lodLoader.loadLod(I.lodLoader.userParams, obj, lod, false))
+			throw ApiError("the LoD loader failed to load LoD " + std::to_string(lod) + " of object '" + obj->name + "'");
+		CHECK(obj->lods.count(lod), "the LoD loader did not add LoD " + std::to_string(lod) + " of object '" + obj->name + "'");
+	}
+}
+
 void load_scene_if_needed(MufflonInstance& I) {
 	if(!I.sceneDirty && I.scene.valid) return;
+	load_missing_lods(I);
 	std::string err;
 	if(!build_device_scene(I, err)) throw ApiError(err);
 	I.sceneDirty = false;
@@ -199,6 +220,20 @@ int32_t mufflon_get_cuda_device_index(void) {
 Boolean mufflon_is_cuda_available(void) {
 	int count = 0;
 	return cudaGetDeviceCount(&count) == cudaSuccess && count > 0;
+}
+
+Boolean mufflon_set_lod_loader(MufflonInstanceHdl h, Boolean (*func)(void*, ObjectHdl, uint32_t, Boolean),
+                               Boolean (*objFunc)(void*, uint32_t, uint16_t*, uint32_t*),
+                               Boolean (*metaFunc)(void*, LodMetadata*, size_t*), void* userParams) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	I.lodLoader.loadLod = func;
+	I.lodLoader.loadMatIndices = objFunc;
+	I.lodLoader.loadMetadata = metaFunc;
+	I.lodLoader.userParams = userParams;
+	return true;
+	CATCH_ALL(false)
 }
 
 // interface.cpp:241-262: a library-owned copy of the cumulative target
@@ -446,6 +481,7 @@ ObjectHdl world_create_object(MufflonInstanceHdl h, const char* name, ObjectFlag
 	auto o = std::make_unique<HostObject>();
 	o->name = name ? name : "";
 	o->flags = uint32_t(flags);
+	o->id = uint32_t(I.objects.size());
 	I.objects.push_back(std::move(o));
 	I.sceneDirty = true;
 	return I.objects.back().get();
@@ -461,9 +497,26 @@ const char* world_get_object_name(ObjectHdl o) { TRY CHECK(o, "invalid object");
 Boolean object_has_lod(ConstObjectHdl o, LodLevel level) {
 	TRY CHECK(o, "invalid object"); return static_cast<const HostObject*>(o)->lods.count(level) > 0; CATCH_ALL(false)
 }
+Boolean object_allocate_lod_slots(ObjectHdl o, LodLevel slots) {
+	TRY
+	CHECK(o, "invalid object");
+	CHECK(slots >= 1, "an object needs at least one LoD slot");
+	static_cast<HostObject*>(o)->lodSlots = slots;
+	return true;
+	CATCH_ALL(false)
+}
+Boolean object_get_id(ObjectHdl o, uint32_t* id) {
+	TRY
+	CHECK(o && id, "invalid object or id pointer");
+	*id = static_cast<HostObject*>(o)->id;
+	return true;
+	CATCH_ALL(false)
+}
 LodHdl object_add_lod(ObjectHdl o, LodLevel level, Boolean) {
 	TRY
 	CHECK(o, "invalid object");
+	CHECK(static_cast<HostObject*>(o)->lodSlots == 0 || level < static_cast<HostObject*>(o)->lodSlots,
+	      "LoD level beyond the object's LoD slots");
 	auto& slot = static_cast<HostObject*>(o)->lods[level];
 	if(!slot) slot = std::make_unique<HostLod>();
 	return slot.get();
@@ -472,54 +525,66 @@ LodHdl object_add_lod(ObjectHdl o, LodLevel level, Boolean) {
 void world_reserve_objects_instances(MufflonInstanceHdl h, const uint32_t o, const uint32_t i) {
 	TRY minst(h).objects.reserve(o); minst(h).instances.reserve(i); CATCH_ALL()
 }
-InstanceHdl world_create_instance(MufflonInstanceHdl h, ObjectHdl obj, const uint32_t) {
+InstanceHdl world_create_instance(MufflonInstanceHdl h, ObjectHdl obj, const uint32_t animationFrame) {
 	TRY
 	MufflonInstance& I = minst(h);
 	CHECK(obj, "invalid object");
 	auto inst = std::make_unique<HostInstance>();
 	inst->object = static_cast<HostObject*>(obj);
 	inst->index = uint32_t(I.instances.size());
+	inst->frame = animationFrame;
 	I.instances.push_back(std::move(inst));
 	I.sceneDirty = true;
 	return I.instances.back().get();
 	CATCH_ALL(nullptr)
 }
-uint32_t world_get_instance_count(MufflonInstanceHdl h, const uint32_t) { TRY return uint32_t(minst(h).instances.size()); CATCH_ALL(0) }
+uint32_t world_get_instance_count(MufflonInstanceHdl h, const uint32_t frame) {
+	TRY
+	uint32_t n = 0;
+	for(const auto& i : minst(h).instances) n += (i->frame == frame) ? 1u : 0u;
+	return n;
+	CATCH_ALL(0)
+}
+Boolean world_get_frame_count(MufflonInstanceHdl h, uint32_t* frameCount) {
+	TRY (void)minst(h); CHECK(frameCount, "frame count pointer is null"); *frameCount = 1u; return true; CATCH_ALL(false)
+}
+
+// Inverse of an affine 3x4 (row-major, translation in the last column), as
+// InstanceData::compute_instance_to_world_transformation computes it; the same
+// formula maps either direction.
+static void invert_affine(const float* r, float* o) {
+	const float m00 = r[5] * r[10] - r[9] * r[6], m01 = r[9] * r[2] - r[1] * r[10], m02 = r[1] * r[6] - r[5] * r[2];
+	const float m10 = r[8] * r[6] - r[4] * r[10], m11 = r[0] * r[10] - r[8] * r[2], m12 = r[4] * r[2] - r[0] * r[6];
+	const float m20 = r[4] * r[9] - r[8] * r[5], m21 = r[8] * r[1] - r[0] * r[9], m22 = r[0] * r[5] - r[4] * r[1];
+	const float det = r[0] * m00 + r[1] * m10 + r[2] * m20;
+	CHECK(det != 0.0f, "singular transformation");
+	const float id = 1.0f / det;
+	const float i[9] = { id * m00, id * m01, id * m02, id * m10, id * m11, id * m12, id * m20, id * m21, id * m22 };
+	for(int row = 0; row < 3; ++row) {
+		o[4 * row] = i[3 * row]; o[4 * row + 1] = i[3 * row + 1]; o[4 * row + 2] = i[3 * row + 2];
+		o[4 * row + 3] = -(i[3 * row] * r[3] + i[3 * row + 1] * r[7] + i[3 * row + 2] * r[11]);
+	}
+}
 
 // instance_set_transformation_matrix: the stored matrix is world-to-instance;
-// an instance-to-world input is inverted exactly like
-// InstanceData::compute_instance_to_world_transformation (the inverse of an
-// affine 3x4 is the same formula in both directions).
+// an instance-to-world input is inverted.
 Boolean instance_set_transformation_matrix(MufflonInstanceHdl h, InstanceHdl inst, const Mat3x4* mat, const Boolean isWorldToInst) {
 	TRY
 	MufflonInstance& I = minst(h);
 	CHECK(inst && mat, "invalid instance or matrix");
 	HostInstance& in = *static_cast<HostInstance*>(inst);
 	if(isWorldToInst) std::memcpy(in.worldToInstance, mat->v, sizeof(in.worldToInstance));
-	else {
-		const float* r = mat->v;
-		const float m00 = r[5] * r[10] - r[9] * r[6], m01 = r[9] * r[2] - r[1] * r[10], m02 = r[1] * r[6] - r[5] * r[2];
-		const float m10 = r[8] * r[6] - r[4] * r[10], m11 = r[0] * r[10] - r[8] * r[2], m12 = r[4] * r[2] - r[0] * r[6];
-		const float m20 = r[4] * r[9] - r[8] * r[5], m21 = r[8] * r[1] - r[0] * r[9], m22 = r[0] * r[5] - r[4] * r[1];
-		const float det = r[0] * m00 + r[1] * m10 + r[2] * m20;
-		CHECK(det != 0.0f, "singular transformation");
-		const float id = 1.0f / det;
-		float* o = in.worldToInstance;
-		const float i[9] = { id * m00, id * m01, id * m02, id * m10, id * m11, id * m12, id * m20, id * m21, id * m22 };
-		for(int row = 0; row < 3; ++row) {
-			o[4 * row] = i[3 * row]; o[4 * row + 1] = i[3 * row + 1]; o[4 * row + 2] = i[3 * row + 2];
-			o[4 * row + 3] = -(i[3 * row] * r[3] + i[3 * row + 1] * r[7] + i[3 * row + 2] * r[11]);
-		}
-	}
+	else invert_affine(mat->v, in.worldToInstance);
 	I.sceneDirty = true;
 	return true;
 	CATCH_ALL(false)
 }
+// interface.cpp:1017-1027: returns the instance-to-world transformation
 Boolean instance_get_transformation_matrix(MufflonInstanceHdl h, InstanceHdl inst, Mat3x4* mat) {
 	TRY
 	(void)minst(h);
 	CHECK(inst && mat, "invalid instance or matrix");
-	std::memcpy(mat->v, static_cast<HostInstance*>(inst)->worldToInstance, sizeof(mat->v));
+	invert_affine(static_cast<HostInstance*>(inst)->worldToInstance, mat->v);
 	return true;
 	CATCH_ALL(false)
 }
@@ -542,10 +607,14 @@ MaterialHdl world_add_material(MufflonInstanceHdl h, const char* name, const Mat
 			m->type = MAT_TORRANCE;
 			m->albedo = static_cast<HostTexture*>(p->inner.torrance.albedo);
 			m->roughness = static_cast<HostTexture*>(p->inner.torrance.roughness);
+			CHECK(!m->roughness || (m->roughness->width == 1 && m->roughness->height == 1),
+			      "the CUDA path tracer takes a constant roughness (a 1x1 value texture)");
 			break;
 		case MATERIAL_EMISSIVE:
 			m->type = MAT_EMISSIVE;
 			m->radiance = static_cast<HostTexture*>(p->inner.emissive.radiance);
+			CHECK(!m->radiance || (m->radiance->width == 1 && m->radiance->height == 1),
+			      "the CUDA path tracer takes a constant emitted radiance (a 1x1 value texture)");
 			m->scale[0] = p->inner.emissive.scale.x; m->scale[1] = p->inner.emissive.scale.y; m->scale[2] = p->inner.emissive.scale.z;
 			break;
 		default:
@@ -619,8 +688,17 @@ Boolean world_set_camera_direction(CameraHdl cam, Vec3 d, Vec3 u, const uint32_t
 Boolean world_set_pinhole_camera_fov(CameraHdl cam, float vFov) {
 	TRY CHECK(cam, "invalid camera"); static_cast<HostCamera*>(cam)->vFov = vFov; return true; CATCH_ALL(false)
 }
+Boolean world_set_camera_near(CameraHdl cam, float nearP) {
+	TRY CHECK(cam, "invalid camera"); CHECK(nearP > 0.0f, "near plane must be positive");
+	static_cast<HostCamera*>(cam)->nearPlane = nearP; return true; CATCH_ALL(false)
+}
+Boolean world_set_camera_far(CameraHdl cam, float farP) {
+	TRY CHECK(cam, "invalid camera"); CHECK(farP > 0.0f, "far plane must be positive");
+	static_cast<HostCamera*>(cam)->farPlane = farP; return true; CATCH_ALL(false)
+}
 
 // ---------------------------------------------------------------- scenarios
+void world_reserve_scenarios(MufflonInstanceHdl h, const uint32_t n) { TRY minst(h).scenarios.reserve(n); CATCH_ALL() }
 ScenarioHdl world_create_scenario(MufflonInstanceHdl h, const char* name) {
 	TRY
 	MufflonInstance& I = minst(h);
@@ -672,6 +750,46 @@ Boolean scenario_set_camera(MufflonInstanceHdl h, ScenarioHdl s, CameraHdl cam) 
 Boolean scenario_mask_instance(ScenarioHdl s, InstanceHdl inst) {
 	TRY CHECK(s && inst, "invalid scenario or instance");
 	static_cast<HostScenario*>(s)->maskedInstances.push_back(static_cast<HostInstance*>(inst)->index); return true; CATCH_ALL(false)
+}
+Boolean scenario_mask_object(ScenarioHdl s, ObjectHdl obj) {
+	TRY CHECK(s && obj, "invalid scenario or object");
+	auto& m = static_cast<HostScenario*>(s)->maskedObjects;
+	if(std::find(m.begin(), m.end(), static_cast<const HostObject*>(obj)) == m.end()) m.push_back(static_cast<const HostObject*>(obj));
+	return true;
+	CATCH_ALL(false)
+}
+Boolean scenario_is_object_masked(ScenarioHdl s, ObjectHdl obj) {
+	TRY CHECK(s && obj, "invalid scenario or object");
+	const auto& m = static_cast<HostScenario*>(s)->maskedObjects;
+	return std::find(m.begin(), m.end(), static_cast<const HostObject*>(obj)) != m.end();
+	CATCH_ALL(false)
+}
+LodLevel scenario_get_global_lod_level(ScenarioHdl s) { TRY CHECK(s, "invalid scenario"); return static_cast<HostScenario*>(s)->globalLod; CATCH_ALL(0u) }
+Boolean scenario_set_global_lod_level(ScenarioHdl s, LodLevel level) {
+	TRY CHECK(s, "invalid scenario"); static_cast<HostScenario*>(s)->globalLod = level; return true; CATCH_ALL(false)
+}
+LodLevel scenario_get_object_lod(ScenarioHdl s, ObjectHdl obj) {
+	TRY CHECK(s && obj, "invalid scenario or object");
+	const auto* sc = static_cast<HostScenario*>(s);
+	auto it = sc->objectLods.find(static_cast<const HostObject*>(obj));
+	return it == sc->objectLods.end() ? sc->globalLod : it->second;
+	CATCH_ALL(0u)
+}
+Boolean scenario_set_object_lod(ScenarioHdl s, ObjectHdl obj, LodLevel level) {
+	TRY CHECK(s && obj, "invalid scenario or object");
+	static_cast<HostScenario*>(s)->objectLods[static_cast<const HostObject*>(obj)] = level; return true; CATCH_ALL(false)
+}
+Boolean scenario_set_instance_lod(ScenarioHdl s, InstanceHdl inst, LodLevel level) {
+	TRY CHECK(s && inst, "invalid scenario or instance");
+	static_cast<HostScenario*>(s)->instanceLods[static_cast<HostInstance*>(inst)->index] = level; return true; CATCH_ALL(false)
+}
+void scenario_reserve_material_slots(ScenarioHdl s, size_t n) {
+	TRY CHECK(s, "invalid scenario"); auto* sc = static_cast<HostScenario*>(s);
+	sc->slotNames.reserve(n); sc->slotMaterials.reserve(n); CATCH_ALL()
+}
+void scenario_reserve_custom_object_properties(ScenarioHdl s, size_t) { TRY CHECK(s, "invalid scenario"); CATCH_ALL() }
+void scenario_reserve_custom_instance_properties(ScenarioHdl s, size_t n) {
+	TRY CHECK(s, "invalid scenario"); static_cast<HostScenario*>(s)->maskedInstances.reserve(n); CATCH_ALL()
 }
 Boolean scenario_add_light(MufflonInstanceHdl h, ScenarioHdl s, LightHdl hdl) {
 	TRY
@@ -730,13 +848,14 @@ Boolean scene_get_bounding_box(SceneHdl s, Vec3* mn, Vec3* mx) {
 }
 
 // ---------------------------------------------------------------- lights
-LightHdl world_add_light(MufflonInstanceHdl h, const char* name, LightType type, const uint32_t) {
+LightHdl world_add_light(MufflonInstanceHdl h, const char* name, LightType type, const uint32_t count) {
 	LightHdl bad; bad.type = 7; bad.index = 0x1FFFFFFF;
 	TRY
 	MufflonInstance& I = minst(h);
 	CHECK(type == LIGHT_POINT, "the CUDA path tracer implements point, area and environment lights");
 	HostPointLight l;
 	l.name = name ? name : "";
+	l.frames = std::max<uint32_t>(count, 1u);
 	I.pointLights.push_back(l);
 	LightHdl r; r.type = LIGHT_POINT; r.index = uint32_t(I.pointLights.size() - 1);
 	return r;
@@ -754,13 +873,19 @@ LightHdl world_add_background_light(MufflonInstanceHdl h, const char* name, Back
 	return r;
 	CATCH_ALL(bad)
 }
-Boolean world_set_point_light_position(MufflonInstanceHdl h, LightHdl l, Vec3 p, const uint32_t) {
+// Point lights keep the values of animation frame 0, the frame the world shows;
+// other frames (< the count given to world_add_light) are accepted and unused.
+Boolean world_set_point_light_position(MufflonInstanceHdl h, LightHdl l, Vec3 p, const uint32_t frame) {
 	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_POINT && l.index < I.pointLights.size(), "invalid point light");
-	auto& L = I.pointLights[l.index]; L.position[0] = p.x; L.position[1] = p.y; L.position[2] = p.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+	auto& L = I.pointLights[l.index]; CHECK(frame < L.frames, "animation frame out of range");
+	if(frame != 0) return true;
+	L.position[0] = p.x; L.position[1] = p.y; L.position[2] = p.z; I.sceneDirty = true; return true; CATCH_ALL(false)
 }
-Boolean world_set_point_light_intensity(MufflonInstanceHdl h, LightHdl l, Vec3 v, const uint32_t) {
+Boolean world_set_point_light_intensity(MufflonInstanceHdl h, LightHdl l, Vec3 v, const uint32_t frame) {
 	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_POINT && l.index < I.pointLights.size(), "invalid point light");
-	auto& L = I.pointLights[l.index]; L.intensity[0] = v.x; L.intensity[1] = v.y; L.intensity[2] = v.z; I.sceneDirty = true; return true; CATCH_ALL(false)
+	auto& L = I.pointLights[l.index]; CHECK(frame < L.frames, "animation frame out of range");
+	if(frame != 0) return true;
+	L.intensity[0] = v.x; L.intensity[1] = v.y; L.intensity[2] = v.z; I.sceneDirty = true; return true; CATCH_ALL(false)
 }
 Boolean world_set_env_light_color(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
 	TRY MufflonInstance& I = minst(h); CHECK(l.type == LIGHT_ENVMAP && l.index < I.backgrounds.size(), "invalid background light");

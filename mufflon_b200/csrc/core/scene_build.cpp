@@ -294,6 +294,19 @@ void DeviceScene::release() {
 	valid = false;
 }
 
+// scenario.cpp:131-154, with the level clamped to the object's LoD slots in every case
+uint32_t HostScenario::effective_lod(const HostInstance& inst) const {
+	uint32_t level = globalLod;
+	auto ii = instanceLods.find(inst.index);
+	if(ii != instanceLods.end()) level = ii->second;
+	else if(inst.object) {
+		auto oi = objectLods.find(inst.object);
+		if(oi != objectLods.end()) level = oi->second;
+	}
+	const uint32_t slots = inst.object ? inst.object->lod_slot_count() : 1u;
+	return std::min(level, slots - 1u);
+}
+
 bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	HostScenario* sc = inst.current;
 	if(!sc) { err = "no scenario loaded"; return false; }
@@ -345,13 +358,33 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	std::map<const HostLod*, uint32_t> lodIndex;
 	std::vector<uint8_t> masked(numInst, 0);
 	for(uint32_t m : sc->maskedInstances) if(m < numInst) masked[m] = 1;
+	const uint32_t numSlots = uint32_t(std::max<size_t>(sc->slotMaterials.size(), 1));
 	for(uint32_t i = 0; i < numInst; ++i) {
 		if(masked[i]) continue;
-		HostObject* obj = inst.instances[i]->object;
+		const HostInstance& hi = *inst.instances[i];
+		if(hi.frame != NO_FRAME && hi.frame != 0) continue;
+		HostObject* obj = hi.object;
 		if(!obj || obj->lods.empty()) continue;
-		const HostLod* lod = obj->lods.begin()->second.get();
+		if(std::find(sc->maskedObjects.begin(), sc->maskedObjects.end(), obj) != sc->maskedObjects.end()) continue;
+		const uint32_t level = sc->effective_lod(hi);
+		auto lit = obj->lods.find(level);
+		if(lit == obj->lods.end()) {
+			err = "object '" + obj->name + "' has no LoD " + std::to_string(level);
+			return false;
+		}
+		const HostLod* lod = lit->second.get();
 		auto it = lodIndex.find(lod);
 		if(it == lodIndex.end()) {
+			// every material index must name a slot of the scenario: the device reads materials[index]
+			uint32_t maxMat = 0;
+			for(uint16_t m : lod->triMat) maxMat = std::max<uint32_t>(maxMat, m);
+			for(uint16_t m : lod->quadMat) maxMat = std::max<uint32_t>(maxMat, m);
+			for(uint16_t m : lod->sphereMat) maxMat = std::max<uint32_t>(maxMat, m);
+			if(lod->num_prims() > 0 && maxMat >= numSlots) {
+				err = "object '" + obj->name + "' uses material index " + std::to_string(maxMat) + " but the scenario declares "
+				      + std::to_string(sc->slotMaterials.size()) + " material slots";
+				return false;
+			}
 			const uint32_t idx = uint32_t(D.lodSources.size());
 			lodIndex[lod] = idx;
 			D.lodSources.push_back(lod);

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../../include/mufflon_core.h"
 #include "../trace/scene_types.hpp"
 #include "../lbvh/lbvh.hpp"
 #include "../trace/wavefront.hpp"
@@ -57,12 +58,23 @@ struct HostLod {
 struct HostObject {
 	std::string name;
 	uint32_t flags = 0;
+	uint32_t id = 0;        // creation index (object_get_id)
+	uint32_t lodSlots = 0;  // object_allocate_lod_slots; 0: highest added level + 1
 	std::map<uint32_t, std::unique_ptr<HostLod>> lods;
+	uint32_t lod_slot_count() const {
+		if(lodSlots > 0) return lodSlots;
+		return lods.empty() ? 1u : lods.rbegin()->first + 1u;
+	}
 };
+
+// Instances of animation frame NO_FRAME exist in every frame; the world is
+// shown at frame 0, so a scene holds the NO_FRAME and frame-0 instances.
+constexpr uint32_t NO_FRAME = 0xFFFFFFFFu;
 
 struct HostInstance {
 	HostObject* object = nullptr;
 	uint32_t index = 0;
+	uint32_t frame = NO_FRAME;
 	float worldToInstance[12] = { 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0 };
 };
 
@@ -92,7 +104,7 @@ struct HostCamera {
 	float nearPlane = 1e-4f, farPlane = 1e10f;
 };
 
-struct HostPointLight { std::string name; float position[3] = { 0, 0, 0 }; float intensity[3] = { 1, 1, 1 }; };
+struct HostPointLight { std::string name; uint32_t frames = 1; float position[3] = { 0, 0, 0 }; float intensity[3] = { 1, 1, 1 }; };
 struct HostBackground { std::string name; int32_t type = 0; float color[3] = { 0, 0, 0 }; float scale[3] = { 1, 1, 1 }; };
 
 struct HostScenario {
@@ -104,6 +116,21 @@ struct HostScenario {
 	std::vector<std::string> slotNames;
 	std::vector<HostMaterial*> slotMaterials;
 	std::vector<uint32_t> maskedInstances;
+	// level of detail: per-instance over per-object over global (scenario.cpp:131-154)
+	uint32_t globalLod = 0;
+	std::map<const HostObject*, uint32_t> objectLods;
+	std::map<uint32_t, uint32_t> instanceLods;    // instance index -> level
+	std::vector<const HostObject*> maskedObjects;
+	uint32_t effective_lod(const HostInstance& inst) const;
+};
+
+// Callbacks through which a scene loader supplies object LoDs on demand
+// (mufflon_set_lod_loader, core_interface.h:355-357).
+struct LodLoader {
+	Boolean (*loadLod)(void*, ObjectHdl, uint32_t, Boolean) = nullptr;
+	Boolean (*loadMatIndices)(void*, uint32_t, uint16_t*, uint32_t*) = nullptr;
+	Boolean (*loadMetadata)(void*, LodMetadata*, size_t*) = nullptr;
+	void* userParams = nullptr;
 };
 
 // Device buffers of one LoD. Buffers only grow: a reload of the same scene
@@ -213,6 +240,7 @@ struct MufflonInstance {
 	std::vector<HostBackground> backgrounds;
 	std::vector<std::unique_ptr<HostScenario>> scenarios;
 	HostScenario* current = nullptr;
+	LodLoader lodLoader;
 	bool sceneDirty = true;
 	DeviceScene scene;
 	LbvhBuilder builder;

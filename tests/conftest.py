@@ -31,3 +31,15 @@ def dll(core_lib_path):
     d = bindings.DllInterface(core_lib_path)
     yield d
     d.close()
+
+
+def build_c_example(core_lib_path, out_dir):
+    """Compiles tests/cpp/load_and_render.c with gcc -std=c99 against include/
+    and the in-tree libraries; returns the executable's path."""
+    import subprocess
+    lib_dir = os.path.dirname(core_lib_path)
+    exe = os.path.join(out_dir, "load_and_render")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "load_and_render.c"), "-o", exe, "-L", lib_dir,
+                    "-lmufflon_loader", "-lmufflon_core", f"-Wl,-rpath,{lib_dir}"], check=True, capture_output=True)
+    return exe

@@ -9,11 +9,11 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
-    src = open(os.path.join(ROOT, "include", "mufflon_core.h")).read()
+def declared_functions(header="mufflon_core.h", macro="CORE_API"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = "\n".join(l for l in src.splitlines() if not l.lstrip().startswith("#"))
-    return sorted(set(re.findall(r"CORE_API\s+[^;]*?\b(\w+)\s*\(", src)))
+    return sorted(set(re.findall(macro + r"\s+[^;]*?\b(\w+)\s*\(", src)))
 
 
 def test_header_declares_core_interface():
@@ -59,3 +59,22 @@ def test_missing_library_raises(tmp_path):
     from mufflon_b200 import bindings
     with pytest.raises(RuntimeError):
         bindings.DllHolder(str(tmp_path / "nope.so"))
+
+
+def test_loader_library_exports_all_declared_symbols(core_lib_path):
+    names = declared_functions("mff_interface.h", "LOADER_API")
+    for required in ["loader_initialize", "loader_destroy", "loader_load_json", "loader_get_dll_error",
+                     "loader_load_lod", "loader_abort", "loader_get_loading_status"]:
+        assert required in names, required
+    ctypes.CDLL(core_lib_path, mode=ctypes.RTLD_GLOBAL)
+    lib = ctypes.CDLL(os.path.join(os.path.dirname(core_lib_path), "libmufflon_loader.so"))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_reference_header_names_compile_and_link(core_lib_path, tmp_path):
+    """A C99 program written against core_interface.h + mff_interface.h (the
+    flow of examples/example.c) compiles and links against both libraries."""
+    from tests.conftest import build_c_example
+    exe = build_c_example(core_lib_path, str(tmp_path))
+    assert os.path.exists(exe)
