@@ -51,8 +51,9 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint"],
-                   help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one")
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load"],
+                   help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one; "
+                        "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene")
     p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
@@ -568,6 +569,61 @@ def run_adjoint(args):
     d.close()
 
 
+def run_load(args):
+    """Scene-file import of the headline scene (the 1.3 M-triangle displaced
+    icosphere at 1080p) written as JSON + binary: loader_load_json wall time
+    (JSON parse, binary header, LoD read through the core's LoD callback,
+    geometry upload, LBVH + 8-wide build, lights and materials), for an
+    uncompressed file and a DEFLATE file with packed normals, the file in the
+    page cache. Each load is checked: one iteration's hit ids must equal the
+    same scene built through the world API."""
+    import tempfile
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import bindings, build, scenefile, scenes
+    build.build()
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        d = bindings.DllInterface(useLoader=True)
+        for name, kw in [("raw", dict()), ("deflate_packed_normals", dict(deflate=True, compressed_normals=True))]:
+            jp = os.path.join(tmp, f"{name}.json")
+            loaded = scenefile.write_scene(spec, jp, **kw)
+            binp = os.path.join(tmp, json.load(open(jp))["binary"])
+            times, stats = [], []
+            for i in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                bindings.load_scene_file(d, jp)
+                dt = (time.perf_counter() - t0) * 1e3
+                if i >= args.warmup:
+                    times.append(dt)
+                    stats.append(d.load_stats())
+            assert d.render_enable_renderer(0, 0)
+            d.render_enable_render_target("Hit ID", False)
+            d.render_reset()
+            d.render_iterate()
+            hid = d.get_target_image("Hit ID").copy()
+            ref = bindings.DllInterface()
+            bindings.load_scene_spec(ref, loaded)
+            assert ref.render_enable_renderer(0, 0)
+            ref.render_enable_render_target("Hit ID", False)
+            ref.render_iterate()
+            same = bool(np.array_equal(hid, ref.get_target_image("Hit ID")))
+            ref.close()
+            ms = float(np.median(times))
+            mb = os.path.getsize(binp) / 1e6
+            core = {k: round(float(np.median([st[k] for st in stats])), 3) for k in ("totalMs", "uploadMs", "bvhMs")}
+            out[name] = {"load_ms": round(ms, 2), "file_mb": round(mb, 1), "file_mb_per_s": round(mb / (ms / 1e3), 1),
+                         "core_load_ms": core, "hit_ids_equal_api_scene": same}
+        d.close()
+    line = {"metric": "scene-file load time (JSON + binary, 1.3 M triangles)", "value": out["raw"]["load_ms"],
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "scene_file_load_" + WORKLOAD, "triangles": int(spec.num_prims)},
+            "files": out}
+    print(json.dumps(line), flush=True)
+
+
 def dataclasses_replace_texture(spec, tex3):
     import dataclasses
     t = np.ones(tex3.shape[:2] + (4,), np.float32)
@@ -582,6 +638,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint(args)
+        return
+    if args.workload == "load":
+        run_load(args)
         return
     if args.impl == "reference":
         run_reference(args)
