@@ -51,9 +51,10 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights"],
                    help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one; "
-                        "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene")
+                        "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
+                        "lights: GPU light-tree build of 262 145 lights")
     p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
@@ -624,6 +625,47 @@ def run_load(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lights(args):
+    """Light list and light tree of 256 instances x 1024 emissive quads + 1
+    point light (262 145 leaves), built on the GPU at every scene load
+    (light_build.cu: quad corners, Hilbert keys, two stable radix sorts,
+    128-sample quad fluxes, the tree level by level, the sorted code map),
+    timed on the host around the lights stage of world_load_scenario, next to
+    the oracle's single-threaded CPU build of the same tree; the two trees
+    are compared byte for byte."""
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import bindings, build, scenes
+    build.build()
+    spec = scenes.emissive_panels(0, 256, 1024, 1, width=WIDTH, height=HEIGHT)
+    d = bindings.DllInterface()
+    sc = bindings.load_scene_spec(d, spec)
+    times = []
+    for i in range(args.warmup + args.steps):
+        assert d.world_load_scenario(sc)
+        if i >= args.warmup:
+            times.append(d.load_stats()["otherMs"])
+    gpu_tree = d.light_tree()
+    d.close()
+    ms = float(np.median(times))
+    n = len(gpu_tree[0])
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle
+        osc = pyoracle.OracleScene(spec)
+        ref = osc.light_tree()
+        same = all(np.array_equal(a, b) for a, b in zip(gpu_tree[:4], ref[:4])) and \
+            np.float32(gpu_tree[4]).view(np.uint32) == np.float32(ref[4]).view(np.uint32)
+        cpu = {"value": round(osc.light_build_ms(), 2), "unit": "ms", "cores": 1, "kind": "port",
+               "sample": "the same 262 145-light build (light_tree.cpp restated, one thread)", "tree_identical": bool(same)}
+    line = {"metric": "light-tree build time (262 145 lights)", "value": round(ms, 3), "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+            "dtype": "f32", "config": {"workload": "emissive_panels_256x1024_quads_1_point", "lights": n},
+            "note": "host wall time of the lights stage of world_load_scenario (light build + materials + textures, one sync)",
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def dataclasses_replace_texture(spec, tex3):
     import dataclasses
     t = np.ones(tex3.shape[:2] + (4,), np.float32)
@@ -641,6 +683,9 @@ def main():
         return
     if args.workload == "load":
         run_load(args)
+        return
+    if args.workload == "lights":
+        run_lights(args)
         return
     if args.impl == "reference":
         run_reference(args)

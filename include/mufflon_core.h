@@ -366,6 +366,15 @@ typedef struct {
 	uint64_t h2dBytes;
 } MufflonLoadStats;
 CORE_API Boolean CDECL mufflon_get_load_stats(MufflonInstanceHdl instHdl, MufflonLoadStats* stats);
+/* EXTENSION: the loaded scene's light list (108 bytes per light: u16 type,
+ * u16 material, position[3], intensity[3], quad vectors[4][3], uv vectors[4][2])
+ * and light tree (20 bytes per node: left/right flux, left/right index,
+ * left/right type), as built on the GPU, plus the sorted
+ * (instance << 32 | primitive) -> node-path code map of the area lights.
+ * Counts are always written; arrays may be NULL. */
+CORE_API Boolean CDECL mufflon_get_light_tree(MufflonInstanceHdl instHdl, uint32_t* numLights, uint32_t* numNodes,
+                                              uint32_t* numAreaLights, void* lights, void* nodes, uint64_t* primKeys,
+                                              uint32_t* primCodes, float* rootFlux);
 
 /* Closest hits of n rays (6 floats: origin, direction) against the loaded
  * scene, with the path tracer's epsilon offset along geoNormals (may be NULL). */

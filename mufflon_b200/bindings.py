@@ -329,6 +329,7 @@ class DllHolder:
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
             "mufflon_get_load_stats": (c_uint32, [c_void_p, POINTER(MufflonLoadStats)]),
+            "mufflon_get_light_tree": (c_uint32, [c_void_p] + [c_void_p] * 8),
             "mufflon_texture_update": (c_uint32, [c_void_p, c_void_p, c_void_p]),
             "mufflon_albedo_gradient": (c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_float)]),
             "mufflon_render_batch": (c_uint32, [POINTER(MufflonBatchJob), c_uint32, c_int32, c_void_p, c_void_p,
@@ -550,6 +551,22 @@ class DllInterface:
         s = MufflonStageStats()
         self._check(self.core.mufflon_get_stage_stats(self.muffInst, byref(s)), "mufflon_get_stage_stats")
         return {k: getattr(s, k) for k, _ in MufflonStageStats._fields_}
+
+    def light_tree(self):
+        """The GPU-built light list and tree: (lights (n, 108) uint8, nodes (m, 20) uint8,
+        area-light keys uint64, codes uint32, root flux); layout in include/mufflon_core.h."""
+        nl, nn, na = c_uint32(), c_uint32(), c_uint32()
+        rf = c_float()
+        self._check(self.core.mufflon_get_light_tree(self.muffInst, byref(nl), byref(nn), byref(na), None, None, None,
+                                                     None, byref(rf)), "mufflon_get_light_tree")
+        lights = np.zeros((nl.value, 108), np.uint8)
+        nodes = np.zeros((nn.value, 20), np.uint8)
+        keys = np.zeros(na.value, np.uint64)
+        codes = np.zeros(na.value, np.uint32)
+        self._check(self.core.mufflon_get_light_tree(self.muffInst, byref(nl), byref(nn), byref(na), _ptr(lights),
+                                                     _ptr(nodes), _ptr(keys), _ptr(codes), byref(rf)),
+                    "mufflon_get_light_tree")
+        return lights, nodes, keys, codes, rf.value
 
     def load_stats(self):
         s = MufflonLoadStats()

@@ -1507,6 +1507,27 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 	CATCH_ALL(false)
 }
 
+Boolean mufflon_get_light_tree(MufflonInstanceHdl h, uint32_t* numLights, uint32_t* numNodes, uint32_t* numAreaLights,
+                               void* lights, void* nodes, uint64_t* primKeys, uint32_t* primCodes, float* rootFlux) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	load_scene_if_needed(I);
+	const DeviceScene& D = I.scene;
+	const uint32_t nArea = D.desc.numLightPrims;
+	if(numLights) *numLights = D.numLights;
+	if(numNodes) *numNodes = D.numLightNodes;
+	if(numAreaLights) *numAreaLights = nArea;
+	if(rootFlux) *rootFlux = D.desc.rootFlux;
+	static_assert(sizeof(DLight) == 108 && sizeof(DLightNode) == 20, "light layouts");
+	if(lights && D.numLights) CHECK_CUDA(cudaMemcpy(lights, D.dLights, sizeof(DLight) * D.numLights, cudaMemcpyDeviceToHost));
+	if(nodes && D.numLightNodes) CHECK_CUDA(cudaMemcpy(nodes, D.dLightNodes, sizeof(DLightNode) * D.numLightNodes, cudaMemcpyDeviceToHost));
+	if(primKeys && nArea) CHECK_CUDA(cudaMemcpy(primKeys, D.dLightKeys, sizeof(uint64_t) * nArea, cudaMemcpyDeviceToHost));
+	if(primCodes && nArea) CHECK_CUDA(cudaMemcpy(primCodes, D.dLightCodes, sizeof(uint32_t) * nArea, cudaMemcpyDeviceToHost));
+	return true;
+	CATCH_ALL(false)
+}
+
 Boolean mufflon_get_load_stats(MufflonInstanceHdl h, MufflonLoadStats* s) {
 	TRY
 	MufflonInstance& I = minst(h);

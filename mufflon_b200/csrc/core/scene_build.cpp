@@ -13,6 +13,7 @@
 // It is compiled without FP contraction so that it rounds exactly like the
 // CPU oracle's copy of the same steps.
 #include "world.hpp"
+#include "light_build.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -88,141 +89,17 @@ Box xform_box(const Mat34& M, Box b) {
 
 constexpr float PI = 3.14159265358979f;
 
-inline uint64_t scramble_seed(uint32_t x) {
-	uint64_t z = uint64_t(x) + 0x9e3779b97f4a7c15ull;
-	z = (z ^ (z >> 30u)) * 0xbf58476d1ce4e5b9ull;
-	z = (z ^ (z >> 27u)) * 0x94d049bb133111ebull;
-	return z ^ (z >> 31u);
-}
-inline float sample_uniform(uint32_t u) { return float(u) / 4294967810.0f; }
-
-struct HostLight {
-	uint16_t type;
-	V3 position, intensity;
-	V3 posV[4];
-	float uvV[4][2];
-	uint16_t material;
-	int32_t primInst = -1, primId = -1;
-};
-
-inline V3 light_center(const HostLight& l) {
-	if(l.type == LT_QUAD) return (l.posV[0] + (l.posV[1] + l.posV[2]) * 0.5f) + l.posV[3] * 0.25f;
-	return l.position;
-}
-
-// lights.cpp:16-62 (the quad variant samples a low-discrepancy 2D sequence;
-// its seed is derived from the primitive instead of the light's address)
-float light_flux(const HostLight& l, const std::vector<DMaterial>& mats) {
-	if(l.type == LT_POINT) {
-		const V3 f = l.intensity * 4.0f * PI;
-		return (f.x + f.y) + f.z;
-	}
-	const DMaterial& m = mats[l.material];
-	const V3 rad = ld3(m.radiance);
-	uint64_t state = scramble_seed(uint32_t(l.primId) * 2654435761u + uint32_t(l.primInst));
-	V3 sum = { 0, 0, 0 };
-	for(int i = 0; i < 128; ++i) {
-		uint64_t s = state;
-		state += 11400714819323198485ull;
-		s = s ^ (s >> 1);
-		s = ((s >> 1) & 0x2222222222222222ull) | ((s << 1) & 0x4444444444444444ull) | (s & 0x9999999999999999ull);
-		s = ((s >> 2) & 0x0c0c0c0c0c0c0c0cull) | ((s << 2) & 0x3030303030303030ull) | (s & 0xc3c3c3c3c3c3c3c3ull);
-		s = ((s >> 4) & 0x00f000f000f000f0ull) | ((s << 4) & 0x0f000f000f000f00ull) | (s & 0xf00ff00ff00ff00full);
-		s = ((s >> 8) & 0x0000ff000000ff00ull) | ((s << 8) & 0x00ff000000ff0000ull) | (s & 0xff0000ffff0000ffull);
-		s = ((s >> 16) & 0x00000000ffff0000ull) | ((s << 16) & 0x0000ffff00000000ull) | (s & 0xffff00000000ffffull);
-		const float ux = sample_uniform(uint32_t(s & 0xffffffffull));
-		const float uy = sample_uniform(uint32_t(s >> 32ull));
-		const V3 tx = l.posV[1] + ux * l.posV[3];
-		const V3 ty = l.posV[2] + uy * l.posV[3];
-		const float area = len(cross(ty, tx));
-		sum = sum + area * rad;
-	}
-	sum = sum / 128.0f;
-	const V3 f = sum * 2.0f * PI;
-	return (f.x + f.y) + f.z;
-}
-
-struct LightTreeOut {
-	std::vector<DLightNode> nodes;
-	std::vector<std::pair<uint64_t, uint32_t>> codes;
-	float rootFlux = 0.0f;
-	uint16_t rootType = LT_INTERNAL;
-	int32_t rootIndex = 0;
-};
-
-// light_tree.cpp:120-259 (balanced tree with extra bottom nodes) and fill_map
-LightTreeOut build_pos_tree(const std::vector<HostLight>& lights, const std::vector<DMaterial>& mats) {
-	LightTreeOut T;
-	const size_t n = lights.size();
-	if(n == 0) return T;
-	std::vector<float> flux(n);
-	for(size_t i = 0; i < n; ++i) flux[i] = light_flux(lights[i], mats);
-	auto key = [&](const HostLight& l) { return (uint64_t(uint32_t(l.primInst)) << 32) | uint32_t(l.primId); };
-	if(n == 1) {
-		T.rootType = lights[0].type;
-		T.rootIndex = 0;
-		T.rootFlux = flux[0];
-		if(lights[0].primInst != -1) T.codes.push_back({ key(lights[0]), 0u });
-		return T;
-	}
-	size_t height = 0;
-	while((size_t(1) << (height + 1)) <= n) ++height;
-	const size_t extra = n - (size_t(1) << height);
-	const size_t internalCount = ((size_t(1) << height) - 1) + extra;
-	T.nodes.assign(internalCount, DLightNode{});
-	std::vector<V3> centers(internalCount, V3{ 0, 0, 0 });
-	struct Ref { float flux; int32_t index; uint16_t type; };
-	auto lightRef = [&](size_t i) { return Ref{ flux[i], int32_t(i), lights[i].type }; };
-	auto nodeRef = [&](size_t i) { return Ref{ T.nodes[i].leftFlux + T.nodes[i].rightFlux, int32_t(i), uint16_t(LT_INTERNAL) }; };
-	auto refCenter = [&](const Ref& r) { return r.type == LT_INTERNAL ? centers[r.index] : light_center(lights[r.index]); };
-	auto makeNode = [&](size_t at, Ref l, Ref r) {
-		DLightNode nd;
-		nd.leftFlux = l.flux; nd.leftIndex = l.index; nd.leftType = l.type;
-		nd.rightFlux = r.flux; nd.rightIndex = r.index; nd.rightType = r.type;
-		T.nodes[at] = nd;
-		centers[at] = (refCenter(l) + refCenter(r)) / 2.0f;
-	};
-	if(extra > 0) {
-		const size_t startNode = (size_t(1) << height) - 1;
-		const size_t startLight = n - 2 * extra;
-		for(size_t i = 0; i < extra; ++i) makeNode(startNode + i, lightRef(startLight + 2 * i), lightRef(startLight + 2 * i + 1));
-		const size_t startInner = (size_t(1) << (height - 1)) - 1;
-		for(size_t i = 0; i < extra / 2; ++i) makeNode(startInner + i, nodeRef(startNode + 2 * i), nodeRef(startNode + 2 * i + 1));
-		if(extra % 2 != 0) makeNode(startInner + extra / 2, nodeRef(startNode + extra - 1), lightRef(0));
-	}
-	const size_t startLight = (extra % 2 == 0) ? 0 : 1;
-	const size_t levelNodeCount = n - 2 * extra - startLight;
-	const size_t nodeCount = levelNodeCount / 2;
-	const size_t startNodeIndex = (size_t(1) << height) - nodeCount - 1;
-	for(size_t i = 0; i < nodeCount; ++i) makeNode(startNodeIndex + i, lightRef(startLight + 2 * i), lightRef(startLight + 2 * i + 1));
-	if(height > 1) {
-		for(size_t level = height - 1; level >= 1; --level) {
-			const size_t nodes = size_t(1) << level;
-			const size_t inner = nodes / 2 - 1;
-			for(size_t i = 0; i < nodes / 2; ++i) makeNode(inner + i, nodeRef(nodes - 1 + 2 * i), nodeRef(nodes - 1 + 2 * i + 1));
-		}
-	}
-	T.rootType = LT_INTERNAL;
-	T.rootIndex = 0;
-	T.rootFlux = T.nodes[0].leftFlux + T.nodes[0].rightFlux;
-	int h = int(height);
-	const uint32_t lowerLightCount = uint32_t(1u << h) - uint32_t(extra);
-	uint32_t i = 0;
-	if(extra > 0) {
-		for(; i < lowerLightCount; ++i) {
-			if(lights[i].primInst != -1) {
-				uint32_t code = ((1u << h) - 1) - (lowerLightCount - i - 1);
-				code <<= (32 - h);
-				T.codes.push_back({ key(lights[i]), code });
-			}
-		}
-		h += 1;
-	}
-	for(; i < n; ++i) {
-		if(lights[i].primInst != -1) T.codes.push_back({ key(lights[i]), (i - lowerLightCount) << (32 - h) });
-	}
-	std::sort(T.codes.begin(), T.codes.end());
-	return T;
+// Grows a device buffer to hold at least count elements (contents are not kept).
+template < class T >
+bool reserve_device(T*& p, size_t& cap, size_t count, std::string& err) {
+	if(count <= cap && p) return true;
+	if(p) cudaFree(p);
+	p = nullptr;
+	cap = 0;
+	const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * std::max<size_t>(count, 1));
+	if(e != cudaSuccess) { err = std::string("device allocation failed: ") + cudaGetErrorString(e); return false; }
+	cap = std::max<size_t>(count, 1);
+	return true;
 }
 
 // Copies count elements (in up to two parts) into a grow-only device buffer.
@@ -289,6 +166,13 @@ void DeviceScene::release() {
 	dLods = nullptr; dW2I = nullptr; dInstLod = nullptr; dInstBoxes = nullptr; dInstCentroids = nullptr;
 	dMaterials = nullptr; dTextures = nullptr; dLights = nullptr; dLightNodes = nullptr;
 	dLightKeys = nullptr; dLightCodes = nullptr;
+	cudaFree(dLightI2W); cudaFree(dLightMirror); cudaFree(dLightFirst); cudaFree(dLightLods);
+	cudaFree(dEmissiveQuads); cudaFree(dQuadMaterial); cudaFree(dPointLights);
+	dLightI2W = nullptr; dLightMirror = nullptr; dLightFirst = nullptr; dLightLods = nullptr;
+	dEmissiveQuads = nullptr; dQuadMaterial = nullptr; dPointLights = nullptr;
+	for(size_t& c : lightCap) c = 0;
+	lightScratch.release();
+	numLights = numLightNodes = 0;
 	for(size_t& c : cap) c = 0;
 	desc = DScene{};
 	valid = false;
@@ -472,98 +356,88 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	const float instMs = msSince(tInst);
 	const auto tLights = clk::now();
 
-	// --- lights (world_container.cpp:869-990)
-	std::vector<HostLight> lights;
+	// --- lights (world_container.cpp:869-990), list and tree built on the GPU (light_build.cu)
+	if(!upload(D.dMaterials, D.cap[9], mats.data(), mats.size(), s, err)) return false;
+	// world_container.cpp:929-988 also makes emissive triangles and spheres
+	// area lights; this path tracer samples quad area lights only, so a
+	// scenario with other emitters is refused rather than rendered without
+	// their next-event estimation. Emissive quads are listed once per LoD.
+	std::vector<uint32_t> lodQuadStart(D.lodSources.size(), 0), lodQuadCount(D.lodSources.size(), 0);
+	std::vector<uint32_t> emissiveQuads;
+	std::vector<uint16_t> quadMaterial;
+	for(size_t li = 0; li < D.lodSources.size(); ++li) {
+		const HostLod& h = *D.lodSources[li];
+		auto emissive = [&](uint16_t m) { return m < mats.size() && mats[m].type == MAT_EMISSIVE; };
+		for(uint16_t m : h.triMat)
+			if(emissive(m)) { err = "emissive triangles are not area lights in the CUDA path tracer; emitters must be quads"; return false; }
+		for(uint16_t m : h.sphereMat)
+			if(emissive(m)) { err = "emissive spheres are not area lights in the CUDA path tracer; emitters must be quads"; return false; }
+		lodQuadStart[li] = uint32_t(emissiveQuads.size());
+		for(uint32_t q = 0; q < h.num_quads(); ++q)
+			if(emissive(h.quadMat[q])) { emissiveQuads.push_back(q); quadMaterial.push_back(h.quadMat[q]); }
+		lodQuadCount[li] = uint32_t(emissiveQuads.size()) - lodQuadStart[li];
+	}
+	// per instance: instance-to-world, mirroring, first light index (area lights in instance order)
+	std::vector<float> lightI2W(size_t(std::max<uint32_t>(numInst, 1)) * 12, 0.0f);
+	std::vector<uint8_t> lightMirror(std::max<uint32_t>(numInst, 1), 0);
+	std::vector<uint32_t> firstLight(size_t(numInst) + 1, 0);
+	uint64_t numArea64 = 0;
 	for(uint32_t i = 0; i < numInst; ++i) {
-		if(instLod[i] == 0xFFFFFFFFu) continue;
-		const HostLod& h = *D.lodSources[instLod[i]];
+		firstLight[i] = uint32_t(numArea64);
+		if(instLod[i] == 0xFFFFFFFFu || lodQuadCount[instLod[i]] == 0) continue;
 		const Mat34 i2w = instance_to_world(inst.instances[i]->worldToInstance);
 		const float* m = i2w.m;
+		std::memcpy(&lightI2W[12 * size_t(i)], m, 12 * sizeof(float));
 		const float det3 = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[1] * (m[4] * m[10] - m[8] * m[6]) + m[2] * (m[4] * m[9] - m[8] * m[5]);
-		const bool mirroring = det3 < 0.0f;
-		const uint32_t nT = h.num_triangles();
-		for(uint32_t q = 0; q < h.num_quads(); ++q) {
-			const uint16_t slot = h.quadMat[q];
-			if(slot >= mats.size() || mats[slot].type != MAT_EMISSIVE) continue;
-			V3 pts[4]; float uv[4][2];
-			for(int k = 0; k < 4; ++k) {
-				const uint32_t vi = h.quadIdx[4 * q + k];
-				pts[k] = xform_point(i2w, ld3(&h.vertices[3 * vi]));
-				uv[k][0] = h.uvs.empty() ? 0.0f : h.uvs[2 * vi];
-				uv[k][1] = h.uvs.empty() ? 0.0f : h.uvs[2 * vi + 1];
-			}
-			if(mirroring) { std::swap(pts[1], pts[3]); std::swap(uv[1], uv[3]); }
-			HostLight L{};
-			L.type = LT_QUAD;
-			L.posV[0] = pts[0];
-			L.posV[1] = pts[3] - pts[0];
-			L.posV[2] = pts[1] - pts[0];
-			L.posV[3] = (pts[2] - pts[3]) - L.posV[2];
-			for(int c = 0; c < 2; ++c) {
-				L.uvV[0][c] = uv[0][c];
-				L.uvV[1][c] = uv[3][c] - uv[0][c];
-				L.uvV[2][c] = uv[1][c] - uv[0][c];
-				L.uvV[3][c] = (uv[2][c] - uv[3][c]) - L.uvV[2][c];
-			}
-			L.material = slot;
-			L.primInst = int32_t(i);
-			L.primId = int32_t(nT + q);
-			lights.push_back(L);
-		}
+		lightMirror[i] = det3 < 0.0f ? 1 : 0;
+		numArea64 += lodQuadCount[instLod[i]];
 	}
+	firstLight[numInst] = uint32_t(numArea64);
+	std::vector<float> pointData;
 	for(uint32_t li : sc->pointLights) {
 		if(li >= inst.pointLights.size()) continue;
-		HostLight L{};
-		L.type = LT_POINT;
-		L.position = ld3(inst.pointLights[li].position);
-		L.intensity = ld3(inst.pointLights[li].intensity);
-		lights.push_back(L);
+		const HostPointLight& P = inst.pointLights[li];
+		pointData.insert(pointData.end(), { P.position[0], P.position[1], P.position[2], P.intensity[0], P.intensity[1], P.intensity[2] });
 	}
-	if(lights.size() > 1) {
-		const V3 scale = sceneBox.mx - sceneBox.mn;
-		auto conv = [](float v) { return v <= 0.0f ? 0u : (v >= 4294967040.0f ? 0xFFFFFF00u : uint32_t(v)); };
-		auto p16 = [](uint32_t x) {
-			uint64_t r = x & 0xFFFF;
-			r = (r | (r << 16)) & 0x0000ff0000ffull;
-			r = (r | (r << 8)) & 0x00f00f00f00full;
-			r = (r | (r << 4)) & 0x0c30c30c30c3ull;
-			r = (r | (r << 2)) & 0x249249249249ull;
-			return r;
-		};
-		auto hilbert = [&](uint32_t a, uint32_t b, uint32_t c) {
-			uint64_t num = p16(a) | (p16(b) << 1u) | (p16(c) << 2u);
-			num = num ^ (num >> 32); num = num ^ (num >> 16); num = num ^ (num >> 8);
-			num = num ^ (num >> 4); num = num ^ (num >> 2); num = num ^ (num >> 1);
-			return num;
-		};
-		std::stable_sort(lights.begin(), lights.end(), [&](const HostLight& a, const HostLight& b) {
-			const V3 ca = light_center(a) * scale, cb = light_center(b) * scale;
-			const uint32_t ax = conv(ca.x), ay = conv(ca.y), az = conv(ca.z);
-			const uint32_t bx = conv(cb.x), by = conv(cb.y), bz = conv(cb.z);
-			uint64_t A = hilbert(ax >> 16, ay >> 16, az >> 16), B = hilbert(bx >> 16, by >> 16, bz >> 16);
-			if(A == B) { A = hilbert(ax & 0xffff, ay & 0xffff, az & 0xffff); B = hilbert(bx & 0xffff, by & 0xffff, bz & 0xffff); }
-			return A < B;
-		});
+	const uint64_t numLights64 = numArea64 + pointData.size() / 6;
+	if(numLights64 >= (uint64_t(1) << 30)) { err = "too many lights for the light tree"; return false; }
+	const uint32_t numArea = uint32_t(numArea64), numLights = uint32_t(numLights64);
+	std::vector<LightLodInfo> lodInfo(std::max<size_t>(D.lodSources.size(), 1));
+	for(size_t li = 0; li < D.lodSources.size(); ++li) {
+		const HostLod& h = *D.lodSources[li];
+		lodInfo[li] = LightLodInfo{ D.lods[li].vertices, h.uvs.empty() ? nullptr : D.lods[li].uvs, D.lods[li].indices,
+		                            h.num_triangles(), lodQuadStart[li] };
 	}
-	LightTreeOut T = build_pos_tree(lights, mats);
-	std::vector<DLight> dlights(std::max<size_t>(lights.size(), 1));
-	for(size_t i = 0; i < lights.size(); ++i) {
-		DLight& d = dlights[i];
-		d = DLight{};
-		d.type = lights[i].type;
-		d.material = lights[i].material;
-		st3(d.position, lights[i].position);
-		st3(d.intensity, lights[i].intensity);
-		for(int k = 0; k < 4; ++k) { st3(d.posV[k], lights[i].posV[k]); d.uvV[k][0] = lights[i].uvV[k][0]; d.uvV[k][1] = lights[i].uvV[k][1]; }
+	if(!upload(D.dLightI2W, D.lightCap[0], lightI2W.data(), numArea ? lightI2W.size() : 0, s, err)) return false;
+	if(!upload(D.dLightMirror, D.lightCap[1], lightMirror.data(), numArea ? lightMirror.size() : 0, s, err)) return false;
+	if(!upload(D.dLightFirst, D.lightCap[2], firstLight.data(), numArea ? firstLight.size() : 0, s, err)) return false;
+	if(!upload(D.dLightLods, D.lightCap[3], lodInfo.data(), numArea ? D.lodSources.size() : 0, s, err)) return false;
+	if(!upload(D.dEmissiveQuads, D.lightCap[4], emissiveQuads.data(), emissiveQuads.size(), s, err)) return false;
+	if(!upload(D.dQuadMaterial, D.lightCap[5], quadMaterial.data(), quadMaterial.size(), s, err)) return false;
+	if(!upload(D.dPointLights, D.lightCap[6], pointData.data(), pointData.size(), s, err)) return false;
+	if(!reserve_device(D.dLights, D.cap[5], numLights, err) || !reserve_device(D.dLightNodes, D.cap[6], numLights, err) ||
+	   !reserve_device(D.dLightKeys, D.cap[7], numLights, err) || !reserve_device(D.dLightCodes, D.cap[8], numLights, err))
+		return false;
+	LightBuildInput lin{};
+	lin.numInstances = numInst;
+	lin.instLod = D.dInstLod;
+	lin.instToWorld = D.dLightI2W;
+	lin.mirroring = D.dLightMirror;
+	lin.instFirstLight = D.dLightFirst;
+	lin.lods = D.dLightLods;
+	lin.emissiveQuads = D.dEmissiveQuads;
+	lin.quadMaterial = D.dQuadMaterial;
+	lin.numArea = numArea;
+	lin.pointLights = D.dPointLights;
+	lin.numPoint = numLights - numArea;
+	lin.materials = D.dMaterials;
+	st3(lin.sceneScale, sceneBox.mx - sceneBox.mn);
+	LightTreeInfo tree;
+	{
+		const cudaError_t e = build_lights_gpu(lin, D.lightScratch, inst.builder,
+		                                       LightBuildOutput{ D.dLights, D.dLightNodes, D.dLightKeys, D.dLightCodes }, tree, s);
+		if(e != cudaSuccess) { err = std::string("light tree build failed: ") + cudaGetErrorString(e); return false; }
 	}
-	std::vector<uint64_t> keys;
-	std::vector<uint32_t> codes;
-	for(auto& kc : T.codes) { keys.push_back(kc.first); codes.push_back(kc.second); }
-	if(!upload(D.dLights, D.cap[5], dlights.data(), lights.size(), s, err)) return false;
-	if(!upload(D.dLightNodes, D.cap[6], T.nodes.data(), T.nodes.size(), s, err)) return false;
-	if(!upload(D.dLightKeys, D.cap[7], keys.data(), keys.size(), s, err)) return false;
-	if(!upload(D.dLightCodes, D.cap[8], codes.data(), codes.size(), s, err)) return false;
-	if(!upload(D.dMaterials, D.cap[9], mats.data(), mats.size(), s, err)) return false;
 	// textures
 	std::vector<DTexture> dtex(std::max<size_t>(texList.size(), 1));
 	for(size_t t = 0; t < texList.size(); ++t) {
@@ -586,8 +460,9 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	S.tlasWide = D.tlas.wnodes; S.tlasWidePrims = D.tlas.wprims; S.tlasNumWide = D.tlas.numWide;
 	S.materials = D.dMaterials; S.textures = D.dTextures;
 	S.lights = D.dLights; S.lightNodes = D.dLightNodes; S.lightPrimKeys = D.dLightKeys; S.lightPrimCodes = D.dLightCodes;
-	S.numLightPrims = uint32_t(keys.size());
-	S.rootFlux = T.rootFlux; S.rootType = T.rootType; S.rootIndex = T.rootIndex;
+	S.numLightPrims = numArea;
+	S.rootFlux = tree.rootFlux; S.rootType = tree.rootType; S.rootIndex = tree.rootIndex;
+	D.numLights = numLights; D.numLightNodes = tree.numNodes;
 	S.dirFlux = 0.0f;
 	S.hasBackground = 0;
 	if(sc->background >= 0 && size_t(sc->background) < inst.backgrounds.size()) {

@@ -20,6 +20,7 @@
 #include "../trace/scene_types.hpp"
 #include "../lbvh/lbvh.hpp"
 #include "../trace/wavefront.hpp"
+#include "light_build.hpp"
 
 namespace mb {
 
@@ -167,6 +168,17 @@ struct DeviceScene {
 	DLightNode* dLightNodes = nullptr;
 	uint64_t* dLightKeys = nullptr;
 	uint32_t* dLightCodes = nullptr;
+	uint32_t numLights = 0, numLightNodes = 0;
+	// inputs and scratch of the GPU light-tree build
+	float* dLightI2W = nullptr;
+	uint8_t* dLightMirror = nullptr;
+	uint32_t* dLightFirst = nullptr;
+	LightLodInfo* dLightLods = nullptr;
+	uint32_t* dEmissiveQuads = nullptr;
+	uint16_t* dQuadMaterial = nullptr;
+	float* dPointLights = nullptr;
+	size_t lightCap[7] = {};
+	LightBuildScratch lightScratch;
 	DScene desc{};
 	float aabb[6] = { 0, 0, 0, 0, 0, 0 };
 	bool valid = false;

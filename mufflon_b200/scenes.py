@@ -413,3 +413,69 @@ def displaced_plane(seed: int = 0, n: int = 224, width: int = 512, height: int =
     return SceneSpec([lod], np.array([identity34()], np.float32), np.array([0], np.uint32), mats, lights,
                      ((0.2, 0.2, 0.25), (1.0, 1.0, 1.0)), (0.0, 4.0, 8.0), (0.0, -0.5, -1.0), (0.0, 1.0, 0.0),
                      math.radians(50.0), width, height, name="displaced_plane")
+
+
+def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: int = 16, num_point_lights: int = 1,
+                    width: int = 96, height: int = 64) -> SceneSpec:
+    """Many small emissive quads: a ground quad, and `num_instances` instances
+    (one of them mirrored) of a panel set holding a few non-emissive triangles,
+    `quads_per_instance` emissive quads of three radiances and some
+    non-emissive quads; plus point lights. The light tree then has
+    num_instances * quads_per_instance + num_point_lights leaves."""
+    rng = np.random.default_rng(seed)
+    mats = [MaterialSpec(MAT_LAMBERT, albedo=(0.6, 0.6, 0.55), name="ground"),
+            MaterialSpec(MAT_LAMBERT, albedo=(0.3, 0.5, 0.7), name="frame")]
+    for k in range(3):
+        mats.append(MaterialSpec(MAT_EMISSIVE, radiance=tuple(float(x) for x in rng.uniform(2.0, 12.0, 3)), name=f"emit{k}"))
+    gp, gn = _quad((-20, 0, -20), (-20, 0, 20), (20, 0, 20), (20, 0, -20))
+    ground = _lod(gp, gn, np.array([(0, 0), (1, 0), (1, 1), (0, 1)], np.float32),
+                  quads=np.arange(4, dtype=np.uint32).reshape(1, 4), mats=np.array([0], np.uint16), name="ground")
+    # the panel set: frame triangles first, then emissive and frame quads interleaved
+    verts, norms, uvs, tris, quads, qmats = [], [], [], [], [], []
+    for t in range(3):
+        c = rng.uniform(-1.5, 1.5, 3)
+        p = (c + rng.normal(scale=0.3, size=(3, 3))).astype(np.float32)
+        n = np.cross(p[1] - p[0], p[2] - p[0])
+        n /= np.linalg.norm(n)
+        base = len(verts)
+        verts += list(p)
+        norms += [n] * 3
+        uvs += [(0, 0), (1, 0), (0, 1)]
+        tris.append((base, base + 1, base + 2))
+    num_frame = max(1, quads_per_instance // 4)
+    kinds = [2 + int(rng.integers(0, 3)) for _ in range(quads_per_instance)] + [1] * num_frame
+    rng.shuffle(kinds)
+    for kind in kinds:
+        c = rng.uniform(-1.5, 1.5, 3) + np.array([0.0, 2.0, 0.0])
+        a, b = rng.normal(size=3), rng.normal(size=3)
+        a /= np.linalg.norm(a)
+        b = b - a * np.dot(a, b)
+        b /= np.linalg.norm(b)
+        s = rng.uniform(0.03, 0.12, 2)
+        p = np.array([c - s[0] * a - s[1] * b, c + s[0] * a - s[1] * b, c + s[0] * a + s[1] * b,
+                      c - s[0] * a + s[1] * b], np.float32)
+        n = np.cross(p[1] - p[0], p[3] - p[0])
+        n /= np.linalg.norm(n)
+        base = len(verts)
+        verts += list(p)
+        norms += [n] * 4
+        uvs += [(0, 0), (1, 0), (1, 1), (0, 1)]
+        quads.append((base, base + 1, base + 2, base + 3))
+        qmats.append(kind)
+    panel = _lod(np.array(verts, np.float32), np.array(norms, np.float32), np.array(uvs, np.float32),
+                 tris=np.array(tris, np.uint32), quads=np.array(quads, np.uint32),
+                 mats=np.array([1] * len(tris) + qmats, np.uint16), name="panels")
+    w2i, inst_lod = [identity34()], [0]
+    for i in range(num_instances):
+        rot = _random_rotation(rng)
+        if i == 0:
+            rot = rot @ np.diag([1.0, 1.0, -1.0])  # a mirroring instance
+        w2i.append(_w2i_from_rt(rot, rng.uniform(-8.0, 8.0, 3) * np.array([1.0, 0.0, 1.0]) + np.array([0.0, 0.5, 0.0]),
+                                float(rng.uniform(0.7, 1.5))))
+        inst_lod.append(1)
+    lights = np.array([np.concatenate([rng.uniform(-6, 6, 3) * np.array([1.0, 0.0, 1.0]) + np.array([0.0, 6.0, 0.0]),
+                                       rng.uniform(20.0, 60.0, 3)]) for _ in range(num_point_lights)],
+                      np.float32).reshape(-1, 6)
+    return SceneSpec([ground, panel], np.array(w2i, np.float32), np.array(inst_lod, np.uint32), mats, lights, None,
+                     (0.0, 6.0, 16.0), (0.0, -0.35, -1.0), (0.0, 1.0, 0.0), math.radians(50.0), width, height,
+                     name="emissive_panels")

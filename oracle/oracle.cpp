@@ -50,6 +50,7 @@
 #include "../mufflon_b200/csrc/common/fmath.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cfloat>
 #include <cmath>
@@ -338,6 +339,7 @@ struct Scene {
 	std::vector<Material> materials;
 	std::vector<Texture> textures;
 	LightTree lightTree;
+	double lightBuildMs = 0.0;   // host time of the light list and tree build
 	Camera cam;
 	Box aabb = empty_box();
 	u32 width = 0, height = 0;
@@ -1924,6 +1926,7 @@ Scene* create_scene(const OrSceneDesc* d) {
 		S->cam.resX = u16(d->width); S->cam.resY = u16(d->height);
 	}
 	// Lights (world_container.cpp:869-990, light_tree.cpp:340-447)
+	const auto tLights = std::chrono::steady_clock::now();
 	LightTree& T = S->lightTree;
 	for(u32 inst = 0; inst < d->numInstances; ++inst) {
 		if(S->instLod[inst] == 0xFFFFFFFFu) continue;
@@ -1989,6 +1992,7 @@ Scene* create_scene(const OrSceneDesc* d) {
 		});
 	}
 	build_pos_tree(*S, T);
+	S->lightBuildMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tLights).count();
 	T.hasBackground = d->hasBackground != 0;
 	if(T.hasBackground) {
 		T.bgColor = { d->backgroundColor[0], d->backgroundColor[1], d->backgroundColor[2] };
@@ -2043,6 +2047,48 @@ int oracle_scene_aabb(void* s, float* a) {
 	Scene* S = static_cast<Scene*>(s);
 	a[0] = S->aabb.mn.x; a[1] = S->aabb.mn.y; a[2] = S->aabb.mn.z;
 	a[3] = S->aabb.mx.x; a[4] = S->aabb.mx.y; a[5] = S->aabb.mx.z;
+	return 1;
+}
+
+// The light list and tree in the core's device layout (scene_types.hpp
+// DLight 108 bytes, DLightNode 20 bytes) so tests compare them byte for byte.
+double oracle_light_build_ms(void* s) { return static_cast<const Scene*>(s)->lightBuildMs; }
+
+int oracle_light_tree(void* s, uint32_t* numLights, uint32_t* numNodes, uint32_t* numCodes, void* lightsOut,
+                      void* nodesOut, uint64_t* keysOut, uint32_t* codesOut, float* rootFlux) {
+	const Scene* S = static_cast<const Scene*>(s);
+	const LightTree& T = S->lightTree;
+	if(numLights) *numLights = u32(T.lights.size());
+	if(numNodes) *numNodes = u32(T.nodes.size());
+	if(numCodes) *numCodes = u32(T.primToNodePath.size());
+	if(rootFlux) *rootFlux = T.rootFlux;
+	if(lightsOut) {
+		unsigned char* o = static_cast<unsigned char*>(lightsOut);
+		for(const PosLight& l : T.lights) {
+			float f[26] = { l.position.x, l.position.y, l.position.z, l.intensity.x, l.intensity.y, l.intensity.z };
+			for(int k = 0; k < 4; ++k) { f[6 + 3 * k] = l.posV[k].x; f[7 + 3 * k] = l.posV[k].y; f[8 + 3 * k] = l.posV[k].z; }
+			for(int k = 0; k < 4; ++k) { f[18 + 2 * k] = l.uvV[k].x; f[19 + 2 * k] = l.uvV[k].y; }
+			std::memcpy(o, &l.type, 2);
+			std::memcpy(o + 2, &l.material, 2);
+			std::memcpy(o + 4, f, sizeof(f));
+			o += 108;
+		}
+	}
+	if(nodesOut) {
+		unsigned char* o = static_cast<unsigned char*>(nodesOut);
+		for(const LightNode& n : T.nodes) {
+			std::memcpy(o, &n.left.flux, 4); std::memcpy(o + 4, &n.right.flux, 4);
+			std::memcpy(o + 8, &n.left.index, 4); std::memcpy(o + 12, &n.right.index, 4);
+			std::memcpy(o + 16, &n.left.type, 2); std::memcpy(o + 18, &n.right.type, 2);
+			o += 20;
+		}
+	}
+	size_t k = 0;
+	for(const auto& [prim, code] : T.primToNodePath) {
+		if(keysOut) keysOut[k] = (u64(u32(prim.first)) << 32) | u32(prim.second);
+		if(codesOut) codesOut[k] = code;
+		++k;
+	}
 	return 1;
 }
 

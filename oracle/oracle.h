@@ -101,6 +101,13 @@ int oracle_bvh_get(void* scene, int32_t which, uint64_t* mortonSorted, int32_t* 
                    float* nodes /* 8 words per node: min3 max3 index primCount (as int bits) */,
                    int32_t* primIds);
 int oracle_scene_aabb(void* scene, float* aabb6);
+/* Light list (108 bytes per light) and tree (20 bytes per node) in the core's
+ * device layout, and the sorted (instance << 32 | primitive) -> node-path code
+ * map of the area lights. Arrays may be NULL to query the counts. */
+/* Host time (ms, one thread) that building the scene's light list and tree took. */
+double oracle_light_build_ms(void* scene);
+int oracle_light_tree(void* scene, uint32_t* numLights, uint32_t* numNodes, uint32_t* numCodes, void* lights,
+                      void* nodes, uint64_t* keys, uint32_t* codes, float* rootFlux);
 
 /* Ray queries. rays: 6 floats per ray (origin, direction). */
 int oracle_trace_first(void* scene, const float* rays, const float* geoNormals, float tmax,

@@ -73,6 +73,9 @@ def lib():
         L.oracle_bvh_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.oracle_bvh_get.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_scene_aabb.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_light_tree.argtypes = [C.c_void_p] + [C.c_void_p] * 8
+        L.oracle_light_build_ms.restype = C.c_double
+        L.oracle_light_build_ms.argtypes = [C.c_void_p]
         L.oracle_trace_first.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_uint32,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_trace_any.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
@@ -191,6 +194,24 @@ class OracleScene:
         a = np.zeros(6, np.float32)
         lib().oracle_scene_aabb(self.handle, _ptr(a))
         return a
+
+    def light_build_ms(self):
+        """Host time of this scene's light list and tree build (one thread)."""
+        return lib().oracle_light_build_ms(self.handle)
+
+    def light_tree(self):
+        """(lights (n, 108) uint8, nodes (m, 20) uint8, keys uint64, codes uint32, root flux) in the
+        core's device layout."""
+        nl, nn, nc = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        rf = C.c_float()
+        lib().oracle_light_tree(self.handle, C.byref(nl), C.byref(nn), C.byref(nc), None, None, None, None, None)
+        lights = np.zeros((nl.value, 108), np.uint8)
+        nodes = np.zeros((nn.value, 20), np.uint8)
+        keys = np.zeros(nc.value, np.uint64)
+        codes = np.zeros(nc.value, np.uint32)
+        lib().oracle_light_tree(self.handle, C.byref(nl), C.byref(nn), C.byref(nc), _ptr(lights), _ptr(nodes),
+                                _ptr(keys), _ptr(codes), C.byref(rf))
+        return lights, nodes, keys, codes, rf.value
 
     def trace_first(self, rays: np.ndarray, tmax: float = 1048576.0, geo_normals=None):
         rays = np.ascontiguousarray(rays, np.float32)
