@@ -709,7 +709,7 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
             p.innerType = MaterialParamType.TORRANCE
             p.inner.torrance.albedo = textures[m.albedo_texture] if m.albedo_texture >= 0 else tex_value(m.albedo)
             p.inner.torrance.roughness = tex_value(m.roughness)
-            p.inner.torrance.shadowingModel = ShadowingModel.SMITH
+            p.inner.torrance.shadowingModel = ShadowingModel.SMITH if m.shadowing == 1 else ShadowingModel.VCAVITY
             p.inner.torrance.ndf = NormalDistFunction.GGX
         else:
             p.innerType = MaterialParamType.EMISSIVE

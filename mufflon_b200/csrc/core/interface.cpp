@@ -602,9 +602,11 @@ MaterialHdl world_add_material(MufflonInstanceHdl h, const char* name, const Mat
 			m->albedo = static_cast<HostTexture*>(p->inner.lambert.albedo);
 			break;
 		case MATERIAL_TORRANCE:
-			CHECK(p->inner.torrance.ndf == NDF_GGX && p->inner.torrance.shadowingModel == SHADOWING_SMITH,
-			      "the CUDA path tracer implements Torrance with GGX and Smith shadowing");
+			CHECK(p->inner.torrance.ndf == NDF_GGX, "the CUDA path tracer implements Torrance with the GGX distribution");
+			CHECK(p->inner.torrance.shadowingModel == SHADOWING_SMITH || p->inner.torrance.shadowingModel == SHADOWING_VCAVITY,
+			      "unknown shadowing model");
 			m->type = MAT_TORRANCE;
+			m->shadowing = p->inner.torrance.shadowingModel == SHADOWING_SMITH ? SHADOW_SMITH : SHADOW_VCAVITY;
 			m->albedo = static_cast<HostTexture*>(p->inner.torrance.albedo);
 			m->roughness = static_cast<HostTexture*>(p->inner.torrance.roughness);
 			CHECK(!m->roughness || (m->roughness->width == 1 && m->roughness->height == 1),

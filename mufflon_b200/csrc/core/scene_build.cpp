@@ -220,6 +220,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		d.albedoTex = -1;
 		if(!m) { d.type = MAT_LAMBERT; continue; }
 		d.type = m->type;
+		d.shadowing = m->shadowing;
 		const V3 alb = tex_value(m->albedo, V3{ 0.5f, 0.5f, 0.5f });
 		st3(d.albedo, alb);
 		if(m->albedo && (m->albedo->width > 1 || m->albedo->height > 1)) {

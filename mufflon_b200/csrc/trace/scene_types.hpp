@@ -15,6 +15,8 @@ namespace mb {
 struct WideNode; // lbvh/wide.hpp
 
 enum : int32_t { MAT_LAMBERT = 0, MAT_TORRANCE = 1, MAT_EMISSIVE = 2 };
+// Torrance shadowing models, numbered as core_interface.h ShadowingModel
+enum : int32_t { SHADOW_VCAVITY = 0, SHADOW_SMITH = 1 };
 enum : uint16_t { LT_POINT = 0, LT_QUAD = 3, LT_INTERNAL = 0xFFFF };
 
 // Reference binary node (src/core/scene/accel_structs/lbvh.hpp:14-18):
@@ -55,6 +57,7 @@ struct DMaterial {
 	float roughness[2];
 	float radiance[3];            // emission * scale
 	int32_t albedoTex;            // -1: constant albedo
+	int32_t shadowing;            // Torrance: SHADOW_VCAVITY or SHADOW_SMITH
 };
 
 struct DTexture {

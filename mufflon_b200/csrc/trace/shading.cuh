@@ -12,7 +12,7 @@
 
 namespace mb {
 
-struct Params { int type; f3 albedo; f2 roughness; f3 radiance; };
+struct Params { int type; f3 albedo; f2 roughness; f3 radiance; int shadowing; };
 
 MBD f3 sample_texture(const DTexture& t, f2 uv) {
 	const float fx = uv.x - floorf(uv.x), fy = uv.y - floorf(uv.y);
@@ -30,6 +30,7 @@ MBD Params fetch_material(const DScene& S, uint16_t idx, f2 uv) {
 	p.albedo = (m.albedoTex >= 0) ? sample_texture(S.textures[m.albedoTex], uv) : load3(m.albedo);
 	p.roughness = make2(m.roughness[0], m.roughness[1]);
 	p.radiance = load3(m.radiance);
+	p.shadowing = m.shadowing;
 	return p;
 }
 
@@ -120,6 +121,50 @@ MBD f3 sample_visible_normal_smith(f3 inc, f2 r, float u0, float u1, u64& rnd2) 
 	sl.y *= r.y;
 	return normalize(make3(-sl.x, -sl.y, 1.0f));
 }
+// microfacet_base.hpp:73-81: V-cavity shadowing of one direction
+MBD float geo_vcavity(float wDotH, float wDotN, float hDotN) {
+	if(wDotH * wDotN <= 0.0f) return 0.0f;
+	return fmin_(1.0f, 2.0f * fabsf(sdiv(hDotN * wDotN, wDotH)));
+}
+// microfacet_base.hpp:116-142: the multi-bounce compensation applied to
+// min(Gi, Ge) for reflection. The eighth power is three squarings.
+MBD float vcavity_reflection(float gi, float ge) {
+	const float g = fmin_(gi, ge);
+	if(g < 0.11f) {
+		const float x = g + 0.74299714456847f;
+		const float x2 = x * x, x4 = x2 * x2;
+		return x4 * x4 - 0.092874643071059f;
+	}
+	return ((1.139400367544197f * g - 3.317658394008854f) * g + 3.317115685385115f) * g - 0.13885765892046f;
+}
+// microfacet_base.hpp:323-343: a microfacet normal drawn from the GGX
+// distribution itself (slope space), with its pdf
+MBD f3 sample_ndf_ggx(f2 r, float u0, float u1, float& pdf) {
+	const float phi = 2.0f * PI * u0;
+	const float e = sqrt_(__fdiv_rn(u1, 1.0f - u1));
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	float slopeX = e * c, slopeY = e * s;
+	const float norm = PI * r.x * r.y;
+	const float tmp = 1.0f + slopeX * slopeX + slopeY * slopeY;
+	slopeX *= r.x;
+	slopeY *= r.y;
+	const f3 dir = normalize(make3(-slopeX, -slopeY, 1.0f));
+	pdf = __fdiv_rn(1.0f, fmax_(norm * tmp * tmp * dir.z * dir.z * dir.z, 1e-20f));
+	return dir;
+}
+// microfacet_base.hpp:149-170: the cavity normal or its mirror image, chosen
+// in proportion to their visibility from the incident direction
+MBD f3 sample_visible_normal_vcavity(f3 inc, f3 cav, u64 rnd, float& iDotH) {
+	const f3 adj = make3(-cav.x, -cav.y, cav.z);
+	const float dOut = dot(inc, cav), dAdj = dot(inc, adj);
+	const float t = inc.z > 0.0f ? __fdiv_rn(fmax_(0.0f, dAdj), fmax_(0.0f, dOut) + fmax_(0.0f, dAdj))
+	                             : __fdiv_rn(fmax_(0.0f, -dAdj), fmax_(0.0f, -dOut) + fmax_(0.0f, -dAdj));
+	if(rnd < percentage_of(~0ull, t)) { iDotH = dAdj; return adj; }
+	iDotH = dOut;
+	return cav;
+}
+
 MBD f3 half_vector(f3 inTS, f3 exTS) {
 	const f3 h = 1.0f * inTS + 1.0f * exTS;
 	const float l = len(h) * sgn(h.z);
@@ -139,15 +184,30 @@ MBD PathSample material_sample(const TangentSpace& ts, const Params& p, f3 incid
 		res.pdfF = __fdiv_rn(e.z, PI);
 		res.pdfB = __fdiv_rn(fabsf(inTS.z), PI);
 	} else if(p.type == MAT_TORRANCE) {
+		// microfacet_specular.hpp:26-79
 		u64 rnd = i0;
-		const f3 h = sample_visible_normal_smith(inTS, p.roughness, u0, u1, rnd);
-		float cavityPdf = eval_ggx(p.roughness, h);
-		cavityPdf *= h.z;
-		const float iDotH = dot(inTS, h);
+		f3 h;
+		float cavityPdf, iDotH;
+		if(p.shadowing == SHADOW_SMITH) {
+			h = sample_visible_normal_smith(inTS, p.roughness, u0, u1, rnd);
+			cavityPdf = eval_ggx(p.roughness, h);
+			cavityPdf *= h.z;
+			iDotH = dot(inTS, h);
+		} else {
+			const f3 cav = sample_ndf_ggx(p.roughness, u0, u1, cavityPdf);
+			h = sample_visible_normal_vcavity(inTS, cav, rnd, iDotH);
+		}
 		const f3 exTS = (2.0f * iDotH) * h - inTS;
-		const float ge = geo_smith(iDotH, exTS, p.roughness);
-		const float gi = geo_smith(iDotH, inTS, p.roughness);
-		const float g = gi * ge;
+		float ge, gi, g;
+		if(p.shadowing == SHADOW_SMITH) {
+			ge = geo_smith(iDotH, exTS, p.roughness);
+			gi = geo_smith(iDotH, inTS, p.roughness);
+			g = gi * ge;
+		} else {
+			ge = geo_vcavity(iDotH, exTS.z, h.z);
+			gi = geo_vcavity(iDotH, inTS.z, h.z);
+			g = vcavity_reflection(gi, ge);
+		}
 		if(ge == 0.0f || gi == 0.0f) return none;
 		res.throughput = p.albedo * sdiv(g, gi); res.valid = true; res.excident = exTS;
 		res.pdfF = cavityPdf * sdiv(gi, fabsf(4.0f * inTS.z * h.z));
@@ -192,9 +252,16 @@ MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 inci
 		const f3 h = half_vector(inTS, exTS);
 		if(inTS.z * exTS.z < 0.0f) return none;
 		const float iDotH = dot(inTS, h);
-		const float ge = geo_smith(iDotH, exTS, p.roughness);
-		const float gi = geo_smith(iDotH, inTS, p.roughness);
-		const float g = gi * ge;
+		float ge, gi, g;
+		if(p.shadowing == SHADOW_SMITH) {
+			ge = geo_smith(iDotH, exTS, p.roughness);
+			gi = geo_smith(iDotH, inTS, p.roughness);
+			g = gi * ge;
+		} else {
+			ge = geo_vcavity(iDotH, exTS.z, h.z);
+			gi = geo_vcavity(iDotH, inTS.z, h.z);
+			g = vcavity_reflection(gi, ge);
+		}
 		if(ge == 0.0f || gi == 0.0f) return none;
 		const float dd = eval_ggx(p.roughness, h);
 		value = p.albedo * sdiv(g * dd, fabsf(4.0f * inTS.z * exTS.z));

@@ -221,7 +221,8 @@ def material_json(m, texture_file: Optional[str] = None) -> dict:
     if m.type == 0:
         return {"type": "lambert", "albedo": texture_file or _floats(m.albedo)}
     if m.type == 1:
-        return {"type": "torrance", "ndf": "GGX", "shadowingModel": "smith", "roughness": _floats(m.roughness),
+        return {"type": "torrance", "ndf": "GGX", "shadowingModel": "smith" if m.shadowing == 1 else "vcavity",
+                "roughness": _floats(m.roughness),
                 "albedo": texture_file or _floats(m.albedo)}
     return {"type": "emissive", "radiance": _floats(m.radiance), "scale": _floats(m.scale)}
 

@@ -61,6 +61,7 @@ class MaterialSpec:
     scale: tuple = (1.0, 1.0, 1.0)
     albedo_texture: int = -1
     name: str = "material"
+    shadowing: int = 1                  # Torrance: 1 Smith, 0 V-cavity (core_interface.h ShadowingModel)
 
 
 @dataclasses.dataclass

@@ -1112,7 +1112,7 @@ TangentSpace tangent_space(const Scene& S, const Intersection& h) {
 }
 
 // ---------------------------------------------------------------- materials
-struct Params { i32 type; V3 albedo; V2 roughness; V3 radiance; };
+struct Params { i32 type; V3 albedo; V2 roughness; V3 radiance; i32 shadowing; };
 
 inline V3 sample_texture(const Texture& t, V2 uv) {
 	// nearest sampling with wrap-around
@@ -1131,6 +1131,7 @@ inline Params fetch_material(const Scene& S, u16 matIdx, V2 uv) {
 	p.albedo = (m.albedoTex >= 0) ? sample_texture(S.textures[m.albedoTex], uv) : m.albedo;
 	p.roughness = m.roughness;
 	p.radiance = m.radiance * m.scale;
+	p.shadowing = m.shadowing;
 	return p;
 }
 
@@ -1228,6 +1229,50 @@ inline V3 sample_visible_normal_smith(V3 inc, V2 r, float u0, float u1, u64& rnd
 	return normalize(V3{ -sl.x, -sl.y, 1.0f });
 }
 
+// microfacet_base.hpp:73-81: V-cavity shadowing of one direction
+inline float geo_vcavity(float wDotH, float wDotN, float hDotN) {
+	if(wDotH * wDotN <= 0.0f) return 0.0f;
+	return fmin_(1.0f, 2.0f * std::fabs(sdiv(hDotN * wDotN, wDotH)));
+}
+// microfacet_base.hpp:116-142: the multi-bounce compensation applied to
+// min(Gi, Ge) for reflection. The eighth power is three squarings.
+inline float vcavity_reflection(float gi, float ge) {
+	const float g = fmin_(gi, ge);
+	if(g < 0.11f) {
+		const float x = g + 0.74299714456847f;
+		const float x2 = x * x, x4 = x2 * x2;
+		return x4 * x4 - 0.092874643071059f;
+	}
+	return ((1.139400367544197f * g - 3.317658394008854f) * g + 3.317115685385115f) * g - 0.13885765892046f;
+}
+// microfacet_base.hpp:323-343: a microfacet normal drawn from the GGX
+// distribution itself (slope space), with its pdf
+inline V3 sample_ndf_ggx(V2 r, float u0, float u1, float& pdf) {
+	const float phi = 2.0f * PI * u0;
+	const float e = mbmath::sqrt(u1 / (1.0f - u1));
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	float slopeX = e * c, slopeY = e * s;
+	const float norm = PI * r.x * r.y;
+	const float tmp = 1.0f + slopeX * slopeX + slopeY * slopeY;
+	slopeX *= r.x;
+	slopeY *= r.y;
+	const V3 dir = normalize(V3{ -slopeX, -slopeY, 1.0f });
+	pdf = 1.0f / fmax_(norm * tmp * tmp * dir.z * dir.z * dir.z, 1e-20f);
+	return dir;
+}
+// microfacet_base.hpp:149-170: the cavity normal or its mirror image, chosen
+// in proportion to their visibility from the incident direction
+inline V3 sample_visible_normal_vcavity(V3 inc, V3 cav, u64 rnd, float& iDotH) {
+	const V3 adj = { -cav.x, -cav.y, cav.z };
+	const float dOut = dot(inc, cav), dAdj = dot(inc, adj);
+	const float t = inc.z > 0.0f ? fmax_(0.0f, dAdj) / (fmax_(0.0f, dOut) + fmax_(0.0f, dAdj))
+	                             : fmax_(0.0f, -dAdj) / (fmax_(0.0f, -dOut) + fmax_(0.0f, -dAdj));
+	if(rnd < percentage_of(~0ull, t)) { iDotH = dAdj; return adj; }
+	iDotH = dOut;
+	return cav;
+}
+
 // half vector for vacuum on both sides (microfacet_base.hpp:15-27)
 inline V3 half_vector(V3 inTS, V3 exTS) {
 	const V3 h = 1.0f * inTS + 1.0f * exTS;
@@ -1248,15 +1293,30 @@ PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident,
 		const V3 e = sample_dir_cosine(u0, u1, cosT);
 		res = { p.albedo, true, e * sgn(inTS.z), e.z / PI, std::fabs(inTS.z) / PI };
 	} else if(p.type == OR_MAT_TORRANCE) {
+		// microfacet_specular.hpp:26-79
 		u64 rnd = i0;
-		const V3 h = sample_visible_normal_smith(inTS, p.roughness, u0, u1, rnd);
-		float cavityPdf = eval_ggx(p.roughness, h);
-		cavityPdf *= h.z;
-		const float iDotH = dot(inTS, h);
+		V3 h;
+		float cavityPdf, iDotH;
+		if(p.shadowing == 1) {
+			h = sample_visible_normal_smith(inTS, p.roughness, u0, u1, rnd);
+			cavityPdf = eval_ggx(p.roughness, h);
+			cavityPdf *= h.z;
+			iDotH = dot(inTS, h);
+		} else {
+			const V3 cav = sample_ndf_ggx(p.roughness, u0, u1, cavityPdf);
+			h = sample_visible_normal_vcavity(inTS, cav, rnd, iDotH);
+		}
 		const V3 exTS = (2.0f * iDotH) * h - inTS;
-		const float ge = geo_smith(iDotH, exTS, p.roughness);
-		const float gi = geo_smith(iDotH, inTS, p.roughness);
-		const float g = gi * ge;
+		float ge, gi, g;
+		if(p.shadowing == 1) {
+			ge = geo_smith(iDotH, exTS, p.roughness);
+			gi = geo_smith(iDotH, inTS, p.roughness);
+			g = gi * ge;
+		} else {
+			ge = geo_vcavity(iDotH, exTS.z, h.z);
+			gi = geo_vcavity(iDotH, inTS.z, h.z);
+			g = vcavity_reflection(gi, ge);
+		}
 		if(ge == 0.0f || gi == 0.0f) return none;
 		res = { p.albedo * sdiv(g, gi), true, exTS,
 		        cavityPdf * sdiv(gi, std::fabs(4.0f * inTS.z * h.z)),
@@ -1303,9 +1363,16 @@ EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident
 		const V3 h = half_vector(inTS, exTS);
 		if(inTS.z * exTS.z < 0.0f) return none;
 		const float iDotH = dot(inTS, h);
-		const float ge = geo_smith(iDotH, exTS, p.roughness);
-		const float gi = geo_smith(iDotH, inTS, p.roughness);
-		const float g = gi * ge;
+		float ge, gi, g;
+		if(p.shadowing == 1) {
+			ge = geo_smith(iDotH, exTS, p.roughness);
+			gi = geo_smith(iDotH, inTS, p.roughness);
+			g = gi * ge;
+		} else {
+			ge = geo_vcavity(iDotH, exTS.z, h.z);
+			gi = geo_vcavity(iDotH, inTS.z, h.z);
+			g = vcavity_reflection(gi, ge);
+		}
 		if(ge == 0.0f || gi == 0.0f) return none;
 		const float dd = eval_ggx(p.roughness, h);
 		value = p.albedo * sdiv(g * dd, std::fabs(4.0f * inTS.z * exTS.z));

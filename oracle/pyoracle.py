@@ -126,7 +126,8 @@ class OracleScene:
                             *[_ptr(a) for a in arrs])
         mats = (OrMaterial * max(1, len(spec.materials)))()
         for i, m in enumerate(spec.materials):
-            mats[i] = OrMaterial(m.type, (C.c_float * 3)(*m.albedo), (C.c_float * 2)(*m.roughness), 1, 0,
+            mats[i] = OrMaterial(m.type, (C.c_float * 3)(*m.albedo), (C.c_float * 2)(*m.roughness),
+                                 int(m.shadowing), 0,
                                  (C.c_float * 3)(*m.radiance), (C.c_float * 3)(*m.scale), m.albedo_texture)
         texs = (OrTexture * max(1, len(spec.textures)))()
         for i, t in enumerate(spec.textures):

@@ -64,10 +64,17 @@ def _specs():
         "inst": scenes.instanced_scene(3, num_meshes=3, num_instances=30, num_spheres=60, tri_range=(500, 2000),
                                        width=48, height=27),
         "tex": scenes.cornell_box_textured(2, 40, 40, texture=tex),
+        "vcavity": _vcavity(scenes.displaced_icosphere(4, subdiv=3, width=40, height=24)),
     }
 
 
-@pytest.mark.parametrize("name", ["cornell", "ico", "inst", "tex"])
+def _vcavity(spec):
+    """Torrance materials with the file format's default shadowing model (V-cavity)."""
+    return dataclasses.replace(spec, materials=[dataclasses.replace(m, shadowing=0) if m.type == scenes.MAT_TORRANCE
+                                                else m for m in spec.materials])
+
+
+@pytest.mark.parametrize("name", ["cornell", "ico", "inst", "tex", "vcavity"])
 @pytest.mark.parametrize("deflate,packed", [(False, False), (True, False), (True, True)])
 def test_loaded_file_equals_api_built_scene(tmp_path, loader_dll, name, deflate, packed):
     spec = _specs()[name]
