@@ -32,6 +32,8 @@ namespace {
 // counters: queue sizes, the shadow-slot count, the "paths handed to the tail"
 // flag, then one work counter per persistent launch
 enum { C_QUEUE0 = 0, C_QUEUE1 = 1, C_SHADOW0 = 2, C_SHADOW1 = 3, C_TAILED = 4, C_WORK = 5 };
+// Threads per block of the trace and tail kernels (their shared-memory stacks are sized for it).
+constexpr uint32_t WF_BLOCK = 128;
 // Shade of bounce b appends its next rays to queue (b + 1) & 1 and its shadow
 // rays to shadow counter C_SHADOW0 + (b & 1); the trace launch of bounce b
 // reads queue b & 1 and shadow counter C_SHADOW0 + ((b - 1) & 1) and resets
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 		W.counters[C_SHADOW0 + q] = 0u;
 		if(bounce < int(WF_BOUNCE_STATS)) W.counters[WF_COUNTERS - WF_BOUNCE_STATS + bounce] = W.counters[q];
 	}
-	uint2 stack[WIDE_STACK];
+	LocalStack stack;
 	LocalCounters cnt;
 	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW0 + (q ^ 1)) / unsigned(neeCount);
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	// takes over only the first bounce whose queue holds at most tailMax paths
 	if(*reinterpret_cast<volatile unsigned*>(W.counters + C_TAILED) || count > tailMax) return;
-	uint2 stack[WIDE_STACK];
+	LocalStack stack;
 	for(;;) {
 		const unsigned item = atomicAdd(W.counters + C_WORK + workIdx, 1u);
 		if(item >= count) break;
@@ -613,7 +615,7 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
                                                             uint32_t numPixels, uint32_t width, int texIndex,
                                                             const float* __restrict__ imageGrad, float scale,
                                                             float* texGrad) {
-	uint2 stack[WIDE_STACK];
+	LocalStack stack;
 	const DTexture tex = S.textures[texIndex];
 	for(uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < numPixels; p += gridDim.x * blockDim.x) {
 		u64 r = rng[p];
@@ -704,7 +706,7 @@ __global__ void k_finalize_batch(const DJob* jobs, WfState W, const uint16_t* pa
 // hierarchies (the parity and measurement entry points).
 __global__ void k_trace_rays_wide(const DScene S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
                                   float* tOut, int32_t* instOut, int32_t* primOut, float* spOut) {
-	uint2 stack[WIDE_STACK];
+	LocalStack stack;
 	LocalCounters cnt;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 		f3 o = make3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
@@ -719,7 +721,7 @@ __global__ void k_trace_rays_wide(const DScene S, const float* rays, const float
 }
 
 __global__ void k_occlusion_wide(const DScene S, const float* a, const float* b, uint32_t n, uint8_t* out) {
-	uint2 stack[WIDE_STACK];
+	LocalStack stack;
 	LocalCounters cnt;
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
 		const f3 pa = make3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
@@ -748,7 +750,7 @@ template < class SP > TraceKernel<SP> trace_kernel(int perSm) {
 	static const int occ[4] = { 4, 5, 6, 8 };
 	int idx = 2;
 	for(int i = 0; i < 4; ++i) if(occ[i] == perSm) idx = i;
-	if(!table[idx].fn) table[idx] = { fns[idx], persistent_blocks(reinterpret_cast<const void*>(fns[idx]), 128) };
+	if(!table[idx].fn) table[idx] = { fns[idx], persistent_blocks(reinterpret_cast<const void*>(fns[idx]), int(WF_BLOCK)) };
 	return table[idx];
 }
 
@@ -759,7 +761,7 @@ template < class SP > struct TailKernel {
 };
 template < class SP > TailKernel<SP> tail_kernel() {
 	static TailKernel<SP> k = {};
-	if(!k.fn) k = { k_tail<4, SP>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4, SP>), 128) };
+	if(!k.fn) k = { k_tail<4, SP>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4, SP>), int(WF_BLOCK)) };
 	return k;
 }
 
@@ -800,14 +802,14 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 			work = 0;
 		}
 		log.begin(WF_EXTEND);
-		tk.fn<<<tk.blocks, 128, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes, b);
+		tk.fn<<<tk.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes, b);
 		log.end();
 		if(tuning.tailBounce >= 0) {
 			// planned schedule: the tail takes over at tailBounce, nothing follows
 			if(b == tuning.tailBounce && b + 1 < maxBounces) {
 				const TailKernel<SP> tl = tail_kernel<SP>();
 				log.begin(WF_TAIL);
-				tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters, 0xFFFFFFFFu);
+				tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, 0xFFFFFFFFu);
 				log.end();
 				break;
 			}
@@ -823,7 +825,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 		if(tailAllowed) {
 			const TailKernel<SP> tl = tail_kernel<SP>();
 			log.begin(WF_TAIL);
-			tl.fn<<<tl.blocks, 128, 0, stream>>>(sp, W, q, b, int(work++), counters, tailMax);
+			tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, tailMax);
 			log.end();
 		}
 		// the shade of this bounce appends to the other queue and to the shadow

@@ -27,6 +27,17 @@
 namespace mb {
 
 constexpr int WIDE_STACK = 64;
+
+// The traversal stack of one ray. The node group being visited lives in
+// registers (WideTracer::ngBase/ngImask/ngHits, pgBase/pgHits); pushed groups
+// go to this per-thread array in local memory, which the L1 cache serves.
+// (Keeping the first 4, 8 or 16 entries in shared memory instead, thread-
+// interleaved, measured 5-7 % slower in the trace kernel on the B200.)
+struct LocalStack {
+	uint2 e[WIDE_STACK];
+	MBD void put(int i, uint2 v) { e[i] = v; }
+	MBD uint2 get(int i) const { return e[i]; }
+};
 constexpr uint32_t PRIM_GROUP = 0x80000000u;
 // Primitive masks use bits 0..8*leafMax-1; bit 31 tags primitive groups.
 static_assert(8 * WIDE_LEAF_MAX <= 31 && 8 * WIDE_TLAS_LEAF_MAX <= 31, "primitive mask width");
@@ -161,7 +172,8 @@ struct WideTracer {
 		instSp = sp;
 	}
 
-	MBD bool step(const DScene& S, LocalCounters& cnt, uint2* stack) {
+	template < class Stack >
+	MBD bool step(const DScene& S, LocalCounters& cnt, Stack& stack) {
 		if(done) return true;
 		if(++steps > MAX_TRAVERSAL_STEPS) { ++cnt.errors; done = true; return true; }
 		if(ngHits) {
@@ -171,7 +183,7 @@ struct WideTracer {
 			const uint32_t child = ngBase + uint32_t(__popc(ngImask & ((1u << s) - 1u)));
 			if(ngHits) {
 				if(sp >= WIDE_STACK) { ++cnt.errors; done = true; return true; }
-				stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
+				stack.put(sp++, make_uint2(ngBase, ngImask | (ngHits << 8)));
 			}
 			++cnt.nodes;
 			const float tmaxBox = (any ? tmaxW : best.t) * scale * BOX_SLACK;
@@ -213,8 +225,8 @@ struct WideTracer {
 				pgHits &= pgHits - 1u;
 				const uint32_t id = uint32_t(__ldg(S.tlasWidePrims + pgBase + j));
 				if(sp + 2 > WIDE_STACK) { ++cnt.errors; done = true; return true; }
-				if(ngHits) stack[sp++] = make_uint2(ngBase, ngImask | (ngHits << 8));
-				if(pgHits) stack[sp++] = make_uint2(pgBase, pgHits | PRIM_GROUP);
+				if(ngHits) stack.put(sp++, make_uint2(ngBase, ngImask | (ngHits << 8)));
+				if(pgHits) stack.put(sp++, make_uint2(pgBase, pgHits | PRIM_GROUP));
 				enter(S, id, cnt);
 				return false;
 			}
@@ -229,7 +241,7 @@ struct WideTracer {
 				instSp = -1;
 			}
 			if(sp == 0) { done = true; return true; }
-			const uint2 e = stack[--sp];
+			const uint2 e = stack.get(--sp);
 			if(e.y & PRIM_GROUP) { pgBase = e.x; pgHits = e.y & ~PRIM_GROUP; }
 			else { ngBase = e.x; ngImask = e.y & 0xFFu; ngHits = e.y >> 8; }
 		}
@@ -239,7 +251,8 @@ struct WideTracer {
 };
 
 // Closest hit of a world-space ray whose origin is already offset.
-MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
+template < class Stack >
+MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, Stack& stack) {
 	++cnt.rays;
 	WideTracer t;
 	t.init(S, o, dir, tmax, false, cnt);
@@ -248,7 +261,8 @@ MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCoun
 }
 
 // Occlusion of a prepared shadow ray (origin offset, unit direction, length tmax).
-MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, uint2* stack) {
+template < class Stack >
+MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, Stack& stack) {
 	++cnt.rays; ++cnt.shadow;
 	WideTracer t;
 	t.init(S, a, dir, tmax, true, cnt);
