@@ -14,6 +14,7 @@
 // CPU oracle's copy of the same steps.
 #include "world.hpp"
 #include "light_build.hpp"
+#include "instance_boxes.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -166,9 +167,9 @@ void DeviceScene::release() {
 	dLods = nullptr; dW2I = nullptr; dInstLod = nullptr; dInstBoxes = nullptr; dInstCentroids = nullptr;
 	dMaterials = nullptr; dTextures = nullptr; dLights = nullptr; dLightNodes = nullptr;
 	dLightKeys = nullptr; dLightCodes = nullptr;
-	cudaFree(dLightI2W); cudaFree(dLightMirror); cudaFree(dLightFirst); cudaFree(dLightLods);
+	cudaFree(dInstI2W); cudaFree(dWideInstBoxes); cudaFree(dLightMirror); cudaFree(dLightFirst); cudaFree(dLightLods);
 	cudaFree(dEmissiveQuads); cudaFree(dQuadMaterial); cudaFree(dPointLights);
-	dLightI2W = nullptr; dLightMirror = nullptr; dLightFirst = nullptr; dLightLods = nullptr;
+	dInstI2W = nullptr; dWideInstBoxes = nullptr; wideBoxCap = 0; dLightMirror = nullptr; dLightFirst = nullptr; dLightLods = nullptr;
 	dEmissiveQuads = nullptr; dQuadMaterial = nullptr; dPointLights = nullptr;
 	for(size_t& c : lightCap) c = 0;
 	lightScratch.release();
@@ -321,6 +322,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	// --- instance transforms, boxes, scene box (scene.cpp:203-303)
 	std::vector<float4> w2i(size_t(std::max<uint32_t>(numInst, 1)) * 3);
 	std::vector<float> boxes(size_t(std::max<uint32_t>(numInst, 1)) * 6, 0.0f), cents(size_t(std::max<uint32_t>(numInst, 1)) * 3, 0.0f);
+	std::vector<float> i2wAll(size_t(std::max<uint32_t>(numInst, 1)) * 12, 0.0f);
 	Box sceneBox = empty_box();
 	int32_t active = 0;
 	uint32_t valid = 0xFFFFFFFFu;
@@ -333,6 +335,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		++active;
 		if(valid == 0xFFFFFFFFu) valid = i;
 		const Mat34 i2w = instance_to_world(m);
+		std::memcpy(&i2wAll[12 * size_t(i)], i2w.m, sizeof(i2w.m));
 		const DLod& d = dl[instLod[i]];
 		const Box lb = { ld3(d.aabbMin), ld3(d.aabbMax) };
 		const Box ib = xform_box(i2w, lb);
@@ -345,12 +348,18 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	if(!upload(D.dInstLod, D.cap[2], instLod.data(), numInst, s, err)) return false;
 	if(!upload(D.dInstBoxes, D.cap[3], boxes.data(), size_t(numInst) * 6, s, err)) return false;
 	if(!upload(D.dInstCentroids, D.cap[4], cents.data(), size_t(numInst) * 3, s, err)) return false;
+	if(!upload(D.dInstI2W, D.lightCap[0], i2wAll.data(), size_t(numInst) * 12, s, err)) return false;
 	if(active > 1) {
 		SceneBuildInput sin{};
 		sin.numInstances = numInst; sin.activeInstances = uint32_t(active);
 		sin.instBoxes = D.dInstBoxes; sin.instCentroids = D.dInstCentroids; sin.instanceLod = D.dInstLod;
 		st3(sin.aabbMin, sceneBox.mn); st3(sin.aabbMax, sceneBox.mx);
-		cudaError_t e = inst.builder.build_scene(sin, D.tlas, s);
+		// the 8-wide instance level is refitted to tight boxes (instance_boxes.cu)
+		if(!reserve_device(D.dWideInstBoxes, D.wideBoxCap, size_t(numInst) * 6, err)) return false;
+		cudaError_t e = tight_instance_boxes(D.dLods, D.dInstLod, D.dInstI2W, numInst, D.dInstBoxes, D.dWideInstBoxes, s);
+		if(e != cudaSuccess) { err = std::string("instance boxes failed: ") + cudaGetErrorString(e); return false; }
+		sin.wideBoxes = D.dWideInstBoxes;
+		e = inst.builder.build_scene(sin, D.tlas, s);
 		if(e != cudaSuccess) { err = std::string("instance BVH build failed: ") + cudaGetErrorString(e); return false; }
 	}
 	st3(D.aabb, sceneBox.mn); st3(D.aabb + 3, sceneBox.mx);
@@ -379,16 +388,13 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		lodQuadCount[li] = uint32_t(emissiveQuads.size()) - lodQuadStart[li];
 	}
 	// per instance: instance-to-world, mirroring, first light index (area lights in instance order)
-	std::vector<float> lightI2W(size_t(std::max<uint32_t>(numInst, 1)) * 12, 0.0f);
 	std::vector<uint8_t> lightMirror(std::max<uint32_t>(numInst, 1), 0);
 	std::vector<uint32_t> firstLight(size_t(numInst) + 1, 0);
 	uint64_t numArea64 = 0;
 	for(uint32_t i = 0; i < numInst; ++i) {
 		firstLight[i] = uint32_t(numArea64);
 		if(instLod[i] == 0xFFFFFFFFu || lodQuadCount[instLod[i]] == 0) continue;
-		const Mat34 i2w = instance_to_world(inst.instances[i]->worldToInstance);
-		const float* m = i2w.m;
-		std::memcpy(&lightI2W[12 * size_t(i)], m, 12 * sizeof(float));
+		const float* m = &i2wAll[12 * size_t(i)];
 		const float det3 = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[1] * (m[4] * m[10] - m[8] * m[6]) + m[2] * (m[4] * m[9] - m[8] * m[5]);
 		lightMirror[i] = det3 < 0.0f ? 1 : 0;
 		numArea64 += lodQuadCount[instLod[i]];
@@ -409,7 +415,6 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 		lodInfo[li] = LightLodInfo{ D.lods[li].vertices, h.uvs.empty() ? nullptr : D.lods[li].uvs, D.lods[li].indices,
 		                            h.num_triangles(), lodQuadStart[li] };
 	}
-	if(!upload(D.dLightI2W, D.lightCap[0], lightI2W.data(), numArea ? lightI2W.size() : 0, s, err)) return false;
 	if(!upload(D.dLightMirror, D.lightCap[1], lightMirror.data(), numArea ? lightMirror.size() : 0, s, err)) return false;
 	if(!upload(D.dLightFirst, D.lightCap[2], firstLight.data(), numArea ? firstLight.size() : 0, s, err)) return false;
 	if(!upload(D.dLightLods, D.lightCap[3], lodInfo.data(), numArea ? D.lodSources.size() : 0, s, err)) return false;
@@ -422,7 +427,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	LightBuildInput lin{};
 	lin.numInstances = numInst;
 	lin.instLod = D.dInstLod;
-	lin.instToWorld = D.dLightI2W;
+	lin.instToWorld = D.dInstI2W;
 	lin.mirroring = D.dLightMirror;
 	lin.instFirstLight = D.dLightFirst;
 	lin.lods = D.dLightLods;

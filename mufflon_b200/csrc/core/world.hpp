@@ -169,8 +169,10 @@ struct DeviceScene {
 	uint64_t* dLightKeys = nullptr;
 	uint32_t* dLightCodes = nullptr;
 	uint32_t numLights = 0, numLightNodes = 0;
+	float* dInstI2W = nullptr;          // 12 per instance: instance-to-world
+	float* dWideInstBoxes = nullptr;    // 6 per instance: tight boxes of the 8-wide instance level
+	size_t wideBoxCap = 0;
 	// inputs and scratch of the GPU light-tree build
-	float* dLightI2W = nullptr;
 	uint8_t* dLightMirror = nullptr;
 	uint32_t* dLightFirst = nullptr;
 	LightLodInfo* dLightLods = nullptr;

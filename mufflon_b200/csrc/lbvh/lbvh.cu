@@ -236,6 +236,38 @@ __global__ void k_bbox(int mode, LodBuildInput lod, SceneBuildInput scene, int u
 	}
 }
 
+// Refits the binary hierarchy's node boxes (xyz only; counts and costs in .w
+// stay) to other leaf boxes, bottom-up as k_bbox: for the 8-wide conversion of
+// the instance level, after the reference-layout nodes have been emitted.
+__global__ void k_refit_boxes(int used, int numInternal, const int32_t* __restrict__ primIds,
+                              const int32_t* __restrict__ parents, const int32_t* __restrict__ children,
+                              const float* __restrict__ boxes, float4* nodeData, unsigned int* flags) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i >= used) return;
+	const float* b = boxes + 6 * size_t(primIds[i]);
+	const int leaf = numInternal + i;
+	nodeData[2 * leaf] = make_float4(b[0], b[1], b[2], nodeData[2 * leaf].w);
+	nodeData[2 * leaf + 1] = make_float4(b[3], b[4], b[5], nodeData[2 * leaf + 1].w);
+	int cur = parents[leaf];
+	if(cur < 0) cur = ~cur;
+	for(int depth = 0; depth < MAX_DEPTH; ++depth) {
+		__threadfence();
+		const unsigned prev = atomicAdd(&flags[cur], 1u);
+		if(prev == 0) return;
+		__threadfence();
+		const int L = children[2 * cur], R = children[2 * cur + 1];
+		const float4 l0 = __ldcg(&nodeData[2 * L]), l1 = __ldcg(&nodeData[2 * L + 1]);
+		const float4 r0 = __ldcg(&nodeData[2 * R]), r1 = __ldcg(&nodeData[2 * R + 1]);
+		const f3 nmn = vmin3(make3(r0.x, r0.y, r0.z), make3(l0.x, l0.y, l0.z));
+		const f3 nmx = vmax3(make3(r1.x, r1.y, r1.z), make3(l1.x, l1.y, l1.z));
+		nodeData[2 * cur] = make_float4(nmn.x, nmn.y, nmn.z, nodeData[2 * cur].w);
+		nodeData[2 * cur + 1] = make_float4(nmx.x, nmx.y, nmx.z, nodeData[2 * cur + 1].w);
+		if(cur == 0) return;
+		cur = parents[cur];
+		if(cur < 0) cur = ~cur;
+	}
+}
+
 // build_lbvh.cu:417-463
 __global__ void k_mark(int mode, int used, int numInternal, const int32_t* __restrict__ parents,
                        const float4* __restrict__ nodeData, int32_t* marks) {
@@ -588,6 +620,11 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	if(mode == MODE_LOD && withSoup)
 		k_soup<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*lod, int(numPrimitives), out.primIds, out.triSoup);
 	if(m_timing) cudaEventRecord(m_ev[8], stream);
+	if(wide && mode == MODE_SCENE && scene && scene->wideBoxes && used > 1) {
+		cudaMemsetAsync(m_flags, 0, sizeof(unsigned int) * numInternal, stream);
+		k_refit_boxes<<<blocks_for(used, 128), 128, 0, stream>>>(int(used), numInternal, m_valsA, m_parents, m_children,
+		                                                        scene->wideBoxes, m_nodeData, m_flags);
+	}
 	if(wide) {
 		WideBuildArgs wa{};
 		wa.n = n;

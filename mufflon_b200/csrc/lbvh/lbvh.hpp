@@ -39,6 +39,9 @@ struct SceneBuildInput {
 	const float* instCentroids; // device, 3 per instance
 	const uint32_t* instanceLod;// device, UINT32_MAX = masked
 	float aabbMin[3], aabbMax[3];
+	// device, 6 per instance, or nullptr: boxes the 8-wide hierarchy is refitted
+	// to (the binary hierarchy in the reference layout keeps instBoxes)
+	const float* wideBoxes;
 };
 
 struct BvhBuffers {
