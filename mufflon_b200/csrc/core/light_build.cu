@@ -36,6 +36,7 @@ __device__ __forceinline__ F3 xform_point(const float* m, F3 p) {
 
 __device__ __forceinline__ F3 light_center(const DLight& l) {
 	if(l.type == LT_QUAD) return (ld(l.posV[0]) + (ld(l.posV[1]) + ld(l.posV[2])) * 0.5f) + ld(l.posV[3]) * 0.25f;
+	if(l.type == LT_TRI) return ld(l.posV[0]) + (ld(l.posV[1]) + ld(l.posV[2])) / 3.0f;
 	return ld(l.position);
 }
 
@@ -66,7 +67,8 @@ __device__ __forceinline__ uint64_t scramble_seed(uint32_t x) {
 }
 __device__ __forceinline__ float sample_uniform(uint32_t u) { return __fdiv_rn(float(u), 4294967810.0f); }
 
-// lights.cpp:16-62: a point light's flux from its intensity; a quad's from 128
+// lights.cpp:16-62: a point light's flux from its intensity; a triangle's
+// from its area and the mean emitted radiance; a quad's from 128
 // low-discrepancy samples of its area times the emitted radiance.
 __device__ float light_flux(const DLight& l, int32_t primInst, int32_t primId, const DMaterial* mats) {
 	if(l.type == LT_POINT) {
@@ -74,6 +76,16 @@ __device__ float light_flux(const DLight& l, int32_t primInst, int32_t primId, c
 		return (f.x + f.y) + f.z;
 	}
 	const F3 rad = ld(mats[l.material].radiance);
+	if(l.type == LT_TRI) {
+		// lights.cpp:24-40: the mean of 128 samples of the (constant) radiance,
+		// times area times 2 pi
+		const float area = __fdiv_rn(len(cross(ld(l.posV[1]), ld(l.posV[2]))), 2.0f);
+		F3 sum = f3(0, 0, 0);
+		for(int i = 0; i < 128; ++i) sum = sum + rad;
+		sum = sum / 128.0f;
+		const F3 f = sum * area * 2.0f * LB_PI;
+		return (f.x + f.y) + f.z;
+	}
 	uint64_t state = scramble_seed(uint32_t(primId) * 2654435761u + uint32_t(primInst));
 	const F3 v1 = ld(l.posV[1]), v2 = ld(l.posV[2]), v3 = ld(l.posV[3]);
 	F3 sum = f3(0, 0, 0);
@@ -113,37 +125,56 @@ __global__ void k_make_lights(const LightBuildInput in, uint32_t n, DLight* ligh
 		}
 		const uint32_t i = lo;
 		const LightLodInfo lod = in.lods[in.instLod[i]];
-		const uint32_t entry = lod.quadListStart + (t - in.instFirstLight[i]);
-		const uint32_t q = in.emissiveQuads[entry];
+		const uint32_t entry = lod.faceListStart + (t - in.instFirstLight[i]);
+		const uint32_t f = in.emissiveFaces[entry];
 		const float* m = in.instToWorld + 12 * size_t(i);
-		const uint32_t base = 3u * lod.numTriangles + 4u * q;
+		const bool tri = f < lod.numTriangles;
+		const int corners = tri ? 3 : 4;
+		const uint32_t base = tri ? 3u * f : 3u * lod.numTriangles + 4u * (f - lod.numTriangles);
 		F3 pts[4]; float uv[4][2];
-		for(int k = 0; k < 4; ++k) {
+		for(int k = 0; k < corners; ++k) {
 			const uint32_t vi = lod.indices[base + k];
 			pts[k] = xform_point(m, ld(lod.vertices + 3 * size_t(vi)));
 			uv[k][0] = lod.uvs ? lod.uvs[2 * size_t(vi)] : 0.0f;
 			uv[k][1] = lod.uvs ? lod.uvs[2 * size_t(vi) + 1] : 0.0f;
 		}
-		if(in.mirroring[i]) {
-			const F3 tp = pts[1]; pts[1] = pts[3]; pts[3] = tp;
-			for(int c = 0; c < 2; ++c) { const float tu = uv[1][c]; uv[1][c] = uv[3][c]; uv[3][c] = tu; }
-		}
-		L.type = LT_QUAD;
-		L.material = in.quadMaterial[entry];
-		const F3 e2 = pts[1] - pts[0];
-		st(L.posV[0], pts[0]);
-		st(L.posV[1], pts[3] - pts[0]);
-		st(L.posV[2], e2);
-		st(L.posV[3], (pts[2] - pts[3]) - e2);
-		for(int c = 0; c < 2; ++c) {
-			const float u2 = uv[1][c] - uv[0][c];
-			L.uvV[0][c] = uv[0][c];
-			L.uvV[1][c] = uv[3][c] - uv[0][c];
-			L.uvV[2][c] = u2;
-			L.uvV[3][c] = (uv[2][c] - uv[3][c]) - u2;
+		L.material = in.faceMaterial[entry];
+		if(tri) {
+			// world_container.cpp:929-948 (mirroring swaps the last two corners)
+			if(in.mirroring[i]) {
+				const F3 tp = pts[1]; pts[1] = pts[2]; pts[2] = tp;
+				for(int c = 0; c < 2; ++c) { const float tu = uv[1][c]; uv[1][c] = uv[2][c]; uv[2][c] = tu; }
+			}
+			L.type = LT_TRI;
+			st(L.posV[0], pts[0]);
+			st(L.posV[1], pts[1] - pts[0]);
+			st(L.posV[2], pts[2] - pts[0]);
+			for(int c = 0; c < 2; ++c) {
+				L.uvV[0][c] = uv[0][c];
+				L.uvV[1][c] = uv[1][c] - uv[0][c];
+				L.uvV[2][c] = uv[2][c] - uv[0][c];
+			}
+		} else {
+			if(in.mirroring[i]) {
+				const F3 tp = pts[1]; pts[1] = pts[3]; pts[3] = tp;
+				for(int c = 0; c < 2; ++c) { const float tu = uv[1][c]; uv[1][c] = uv[3][c]; uv[3][c] = tu; }
+			}
+			L.type = LT_QUAD;
+			const F3 e2 = pts[1] - pts[0];
+			st(L.posV[0], pts[0]);
+			st(L.posV[1], pts[3] - pts[0]);
+			st(L.posV[2], e2);
+			st(L.posV[3], (pts[2] - pts[3]) - e2);
+			for(int c = 0; c < 2; ++c) {
+				const float u2 = uv[1][c] - uv[0][c];
+				L.uvV[0][c] = uv[0][c];
+				L.uvV[1][c] = uv[3][c] - uv[0][c];
+				L.uvV[2][c] = u2;
+				L.uvV[3][c] = (uv[2][c] - uv[3][c]) - u2;
+			}
 		}
 		inst = int32_t(i);
-		prim = int32_t(lod.numTriangles + q);
+		prim = int32_t(f);
 	} else {
 		const float* p = in.pointLights + 6 * size_t(t - in.numArea);
 		L.type = LT_POINT;

@@ -3,11 +3,11 @@
 // LightTreeBuilder::build: Hilbert-order sort, balanced tree with extra bottom
 // nodes, per-node fluxes, the (instance, primitive) -> node-path code map).
 //
-// The host decides what emits (a scan of each used LoD's quad materials) and
+// The host decides what emits (a scan of each used LoD's face materials) and
 // hands over, per instance, its instance-to-world matrix, mirroring flag and
-// first light index; everything per light — transforming the quad corners,
-// the Hilbert keys, the stable two-key sort, the 128-sample flux of each
-// quad, the tree and the sorted code map — runs on the device, with the
+// first light index; everything per light — transforming the corners,
+// the Hilbert keys, the stable two-key sort, the flux of each light, the
+// tree and the sorted code map — runs on the device, with the
 // same float operations as the CPU restatement, so the tree is bit-identical.
 #pragma once
 
@@ -20,13 +20,13 @@ namespace mb {
 
 class LbvhBuilder;
 
-// Per used LoD: where its geometry is on the device and which of its quads emit.
+// Per used LoD: where its geometry is on the device and which of its faces emit.
 struct LightLodInfo {
 	const float* vertices;
 	const float* uvs;             // nullptr: the LoD has no uvs (zeros are used)
 	const uint32_t* indices;      // 3 per triangle, then 4 per quad
 	uint32_t numTriangles;
-	uint32_t quadListStart;       // into LightBuildInput::emissiveQuads
+	uint32_t faceListStart;       // into LightBuildInput::emissiveFaces
 };
 
 struct LightBuildInput {
@@ -34,11 +34,11 @@ struct LightBuildInput {
 	const uint32_t* instLod;      // device: used-LoD index per instance (0xFFFFFFFF: none)
 	const float* instToWorld;     // device: 12 floats per instance
 	const uint8_t* mirroring;     // device: per instance, det of the 3x3 part < 0
-	const uint32_t* instFirstLight; // device: numInstances + 1 prefix sums of emissive quads
+	const uint32_t* instFirstLight; // device: numInstances + 1 prefix sums of emissive faces
 	const LightLodInfo* lods;     // device: per used LoD
-	const uint32_t* emissiveQuads;// device: quad indices (within the LoD's quads) of emissive quads
-	const uint16_t* quadMaterial; // device: material slot of each entry of emissiveQuads
-	uint32_t numArea;             // area lights (emissive quads over all instances)
+	const uint32_t* emissiveFaces;// device: per LoD, its emissive faces (triangles first, then quads; index in the LoD's faces)
+	const uint16_t* faceMaterial; // device: material slot of each entry of emissiveFaces
+	uint32_t numArea;             // area lights (emissive faces over all instances)
 	const float* pointLights;     // device: 6 floats (position, intensity) per point light
 	uint32_t numPoint;
 	const DMaterial* materials;   // device

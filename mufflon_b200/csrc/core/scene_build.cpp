@@ -368,23 +368,24 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 
 	// --- lights (world_container.cpp:869-990), list and tree built on the GPU (light_build.cu)
 	if(!upload(D.dMaterials, D.cap[9], mats.data(), mats.size(), s, err)) return false;
-	// world_container.cpp:929-988 also makes emissive triangles and spheres
-	// area lights; this path tracer samples quad area lights only, so a
-	// scenario with other emitters is refused rather than rendered without
-	// their next-event estimation. Emissive quads are listed once per LoD.
+	// world_container.cpp:929-988: emissive triangles and quads become area
+	// lights (triangles first, then quads, per instance). Emissive spheres are
+	// area lights there too; this path tracer does not sample them, so a
+	// scenario with emissive spheres is refused rather than rendered without
+	// their next-event estimation. Emissive faces are listed once per LoD.
 	std::vector<uint32_t> lodQuadStart(D.lodSources.size(), 0), lodQuadCount(D.lodSources.size(), 0);
 	std::vector<uint32_t> emissiveQuads;
 	std::vector<uint16_t> quadMaterial;
 	for(size_t li = 0; li < D.lodSources.size(); ++li) {
 		const HostLod& h = *D.lodSources[li];
 		auto emissive = [&](uint16_t m) { return m < mats.size() && mats[m].type == MAT_EMISSIVE; };
-		for(uint16_t m : h.triMat)
-			if(emissive(m)) { err = "emissive triangles are not area lights in the CUDA path tracer; emitters must be quads"; return false; }
 		for(uint16_t m : h.sphereMat)
-			if(emissive(m)) { err = "emissive spheres are not area lights in the CUDA path tracer; emitters must be quads"; return false; }
+			if(emissive(m)) { err = "emissive spheres are not area lights in the CUDA path tracer; emitters must be triangles or quads"; return false; }
 		lodQuadStart[li] = uint32_t(emissiveQuads.size());
+		for(uint32_t t = 0; t < h.num_triangles(); ++t)
+			if(emissive(h.triMat[t])) { emissiveQuads.push_back(t); quadMaterial.push_back(h.triMat[t]); }
 		for(uint32_t q = 0; q < h.num_quads(); ++q)
-			if(emissive(h.quadMat[q])) { emissiveQuads.push_back(q); quadMaterial.push_back(h.quadMat[q]); }
+			if(emissive(h.quadMat[q])) { emissiveQuads.push_back(h.num_triangles() + q); quadMaterial.push_back(h.quadMat[q]); }
 		lodQuadCount[li] = uint32_t(emissiveQuads.size()) - lodQuadStart[li];
 	}
 	// per instance: instance-to-world, mirroring, first light index (area lights in instance order)
@@ -431,8 +432,8 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	lin.mirroring = D.dLightMirror;
 	lin.instFirstLight = D.dLightFirst;
 	lin.lods = D.dLightLods;
-	lin.emissiveQuads = D.dEmissiveQuads;
-	lin.quadMaterial = D.dQuadMaterial;
+	lin.emissiveFaces = D.dEmissiveQuads;
+	lin.faceMaterial = D.dQuadMaterial;
 	lin.numArea = numArea;
 	lin.pointLights = D.dPointLights;
 	lin.numPoint = numLights - numArea;

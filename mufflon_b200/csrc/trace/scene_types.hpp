@@ -17,7 +17,7 @@ struct WideNode; // lbvh/wide.hpp
 enum : int32_t { MAT_LAMBERT = 0, MAT_TORRANCE = 1, MAT_EMISSIVE = 2 };
 // Torrance shadowing models, numbered as core_interface.h ShadowingModel
 enum : int32_t { SHADOW_VCAVITY = 0, SHADOW_SMITH = 1 };
-enum : uint16_t { LT_POINT = 0, LT_QUAD = 3, LT_INTERNAL = 0xFFFF };
+enum : uint16_t { LT_POINT = 0, LT_TRI = 2, LT_QUAD = 3, LT_INTERNAL = 0xFFFF };
 
 // Reference binary node (src/core/scene/accel_structs/lbvh.hpp:14-18):
 // 32 bytes, two per internal node.
@@ -70,7 +70,7 @@ struct DLight {
 	uint16_t material;
 	float position[3];
 	float intensity[3];
-	float posV[4][3];             // quad: v0, v3-v0, v1-v0, v2-v3-(v1-v0)
+	float posV[4][3];             // quad: v0, v3-v0, v1-v0, v2-v3-(v1-v0); triangle: v0, v1-v0, v2-v0
 	float uvV[4][2];
 };
 

@@ -312,6 +312,32 @@ MBD Nee connect_quad(const DScene& S, const DLight& l, f3 pos, float u0, float u
 	return n;
 }
 
+// light_sampling.hpp:117-140 + 347-368; sampling.hpp:123-128 (barycentric sample)
+MBD Nee connect_tri(const DScene& S, const DLight& l, f3 pos, float u0, float u1) {
+	f3 normal = cross(lv(l.posV[1]), lv(l.posV[2]));
+	const float area2 = len(normal);
+	normal = normal / area2;
+	const float area = area2 * 0.5f;
+	const float bs = 1.0f - sqrt_(1.0f - u0);
+	const float bt = (1.0f - bs) * u1;
+	const f3 position = (lv(l.posV[0]) + lv(l.posV[1]) * bs) + lv(l.posV[2]) * bt;
+	const DMaterial& m = S.materials[l.material];
+	const f3 radiance = m.type == MAT_EMISSIVE ? load3(m.radiance) : make3(0, 0, 0);
+	const f3 intensity = radiance * area;
+	const float pdf = __fdiv_rn(1.0f, area);
+	f3 direction = position - pos;
+	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
+	const float dist = sqrt_(distSq);
+	direction = direction / dist;
+	const float cosOut = dot(normal, -direction);
+	f3 value = make3(0, 0, 0); float vcos = 0.0f;
+	if(cosOut > 0.0f) { value = intensity; vcos = cosOut; }
+	Nee n;
+	n.position = position; n.creationPdf = pdf; n.dir = direction; n.cosOut = vcos;
+	n.diffIrradiance = value / distSq; n.geoNormal = normal; n.distSq = distSq; n.valid = true;
+	return n;
+}
+
 MBD Nee connect_point(const DLight& l, f3 pos) {
 	f3 direction = lv(l.position) - pos;
 	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
@@ -372,10 +398,11 @@ MBD Nee lights_connect(const DScene& S, u64 index, u64 numIndices, u64 seed, f3 
 	}
 	const DLight& l = S.lights[idx];
 	if(l.type == LT_QUAD) return adjust(connect_quad(S, l, position, u0, u1), lightProb);
+	if(l.type == LT_TRI) return adjust(connect_tri(S, l, position, u0, u1), lightProb);
 	return adjust(connect_point(l, position), lightProb);
 }
 
-// light_tree_sampling.hpp:340-412 (quad area lights)
+// light_tree_sampling.hpp:340-412 (triangle and quad area lights)
 MBD float light_connect_pdf(const DScene& S, int inst, int prim, f2 sp) {
 	const float bgSum = (S.bgFlux[0] + S.bgFlux[1]) + S.bgFlux[2];
 	float p = __fdiv_rn(S.rootFlux, (S.dirFlux + S.rootFlux) + bgSum);
@@ -406,6 +433,7 @@ MBD float light_connect_pdf(const DScene& S, int inst, int prim, f2 sp) {
 		const f3 ty = lv(l.posV[2]) + sp.y * lv(l.posV[3]);
 		return __fdiv_rn(p, len(cross(ty, tx)));
 	}
+	if(l.type == LT_TRI) return __fdiv_rn(p, __fdiv_rn(len(cross(lv(l.posV[1]), lv(l.posV[2]))), 2.0f));
 	return 0.0f;
 }
 

@@ -417,12 +417,14 @@ def displaced_plane(seed: int = 0, n: int = 224, width: int = 512, height: int =
 
 
 def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: int = 16, num_point_lights: int = 1,
-                    width: int = 96, height: int = 64) -> SceneSpec:
+                    width: int = 96, height: int = 64, emissive_triangles: int = 0) -> SceneSpec:
     """Many small emissive quads: a ground quad, and `num_instances` instances
-    (one of them mirrored) of a panel set holding a few non-emissive triangles,
+    (one of them mirrored) of a panel set holding non-emissive triangles,
     `quads_per_instance` emissive quads of three radiances and some
-    non-emissive quads; plus point lights. The light tree then has
-    num_instances * quads_per_instance + num_point_lights leaves."""
+    non-emissive quads; plus point lights. With `emissive_triangles` > 0 the
+    panel set also holds that many emissive triangles. The light tree then has
+    num_instances * (quads_per_instance + emissive_triangles) + num_point_lights
+    leaves."""
     rng = np.random.default_rng(seed)
     mats = [MaterialSpec(MAT_LAMBERT, albedo=(0.6, 0.6, 0.55), name="ground"),
             MaterialSpec(MAT_LAMBERT, albedo=(0.3, 0.5, 0.7), name="frame")]
@@ -433,8 +435,8 @@ def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: i
                   quads=np.arange(4, dtype=np.uint32).reshape(1, 4), mats=np.array([0], np.uint16), name="ground")
     # the panel set: frame triangles first, then emissive and frame quads interleaved
     verts, norms, uvs, tris, quads, qmats = [], [], [], [], [], []
-    for t in range(3):
-        c = rng.uniform(-1.5, 1.5, 3)
+    for t in range(3 + emissive_triangles):
+        c = rng.uniform(-1.5, 1.5, 3) + (np.array([0.0, 2.0, 0.0]) if t >= 3 else 0.0)
         p = (c + rng.normal(scale=0.3, size=(3, 3))).astype(np.float32)
         n = np.cross(p[1] - p[0], p[2] - p[0])
         n /= np.linalg.norm(n)
@@ -465,7 +467,8 @@ def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: i
         qmats.append(kind)
     panel = _lod(np.array(verts, np.float32), np.array(norms, np.float32), np.array(uvs, np.float32),
                  tris=np.array(tris, np.uint32), quads=np.array(quads, np.uint32),
-                 mats=np.array([1] * len(tris) + qmats, np.uint16), name="panels")
+                 mats=np.array([1] * 3 + [2 + t % 3 for t in range(emissive_triangles)] + qmats, np.uint16),
+                 name="panels")
     w2i, inst_lod = [identity34()], [0]
     for i in range(num_instances):
         rot = _random_rotation(rng)

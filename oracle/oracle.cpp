@@ -1391,11 +1391,24 @@ inline V3 quad_light_center(const PosLight& l) {
 }
 inline V3 light_center(const PosLight& l) {
 	if(l.type == LT_QUAD) return quad_light_center(l);
+	if(l.type == LT_TRI) return l.posV[0] + (l.posV[1] + l.posV[2]) / 3.0f; // lights.hpp:216-220
 	return l.position;
 }
 inline float light_flux(const Scene& S, const PosLight& l) {
 	if(l.type == LT_POINT) {
 		const V3 f = l.intensity * 4.0f * PI;
+		return (f.x + f.y) + f.z;
+	}
+	if(l.type == LT_TRI) {
+		// lights.cpp:24-40: the mean of 128 radiance samples (a constant emission
+		// adds the same value every time) times area times 2 pi
+		const Material& m = S.materials[l.material];
+		const V3 rad = m.radiance * m.scale;
+		const float area = len(cross(l.posV[1], l.posV[2])) / 2.0f;
+		V3 sum = { 0, 0, 0 };
+		for(int i = 0; i < 128; ++i) sum = sum + rad;
+		sum = sum / 128.0f;
+		const V3 f = sum * area * 2.0f * PI;
 		return (f.x + f.y) + f.z;
 	}
 	// lights.cpp:43-62: for constant emission textures every one of the 128
@@ -1549,6 +1562,30 @@ Nee connect_quad(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) 
 	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true };
 }
 
+// light_sampling.hpp:117-140 + 347-368; sampling.hpp:123-128 (barycentric sample)
+Nee connect_tri(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
+	V3 normal = cross(l.posV[1], l.posV[2]);
+	const float area2 = len(normal);
+	normal = normal / area2;
+	const float area = area2 * 0.5f;
+	const float bs = 1.0f - mbmath::sqrt(1.0f - u0);
+	const float bt = (1.0f - bs) * u1;
+	const V3 position = (l.posV[0] + l.posV[1] * bs) + l.posV[2] * bt;
+	const Material& m = S.materials[l.material];
+	const V3 radiance = m.type == OR_MAT_EMISSIVE ? m.radiance * m.scale : V3{ 0, 0, 0 };
+	const V3 intensity = radiance * area;
+	const float pdf = 1.0f / area;
+	V3 direction = position - pos;
+	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
+	const float dist = mbmath::sqrt(distSq);
+	direction = direction / dist;
+	const float cosOut = dot(normal, -direction);
+	V3 value = { 0, 0, 0 }; float vcos = 0.0f, vpdf = 0.0f;
+	if(cosOut > 0.0f) { value = intensity; vcos = cosOut; vpdf = cosOut / PI; }
+	const V3 diff = value / distSq;
+	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true };
+}
+
 // light_sampling.hpp:308-325
 Nee connect_point(const PosLight& l, V3 pos) {
 	V3 direction = l.position - pos;
@@ -1579,6 +1616,7 @@ inline Nee adjust(Nee n, float chance) {
 
 Nee connect_pos_light(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
 	if(l.type == LT_QUAD) return connect_quad(S, l, pos, u0, u1);
+	if(l.type == LT_TRI) return connect_tri(S, l, pos, u0, u1);
 	return connect_point(l, pos);
 }
 
@@ -1651,6 +1689,7 @@ float light_connect_pdf(const Scene& S, i32 inst, i32 prim, V2 sp) {
 		const V3 ty = l.posV[2] + sp.y * l.posV[3];
 		return p / len(cross(ty, tx));
 	}
+	if(l.type == LT_TRI) return p / (len(cross(l.posV[1], l.posV[2])) / 2.0f);
 	return 0.0f;
 }
 
@@ -2002,6 +2041,26 @@ Scene* create_scene(const OrSceneDesc* d) {
 		const float* m = i2w.m;
 		const float det3 = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[1] * (m[4] * m[10] - m[8] * m[6]) + m[2] * (m[4] * m[9] - m[8] * m[5]);
 		const bool mirroring = det3 < 0.0f;
+		// world_container.cpp:929-948: emissive triangles first, then quads
+		for(u32 t = 0; t < l.nT; ++t) {
+			const u16 mi = l.faceMat[t];
+			if(S->materials[mi].type != OR_MAT_EMISSIVE) continue;
+			V3 pts[3]; V2 uvs[3];
+			for(int k = 0; k < 3; ++k) { pts[k] = xform_point(i2w, l.verts[l.idx[3 * t + k]]); uvs[k] = l.uvs[l.idx[3 * t + k]]; }
+			if(mirroring) { std::swap(pts[1], pts[2]); std::swap(uvs[1], uvs[2]); }
+			PosLight pl{};
+			pl.type = LT_TRI;
+			pl.posV[0] = pts[0];
+			pl.posV[1] = pts[1] - pts[0];
+			pl.posV[2] = pts[2] - pts[0];
+			pl.uvV[0] = uvs[0];
+			pl.uvV[1] = uvs[1] - uvs[0];
+			pl.uvV[2] = uvs[2] - uvs[0];
+			pl.material = mi;
+			pl.primInst = i32(inst);
+			pl.primId = i32(t);
+			T.lights.push_back(pl);
+		}
 		for(u32 q = 0; q < l.nQ; ++q) {
 			const u16 mi = l.faceMat[l.nT + q];
 			if(S->materials[mi].type != OR_MAT_EMISSIVE) continue;

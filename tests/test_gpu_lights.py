@@ -3,7 +3,8 @@ the oracle's CPU build (light_tree.cpp:120-447 restated), byte for byte:
 lights in Hilbert order, node fluxes, indices and types, the sorted
 (instance, primitive) -> node-path codes and the root flux. Light counts cover
 the tree's shapes: one leaf, powers of two, odd and even numbers of extra
-bottom nodes, point lights only, area lights only, a mirroring instance."""
+bottom nodes, point lights only, area lights only, triangle and quad emitters,
+a mirroring instance."""
 import numpy as np
 import pytest
 
@@ -11,9 +12,10 @@ from mufflon_b200 import bindings, scenes
 
 pytestmark = pytest.mark.gpu
 
-# (instances, emissive quads per instance, point lights)
-CASES = [(0, 0, 1), (0, 0, 2), (1, 1, 0), (1, 1, 1), (2, 1, 1), (1, 7, 0), (2, 4, 1), (1, 8, 0), (3, 17, 3),
-         (5, 3, 0), (8, 125, 1), (16, 256, 1), (64, 1024, 2)]
+# (instances, emissive quads per instance, point lights, emissive triangles per instance)
+CASES = [(0, 0, 1, 0), (0, 0, 2, 0), (1, 1, 0, 0), (1, 1, 1, 0), (2, 1, 1, 0), (1, 7, 0, 0), (2, 4, 1, 0), (1, 8, 0, 0),
+         (3, 17, 3, 0), (5, 3, 0, 0), (8, 125, 1, 0), (16, 256, 1, 0), (64, 1024, 2, 0),
+         (1, 0, 0, 1), (2, 3, 1, 5), (5, 40, 2, 17), (32, 100, 1, 37)]
 
 
 def _gpu_tree(spec):
@@ -25,24 +27,25 @@ def _gpu_tree(spec):
         d.close()
 
 
-@pytest.mark.parametrize("case", CASES, ids=[f"{m}x{k}+{p}" for m, k, p in CASES])
+@pytest.mark.parametrize("case", CASES, ids=[f"{m}x({k}q+{t}t)+{p}" for m, k, p, t in CASES])
 def test_gpu_light_tree_equals_oracle(oracle, case):
-    m, k, p = case
-    spec = scenes.emissive_panels(11 + m + k + p, m, k, p, width=16, height=16)
+    m, k, p, t = case
+    spec = scenes.emissive_panels(11 + m + k + p + t, m, k, p, width=16, height=16, emissive_triangles=t)
     gl, gn, gk, gc, grf = _gpu_tree(spec)
     ol, on, ok, oc, orf = oracle.OracleScene(spec).light_tree()
-    n = m * k + p
+    n = m * (k + t) + p
     assert len(gl) == len(ol) == n
     assert len(gn) == len(on) == max(n - 1, 0)
-    assert len(gk) == len(ok) == m * k
+    assert len(gk) == len(ok) == m * (k + t)
     assert np.array_equal(gl, ol), "lights differ (order or values)"
     assert np.array_equal(gn, on), "tree nodes differ"
     assert np.array_equal(gk, ok) and np.array_equal(gc, oc), "node-path codes differ"
     assert np.float32(grf).view(np.uint32) == np.float32(orf).view(np.uint32)
 
 
-def test_render_with_many_area_lights_matches_oracle(oracle):
-    spec = scenes.emissive_panels(5, 6, 40, 2, width=64, height=48)
+@pytest.mark.parametrize("tris", [0, 12])
+def test_render_with_many_area_lights_matches_oracle(oracle, tris):
+    spec = scenes.emissive_panels(5, 6, 40, 2, width=64, height=48, emissive_triangles=tris)
     d = bindings.DllInterface()
     try:
         bindings.load_scene_spec(d, spec)
@@ -64,26 +67,19 @@ def test_render_with_many_area_lights_matches_oracle(oracle):
     assert np.sqrt(np.mean((img - ref) ** 2)) <= 1e-4 * np.sqrt(np.mean(ref ** 2))
 
 
-@pytest.mark.parametrize("kind", ["triangle", "sphere"])
-def test_emissive_triangles_and_spheres_are_refused(kind):
-    """Only quads are area lights in this path tracer; other emitters must not
-    render silently without their next-event estimation."""
+def test_emissive_spheres_are_refused():
+    """Triangles and quads are area lights in this path tracer; emissive
+    spheres must not render silently without their next-event estimation."""
     import dataclasses
     spec = scenes.emissive_panels(2, 2, 3, 1, width=16, height=16)
-    panel = spec.lods[1]
-    if kind == "triangle":
-        fm = np.asarray(panel.face_materials).copy()
-        fm[0] = 2  # the first triangle emits
-        spec = dataclasses.replace(spec, lods=[spec.lods[0], dataclasses.replace(panel, face_materials=fm)])
-    else:
-        sph = scenes._lod(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 2)),
-                          spheres=np.array([[0, 3, 0, 0.5]], np.float32), sphere_mats=np.array([2], np.uint16))
-        spec = dataclasses.replace(spec, lods=list(spec.lods) + [sph],
-                                   world_to_instance=np.concatenate([spec.world_to_instance, [scenes.identity34()]]),
-                                   instance_lod=np.append(spec.instance_lod, 2).astype(np.uint32))
+    sph = scenes._lod(np.zeros((0, 3)), np.zeros((0, 3)), np.zeros((0, 2)),
+                      spheres=np.array([[0, 3, 0, 0.5]], np.float32), sphere_mats=np.array([2], np.uint16))
+    spec = dataclasses.replace(spec, lods=list(spec.lods) + [sph],
+                               world_to_instance=np.concatenate([spec.world_to_instance, [scenes.identity34()]]),
+                               instance_lod=np.append(spec.instance_lod, 2).astype(np.uint32))
     d = bindings.DllInterface()
     try:
-        with pytest.raises(bindings.MufflonError, match=f"emissive {kind}s are not area lights"):
+        with pytest.raises(bindings.MufflonError, match="emissive spheres are not area lights"):
             bindings.load_scene_spec(d, spec)
     finally:
         d.close()
