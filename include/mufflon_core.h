@@ -310,6 +310,15 @@ typedef struct {
 } MufflonStageStats;
 CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
 
+/* EXTENSION with no counterpart in the reference: the camera connections of
+ * the light tracer's last iteration, kept while its integer parameter
+ * "Record connections" is non-zero. slots = width * height * "Max. path
+ * length" (photon major, then the photon's path length at the connection);
+ * pixels[k] receives the pixel index the connection added to, or -1, and
+ * values[5k..5k+4] the radiance rgb, lightness and density it added. */
+CORE_API Boolean CDECL mufflon_get_lt_records(MufflonInstanceHdl instHdl, int32_t* pixels, float* values,
+                                              uint64_t slots);
+
 /* EXTENSION with no counterpart in the reference: renders many jobs at once.
  * A job is the loaded scenario of a library instance (so jobs may use
  * different scenes), rendered at its own resolution (0 = the scenario's),

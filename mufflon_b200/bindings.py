@@ -330,6 +330,7 @@ class DllHolder:
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
             "mufflon_get_load_stats": (c_uint32, [c_void_p, POINTER(MufflonLoadStats)]),
             "mufflon_get_light_tree": (c_uint32, [c_void_p] + [c_void_p] * 8),
+            "mufflon_get_lt_records": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint64]),
             "mufflon_texture_update": (c_uint32, [c_void_p, c_void_p, c_void_p]),
             "mufflon_albedo_gradient": (c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_float)]),
             "mufflon_render_batch": (c_uint32, [POINTER(MufflonBatchJob), c_uint32, c_int32, c_void_p, c_void_p,
@@ -551,6 +552,17 @@ class DllInterface:
         s = MufflonStageStats()
         self._check(self.core.mufflon_get_stage_stats(self.muffInst, byref(s)), "mufflon_get_stage_stats")
         return {k: getattr(s, k) for k, _ in MufflonStageStats._fields_}
+
+    def lt_records(self, max_path_length: int):
+        """The light tracer's camera connections of the last iteration (integer parameter "Record
+        connections" set): pixel index per (photon, path length) slot, -1 for none, and the
+        (radiance rgb, lightness, density) each added."""
+        w, h = self.current_resolution()
+        n = w * h * max(1, max_path_length)
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 5), np.float32)
+        self._check(self.core.mufflon_get_lt_records(self.muffInst, _ptr(pix), _ptr(val), n), "mufflon_get_lt_records")
+        return pix, val
 
     def light_tree(self):
         """The GPU-built light list and tree: (lights (n, 108) uint8, nodes (m, 20) uint8,

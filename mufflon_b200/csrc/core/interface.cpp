@@ -59,11 +59,25 @@ const ParamDesc PT_PARAMS[] = {
 	{ "Trace refill lanes", PARAM_INT }, { "Tail paths", PARAM_INT }, { "Iteration graph", PARAM_INT },
 	{ "Planned tail", PARAM_INT },
 };
+// lt_params.hpp:8-12, plus the recording switch of the parity tests
+const ParamDesc LT_PARAMS[] = {
+	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
+	{ "Record connections", PARAM_INT },
+};
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
 const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
+// Render targets of the light tracer (lt_params.hpp:14-17), all implemented.
+const char* LT_TARGETS[] = { "Radiance", "Lightness", "Density" };
 
 int32_t* param_ptr(RendererState& r, const char* name) {
+	if(r.kind == 1) {
+		if(!std::strcmp(name, "Seed")) return &r.ltParams.seed;
+		if(!std::strcmp(name, "Min. path length")) return &r.ltParams.minPathLength;
+		if(!std::strcmp(name, "Max. path length")) return &r.ltParams.maxPathLength;
+		if(!std::strcmp(name, "Record connections")) return &r.ltRecord;
+		return nullptr;
+	}
 	if(!std::strcmp(name, "Seed")) return &r.params.seed;
 	if(!std::strcmp(name, "Min. path length")) return &r.params.minPathLength;
 	if(!std::strcmp(name, "Max. path length")) return &r.params.maxPathLength;
@@ -121,6 +135,65 @@ void ensure_wavefront_buffers(MufflonInstance& I) {
 	r.wfPixels = n;
 }
 
+// Light tracer buffers for the current resolution: the iteration buffers, the
+// cumulative 1-channel targets and, when recording, the connection records.
+void ensure_lt_buffers(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	const size_t n = size_t(r.width) * r.height;
+	if(!r.ltIter) {
+		CHECK_CUDA(cudaMalloc(&r.ltIter, n * sizeof(float4)));
+		CHECK_CUDA(cudaMalloc(&r.ltIterDensity, n * sizeof(float)));
+		CHECK_CUDA(cudaMalloc(&r.lightness, n * sizeof(float)));
+		CHECK_CUDA(cudaMalloc(&r.density, n * sizeof(float)));
+		CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, n * sizeof(float), I.stream));
+		CHECK_CUDA(cudaMemsetAsync(r.density, 0, n * sizeof(float), I.stream));
+	}
+	const size_t slots = r.ltRecord ? n * size_t(std::max(1, r.ltParams.maxPathLength)) : 0;
+	if(slots != r.ltRecSlots) {
+		cudaFree(r.ltRecPixel); cudaFree(r.ltRecValue);
+		r.ltRecPixel = nullptr; r.ltRecValue = nullptr; r.ltRecSlots = 0;
+		if(slots) {
+			CHECK_CUDA(cudaMalloc(&r.ltRecPixel, slots * sizeof(int32_t)));
+			CHECK_CUDA(cudaMalloc(&r.ltRecValue, slots * 5 * sizeof(float)));
+			CHECK_CUDA(cudaMemsetAsync(r.ltRecPixel, 0xFF, slots * sizeof(int32_t), I.stream));
+			CHECK_CUDA(cudaMemsetAsync(r.ltRecValue, 0, slots * 5 * sizeof(float), I.stream));
+			r.ltRecSlots = slots;
+		}
+	}
+}
+
+// One light-tracing iteration (gpu_lt.cpp / lt_common.hpp): width * height
+// photons, each walk's vertices connected to the camera.
+void iterate_lt(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	const DScene& S = I.scene.desc;
+	LtTargets t{};
+	t.rngState = r.rng;
+	t.iter = r.ltIter;
+	t.iterDensity = r.ltIterDensity;
+	t.radiance = r.targetRadiance ? r.radiance : nullptr;
+	t.lightness = r.targetLightness ? r.lightness : nullptr;
+	t.density = r.targetDensity ? r.density : nullptr;
+	t.recPixel = r.ltRecSlots ? r.ltRecPixel : nullptr;
+	t.recValue = r.ltRecSlots ? r.ltRecValue : nullptr;
+	t.width = r.width; t.height = r.height;
+	t.iteration = r.iteration;
+	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
+	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
+	CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
+	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
+	TraceCounters c{};
+	CHECK_CUDA(cudaMemcpyAsync(&c, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
+	CHECK_CUDA(cudaEventElapsedTime(&r.lastKernelMs, r.evStart, r.evStop));
+	r.lastCounters = c;
+	r.lastExtend = TraceCounters{};
+	r.lastShadow = TraceCounters{};
+	r.lastLaunches = 2;
+	for(float& m : r.stageMs) m = 0.0f;
+	if(c.errors) log_msg(LOG_WARNING, "traversal stack overflow in " + std::to_string(c.errors) + " rays");
+}
+
 // Brings in, through the registered LoD loader, every LoD the current
 // scenario shows but its object does not hold yet (world_container.cpp
 // load_scene: missing LoDs are requested from the loader).
@@ -166,6 +239,10 @@ void RendererState::release() {
 	for(cudaEvent_t e : stageEvents) cudaEventDestroy(e);
 	stageEvents.clear();
 	cudaFree(rng); cudaFree(radiance); cudaFree(hitId); cudaFree(workCounter); cudaFree(counters);
+	cudaFree(ltIter); cudaFree(ltIterDensity); cudaFree(lightness); cudaFree(density);
+	cudaFree(ltRecPixel); cudaFree(ltRecValue);
+	ltIter = nullptr; ltIterDensity = nullptr; lightness = nullptr; density = nullptr;
+	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0;
 	if(evStart) cudaEventDestroy(evStart);
 	if(evStop) cudaEventDestroy(evStop);
 	rng = nullptr; radiance = nullptr; hitId = nullptr; workCounter = nullptr; counters = nullptr;
@@ -252,13 +329,22 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 		r.screen.resize(n * 3);
 		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 3;
-	} else if(!std::strcmp(name, "Hit ID")) {
+	} else if(r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) {
+		const bool light = !std::strcmp(name, "Lightness");
+		CHECK(light ? r.targetLightness : r.targetDensity, std::string("target '") + name + "' is not enabled");
+		const float* src = light ? r.lightness : r.density;
+		CHECK(src != nullptr, "no image yet");
+		r.screen.resize(n);
+		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		r.screenChannels = 1;
+	} else if(r.kind == 0 && !std::strcmp(name, "Hit ID")) {
 		CHECK(r.targetHitId, "target 'Hit ID' is not enabled");
 		r.screen.resize(n * 2);
 		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 2;
 	} else {
-		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA path tracer");
+		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
+		               (r.kind == 1 ? "light tracer" : "path tracer"));
 	}
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	if(ptr) *ptr = r.screen.data();
@@ -899,25 +985,30 @@ Boolean world_set_env_light_scale(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
 }
 
 // ---------------------------------------------------------------- renderers
-uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 1u; CATCH_ALL(0u) }
+// Renderers grouped by name in the reference's registry order (renderers.hpp:23-31,
+// interface.cpp:126-154): the path tracer, then the light tracer, each with its
+// CUDA variation.
+const char* RENDERER_NAMES[2][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" } };
+uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 2u; CATCH_ALL(0u) }
 uint32_t render_get_renderer_variations(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
+	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
 }
 const char* render_get_renderer_name(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return "Pathtracer"; CATCH_ALL(nullptr)
+	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return RENDERER_NAMES[index][0]; CATCH_ALL(nullptr)
 }
 const char* render_get_renderer_short_name(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index == 0, "renderer index out of bounds"); return "PT"; CATCH_ALL(nullptr)
+	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return RENDERER_NAMES[index][1]; CATCH_ALL(nullptr)
 }
 RenderDevice render_get_renderer_devices(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
-	TRY (void)minst(h); CHECK(index == 0 && variation == 0, "renderer index out of bounds"); return DEVICE_CUDA; CATCH_ALL(DEVICE_NONE)
+	TRY (void)minst(h); CHECK(index < 2 && variation == 0, "renderer index out of bounds"); return DEVICE_CUDA; CATCH_ALL(DEVICE_NONE)
 }
 Boolean render_enable_renderer(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
 	TRY
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
-	CHECK(index == 0 && variation == 0, "renderer index out of bounds");
+	CHECK(index < 2 && variation == 0, "renderer index out of bounds");
 	I.renderer.enabled = true;
+	I.renderer.kind = int32_t(index);
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
@@ -936,16 +1027,34 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	ensure_render_buffers(I);
 	RendererState& r = I.renderer;
 	const uint32_t n = r.width * r.height;
+	if(r.kind == 1) {
+		const DScene& S = I.scene.desc;
+		CHECK((S.bgFlux[0] + S.bgFlux[1]) + S.bgFlux[2] == 0.0f,
+		      "the light tracer emits photons from point, triangle and quad lights only; this scene has environment light");
+		ensure_lt_buffers(I);
+	}
 	if(r.needsReset) {
-		CHECK_CUDA(launch_seed_rng(r.rng, n, r.params.seed, I.stream));
+		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
+		CHECK_CUDA(launch_seed_rng(r.rng, n, r.kind == 1 ? r.ltParams.seed : r.params.seed, I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.radiance, 0, size_t(n) * 3 * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
+		if(r.lightness) CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, size_t(n) * sizeof(float), I.stream));
+		if(r.density) CHECK_CUDA(cudaMemsetAsync(r.density, 0, size_t(n) * sizeof(float), I.stream));
 		r.iteration = 0;
 		r.needsReset = false;
 	} else {
 		++r.iteration;
 	}
 	auto t1 = clk::now();
+	if(r.kind == 1) {
+		iterate_lt(I);
+		auto t2 = clk::now();
+		auto us = [](clk::duration d) { return uint64_t(std::chrono::duration_cast<std::chrono::microseconds>(d).count()); };
+		if(preTime) { preTime->cycles = 0; preTime->microseconds = us(t1 - t0); }
+		if(iterTime) { iterTime->cycles = 0; iterTime->microseconds = us(t2 - t1); }
+		if(postTime) { postTime->cycles = 0; postTime->microseconds = 0; }
+		return true;
+	}
 	RenderState rs{};
 	rs.rngState = r.rng;
 	rs.radiance = r.targetRadiance ? r.radiance : nullptr;
@@ -1100,9 +1209,13 @@ Boolean render_save_screenshot(MufflonInstanceHdl h, const char* filename, const
 	CATCH_ALL(false)
 }
 
-uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 8u; CATCH_ALL(0u) }
+uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY return minst(h).renderer.kind == 1 ? 3u : 8u; CATCH_ALL(0u) }
 const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index < 8, "render target index out of bounds"); return TARGETS[index]; CATCH_ALL(nullptr)
+	TRY
+	const bool lt = minst(h).renderer.kind == 1;
+	CHECK(index < (lt ? 3u : 8u), "render target index out of bounds");
+	return lt ? LT_TARGETS[index] : TARGETS[index];
+	CATCH_ALL(nullptr)
 }
 Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
 	TRY
@@ -1112,7 +1225,9 @@ Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Bo
 	CHECK(!variance, "variance targets are not recorded by this renderer");
 	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = true;
 	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = true;
-	else throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA path tracer");
+	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = true;
+	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = true;
+	else throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA renderers");
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
@@ -1124,6 +1239,8 @@ Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, B
 	CHECK(target, "target name is null");
 	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = false;
 	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = false;
+	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = false;
+	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = false;
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
@@ -1134,17 +1251,26 @@ Boolean render_is_render_target_enabled(MufflonInstanceHdl h, const char* name, 
 	if(variance || !name) return false;
 	if(!std::strcmp(name, "Radiance")) return I.renderer.targetRadiance;
 	if(!std::strcmp(name, "Hit ID")) return I.renderer.targetHitId;
+	if(!std::strcmp(name, "Lightness")) return I.renderer.targetLightness;
+	if(!std::strcmp(name, "Density")) return I.renderer.targetDensity;
 	return false;
 	CATCH_ALL(false)
 }
 
-uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) { TRY (void)minst(h); return uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0])); CATCH_ALL(0u) }
+uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) {
+	TRY
+	const bool lt = minst(h).renderer.kind == 1;
+	return lt ? uint32_t(sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0])) : uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]));
+	CATCH_ALL(0u)
+}
 const char* renderer_get_parameter_desc(MufflonInstanceHdl h, uint32_t idx, ParameterType* type) {
 	TRY
-	(void)minst(h);
-	CHECK(idx < sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]), "parameter index out of bounds");
-	if(type) *type = PT_PARAMS[idx].type;
-	return PT_PARAMS[idx].name;
+	const bool lt = minst(h).renderer.kind == 1;
+	const ParamDesc* table = lt ? LT_PARAMS : PT_PARAMS;
+	const size_t count = lt ? sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0]) : sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]);
+	CHECK(idx < count, "parameter index out of bounds");
+	if(type) *type = table[idx].type;
+	return table[idx].name;
 	CATCH_ALL(nullptr)
 }
 Boolean renderer_set_parameter_int(MufflonInstanceHdl h, const char* name, int32_t value) {
@@ -1226,6 +1352,20 @@ Boolean mufflon_get_stage_stats(MufflonInstanceHdl h, MufflonStageStats* s) {
 	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE];
 	s->launches = uint32_t(r.lastLaunches);
 	s->wavefront = r.megakernel ? 0u : 1u;
+	return true;
+	CATCH_ALL(false)
+}
+
+Boolean mufflon_get_lt_records(MufflonInstanceHdl h, int32_t* pixels, float* values, uint64_t slots) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	const RendererState& r = I.renderer;
+	CHECK(r.kind == 1 && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer iteration");
+	CHECK(pixels && values && slots == r.ltRecSlots, "the record buffers must hold width * height * max. path length slots");
+	CHECK_CUDA(cudaMemcpyAsync(pixels, r.ltRecPixel, slots * sizeof(int32_t), cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(values, r.ltRecValue, slots * 5 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	return true;
 	CATCH_ALL(false)
 }

@@ -20,6 +20,7 @@
 #include "../trace/scene_types.hpp"
 #include "../lbvh/lbvh.hpp"
 #include "../trace/wavefront.hpp"
+#include "../trace/lt_api.hpp"
 #include "light_build.hpp"
 
 namespace mb {
@@ -225,6 +226,18 @@ struct RendererState {
 	TraceCounters lastExtend{}, lastShadow{};
 	bool targetRadiance = true;
 	bool targetHitId = false;
+	bool targetLightness = false;  // light tracer targets (lt_params.hpp:14-17)
+	bool targetDensity = false;
+	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer" (renderer registry order)
+	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
+	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
+	float4* ltIter = nullptr;      // light tracer iteration buffers (radiance rgb + lightness, density)
+	float* ltIterDensity = nullptr;
+	float* lightness = nullptr;    // cumulative means of the 1-channel light tracer targets
+	float* density = nullptr;
+	int32_t* ltRecPixel = nullptr;
+	float* ltRecValue = nullptr;
+	size_t ltRecSlots = 0;
 	bool needsReset = true;
 	int32_t iteration = -1;
 	uint32_t width = 0, height = 0;

@@ -1,0 +1,38 @@
+// Host-side launch interface of the light tracer (the CUDA "Lighttracer").
+#pragma once
+
+#include <cuda_runtime.h>
+#include "scene_types.hpp"
+
+namespace mb {
+
+// lt_params.hpp:8-12
+struct LtParams {
+	int32_t seed;
+	int32_t minPathLength;
+	int32_t maxPathLength;
+};
+
+// Output of one light-tracing iteration. Photons land in arbitrary pixels, so
+// they are added to an iteration buffer with atomics; the running means are
+// updated from it after all photons have finished.
+struct LtTargets {
+	uint64_t* rngState;   // one PCG64 state per photon (photon i uses the generator of pixel i)
+	float4* iter;         // iteration buffer: radiance rgb, lightness (zeroed by launch_lt)
+	float* iterDensity;   // iteration buffer of the density (zeroed by launch_lt)
+	float* radiance;      // cumulative means: 3 per pixel (may be null)
+	float* lightness;     // 1 per pixel (may be null)
+	float* density;       // 1 per pixel; null: the Density target is off, which also
+	                      // skips the connections that carry no radiance (lt_common.hpp:51)
+	int32_t* recPixel;    // optional connection records: maxPathLength slots per photon,
+	float* recValue;      // pixel (-1: none) and radiance rgb, lightness, density as added
+	uint32_t width, height;
+	int32_t iteration;    // 0 for the first iteration after a reset
+};
+
+// One light-tracing iteration (width * height photons): clears the iteration
+// buffers and records, traces the photons, updates the running means.
+cudaError_t launch_lt(const DScene& scene, const LtParams& params, const LtTargets& targets,
+                      unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
+
+} // namespace mb

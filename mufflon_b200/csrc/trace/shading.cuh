@@ -171,7 +171,12 @@ MBD f3 half_vector(f3 inTS, f3 exTS) {
 	return make3(sdiv(h.x, l), sdiv(h.y, l), sdiv(h.z, l));
 }
 
-MBD PathSample material_sample(const TangentSpace& ts, const Params& p, f3 incident, float u0, float u1, u64 i0) {
+constexpr float SHADING_NORMAL_EPS = 1e-3f; // material_sampling.hpp:56
+
+// material_sampling.hpp:77-141. adjoint: a vertex of a light sub-path; the
+// throughput gets the shading-normal correction of :132-135.
+MBD PathSample material_sample(const TangentSpace& ts, const Params& p, f3 incident, float u0, float u1, u64 i0,
+                               bool adjoint = false) {
 	PathSample none; none.valid = false; none.throughput = make3(0, 0, 0); none.excident = make3(0, 0, 0); none.pdfF = none.pdfB = 0.0f;
 	const float iDotG = -dot(incident, ts.geoN);
 	const float iDotN = -dot(incident, ts.shadingN);
@@ -224,10 +229,17 @@ MBD PathSample material_sample(const TangentSpace& ts, const Params& p, f3 incid
 	res.excident = g;
 	res.pdfF = fmin_(res.pdfF, 1e9f);
 	res.pdfB = fmin_(res.pdfB, 1e9f);
+	if(adjoint)
+		res.throughput = res.throughput * __fdiv_rn(SHADING_NORMAL_EPS + fabsf(iDotN * eDotG),
+		                                            SHADING_NORMAL_EPS + fabsf(iDotG * eDotN));
 	return res;
 }
 
-MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 incident, f3 excident) {
+// material_sampling.hpp:156-237 (no merge normal). adjoint: a light sub-path
+// vertex; the tangent-space directions are swapped for the BSDF, the value
+// gets the shading-normal correction and the pdfs are swapped back.
+MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 incident, f3 excident,
+                                bool adjoint = false) {
 	EvalValue none; none.value = make3(0, 0, 0); none.cosOut = 0.0f; none.pdfF = none.pdfB = 0.0f;
 	const float iDotN = -dot(incident, ts.shadingN);
 	const float eDotN = dot(excident, ts.shadingN);
@@ -240,8 +252,9 @@ MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 inci
 	const float iDotG = -dot(incident, ts.geoN);
 	const float eDotG = dot(excident, ts.geoN);
 	if(eDotG * eDotN <= 0.0f || iDotG * iDotN <= 0.0f) return none;
-	const f3 inTS = make3(-dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN);
-	const f3 exTS = make3(dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN);
+	f3 inTS = make3(-dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN);
+	f3 exTS = make3(dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN);
+	if(adjoint) { const f3 t = inTS; inTS = exTS; exTS = t; }
 	f3 value; float pf, pb;
 	if(p.type == MAT_LAMBERT) {
 		if(inTS.z * exTS.z < 0.0f) return none;
@@ -272,6 +285,10 @@ MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 inci
 	}
 	if(!nonzero(value)) return none;
 	EvalValue r; r.value = value; r.cosOut = fabsf(eDotN); r.pdfF = fmin_(pf, 1e9f); r.pdfB = fmin_(pb, 1e9f);
+	if(adjoint) {
+		r.value = value * __fdiv_rn(SHADING_NORMAL_EPS + fabsf(iDotN * eDotG), SHADING_NORMAL_EPS + fabsf(iDotG * eDotN));
+		r.pdfF = fmin_(pb, 1e9f); r.pdfB = fmin_(pf, 1e9f);
+	}
 	return r;
 }
 

@@ -1280,8 +1280,10 @@ inline V3 half_vector(V3 inTS, V3 exTS) {
 	return { sdiv(h.x, l), sdiv(h.y, l), sdiv(h.z, l) };
 }
 
-// material_sampling.hpp:77-141 with the Lambert / Torrance(Smith, GGX) / Emissive samplers
-PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident, float u0, float u1, u64 i0) {
+// material_sampling.hpp:77-141 with the Lambert / Torrance(Smith, GGX) / Emissive samplers;
+// adjoint: a light sub-path vertex (the shading-normal correction of :132-135)
+PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident, float u0, float u1, u64 i0,
+                           bool adjoint = false) {
 	PathSample none = { { 0, 0, 0 }, false, { 0, 0, 0 }, 0, 0 };
 	const float iDotG = -dot(incident, ts.geoN);
 	const float iDotN = -dot(incident, ts.shadingN);
@@ -1333,11 +1335,16 @@ PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident,
 	res.excident = g;
 	res.pdfF = fmin_(res.pdfF, 1e9f);
 	res.pdfB = fmin_(res.pdfB, 1e9f);
+	if(adjoint)
+		res.throughput = res.throughput * ((SHADING_NORMAL_EPS + std::fabs(iDotN * eDotG))
+		                                   / (SHADING_NORMAL_EPS + std::fabs(iDotG * eDotN)));
 	return res;
 }
 
-// material_sampling.hpp:156-237 (adjoint = false, no merge normal)
-EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident, V3 excident) {
+// material_sampling.hpp:156-237 (no merge normal). adjoint: a light sub-path
+// vertex; the tangent-space directions are swapped for the BSDF, the value
+// gets the shading-normal correction and the pdfs are swapped back.
+EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident, V3 excident, bool adjoint = false) {
 	EvalValue none = { { 0, 0, 0 }, 0, 0, 0 };
 	const float iDotN = -dot(incident, ts.shadingN);
 	const float eDotN = dot(excident, ts.shadingN);
@@ -1351,8 +1358,9 @@ EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident
 	const float iDotG = -dot(incident, ts.geoN);
 	const float eDotG = dot(excident, ts.geoN);
 	if(eDotG * eDotN <= 0.0f || iDotG * iDotN <= 0.0f) return none;
-	const V3 inTS = { -dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN };
-	const V3 exTS = { dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN };
+	V3 inTS = { -dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN };
+	V3 exTS = { dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN };
+	if(adjoint) std::swap(inTS, exTS);
 	V3 value; float pf, pb;
 	if(p.type == OR_MAT_LAMBERT) {
 		if(inTS.z * exTS.z < 0.0f) return none;
@@ -1382,6 +1390,10 @@ EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident
 		return none;
 	}
 	if(!nonzero(value)) return none;
+	if(adjoint) {
+		value = value * ((SHADING_NORMAL_EPS + std::fabs(iDotN * eDotG)) / (SHADING_NORMAL_EPS + std::fabs(iDotG * eDotN)));
+		return { value, std::fabs(eDotN), fmin_(pb, 1e9f), fmin_(pf, 1e9f) };
+	}
 	return { value, std::fabs(eDotN), fmin_(pf, 1e9f), fmin_(pb, 1e9f) };
 }
 
@@ -1935,6 +1947,277 @@ void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
 	st.stats.add(total);
 }
 
+// ---------------------------------------------------------------- light tracer
+// A photon's start on a light (light_sampling.hpp:20-49 Emitter): the
+// position, the intensity divided by the probability of choosing the light
+// (light_tree_sampling.hpp:12-16) and, for an area light, its normal.
+struct Emitter { V3 position, intensity, normal; bool area, valid; };
+
+// A vector perpendicular to n (not normalised): n crossed with the coordinate
+// axis of n's smallest component. The reference takes `perpendicular` from
+// its math library (epsilon, absent); the emission lobe it orients is
+// rotationally symmetric about n, so the choice of axis changes which
+// direction a random number pair maps to, not the image's expectation.
+inline V3 perpendicular(V3 n) {
+	const float ax = std::fabs(n.x), ay = std::fabs(n.y), az = std::fabs(n.z);
+	if(ax <= ay && ax <= az) return { 0.0f, n.z, -n.y };
+	if(ay <= az) return { -n.z, 0.0f, n.x };
+	return { n.y, -n.x, 0.0f };
+}
+
+// light_sampling.hpp:80-84 (point), 117-140 (triangle), 143-171 (quad)
+Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, float lightProb) {
+	Emitter e{};
+	e.valid = true;
+	if(l.type == LT_POINT) {
+		e.position = l.position;
+		e.intensity = l.intensity / lightProb;
+		e.normal = { 0, 0, 0 };
+		e.area = false;
+		return e;
+	}
+	const Material& m = S.materials[l.material];
+	const V3 radiance = m.type == OR_MAT_EMISSIVE ? m.radiance * m.scale : V3{ 0, 0, 0 };
+	V3 normal, position;
+	float area;
+	if(l.type == LT_TRI) {
+		normal = cross(l.posV[1], l.posV[2]);
+		const float area2 = len(normal);
+		normal = normal / area2;
+		area = area2 * 0.5f;
+		const float bs = 1.0f - mbmath::sqrt(1.0f - u0);
+		const float bt = (1.0f - bs) * u1;
+		position = (l.posV[0] + l.posV[1] * bs) + l.posV[2] * bt;
+	} else {
+		const V3 tx = l.posV[1] + u0 * l.posV[3];
+		const V3 ty = l.posV[2] + u1 * l.posV[3];
+		normal = cross(ty, tx);
+		area = len(normal);
+		normal = normal / area;
+		position = (l.posV[0] + tx * u1) + l.posV[2] * u0;
+	}
+	e.position = position;
+	e.intensity = (radiance * area) / lightProb;
+	e.normal = normal;
+	e.area = true;
+	return e;
+}
+
+// light_tree_sampling.hpp:141-188 with the sub-tree descent of :81-131. The
+// photon index spreads the photons over the flux interval before the seed's
+// random offset. Scenes with environment light are refused by the light
+// tracer (no photon leaves the background here); there are no directional
+// lights.
+Emitter lights_emit(const Scene& S, u64 index, u64 numIndices, u64 seed, float u0, float u1) {
+	const LightTree& T = S.lightTree;
+	u64 rndChoice = numIndices > 0 ? seed + index * (~0ull / numIndices) : seed;
+	if(rndChoice == ~0ull) --rndChoice;
+	const float bgSum = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+	const float fluxSum = (bgSum + T.dirFlux) + T.rootFlux;
+	Emitter none{};
+	none.valid = false;
+	if(!(fluxSum > 0.0f)) return none;
+	const float envProb = bgSum / fluxSum;
+	const float dirProb = T.dirFlux / fluxSum;
+	const float posProb = T.rootFlux / fluxSum;
+	if(rndChoice < percentage_of(~0ull, envProb)) return none;
+	const u64 right = percentage_of(~0ull, envProb + dirProb);
+	if(rndChoice < right) return none;
+	u64 iL = right, iR = ~0ull;
+	float lightProb = posProb;
+	u16 type = T.rootType;
+	i32 idx = T.rootIndex;
+	i32 nodeIdx = 0;
+	while(type == INTERNAL_NODE) {
+		const LightNode& nd = T.nodes[nodeIdx];
+		const float probLeft = nd.left.flux / (nd.left.flux + nd.right.flux);
+		const u64 boundary = iL + percentage_of(iR - iL, probLeft);
+		if(rndChoice < boundary) { type = nd.left.type; idx = nd.left.index; iR = boundary; lightProb *= probLeft; }
+		else { type = nd.right.type; idx = nd.right.index; iL = boundary; lightProb *= (1.0f - probLeft); }
+		nodeIdx = idx;
+	}
+	return sample_light_pos(S, T.lights[idx], u0, u1, lightProb);
+}
+
+// pinhole.hpp:86-116: the pixel a direction leaving the camera falls in and
+// the sensor response w (equal to the sampling pdf); false when the direction
+// points behind the camera or off the image.
+inline bool pinhole_project(const Camera& c, V3 excident, i32& px, i32& py, float& w) {
+	const float cosOut = dot(c.viewDir, excident);
+	if(cosOut < 0.0f) return false;
+	const V3 xAxis = cross(c.viewDir, c.up);
+	const float d = cosOut * c.tanVFov;
+	float ux = dot(xAxis, excident) / d;
+	const float uy = dot(c.up, excident) / d;
+	const float aspect = float(c.resX) / float(c.resY);
+	ux = ux / aspect;
+	if(!(ux > -1.0f && ux <= 1.0f && uy > -1.0f && uy <= 1.0f)) return false;
+	px = i32(std::floor((ux * 0.5f + 0.5f) * float(c.resX)));
+	py = i32(std::floor((uy * 0.5f + 0.5f) * float(c.resY)));
+	if(px >= i32(c.resX)) px = i32(c.resX) - 1;
+	if(py >= i32(c.resY)) py = i32(c.resY) - 1;
+	const float t2 = 2.0f * c.tanVFov;
+	const float pixelArea = (t2 * t2) * aspect;
+	w = 1.0f / (((pixelArea * cosOut) * cosOut) * cosOut);
+	return true;
+}
+
+inline V3 decode_incident(V3 e) {
+	float t = 1.0f - e.x * e.x - e.y * e.y;
+	t = std::fmin(std::fmax(t, 0.0f), 1.0f);
+	return { e.x, e.y, sgn(e.z) * mbmath::sqrt(t) };
+}
+
+struct LtState {
+	const Scene* scene;
+	OrLtParams params;
+	std::vector<Pcg64> rngs;
+	std::vector<float> radiance, lightness, density; // cumulative means
+	std::vector<i32> recPixel;   // last iteration, per photon and path length: pixel or -1
+	std::vector<float> recValue; // ... radiance rgb, lightness, density as added
+	i32 iteration = -1;
+	Counters stats;
+};
+
+enum LtKind { LV_POINT, LV_AREA, LV_SURFACE };
+
+// lt_common.hpp:19-77: one photon's random walk from a light, every vertex
+// (the light vertex included) connected to the camera. The connections are
+// written to rec (one slot per path length).
+void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* recPixel, float* recValue, Counters& cnt) {
+	const Scene& S = *st.scene;
+	const OrLtParams& P = st.params;
+	V3 throughput = { 1, 1, 1 };
+	const u64 r0 = rng.next();
+	const float su0 = sample_uniform(u32(r0)), su1 = sample_uniform(u32(r0 >> 32));
+	const u64 treeSeed = rng.next();
+	const Emitter em = lights_emit(S, photon, numPhotons, treeSeed, su0, su1);
+	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
+	if(!em.valid) return;
+	LtKind kind = em.area ? LV_AREA : LV_POINT;
+	V3 position = em.position;
+	const V3 normal = em.normal, intensity = em.intensity;
+	TangentSpace ts{};
+	Params mat{};
+	V3 incEnc = { 0, 0, 0 };
+	const V3 camPos = S.cam.position;
+	i32 pathLen = 0;
+	do {
+		if(pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
+			// get_connection(camera, vertex) (path_util.hpp:384-403)
+			const V3 c = position - camPos;
+			const float distSq = lensq(c);
+			const float dist = mbmath::sqrt(distSq);
+			const V3 dir = { sdiv(c.x, dist), sdiv(c.y, dist), sdiv(c.z, dist) };
+			i32 px = -1, py = -1;
+			float w = 0.0f;
+			if(pinhole_project(S.cam, dir, px, py, w)) {
+				// vertex.evaluate(-dir, adjoint) (path_util.hpp:245-293, lights.hpp:263-293)
+				const V3 ex = -dir;
+				V3 lvalue = { 0, 0, 0 };
+				float lcos = 0.0f;
+				if(kind == LV_POINT) { lvalue = intensity; lcos = 1.0f; }
+				else if(kind == LV_AREA) { const float co = dot(normal, ex); if(co > 0.0f) { lvalue = intensity; lcos = co; } }
+				else { const EvalValue ev = material_evaluate(ts, mat, decode_incident(incEnc), ex, true); lvalue = ev.value; lcos = ev.cosOut; }
+				V3 bxdfProd = V3{ w, w, w } * lvalue;
+				const float cosProd = 1.0f * lcos;
+				if(P.density || (any_pos(bxdfProd) && cosProd > 0.0f)) {
+					const V3 vGeo = kind == LV_SURFACE ? ts.geoN : (kind == LV_AREA ? normal : V3{ 0, 0, 0 });
+					if(!any_intersection(S, camPos, position, V3{ 0, 0, 0 }, vGeo, dir, cnt)) {
+						bxdfProd = bxdfProd / distSq;
+						const V3 rad = (throughput * cosProd) * bxdfProd;
+						const float light = (((throughput.x + throughput.y) + throughput.z) / 3.0f) * cosProd;
+						float dens = 0.0f;
+						if(P.density) {
+							dens = (w * 1.0f) / distSq;
+							const float gf = kind == LV_SURFACE ? dot(dir, ts.shadingN) : (kind == LV_AREA ? dot(dir, normal) : 0.0f);
+							dens *= std::fabs(gf);
+						}
+						recPixel[pathLen] = py * i32(S.width) + px;
+						float* v = recValue + 5 * size_t(pathLen);
+						v[0] = nan_to_zero(rad.x); v[1] = nan_to_zero(rad.y); v[2] = nan_to_zero(rad.z);
+						v[3] = nan_to_zero(light);
+						v[4] = nan_to_zero(dens);
+					}
+				}
+			}
+		}
+		// walk (random_walk.hpp:38-113), Russian roulette always on
+		const u64 x0 = rng.next(), x1 = rng.next();
+		const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
+		const float rr = sample_uniform(u32(rng.next()));
+		V3 excident, sThroughput;
+		if(kind == LV_POINT) {
+			// sample_light_dir_point (light_sampling.hpp:85-89)
+			excident = sample_dir_sphere_uniform(ru0, ru1);
+			sThroughput = (intensity * 4.0f) * PI;
+		} else if(kind == LV_AREA) {
+			// sample_light_dir_area (light_sampling.hpp:197-210)
+			float cosT;
+			const V3 d = sample_dir_cosine(ru0, ru1, cosT);
+			const V3 tx = normalize(perpendicular(normal));
+			const V3 ty = cross(normal, tx);
+			excident = (d.x * tx + d.y * ty) + d.z * normal;
+			sThroughput = intensity * PI;
+		} else {
+			const PathSample smp = material_sample(ts, mat, decode_incident(incEnc), ru0, ru1, x1, true);
+			if(!smp.valid) break;
+			excident = smp.excident;
+			sThroughput = smp.throughput;
+		}
+		throughput = throughput * sThroughput;
+		const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
+		if(rr >= cp) break;
+		throughput = throughput / cp;
+		const V3 geoN = kind == LV_SURFACE ? ts.geoN : (kind == LV_AREA ? normal : V3{ 0, 0, 0 });
+		V3 origin = position;
+		const Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt);
+		if(hit.inst < 0) break;
+		position = origin + excident * hit.distance;
+		ts = tangent_space(S, hit);
+		mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+		incEnc = { excident.x, excident.y, hit.distance * sgn(excident.z) };
+		kind = LV_SURFACE;
+		++pathLen;
+	} while(pathLen < P.maxPathLength);
+}
+
+// cpu_lt.cpp:18-39: one photon per pixel index per iteration. The terms are
+// added to the iteration buffer in photon order, then the running means are
+// updated (output_handler_variance.hpp:7-31).
+void lt_iterate(LtState& st, int numThreads) {
+	const Scene& S = *st.scene;
+	const u32 n = S.width * S.height;
+	const size_t maxL = size_t(std::max(1, st.params.maxPathLength));
+	++st.iteration;
+	st.recPixel.assign(size_t(n) * maxL, -1);
+	st.recValue.assign(size_t(n) * maxL * 5, 0.0f);
+	Counters total;
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(dynamic, 256)
+		for(i32 photon = 0; photon < i32(n); ++photon)
+			lt_sample(st, u32(photon), n, st.rngs[size_t(photon)], &st.recPixel[size_t(photon) * maxL],
+			          &st.recValue[size_t(photon) * maxL * 5], local);
+#pragma omp critical
+		total.add(local);
+	}
+	st.stats.add(total);
+	std::vector<float> iter(size_t(n) * 5, 0.0f);
+	for(size_t k = 0; k < st.recPixel.size(); ++k) {
+		if(st.recPixel[k] < 0) continue;
+		float* d = &iter[size_t(st.recPixel[k]) * 5];
+		for(int c = 0; c < 5; ++c) d[c] += st.recValue[5 * k + size_t(c)];
+	}
+	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	for(size_t p = 0; p < n; ++p) {
+		for(int c = 0; c < 3; ++c) { float& cr = st.radiance[3 * p + size_t(c)]; const float diff = iter[5 * p + size_t(c)] - cr; cr += diff / den; }
+		{ float& cl = st.lightness[p]; const float diff = iter[5 * p + 3] - cl; cl += diff / den; }
+		{ float& cd = st.density[p]; const float diff = iter[5 * p + 4] - cd; cd += diff / den; }
+	}
+}
+
 // ---------------------------------------------------------------- scene setup
 Scene* create_scene(const OrSceneDesc* d) {
 	auto S = std::make_unique<Scene>();
@@ -2333,6 +2616,55 @@ int oracle_pt_get_target(void* p, int32_t target, float* out) {
 
 int oracle_pt_stats(void* p, OrStats* o) {
 	PtState* st = static_cast<PtState*>(p);
+	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
+	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
+	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
+	return 1;
+}
+
+void* oracle_lt_create(void* s, const OrLtParams* params) {
+	Scene* S = static_cast<Scene*>(s);
+	const LightTree& T = S->lightTree;
+	if((T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z > 0.0f) return nullptr; // no photons from the environment
+	auto* st = new LtState();
+	st->scene = S;
+	st->params = *params;
+	const i32 num = i32(S->width * S->height);
+	st->rngs.resize(size_t(num));
+	// cpu_lt.cpp:33-38
+	const i32 seed = i32(u32(params->seed) * u32(num + 1));
+	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
+	st->radiance.assign(size_t(num) * 3, 0.0f);
+	st->lightness.assign(size_t(num), 0.0f);
+	st->density.assign(size_t(num), 0.0f);
+	return st;
+}
+
+void oracle_lt_destroy(void* p) { delete static_cast<LtState*>(p); }
+
+int oracle_lt_iterate(void* p, int32_t nt) {
+	lt_iterate(*static_cast<LtState*>(p), nt > 0 ? nt : 1);
+	return 1;
+}
+
+int oracle_lt_get_target(void* p, int32_t target, float* out) {
+	const LtState* st = static_cast<const LtState*>(p);
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness : target == 2 ? &st->density : nullptr;
+	if(!v) return 0;
+	std::memcpy(out, v->data(), v->size() * 4);
+	return 1;
+}
+
+int oracle_lt_records(void* p, int32_t* pixels, float* values) {
+	const LtState* st = static_cast<const LtState*>(p);
+	if(st->iteration < 0) return 0;
+	std::memcpy(pixels, st->recPixel.data(), st->recPixel.size() * 4);
+	std::memcpy(values, st->recValue.data(), st->recValue.size() * 4);
+	return 1;
+}
+
+int oracle_lt_stats(void* p, OrStats* o) {
+	const LtState* st = static_cast<const LtState*>(p);
 	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
 	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
 	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;

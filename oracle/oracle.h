@@ -133,6 +133,25 @@ int oracle_pt_stats(void* pt, OrStats* stats);
 /* One iteration restricted to rows [y0, y1) (for bounded CPU baselines). */
 int oracle_pt_iterate_rows(void* pt, int32_t numThreads, uint32_t y0, uint32_t y1);
 
+/* Light tracer (CpuLightTracer equivalent, lt_common.hpp). */
+typedef struct {
+	int32_t seed;
+	int32_t minPathLength;
+	int32_t maxPathLength;
+	int32_t density;        /* the Density target is enabled (it changes which connections are tested) */
+} OrLtParams;
+/* NULL for scenes with environment light (photons are emitted from point,
+ * triangle and quad lights only). */
+void* oracle_lt_create(void* scene, const OrLtParams* params);
+void oracle_lt_destroy(void* lt);
+int oracle_lt_iterate(void* lt, int32_t numThreads);
+/* Cumulative target: 0 radiance (3 ch), 1 lightness (1 ch), 2 density (1 ch) */
+int oracle_lt_get_target(void* lt, int32_t target, float* out);
+/* The last iteration's camera connections, W*H*maxPathLength slots (photon
+ * major, then path length): pixels[k] = pixel index or -1, values[5k..5k+4] =
+ * radiance rgb, lightness, density as added to the iteration buffer. */
+int oracle_lt_records(void* lt, int32_t* pixels, float* values);
+int oracle_lt_stats(void* lt, OrStats* stats);
 /* Building blocks exposed for known-answer tests. */
 int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);

@@ -49,6 +49,11 @@ class OrPtParams(C.Structure):
                 ("neeCount", C.c_int32), ("neePositionGuide", C.c_int32), ("rrStartDepth", C.c_int32)]
 
 
+class OrLtParams(C.Structure):
+    _fields_ = [("seed", C.c_int32), ("minPathLength", C.c_int32), ("maxPathLength", C.c_int32),
+                ("density", C.c_int32)]
+
+
 class OrStats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("shadowRays", C.c_uint64), ("nodeVisits", C.c_uint64),
                 ("instanceVisits", C.c_uint64), ("triTests", C.c_uint64), ("quadTests", C.c_uint64),
@@ -88,6 +93,13 @@ def lib():
         L.oracle_pt_iterate_rows.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32]
         L.oracle_pt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.oracle_pt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_lt_create.restype = C.c_void_p
+        L.oracle_lt_create.argtypes = [C.c_void_p, C.POINTER(OrLtParams)]
+        L.oracle_lt_destroy.argtypes = [C.c_void_p]
+        L.oracle_lt_iterate.argtypes = [C.c_void_p, C.c_int32]
+        L.oracle_lt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.oracle_lt_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_lt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
         L.oracle_pcg64_seed.restype = C.c_uint64
         L.oracle_pcg64_seed.argtypes = [C.c_uint32]
         L.oracle_pcg64_next.restype = C.c_uint64
@@ -282,6 +294,59 @@ class OraclePathTracer:
     def close(self):
         if self.handle:
             lib().oracle_pt_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleLightTracer:
+    """CPU restatement of the light tracer (lt_common.hpp, cpu_lt.cpp): one photon per pixel index and
+    iteration, every path vertex connected to the camera."""
+
+    TARGETS = {"Radiance": (0, 3), "Lightness": (1, 1), "Density": (2, 1)}
+
+    def __init__(self, scene: OracleScene, seed=0, min_path=0, max_path=16, density=False):
+        self.scene = scene
+        self.max_path = max(1, max_path)
+        p = OrLtParams(seed, min_path, max_path, 1 if density else 0)
+        self.handle = lib().oracle_lt_create(scene.handle, C.byref(p))
+        if not self.handle:
+            raise ValueError("the light tracer does not emit photons from environment light")
+
+    def iterate(self, threads: int = 0):
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        lib().oracle_lt_iterate(self.handle, threads)
+
+    def target(self, name: str):
+        w, h = self.scene.spec.width, self.scene.spec.height
+        idx, ch = self.TARGETS[name]
+        out = np.zeros((h, w, ch), np.float32)
+        lib().oracle_lt_get_target(self.handle, idx, _ptr(out))
+        return out
+
+    def records(self):
+        """The last iteration's camera connections: pixel index per (photon, path length) slot (-1: none)
+        and (radiance rgb, lightness, density) as added."""
+        n = self.scene.spec.width * self.scene.spec.height * self.max_path
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 5), np.float32)
+        if not lib().oracle_lt_records(self.handle, _ptr(pix), _ptr(val)):
+            raise RuntimeError("no iteration has run")
+        return pix, val
+
+    def stats(self):
+        s = OrStats()
+        lib().oracle_lt_stats(self.handle, C.byref(s))
+        return {k: getattr(s, k) for k, _ in OrStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().oracle_lt_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
