@@ -28,11 +28,24 @@ struct FastRay {
 	float Sx, Sy, Sz;
 };
 
+// Reciprocal of a direction component for the slab tests, clamped to
+// +-2^64. With an infinite reciprocal (a zero component), an offset of 0 in a
+// slab test gives 0 * inf = NaN, which the min/max chains drop; in the 8-wide
+// test every child plane on the node's origin has offset 0, so that axis
+// stops culling and a ray along a coordinate axis visits every box (one such
+// photon ray took a second). The finite value keeps the culling: a box whose
+// slab holds the ray's constant coordinate spans t = -2^64 * d .. +2^64 * d
+// and is kept, one whose slab does not starts beyond any ray length. Hits
+// depend on the choice only for a ray lying exactly in a box's face plane.
+MBD float slab_rcp(float x) {
+	return fminf(fmaxf(__fdiv_rn(1.0f, x), -18446744073709551616.0f), 18446744073709551616.0f);
+}
+
 MBD FastRay make_ray(f3 o, f3 d) {
 	FastRay r;
 	r.o = o;
 	r.d = d;
-	r.inv = make3(__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z));
+	r.inv = make3(slab_rcp(d.x), slab_rcp(d.y), slab_rcp(d.z));
 	const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
 	int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
 	int kx = kz + 1 == 3 ? 0 : kz + 1;

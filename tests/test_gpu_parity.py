@@ -174,6 +174,54 @@ def test_first_hit_bit_exact(dll, oracle, scene, kernel):
 
 
 @pytest.mark.parametrize("kernel", list(KERNELS))
+@pytest.mark.parametrize("scene", ["icosphere6", "instanced", "mixed"])
+def test_axis_aligned_rays_bit_exact(dll, oracle, scene, kernel):
+    """Rays along the coordinate axes, with +0 and -0 in the other components
+    (a point light's photon drawn at cos = -1 leaves as (-0, 0, -1)): their
+    slab tests use finite reciprocals, and the hits stay the oracle's. Half
+    of the rays pass through triangle interiors. (A ray exactly through a
+    vertex along an axis is left out: there the reference's NaN slab results
+    decide whether the box holding the hit is culled, which no other
+    hierarchy can reproduce.)"""
+    if scene == "icosphere6":
+        spec = scenes.displaced_icosphere(1, subdiv=6, width=64, height=36)
+    elif scene == "mixed":
+        spec = _single_lod_spec(_mixed_lod(7))
+    else:
+        spec = _small_instanced(2)
+    _load(dll, spec)
+    assert dll.renderer_set_parameter_int("Megakernel", KERNELS[kernel])
+    sc = oracle.OracleScene(spec)
+    rng = np.random.default_rng(11)
+    a = sc.aabb()
+    n = 6000
+    org = rng.uniform(a[:3], a[3:], (n, 3)).astype(np.float32)
+    # half of the rays through points inside triangles of the first object
+    lod = spec.lods[0]
+    if scene != "instanced" and len(lod.triangles):
+        k = rng.integers(0, len(lod.triangles), n // 2)
+        b = rng.uniform(0.1, 0.8, (n // 2, 2))
+        b[b.sum(1) > 0.9] *= 0.5
+        v = lod.vertices[lod.triangles[k]].astype(np.float64)
+        org[: n // 2] = (v[:, 0] + b[:, :1] * (v[:, 1] - v[:, 0]) + b[:, 1:] * (v[:, 2] - v[:, 0])).astype(np.float32)
+    axis = rng.integers(0, 3, n)
+    sign = np.where(rng.uniform(size=n) < 0.5, -1.0, 1.0).astype(np.float32)
+    dirs = np.zeros((n, 3), np.float32)
+    dirs[np.arange(n), axis] = sign
+    zsign = rng.uniform(size=(n, 3)) < 0.5
+    dirs[(dirs == 0) & zsign] = np.float32(-0.0)
+    if scene != "instanced":
+        org[np.arange(n // 2), axis[: n // 2]] -= 3.0 * sign[: n // 2]
+    rays = np.concatenate([org, dirs], 1)
+    gt, gi, gp, gs = dll.trace_rays(rays)
+    ot, oi, op, os_ = sc.trace_first(rays)
+    assert np.array_equal(gi, oi) and np.array_equal(gp, op)
+    assert np.array_equal(gt.view(np.uint32), ot.view(np.uint32))
+    assert np.array_equal(gs.view(np.uint32), os_.view(np.uint32))
+    assert (gi >= 0).mean() > (0.02 if scene == "instanced" else 0.3)
+
+
+@pytest.mark.parametrize("kernel", list(KERNELS))
 @pytest.mark.parametrize("scene", ["cornell", "instanced"])
 def test_occlusion_matches_oracle(dll, oracle, scene, kernel):
     spec = scenes.cornell_box(4) if scene == "cornell" else _small_instanced(3)
