@@ -667,20 +667,17 @@ def run_lights(args):
 
 
 def run_lt(args):
-    """The light tracer ("Lighttracer", lt.cu) on the 1080p icosphere lit by
-    its point light (the environment light removed: photons start on point,
-    triangle and quad lights): 16 iterations of 1920 x 1080 photons per step,
-    path length up to 10. Device time per iteration from CUDA events around
-    the launches; rays = extension rays + camera-connection shadow rays. The
-    CPU baseline is one iteration of the oracle's light tracer on all host
-    cores."""
-    import dataclasses
+    """The light tracer ("Lighttracer", lt.cu) on the headline scene (the
+    1080p icosphere, its point light and colored background): 16 iterations
+    of 1920 x 1080 photons per step, path length up to 10. Device time per
+    iteration from CUDA events around the launches; rays = extension rays +
+    camera-connection shadow rays. The CPU baseline is one iteration of the
+    oracle's light tracer on all host cores."""
     import torch
     torch.cuda.set_device(0)
     from mufflon_b200 import bindings, build, scenes
     build.build()
-    spec = dataclasses.replace(scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT),
-                               background=None)
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
     d = bindings.DllInterface()
     bindings.load_scene_spec(d, spec)
     assert d.render_enable_renderer(1, 0)

@@ -1027,12 +1027,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	ensure_render_buffers(I);
 	RendererState& r = I.renderer;
 	const uint32_t n = r.width * r.height;
-	if(r.kind == 1) {
-		const DScene& S = I.scene.desc;
-		CHECK((S.bgFlux[0] + S.bgFlux[1]) + S.bgFlux[2] == 0.0f,
-		      "the light tracer emits photons from point, triangle and quad lights only; this scene has environment light");
-		ensure_lt_buffers(I);
-	}
+	if(r.kind == 1) ensure_lt_buffers(I);
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
 		CHECK_CUDA(launch_seed_rng(r.rng, n, r.kind == 1 ? r.ltParams.seed : r.params.seed, I.stream));

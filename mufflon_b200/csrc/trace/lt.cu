@@ -19,10 +19,14 @@
 namespace mb {
 namespace {
 
+enum LtKind { LV_POINT = 0, LV_AREA = 1, LV_SURFACE = 2, LV_ENV = 3 };
+
 // A photon's start on a light (light_sampling.hpp:20-49 Emitter): the
 // position, the intensity divided by the probability of choosing the light
-// (light_tree_sampling.hpp:12-16) and, for an area light, its normal.
-struct Emitter { f3 position, intensity, normal; bool area, valid; };
+// (light_tree_sampling.hpp:12-16) and, for an area light, its normal; for
+// the environment, the direction the photon travels (in `normal`) and the
+// irradiance.
+struct Emitter { f3 position, intensity, normal; int kind; bool valid; };
 
 // render_target.hpp:64-75: a NaN channel of a contribution is added as 0
 MBD float nan_to_zero(float x) { return isnan(x) ? 0.0f : x; }
@@ -47,7 +51,7 @@ MBD Emitter sample_light_pos(const DScene& S, const DLight& l, float u0, float u
 		e.position = lv(l.position);
 		e.intensity = lv(l.intensity) / lightProb;
 		e.normal = make3(0.0f, 0.0f, 0.0f);
-		e.area = false;
+		e.kind = LV_POINT;
 		return e;
 	}
 	const DMaterial& m = S.materials[l.material];
@@ -73,14 +77,29 @@ MBD Emitter sample_light_pos(const DScene& S, const DLight& l, float u0, float u
 	e.position = position;
 	e.intensity = (radiance * area) / lightProb;
 	e.normal = normal;
-	e.area = true;
+	e.kind = LV_AREA;
+	return e;
+}
+
+// light_sampling.hpp:226-232 and 292-306 (a colored background), scaled by
+// the environment's choice probability (light_tree_sampling.hpp:158-167): a
+// direction drawn uniformly on the sphere; the photon travels against it.
+MBD Emitter sample_background(const DScene& S, float u0, float u1, float envProb) {
+	const f3 dir = sample_dir_sphere_uniform(u0, u1);
+	const float dirPdf = __fdiv_rn(1.0f, 4.0f * PI);
+	const f3 irradiance = (lv(S.bgColor) * lv(S.bgScale)) / dirPdf;
+	Emitter e;
+	e.valid = true;
+	e.kind = LV_ENV;
+	e.position = make3(0.0f, 0.0f, 0.0f);
+	e.normal = -dir;
+	e.intensity = irradiance / envProb;
 	return e;
 }
 
 // light_tree_sampling.hpp:141-188 with the sub-tree descent of :81-131: the
 // photon index spreads the photons evenly over the flux interval before the
-// seed's random offset. Scenes with environment light are refused by the
-// renderer before launch; there are no directional lights.
+// seed's random offset. There are no directional lights.
 MBD Emitter lights_emit(const DScene& S, u64 index, u64 numIndices, u64 seed, float u0, float u1) {
 	u64 rndChoice = numIndices > 0 ? seed + index * (~0ull / numIndices) : seed;
 	if(rndChoice == ~0ull) --rndChoice;
@@ -92,7 +111,7 @@ MBD Emitter lights_emit(const DScene& S, u64 index, u64 numIndices, u64 seed, fl
 	const float envProb = __fdiv_rn(bgSum, fluxSum);
 	const float dirProb = __fdiv_rn(S.dirFlux, fluxSum);
 	const float posProb = __fdiv_rn(S.rootFlux, fluxSum);
-	if(rndChoice < percentage_of(~0ull, envProb)) return none;
+	if(rndChoice < percentage_of(~0ull, envProb)) return sample_background(S, u0, u1, envProb);
 	const u64 right = percentage_of(~0ull, envProb + dirProb);
 	if(rndChoice < right) return none;
 	u64 iL = right, iR = ~0ull;
@@ -141,7 +160,6 @@ MBD f3 decode_incident(f3 e) {
 	return make3(e.x, e.y, sgn(e.z) * sqrt_(t));
 }
 
-enum LtKind { LV_POINT = 0, LV_AREA = 1, LV_SURFACE = 2 };
 enum LtPhase { PH_IDLE = 0, PH_CONNECT = 1, PH_EXTEND = 2, PH_EXIT = 3 };
 
 // The state of one photon's current path vertex.
@@ -156,14 +174,14 @@ struct Photon {
 
 // lt_common.hpp:19-37: the start vertex on a light. The generator draws, in
 // order, the position numbers, the light-tree seed and the camera's number.
-MBD bool lt_emit(const DScene& S, Photon& ph, uint32_t numPhotons) {
+static __device__ __noinline__ bool lt_emit(const DScene& S, Photon& ph, uint32_t numPhotons) {
 	ph.throughput = make3(1.0f, 1.0f, 1.0f);
 	const u64 r0 = pcg_next(ph.rng);
 	const float su0 = sample_uniform(uint32_t(r0)), su1 = sample_uniform(uint32_t(r0 >> 32));
 	const u64 treeSeed = pcg_next(ph.rng);
 	const Emitter em = lights_emit(S, ph.photon, numPhotons, treeSeed, su0, su1);
 	(void)pcg_next(ph.rng); // create_camera consumes one number (unused by the pinhole camera)
-	ph.kind = em.area ? LV_AREA : LV_POINT;
+	ph.kind = em.kind;
 	ph.position = em.position;
 	ph.normal = em.normal;
 	ph.intensity = em.intensity;
@@ -176,17 +194,51 @@ MBD f3 vertex_geo_normal(const Photon& ph) {
 	return ph.kind == LV_SURFACE ? ph.ts.geoN : (ph.kind == LV_AREA ? ph.normal : make3(0.0f, 0.0f, 0.0f));
 }
 
+// math/sampling.hpp:132-158: a start point for a photon of direction dir on
+// the faces of the scene box it enters through, and the inverse of the
+// box's projected area (the position pdf).
+MBD f3 sample_position(const DScene& S, f3 dir, float u0, float u1, float& pdf) {
+	const f3 mn = lv(S.aabbMin);
+	const f3 sides = lv(S.aabbMax) - mn;
+	const float projAx = (sides.y * sides.z) * fabsf(dir.x);
+	const float projAy = (sides.x * sides.z) * fabsf(dir.y);
+	const float projAz = (sides.x * sides.y) * fabsf(dir.z);
+	const float area = (projAx + projAy) + projAz;
+	float x = u0 * area;
+	f3 p;
+	if(x < projAx) {
+		x = __fdiv_rn(x - 0.0f, projAx - 0.0f);
+		p = make3(dir.x < 0.0f ? 1.0f : 0.0f, u1, x);
+	} else if(x < projAx + projAy) {
+		x = __fdiv_rn(x - projAx, (projAx + projAy) - projAx);
+		p = make3(u1, dir.y < 0.0f ? 1.0f : 0.0f, x);
+	} else {
+		x = __fdiv_rn(x - (projAx + projAy), area - (projAx + projAy));
+		p = make3(u1, x, dir.z < 0.0f ? 1.0f : 0.0f);
+	}
+	pdf = __fdiv_rn(1.0f, area);
+	return (mn + p * sides) - dir * 1e-3f;
+}
+
 // lt_common.hpp:39-72: the connection of the current vertex to the camera.
 // Returns true with the shadow ray and the terms it adds when it needs an
 // occlusion test.
-MBD bool lt_connect(const DScene& S, const LtTargets& T, const Photon& ph, f3& so, f3& sd, float& stmax,
+static __device__ __noinline__ bool lt_connect(const DScene& S, const LtTargets& T, const Photon& ph, f3& so, f3& sd, float& stmax,
                     uint32_t& pix, float4& add, float& dens) {
 	const f3 camPos = lv(S.camera.position);
-	// get_connection(camera, vertex) (path_util.hpp:384-403)
-	const f3 c = ph.position - camPos;
-	const float distSq = lensq(c);
-	const float dist = sqrt_(distSq);
-	const f3 dir = make3(sdiv(c.x, dist), sdiv(c.y, dist), sdiv(c.z, dist));
+	// get_connection(camera, vertex) (path_util.hpp:384-403); an environment
+	// vertex has no position: the connection is its direction at distance 1
+	f3 dir;
+	float distSq;
+	if(ph.kind == LV_ENV) {
+		dir = -ph.normal;
+		distSq = 1.0f;
+	} else {
+		const f3 c = ph.position - camPos;
+		distSq = lensq(c);
+		const float dist = sqrt_(distSq);
+		dir = make3(sdiv(c.x, dist), sdiv(c.y, dist), sdiv(c.z, dist));
+	}
 	int px, py;
 	float w;
 	if(!pinhole_project(S.camera, dir, px, py, w)) return false;
@@ -194,20 +246,23 @@ MBD bool lt_connect(const DScene& S, const LtTargets& T, const Photon& ph, f3& s
 	const f3 ex = -dir;
 	f3 lvalue = make3(0.0f, 0.0f, 0.0f);
 	float lcos = 0.0f;
-	if(ph.kind == LV_POINT) { lvalue = ph.intensity; lcos = 1.0f; }
+	if(ph.kind == LV_POINT || ph.kind == LV_ENV) { lvalue = ph.intensity; lcos = 1.0f; }
 	else if(ph.kind == LV_AREA) { const float co = dot(ph.normal, ex); if(co > 0.0f) { lvalue = ph.intensity; lcos = co; } }
 	else { const EvalValue ev = material_evaluate(ph.ts, ph.mat, decode_incident(ph.incEnc), ex, true); lvalue = ev.value; lcos = ev.cosOut; }
 	f3 bxdfProd = make3(w, w, w) * lvalue;
 	const float cosProd = 1.0f * lcos;
 	if(!(T.density || (any_pos(bxdfProd) && cosProd > 0.0f))) return false;
-	shadow_ray(camPos, ph.position, make3(0.0f, 0.0f, 0.0f), vertex_geo_normal(ph), dir, so, sd, stmax);
+	// the environment vertex is placed the maximum scene size away (path_util.hpp:130-137)
+	const f3 vpos = ph.kind == LV_ENV ? camPos - decode_incident(ph.normal) * MAX_SCENE_SIZE : ph.position;
+	shadow_ray(camPos, vpos, make3(0.0f, 0.0f, 0.0f), vertex_geo_normal(ph), dir, so, sd, stmax);
 	bxdfProd = bxdfProd / distSq;
 	const f3 rad = (ph.throughput * cosProd) * bxdfProd;
 	const float light = __fdiv_rn((ph.throughput.x + ph.throughput.y) + ph.throughput.z, 3.0f) * cosProd;
 	dens = 0.0f;
 	if(T.density) {
 		dens = __fdiv_rn(w * 1.0f, distSq);
-		const float gf = ph.kind == LV_SURFACE ? dot(dir, ph.ts.shadingN) : (ph.kind == LV_AREA ? dot(dir, ph.normal) : 0.0f);
+		const float gf = ph.kind == LV_SURFACE ? dot(dir, ph.ts.shadingN)
+		               : ph.kind == LV_AREA ? dot(dir, ph.normal) : ph.kind == LV_ENV ? 1.0f : 0.0f;
 		dens *= fabsf(gf);
 	}
 	add = make_float4(nan_to_zero(rad.x), nan_to_zero(rad.y), nan_to_zero(rad.z), nan_to_zero(light));
@@ -218,11 +273,12 @@ MBD bool lt_connect(const DScene& S, const LtTargets& T, const Photon& ph, f3& s
 
 // random_walk.hpp:38-75 (Russian roulette always on): the next direction
 // and throughput; false when the path ends here. The ray origin is offset.
-MBD bool lt_walk(Photon& ph, f3& origin, f3& excident) {
+static __device__ __noinline__ bool lt_walk(const DScene& S, Photon& ph, f3& origin, f3& excident) {
 	const u64 x0 = pcg_next(ph.rng), x1 = pcg_next(ph.rng);
 	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
 	const float rr = sample_uniform(uint32_t(pcg_next(ph.rng)));
 	f3 sThroughput;
+	f3 start = ph.position;
 	if(ph.kind == LV_POINT) {
 		// sample_light_dir_point (light_sampling.hpp:85-89)
 		excident = sample_dir_sphere_uniform(ru0, ru1);
@@ -234,6 +290,12 @@ MBD bool lt_walk(Photon& ph, f3& origin, f3& excident) {
 		const f3 ty = cross(ph.normal, tx);
 		excident = (d.x * tx + d.y * ty) + d.z * ph.normal;
 		sThroughput = ph.intensity * PI;
+	} else if(ph.kind == LV_ENV) {
+		// path_util.hpp:312-320: a start point on the scene box, travelling along the photon's direction
+		float pdf;
+		start = sample_position(S, ph.normal, ru0, ru1, pdf);
+		excident = ph.normal;
+		sThroughput = ph.intensity / pdf;
 	} else {
 		const PathSample smp = material_sample(ph.ts, ph.mat, decode_incident(ph.incEnc), ru0, ru1, x1, true);
 		if(!smp.valid) return false;
@@ -244,11 +306,14 @@ MBD bool lt_walk(Photon& ph, f3& origin, f3& excident) {
 	const float cp = fmin_(maxc(ph.throughput) + 0.1f, 1.0f);
 	if(rr >= cp) return false;
 	ph.throughput = ph.throughput / cp;
-	origin = ph.position;
+	origin = start;
 	add_epsilon(origin, excident, vertex_geo_normal(ph));
 	return true;
 }
 
+// (lt_emit, lt_connect and lt_walk are out of line: once per vertex, they
+// would otherwise crowd the traversal loop out of the instruction cache; 3 %
+// faster on the instanced scene.)
 // lt_common.hpp:19-77 as a per-lane state machine: a lane takes a new photon
 // as soon as its photon ends (the warp claims all its idle lanes' photons with
 // one atomic), and every pass of the loop traces at most one ray per lane
@@ -299,7 +364,7 @@ __global__ void __launch_bounds__(128, 5) k_lt(const DScene S, const LtParams P,
 			phase = PH_EXTEND;
 		}
 		if(!trace && phase == PH_EXTEND) {
-			if(lt_walk(ph, ro, rd)) { trace = true; tmax = MAX_SCENE_SIZE; }
+			if(lt_walk(S, ph, ro, rd)) { trace = true; tmax = MAX_SCENE_SIZE; }
 			else { T.rngState[ph.photon] = ph.rng; phase = PH_IDLE; }
 		}
 		if(trace) {

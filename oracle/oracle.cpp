@@ -1948,10 +1948,14 @@ void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
 }
 
 // ---------------------------------------------------------------- light tracer
+enum LtKind { LV_POINT, LV_AREA, LV_SURFACE, LV_ENV };
+
 // A photon's start on a light (light_sampling.hpp:20-49 Emitter): the
 // position, the intensity divided by the probability of choosing the light
-// (light_tree_sampling.hpp:12-16) and, for an area light, its normal.
-struct Emitter { V3 position, intensity, normal; bool area, valid; };
+// (light_tree_sampling.hpp:12-16) and, for an area light, its normal; for
+// the environment, the direction the photon travels (in `normal`) and the
+// irradiance.
+struct Emitter { V3 position, intensity, normal; LtKind kind; bool valid; };
 
 // A vector perpendicular to n (not normalised): n crossed with the coordinate
 // axis of n's smallest component. The reference takes `perpendicular` from
@@ -1973,7 +1977,7 @@ Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, 
 		e.position = l.position;
 		e.intensity = l.intensity / lightProb;
 		e.normal = { 0, 0, 0 };
-		e.area = false;
+		e.kind = LV_POINT;
 		return e;
 	}
 	const Material& m = S.materials[l.material];
@@ -1999,15 +2003,54 @@ Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, 
 	e.position = position;
 	e.intensity = (radiance * area) / lightProb;
 	e.normal = normal;
-	e.area = true;
+	e.kind = LV_AREA;
 	return e;
+}
+
+// light_sampling.hpp:226-232 and 292-306 (a colored background), scaled by
+// the environment's choice probability (light_tree_sampling.hpp:158-167): a
+// direction drawn uniformly on the sphere; the photon travels against it.
+Emitter sample_background(const LightTree& T, float u0, float u1, float envProb) {
+	const V3 dir = sample_dir_sphere_uniform(u0, u1);
+	const float dirPdf = 1.0f / (4.0f * PI);
+	const V3 irradiance = (T.bgColor * T.bgScale) / dirPdf;
+	Emitter e{};
+	e.valid = true;
+	e.kind = LV_ENV;
+	e.position = { 0, 0, 0 };
+	e.normal = -dir;
+	e.intensity = irradiance / envProb;
+	return e;
+}
+
+// math/sampling.hpp:132-158: a start point for a photon of direction dir on
+// the faces of the scene box it enters through, and the inverse of the
+// box's projected area (the position pdf).
+V3 sample_position(const Box& b, V3 dir, float u0, float u1, float& pdf) {
+	const V3 sides = b.mx - b.mn;
+	const float projAx = (sides.y * sides.z) * std::fabs(dir.x);
+	const float projAy = (sides.x * sides.z) * std::fabs(dir.y);
+	const float projAz = (sides.x * sides.y) * std::fabs(dir.z);
+	const float area = (projAx + projAy) + projAz;
+	float x = u0 * area;
+	V3 p;
+	if(x < projAx) {
+		x = (x - 0.0f) / (projAx - 0.0f);
+		p = { dir.x < 0.0f ? 1.0f : 0.0f, u1, x };
+	} else if(x < projAx + projAy) {
+		x = (x - projAx) / ((projAx + projAy) - projAx);
+		p = { u1, dir.y < 0.0f ? 1.0f : 0.0f, x };
+	} else {
+		x = (x - (projAx + projAy)) / (area - (projAx + projAy));
+		p = { u1, x, dir.z < 0.0f ? 1.0f : 0.0f };
+	}
+	pdf = 1.0f / area;
+	return (b.mn + p * sides) - dir * 1e-3f;
 }
 
 // light_tree_sampling.hpp:141-188 with the sub-tree descent of :81-131. The
 // photon index spreads the photons over the flux interval before the seed's
-// random offset. Scenes with environment light are refused by the light
-// tracer (no photon leaves the background here); there are no directional
-// lights.
+// random offset. There are no directional lights.
 Emitter lights_emit(const Scene& S, u64 index, u64 numIndices, u64 seed, float u0, float u1) {
 	const LightTree& T = S.lightTree;
 	u64 rndChoice = numIndices > 0 ? seed + index * (~0ull / numIndices) : seed;
@@ -2020,7 +2063,7 @@ Emitter lights_emit(const Scene& S, u64 index, u64 numIndices, u64 seed, float u
 	const float envProb = bgSum / fluxSum;
 	const float dirProb = T.dirFlux / fluxSum;
 	const float posProb = T.rootFlux / fluxSum;
-	if(rndChoice < percentage_of(~0ull, envProb)) return none;
+	if(rndChoice < percentage_of(~0ull, envProb)) return sample_background(T, u0, u1, envProb);
 	const u64 right = percentage_of(~0ull, envProb + dirProb);
 	if(rndChoice < right) return none;
 	u64 iL = right, iR = ~0ull;
@@ -2079,8 +2122,6 @@ struct LtState {
 	Counters stats;
 };
 
-enum LtKind { LV_POINT, LV_AREA, LV_SURFACE };
-
 // lt_common.hpp:19-77: one photon's random walk from a light, every vertex
 // (the light vertex included) connected to the camera. The connections are
 // written to rec (one slot per path length).
@@ -2094,7 +2135,7 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 	const Emitter em = lights_emit(S, photon, numPhotons, treeSeed, su0, su1);
 	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
 	if(!em.valid) return;
-	LtKind kind = em.area ? LV_AREA : LV_POINT;
+	LtKind kind = em.kind;
 	V3 position = em.position;
 	const V3 normal = em.normal, intensity = em.intensity;
 	TangentSpace ts{};
@@ -2104,11 +2145,20 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 	i32 pathLen = 0;
 	do {
 		if(pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
-			// get_connection(camera, vertex) (path_util.hpp:384-403)
-			const V3 c = position - camPos;
-			const float distSq = lensq(c);
-			const float dist = mbmath::sqrt(distSq);
-			const V3 dir = { sdiv(c.x, dist), sdiv(c.y, dist), sdiv(c.z, dist) };
+			// get_connection(camera, vertex) (path_util.hpp:384-403); an
+			// environment vertex has no position: the connection is its
+			// direction at distance 1
+			V3 dir;
+			float distSq;
+			if(kind == LV_ENV) {
+				dir = -normal;
+				distSq = 1.0f;
+			} else {
+				const V3 c = position - camPos;
+				distSq = lensq(c);
+				const float dist = mbmath::sqrt(distSq);
+				dir = { sdiv(c.x, dist), sdiv(c.y, dist), sdiv(c.z, dist) };
+			}
 			i32 px = -1, py = -1;
 			float w = 0.0f;
 			if(pinhole_project(S.cam, dir, px, py, w)) {
@@ -2116,21 +2166,24 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 				const V3 ex = -dir;
 				V3 lvalue = { 0, 0, 0 };
 				float lcos = 0.0f;
-				if(kind == LV_POINT) { lvalue = intensity; lcos = 1.0f; }
+				if(kind == LV_POINT || kind == LV_ENV) { lvalue = intensity; lcos = 1.0f; }
 				else if(kind == LV_AREA) { const float co = dot(normal, ex); if(co > 0.0f) { lvalue = intensity; lcos = co; } }
 				else { const EvalValue ev = material_evaluate(ts, mat, decode_incident(incEnc), ex, true); lvalue = ev.value; lcos = ev.cosOut; }
 				V3 bxdfProd = V3{ w, w, w } * lvalue;
 				const float cosProd = 1.0f * lcos;
 				if(P.density || (any_pos(bxdfProd) && cosProd > 0.0f)) {
 					const V3 vGeo = kind == LV_SURFACE ? ts.geoN : (kind == LV_AREA ? normal : V3{ 0, 0, 0 });
-					if(!any_intersection(S, camPos, position, V3{ 0, 0, 0 }, vGeo, dir, cnt)) {
+					// the environment vertex is placed the maximum scene size away (path_util.hpp:130-137)
+					const V3 vpos = kind == LV_ENV ? camPos - decode_incident(normal) * MAX_SCENE_SIZE : position;
+					if(!any_intersection(S, camPos, vpos, V3{ 0, 0, 0 }, vGeo, dir, cnt)) {
 						bxdfProd = bxdfProd / distSq;
 						const V3 rad = (throughput * cosProd) * bxdfProd;
 						const float light = (((throughput.x + throughput.y) + throughput.z) / 3.0f) * cosProd;
 						float dens = 0.0f;
 						if(P.density) {
 							dens = (w * 1.0f) / distSq;
-							const float gf = kind == LV_SURFACE ? dot(dir, ts.shadingN) : (kind == LV_AREA ? dot(dir, normal) : 0.0f);
+							const float gf = kind == LV_SURFACE ? dot(dir, ts.shadingN)
+							               : kind == LV_AREA ? dot(dir, normal) : kind == LV_ENV ? 1.0f : 0.0f;
 							dens *= std::fabs(gf);
 						}
 						recPixel[pathLen] = py * i32(S.width) + px;
@@ -2147,6 +2200,7 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 		const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
 		const float rr = sample_uniform(u32(rng.next()));
 		V3 excident, sThroughput;
+		V3 start = position;
 		if(kind == LV_POINT) {
 			// sample_light_dir_point (light_sampling.hpp:85-89)
 			excident = sample_dir_sphere_uniform(ru0, ru1);
@@ -2159,6 +2213,12 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 			const V3 ty = cross(normal, tx);
 			excident = (d.x * tx + d.y * ty) + d.z * normal;
 			sThroughput = intensity * PI;
+		} else if(kind == LV_ENV) {
+			// path_util.hpp:312-320: a start point on the scene box, travelling along the photon's direction
+			float pdf;
+			start = sample_position(S.aabb, normal, ru0, ru1, pdf);
+			excident = normal;
+			sThroughput = intensity / pdf;
 		} else {
 			const PathSample smp = material_sample(ts, mat, decode_incident(incEnc), ru0, ru1, x1, true);
 			if(!smp.valid) break;
@@ -2170,7 +2230,7 @@ void lt_sample(const LtState& st, u32 photon, u32 numPhotons, Pcg64& rng, i32* r
 		if(rr >= cp) break;
 		throughput = throughput / cp;
 		const V3 geoN = kind == LV_SURFACE ? ts.geoN : (kind == LV_AREA ? normal : V3{ 0, 0, 0 });
-		V3 origin = position;
+		V3 origin = start;
 		const Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt);
 		if(hit.inst < 0) break;
 		position = origin + excident * hit.distance;
@@ -2624,8 +2684,6 @@ int oracle_pt_stats(void* p, OrStats* o) {
 
 void* oracle_lt_create(void* s, const OrLtParams* params) {
 	Scene* S = static_cast<Scene*>(s);
-	const LightTree& T = S->lightTree;
-	if((T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z > 0.0f) return nullptr; // no photons from the environment
 	auto* st = new LtState();
 	st->scene = S;
 	st->params = *params;

@@ -140,8 +140,7 @@ typedef struct {
 	int32_t maxPathLength;
 	int32_t density;        /* the Density target is enabled (it changes which connections are tested) */
 } OrLtParams;
-/* NULL for scenes with environment light (photons are emitted from point,
- * triangle and quad lights only). */
+/* Photons leave point, triangle and quad lights and the colored background. */
 void* oracle_lt_create(void* scene, const OrLtParams* params);
 void oracle_lt_destroy(void* lt);
 int oracle_lt_iterate(void* lt, int32_t numThreads);

@@ -315,7 +315,7 @@ class OracleLightTracer:
         p = OrLtParams(seed, min_path, max_path, 1 if density else 0)
         self.handle = lib().oracle_lt_create(scene.handle, C.byref(p))
         if not self.handle:
-            raise ValueError("the light tracer does not emit photons from environment light")
+            raise ValueError("oracle_lt_create failed")
 
     def iterate(self, threads: int = 0):
         if threads <= 0:

@@ -3,12 +3,12 @@
 
 Every camera connection of an iteration is recorded per photon and path
 length (pixel and added radiance, lightness, density) and compared bit for
-bit: emission from point, triangle and quad lights picked through the light
-tree, the camera projection, adjoint BSDF evaluation and sampling of Lambert
+bit: emission from point, triangle and quad lights and the colored
+background picked through the light tree, the camera projection, adjoint BSDF evaluation and sampling of Lambert
 and both Torrance shadowing models, the walk through single- and
 multi-level hierarchies and the generator stream across iterations. The
 images differ only in the order the atomics add the same terms: relative
-RMSE within 1e-5. The renderer registry and the refusals are checked too."""
+RMSE within 1e-5. The renderer registry and the target checks are tested too."""
 import dataclasses
 
 import numpy as np
@@ -42,6 +42,8 @@ CASES = {
     "icosphere_smith": lambda: _glossy_icosphere(1),
     "icosphere_vcavity": lambda: _glossy_icosphere(0),
     "instanced": _instanced,
+    # a colored background next to a point light: photons from the environment too
+    "icosphere_env": lambda: scenes.displaced_icosphere(2, subdiv=4, width=64, height=36),
 }
 
 
@@ -145,18 +147,6 @@ def test_lt_and_pt_keep_separate_parameters():
         assert d.renderer_get_parameter_int("Seed") == 0
         assert d.render_enable_renderer(1, 0)
         assert d.renderer_get_parameter_int("Seed") == 77
-    finally:
-        d.close()
-
-
-def test_environment_light_is_refused():
-    spec = scenes.displaced_icosphere(1, subdiv=2, width=16, height=16)
-    d = bindings.DllInterface()
-    try:
-        bindings.load_scene_spec(d, spec)
-        assert d.render_enable_renderer(1, 0)
-        with pytest.raises(bindings.MufflonError, match="environment light"):
-            d.render_iterate()
     finally:
         d.close()
 

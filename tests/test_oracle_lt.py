@@ -8,7 +8,8 @@
   against an independent estimator.
 * The connection records and the image agree: the first iteration's
   radiance is the records added per pixel in photon order.
-* Scenes with environment light are refused.
+* Photons from the environment light estimate the same image as the path
+  tracer's background hits and next-event estimation.
 """
 import dataclasses
 
@@ -77,12 +78,21 @@ def test_point_lights_are_seen_by_the_light_tracer_only(oracle):
     lt.close(); pt.close(); S.close()
 
 
-def test_environment_light_is_refused(oracle):
-    spec = scenes.displaced_icosphere(1, subdiv=2, width=16, height=16)
-    assert spec.background is not None
+def test_environment_photons_match_the_path_tracer(oracle):
+    """With a colored background, photons also leave the environment
+    (light_sampling.hpp:292-306): at path length 1 they show the background
+    itself, at length 2 the ground lit by it; both estimates agree with the
+    path tracer's."""
+    spec = dataclasses.replace(scenes.emissive_panels(5, 0, 0, 0, width=48, height=32),
+                               background=((0.3, 0.4, 0.5), (1.0, 1.0, 1.0)))
     S = oracle.OracleScene(spec)
-    with pytest.raises(ValueError, match="environment"):
-        oracle.OracleLightTracer(S)
-    ok = oracle.OracleLightTracer(oracle.OracleScene(dataclasses.replace(spec, background=None)))
-    ok.iterate()
+    for path_len in (1, 2):
+        lt = oracle.OracleLightTracer(S, seed=3, min_path=path_len, max_path=path_len)
+        pt = oracle.OraclePathTracer(S, seed=5, min_path=path_len, max_path=path_len)
+        for _ in range(300):
+            lt.iterate()
+            pt.iterate()
+        ma, mb = lt.target("Radiance").mean(axis=(0, 1)), pt.target("Radiance").mean(axis=(0, 1))
+        assert np.all(mb > 0.0) and np.all(np.abs(ma - mb) <= 0.03 * mb), (path_len, ma, mb)
+        lt.close(); pt.close()
     S.close()
