@@ -521,8 +521,10 @@ class DllInterface:
         return self.core.instance_set_transformation_matrix(self.muffInst, instHdl, byref(mat), int(isWorldToInst)) != 0
 
     # -- image readback
-    def get_target_image(self, targetName: str) -> np.ndarray:
-        """Cumulative mean of a target as (height, width, channels) float32, y = 0 first."""
+    def get_target_image(self, targetName: str, copy: bool = True) -> np.ndarray:
+        """Cumulative mean of a target as (height, width, channels) float32, y = 0 first. With
+        copy=False the array is a view of the library's page-locked read-back buffer, valid until the
+        next call of this function (the C API's ownership rule)."""
         p = POINTER(c_float)()
         self._check(self.core.mufflon_get_target_image(self.muffInst, targetName.encode(), 0, byref(p)),
                     "mufflon_get_target_image")
@@ -531,7 +533,8 @@ class DllInterface:
         if not p:
             return None
         w, h = self.current_resolution()
-        return np.ctypeslib.as_array(p, shape=(h * w * ch.value,)).reshape(h, w, ch.value).copy()
+        view = np.ctypeslib.as_array(p, shape=(h * w * ch.value,)).reshape(h, w, ch.value)
+        return view.copy() if copy else view
 
     def current_resolution(self):
         """(width, height) of the loaded scenario."""

@@ -243,6 +243,8 @@ void RendererState::release() {
 	cudaFree(ltRecPixel); cudaFree(ltRecValue);
 	ltIter = nullptr; ltIterDensity = nullptr; lightness = nullptr; density = nullptr;
 	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0;
+	if(screen) cudaFreeHost(screen);
+	screen = nullptr; screenCap = 0;
 	if(evStart) cudaEventDestroy(evStart);
 	if(evStop) cudaEventDestroy(evStop);
 	rng = nullptr; radiance = nullptr; hitId = nullptr; workCounter = nullptr; counters = nullptr;
@@ -313,6 +315,20 @@ Boolean mufflon_set_lod_loader(MufflonInstanceHdl h, Boolean (*func)(void*, Obje
 	CATCH_ALL(false)
 }
 
+// The page-locked read-back buffer of mufflon_get_target_image (grow-only:
+// a device-to-host copy into page-locked memory runs at the link's speed,
+// into pageable memory it is staged through a driver buffer).
+static float* screen_buffer(RendererState& r, size_t floats) {
+	if(floats > r.screenCap) {
+		if(r.screen) cudaFreeHost(r.screen);
+		r.screen = nullptr;
+		r.screenCap = 0;
+		CHECK_CUDA(cudaMallocHost(&r.screen, floats * sizeof(float)));
+		r.screenCap = floats;
+	}
+	return r.screen;
+}
+
 // interface.cpp:241-262: a library-owned copy of the cumulative target
 Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean variance, const float** ptr) {
 	TRY
@@ -326,28 +342,25 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 	const size_t n = size_t(r.width) * r.height;
 	if(!std::strcmp(name, "Radiance")) {
 		CHECK(r.targetRadiance, "target 'Radiance' is not enabled");
-		r.screen.resize(n * 3);
-		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 3;
 	} else if(r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) {
 		const bool light = !std::strcmp(name, "Lightness");
 		CHECK(light ? r.targetLightness : r.targetDensity, std::string("target '") + name + "' is not enabled");
 		const float* src = light ? r.lightness : r.density;
 		CHECK(src != nullptr, "no image yet");
-		r.screen.resize(n);
-		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n), src, n * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 1;
 	} else if(r.kind == 0 && !std::strcmp(name, "Hit ID")) {
 		CHECK(r.targetHitId, "target 'Hit ID' is not enabled");
-		r.screen.resize(n * 2);
-		CHECK_CUDA(cudaMemcpyAsync(r.screen.data(), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 2), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 2;
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
 		               (r.kind == 1 ? "light tracer" : "path tracer"));
 	}
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
-	if(ptr) *ptr = r.screen.data();
+	if(ptr) *ptr = r.screen;
 	return true;
 	CATCH_ALL(false)
 }

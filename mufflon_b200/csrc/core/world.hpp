@@ -249,7 +249,8 @@ struct RendererState {
 	cudaEvent_t evStart = nullptr, evStop = nullptr;
 	TraceCounters lastCounters{};
 	float lastKernelMs = 0.0f;
-	std::vector<float> screen;
+	float* screen = nullptr;       // page-locked copy of the last target read back (library-owned)
+	size_t screenCap = 0;          // its capacity in floats
 	int screenChannels = 0;
 	void release();
 };
