@@ -51,10 +51,10 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt", "bpt"],
                    help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one; "
                         "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
-                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p")
+                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p")
     p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
@@ -725,6 +725,66 @@ def run_lt(args):
     print(json.dumps(line), flush=True)
 
 
+def run_bpt(args):
+    """The bidirectional path tracer ("Bidirectional Pathtracer", bpt.cu) on
+    the headline scene (1080p icosphere, point light, colored background):
+    16 iterations of one light and one view subpath per pixel per step, path
+    length up to 10. Device time from CUDA events; rays = subpath segments +
+    connection shadow rays. The CPU baseline is one iteration of the oracle's
+    bidirectional path tracer on all host cores at 480 x 270 (the same scene
+    and camera)."""
+    import dataclasses
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import bindings, build, scenes
+    build.build()
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    d = bindings.DllInterface()
+    bindings.load_scene_spec(d, spec)
+    assert d.render_enable_renderer(2, 0)
+    assert d.renderer_set_parameter_int("Max. path length", MAX_PATH)
+    d.render_enable_render_target("Radiance", False)
+    iters = SPP_PER_FRAME
+    for _ in range(args.warmup * iters):
+        d.render_iterate()
+    torch.cuda.synchronize()
+    ms = rays = shadow = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps * iters):
+        d.render_iterate()
+        st = d.render_stats()
+        ms += st["kernelMs"]; rays += st["rays"]; shadow += st["shadowRays"]
+        if st["errors"]:
+            raise RuntimeError(f"traversal errors reported: {st['errors']}")
+    wall = time.perf_counter() - t0
+    img = d.get_target_image("Radiance")
+    d.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle
+        threads = os.cpu_count() or 1
+        small = dataclasses.replace(spec, width=WIDTH // 4, height=HEIGHT // 4)
+        ob = pyoracle.OracleBidirPathTracer(pyoracle.OracleScene(small), seed=0, max_path=MAX_PATH)
+        t1 = time.perf_counter()
+        ob.iterate(threads)
+        el = time.perf_counter() - t1
+        r = ob.stats()["rays"]
+        cpu = {"value": round(r / el / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+               "sample": f"one iteration at {small.width}x{small.height}: {r} rays, {el:.1f} s"}
+    line = {"metric": "bidirectional path tracer Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+            "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
+            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_1920x1080_bpt_16it_depth{MAX_PATH}",
+                       "samples_per_step": iters * WIDTH * HEIGHT,
+                       "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
+            "samples_per_s": round(args.steps * iters * WIDTH * HEIGHT / (ms / 1e3), 1),
+            "rays_per_step": int(rays / args.steps), "shadow_rays_per_step": int(shadow / args.steps),
+            "e2e": {"value": round(rays / wall / 1e6, 2), "unit": "Mrays/s", "note": "wall clock around render_iterate + stats"},
+            "image_mean": [round(float(x), 5) for x in img.reshape(-1, 3).mean(0)],
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def dataclasses_replace_texture(spec, tex3):
     import dataclasses
     t = np.ones(tex3.shape[:2] + (4,), np.float32)
@@ -748,6 +808,9 @@ def main():
         return
     if args.workload == "lt":
         run_lt(args)
+        return
+    if args.workload == "bpt":
+        run_bpt(args)
         return
     if args.impl == "reference":
         run_reference(args)

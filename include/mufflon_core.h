@@ -310,12 +310,16 @@ typedef struct {
 } MufflonStageStats;
 CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
 
-/* EXTENSION with no counterpart in the reference: the camera connections of
- * the light tracer's last iteration, kept while its integer parameter
- * "Record connections" is non-zero. slots = width * height * "Max. path
- * length" (photon major, then the photon's path length at the connection);
- * pixels[k] receives the pixel index the connection added to, or -1, and
- * values[5k..5k+4] the radiance rgb, lightness and density it added. */
+/* EXTENSION with no counterpart in the reference: the contributions of the
+ * last iteration of the light tracer or the bidirectional path tracer, kept
+ * while the renderer's integer parameter "Record connections" is non-zero.
+ * pixels[k] receives the pixel index a contribution was added to, or -1.
+ * Light tracer: slots = width * height * M (M = "Max. path length"; photon
+ * major, then the photon's path length at the camera connection) and
+ * values[5k..5k+4] = radiance rgb, lightness, density. Bidirectional path
+ * tracer: slots = width * height * (M * M + M) (pixel major; first the
+ * connections [view path length][light vertex], then the emitter hits [view
+ * path length - 1]) and values[4k..4k+3] = radiance rgb, lightness. */
 CORE_API Boolean CDECL mufflon_get_lt_records(MufflonInstanceHdl instHdl, int32_t* pixels, float* values,
                                               uint64_t slots);
 

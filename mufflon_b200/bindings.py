@@ -567,6 +567,18 @@ class DllInterface:
         self._check(self.core.mufflon_get_lt_records(self.muffInst, _ptr(pix), _ptr(val), n), "mufflon_get_lt_records")
         return pix, val
 
+    def bpt_records(self, max_path_length: int):
+        """The bidirectional path tracer's contributions of the last iteration (integer parameter
+        "Record connections" set): per pixel M*M connection slots [view length][light vertex], then M
+        emitter-hit slots (M = max. path length); pixel index (-1: none) and (radiance rgb, lightness)."""
+        w, h = self.current_resolution()
+        m = max(1, max_path_length)
+        n = w * h * (m * m + m)
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 4), np.float32)
+        self._check(self.core.mufflon_get_lt_records(self.muffInst, _ptr(pix), _ptr(val), n), "mufflon_get_lt_records")
+        return pix, val
+
     def light_tree(self):
         """The GPU-built light list and tree: (lights (n, 108) uint8, nodes (m, 20) uint8,
         area-light keys uint64, codes uint32, root flux); layout in include/mufflon_core.h."""

@@ -27,7 +27,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/wide.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu",
-              "core/light_build.cu", "core/instance_boxes.cu", "trace/lt.cu"]
+              "core/light_build.cu", "core/instance_boxes.cu", "trace/lt.cu",
+              "trace/bpt.cu"]
 CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
 # the scene-file loader: its own library on top of the core's C API
 LOADER_SOURCES = ["loader/json.cpp", "loader/mff_binary.cpp", "loader/scene_loader.cpp", "loader/interface.cpp"]
@@ -35,7 +36,8 @@ LOADER_HEADERS = ["loader/json.hpp", "loader/mff_binary.hpp", "loader/scene_load
 HEADERS = ["common/fmath.hpp", "trace/dmath.cuh", "trace/intersect.cuh", "trace/shading.cuh",
            "trace/scene_types.hpp", "trace/pt_api.hpp", "lbvh/lbvh.hpp", "lbvh/radix_sort.cuh",
            "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "trace/wide_traverse.cuh", "lbvh/wide.hpp", "core/world.hpp",
-           "core/light_build.hpp", "core/instance_boxes.hpp", "trace/lt_api.hpp"]
+           "core/light_build.hpp", "core/instance_boxes.hpp", "trace/lt_api.hpp",
+           "trace/emit.cuh"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-Xptxas", "-v",

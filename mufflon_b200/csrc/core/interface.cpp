@@ -67,15 +67,17 @@ const ParamDesc LT_PARAMS[] = {
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
 const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
-// Render targets of the light tracer (lt_params.hpp:14-17), all implemented.
+// Render targets of the light tracer (lt_params.hpp:14-17) and of the
+// bidirectional path tracer (bpt_params.hpp:14-17, its first two), all implemented.
 const char* LT_TARGETS[] = { "Radiance", "Lightness", "Density" };
 
 int32_t* param_ptr(RendererState& r, const char* name) {
-	if(r.kind == 1) {
-		if(!std::strcmp(name, "Seed")) return &r.ltParams.seed;
-		if(!std::strcmp(name, "Min. path length")) return &r.ltParams.minPathLength;
-		if(!std::strcmp(name, "Max. path length")) return &r.ltParams.maxPathLength;
-		if(!std::strcmp(name, "Record connections")) return &r.ltRecord;
+	if(r.kind == 1 || r.kind == 2) {
+		LtParams& p = r.kind == 1 ? r.ltParams : r.bptParams;
+		if(!std::strcmp(name, "Seed")) return &p.seed;
+		if(!std::strcmp(name, "Min. path length")) return &p.minPathLength;
+		if(!std::strcmp(name, "Max. path length")) return &p.maxPathLength;
+		if(!std::strcmp(name, "Record connections")) return r.kind == 1 ? &r.ltRecord : &r.bptRecord;
 		return nullptr;
 	}
 	if(!std::strcmp(name, "Seed")) return &r.params.seed;
@@ -148,22 +150,39 @@ void ensure_lt_buffers(MufflonInstance& I) {
 		CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, n * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.density, 0, n * sizeof(float), I.stream));
 	}
-	const size_t slots = r.ltRecord ? n * size_t(std::max(1, r.ltParams.maxPathLength)) : 0;
-	if(slots != r.ltRecSlots) {
+	// records: light tracer M slots of 5 floats per photon, bidirectional
+	// path tracer M*M + M slots of 4 floats per pixel (M = max. path length)
+	const size_t m = size_t(std::max(1, r.kind == 2 ? r.bptParams.maxPathLength : r.ltParams.maxPathLength));
+	const bool record = r.kind == 2 ? r.bptRecord != 0 : r.ltRecord != 0;
+	const size_t slots = record ? (r.kind == 2 ? n * (m * m + m) : n * m) : 0;
+	const size_t floats = slots * (r.kind == 2 ? 4 : 5);
+	if(slots != r.ltRecSlots || floats != r.ltRecFloats) {
 		cudaFree(r.ltRecPixel); cudaFree(r.ltRecValue);
-		r.ltRecPixel = nullptr; r.ltRecValue = nullptr; r.ltRecSlots = 0;
+		r.ltRecPixel = nullptr; r.ltRecValue = nullptr; r.ltRecSlots = 0; r.ltRecFloats = 0;
 		if(slots) {
 			CHECK_CUDA(cudaMalloc(&r.ltRecPixel, slots * sizeof(int32_t)));
-			CHECK_CUDA(cudaMalloc(&r.ltRecValue, slots * 5 * sizeof(float)));
+			CHECK_CUDA(cudaMalloc(&r.ltRecValue, floats * sizeof(float)));
 			CHECK_CUDA(cudaMemsetAsync(r.ltRecPixel, 0xFF, slots * sizeof(int32_t), I.stream));
-			CHECK_CUDA(cudaMemsetAsync(r.ltRecValue, 0, slots * 5 * sizeof(float), I.stream));
+			CHECK_CUDA(cudaMemsetAsync(r.ltRecValue, 0, floats * sizeof(float), I.stream));
 			r.ltRecSlots = slots;
+			r.ltRecFloats = floats;
+		}
+	}
+	if(r.kind == 2) {
+		const size_t bytes = bpt_scratch_bytes(r.bptParams.maxPathLength);
+		if(bytes > r.bptScratchBytes) {
+			cudaFree(r.bptScratch);
+			r.bptScratch = nullptr;
+			r.bptScratchBytes = 0;
+			CHECK_CUDA(cudaMalloc(&r.bptScratch, bytes));
+			r.bptScratchBytes = bytes;
 		}
 	}
 }
 
 // One light-tracing iteration (gpu_lt.cpp / lt_common.hpp): width * height
-// photons, each walk's vertices connected to the camera.
+// photons, each walk's vertices connected to the camera; or one
+// bidirectional path-tracing iteration (cpu_bpt.cpp), into the same buffers.
 void iterate_lt(MufflonInstance& I) {
 	RendererState& r = I.renderer;
 	const DScene& S = I.scene.desc;
@@ -180,7 +199,10 @@ void iterate_lt(MufflonInstance& I) {
 	t.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
-	CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
+	if(r.kind == 2) {
+		t.density = nullptr;
+		CHECK_CUDA(launch_bpt(S, r.bptParams, t, r.bptScratch, r.workCounter, r.counters, I.stream));
+	} else CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters c{};
 	CHECK_CUDA(cudaMemcpyAsync(&c, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
@@ -242,7 +264,9 @@ void RendererState::release() {
 	cudaFree(ltIter); cudaFree(ltIterDensity); cudaFree(lightness); cudaFree(density);
 	cudaFree(ltRecPixel); cudaFree(ltRecValue);
 	ltIter = nullptr; ltIterDensity = nullptr; lightness = nullptr; density = nullptr;
-	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0;
+	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0; ltRecFloats = 0;
+	cudaFree(bptScratch);
+	bptScratch = nullptr; bptScratchBytes = 0;
 	if(screen) cudaFreeHost(screen);
 	screen = nullptr; screenCap = 0;
 	if(evStart) cudaEventDestroy(evStart);
@@ -344,7 +368,8 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 		CHECK(r.targetRadiance, "target 'Radiance' is not enabled");
 		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 3;
-	} else if(r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) {
+	} else if((r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) ||
+	          (r.kind == 2 && !std::strcmp(name, "Lightness"))) {
 		const bool light = !std::strcmp(name, "Lightness");
 		CHECK(light ? r.targetLightness : r.targetDensity, std::string("target '") + name + "' is not enabled");
 		const float* src = light ? r.lightness : r.density;
@@ -357,7 +382,7 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 		r.screenChannels = 2;
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
-		               (r.kind == 1 ? "light tracer" : "path tracer"));
+		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "bidirectional path tracer" : "path tracer"));
 	}
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	if(ptr) *ptr = r.screen;
@@ -999,27 +1024,29 @@ Boolean world_set_env_light_scale(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
 
 // ---------------------------------------------------------------- renderers
 // Renderers grouped by name in the reference's registry order (renderers.hpp:23-31,
-// interface.cpp:126-154): the path tracer, then the light tracer, each with its
-// CUDA variation.
-const char* RENDERER_NAMES[2][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" } };
-uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return 2u; CATCH_ALL(0u) }
+// interface.cpp:126-154): the path tracer, the light tracer and the
+// bidirectional path tracer (CPU-only in the reference), each with a CUDA
+// variation; the wireframe renderers between them are not provided.
+const char* RENDERER_NAMES[3][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" }, { "Bidirectional Pathtracer", "BPT" } };
+constexpr uint32_t NUM_RENDERERS = 3u;
+uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return NUM_RENDERERS; CATCH_ALL(0u) }
 uint32_t render_get_renderer_variations(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
+	TRY (void)minst(h); CHECK(index < NUM_RENDERERS, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
 }
 const char* render_get_renderer_name(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return RENDERER_NAMES[index][0]; CATCH_ALL(nullptr)
+	TRY (void)minst(h); CHECK(index < NUM_RENDERERS, "renderer index out of bounds"); return RENDERER_NAMES[index][0]; CATCH_ALL(nullptr)
 }
 const char* render_get_renderer_short_name(MufflonInstanceHdl h, uint32_t index) {
-	TRY (void)minst(h); CHECK(index < 2, "renderer index out of bounds"); return RENDERER_NAMES[index][1]; CATCH_ALL(nullptr)
+	TRY (void)minst(h); CHECK(index < NUM_RENDERERS, "renderer index out of bounds"); return RENDERER_NAMES[index][1]; CATCH_ALL(nullptr)
 }
 RenderDevice render_get_renderer_devices(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
-	TRY (void)minst(h); CHECK(index < 2 && variation == 0, "renderer index out of bounds"); return DEVICE_CUDA; CATCH_ALL(DEVICE_NONE)
+	TRY (void)minst(h); CHECK(index < NUM_RENDERERS && variation == 0, "renderer index out of bounds"); return DEVICE_CUDA; CATCH_ALL(DEVICE_NONE)
 }
 Boolean render_enable_renderer(MufflonInstanceHdl h, uint32_t index, uint32_t variation) {
 	TRY
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
-	CHECK(index < 2 && variation == 0, "renderer index out of bounds");
+	CHECK(index < NUM_RENDERERS && variation == 0, "renderer index out of bounds");
 	I.renderer.enabled = true;
 	I.renderer.kind = int32_t(index);
 	I.renderer.needsReset = true;
@@ -1040,10 +1067,11 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	ensure_render_buffers(I);
 	RendererState& r = I.renderer;
 	const uint32_t n = r.width * r.height;
-	if(r.kind == 1) ensure_lt_buffers(I);
+	if(r.kind != 0) ensure_lt_buffers(I);
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
-		CHECK_CUDA(launch_seed_rng(r.rng, n, r.kind == 1 ? r.ltParams.seed : r.params.seed, I.stream));
+		const int32_t seed = r.kind == 1 ? r.ltParams.seed : r.kind == 2 ? r.bptParams.seed : r.params.seed;
+		CHECK_CUDA(launch_seed_rng(r.rng, n, seed, I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.radiance, 0, size_t(n) * 3 * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
 		if(r.lightness) CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, size_t(n) * sizeof(float), I.stream));
@@ -1054,7 +1082,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 		++r.iteration;
 	}
 	auto t1 = clk::now();
-	if(r.kind == 1) {
+	if(r.kind != 0) {
 		iterate_lt(I);
 		auto t2 = clk::now();
 		auto us = [](clk::duration d) { return uint64_t(std::chrono::duration_cast<std::chrono::microseconds>(d).count()); };
@@ -1217,12 +1245,13 @@ Boolean render_save_screenshot(MufflonInstanceHdl h, const char* filename, const
 	CATCH_ALL(false)
 }
 
-uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY return minst(h).renderer.kind == 1 ? 3u : 8u; CATCH_ALL(0u) }
+static uint32_t target_count(int32_t kind) { return kind == 1 ? 3u : kind == 2 ? 2u : 8u; }
+uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY return target_count(minst(h).renderer.kind); CATCH_ALL(0u) }
 const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) {
 	TRY
-	const bool lt = minst(h).renderer.kind == 1;
-	CHECK(index < (lt ? 3u : 8u), "render target index out of bounds");
-	return lt ? LT_TARGETS[index] : TARGETS[index];
+	const int32_t kind = minst(h).renderer.kind;
+	CHECK(index < target_count(kind), "render target index out of bounds");
+	return kind != 0 ? LT_TARGETS[index] : TARGETS[index];
 	CATCH_ALL(nullptr)
 }
 Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
@@ -1267,13 +1296,13 @@ Boolean render_is_render_target_enabled(MufflonInstanceHdl h, const char* name, 
 
 uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) {
 	TRY
-	const bool lt = minst(h).renderer.kind == 1;
+	const bool lt = minst(h).renderer.kind != 0;
 	return lt ? uint32_t(sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0])) : uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]));
 	CATCH_ALL(0u)
 }
 const char* renderer_get_parameter_desc(MufflonInstanceHdl h, uint32_t idx, ParameterType* type) {
 	TRY
-	const bool lt = minst(h).renderer.kind == 1;
+	const bool lt = minst(h).renderer.kind != 0;
 	const ParamDesc* table = lt ? LT_PARAMS : PT_PARAMS;
 	const size_t count = lt ? sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0]) : sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]);
 	CHECK(idx < count, "parameter index out of bounds");
@@ -1369,10 +1398,10 @@ Boolean mufflon_get_lt_records(MufflonInstanceHdl h, int32_t* pixels, float* val
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	const RendererState& r = I.renderer;
-	CHECK(r.kind == 1 && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer iteration");
-	CHECK(pixels && values && slots == r.ltRecSlots, "the record buffers must hold width * height * max. path length slots");
+	CHECK(r.kind != 0 && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer or bidirectional iteration");
+	CHECK(pixels && values && slots == r.ltRecSlots, "the record buffers must hold the renderer's number of slots");
 	CHECK_CUDA(cudaMemcpyAsync(pixels, r.ltRecPixel, slots * sizeof(int32_t), cudaMemcpyDeviceToHost, I.stream));
-	CHECK_CUDA(cudaMemcpyAsync(values, r.ltRecValue, slots * 5 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+	CHECK_CUDA(cudaMemcpyAsync(values, r.ltRecValue, r.ltRecFloats * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	return true;
 	CATCH_ALL(false)

@@ -228,9 +228,14 @@ struct RendererState {
 	bool targetHitId = false;
 	bool targetLightness = false;  // light tracer targets (lt_params.hpp:14-17)
 	bool targetDensity = false;
-	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer" (renderer registry order)
+	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer", 2: "Bidirectional Pathtracer"
 	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
 	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
+	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters
+	int32_t bptRecord = 0;         // keep its contributions of the last iteration
+	void* bptScratch = nullptr;    // its per-lane light subpaths
+	size_t bptScratchBytes = 0;
+	size_t ltRecFloats = 0;        // floats allocated at ltRecValue
 	float4* ltIter = nullptr;      // light tracer iteration buffers (radiance rgb + lightness, density)
 	float* ltIterDensity = nullptr;
 	float* lightness = nullptr;    // cumulative means of the 1-channel light tracer targets

@@ -35,4 +35,15 @@ struct LtTargets {
 cudaError_t launch_lt(const DScene& scene, const LtParams& params, const LtTargets& targets,
                       unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
 
+// Bytes of the bidirectional path tracer's per-lane light-subpath storage
+// (one slice of max. path length vertices per resident thread).
+size_t bpt_scratch_bytes(int maxPathLength);
+
+// One bidirectional path-tracing iteration (one light and one view subpath
+// per pixel) into the same targets as the light tracer (radiance and
+// lightness; no density); records hold 4 floats per slot, M*M + M slots per
+// pixel for maximum path length M.
+cudaError_t launch_bpt(const DScene& scene, const LtParams& params, const LtTargets& targets, void* scratch,
+                       unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
+
 } // namespace mb

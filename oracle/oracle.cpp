@@ -1955,7 +1955,7 @@ enum LtKind { LV_POINT, LV_AREA, LV_SURFACE, LV_ENV };
 // (light_tree_sampling.hpp:12-16) and, for an area light, its normal; for
 // the environment, the direction the photon travels (in `normal`) and the
 // irradiance.
-struct Emitter { V3 position, intensity, normal; LtKind kind; bool valid; };
+struct Emitter { V3 position, intensity, normal; LtKind kind; bool valid; float pChoice, pdf; };
 
 // A vector perpendicular to n (not normalised): n crossed with the coordinate
 // axis of n's smallest component. The reference takes `perpendicular` from
@@ -1978,6 +1978,8 @@ Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, 
 		e.intensity = l.intensity / lightProb;
 		e.normal = { 0, 0, 0 };
 		e.kind = LV_POINT;
+		e.pChoice = lightProb;
+		e.pdf = INF_PDF;
 		return e;
 	}
 	const Material& m = S.materials[l.material];
@@ -2004,6 +2006,8 @@ Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, 
 	e.intensity = (radiance * area) / lightProb;
 	e.normal = normal;
 	e.kind = LV_AREA;
+	e.pChoice = lightProb;
+	e.pdf = 1.0f / area;
 	return e;
 }
 
@@ -2020,6 +2024,8 @@ Emitter sample_background(const LightTree& T, float u0, float u1, float envProb)
 	e.position = { 0, 0, 0 };
 	e.normal = -dir;
 	e.intensity = irradiance / envProb;
+	e.pChoice = envProb;
+	e.pdf = dirPdf;
 	return e;
 }
 
@@ -2275,6 +2281,374 @@ void lt_iterate(LtState& st, int numThreads) {
 		for(int c = 0; c < 3; ++c) { float& cr = st.radiance[3 * p + size_t(c)]; const float diff = iter[5 * p + size_t(c)] - cr; cr += diff / den; }
 		{ float& cl = st.lightness[p]; const float diff = iter[5 * p + 3] - cl; cl += diff / den; }
 		{ float& cd = st.density[p]; const float diff = iter[5 * p + 4] - cd; cd += diff / den; }
+	}
+}
+
+// ---------------------------------------------------------------- bidirectional path tracer
+// cpu_bpt.cpp:1-247 with the vertex machinery of path_util.hpp it uses. A
+// vertex keeps what the reference's PathVertex<BptVertexExt> keeps: its kind,
+// position, encoded incident direction (surfaces: x, y of the direction and
+// the distance with the sign of z; a miss: the direction; an area light: its
+// normal; a point light: its intensity; the environment: the photon's
+// direction), surface data, and the MIS extension (incident area pdf, cached
+// sum of relative probabilities of the earlier events, subpath throughput).
+enum BKind { BV_VIRTUAL, BV_CAMERA, BV_SURFACE, BV_VOID, BV_POINT, BV_AREA, BV_ENV };
+
+struct BVertex {
+	BKind kind;
+	V3 position;
+	V3 incEnc;
+	V3 intensity;       // area light intensity / environment irradiance
+	float projSceneArea; // environment
+	TangentSpace ts;
+	Params mat;
+	i32 inst, prim;
+	V2 sp;
+	i32 prev;           // index of the previous vertex in its subpath, or -1
+	float incidentPdf;  // BptVertexExt::incidentPdf
+	float prevRelSum;   // BptVertexExt::prevRelativeProbabilitySum
+	V3 throughput;      // BptVertexExt::throughput
+};
+
+inline bool bv_ortho(BKind k) { return k == BV_VOID || k == BV_ENV; }           // path_util.hpp:41-46
+inline bool bv_camera(BKind k) { return k == BV_CAMERA; }
+inline bool bv_end(BKind k) { return k != BV_SURFACE; }                          // path_util.hpp:33-35
+
+// path_util.hpp:160-176
+inline float bv_geo_factor(const BVertex& v, V3 dir) {
+	if(v.kind == BV_AREA) return dot(dir, v.incEnc);
+	if(v.kind == BV_SURFACE) return dot(dir, v.ts.shadingN);
+	if(v.kind == BV_ENV || v.kind == BV_VOID) return 1.0f;
+	return 0.0f;
+}
+inline V3 bv_geo_normal(const BVertex& v) {
+	if(v.kind == BV_AREA) return v.incEnc;
+	if(v.kind == BV_SURFACE) return v.ts.geoN;
+	return { 0, 0, 0 };
+}
+inline V3 bv_incident_dir(const BVertex& v) { return decode_incident(v.incEnc); }
+inline float bv_incident_dist_sq(const BVertex& v) { return bv_end(v.kind) ? 0.0f : v.incEnc.z * v.incEnc.z; }
+// path_util.hpp:130-137
+inline V3 bv_position(const BVertex& v, V3 ref) {
+	if(v.kind == BV_ENV) return ref - bv_incident_dir(v) * MAX_SCENE_SIZE;
+	return v.position;
+}
+// path_util.hpp:208-221: a sampling pdf converted into an area pdf at v
+inline float bv_convert_pdf(const BVertex& v, BKind source, float samplePdf, V3 dir, float distSq) {
+	if(source == BV_VIRTUAL) return samplePdf;
+	const float geo = bv_geo_factor(v, dir);
+	if(bv_ortho(source) || bv_ortho(v.kind)) return samplePdf * std::fabs(geo);
+	return samplePdf * std::fabs(geo) / distSq;
+}
+
+// path_util.hpp:245-293: value, cosine and pdfs of leaving v along excident;
+// a camera also yields the pixel (-1 off the image)
+EvalValue bv_evaluate(const Scene& S, const BVertex& v, V3 excident, bool adjoint, i32& px, i32& py) {
+	EvalValue none = { { 0, 0, 0 }, 0, 0, 0 };
+	switch(v.kind) {
+		case BV_POINT: return { v.incEnc, 1.0f, 1.0f / (4.0f * PI), 0.0f };
+		case BV_AREA: {
+			const float cosOut = dot(v.incEnc, excident);
+			if(cosOut <= 0.0f) return none;
+			return { v.intensity, cosOut, cosOut / PI, 0.0f };
+		}
+		case BV_ENV: return { v.intensity, 1.0f, 1.0f / v.projSceneArea, 0.0f };
+		case BV_CAMERA: {
+			float w = 0.0f;
+			if(!pinhole_project(S.cam, excident, px, py, w)) { px = -1; py = -1; return { { 0, 0, 0 }, 1.0f, 0.0f, 0.0f }; }
+			return { { w, w, w }, 1.0f, w, 0.0f };
+		}
+		case BV_SURFACE: return material_evaluate(v.ts, v.mat, bv_incident_dir(v), excident, adjoint);
+		default: return none;
+	}
+}
+
+// cpu_bpt.cpp:68-88
+float bpt_mis_part(const std::vector<BVertex>& path, const BVertex& v, float vertexPdfBack, float nextPdfBack,
+                   BKind nextType, V3 dir, float distSq) {
+	float reversePdf = bv_convert_pdf(v, nextType, nextPdfBack, dir, distSq);
+	const float relPdf = reversePdf / v.incidentPdf;
+	if(v.prev >= 0) {
+		const BVertex& p = path[size_t(v.prev)];
+		reversePdf = bv_convert_pdf(p, v.kind, vertexPdfBack, bv_incident_dir(v), bv_incident_dist_sq(v));
+		const float prevRelPdf = reversePdf / p.incidentPdf;
+		return relPdf + relPdf * (prevRelPdf + prevRelPdf * p.prevRelSum);
+	}
+	return relPdf;
+}
+
+struct BptState {
+	const Scene* scene;
+	OrLtParams params;
+	std::vector<Pcg64> rngs;
+	std::vector<float> radiance, lightness; // cumulative means
+	std::vector<i32> recPixel;               // last iteration, per pixel: connections [view length][light index], then hits [view length]
+	std::vector<float> recValue;             // radiance rgb, lightness as added
+	i32 iteration = -1;
+	Counters stats;
+};
+
+inline size_t bpt_slots(i32 maxPath) { return size_t(maxPath) * size_t(maxPath) + size_t(maxPath); }
+
+// random_walk.hpp:38-113 for a BPT vertex: samples v (updating its MIS
+// extension), applies Russian roulette and traces; out gets the next vertex.
+// Returns 0: cancelled, 1: hit, 2: miss (out is a void vertex).
+int bpt_walk(const Scene& S, std::vector<BVertex>& path, i32 vi, const OrLtParams& P, i32 px, i32 py, Pcg64& rng,
+             bool adjoint, V3& throughput, BVertex& out, Counters& cnt) {
+	BVertex& v = path[size_t(vi)];
+	const u64 x0 = rng.next(), x1 = rng.next();
+	const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
+	const float rr = sample_uniform(u32(rng.next()));
+	(void)P;
+	V3 excident, sThroughput, origin = v.position;
+	float pdfF = 0.0f, pdfB = 0.0f;
+	switch(v.kind) {
+		case BV_POINT:
+			excident = sample_dir_sphere_uniform(ru0, ru1);
+			sThroughput = (v.incEnc * 4.0f) * PI;
+			pdfF = 1.0f / (4.0f * PI);
+			break;
+		case BV_AREA: {
+			float cosT;
+			const V3 d = sample_dir_cosine(ru0, ru1, cosT);
+			const V3 tx = normalize(perpendicular(v.incEnc));
+			const V3 ty = cross(v.incEnc, tx);
+			excident = (d.x * tx + d.y * ty) + d.z * v.incEnc;
+			sThroughput = v.intensity * PI;
+			pdfF = d.z / PI;
+			break;
+		}
+		case BV_ENV: {
+			float pdf;
+			origin = sample_position(S.aabb, v.incEnc, ru0, ru1, pdf);
+			excident = v.incEnc;
+			sThroughput = v.intensity / pdf;
+			pdfF = pdf;
+			break;
+		}
+		case BV_CAMERA:
+			excident = pinhole_ray(S.cam, px, py, ru0, ru1, pdfF);
+			sThroughput = { 1, 1, 1 };
+			break;
+		case BV_SURFACE: {
+			const PathSample smp = material_sample(v.ts, v.mat, bv_incident_dir(v), ru0, ru1, x1, adjoint);
+			if(!smp.valid) { throughput = { 0, 0, 0 }; return 0; }
+			excident = smp.excident;
+			sThroughput = smp.throughput;
+			pdfF = smp.pdfF;
+			pdfB = smp.pdfB;
+			break;
+		}
+		default: return 0;
+	}
+	// BptVertexExt::update after sampling (cpu_bpt.cpp:49-58)
+	if(v.prev >= 0) {
+		const BVertex& p = path[size_t(v.prev)];
+		const float prevReversePdf = bv_convert_pdf(p, v.kind, pdfB, bv_incident_dir(v), bv_incident_dist_sq(v));
+		const float relToPrev = prevReversePdf / p.incidentPdf;
+		v.prevRelSum = relToPrev + relToPrev * p.prevRelSum;
+	}
+	throughput = throughput * sThroughput;
+	const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
+	if(rr >= cp) { throughput = { 0, 0, 0 }; return 0; }
+	throughput = throughput / cp;
+	const Intersection hit = first_intersection(S, origin, excident, bv_geo_normal(v), MAX_SCENE_SIZE, cnt);
+	out = BVertex{};
+	out.prev = vi;
+	out.prevRelSum = 0.0f;
+	out.inst = out.prim = -1;
+	if(hit.inst < 0) {
+		out.kind = BV_VOID;
+		out.position = { 0, 0, 0 };
+		out.incEnc = excident;
+	} else {
+		out.kind = BV_SURFACE;
+		out.position = origin + excident * hit.distance;
+		out.incEnc = { excident.x, excident.y, hit.distance * sgn(excident.z) };
+		out.ts = tangent_space(S, hit);
+		out.inst = hit.inst;
+		out.prim = hit.prim;
+		out.sp = hit.sp;
+		out.mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+	}
+	// BptVertexExt::update after the segment (cpu_bpt.cpp:36-47)
+	const float inCosAbs = std::fabs(bv_geo_factor(out, excident));
+	const bool ortho = bv_ortho(v.kind) || bv_ortho(out.kind);
+	out.incidentPdf = ortho ? pdfF * inCosAbs : pdfF * std::fabs(inCosAbs) / (hit.distance * hit.distance);
+	out.throughput = throughput;
+	return hit.inst < 0 ? 2 : 1;
+}
+
+// cpu_bpt.cpp:170-232: one light subpath and one view subpath for a pixel,
+// every view vertex connected to every light vertex, random emitter hits
+// weighted by the balance heuristic.
+void bpt_sample(const BptState& st, i32 px, i32 py, u32 idx, u32 numPixels, Pcg64& rng, i32* recPixel, float* recValue,
+                Counters& cnt) {
+	const Scene& S = *st.scene;
+	const OrLtParams& P = st.params;
+	const i32 maxP = std::max(1, P.maxPathLength);
+	const i32 pixel = py * i32(S.width) + px;
+	std::vector<BVertex> lpath(size_t(maxP) + 1), vpath(size_t(maxP) + 1);
+	// light subpath
+	const u64 r0 = rng.next();
+	const float su0 = sample_uniform(u32(r0)), su1 = sample_uniform(u32(r0 >> 32));
+	const u64 treeSeed = rng.next();
+	const Emitter em = lights_emit(S, idx, numPixels, treeSeed, su0, su1);
+	i32 lightPathLen = -1;
+	if(em.valid) {
+		BVertex& l0 = lpath[0];
+		l0 = BVertex{};
+		l0.prev = -1;
+		l0.position = em.position;
+		l0.throughput = { 1, 1, 1 };
+		l0.prevRelSum = 0.0f;
+		if(em.kind == LV_POINT) { l0.kind = BV_POINT; l0.incEnc = em.intensity; l0.incidentPdf = em.pChoice; }
+		else if(em.kind == LV_AREA) { l0.kind = BV_AREA; l0.incEnc = em.normal; l0.intensity = em.intensity; l0.incidentPdf = em.pdf * em.pChoice; }
+		else {
+			l0.kind = BV_ENV; l0.incEnc = em.normal; l0.intensity = em.intensity; l0.incidentPdf = em.pdf * em.pChoice;
+			l0.position = { 0, 0, 0 };
+			l0.projSceneArea = projected_area(-em.normal, S.aabb);
+		}
+		lightPathLen = 0;
+		V3 thr = { 1, 1, 1 };
+		if(maxP > 1) do {
+			if(bpt_walk(S, lpath, lightPathLen, P, px, py, rng, true, thr, lpath[size_t(lightPathLen) + 1], cnt) != 1) break;
+			++lightPathLen;
+		} while(lightPathLen < maxP - 1);
+	}
+	// view subpath
+	BVertex& c = vpath[0];
+	c = BVertex{};
+	c.kind = BV_CAMERA;
+	c.prev = -1;
+	c.position = S.cam.position;
+	c.incEnc = { float(px), float(py), 0.0f };
+	c.incidentPdf = 1.0f;
+	c.prevRelSum = 0.0f;
+	c.throughput = { 1, 1, 1 };
+	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
+	V3 throughput = { 1, 1, 1 };
+	i32 viewPathLen = 0;
+	const size_t hitBase = size_t(maxP) * size_t(maxP);
+	do {
+		const BVertex& v = vpath[size_t(viewPathLen)];
+		const i32 maxL = std::min(lightPathLen + 1, maxP - viewPathLen);
+		for(i32 l = std::max(0, P.minPathLength - viewPathLen - 1); l < maxL; ++l) {
+			const BVertex& w = lpath[size_t(l)];
+			// connect (cpu_bpt.cpp:120-148)
+			i32 ox = px, oy = py;
+			V3 bxdfs = { 0, 0, 0 };
+			float cosines = 0.0f;
+			if(!((bv_ortho(v.kind) && bv_ortho(w.kind)) || (bv_ortho(v.kind) && bv_camera(w.kind)) ||
+			     (bv_camera(v.kind) && bv_ortho(w.kind)))) {
+				V3 dir, v0;
+				float distSq;
+				if(bv_ortho(w.kind)) { dir = -w.incEnc; distSq = 1.0f; v0 = v.position; }
+				else {
+					const V3 cv = w.position - v.position;
+					distSq = lensq(cv);
+					const float dist = mbmath::sqrt(distSq);
+					dir = { sdiv(cv.x, dist), sdiv(cv.y, dist), sdiv(cv.z, dist) };
+					v0 = v.position;
+				}
+				const EvalValue val0 = bv_evaluate(S, v, dir, false, ox, oy);
+				const EvalValue val1 = bv_evaluate(S, w, -dir, true, ox, oy);
+				if(ox != -1) {
+					const V3 bxdfProd = val0.value * val1.value;
+					const float cosProd = val0.cosOut * val1.cosOut;
+					if(any_pos(bxdfProd) && cosProd > 0.0f &&
+					   !any_intersection(S, v0, bv_position(w, v0), bv_geo_normal(v), bv_geo_normal(w), dir, cnt)) {
+						const float rp0 = bpt_mis_part(vpath, v, val0.pdfB, val1.pdfF, w.kind, dir, distSq);
+						const float rp1 = bpt_mis_part(lpath, w, val1.pdfB, val0.pdfF, v.kind, dir, distSq);
+						const float mis = 1.0f / ((1.0f + rp0) + rp1);
+						bxdfs = bxdfProd * (mis / distSq);
+						cosines = cosProd;
+					}
+				}
+			}
+			if(ox != -1) {
+				const V3 full = throughput * w.throughput;
+				const V3 rad = (full * cosines) * bxdfs;
+				const float light = (((full.x + full.y) + full.z) / 3.0f) * cosines;
+				const size_t slot = size_t(viewPathLen) * size_t(maxP) + size_t(l);
+				recPixel[slot] = oy * i32(S.width) + ox;
+				float* o = recValue + 4 * slot;
+				o[0] = nan_to_zero(rad.x); o[1] = nan_to_zero(rad.y); o[2] = nan_to_zero(rad.z); o[3] = nan_to_zero(light);
+			}
+		}
+		// walk (view subpath, not adjoint)
+		const i32 r = bpt_walk(S, vpath, viewPathLen, P, px, py, rng, false, throughput, vpath[size_t(viewPathLen) + 1], cnt);
+		if(r == 0) break;
+		++viewPathLen;
+		const BVertex& h = vpath[size_t(viewPathLen)];
+		if(viewPathLen >= P.minPathLength) {
+			// get_emission (path_util.hpp:410-458) and the random-hit weight (cpu_bpt.cpp:104-115)
+			V3 value = { 0, 0, 0 };
+			float backPdf = 0.0f, startPdf = 0.0f;
+			if(h.kind == BV_VOID) {
+				const LightTree& T = S.lightTree;
+				if(T.hasBackground) {
+					value = T.bgColor * T.bgScale;
+					if(nonzero(value)) {
+						backPdf = 1.0f / projected_area(h.incEnc, S.aabb);
+						const float bgFlux = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+						const float p = bgFlux / ((T.dirFlux + T.rootFlux) + bgFlux);
+						startPdf = (1.0f / (4.0f * PI)) * p;
+					}
+				}
+			} else if(h.mat.type == OR_MAT_EMISSIVE) {
+				const float cosOut = dot(h.ts.geoN, -bv_incident_dir(h));
+				if(cosOut > 0.0f) {
+					value = h.mat.radiance;
+					backPdf = cosOut / PI;
+					if(nonzero(value)) startPdf = light_connect_pdf(S, h.inst, h.prim, h.sp);
+				}
+			}
+			if(nonzero(value)) {
+				const float sum = bpt_mis_part(vpath, h, backPdf, startPdf, BV_VIRTUAL, { 0, 0, 0 }, 0.0f);
+				value = value * (1.0f / (1.0f + sum));
+			}
+			const V3 rad = throughput * value;
+			const float light = ((throughput.x + throughput.y) + throughput.z) / 3.0f * (((value.x + value.y) + value.z) / 3.0f);
+			const size_t slot = hitBase + size_t(viewPathLen - 1);
+			recPixel[slot] = pixel;
+			float* o = recValue + 4 * slot;
+			o[0] = nan_to_zero(rad.x); o[1] = nan_to_zero(rad.y); o[2] = nan_to_zero(rad.z); o[3] = nan_to_zero(light);
+		}
+		if(bv_end(h.kind)) break;
+	} while(viewPathLen < maxP);
+}
+
+void bpt_iterate(BptState& st, int numThreads) {
+	const Scene& S = *st.scene;
+	const u32 n = S.width * S.height;
+	const i32 maxP = std::max(1, st.params.maxPathLength);
+	const size_t slots = bpt_slots(maxP);
+	++st.iteration;
+	st.recPixel.assign(size_t(n) * slots, -1);
+	st.recValue.assign(size_t(n) * slots * 4, 0.0f);
+	Counters total;
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(dynamic, 256)
+		for(i32 pixel = 0; pixel < i32(n); ++pixel)
+			bpt_sample(st, pixel % i32(S.width), pixel / i32(S.width), u32(pixel), n, st.rngs[size_t(pixel)],
+			           &st.recPixel[size_t(pixel) * slots], &st.recValue[size_t(pixel) * slots * 4], local);
+#pragma omp critical
+		total.add(local);
+	}
+	st.stats.add(total);
+	std::vector<float> iter(size_t(n) * 4, 0.0f);
+	for(size_t k = 0; k < st.recPixel.size(); ++k) {
+		if(st.recPixel[k] < 0) continue;
+		float* d = &iter[size_t(st.recPixel[k]) * 4];
+		for(int c = 0; c < 4; ++c) d[c] += st.recValue[4 * k + size_t(c)];
+	}
+	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	for(size_t p = 0; p < n; ++p) {
+		for(int c = 0; c < 3; ++c) { float& cr = st.radiance[3 * p + size_t(c)]; const float diff = iter[4 * p + size_t(c)] - cr; cr += diff / den; }
+		{ float& cl = st.lightness[p]; const float diff = iter[4 * p + 3] - cl; cl += diff / den; }
 	}
 }
 
@@ -2723,6 +3097,52 @@ int oracle_lt_records(void* p, int32_t* pixels, float* values) {
 
 int oracle_lt_stats(void* p, OrStats* o) {
 	const LtState* st = static_cast<const LtState*>(p);
+	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
+	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
+	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
+	return 1;
+}
+
+void* oracle_bpt_create(void* s, const OrLtParams* params) {
+	Scene* S = static_cast<Scene*>(s);
+	auto* st = new BptState();
+	st->scene = S;
+	st->params = *params;
+	const i32 num = i32(S->width * S->height);
+	st->rngs.resize(size_t(num));
+	// cpu_bpt.cpp:239-244
+	const i32 seed = i32(u32(params->seed) * u32(num + 1));
+	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
+	st->radiance.assign(size_t(num) * 3, 0.0f);
+	st->lightness.assign(size_t(num), 0.0f);
+	return st;
+}
+
+void oracle_bpt_destroy(void* p) { delete static_cast<BptState*>(p); }
+
+int oracle_bpt_iterate(void* p, int32_t nt) {
+	bpt_iterate(*static_cast<BptState*>(p), nt > 0 ? nt : 1);
+	return 1;
+}
+
+int oracle_bpt_get_target(void* p, int32_t target, float* out) {
+	const BptState* st = static_cast<const BptState*>(p);
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness : nullptr;
+	if(!v) return 0;
+	std::memcpy(out, v->data(), v->size() * 4);
+	return 1;
+}
+
+int oracle_bpt_records(void* p, int32_t* pixels, float* values) {
+	const BptState* st = static_cast<const BptState*>(p);
+	if(st->iteration < 0) return 0;
+	std::memcpy(pixels, st->recPixel.data(), st->recPixel.size() * 4);
+	std::memcpy(values, st->recValue.data(), st->recValue.size() * 4);
+	return 1;
+}
+
+int oracle_bpt_stats(void* p, OrStats* o) {
+	const BptState* st = static_cast<const BptState*>(p);
 	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
 	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
 	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;

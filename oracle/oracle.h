@@ -151,6 +151,19 @@ int oracle_lt_get_target(void* lt, int32_t target, float* out);
  * radiance rgb, lightness, density as added to the iteration buffer. */
 int oracle_lt_records(void* lt, int32_t* pixels, float* values);
 int oracle_lt_stats(void* lt, OrStats* stats);
+/* Bidirectional path tracer (CpuBidirPathTracer equivalent, cpu_bpt.cpp);
+ * the parameters are the light tracer's (density unused). */
+void* oracle_bpt_create(void* scene, const OrLtParams* params);
+void oracle_bpt_destroy(void* bpt);
+int oracle_bpt_iterate(void* bpt, int32_t numThreads);
+/* Cumulative target: 0 radiance (3 ch), 1 lightness (1 ch) */
+int oracle_bpt_get_target(void* bpt, int32_t target, float* out);
+/* The last iteration's contributions, W*H*(M*M + M) slots for maximum path
+ * length M (pixel major): first the connections [view path length][light
+ * vertex], then the emitter hits [view path length - 1]; pixels[k] = pixel
+ * index or -1, values[4k..4k+3] = radiance rgb and lightness as added. */
+int oracle_bpt_records(void* bpt, int32_t* pixels, float* values);
+int oracle_bpt_stats(void* bpt, OrStats* stats);
 /* Building blocks exposed for known-answer tests. */
 int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);

@@ -100,6 +100,13 @@ def lib():
         L.oracle_lt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.oracle_lt_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_lt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_bpt_create.restype = C.c_void_p
+        L.oracle_bpt_create.argtypes = [C.c_void_p, C.POINTER(OrLtParams)]
+        L.oracle_bpt_destroy.argtypes = [C.c_void_p]
+        L.oracle_bpt_iterate.argtypes = [C.c_void_p, C.c_int32]
+        L.oracle_bpt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.oracle_bpt_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_bpt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
         L.oracle_pcg64_seed.restype = C.c_uint64
         L.oracle_pcg64_seed.argtypes = [C.c_uint32]
         L.oracle_pcg64_next.restype = C.c_uint64
@@ -347,6 +354,61 @@ class OracleLightTracer:
     def close(self):
         if self.handle:
             lib().oracle_lt_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleBidirPathTracer:
+    """CPU restatement of the bidirectional path tracer (cpu_bpt.cpp): per pixel and iteration one light
+    subpath and one view subpath, all connections and emitter hits weighted by the balance heuristic."""
+
+    TARGETS = {"Radiance": (0, 3), "Lightness": (1, 1)}
+
+    def __init__(self, scene: OracleScene, seed=0, min_path=0, max_path=16):
+        self.scene = scene
+        self.max_path = max(1, max_path)
+        p = OrLtParams(seed, min_path, max_path, 0)
+        self.handle = lib().oracle_bpt_create(scene.handle, C.byref(p))
+        if not self.handle:
+            raise ValueError("oracle_bpt_create failed")
+
+    def iterate(self, threads: int = 0):
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        lib().oracle_bpt_iterate(self.handle, threads)
+
+    def target(self, name: str):
+        w, h = self.scene.spec.width, self.scene.spec.height
+        idx, ch = self.TARGETS[name]
+        out = np.zeros((h, w, ch), np.float32)
+        lib().oracle_bpt_get_target(self.handle, idx, _ptr(out))
+        return out
+
+    def records(self):
+        """The last iteration's contributions per pixel: M*M connection slots [view length][light vertex]
+        then M emitter-hit slots (M = max. path length); pixel index (-1: none) and (radiance rgb,
+        lightness) as added."""
+        m = self.max_path
+        n = self.scene.spec.width * self.scene.spec.height * (m * m + m)
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 4), np.float32)
+        if not lib().oracle_bpt_records(self.handle, _ptr(pix), _ptr(val)):
+            raise RuntimeError("no iteration has run")
+        return pix, val
+
+    def stats(self):
+        s = OrStats()
+        lib().oracle_bpt_stats(self.handle, C.byref(s))
+        return {k: getattr(s, k) for k, _ in OrStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().oracle_bpt_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
