@@ -18,6 +18,11 @@
 //   rng / sampling .... src/core/math/rng.hpp:126-207, sampling.hpp:23-199
 //   pixel loop ........ src/core/renderer/pt/cpu_pt.cpp:18-45
 //   accumulation ...... src/core/renderer/targets/output_handler_variance.hpp:7-31
+//   light tracer ...... src/core/renderer/lt/lt_common.hpp:19-77, cpu_lt.cpp:18-39,
+//                       src/core/scene/lights/light_tree_sampling.hpp:81-188,
+//                       light_sampling.hpp:80-306, src/core/cameras/pinhole.hpp:86-116
+//   bidirectional PT .. src/core/renderer/bpt/cpu_bpt.cpp:18-247,
+//                       src/core/renderer/path_util.hpp:41-794
 //
 // Pinned deviations from the reference (each needed because the reference is
 // either order-dependent or relies on the missing "epsilon" library):
@@ -45,7 +50,9 @@
 //      uses an FMA;
 //  10. sphere primitives are indexed from the sphere offset (the reference's
 //      intersection.cu:270 and descriptors.hpp:198 index the sphere arrays
-//      with the global primitive id, which only works for sphere-only LoDs).
+//      with the global primitive id, which only works for sphere-only LoDs);
+//  11. the frame of an area light's emission lobe uses n x (the axis of n's
+//      smallest component) for epsilon's `perpendicular`.
 #include "oracle.h"
 #include "../mufflon_b200/csrc/common/fmath.hpp"
 
@@ -1815,7 +1822,6 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 			}
 		}
 		// walk (random_walk.hpp:38-113)
-		const V3 lastPosition = (v.type == V_VOID) ? V3{ 0, 0, 0 } : v.position;
 		const u64 x0 = rng.next(), x1 = rng.next();
 		const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
 		const float rr = sample_uniform(u32(rng.next()));

@@ -2,8 +2,9 @@
  * CPU oracle for the Mufflon path-tracer hot path: TEST INFRASTRUCTURE ONLY.
  *
  * This library is a CPU restatement of the reference renderer's CPU path
- * (LBVH build, two-level traversal, pt_sample), written to check the CUDA
- * implementation in mufflon_b200/ bit for bit. Only tests/, the smoke()
+ * (LBVH build, two-level traversal, pt_sample, the light tree, and the light
+ * tracer's and bidirectional path tracer's samplers), written to check the
+ * CUDA implementation in mufflon_b200/ bit for bit. Only tests/, the smoke()
  * entry point and bench.py's CPU-baseline leg load it. The product library
  * never links, loads or calls it.
  *
