@@ -450,7 +450,10 @@ def run_batch(args):
         bindings.load_scene_spec(d, spec)
         assert d.render_enable_renderer(0, 0)
         worlds.append(d)
-    tuned = autotune.autotune(worlds[1], iterations=2, warmup=1)  # tuning of the largest mesh, used by the batch
+    # The batch runs with the first job's schedule settings (the defaults here). Tuning them on one
+    # scene does not carry over: the icosphere's best (4 trace blocks per SM) makes this mixed batch
+    # slower (16.9 vs 18.6 jobs/s), the instanced scene's best is the default.
+    schedule = {k: worlds[0].renderer_get_parameter_int(v) for k, v in autotune.PARAMS.items()}
     jobs = batch_jobs(args.jobs)
     req = [dict(instance=worlds[j["scene"]], width=j["width"], height=j["height"], spp=j["spp"],
                 max_path=j["max_path"], seed=j["seed"]) for j in jobs]
@@ -498,7 +501,7 @@ def run_batch(args):
                                      {"jobs": v[2], "device_ms": round(v[1], 1),
                                       "msamples_per_s": round(v[0] / (v[1] * 1e-3) / 1e6, 1)}
                                      for k, v in sorted(per_scene.items())},
-            "autotune": tuned["best"]}
+            "schedule": schedule}
     print(json.dumps(line), flush=True)
     for d in worlds:
         d.close()
