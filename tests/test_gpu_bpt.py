@@ -119,3 +119,30 @@ def test_bpt_in_the_registry():
         assert d.renderer_get_parameter_int("Seed") == 0
     finally:
         d.close()
+
+
+def _dark_icosphere():
+    """No light at all: no point light, no emitter, no background."""
+    spec = scenes.displaced_icosphere(4, subdiv=3, width=24, height=16)
+    return dataclasses.replace(spec, background=None, point_lights=np.zeros((0, 6), np.float32))
+
+
+@pytest.mark.parametrize("case,max_path", [("panels", 1), ("cornell", 2), ("dark", 4)])
+def test_bpt_edge_cases_match_oracle(oracle, case, max_path):
+    """Path length 1 (no light-subpath walk), 2, and a scene without lights
+    (no light subpath; only the view subpath runs and the image stays black)."""
+    spec = _dark_icosphere() if case == "dark" else CASES[case]()
+    params = {"Seed": 1, "Min. path length": 0, "Max. path length": max_path}
+    ob = oracle.OracleBidirPathTracer(oracle.OracleScene(spec), seed=1, min_path=0, max_path=max_path)
+
+    def check(it, rec):
+        ob.iterate()
+        op, ov = ob.records()
+        assert np.array_equal(rec[0], op) and np.array_equal(rec[1].view(np.uint32), ov.view(np.uint32))
+
+    out, stats = _gpu_bpt(spec, params, 2, check)
+    if case == "dark":
+        assert not out["Radiance"].any() and stats["rays"] > 0
+    else:
+        assert out["Radiance"].any()
+        assert _rel_rmse(out["Radiance"], ob.target("Radiance")) <= 1e-5

@@ -163,3 +163,30 @@ def test_hit_id_is_not_a_light_tracer_target():
             d.get_target_image("Hit ID")
     finally:
         d.close()
+
+
+def _dark_icosphere():
+    """No light at all: no point light, no emitter, no background."""
+    spec = scenes.displaced_icosphere(4, subdiv=3, width=24, height=16)
+    return dataclasses.replace(spec, background=None, point_lights=np.zeros((0, 6), np.float32))
+
+
+@pytest.mark.parametrize("case,max_path", [("panels", 1), ("cornell", 2), ("dark", 4)])
+def test_lt_edge_cases_match_oracle(oracle, case, max_path):
+    """Path length 1 (only the light vertices' own connections), 2, and a
+    scene without lights (no photon starts; the image stays black)."""
+    spec = _dark_icosphere() if case == "dark" else CASES[case]()
+    params = {"Seed": 1, "Min. path length": 0, "Max. path length": max_path}
+    lt = oracle.OracleLightTracer(oracle.OracleScene(spec), seed=1, min_path=0, max_path=max_path)
+
+    def check(it, rec):
+        lt.iterate()
+        op, ov = lt.records()
+        assert np.array_equal(rec[0], op) and np.array_equal(rec[1].view(np.uint32), ov.view(np.uint32))
+
+    out, stats = _gpu_lt(spec, params, 2, False, check)
+    if case == "dark":
+        assert not out["Radiance"].any() and stats["rays"] == 0
+    else:
+        assert out["Radiance"].any()
+        assert _rel_rmse(out["Radiance"], lt.target("Radiance")) <= 1e-5
