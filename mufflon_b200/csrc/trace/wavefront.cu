@@ -303,10 +303,20 @@ struct VertexInfo {
 	f3 albedo;
 };
 
-template < class ShadowFn, class VertexFn >
-MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
-                      f3& throughput, float& pdfF, f3& radiance, u64& rng, float2* hit0, f3& nextO, f3& nextD,
-                      ShadowFn&& shadow, VertexFn&& onVertex) {
+// The state of a shaded path vertex between the parts of shade_vertex.
+struct ShadeState {
+	f3 position, incident;
+	TangentSpace ts;
+	Params mat;
+	int pathLen;
+};
+
+// shade_vertex, first part: hit attributes, the first-hit id, the emission
+// term (pt_common.hpp:139-153). False when the path ends at this vertex (a
+// miss, or the maximum path length).
+template < class VertexFn >
+MBD bool shade_begin(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
+                     const f3& throughput, float pdfF, f3& radiance, float2* hit0, ShadeState& v, VertexFn&& onVertex) {
 	bool surface = false;
 	int matIndex = -1;
 	f3 position = make3(0.0f, 0.0f, 0.0f), incidentEncoded;
@@ -363,45 +373,76 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 		                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f) });
 	}
 	if(!surface || !(pathLen < P.maxPathLength)) return false;
-	// -- next loop iteration of pt_sample: next-event estimation
-	const f3 incident = incident_direction(incidentEncoded);
-	if(pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
-		const u64 neeSeed = pcg_next(rng);
-		for(int i = 0; i < P.neeCount; ++i) {
-			const u64 r = pcg_next(rng);
-			const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
-			const Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, position, nu0, nu1);
-			if(!nee.valid) continue;
-			EvalValue val = material_evaluate(ts, mat, incident, nee.dir);
-			if(nee.cosOut != 0.0f) val.cosOut *= nee.cosOut;
-			const f3 rad = val.value * nee.diffIrradiance;
-			if(any_pos(rad) && val.cosOut > 0.0f) {
-				const float hitPdf = __fdiv_rn(val.pdfF * fabsf(nee.cosOut), nee.distSq);
-				const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
-				const f3 c = ((throughput * val.cosOut) * rad) * mis;
-				f3 so, sd; float stmax;
-				shadow_ray(position, nee.position, ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
-				shadow(i, so, sd, stmax, c);
-			}
-		}
-	}
-	// -- walk (random_walk.hpp:38-86)
+	v.position = position;
+	v.incident = incident_direction(incidentEncoded);
+	v.ts = ts;
+	v.mat = mat;
+	v.pathLen = pathLen;
+	return true;
+}
+
+// Whether the next loop iteration of pt_sample estimates direct light.
+MBD bool shade_has_nee(const PtParams& P, const ShadeState& v) {
+	return v.pathLen + 1 >= P.minPathLength && v.pathLen + 1 <= P.maxPathLength;
+}
+
+// Next-event sample i at v (pt_common.hpp:105-124): draws its number; true
+// with the shadow ray and the term it adds when it can contribute.
+MBD bool shade_nee(const DScene& S, const PtParams& P, const ShadeState& v, const f3& throughput, u64& rng, u64 neeSeed,
+                   int i, f3& so, f3& sd, float& stmax, f3& c) {
+	const u64 r = pcg_next(rng);
+	const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
+	const Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, v.position, nu0, nu1);
+	if(!nee.valid) return false;
+	EvalValue val = material_evaluate(v.ts, v.mat, v.incident, nee.dir);
+	if(nee.cosOut != 0.0f) val.cosOut *= nee.cosOut;
+	const f3 rad = val.value * nee.diffIrradiance;
+	if(!(any_pos(rad) && val.cosOut > 0.0f)) return false;
+	const float hitPdf = __fdiv_rn(val.pdfF * fabsf(nee.cosOut), nee.distSq);
+	const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
+	c = ((throughput * val.cosOut) * rad) * mis;
+	shadow_ray(v.position, nee.position, v.ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
+	return true;
+}
+
+// The walk (random_walk.hpp:38-86): BSDF sample, throughput, Russian
+// roulette; false when the path ends. nextO is already offset.
+MBD bool shade_walk(const PtParams& P, const ShadeState& v, f3& throughput, float& pdfF, u64& rng, f3& nextO, f3& nextD) {
 	const u64 x0 = pcg_next(rng), x1 = pcg_next(rng);
 	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
 	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
-	const PathSample smp = material_sample(ts, mat, incident, ru0, ru1, x1);
+	const PathSample smp = material_sample(v.ts, v.mat, v.incident, ru0, ru1, x1);
 	if(!smp.valid) return false;
 	throughput = throughput * smp.throughput;
-	if(pathLen >= P.rrStartDepth) {
+	if(v.pathLen >= P.rrStartDepth) {
 		const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
 		if(rr >= cp) return false;
 		throughput = throughput / cp;
 	}
 	pdfF = smp.pdfF;
-	nextO = position;
-	add_epsilon(nextO, smp.excident, ts.geoN);
+	nextO = v.position;
+	add_epsilon(nextO, smp.excident, v.ts.geoN);
 	nextD = smp.excident;
 	return true;
+}
+
+// One vertex of pt_sample: emission, next-event estimation (each shadow ray
+// handed to `shadow` in order) and the walk to the next ray.
+template < class ShadowFn, class VertexFn >
+MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
+                      f3& throughput, float& pdfF, f3& radiance, u64& rng, float2* hit0, f3& nextO, f3& nextD,
+                      ShadowFn&& shadow, VertexFn&& onVertex) {
+	ShadeState v;
+	if(!shade_begin(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, hit0, v, onVertex)) return false;
+	if(shade_has_nee(P, v)) {
+		const u64 neeSeed = pcg_next(rng);
+		for(int i = 0; i < P.neeCount; ++i) {
+			f3 so, sd, c;
+			float stmax;
+			if(shade_nee(S, P, v, throughput, rng, neeSeed, i, so, sd, stmax, c)) shadow(i, so, sd, stmax, c);
+		}
+	}
+	return shade_walk(P, v, throughput, pdfF, rng, nextO, nextD);
 }
 
 // Shade stage of the wavefront: one thread per queued path. Next-event rays go
@@ -467,11 +508,17 @@ __global__ void __launch_bounds__(128) k_shade(const SP sp, WfState W, int q, in
 }
 
 // Tail of an iteration: persistent threads take the paths of extension queue
-// q (already traced, bounce `bounce`) one at a time and finish each of them in
-// place: shade, trace the next-event rays at once and add their contributions
-// in order, trace the next extension ray, and so on until the path ends. Used
+// q (already traced, bounce `bounce`) and finish each of them in place:
+// shade, trace the next-event rays one by one and add their contributions in
+// order, trace the next extension ray, and so on until the path ends. Used
 // once few paths are left, where a separate launch per bounce would be
 // dominated by launch and drain latency.
+//
+// The lanes run a state machine: a lane takes a new path as soon as its own
+// ends (the warp claims all idle lanes' paths with one atomic), and every pass
+// of the loop traces at most one ray per lane (a shadow ray or the next
+// extension ray) in one traversal loop shared by the warp. A path's random
+// numbers, terms and their order are those of shade_vertex.
 template < int MINB, class SP >
 __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int q, int bounce,
                                                     int workIdx, TraceCounters* counters, unsigned tailMax) {
@@ -481,62 +528,112 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	// takes over only the first bounce whose queue holds at most tailMax paths
 	if(*reinterpret_cast<volatile unsigned*>(W.counters + C_TAILED) || count > tailMax) return;
+	enum { T_IDLE = 0, T_NEE, T_WALK, T_EXIT };
 	LocalStack stack;
-	for(;;) {
-		const unsigned item = atomicAdd(W.counters + C_WORK + workIdx, 1u);
-		if(item >= count) break;
-		const int p = W.qPath[q][item];
+	const unsigned lane = threadIdx.x & 31u;
+	int phase = T_IDLE;
+	int p = 0, b = 0, i = 0;
+	f3 throughput = make3(0.0f, 0.0f, 0.0f), radiance = make3(0.0f, 0.0f, 0.0f), c = make3(0.0f, 0.0f, 0.0f);
+	float pdfF = 0.0f, radW = 0.0f;
+	u64 rng = 0, neeSeed = 0;
+	ShadeState v;
+	auto on_vertex = [&](f3 e, const VertexInfo& vi) {
+		if constexpr(SP::adjoint) adjoint_vertex(sp.A, sp.scene(p), p, e, vi.surface, vi.materialType, vi.materialIndex, vi.uv, vi.albedo);
+	};
+	// shades the vertex a traced extension ray reached; sets the next phase
+	auto begin_vertex = [&](f3 origin, f3 dir, const HitRec& hr) {
 		const DScene& S = sp.scene(p);
 		const PtParams& P = sp.params(p);
-		f3 origin = f4to3(W.qOrg[q][item]);
-		f3 dir = f4to3(W.qDir[q][item]);
-		const float4 hh = W.qHit[q][item];
-		HitRec hr;
-		hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
-		hr.sp = make2(hh.w, W.qHitSpy[q][item]);
-		hr.has = hr.inst >= 0;
-		const float4 tp = W.thrPdf[p];
-		f3 throughput = f4to3(tp);
-		float pdfF = tp.w;
-		const float4 ra = W.rad[p];
-		f3 radiance = f4to3(ra);
-		u64 rng = W.rng[p];
-		for(int b = bounce;; ++b) {
-			f3 nextO, nextD;
-			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
-				nextO, nextD, [&](int, f3 so, f3 sd, float stmax, f3 c) {
-					LocalCounters cnt;
-					const bool occ = occluded_wide(S, so, sd, stmax, cnt, stack);
-					stats_add(stats, 1, cnt);
-					if(!occ) {
-						radiance = contribute(radiance, c);
-						if constexpr(SP::adjoint) adjoint_add(sp.A, p, contribute(make3(0.0f, 0.0f, 0.0f), c));
-					}
-				}, [&](f3 e, const VertexInfo& v) {
-					if constexpr(SP::adjoint) adjoint_vertex(sp.A, S, p, e, v.surface, v.materialType, v.materialIndex, v.uv, v.albedo);
-				});
-			if(!cont) break;
-			origin = nextO;
-			dir = nextD;
-			LocalCounters cnt;
-			hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
-			stats_add(stats, 0, cnt);
+		if(!shade_begin(S, P, b, origin, dir, hr, throughput, pdfF, radiance, W.hit0 + p, v, on_vertex)) {
+			W.rad[p] = pack(radiance, radW);
+			W.rng[p] = rng;
+			phase = T_IDLE;
+			return;
 		}
-		W.rad[p] = pack(radiance, ra.w);
-		W.rng[p] = rng;
+		i = 0;
+		if(shade_has_nee(P, v)) { neeSeed = pcg_next(rng); phase = T_NEE; }
+		else phase = T_WALK;
+	};
+	for(;;) {
+		const unsigned idle = __ballot_sync(0xffffffffu, phase == T_IDLE);
+		if(idle) {
+			const int leader = __ffs(idle) - 1;
+			unsigned base = 0;
+			if(int(lane) == leader) base = atomicAdd(W.counters + C_WORK + workIdx, unsigned(__popc(idle)));
+			base = __shfl_sync(0xffffffffu, base, leader);
+			if(phase == T_IDLE) {
+				const unsigned item = base + unsigned(__popc(idle & ((1u << lane) - 1u)));
+				if(item >= count) phase = T_EXIT;
+				else {
+					p = W.qPath[q][item];
+					const float4 hh = W.qHit[q][item];
+					HitRec hr;
+					hr.t = hh.x; hr.inst = __float_as_int(hh.y); hr.prim = __float_as_int(hh.z);
+					hr.sp = make2(hh.w, W.qHitSpy[q][item]);
+					hr.has = hr.inst >= 0;
+					const float4 tp = W.thrPdf[p];
+					throughput = f4to3(tp);
+					pdfF = tp.w;
+					const float4 ra = W.rad[p];
+					radiance = f4to3(ra);
+					radW = ra.w;
+					rng = W.rng[p];
+					b = bounce;
+					begin_vertex(f4to3(W.qOrg[q][item]), f4to3(W.qDir[q][item]), hr);
+				}
+			}
+		}
+		if(__all_sync(0xffffffffu, phase == T_EXIT)) break;
+		bool trace = false, shadow = false;
+		f3 ro = make3(0.0f, 0.0f, 0.0f), rd = make3(0.0f, 0.0f, 1.0f);
+		float tmax = MAX_SCENE_SIZE;
+		if(phase == T_NEE) {
+			const DScene& S = sp.scene(p);
+			const PtParams& P = sp.params(p);
+			while(i < P.neeCount) {
+				if(shade_nee(S, P, v, throughput, rng, neeSeed, i, ro, rd, tmax, c)) { trace = shadow = true; break; }
+				++i;
+			}
+			if(!trace) phase = T_WALK;
+		}
+		if(!trace && phase == T_WALK) {
+			if(shade_walk(sp.params(p), v, throughput, pdfF, rng, ro, rd)) { trace = true; tmax = MAX_SCENE_SIZE; }
+			else {
+				W.rad[p] = pack(radiance, radW);
+				W.rng[p] = rng;
+				phase = T_IDLE;
+			}
+		}
+		if(!trace) continue;
+		const DScene& S = sp.scene(p);
+		LocalCounters cnt;
+		WideTracer t;
+		t.init(S, ro, rd, tmax, shadow, cnt);
+		while(!t.step(S, cnt, stack)) {}
+		stats_add(stats, shadow ? 1 : 0, cnt);
+		if(shadow) {
+			if(!t.occluded) {
+				radiance = contribute(radiance, c);
+				if constexpr(SP::adjoint) adjoint_add(sp.A, p, contribute(make3(0.0f, 0.0f, 0.0f), c));
+			}
+			++i;
+		} else {
+			++b;
+			begin_vertex(ro, rd, t.best);
+		}
 	}
 	__syncthreads();
 	if(threadIdx.x < 2) {
 		TraceCounters* out = counters + threadIdx.x;
-		const unsigned long long* v = stats.v[threadIdx.x];
-		if(v[3]) {
-			atomicAdd(&out->rays, v[3]);
-			if(threadIdx.x == 1) atomicAdd(&out->shadowRays, v[3]);
-			atomicAdd(&out->nodeVisits, v[0]);
-			atomicAdd(&out->primTests, v[1]);
-			atomicAdd(&out->instanceVisits, v[2]);
+		const unsigned long long* v2 = stats.v[threadIdx.x];
+		if(v2[3]) {
+			atomicAdd(&out->rays, v2[3]);
+			if(threadIdx.x == 1) atomicAdd(&out->shadowRays, v2[3]);
+			atomicAdd(&out->nodeVisits, v2[0]);
+			atomicAdd(&out->primTests, v2[1]);
+			atomicAdd(&out->instanceVisits, v2[2]);
 		}
-		if(v[5]) atomicAdd(&out->errors, unsigned(v[5]));
+		if(v2[5]) atomicAdd(&out->errors, unsigned(v2[5]));
 	}
 }
 
