@@ -51,10 +51,10 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt", "bpt"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt", "bpt", "instanced"],
                    help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one; "
                         "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
-                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p")
+                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; instanced: config 2 (4 096 instances) at 1080p")
     p.add_argument("--jobs", type=int, default=64)
     return p.parse_args()
 
@@ -788,6 +788,52 @@ def run_bpt(args):
     print(json.dumps(line), flush=True)
 
 
+def run_instanced(args):
+    """Config 2: 4 096 rotated and scaled instances of 10 noise-displaced
+    meshes (10 k - 200 k triangles) plus one object of 20 000 spheres, camera
+    inside the box; 1920 x 1080, 64 spp per step, path length 12, Russian
+    roulette from length 3. Device time from CUDA events; the load's object
+    and instance hierarchy build times come from world_load_scenario."""
+    import torch
+    torch.cuda.set_device(0)
+    from mufflon_b200 import bindings, build, scenes
+    build.build()
+    spec = scenes.instanced_scene(0, width=WIDTH, height=HEIGHT)
+    d = bindings.DllInterface()
+    sc = bindings.load_scene_spec(d, spec)
+    assert d.render_enable_renderer(0, 0)
+    for k, v in {"Max. path length": 12, "RR start depth": 3}.items():
+        assert d.renderer_set_parameter_int(k, v)
+    spp = 64
+    for _ in range(args.warmup):
+        d.render_iterate()
+    torch.cuda.synchronize()
+    ms = rays = 0.0
+    for _ in range(args.steps * spp):
+        d.render_iterate()
+        st = d.render_stats()
+        ms += st["kernelMs"]; rays += st["rays"]
+        if st["errors"]:
+            raise RuntimeError(f"traversal errors reported: {st['errors']}")
+    loads = []
+    for _ in range(3):
+        assert d.world_load_scenario(sc)
+        loads.append(d.load_stats())
+    d.close()
+    unique = sum(len(l.triangles) for l in spec.lods)
+    inst_tris = int(sum(len(spec.lods[i].triangles) for i in spec.instance_lod))
+    line = {"metric": "instanced scene Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+            "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
+            "config": {"workload": "instanced_4096x10meshes_20000spheres_1920x1080_64spp_depth12_rr3",
+                       "unique_triangles": unique, "instanced_triangles": inst_tris,
+                       "instances": int(len(spec.instance_lod)), "spheres": int(len(spec.lods[-1].spheres))},
+            "rays_per_step": int(rays / args.steps),
+            "load_ms": {k: round(float(np.median([l[k] for l in loads])), 3)
+                        for k in ("totalMs", "uploadMs", "bvhMs", "instanceBvhMs")}}
+    print(json.dumps(line), flush=True)
+
+
 def dataclasses_replace_texture(spec, tex3):
     import dataclasses
     t = np.ones(tex3.shape[:2] + (4,), np.float32)
@@ -814,6 +860,9 @@ def main():
         return
     if args.workload == "bpt":
         run_bpt(args)
+        return
+    if args.workload == "instanced":
+        run_instanced(args)
         return
     if args.impl == "reference":
         run_reference(args)
