@@ -154,10 +154,11 @@ static __device__ __noinline__ bool lt_walk(const DScene& S, Photon& ph, f3& ori
 // one atomic), and every pass of the loop traces at most one ray per lane
 // (the camera connection's shadow ray or the walk's extension ray) in one
 // traversal loop shared by the warp. Each photon still draws its random
-// numbers in lt_sample's order. Register budget: 5 resident blocks of 128
-// threads (96 registers, some spilled to L1) measured faster than 3 blocks
-// without spills (4.60 vs 4.95 ms per 1080p iteration).
-__global__ void __launch_bounds__(128, 5) k_lt(const DScene S, const LtParams P, const LtTargets T,
+// numbers in lt_sample's order. Register budget: 6 resident blocks of 128
+// threads (80 registers, some spilled to L1) measured fastest on the 1080p
+// headline scene: 616 Mrays/s against 588 with 5 blocks, 559 with 4, and 3
+// blocks without spills slower still.
+__global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P, const LtTargets T,
                                             unsigned int* workCounter, TraceCounters* counters) {
 	LocalStack stack;
 	LocalCounters cnt;
