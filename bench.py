@@ -744,7 +744,7 @@ def run_bpt(args):
     spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
     d = bindings.DllInterface()
     bindings.load_scene_spec(d, spec)
-    assert d.render_enable_renderer(2, 0)
+    assert d.render_enable_renderer(3, 0)
     assert d.renderer_set_parameter_int("Max. path length", MAX_PATH)
     d.render_enable_render_target("Radiance", False)
     iters = SPP_PER_FRAME

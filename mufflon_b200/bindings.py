@@ -324,6 +324,7 @@ class DllHolder:
             "renderer_set_parameter_int": (c_uint32, [c_void_p, c_char_p, c_int32]),
             "renderer_get_parameter_int": (c_uint32, [c_void_p, c_char_p, POINTER(c_int32)]),
             "renderer_set_parameter_float": (c_uint32, [c_void_p, c_char_p, c_float]),
+            "renderer_get_parameter_float": (c_uint32, [c_void_p, c_char_p, POINTER(c_float)]),
             "renderer_set_parameter_bool": (c_uint32, [c_void_p, c_char_p, c_uint32]),
             "renderer_set_parameter_enum": (c_uint32, [c_void_p, c_char_p, c_int32]),
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
@@ -445,6 +446,12 @@ class DllInterface:
 
     def renderer_set_parameter_int(self, parameterName, value):
         return self.core.renderer_set_parameter_int(self.muffInst, parameterName.encode(), int(value)) != 0
+
+    def renderer_get_parameter_float(self, parameterName):
+        v = c_float(0.0)
+        self._check(self.core.renderer_get_parameter_float(self.muffInst, parameterName.encode(), byref(v)),
+                    "renderer_get_parameter_float")
+        return v.value
 
     def renderer_get_parameter_int(self, parameterName):
         v = c_int32(0)

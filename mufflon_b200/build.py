@@ -28,7 +28,7 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/wide.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu",
               "core/light_build.cu", "core/instance_boxes.cu", "trace/lt.cu",
-              "trace/bpt.cu"]
+              "trace/bpt.cu", "trace/wireframe.cu"]
 CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
 # the scene-file loader: its own library on top of the core's C API
 LOADER_SOURCES = ["loader/json.cpp", "loader/mff_binary.cpp", "loader/scene_loader.cpp", "loader/interface.cpp"]

@@ -64,6 +64,8 @@ const ParamDesc LT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "Record connections", PARAM_INT },
 };
+// wireframe_params.hpp:6-26
+const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT } };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
 const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
@@ -72,7 +74,11 @@ const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albe
 const char* LT_TARGETS[] = { "Radiance", "Lightness", "Density" };
 
 int32_t* param_ptr(RendererState& r, const char* name) {
-	if(r.kind == 1 || r.kind == 2) {
+	if(r.kind == 2) {
+		if(!std::strcmp(name, "Maximum trace depth")) return &r.wireParams.maxTraceDepth;
+		return nullptr;
+	}
+	if(r.kind == 1 || r.kind == 3) {
 		LtParams& p = r.kind == 1 ? r.ltParams : r.bptParams;
 		if(!std::strcmp(name, "Seed")) return &p.seed;
 		if(!std::strcmp(name, "Min. path length")) return &p.minPathLength;
@@ -152,10 +158,10 @@ void ensure_lt_buffers(MufflonInstance& I) {
 	}
 	// records: light tracer M slots of 5 floats per photon, bidirectional
 	// path tracer M*M + M slots of 4 floats per pixel (M = max. path length)
-	const size_t m = size_t(std::max(1, r.kind == 2 ? r.bptParams.maxPathLength : r.ltParams.maxPathLength));
-	const bool record = r.kind == 2 ? r.bptRecord != 0 : r.ltRecord != 0;
-	const size_t slots = record ? (r.kind == 2 ? n * (m * m + m) : n * m) : 0;
-	const size_t floats = slots * (r.kind == 2 ? 4 : 5);
+	const size_t m = size_t(std::max(1, r.kind == 3 ? r.bptParams.maxPathLength : r.ltParams.maxPathLength));
+	const bool record = r.kind == 3 ? r.bptRecord != 0 : r.kind == 1 ? r.ltRecord != 0 : false;
+	const size_t slots = record ? (r.kind == 3 ? n * (m * m + m) : n * m) : 0;
+	const size_t floats = slots * (r.kind == 3 ? 4 : 5);
 	if(slots != r.ltRecSlots || floats != r.ltRecFloats) {
 		cudaFree(r.ltRecPixel); cudaFree(r.ltRecValue);
 		r.ltRecPixel = nullptr; r.ltRecValue = nullptr; r.ltRecSlots = 0; r.ltRecFloats = 0;
@@ -168,7 +174,7 @@ void ensure_lt_buffers(MufflonInstance& I) {
 			r.ltRecFloats = floats;
 		}
 	}
-	if(r.kind == 2) {
+	if(r.kind == 3) {
 		const size_t bytes = bpt_scratch_bytes(r.bptParams.maxPathLength);
 		if(bytes > r.bptScratchBytes) {
 			cudaFree(r.bptScratch);
@@ -199,9 +205,13 @@ void iterate_lt(MufflonInstance& I) {
 	t.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
-	if(r.kind == 2) {
+	if(r.kind == 3) {
 		t.density = nullptr;
 		CHECK_CUDA(launch_bpt(S, r.bptParams, t, r.bptScratch, r.workCounter, r.counters, I.stream));
+	} else if(r.kind == 2) {
+		t.radiance = r.radiance; // the "Border" target
+		t.lightness = nullptr; t.density = nullptr; t.recPixel = nullptr; t.recValue = nullptr;
+		CHECK_CUDA(launch_wireframe(S, I.scene.dInstI2W, r.wireParams, t, r.counters, I.stream));
 	} else CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters c{};
@@ -364,25 +374,29 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 	RendererState& r = I.renderer;
 	if(!r.rng || r.iteration < 0) { if(ptr) *ptr = nullptr; return true; }
 	const size_t n = size_t(r.width) * r.height;
-	if(!std::strcmp(name, "Radiance")) {
+	if(!std::strcmp(name, "Radiance") && r.kind != 2) {
 		CHECK(r.targetRadiance, "target 'Radiance' is not enabled");
 		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 3;
 	} else if((r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) ||
-	          (r.kind == 2 && !std::strcmp(name, "Lightness"))) {
+	          (r.kind == 3 && !std::strcmp(name, "Lightness"))) {
 		const bool light = !std::strcmp(name, "Lightness");
 		CHECK(light ? r.targetLightness : r.targetDensity, std::string("target '") + name + "' is not enabled");
 		const float* src = light ? r.lightness : r.density;
 		CHECK(src != nullptr, "no image yet");
 		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n), src, n * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 1;
+	} else if(r.kind == 2 && !std::strcmp(name, "Border")) {
+		CHECK(r.targetBorder, "target 'Border' is not enabled");
+		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
+		r.screenChannels = 3;
 	} else if(r.kind == 0 && !std::strcmp(name, "Hit ID")) {
 		CHECK(r.targetHitId, "target 'Hit ID' is not enabled");
 		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 2), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
 		r.screenChannels = 2;
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
-		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "bidirectional path tracer" : "path tracer"));
+		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "wireframe renderer" : r.kind == 3 ? "bidirectional path tracer" : "path tracer"));
 	}
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	if(ptr) *ptr = r.screen;
@@ -1025,10 +1039,11 @@ Boolean world_set_env_light_scale(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
 // ---------------------------------------------------------------- renderers
 // Renderers grouped by name in the reference's registry order (renderers.hpp:23-31,
 // interface.cpp:126-154): the path tracer, the light tracer and the
-// bidirectional path tracer (CPU-only in the reference), each with a CUDA
-// variation; the wireframe renderers between them are not provided.
-const char* RENDERER_NAMES[3][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" }, { "Bidirectional Pathtracer", "BPT" } };
-constexpr uint32_t NUM_RENDERERS = 3u;
+// wireframe renderer and the bidirectional path tracer (CPU-only in the
+// reference), each with a CUDA variation.
+const char* RENDERER_NAMES[4][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" }, { "Wireframe", "WF" },
+                                     { "Bidirectional Pathtracer", "BPT" } };
+constexpr uint32_t NUM_RENDERERS = 4u;
 uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return NUM_RENDERERS; CATCH_ALL(0u) }
 uint32_t render_get_renderer_variations(MufflonInstanceHdl h, uint32_t index) {
 	TRY (void)minst(h); CHECK(index < NUM_RENDERERS, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
@@ -1070,7 +1085,8 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	if(r.kind != 0) ensure_lt_buffers(I);
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
-		const int32_t seed = r.kind == 1 ? r.ltParams.seed : r.kind == 2 ? r.bptParams.seed : r.params.seed;
+		// the wireframe renderer's generators are seeded with the pixel index (cpu_wireframe.cpp:31-36)
+		const int32_t seed = r.kind == 1 ? r.ltParams.seed : r.kind == 3 ? r.bptParams.seed : r.kind == 2 ? 0 : r.params.seed;
 		CHECK_CUDA(launch_seed_rng(r.rng, n, seed, I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.radiance, 0, size_t(n) * 3 * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
@@ -1245,13 +1261,13 @@ Boolean render_save_screenshot(MufflonInstanceHdl h, const char* filename, const
 	CATCH_ALL(false)
 }
 
-static uint32_t target_count(int32_t kind) { return kind == 1 ? 3u : kind == 2 ? 2u : 8u; }
+static uint32_t target_count(int32_t kind) { return kind == 1 ? 3u : kind == 3 ? 2u : kind == 2 ? 1u : 8u; }
 uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY return target_count(minst(h).renderer.kind); CATCH_ALL(0u) }
 const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) {
 	TRY
 	const int32_t kind = minst(h).renderer.kind;
 	CHECK(index < target_count(kind), "render target index out of bounds");
-	return kind != 0 ? LT_TARGETS[index] : TARGETS[index];
+	return kind == 2 ? "Border" : kind != 0 ? LT_TARGETS[index] : TARGETS[index];
 	CATCH_ALL(nullptr)
 }
 Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
@@ -1264,6 +1280,7 @@ Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Bo
 	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = true;
 	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = true;
 	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = true;
+	else if(!std::strcmp(target, "Border")) I.renderer.targetBorder = true;
 	else throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA renderers");
 	I.renderer.needsReset = true;
 	return true;
@@ -1278,6 +1295,7 @@ Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, B
 	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = false;
 	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = false;
 	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = false;
+	else if(!std::strcmp(target, "Border")) I.renderer.targetBorder = false;
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
@@ -1290,21 +1308,24 @@ Boolean render_is_render_target_enabled(MufflonInstanceHdl h, const char* name, 
 	if(!std::strcmp(name, "Hit ID")) return I.renderer.targetHitId;
 	if(!std::strcmp(name, "Lightness")) return I.renderer.targetLightness;
 	if(!std::strcmp(name, "Density")) return I.renderer.targetDensity;
+	if(!std::strcmp(name, "Border")) return I.renderer.targetBorder;
 	return false;
 	CATCH_ALL(false)
 }
 
 uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) {
 	TRY
-	const bool lt = minst(h).renderer.kind != 0;
-	return lt ? uint32_t(sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0])) : uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]));
+	const int32_t kind = minst(h).renderer.kind;
+	if(kind == 2) return uint32_t(sizeof(WIRE_PARAMS) / sizeof(WIRE_PARAMS[0]));
+	return kind != 0 ? uint32_t(sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0])) : uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]));
 	CATCH_ALL(0u)
 }
 const char* renderer_get_parameter_desc(MufflonInstanceHdl h, uint32_t idx, ParameterType* type) {
 	TRY
-	const bool lt = minst(h).renderer.kind != 0;
-	const ParamDesc* table = lt ? LT_PARAMS : PT_PARAMS;
-	const size_t count = lt ? sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0]) : sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]);
+	const int32_t kind = minst(h).renderer.kind;
+	const ParamDesc* table = kind == 2 ? WIRE_PARAMS : kind != 0 ? LT_PARAMS : PT_PARAMS;
+	const size_t count = kind == 2 ? sizeof(WIRE_PARAMS) / sizeof(WIRE_PARAMS[0])
+	                   : kind != 0 ? sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0]) : sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]);
 	CHECK(idx < count, "parameter index out of bounds");
 	if(type) *type = table[idx].type;
 	return table[idx].name;
@@ -1334,11 +1355,23 @@ Boolean renderer_get_parameter_int(MufflonInstanceHdl h, const char* name, int32
 	return true;
 	CATCH_ALL(false)
 }
-Boolean renderer_set_parameter_float(MufflonInstanceHdl h, const char* name, float) {
-	TRY (void)minst(h); throw ApiError(std::string("unknown float parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+Boolean renderer_set_parameter_float(MufflonInstanceHdl h, const char* name, float value) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(I.renderer.kind == 2 && name && !std::strcmp(name, "Line width"), std::string("unknown float parameter '") + (name ? name : "") + "'");
+	I.renderer.wireParams.lineWidth = value;
+	I.renderer.needsReset = true;
+	return true;
+	CATCH_ALL(false)
 }
-Boolean renderer_get_parameter_float(MufflonInstanceHdl h, const char* name, float*) {
-	TRY (void)minst(h); throw ApiError(std::string("unknown float parameter '") + (name ? name : "") + "'"); CATCH_ALL(false)
+Boolean renderer_get_parameter_float(MufflonInstanceHdl h, const char* name, float* value) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(I.renderer.kind == 2 && name && !std::strcmp(name, "Line width") && value, std::string("unknown float parameter '") + (name ? name : "") + "'");
+	*value = I.renderer.wireParams.lineWidth;
+	return true;
+	CATCH_ALL(false)
 }
 Boolean renderer_set_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean value) {
 	TRY
@@ -1398,7 +1431,7 @@ Boolean mufflon_get_lt_records(MufflonInstanceHdl h, int32_t* pixels, float* val
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	const RendererState& r = I.renderer;
-	CHECK(r.kind != 0 && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer or bidirectional iteration");
+	CHECK((r.kind == 1 || r.kind == 3) && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer or bidirectional iteration");
 	CHECK(pixels && values && slots == r.ltRecSlots, "the record buffers must hold the renderer's number of slots");
 	CHECK_CUDA(cudaMemcpyAsync(pixels, r.ltRecPixel, slots * sizeof(int32_t), cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(values, r.ltRecValue, r.ltRecFloats * sizeof(float), cudaMemcpyDeviceToHost, I.stream));

@@ -228,7 +228,9 @@ struct RendererState {
 	bool targetHitId = false;
 	bool targetLightness = false;  // light tracer targets (lt_params.hpp:14-17)
 	bool targetDensity = false;
-	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer", 2: "Bidirectional Pathtracer"
+	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer", 2: "Wireframe", 3: "Bidirectional Pathtracer"
+	WireParams wireParams{ 1.0f, 1000 }; // the wireframe renderer's "Line width" and "Maximum trace depth"
+	bool targetBorder = true;      // its "Border" target
 	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
 	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
 	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters

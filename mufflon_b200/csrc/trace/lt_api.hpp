@@ -46,4 +46,16 @@ size_t bpt_scratch_bytes(int maxPathLength);
 cudaError_t launch_bpt(const DScene& scene, const LtParams& params, const LtTargets& targets, void* scratch,
                        unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
 
+// wireframe_params.hpp:6-26
+struct WireParams {
+	float lineWidth;        // "Line width" in pixels (default 1)
+	int32_t maxTraceDepth;  // "Maximum trace depth" (default 1000)
+};
+
+// One wireframe iteration: one camera ray per pixel (generators in
+// targets.rngState), the "Border" value per pixel into targets.iter and its
+// running mean into targets.radiance. instToWorld: 12 floats per instance.
+cudaError_t launch_wireframe(const DScene& scene, const float* instToWorld, const WireParams& params,
+                             const LtTargets& targets, TraceCounters* counters, cudaStream_t stream);
+
 } // namespace mb

@@ -2658,6 +2658,114 @@ void bpt_iterate(BptState& st, int numThreads) {
 	}
 }
 
+// ---------------------------------------------------------------- wireframe renderer
+// wireframe_common.hpp:15-180 and cpu_wireframe.cpp:18-38: one camera ray per
+// pixel and iteration, walked through the surfaces until it passes within
+// "Line width" pixels of an edge (white) or leaves the scene (background).
+struct WireState {
+	const Scene* scene;
+	float lineWidth;
+	i32 maxTraceDepth;
+	std::vector<Pcg64> rngs;
+	std::vector<float> border; // cumulative mean, 3 per pixel
+	i32 iteration = -1;
+	Counters stats;
+};
+
+// wireframe_common.hpp:15-78: the point on the closest edge line (triangle
+// AB, AC, BC; quad AB, AC, BD, CD with (A, B, C, D) = (v0, v1, v3, v2))
+V3 closest_line_point(const V3* c, int n, V3 hit) {
+	const int e0[4] = { 0, 0, 1, 2 };
+	const int e1[4] = { 1, 2, n == 3 ? 2 : 3, 3 };
+	V3 best = { 0, 0, 0 };
+	float bestD = 0.0f;
+	for(int k = 0; k < (n == 3 ? 3 : 4); ++k) {
+		const V3 a = c[e0[k]], e = c[e1[k]] - a, ap = hit - a;
+		const V3 on = a + e * (dot(ap, e) / lensq(e));
+		const float d = lensq(on - hit);
+		if(k == 0 || d < bestD) { best = on; bestD = d; }
+	}
+	return best;
+}
+
+V3 wireframe_sample(const WireState& st, i32 px, i32 py, Pcg64& rng, Counters& cnt) {
+	const Scene& S = *st.scene;
+	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
+	const u64 x0 = rng.next();
+	(void)rng.next();
+	float pdf;
+	const V3 dir = pinhole_ray(S.cam, px, py, sample_uniform(u32(x0)), sample_uniform(u32(x0 >> 32)), pdf);
+	const V3 cam = S.cam.position;
+	V3 origin = cam;
+	float total = 0.0f;
+	for(i32 i = 0; i < st.maxTraceDepth; ++i) {
+		const Intersection hit = first_intersection(S, origin, dir, V3{ 0, 0, 0 }, MAX_SCENE_SIZE, cnt);
+		if(hit.inst < 0) {
+			const LightTree& T = S.lightTree;
+			if(T.hasBackground) {
+				const V3 bg = T.bgColor * T.bgScale;
+				if(any_pos(bg)) return bg;
+			}
+			return { 0, 0, 0 };
+		}
+		const float hitDist = hit.distance < 0.001f ? 0.001f : hit.distance;
+		const V3 p = origin + dir * hitDist;
+		total += hitDist;
+		const float pixelSize = total * S.cam.tanVFov / float(S.cam.resY);
+		const Mat34 m = instance_to_world(S.w2i[size_t(hit.inst)]);
+		const Lod& l = S.lods[S.instLod[size_t(hit.inst)]];
+		float rim;
+		if(u32(hit.prim) < l.nT + l.nQ) {
+			V3 c[4];
+			int n;
+			if(u32(hit.prim) < l.nT) {
+				for(int k = 0; k < 3; ++k) c[k] = xform_point(m, l.verts[l.idx[3 * size_t(hit.prim) + size_t(k)]]);
+				n = 3;
+			} else {
+				const size_t o = 3 * size_t(l.nT) + 4 * (size_t(hit.prim) - l.nT);
+				c[0] = xform_point(m, l.verts[l.idx[o]]);
+				c[1] = xform_point(m, l.verts[l.idx[o + 1]]);
+				c[2] = xform_point(m, l.verts[l.idx[o + 3]]);
+				c[3] = xform_point(m, l.verts[l.idx[o + 2]]);
+				n = 4;
+			}
+			const V3 seg = closest_line_point(c, n, p) - cam;
+			const V3 proj = seg - dir * dot(seg, dir);
+			rim = len(proj);
+		} else {
+			const i32 sidx = hit.prim - i32(l.nT + l.nQ);
+			const V3 center = xform_point(m, sphere_center(l, sidx));
+			const V3 toCenter = normalize(center - p);
+			rim = 0.05f * (sphere_radius(l, sidx) * dot(toCenter, dir));
+		}
+		if(rim > st.lineWidth * pixelSize) origin = origin + dir * hitDist;
+		else return { 1.0f, 1.0f, 1.0f };
+	}
+	return { 0, 0, 0 };
+}
+
+void wireframe_iterate(WireState& st, int numThreads) {
+	const Scene& S = *st.scene;
+	const i32 n = i32(S.width * S.height);
+	++st.iteration;
+	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	Counters total;
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(dynamic, 256)
+		for(i32 pixel = 0; pixel < n; ++pixel) {
+			const V3 v = wireframe_sample(st, pixel % i32(S.width), pixel / i32(S.width), st.rngs[size_t(pixel)], local);
+			const float it[3] = { v.x, v.y, v.z };
+			float* cr = &st.border[3 * size_t(pixel)];
+			for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += diff / den; }
+		}
+#pragma omp critical
+		total.add(local);
+	}
+	st.stats.add(total);
+}
+
 // ---------------------------------------------------------------- scene setup
 Scene* create_scene(const OrSceneDesc* d) {
 	auto S = std::make_unique<Scene>();
@@ -3152,6 +3260,26 @@ int oracle_bpt_stats(void* p, OrStats* o) {
 	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
 	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
 	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
+	return 1;
+}
+
+void* oracle_wireframe_create(void* s, float lineWidth, int32_t maxTraceDepth) {
+	Scene* S = static_cast<Scene*>(s);
+	auto* st = new WireState();
+	st->scene = S;
+	st->lineWidth = lineWidth;
+	st->maxTraceDepth = maxTraceDepth;
+	const i32 num = i32(S->width * S->height);
+	st->rngs.resize(size_t(num));
+	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i)); // cpu_wireframe.cpp:31-36
+	st->border.assign(size_t(num) * 3, 0.0f);
+	return st;
+}
+void oracle_wireframe_destroy(void* p) { delete static_cast<WireState*>(p); }
+int oracle_wireframe_iterate(void* p, int32_t nt) { wireframe_iterate(*static_cast<WireState*>(p), nt > 0 ? nt : 1); return 1; }
+int oracle_wireframe_get_target(void* p, float* out) {
+	const WireState* st = static_cast<const WireState*>(p);
+	std::memcpy(out, st->border.data(), st->border.size() * 4);
 	return 1;
 }
 

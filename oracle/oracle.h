@@ -165,6 +165,12 @@ int oracle_bpt_get_target(void* bpt, int32_t target, float* out);
  * index or -1, values[4k..4k+3] = radiance rgb and lightness as added. */
 int oracle_bpt_records(void* bpt, int32_t* pixels, float* values);
 int oracle_bpt_stats(void* bpt, OrStats* stats);
+/* Wireframe renderer (CpuWireframe equivalent, wireframe_common.hpp);
+ * the target is the cumulative "Border" image (3 channels). */
+void* oracle_wireframe_create(void* scene, float lineWidth, int32_t maxTraceDepth);
+void oracle_wireframe_destroy(void* wf);
+int oracle_wireframe_iterate(void* wf, int32_t numThreads);
+int oracle_wireframe_get_target(void* wf, float* out);
 /* Building blocks exposed for known-answer tests. */
 int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);

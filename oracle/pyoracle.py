@@ -107,6 +107,11 @@ def lib():
         L.oracle_bpt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.oracle_bpt_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_bpt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_wireframe_create.restype = C.c_void_p
+        L.oracle_wireframe_create.argtypes = [C.c_void_p, C.c_float, C.c_int32]
+        L.oracle_wireframe_destroy.argtypes = [C.c_void_p]
+        L.oracle_wireframe_iterate.argtypes = [C.c_void_p, C.c_int32]
+        L.oracle_wireframe_get_target.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_pcg64_seed.restype = C.c_uint64
         L.oracle_pcg64_seed.argtypes = [C.c_uint32]
         L.oracle_pcg64_next.restype = C.c_uint64
@@ -409,6 +414,34 @@ class OracleBidirPathTracer:
     def close(self):
         if self.handle:
             lib().oracle_bpt_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleWireframe:
+    """CPU restatement of the wireframe renderer (wireframe_common.hpp, cpu_wireframe.cpp)."""
+
+    def __init__(self, scene: OracleScene, line_width=1.0, max_trace_depth=1000):
+        self.scene = scene
+        self.handle = lib().oracle_wireframe_create(scene.handle, float(line_width), int(max_trace_depth))
+
+    def iterate(self, threads: int = 0):
+        lib().oracle_wireframe_iterate(self.handle, threads if threads > 0 else (os.cpu_count() or 1))
+
+    def target(self):
+        w, h = self.scene.spec.width, self.scene.spec.height
+        out = np.zeros((h, w, 3), np.float32)
+        lib().oracle_wireframe_get_target(self.handle, _ptr(out))
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().oracle_wireframe_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -47,7 +47,7 @@ def _gpu_bpt(spec, params, iterations, per_iteration=None):
     d = bindings.DllInterface()
     try:
         bindings.load_scene_spec(d, spec)
-        assert d.render_enable_renderer(2, 0)
+        assert d.render_enable_renderer(3, 0)
         for k, v in params.items():
             assert d.renderer_set_parameter_int(k, v)
         assert d.renderer_set_parameter_int("Record connections", 1)
@@ -107,11 +107,11 @@ def test_bpt_in_the_registry():
     d = bindings.DllInterface()
     try:
         core, I = d.core, d.muffInst
-        assert d.render_get_renderer_count() == 3
-        assert d.render_get_renderer_name(2) == "Bidirectional Pathtracer"
-        assert d.render_get_renderer_short_name(2) == "BPT"
-        assert core.render_get_renderer_devices(I, 2, 0) == 2  # DEVICE_CUDA
-        assert d.render_enable_renderer(2, 0)
+        assert d.render_get_renderer_count() == 4
+        assert d.render_get_renderer_name(3) == "Bidirectional Pathtracer"
+        assert d.render_get_renderer_short_name(3) == "BPT"
+        assert core.render_get_renderer_devices(I, 3, 0) == 2  # DEVICE_CUDA
+        assert d.render_enable_renderer(3, 0)
         assert [core.render_get_render_target_name(I, i).decode() for i in range(core.render_get_render_target_count(I))] == \
             ["Radiance", "Lightness"]
         assert d.renderer_set_parameter_int("Seed", 5)

@@ -1,0 +1,102 @@
+"""The CUDA "Wireframe" (core/wireframe.cu) against the oracle's restatement
+of the reference's CPU one (wireframe_common.hpp:93-180, cpu_wireframe.cpp:18-38).
+
+The cumulative "Border" image is compared bit for bit after each of two
+iterations (up to 1 pixel in 1000, see the test): camera rays with the per-pixel generator stream, the walk through
+the surfaces (each step re-traced from the hit point), the closest-edge
+distance of triangles and quads, the rim test of spheres, instance transforms
+and the background on a miss. The registry entry, the target list and the
+"Line width" parameter are tested too."""
+import numpy as np
+import pytest
+
+from mufflon_b200 import bindings, scenes
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "cornell": lambda: scenes.cornell_box(1, width=64, height=64),
+    "icosphere_env": lambda: scenes.displaced_icosphere(2, subdiv=3, width=64, height=36),
+    "panels_quads": lambda: scenes.emissive_panels(5, 6, 40, 2, width=64, height=48, emissive_triangles=12),
+    "instanced_spheres": lambda: scenes.instanced_scene(0, num_meshes=3, num_instances=64, num_spheres=300,
+                                                        tri_range=(500, 3000), width=64, height=48),
+}
+
+
+def _gpu_wireframe(spec, iterations, line_width=None, depth=None):
+    d = bindings.DllInterface()
+    out = []
+    try:
+        bindings.load_scene_spec(d, spec)
+        assert d.render_enable_renderer(2, 0)
+        if line_width is not None:
+            assert d.renderer_set_parameter_float("Line width", line_width)
+        if depth is not None:
+            assert d.renderer_set_parameter_int("Maximum trace depth", depth)
+        d.render_enable_render_target("Border", False)
+        for _ in range(iterations):
+            d.render_iterate()
+            out.append(d.get_target_image("Border").copy())
+        return out
+    finally:
+        d.close()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("line_width,depth", [(None, None), (3.5, 4)], ids=["default", "wide_depth4"])
+def test_wireframe_border_matches_oracle(oracle, case, line_width, depth):
+    spec = CASES[case]()
+    imgs = _gpu_wireframe(spec, 2, line_width, depth)
+    ow = oracle.OracleWireframe(oracle.OracleScene(spec), 1.0 if line_width is None else line_width,
+                                1000 if depth is None else depth)
+    for img in imgs:
+        ow.iterate()
+        ref = ow.target()
+        assert img.shape == ref.shape
+        # A walk re-traces from each hit point without an offset, so a ray can
+        # start within 1e-7 of a second, coplanar surface (a box standing on
+        # the floor) and meet it at t ~ 4e-7, where the last bits of the
+        # object-space transform decide hit or miss. At most 1 pixel in 1000
+        # may take the other branch; all others are bit-identical.
+        differ = np.any(img.view(np.uint32) != ref.view(np.uint32), axis=-1)
+        assert int(differ.sum()) <= max(1, differ.size // 1000)
+    # some pixels are edges, some are not
+    assert 0.0 < float(np.mean(imgs[-1][..., 0] == 1.0)) < 1.0
+
+
+def test_wireframe_in_the_registry():
+    d = bindings.DllInterface()
+    try:
+        core, I = d.core, d.muffInst
+        assert d.render_get_renderer_name(2) == "Wireframe"
+        assert d.render_get_renderer_short_name(2) == "WF"
+        assert core.render_get_renderer_devices(I, 2, 0) == 2  # DEVICE_CUDA
+        assert d.render_enable_renderer(2, 0)
+        assert [core.render_get_render_target_name(I, i).decode() for i in range(core.render_get_render_target_count(I))] == \
+            ["Border"]
+        names = [core.renderer_get_parameter_desc(I, i, None).decode() for i in range(core.renderer_get_num_parameters(I))]
+        assert names == ["Line width", "Maximum trace depth"]
+        assert d.renderer_get_parameter_float("Line width") == 1.0
+        assert d.renderer_get_parameter_int("Maximum trace depth") == 1000
+        assert d.renderer_set_parameter_float("Line width", 2.0)
+        assert not d.renderer_set_parameter_int("Seed", 1)
+        assert d.render_enable_renderer(0, 0)
+        assert d.renderer_get_parameter_int("Seed") == 0
+        assert d.render_enable_renderer(2, 0)
+        assert d.renderer_get_parameter_float("Line width") == 2.0
+    finally:
+        d.close()
+
+
+def test_wireframe_radiance_is_not_a_target():
+    spec = CASES["cornell"]()
+    d = bindings.DllInterface()
+    try:
+        bindings.load_scene_spec(d, spec)
+        assert d.render_enable_renderer(2, 0)
+        d.render_enable_render_target("Border", False)
+        d.render_iterate()
+        with pytest.raises(bindings.MufflonError):
+            d.get_target_image("Radiance")
+    finally:
+        d.close()
