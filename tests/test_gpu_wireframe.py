@@ -54,10 +54,11 @@ def test_wireframe_border_matches_oracle(oracle, case, line_width, depth):
         ref = ow.target()
         assert img.shape == ref.shape
         # A walk re-traces from each hit point without an offset, so a ray can
-        # start within 1e-7 of a second, coplanar surface (a box standing on
-        # the floor) and meet it at t ~ 4e-7, where the last bits of the
-        # object-space transform decide hit or miss. At most 1 pixel in 1000
-        # may take the other branch; all others are bit-identical.
+        # start within 1e-7 of two coplanar surfaces (the bottom face of a box
+        # standing on the floor, and the floor) and meet both at t ~ 4e-7;
+        # the last bits of the instance transform then pick the closer one.
+        # At most 1 pixel in 1000 may take the other branch; all others are
+        # bit-identical.
         differ = np.any(img.view(np.uint32) != ref.view(np.uint32), axis=-1)
         assert int(differ.sum()) <= max(1, differ.size // 1000)
     # some pixels are edges, some are not
