@@ -433,9 +433,13 @@ CORE_API Boolean CDECL mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint3
  * cudaMalloc/cudaFree (they may synchronise the device). The scratch space is
  * a fixed array of about 12.3 MiB inside the library, held by every GPU that
  * loads the library until the process exits; n above
- * MUFFLON_SORT_NOALLOC_MAX_PAIRS is rejected with an error. The first call on
- * a device looks up the array's address on that device (make it before any
- * stream capture). All calls share the array, so calls that overlap on the
+ * MUFFLON_SORT_NOALLOC_MAX_PAIRS is rejected with an error. Set-up:
+ * mufflon_initialize looks up the array's address on the device it selects
+ * and loads the sort's kernels there; on any other device the first call does
+ * it. That set-up loads the library's device code, which takes device memory
+ * under CUDA's lazy module loading, so it must come before the caller
+ * reserves its device memory and before any stream capture. Later calls take
+ * no device memory. All calls share the array, so calls that overlap on the
  * GPU race. keys/values are device pointers owned by the caller; stream is a
  * cudaStream_t (NULL: default stream); the call returns after the pairs are
  * sorted. */

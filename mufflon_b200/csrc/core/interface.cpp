@@ -57,15 +57,16 @@ const ParamDesc PT_PARAMS[] = {
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
 	{ "Stage timing", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
 	{ "Trace refill lanes", PARAM_INT }, { "Tail paths", PARAM_INT }, { "Iteration graph", PARAM_INT },
-	{ "Planned tail", PARAM_INT },
+	{ "Planned tail", PARAM_INT }, { "Traversal step limit", PARAM_INT },
 };
 // lt_params.hpp:8-12, plus the recording switch of the parity tests
 const ParamDesc LT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
-	{ "Record connections", PARAM_INT },
+	{ "Record connections", PARAM_INT }, { "Traversal step limit", PARAM_INT },
 };
 // wireframe_params.hpp:6-26
-const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT } };
+const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT },
+                                  { "Traversal step limit", PARAM_INT } };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
 // implements Radiance and Hit ID; the others are recognised names.
 const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
@@ -74,6 +75,9 @@ const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albe
 const char* LT_TARGETS[] = { "Radiance", "Lightness", "Density" };
 
 int32_t* param_ptr(RendererState& r, const char* name) {
+	// every renderer: the traversal steps a ray may take before it is
+	// abandoned, which fails the iteration (0: the default limit)
+	if(!std::strcmp(name, "Traversal step limit")) return &r.stepLimit;
 	if(r.kind == 2) {
 		if(!std::strcmp(name, "Maximum trace depth")) return &r.wireParams.maxTraceDepth;
 		return nullptr;
@@ -107,6 +111,17 @@ size_t read_bulk(const BulkLoader* b, void* dst, size_t bytes) {
 	if(!b) return 0;
 	if(b->type == BULK_ARRAY) { std::memcpy(dst, b->descriptor.bytes, bytes); return bytes; }
 	return std::fread(dst, 1, bytes, b->descriptor.file);
+}
+
+int32_t step_limit(const RendererState& r) { return r.stepLimit > 0 ? r.stepLimit : MAX_TRAVERSAL_STEPS; }
+
+// The reference's error convention (interface.cpp:53-83) for rays whose
+// traversal was abandoned: the call fails with a message rather than
+// returning an image with silently wrong pixels.
+void check_traversal(unsigned errors, int32_t limit) {
+	if(errors)
+		throw ApiError("traversal abandoned " + std::to_string(errors) + " rays (step limit of " + std::to_string(limit) +
+		               " exceeded or traversal stack overflow); the result of this call is incomplete");
 }
 
 void ensure_render_buffers(MufflonInstance& I) {
@@ -223,7 +238,7 @@ void iterate_lt(MufflonInstance& I) {
 	r.lastShadow = TraceCounters{};
 	r.lastLaunches = 2;
 	for(float& m : r.stageMs) m = 0.0f;
-	if(c.errors) log_msg(LOG_WARNING, "traversal stack overflow in " + std::to_string(c.errors) + " rays");
+	check_traversal(c.errors, S.maxSteps);
 }
 
 // Brings in, through the registered LoD loader, every LoD the current
@@ -312,6 +327,9 @@ MufflonInstanceHdl mufflon_initialize(void) {
 		if(p.unifiedAddressing && cc > bestCc) { best = d; bestCc = cc; }
 	}
 	CHECK_CUDA(cudaSetDevice(best));
+	// The allocation-free sort's device array and kernels are loaded now, so
+	// that its later calls on this device take no device memory.
+	CHECK_CUDA(noalloc_prepare_current_device());
 	auto* I = new MufflonInstance();
 	I->device = best;
 	CHECK_CUDA(cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking));
@@ -1081,6 +1099,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	load_scene_if_needed(I);
 	ensure_render_buffers(I);
 	RendererState& r = I.renderer;
+	I.scene.desc.maxSteps = step_limit(r);
 	const uint32_t n = r.width * r.height;
 	if(r.kind != 0) ensure_lt_buffers(I);
 	if(r.needsReset) {
@@ -1225,7 +1244,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	if(preTime) { preTime->cycles = 0; preTime->microseconds = us(t1 - t0); }
 	if(iterTime) { iterTime->cycles = 0; iterTime->microseconds = us(t2 - t1); }
 	if(postTime) { postTime->cycles = 0; postTime->microseconds = 0; }
-	if(r.lastCounters.errors) log_msg(LOG_WARNING, "traversal stack overflow in " + std::to_string(r.lastCounters.errors) + " rays");
+	check_traversal(r.lastCounters.errors, I.scene.desc.maxSteps);
 	return true;
 	CATCH_ALL(false)
 }
@@ -1505,6 +1524,7 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 		CHECK((in.neeCount > 0 ? in.neeCount : 1) == nee, "all jobs of a batch must use the same NEE count");
 		DJob& d = hj[j];
 		d.scene = I.scene.desc;
+		d.scene.maxSteps = step_limit(I.renderer);
 		d.scene.camera.resX = uint16_t(w);
 		d.scene.camera.resY = uint16_t(h);
 		d.params = PtParams{ in.seed, in.minPathLength, in.maxPathLength, nee, in.rrStartDepth };
@@ -1607,6 +1627,11 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	if(graph) cudaGraphDestroy(graph);
 	CHECK_CUDA(se);
 	CHECK_CUDA(cudaGetLastError());
+	{
+		TraceCounters tc[2];
+		CHECK_CUDA(cudaMemcpy(tc, counters, sizeof(tc), cudaMemcpyDeviceToHost));
+		check_traversal(tc[0].errors + tc[1].errors, hj[0].scene.maxSteps);
+	}
 	if(jobDoneMs)
 		for(uint32_t j = 0; j < count; ++j) {
 			float ms = 0.0f;
@@ -1667,6 +1692,7 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 	const uint32_t w = I.current->width, hgt = I.current->height;
 	const size_t n = size_t(w) * hgt, nt = size_t(t->width) * t->height;
 	DScene desc = I.scene.desc;
+	desc.maxSteps = step_limit(r);
 	desc.camera.resX = uint16_t(w);
 	desc.camera.resY = uint16_t(hgt);
 	uint64_t* rng = nullptr;
@@ -1699,6 +1725,7 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		tune.wavefrontBounces = r.wavefrontBounces;
 		tune.refillLanes = r.refillLanes;
 		tune.tailPaths = r.tailPaths;
+		if(wavefront) CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 		for(uint32_t s = 0; s < spp; ++s) {
 			if(wavefront)
 				CHECK_CUDA(launch_adjoint_wavefront(desc, r.params, rng, w, hgt, r.wf, adjMem, r.params.maxPathLength, texIndex,
@@ -1708,8 +1735,11 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		}
 		CHECK_CUDA(cudaEventRecord(b, I.stream));
 		CHECK_CUDA(cudaMemcpyAsync(textureGrad, dGrad, nt * 12, cudaMemcpyDeviceToHost, I.stream));
+		TraceCounters tc[2] = {};
+		if(wavefront) CHECK_CUDA(cudaMemcpyAsync(tc, r.counters, sizeof(tc), cudaMemcpyDeviceToHost, I.stream));
 		CHECK_CUDA(cudaStreamSynchronize(I.stream));
 		if(deviceMs) CHECK_CUDA(cudaEventElapsedTime(deviceMs, a, b));
+		check_traversal(tc[0].errors + tc[1].errors, desc.maxSteps);
 	} catch(...) {
 		cleanup();
 		throw;
@@ -1908,6 +1938,7 @@ Boolean mufflon_measure_l2_bandwidth(uint64_t bytes, int32_t reps, float* gbs) {
 }
 
 // Allocation-free sort: launches and memsets only (sort_noalloc.cu).
+static_assert(NOALLOC_MAX_PAIRS == MUFFLON_SORT_NOALLOC_MAX_PAIRS, "the public limit is the implementation's");
 Boolean mufflon_sort_pairs_device_noalloc(uint64_t* keys, int32_t* values, uint32_t n, void* stream) {
 	TRY
 	CHECK(n <= NOALLOC_MAX_PAIRS, "n = " + std::to_string(n) + " exceeds the maximum of " +

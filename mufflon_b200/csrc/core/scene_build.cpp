@@ -468,6 +468,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	S.lods = D.dLods; S.numLods = uint32_t(D.lods.size());
 	S.worldToInstance = D.dW2I; S.instanceLod = D.dInstLod; S.numInstances = numInst;
 	S.activeInstances = active; S.validInstance = valid;
+	S.maxSteps = MAX_TRAVERSAL_STEPS;
 	S.tlasNodes = D.tlas.nodes; S.tlasPrimIds = D.tlas.primIds; S.tlasNumInternal = D.tlas.numInternal;
 	S.tlasWide = D.tlas.wnodes; S.tlasWidePrims = D.tlas.wprims; S.tlasNumWide = D.tlas.numWide;
 	S.materials = D.dMaterials; S.textures = D.dTextures;

@@ -212,6 +212,7 @@ struct RendererState {
 	int32_t tailPaths = 98304;    // queue length at or below which the tail launch takes over
 	int32_t iterationGraph = 1;   // replay the wavefront launches of an iteration as one CUDA graph
 	int32_t planTail = 1;         // plan the tail bounce from the previous iteration's queue lengths
+	int32_t stepLimit = 0;        // "Traversal step limit" of every renderer; 0: MAX_TRAVERSAL_STEPS
 	std::vector<unsigned char> planKey;
 	int32_t plannedTail = -1;
 	cudaGraphExec_t graphExec = nullptr;

@@ -17,8 +17,12 @@
 //     and calls that overlap on the GPU (different streams, or threads) race;
 //   * host code cannot use the array's name as a device address; the address
 //     is looked up with cudaGetSymbolAddress once per device, with that device
-//     current, by the first call made on that device (make that first call
-//     before any stream capture).
+//     current. mufflon_initialize does this for the device it selects (through
+//     noalloc_prepare_current_device); on any other device the first call does
+//     it. The look-up, and loading the sort's kernels with it, loads this
+//     file's device code onto the device, which takes device memory under
+//     CUDA's lazy module loading: so the set-up must come before the caller
+//     reserves its device memory, and before any stream capture.
 #include "radix_sort.cuh"
 #include "sort_noalloc.hpp"
 
@@ -54,6 +58,11 @@ cudaError_t scratch_for_current_device(unsigned char** base) {
 		if((e = cudaGetSymbolAddress(&p, g_sortScratch)) != cudaSuccess) return e;
 		if((e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SORT_SMEM))) != cudaSuccess)
 			return e;
+		// Load the other two kernels now as well: under lazy loading their
+		// first launch would otherwise load their code into device memory.
+		cudaFuncAttributes attr;
+		if((e = cudaFuncGetAttributes(&attr, k_sort_hist)) != cudaSuccess) return e;
+		if((e = cudaFuncGetAttributes(&attr, k_sort_scan)) != cudaSuccess) return e;
 		g_scratchAddress[dev] = static_cast<unsigned char*>(p);
 	}
 	*base = g_scratchAddress[dev];
@@ -63,6 +72,11 @@ cudaError_t scratch_for_current_device(unsigned char** base) {
 } // namespace
 
 size_t noalloc_scratch_bytes() { return NA_BYTES; }
+
+cudaError_t noalloc_prepare_current_device() {
+	unsigned char* base = nullptr;
+	return scratch_for_current_device(&base);
+}
 
 cudaError_t sort_pairs_noalloc(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream, bool* waitExpired) {
 	if(waitExpired) *waitExpired = false;

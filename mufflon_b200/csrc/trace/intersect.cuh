@@ -20,7 +20,6 @@ namespace mb {
 
 constexpr int BLAS_STACK = 100;
 constexpr int TLAS_STACK = 64;
-constexpr int MAX_TRAVERSAL_STEPS = 1 << 22;
 
 struct FastRay {
 	f3 o, d, inv;
@@ -282,13 +281,13 @@ MBD NodePair load_pair(const BvhNode* nodes, int node) {
 // stack overflowed.
 template < class TmaxFn, class LeafFn >
 MBD bool traverse(const BvhNode* nodes, int nInt, const FastRay& ray, TmaxFn&& tmaxFn, LeafFn&& leaf,
-                  int2* stack, int capacity, LocalCounters& cnt) {
+                  int2* stack, int capacity, int maxSteps, LocalCounters& cnt) {
 	int sp = 0;
 	int node = 0;
 	// A well-formed BVH visits each node at most once; the cap only guards
 	// against a corrupted hierarchy (it records an error instead of spinning).
 	for(int guard = 0;; ++guard) {
-		if(guard >= MAX_TRAVERSAL_STEPS) { ++cnt.errors; return false; }
+		if(guard >= maxSteps) { ++cnt.errors; return false; }
 		++cnt.nodes;
 		const NodePair np = load_pair(nodes, node);
 		const float tmaxBox = tmaxFn();
@@ -357,7 +356,7 @@ MBD void blas_closest(const DScene& S, uint32_t inst, f3 o, f3 d, HitRec& best, 
 	traverse(l.nodes, l.numInternal, ir.ray,
 		[&]() { return best.t * ir.scale * BOX_SLACK; },
 		[&](int first, int count) { for(int k = 0; k < count; ++k) consider(first + k); return true; },
-		stack, BLAS_STACK, cnt);
+		stack, BLAS_STACK, S.maxSteps, cnt);
 }
 
 MBD bool blas_any(const DScene& S, uint32_t inst, f3 o, f3 d, float tmaxWorld, LocalCounters& cnt, int2* stack) {
@@ -386,7 +385,7 @@ MBD bool blas_any(const DScene& S, uint32_t inst, f3 o, f3 d, float tmaxWorld, L
 			for(int k = 0; k < count; ++k) if(test(first + k)) { hit = true; return false; }
 			return true;
 		},
-		stack, BLAS_STACK, cnt);
+		stack, BLAS_STACK, S.maxSteps, cnt);
 	return hit;
 }
 
@@ -428,7 +427,7 @@ MBD HitRec closest_hit(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters&
 				for(int k = 0; k < count; ++k) blas_closest(S, uint32_t(__ldg(S.tlasPrimIds + first + k)), o, dir, best, cnt, bstack);
 				return true;
 			},
-			tstack, TLAS_STACK, cnt);
+			tstack, TLAS_STACK, S.maxSteps, cnt);
 	}
 	return best;
 }
@@ -526,7 +525,7 @@ MBD bool occluded(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt,
 				if(blas_any(S, uint32_t(__ldg(S.tlasPrimIds + first + k)), a, dir, tmax, cnt, bstack)) { occ = true; return false; }
 			return true;
 		},
-		tstack, TLAS_STACK, cnt);
+		tstack, TLAS_STACK, S.maxSteps, cnt);
 	return occ;
 }
 

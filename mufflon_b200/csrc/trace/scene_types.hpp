@@ -88,6 +88,9 @@ struct DCamera {
 	uint16_t resX, resY;
 };
 
+// Default traversal step limit of a ray (DScene::maxSteps).
+constexpr int32_t MAX_TRAVERSAL_STEPS = 1 << 22;
+
 struct DScene {
 	const DLod* lods;
 	uint32_t numLods;
@@ -119,6 +122,11 @@ struct DScene {
 	float bgColor[3], bgScale[3];
 	float aabbMin[3], aabbMax[3];
 	DCamera camera;
+	// Traversal steps a ray may take (per traversal loop of the binary
+	// hierarchies, per ray of the 8-wide ones) before it is abandoned and
+	// counted as an error; MAX_TRAVERSAL_STEPS unless the renderer parameter
+	// "Traversal step limit" sets it.
+	int32_t maxSteps;
 };
 
 struct PtParams {

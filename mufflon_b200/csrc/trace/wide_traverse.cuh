@@ -133,7 +133,7 @@ struct WideTracer {
 	const DLod* lod;
 	const WideNode* nodes;
 	uint32_t flip, ngBase, ngImask, ngHits, pgBase, pgHits;
-	int inst, sp, instSp, steps;
+	int inst, sp, instSp, steps; // steps: what is left of the scene's step limit
 	bool any, single, occluded, done;
 
 	MBD void init(const DScene& S, f3 o, f3 d, float tmax, bool anyHit, LocalCounters& cnt) {
@@ -142,7 +142,7 @@ struct WideTracer {
 		any = anyHit;
 		occluded = false;
 		best.t = tmax; best.inst = -1; best.prim = -1; best.sp = make2(0.0f, 0.0f); best.has = false;
-		sp = 0; instSp = -1; steps = 0; inst = -1; lod = nullptr;
+		sp = 0; instSp = -1; steps = S.maxSteps; inst = -1; lod = nullptr;
 		scale = 1.0f;
 		ngBase = 0; ngImask = 1; ngHits = 0; pgBase = 0; pgHits = 0;
 		single = S.activeInstances == 1;
@@ -175,7 +175,7 @@ struct WideTracer {
 	template < class Stack >
 	MBD bool step(const DScene& S, LocalCounters& cnt, Stack& stack) {
 		if(done) return true;
-		if(++steps > MAX_TRAVERSAL_STEPS) { ++cnt.errors; done = true; return true; }
+		if(--steps < 0) { ++cnt.errors; done = true; return true; }
 		if(ngHits) {
 			const uint32_t k = uint32_t(__ffs(int(ngHits)) - 1);
 			ngHits &= ngHits - 1u;

@@ -20,21 +20,29 @@ MBD f3 xform34(const float* m, f3 p) {
 }
 
 // wireframe_common.hpp:15-41 (triangle) and 43-78 (quad): the point on the
-// closest edge line
+// closest edge line. Edge k is chosen if its distance is <= every other
+// edge's, tried in order, else the last edge (the reference's comparison
+// chain, :36-41 and :70-77): a NaN distance from a zero-length edge never
+// wins a comparison, so such a triangle falls through to its last edge.
 MBD f3 closest_line_point(const f3* c, int n, f3 hit) {
 	// edges: triangle AB, AC, BC; quad AB, AC, BD, CD with (A, B, C, D) = (v0, v1, v3, v2)
-	const int e0[4] = { 0, 0, n == 3 ? 1 : 1, 2 };
+	const int e0[4] = { 0, 0, 1, 2 };
 	const int e1[4] = { 1, 2, n == 3 ? 2 : 3, 3 };
 	const int ne = n == 3 ? 3 : 4;
-	f3 best = make3(0.0f, 0.0f, 0.0f);
-	float bestD = 0.0f;
+	f3 on[4];
+	float d[4];
 	for(int k = 0; k < ne; ++k) {
 		const f3 a = c[e0[k]], e = c[e1[k]] - a, ap = hit - a;
-		const f3 on = a + e * __fdiv_rn(dot(ap, e), lensq(e));
-		const float d = lensq(on - hit);
-		if(k == 0 || d < bestD) { best = on; bestD = d; }
+		on[k] = a + e * __fdiv_rn(dot(ap, e), lensq(e));
+		d[k] = lensq(on[k] - hit);
 	}
-	return best;
+	for(int k = 0; k + 1 < ne; ++k) {
+		bool closest = true;
+		for(int j = 0; j < ne; ++j)
+			if(j != k && !(d[k] <= d[j])) closest = false;
+		if(closest) return on[k];
+	}
+	return on[ne - 1];
 }
 
 __global__ void k_wireframe(const DScene S, const float* instToWorld, WireParams P, uint64_t* rngState, float4* iter,

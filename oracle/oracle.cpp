@@ -2673,19 +2673,28 @@ struct WireState {
 };
 
 // wireframe_common.hpp:15-78: the point on the closest edge line (triangle
-// AB, AC, BC; quad AB, AC, BD, CD with (A, B, C, D) = (v0, v1, v3, v2))
+// AB, AC, BC; quad AB, AC, BD, CD with (A, B, C, D) = (v0, v1, v3, v2)).
+// The choice is the reference's chain (:36-41, :70-77): edge k wins if its
+// distance is <= every other's, tried in order, else the last edge; so with a
+// NaN distance (a zero-length edge) the chain falls through to the last edge.
 V3 closest_line_point(const V3* c, int n, V3 hit) {
 	const int e0[4] = { 0, 0, 1, 2 };
 	const int e1[4] = { 1, 2, n == 3 ? 2 : 3, 3 };
-	V3 best = { 0, 0, 0 };
-	float bestD = 0.0f;
-	for(int k = 0; k < (n == 3 ? 3 : 4); ++k) {
+	const int ne = n == 3 ? 3 : 4;
+	V3 on[4];
+	float d[4];
+	for(int k = 0; k < ne; ++k) {
 		const V3 a = c[e0[k]], e = c[e1[k]] - a, ap = hit - a;
-		const V3 on = a + e * (dot(ap, e) / lensq(e));
-		const float d = lensq(on - hit);
-		if(k == 0 || d < bestD) { best = on; bestD = d; }
+		on[k] = a + e * (dot(ap, e) / lensq(e));
+		d[k] = lensq(on[k] - hit);
 	}
-	return best;
+	for(int k = 0; k + 1 < ne; ++k) {
+		bool closest = true;
+		for(int j = 0; j < ne; ++j)
+			if(j != k && !(d[k] <= d[j])) closest = false;
+		if(closest) return on[k];
+	}
+	return on[ne - 1];
 }
 
 V3 wireframe_sample(const WireState& st, i32 px, i32 py, Pcg64& rng, Counters& cnt) {

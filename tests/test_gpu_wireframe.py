@@ -2,11 +2,13 @@
 of the reference's CPU one (wireframe_common.hpp:93-180, cpu_wireframe.cpp:18-38).
 
 The cumulative "Border" image is compared bit for bit after each of two
-iterations (up to 1 pixel in 1000, see the test): camera rays with the per-pixel generator stream, the walk through
+iterations (one documented pixel of the Cornell box excepted): camera rays with the per-pixel generator stream, the walk through
 the surfaces (each step re-traced from the hit point), the closest-edge
 distance of triangles and quads, the rim test of spheres, instance transforms
 and the background on a miss. The registry entry, the target list and the
 "Line width" parameter are tested too."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -14,13 +16,31 @@ from mufflon_b200 import bindings, scenes
 
 pytestmark = pytest.mark.gpu
 
+
+def _degenerate_quad_room():
+    """The Cornell box's walls and light without the two boxes, with the back
+    wall's last two corners made equal: a quad with a zero-length edge, whose
+    closest-edge distance is NaN for that edge (the reference's comparison
+    chain then falls through to its last edge)."""
+    spec = scenes.cornell_box(1, width=64, height=64)
+    walls = spec.lods[0]
+    v = walls.vertices.copy()
+    v[11] = v[10]
+    lods = [dataclasses.replace(walls, vertices=v), spec.lods[-1]]
+    return dataclasses.replace(spec, lods=lods, world_to_instance=spec.world_to_instance[[0, -1]],
+                               instance_lod=np.array([0, 1], np.uint32))
+
+
 CASES = {
     "cornell": lambda: scenes.cornell_box(1, width=64, height=64),
     "icosphere_env": lambda: scenes.displaced_icosphere(2, subdiv=3, width=64, height=36),
     "panels_quads": lambda: scenes.emissive_panels(5, 6, 40, 2, width=64, height=48, emissive_triangles=12),
     "instanced_spheres": lambda: scenes.instanced_scene(0, num_meshes=3, num_instances=64, num_spheres=300,
                                                         tri_range=(500, 3000), width=64, height=48),
+    "degenerate_quad": _degenerate_quad_room,
 }
+# Pixels allowed to differ from the oracle, per case (see the test).
+ALLOWED_DIFF = {"cornell": 1}
 
 
 def _gpu_wireframe(spec, iterations, line_width=None, depth=None):
@@ -57,10 +77,10 @@ def test_wireframe_border_matches_oracle(oracle, case, line_width, depth):
         # start within 1e-7 of two coplanar surfaces (the bottom face of a box
         # standing on the floor, and the floor) and meet both at t ~ 4e-7;
         # the last bits of the instance transform then pick the closer one.
-        # At most 1 pixel in 1000 may take the other branch; all others are
-        # bit-identical.
+        # On the Cornell box 1 pixel of 4096 takes the other branch; every
+        # other case is bit-identical.
         differ = np.any(img.view(np.uint32) != ref.view(np.uint32), axis=-1)
-        assert int(differ.sum()) <= max(1, differ.size // 1000)
+        assert int(differ.sum()) <= ALLOWED_DIFF.get(case, 0), np.argwhere(differ)
     # some pixels are edges, some are not
     assert 0.0 < float(np.mean(imgs[-1][..., 0] == 1.0)) < 1.0
 
@@ -76,7 +96,7 @@ def test_wireframe_in_the_registry():
         assert [core.render_get_render_target_name(I, i).decode() for i in range(core.render_get_render_target_count(I))] == \
             ["Border"]
         names = [core.renderer_get_parameter_desc(I, i, None).decode() for i in range(core.renderer_get_num_parameters(I))]
-        assert names == ["Line width", "Maximum trace depth"]
+        assert names == ["Line width", "Maximum trace depth", "Traversal step limit"]
         assert d.renderer_get_parameter_float("Line width") == 1.0
         assert d.renderer_get_parameter_int("Maximum trace depth") == 1000
         assert d.renderer_set_parameter_float("Line width", 2.0)
