@@ -528,13 +528,13 @@ class DllInterface:
         return self.core.instance_set_transformation_matrix(self.muffInst, instHdl, byref(mat), int(isWorldToInst)) != 0
 
     # -- image readback
-    def get_target_image(self, targetName: str, copy: bool = True) -> np.ndarray:
-        """Cumulative mean of a target as (height, width, channels) float32, y = 0 first. With
-        copy=False the array is a view of the library's page-locked read-back buffer, valid until the
-        next call of this function (the C API's ownership rule)."""
+    def get_target_image(self, targetName: str, copy: bool = True, variance: bool = False) -> np.ndarray:
+        """Cumulative mean of a target (with variance=True: its recorded variance) as (height, width,
+        channels) float32, y = 0 first. With copy=False the array is a view of the library's page-locked
+        read-back buffer, valid until the next call of this function (the C API's ownership rule)."""
         p = POINTER(c_float)()
-        self._check(self.core.mufflon_get_target_image(self.muffInst, targetName.encode(), 0, byref(p)),
-                    "mufflon_get_target_image")
+        self._check(self.core.mufflon_get_target_image(self.muffInst, targetName.encode(), 1 if variance else 0,
+                                                       byref(p)), "mufflon_get_target_image")
         ch = c_int(0)
         self.core.mufflon_get_target_image_num_channels(self.muffInst, byref(ch))
         if not p:

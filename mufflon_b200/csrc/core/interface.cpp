@@ -142,6 +142,23 @@ void ensure_render_buffers(MufflonInstance& I) {
 	r.needsReset = true;
 }
 
+// Variance buffers of the targets whose variance is recorded (grow-only until
+// the resolution changes; cleared at every reset).
+void ensure_variance_buffers(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	const size_t n = size_t(r.width) * r.height;
+	auto need = [&](float*& buf, bool on, size_t channels) {
+		if(on && !buf) {
+			CHECK_CUDA(cudaMalloc(&buf, n * channels * sizeof(float)));
+			CHECK_CUDA(cudaMemsetAsync(buf, 0, n * channels * sizeof(float), I.stream));
+		}
+	};
+	need(r.radianceVar, r.varRadiance || r.varBorder, 3);
+	need(r.hitIdVar, r.varHitId, 2);
+	need(r.lightnessVar, r.varLightness, 1);
+	need(r.densityMean, r.varDensity, 1);
+}
+
 // Wavefront state for the current resolution and NEE count (one slab).
 void ensure_wavefront_buffers(MufflonInstance& I) {
 	RendererState& r = I.renderer;
@@ -214,6 +231,9 @@ void iterate_lt(MufflonInstance& I) {
 	t.radiance = r.targetRadiance ? r.radiance : nullptr;
 	t.lightness = r.targetLightness ? r.lightness : nullptr;
 	t.density = r.targetDensity ? r.density : nullptr;
+	t.radianceVar = r.targetRadiance && r.varRadiance ? r.radianceVar : nullptr;
+	t.lightnessVar = r.targetLightness && r.varLightness ? r.lightnessVar : nullptr;
+	t.densityMean = r.targetDensity && r.varDensity ? r.densityMean : nullptr;
 	t.recPixel = r.ltRecSlots ? r.ltRecPixel : nullptr;
 	t.recValue = r.ltRecSlots ? r.ltRecValue : nullptr;
 	t.width = r.width; t.height = r.height;
@@ -222,10 +242,13 @@ void iterate_lt(MufflonInstance& I) {
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
 	if(r.kind == 3) {
 		t.density = nullptr;
+		t.densityMean = nullptr;
 		CHECK_CUDA(launch_bpt(S, r.bptParams, t, r.bptScratch, r.workCounter, r.counters, I.stream));
 	} else if(r.kind == 2) {
 		t.radiance = r.radiance; // the "Border" target
+		t.radianceVar = r.varBorder ? r.radianceVar : nullptr;
 		t.lightness = nullptr; t.density = nullptr; t.recPixel = nullptr; t.recValue = nullptr;
+		t.lightnessVar = nullptr; t.densityMean = nullptr;
 		CHECK_CUDA(launch_wireframe(S, I.scene.dInstI2W, r.wireParams, t, r.counters, I.stream));
 	} else CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
@@ -292,6 +315,8 @@ void RendererState::release() {
 	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0; ltRecFloats = 0;
 	cudaFree(bptScratch);
 	bptScratch = nullptr; bptScratchBytes = 0;
+	cudaFree(radianceVar); cudaFree(hitIdVar); cudaFree(lightnessVar); cudaFree(densityMean);
+	radianceVar = nullptr; hitIdVar = nullptr; lightnessVar = nullptr; densityMean = nullptr;
 	if(screen) cudaFreeHost(screen);
 	screen = nullptr; screenCap = 0;
 	if(evStart) cudaEventDestroy(evStart);
@@ -388,30 +413,30 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	CHECK(I.renderer.enabled, "no renderer enabled");
 	CHECK(name != nullptr, "target name is null");
-	CHECK(!variance, "variance targets are not recorded by this renderer");
 	RendererState& r = I.renderer;
 	if(!r.rng || r.iteration < 0) { if(ptr) *ptr = nullptr; return true; }
 	const size_t n = size_t(r.width) * r.height;
+	// output_handler.hpp:301-318: the cumulative buffer, or with `variance`
+	// the variance buffer, which must be recorded
+	auto read = [&](const char* tname, bool enabled, bool varEnabled, const float* cum, const float* var, int channels) {
+		CHECK(enabled, std::string("target '") + tname + "' is not enabled");
+		CHECK(!variance || varEnabled, std::string("render target '") + tname + "' does not record variance");
+		const float* src = variance ? var : cum;
+		CHECK(src != nullptr, "no image yet");
+		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * size_t(channels)), src, n * size_t(channels) * sizeof(float),
+		                           cudaMemcpyDeviceToHost, I.stream));
+		r.screenChannels = channels;
+	};
 	if(!std::strcmp(name, "Radiance") && r.kind != 2) {
-		CHECK(r.targetRadiance, "target 'Radiance' is not enabled");
-		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
-		r.screenChannels = 3;
+		read("Radiance", r.targetRadiance, r.varRadiance, r.radiance, r.radianceVar, 3);
 	} else if((r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) ||
 	          (r.kind == 3 && !std::strcmp(name, "Lightness"))) {
-		const bool light = !std::strcmp(name, "Lightness");
-		CHECK(light ? r.targetLightness : r.targetDensity, std::string("target '") + name + "' is not enabled");
-		const float* src = light ? r.lightness : r.density;
-		CHECK(src != nullptr, "no image yet");
-		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n), src, n * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
-		r.screenChannels = 1;
+		if(!std::strcmp(name, "Lightness")) read("Lightness", r.targetLightness, r.varLightness, r.lightness, r.lightnessVar, 1);
+		else read("Density", r.targetDensity, r.varDensity, r.density, r.densityMean, 1);
 	} else if(r.kind == 2 && !std::strcmp(name, "Border")) {
-		CHECK(r.targetBorder, "target 'Border' is not enabled");
-		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 3), r.radiance, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
-		r.screenChannels = 3;
+		read("Border", r.targetBorder, r.varBorder, r.radiance, r.radianceVar, 3);
 	} else if(r.kind == 0 && !std::strcmp(name, "Hit ID")) {
-		CHECK(r.targetHitId, "target 'Hit ID' is not enabled");
-		CHECK_CUDA(cudaMemcpyAsync(screen_buffer(r, n * 2), r.hitId, n * 2 * sizeof(float), cudaMemcpyDeviceToHost, I.stream));
-		r.screenChannels = 2;
+		read("Hit ID", r.targetHitId, r.varHitId, r.hitId, r.hitIdVar, 2);
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
 		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "wireframe renderer" : r.kind == 3 ? "bidirectional path tracer" : "path tracer"));
@@ -1102,6 +1127,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	I.scene.desc.maxSteps = step_limit(r);
 	const uint32_t n = r.width * r.height;
 	if(r.kind != 0) ensure_lt_buffers(I);
+	ensure_variance_buffers(I);
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
 		// the wireframe renderer's generators are seeded with the pixel index (cpu_wireframe.cpp:31-36)
@@ -1111,6 +1137,10 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
 		if(r.lightness) CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, size_t(n) * sizeof(float), I.stream));
 		if(r.density) CHECK_CUDA(cudaMemsetAsync(r.density, 0, size_t(n) * sizeof(float), I.stream));
+		if(r.radianceVar) CHECK_CUDA(cudaMemsetAsync(r.radianceVar, 0, size_t(n) * 3 * sizeof(float), I.stream));
+		if(r.hitIdVar) CHECK_CUDA(cudaMemsetAsync(r.hitIdVar, 0, size_t(n) * 2 * sizeof(float), I.stream));
+		if(r.lightnessVar) CHECK_CUDA(cudaMemsetAsync(r.lightnessVar, 0, size_t(n) * sizeof(float), I.stream));
+		if(r.densityMean) CHECK_CUDA(cudaMemsetAsync(r.densityMean, 0, size_t(n) * sizeof(float), I.stream));
 		r.iteration = 0;
 		r.needsReset = false;
 	} else {
@@ -1130,6 +1160,8 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	rs.rngState = r.rng;
 	rs.radiance = r.targetRadiance ? r.radiance : nullptr;
 	rs.hitId = r.targetHitId ? r.hitId : nullptr;
+	rs.radianceVar = r.targetRadiance && r.varRadiance ? r.radianceVar : nullptr;
+	rs.hitIdVar = r.targetHitId && r.varHitId ? r.hitIdVar : nullptr;
 	rs.width = r.width; rs.height = r.height;
 	rs.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
@@ -1289,32 +1321,43 @@ const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) 
 	return kind == 2 ? "Border" : kind != 0 ? LT_TARGETS[index] : TARGETS[index];
 	CATCH_ALL(nullptr)
 }
+// The record / record-variance flags of a target implemented by the CUDA
+// renderers (null for other names).
+static std::pair<bool*, bool*> target_flags(RendererState& r, const char* name) {
+	if(!std::strcmp(name, "Radiance")) return { &r.targetRadiance, &r.varRadiance };
+	if(!std::strcmp(name, "Hit ID")) return { &r.targetHitId, &r.varHitId };
+	if(!std::strcmp(name, "Lightness")) return { &r.targetLightness, &r.varLightness };
+	if(!std::strcmp(name, "Density")) return { &r.targetDensity, &r.varDensity };
+	if(!std::strcmp(name, "Border")) return { &r.targetBorder, &r.varBorder };
+	return { nullptr, nullptr };
+}
+
+// output_handler.hpp:391-431: enabling records the target and, with
+// `variance`, its variance too; disabling with `variance` stops only the
+// variance, without it both.
 Boolean render_enable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
 	TRY
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	CHECK(target, "target name is null");
-	CHECK(!variance, "variance targets are not recorded by this renderer");
-	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = true;
-	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = true;
-	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = true;
-	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = true;
-	else if(!std::strcmp(target, "Border")) I.renderer.targetBorder = true;
-	else throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA renderers");
+	const auto f = target_flags(I.renderer, target);
+	if(!f.first) throw ApiError(std::string("render target '") + target + "' is not produced by the CUDA renderers");
+	*f.first = true;
+	if(variance) *f.second = true;
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
 }
-Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, Boolean) {
+Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, Boolean variance) {
 	TRY
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	CHECK(target, "target name is null");
-	if(!std::strcmp(target, "Radiance")) I.renderer.targetRadiance = false;
-	else if(!std::strcmp(target, "Hit ID")) I.renderer.targetHitId = false;
-	else if(!std::strcmp(target, "Lightness")) I.renderer.targetLightness = false;
-	else if(!std::strcmp(target, "Density")) I.renderer.targetDensity = false;
-	else if(!std::strcmp(target, "Border")) I.renderer.targetBorder = false;
+	const auto f = target_flags(I.renderer, target);
+	if(f.first) {
+		*f.second = false;
+		if(!variance) *f.first = false;
+	}
 	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
@@ -1322,13 +1365,10 @@ Boolean render_disable_render_target(MufflonInstanceHdl h, const char* target, B
 Boolean render_is_render_target_enabled(MufflonInstanceHdl h, const char* name, Boolean variance) {
 	TRY
 	MufflonInstance& I = minst(h);
-	if(variance || !name) return false;
-	if(!std::strcmp(name, "Radiance")) return I.renderer.targetRadiance;
-	if(!std::strcmp(name, "Hit ID")) return I.renderer.targetHitId;
-	if(!std::strcmp(name, "Lightness")) return I.renderer.targetLightness;
-	if(!std::strcmp(name, "Density")) return I.renderer.targetDensity;
-	if(!std::strcmp(name, "Border")) return I.renderer.targetBorder;
-	return false;
+	if(!name) return false;
+	const auto f = target_flags(I.renderer, name);
+	if(!f.first) return false;
+	return variance ? *f.second : *f.first;
 	CATCH_ALL(false)
 }
 

@@ -232,6 +232,14 @@ struct RendererState {
 	int32_t kind = 0;              // 0: "Pathtracer", 1: "Lighttracer", 2: "Wireframe", 3: "Bidirectional Pathtracer"
 	WireParams wireParams{ 1.0f, 1000 }; // the wireframe renderer's "Line width" and "Maximum trace depth"
 	bool targetBorder = true;      // its "Border" target
+	// Variance recording per target (render_enable_render_target(name, true),
+	// output_handler.hpp:391-431) and the buffers, allocated when first used:
+	// running variances, and for "Density" (which reduces moments) its running mean.
+	bool varRadiance = false, varHitId = false, varLightness = false, varDensity = false, varBorder = false;
+	float* radianceVar = nullptr;  // 3 per pixel (also the "Border" variance)
+	float* hitIdVar = nullptr;     // 2 per pixel
+	float* lightnessVar = nullptr; // 1 per pixel
+	float* densityMean = nullptr;  // 1 per pixel
 	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
 	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
 	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters

@@ -18,6 +18,7 @@
 // own slice of a scratch array (max. path length vertices) and the last two
 // view vertices in local memory. Connections from the camera land in other
 // pixels, so all contributions go to an iteration buffer with vector atomics.
+#include "accumulate.cuh"
 #include "wide_traverse.cuh"
 #include "emit.cuh"
 #include "lt_api.hpp"
@@ -459,18 +460,18 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 	}
 }
 
-// output_handler_variance.hpp:7-31 (mean only)
+// output_handler_variance.hpp:7-31: running means and variances
 __global__ void k_bpt_finalize(LtTargets T) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= T.width * T.height) return;
-	const float den = fmaxf(1.0f, float(T.iteration) + 1.0f);
 	const float4 it = T.iter[p];
 	if(T.radiance) {
 		float* cr = T.radiance + 3 * size_t(p);
+		float* vr = T.radianceVar ? T.radianceVar + 3 * size_t(p) : nullptr;
 		const float v[3] = { it.x, it.y, it.z };
-		for(int c = 0; c < 3; ++c) { const float diff = v[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+		for(int c = 0; c < 3; ++c) update_moments(v[c], cr + c, vr ? vr + c : nullptr, T.iteration);
 	}
-	if(T.lightness) { const float diff = it.w - T.lightness[p]; T.lightness[p] += __fdiv_rn(diff, den); }
+	if(T.lightness) update_moments(it.w, T.lightness + p, T.lightnessVar ? T.lightnessVar + p : nullptr, T.iteration);
 }
 
 int bpt_blocks() {

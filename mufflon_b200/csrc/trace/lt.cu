@@ -12,6 +12,7 @@
 // wavefront path tracer. The contributions go to an
 // iteration buffer with vector atomics (radiance and lightness in one float4),
 // and a second kernel folds that buffer into the running means.
+#include "accumulate.cuh"
 #include "shading.cuh"
 #include "wide_traverse.cuh"
 #include "emit.cuh"
@@ -256,19 +257,21 @@ __global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P,
 	}
 }
 
-// output_handler_variance.hpp:7-31 (mean only): cum += (iter - cum) / (it + 1)
+// output_handler_variance.hpp:7-31: running means and variances; Density
+// reduces moments (render_targets.hpp:68-74): its target holds the
+// iteration's value and its variance slot the running mean.
 __global__ void k_lt_finalize(LtTargets T) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= T.width * T.height) return;
-	const float den = fmaxf(1.0f, float(T.iteration) + 1.0f);
 	const float4 it = T.iter[p];
 	if(T.radiance) {
 		float* cr = T.radiance + 3 * size_t(p);
+		float* vr = T.radianceVar ? T.radianceVar + 3 * size_t(p) : nullptr;
 		const float v[3] = { it.x, it.y, it.z };
-		for(int c = 0; c < 3; ++c) { const float diff = v[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+		for(int c = 0; c < 3; ++c) update_moments(v[c], cr + c, vr ? vr + c : nullptr, T.iteration);
 	}
-	if(T.lightness) { const float diff = it.w - T.lightness[p]; T.lightness[p] += __fdiv_rn(diff, den); }
-	if(T.density) { const float diff = T.iterDensity[p] - T.density[p]; T.density[p] += __fdiv_rn(diff, den); }
+	if(T.lightness) update_moments(it.w, T.lightness + p, T.lightnessVar ? T.lightnessVar + p : nullptr, T.iteration);
+	if(T.density) update_reduced(T.iterDensity[p], T.density + p, T.densityMean ? T.densityMean + p : nullptr, T.iteration);
 }
 
 int lt_blocks() {

@@ -24,6 +24,9 @@ struct LtTargets {
 	float* lightness;     // 1 per pixel (may be null)
 	float* density;       // 1 per pixel; null: the Density target is off, which also
 	                      // skips the connections that carry no radiance (lt_common.hpp:51)
+	float* radianceVar;   // running variances of Radiance and Lightness, and the running
+	float* lightnessVar;  // mean of Density (its target reduces moments); null: not recorded
+	float* densityMean;
 	int32_t* recPixel;    // optional connection records: maxPathLength slots per photon,
 	float* recValue;      // pixel (-1: none) and radiance rgb, lightness, density as added
 	uint32_t width, height;

@@ -9,6 +9,7 @@
 // with 8x4 tiles). A pixel is written only by its own thread, so the running
 // mean of output_handler_variance.hpp:7-31 is updated in place, without
 // atomics and without a separate accumulation kernel.
+#include "accumulate.cuh"
 #include "shading.cuh"
 #include "pt_api.hpp"
 
@@ -169,7 +170,6 @@ __global__ void pt_megakernel(const DScene S, const PtParams P, RenderState R, u
 	int2 tstack[TLAS_STACK];
 	LocalCounters cnt;
 	const unsigned lane = threadIdx.x & 31u;
-	const float den = fmaxf(1.0f, float(R.iteration) + 1.0f);
 	for(;;) {
 		unsigned base = 0;
 		if(lane == 0) base = atomicAdd(workCounter, 32u);
@@ -184,13 +184,15 @@ __global__ void pt_megakernel(const DScene S, const PtParams P, RenderState R, u
 			R.rngState[pixel] = rng;
 			if(R.radiance) {
 				float* cr = R.radiance + 3 * size_t(pixel);
+				float* vr = R.radianceVar ? R.radianceVar + 3 * size_t(pixel) : nullptr;
 				const float it[3] = { rad.x, rad.y, rad.z };
-				for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+				for(int c = 0; c < 3; ++c) update_moments(it[c], cr + c, vr ? vr + c : nullptr, R.iteration);
 			}
 			if(R.hitId) {
 				float* ch = R.hitId + 2 * size_t(pixel);
+				float* vh = R.hitIdVar ? R.hitIdVar + 2 * size_t(pixel) : nullptr;
 				const float it[2] = { hid.x, hid.y };
-				for(int c = 0; c < 2; ++c) { const float diff = it[c] - ch[c]; ch[c] += __fdiv_rn(diff, den); }
+				for(int c = 0; c < 2; ++c) update_moments(it[c], ch + c, vh ? vh + c : nullptr, R.iteration);
 			}
 			if(R.iterRadiance) {
 				float* o = R.iterRadiance + 3 * size_t(pixel);

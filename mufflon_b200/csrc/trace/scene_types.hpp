@@ -143,6 +143,8 @@ struct RenderState {
 	float* radiance;        // cumulative mean, 3 per pixel (may be null)
 	float* hitId;           // cumulative mean, 2 per pixel (may be null)
 	float* iterRadiance;    // optional per-iteration radiance (may be null)
+	float* radianceVar;     // running variances of the two targets (null: not recorded)
+	float* hitIdVar;
 	uint32_t width, height;
 	int32_t iteration;      // 0 for the first iteration after a reset
 	const int32_t* dIteration; // if set: the iteration number is read here (a replayed CUDA graph)

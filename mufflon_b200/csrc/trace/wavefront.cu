@@ -19,6 +19,7 @@
 // pt_sample: the shadow kernel of bounce k runs after shade k and before
 // shade k+1, so a next-event contribution is added between the emission terms
 // that surround it, exactly as the sequential loop adds them.
+#include "accumulate.cuh"
 #include "shading.cuh"
 #include "wide_traverse.cuh"
 #include "wavefront.hpp"
@@ -645,18 +646,19 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= numPixels) return;
 	const int iteration = R.dIteration ? *R.dIteration : R.iteration;
-	const float den = fmaxf(1.0f, float(iteration) + 1.0f);
 	const float4 rad = W.rad[p];
 	if(R.radiance) {
 		float* cr = R.radiance + 3 * size_t(p);
+		float* vr = R.radianceVar ? R.radianceVar + 3 * size_t(p) : nullptr;
 		const float it[3] = { rad.x, rad.y, rad.z };
-		for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+		for(int c = 0; c < 3; ++c) update_moments(it[c], cr + c, vr ? vr + c : nullptr, iteration);
 	}
 	if(R.hitId) {
 		const float2 h = W.hit0[p];
 		float* ch = R.hitId + 2 * size_t(p);
+		float* vh = R.hitIdVar ? R.hitIdVar + 2 * size_t(p) : nullptr;
 		const float it[2] = { h.x, h.y };
-		for(int c = 0; c < 2; ++c) { const float diff = it[c] - ch[c]; ch[c] += __fdiv_rn(diff, den); }
+		for(int c = 0; c < 2; ++c) update_moments(it[c], ch + c, vh ? vh + c : nullptr, iteration);
 	}
 	if(R.iterRadiance) {
 		float* o = R.iterRadiance + 3 * size_t(p);

@@ -6,6 +6,7 @@
 // 93-180, cpu_wireframe.cpp:18-38: a persistent generator per pixel seeded
 // with the pixel index). One thread per pixel; the rays are coherent camera
 // rays, traced over the 8-wide hierarchies.
+#include "accumulate.cuh"
 #include "shading.cuh"
 #include "wide_traverse.cuh"
 #include "lt_api.hpp"
@@ -129,16 +130,16 @@ __global__ void k_wireframe(const DScene S, const float* instToWorld, WireParams
 	}
 }
 
-// output_handler_variance.hpp:7-31 (mean only), into the radiance buffer
-// (the "Border" target)
+// output_handler_variance.hpp:7-31, into the radiance buffers (the "Border"
+// target and its variance)
 __global__ void k_wireframe_finalize(LtTargets T) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= T.width * T.height || !T.radiance) return;
-	const float den = fmaxf(1.0f, float(T.iteration) + 1.0f);
 	const float4 it = T.iter[p];
 	float* cr = T.radiance + 3 * size_t(p);
+	float* vr = T.radianceVar ? T.radianceVar + 3 * size_t(p) : nullptr;
 	const float v[3] = { it.x, it.y, it.z };
-	for(int c = 0; c < 3; ++c) { const float diff = v[c] - cr[c]; cr[c] += __fdiv_rn(diff, den); }
+	for(int c = 0; c < 3; ++c) update_moments(v[c], cr + c, vr ? vr + c : nullptr, T.iteration);
 }
 
 } // namespace

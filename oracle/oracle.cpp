@@ -1742,10 +1742,29 @@ struct PtState {
 	const Scene* scene;
 	OrPtParams params;
 	std::vector<Pcg64> rngs;
-	std::vector<float> radiance, hitId;   // cumulative
+	std::vector<float> radiance, hitId;       // cumulative
+	std::vector<float> radianceVar, hitIdVar; // their variances
 	i32 iteration = -1;
 	Counters stats;
 };
+
+// output_handler_variance.hpp:7-31, one channel of a target: the running mean
+// and its variance (UpdateIter<T, false>) ...
+inline void update_moments(float iter, float& cum, float& var, float iteration) {
+	const float diff = iter - cum;
+	cum += diff / std::fmax(1.0f, iteration + 1.0f);
+	const float varIter = diff * (iter - cum);
+	const float varDiff = varIter - var;
+	var += varDiff / std::fmax(1.0f, iteration);
+}
+// ... or, for a target that reduces moments (the light tracer's Density,
+// render_targets.hpp:68-74), the iteration's value and the running mean in
+// the variance slot (UpdateIter<T, true>).
+inline void update_reduced(float iter, float& cum, float& mean, float iteration) {
+	cum = iter;
+	const float diff = iter - mean;
+	mean += diff / std::fmax(1.0f, iteration + 1.0f);
+}
 
 // pinhole.hpp:58-81
 inline V3 pinhole_ray(const Camera& c, i32 px, i32 py, float u0, float u1, float& pdf) {
@@ -1938,13 +1957,11 @@ void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
 			V3 rad; V2 hid;
 			pt_sample(st, pixel % W, pixel / W, st.rngs[pixel], rad, hid, local);
 			if(accumulate) {
-				// output_handler_variance.hpp:7-31 (mean only)
 				const float iter[5] = { rad.x, rad.y, rad.z, hid.x, hid.y };
-				float* cr = &st.radiance[size_t(pixel) * 3];
-				float* ch = &st.hitId[size_t(pixel) * 2];
-				const float den = std::fmax(1.0f, it + 1.0f);
-				for(int c = 0; c < 3; ++c) { const float diff = iter[c] - cr[c]; cr[c] += diff / den; }
-				for(int c = 0; c < 2; ++c) { const float diff = iter[3 + c] - ch[c]; ch[c] += diff / den; }
+				for(int c = 0; c < 3; ++c)
+					update_moments(iter[c], st.radiance[size_t(pixel) * 3 + size_t(c)], st.radianceVar[size_t(pixel) * 3 + size_t(c)], it);
+				for(int c = 0; c < 2; ++c)
+					update_moments(iter[3 + c], st.hitId[size_t(pixel) * 2 + size_t(c)], st.hitIdVar[size_t(pixel) * 2 + size_t(c)], it);
 			}
 		}
 #pragma omp critical
@@ -2127,7 +2144,8 @@ struct LtState {
 	const Scene* scene;
 	OrLtParams params;
 	std::vector<Pcg64> rngs;
-	std::vector<float> radiance, lightness, density; // cumulative means
+	std::vector<float> radiance, lightness, density; // cumulative means (density: the last iteration's)
+	std::vector<float> radianceVar, lightnessVar, densityMean; // variances (density: its running mean)
 	std::vector<i32> recPixel;   // last iteration, per photon and path length: pixel or -1
 	std::vector<float> recValue; // ... radiance rgb, lightness, density as added
 	i32 iteration = -1;
@@ -2282,11 +2300,11 @@ void lt_iterate(LtState& st, int numThreads) {
 		float* d = &iter[size_t(st.recPixel[k]) * 5];
 		for(int c = 0; c < 5; ++c) d[c] += st.recValue[5 * k + size_t(c)];
 	}
-	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	const float itf = float(st.iteration);
 	for(size_t p = 0; p < n; ++p) {
-		for(int c = 0; c < 3; ++c) { float& cr = st.radiance[3 * p + size_t(c)]; const float diff = iter[5 * p + size_t(c)] - cr; cr += diff / den; }
-		{ float& cl = st.lightness[p]; const float diff = iter[5 * p + 3] - cl; cl += diff / den; }
-		{ float& cd = st.density[p]; const float diff = iter[5 * p + 4] - cd; cd += diff / den; }
+		for(int c = 0; c < 3; ++c) update_moments(iter[5 * p + size_t(c)], st.radiance[3 * p + size_t(c)], st.radianceVar[3 * p + size_t(c)], itf);
+		update_moments(iter[5 * p + 3], st.lightness[p], st.lightnessVar[p], itf);
+		update_reduced(iter[5 * p + 4], st.density[p], st.densityMean[p], itf);
 	}
 }
 
@@ -2388,6 +2406,7 @@ struct BptState {
 	OrLtParams params;
 	std::vector<Pcg64> rngs;
 	std::vector<float> radiance, lightness; // cumulative means
+	std::vector<float> radianceVar, lightnessVar;
 	std::vector<i32> recPixel;               // last iteration, per pixel: connections [view length][light index], then hits [view length]
 	std::vector<float> recValue;             // radiance rgb, lightness as added
 	i32 iteration = -1;
@@ -2651,10 +2670,10 @@ void bpt_iterate(BptState& st, int numThreads) {
 		float* d = &iter[size_t(st.recPixel[k]) * 4];
 		for(int c = 0; c < 4; ++c) d[c] += st.recValue[4 * k + size_t(c)];
 	}
-	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	const float itf = float(st.iteration);
 	for(size_t p = 0; p < n; ++p) {
-		for(int c = 0; c < 3; ++c) { float& cr = st.radiance[3 * p + size_t(c)]; const float diff = iter[4 * p + size_t(c)] - cr; cr += diff / den; }
-		{ float& cl = st.lightness[p]; const float diff = iter[4 * p + 3] - cl; cl += diff / den; }
+		for(int c = 0; c < 3; ++c) update_moments(iter[4 * p + size_t(c)], st.radiance[3 * p + size_t(c)], st.radianceVar[3 * p + size_t(c)], itf);
+		update_moments(iter[4 * p + 3], st.lightness[p], st.lightnessVar[p], itf);
 	}
 }
 
@@ -2667,7 +2686,8 @@ struct WireState {
 	float lineWidth;
 	i32 maxTraceDepth;
 	std::vector<Pcg64> rngs;
-	std::vector<float> border; // cumulative mean, 3 per pixel
+	std::vector<float> border;    // cumulative mean, 3 per pixel
+	std::vector<float> borderVar; // its variance
 	i32 iteration = -1;
 	Counters stats;
 };
@@ -2757,7 +2777,7 @@ void wireframe_iterate(WireState& st, int numThreads) {
 	const Scene& S = *st.scene;
 	const i32 n = i32(S.width * S.height);
 	++st.iteration;
-	const float den = std::fmax(1.0f, float(st.iteration) + 1.0f);
+	const float itf = float(st.iteration);
 	Counters total;
 #pragma omp parallel num_threads(numThreads)
 	{
@@ -2766,8 +2786,8 @@ void wireframe_iterate(WireState& st, int numThreads) {
 		for(i32 pixel = 0; pixel < n; ++pixel) {
 			const V3 v = wireframe_sample(st, pixel % i32(S.width), pixel / i32(S.width), st.rngs[size_t(pixel)], local);
 			const float it[3] = { v.x, v.y, v.z };
-			float* cr = &st.border[3 * size_t(pixel)];
-			for(int c = 0; c < 3; ++c) { const float diff = it[c] - cr[c]; cr[c] += diff / den; }
+			for(int c = 0; c < 3; ++c)
+				update_moments(it[c], st.border[3 * size_t(pixel) + size_t(c)], st.borderVar[3 * size_t(pixel) + size_t(c)], itf);
 		}
 #pragma omp critical
 		total.add(local);
@@ -3100,6 +3120,8 @@ void* oracle_pt_create(void* s, const OrPtParams* params) {
 	for(i32 i = 0; i < num; ++i) st->rngs[i] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
 	st->radiance.assign(size_t(num) * 3, 0.0f);
 	st->hitId.assign(size_t(num) * 2, 0.0f);
+	st->radianceVar.assign(size_t(num) * 3, 0.0f);
+	st->hitIdVar.assign(size_t(num) * 2, 0.0f);
 	return st;
 }
 
@@ -3165,9 +3187,11 @@ int oracle_pt_iterate_rows(void* p, int32_t nt, uint32_t y0, uint32_t y1) {
 
 int oracle_pt_get_target(void* p, int32_t target, float* out) {
 	PtState* st = static_cast<PtState*>(p);
-	if(target == 0) std::memcpy(out, st->radiance.data(), st->radiance.size() * 4);
-	else if(target == 1) std::memcpy(out, st->hitId.data(), st->hitId.size() * 4);
-	else return 0;
+	// 0 Radiance, 1 Hit ID; 2 and 3 their variances
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->hitId
+	                            : target == 2 ? &st->radianceVar : target == 3 ? &st->hitIdVar : nullptr;
+	if(!v) return 0;
+	std::memcpy(out, v->data(), v->size() * 4);
 	return 1;
 }
 
@@ -3192,6 +3216,9 @@ void* oracle_lt_create(void* s, const OrLtParams* params) {
 	st->radiance.assign(size_t(num) * 3, 0.0f);
 	st->lightness.assign(size_t(num), 0.0f);
 	st->density.assign(size_t(num), 0.0f);
+	st->radianceVar.assign(size_t(num) * 3, 0.0f);
+	st->lightnessVar.assign(size_t(num), 0.0f);
+	st->densityMean.assign(size_t(num), 0.0f);
 	return st;
 }
 
@@ -3204,7 +3231,10 @@ int oracle_lt_iterate(void* p, int32_t nt) {
 
 int oracle_lt_get_target(void* p, int32_t target, float* out) {
 	const LtState* st = static_cast<const LtState*>(p);
-	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness : target == 2 ? &st->density : nullptr;
+	// 0 Radiance, 1 Lightness, 2 Density; 3, 4, 5 their variance buffers
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness : target == 2 ? &st->density
+	                            : target == 3 ? &st->radianceVar : target == 4 ? &st->lightnessVar
+	                            : target == 5 ? &st->densityMean : nullptr;
 	if(!v) return 0;
 	std::memcpy(out, v->data(), v->size() * 4);
 	return 1;
@@ -3238,6 +3268,8 @@ void* oracle_bpt_create(void* s, const OrLtParams* params) {
 	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
 	st->radiance.assign(size_t(num) * 3, 0.0f);
 	st->lightness.assign(size_t(num), 0.0f);
+	st->radianceVar.assign(size_t(num) * 3, 0.0f);
+	st->lightnessVar.assign(size_t(num), 0.0f);
 	return st;
 }
 
@@ -3250,7 +3282,9 @@ int oracle_bpt_iterate(void* p, int32_t nt) {
 
 int oracle_bpt_get_target(void* p, int32_t target, float* out) {
 	const BptState* st = static_cast<const BptState*>(p);
-	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness : nullptr;
+	// 0 Radiance, 1 Lightness; 2, 3 their variances
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness
+	                            : target == 2 ? &st->radianceVar : target == 3 ? &st->lightnessVar : nullptr;
 	if(!v) return 0;
 	std::memcpy(out, v->data(), v->size() * 4);
 	return 1;
@@ -3282,6 +3316,7 @@ void* oracle_wireframe_create(void* s, float lineWidth, int32_t maxTraceDepth) {
 	st->rngs.resize(size_t(num));
 	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i)); // cpu_wireframe.cpp:31-36
 	st->border.assign(size_t(num) * 3, 0.0f);
+	st->borderVar.assign(size_t(num) * 3, 0.0f);
 	return st;
 }
 void oracle_wireframe_destroy(void* p) { delete static_cast<WireState*>(p); }
@@ -3289,6 +3324,11 @@ int oracle_wireframe_iterate(void* p, int32_t nt) { wireframe_iterate(*static_ca
 int oracle_wireframe_get_target(void* p, float* out) {
 	const WireState* st = static_cast<const WireState*>(p);
 	std::memcpy(out, st->border.data(), st->border.size() * 4);
+	return 1;
+}
+int oracle_wireframe_get_variance(void* p, float* out) {
+	const WireState* st = static_cast<const WireState*>(p);
+	std::memcpy(out, st->borderVar.data(), st->borderVar.size() * 4);
 	return 1;
 }
 

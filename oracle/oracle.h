@@ -171,6 +171,7 @@ void* oracle_wireframe_create(void* scene, float lineWidth, int32_t maxTraceDept
 void oracle_wireframe_destroy(void* wf);
 int oracle_wireframe_iterate(void* wf, int32_t numThreads);
 int oracle_wireframe_get_target(void* wf, float* out);
+int oracle_wireframe_get_variance(void* wf, float* out);
 /* Building blocks exposed for known-answer tests. */
 int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);

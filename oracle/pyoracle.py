@@ -112,6 +112,7 @@ def lib():
         L.oracle_wireframe_destroy.argtypes = [C.c_void_p]
         L.oracle_wireframe_iterate.argtypes = [C.c_void_p, C.c_int32]
         L.oracle_wireframe_get_target.argtypes = [C.c_void_p, C.c_void_p]
+        L.oracle_wireframe_get_variance.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_pcg64_seed.restype = C.c_uint64
         L.oracle_pcg64_seed.argtypes = [C.c_uint32]
         L.oracle_pcg64_next.restype = C.c_uint64
@@ -274,14 +275,15 @@ class OraclePathTracer:
             threads = os.cpu_count() or 1
         lib().oracle_pt_iterate_rows(self.handle, threads, y0, y1)
 
-    def target(self, name: str):
+    def target(self, name: str, variance: bool = False):
+        """Cumulative target, or with variance=True its running variance."""
         w, h = self.scene.spec.width, self.scene.spec.height
         if name == "Radiance":
             out = np.zeros((h, w, 3), np.float32)
-            lib().oracle_pt_get_target(self.handle, 0, _ptr(out))
+            lib().oracle_pt_get_target(self.handle, 2 if variance else 0, _ptr(out))
         elif name == "Hit ID":
             out = np.zeros((h, w, 2), np.float32)
-            lib().oracle_pt_get_target(self.handle, 1, _ptr(out))
+            lib().oracle_pt_get_target(self.handle, 3 if variance else 1, _ptr(out))
         else:
             raise KeyError(name)
         return out
@@ -334,11 +336,13 @@ class OracleLightTracer:
             threads = os.cpu_count() or 1
         lib().oracle_lt_iterate(self.handle, threads)
 
-    def target(self, name: str):
+    def target(self, name: str, variance: bool = False):
+        """Cumulative target (Density: the last iteration's), or with variance=True its variance
+        buffer (Density: its running mean; the target reduces moments)."""
         w, h = self.scene.spec.width, self.scene.spec.height
         idx, ch = self.TARGETS[name]
         out = np.zeros((h, w, ch), np.float32)
-        lib().oracle_lt_get_target(self.handle, idx, _ptr(out))
+        lib().oracle_lt_get_target(self.handle, idx + (3 if variance else 0), _ptr(out))
         return out
 
     def records(self):
@@ -387,11 +391,12 @@ class OracleBidirPathTracer:
             threads = os.cpu_count() or 1
         lib().oracle_bpt_iterate(self.handle, threads)
 
-    def target(self, name: str):
+    def target(self, name: str, variance: bool = False):
+        """Cumulative target, or with variance=True its running variance."""
         w, h = self.scene.spec.width, self.scene.spec.height
         idx, ch = self.TARGETS[name]
         out = np.zeros((h, w, ch), np.float32)
-        lib().oracle_bpt_get_target(self.handle, idx, _ptr(out))
+        lib().oracle_bpt_get_target(self.handle, idx + (2 if variance else 0), _ptr(out))
         return out
 
     def records(self):
@@ -433,10 +438,10 @@ class OracleWireframe:
     def iterate(self, threads: int = 0):
         lib().oracle_wireframe_iterate(self.handle, threads if threads > 0 else (os.cpu_count() or 1))
 
-    def target(self):
+    def target(self, variance: bool = False):
         w, h = self.scene.spec.width, self.scene.spec.height
         out = np.zeros((h, w, 3), np.float32)
-        lib().oracle_wireframe_get_target(self.handle, _ptr(out))
+        (lib().oracle_wireframe_get_variance if variance else lib().oracle_wireframe_get_target)(self.handle, _ptr(out))
         return out
 
     def close(self):

@@ -39,8 +39,10 @@ CASES = {
                                                         tri_range=(500, 3000), width=64, height=48),
     "degenerate_quad": _degenerate_quad_room,
 }
-# Pixels allowed to differ from the oracle, per case (see the test).
-ALLOWED_DIFF = {"cornell": 1}
+# Pixels (row from the bottom, column) allowed to differ from the oracle, per
+# case (see the test): on the Cornell box both lie on the floor inside the
+# footprint of the box standing at x ~ -0.45.
+ALLOWED_DIFF = {"cornell": {(7, 14), (8, 25)}}
 
 
 def _gpu_wireframe(spec, iterations, line_width=None, depth=None):
@@ -77,10 +79,10 @@ def test_wireframe_border_matches_oracle(oracle, case, line_width, depth):
         # start within 1e-7 of two coplanar surfaces (the bottom face of a box
         # standing on the floor, and the floor) and meet both at t ~ 4e-7;
         # the last bits of the instance transform then pick the closer one.
-        # On the Cornell box 1 pixel of 4096 takes the other branch; every
-        # other case is bit-identical.
-        differ = np.any(img.view(np.uint32) != ref.view(np.uint32), axis=-1)
-        assert int(differ.sum()) <= ALLOWED_DIFF.get(case, 0), np.argwhere(differ)
+        # On the Cornell box 2 of 4096 pixels take the other branch (one per
+        # iteration's sub-pixel offsets); every other case is bit-identical.
+        differ = {tuple(int(c) for c in rc) for rc in np.argwhere(np.any(img.view(np.uint32) != ref.view(np.uint32), axis=-1))}
+        assert differ <= ALLOWED_DIFF.get(case, set()), sorted(differ)
     # some pixels are edges, some are not
     assert 0.0 < float(np.mean(imgs[-1][..., 0] == 1.0)) < 1.0
 
