@@ -300,13 +300,19 @@ CORE_API Boolean CDECL mufflon_get_render_stats(MufflonInstanceHdl instHdl, Muff
  * parameter "Stage timing" is non-zero (events around every stage launch):
  * camera rays, the trace launches of the wavefront bounces (extension and
  * shadow rays), the launch that finishes the remaining paths, the shade
- * launches and the accumulation. */
+ * launches, the accumulation, and the binning of queued rays by coherence
+ * (renderer parameter "Ray sort bits"). With the wavefront schedule the
+ * node-visit, primitive-test and instance-entry counts (here and in
+ * MufflonRenderStats) are kept only while the integer renderer parameter
+ * "Traversal statistics" is non-zero, by counting variants of its kernels;
+ * ray counts are always kept. */
 typedef struct {
 	uint64_t extensionRays, extendNodeVisits, extendPrimTests, extendInstanceVisits;
 	uint64_t shadowRays, shadowNodeVisits, shadowPrimTests, shadowInstanceVisits;
 	float cameraMs, extendMs, tailMs, shadeMs, finalizeMs;
 	uint32_t launches;  /* kernel launches of the iteration */
 	uint32_t wavefront; /* 1: wavefront stages, 0: megakernel */
+	float binMs;
 } MufflonStageStats;
 CORE_API Boolean CDECL mufflon_get_stage_stats(MufflonInstanceHdl instHdl, MufflonStageStats* stats);
 

@@ -9,7 +9,9 @@ parameters and keeps the fastest:
 * "Wavefront bounces" and "Tail paths": how many bounces always run as
   separate launches, and the queue length at or below which one launch
   finishes the remaining paths;
-* "Trace refill lanes": how many idle lanes of a warp are refilled together.
+* "Trace refill lanes": how many idle lanes of a warp are refilled together;
+* "Ray sort bits": the resolution of the coherence binning of queued rays
+  (0: traced in queue order).
 
 Every candidate renders the same pixels with the same random numbers, so the
 images are identical and only the time differs. Tuning resets the
@@ -22,12 +24,15 @@ import itertools
 from typing import Dict, List, Optional
 
 PARAMS = {"megakernel": "Megakernel", "trace_blocks": "Trace blocks per SM",
-          "wavefront_bounces": "Wavefront bounces", "refill_lanes": "Trace refill lanes", "tail_paths": "Tail paths"}
+          "wavefront_bounces": "Wavefront bounces", "refill_lanes": "Trace refill lanes", "tail_paths": "Tail paths",
+          "sort_bits": "Ray sort bits"}
 
 
 def default_candidates() -> List[Dict[str, int]]:
     c = [dict(megakernel=0, trace_blocks=b, wavefront_bounces=k, refill_lanes=32, tail_paths=t)
          for b, k, t in itertools.product((4, 6), (1, 2), (32768, 98304, 262144))]
+    c += [dict(megakernel=0, trace_blocks=6, wavefront_bounces=2, refill_lanes=32, tail_paths=98304, sort_bits=s)
+          for s in (0, 16)]
     c.append(dict(megakernel=1))
     return c
 

@@ -185,7 +185,7 @@ class MufflonStageStats(Structure):
                 ("extendInstanceVisits", c_uint64), ("shadowRays", c_uint64), ("shadowNodeVisits", c_uint64),
                 ("shadowPrimTests", c_uint64), ("shadowInstanceVisits", c_uint64), ("cameraMs", c_float),
                 ("extendMs", c_float), ("tailMs", c_float), ("shadeMs", c_float), ("finalizeMs", c_float),
-                ("launches", c_uint32), ("wavefront", c_uint32)]
+                ("launches", c_uint32), ("wavefront", c_uint32), ("binMs", c_float)]
 
 
 class MufflonLoadStats(Structure):

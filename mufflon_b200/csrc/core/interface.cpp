@@ -55,9 +55,10 @@ const ParamDesc PT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "NEE count", PARAM_INT }, { "NEE position guide", PARAM_BOOL },
 	{ "RR start depth", PARAM_INT }, { "Blocks per SM", PARAM_INT }, { "Megakernel", PARAM_INT },
-	{ "Stage timing", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
+	{ "Stage timing", PARAM_INT }, { "Traversal statistics", PARAM_INT }, { "Trace blocks per SM", PARAM_INT }, { "Wavefront bounces", PARAM_INT },
 	{ "Trace refill lanes", PARAM_INT }, { "Tail paths", PARAM_INT }, { "Iteration graph", PARAM_INT },
-	{ "Planned tail", PARAM_INT }, { "Traversal step limit", PARAM_INT },
+	{ "Planned tail", PARAM_INT }, { "Ray sort bits", PARAM_INT }, { "Ray sort direction bits", PARAM_INT },
+	{ "Traversal step limit", PARAM_INT },
 };
 // lt_params.hpp:8-12, plus the recording switch of the parity tests
 const ParamDesc LT_PARAMS[] = {
@@ -98,12 +99,15 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 	if(!std::strcmp(name, "Blocks per SM")) return &r.blocksPerSm;
 	if(!std::strcmp(name, "Megakernel")) return &r.megakernel;
 	if(!std::strcmp(name, "Stage timing")) return &r.stageTiming;
+	if(!std::strcmp(name, "Traversal statistics")) return &r.traversalStats;
 	if(!std::strcmp(name, "Trace blocks per SM")) return &r.traceBlocksPerSm;
 	if(!std::strcmp(name, "Wavefront bounces")) return &r.wavefrontBounces;
 	if(!std::strcmp(name, "Trace refill lanes")) return &r.refillLanes;
 	if(!std::strcmp(name, "Tail paths")) return &r.tailPaths;
 	if(!std::strcmp(name, "Iteration graph")) return &r.iterationGraph;
 	if(!std::strcmp(name, "Planned tail")) return &r.planTail;
+	if(!std::strcmp(name, "Ray sort bits")) return &r.sortBits;
+	if(!std::strcmp(name, "Ray sort direction bits")) return &r.sortDirBits;
 	return nullptr;
 }
 
@@ -1186,6 +1190,9 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	tune.wavefrontBounces = r.wavefrontBounces;
 	tune.refillLanes = r.refillLanes;
 	tune.tailPaths = r.tailPaths;
+	tune.sortBits = r.sortBits;
+	tune.sortDirBits = r.sortDirBits;
+	tune.counters = r.traversalStats != 0; // the counting kernel variants only when asked for
 	// The schedule is planned from the previous iteration's queue lengths
 	// when it ran with the same scene and parameters (every schedule renders
 	// the same bits; only the launch count differs).
@@ -1399,6 +1406,8 @@ Boolean renderer_set_parameter_int(MufflonInstanceHdl h, const char* name, int32
 	CHECK(p != nullptr, std::string("unknown parameter '") + name + "'");
 	if(!std::strcmp(name, "NEE count")) CHECK(value >= 0, "NEE count must be non-negative");
 	if(!std::strcmp(name, "Max. path length")) CHECK(value >= 1, "Max. path length must be at least 1");
+	if(!std::strcmp(name, "Ray sort bits")) CHECK(value >= 0 && value <= WF_SORT_MAX_BITS, "Ray sort bits must be in 0..16");
+	if(!std::strcmp(name, "Ray sort direction bits")) CHECK(value == 0 || value == 3 || value == 6, "Ray sort direction bits must be 0, 3 or 6");
 	*p = value;
 	I.renderer.needsReset = true; // ResetEvent::PARAMETER (renderer.hpp:19-48)
 	return true;
@@ -1478,7 +1487,7 @@ Boolean mufflon_get_stage_stats(MufflonInstanceHdl h, MufflonStageStats* s) {
 	s->shadowRays = sh.rays; s->shadowNodeVisits = sh.nodeVisits; s->shadowPrimTests = sh.primTests;
 	s->shadowInstanceVisits = sh.instanceVisits;
 	s->cameraMs = r.stageMs[WF_CAMERA]; s->extendMs = r.stageMs[WF_EXTEND]; s->tailMs = r.stageMs[WF_TAIL];
-	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE];
+	s->shadeMs = r.stageMs[WF_SHADE]; s->finalizeMs = r.stageMs[WF_FINALIZE]; s->binMs = r.stageMs[WF_BIN];
 	s->launches = uint32_t(r.lastLaunches);
 	s->wavefront = r.megakernel ? 0u : 1u;
 	return true;
@@ -1626,6 +1635,9 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	tune.wavefrontBounces = r0.wavefrontBounces;
 	tune.refillLanes = r0.refillLanes;
 	tune.tailPaths = r0.tailPaths;
+	tune.sortBits = r0.sortBits;
+	tune.sortDirBits = r0.sortDirBits;
+	tune.counters = false;
 	prepare_batch_kernels(tune);
 	while(B.events.size() < size_t(maxSpp) + 1) {
 		cudaEvent_t e;
@@ -1765,6 +1777,9 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		tune.wavefrontBounces = r.wavefrontBounces;
 		tune.refillLanes = r.refillLanes;
 		tune.tailPaths = r.tailPaths;
+		tune.sortBits = r.sortBits;
+		tune.sortDirBits = r.sortDirBits;
+		tune.counters = false;
 		if(wavefront) CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 		for(uint32_t s = 0; s < spp; ++s) {
 			if(wavefront)

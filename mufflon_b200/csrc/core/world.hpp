@@ -206,6 +206,7 @@ struct RendererState {
 	int32_t wfNee = 0;
 	size_t wfPixels = 0;
 	int32_t stageTiming = 0;      // record device time per stage kernel
+	int32_t traversalStats = 0;   // count node visits, primitive tests, instance entries (wavefront kernels)
 	int32_t traceBlocksPerSm = 6; // register budget of the wavefront trace kernel
 	int32_t wavefrontBounces = 2; // bounces run as separate stage launches before the tail launch
 	int32_t refillLanes = 32;     // idle trace lanes refilled together
@@ -213,6 +214,8 @@ struct RendererState {
 	int32_t iterationGraph = 1;   // replay the wavefront launches of an iteration as one CUDA graph
 	int32_t planTail = 1;         // plan the tail bounce from the previous iteration's queue lengths
 	int32_t stepLimit = 0;        // "Traversal step limit" of every renderer; 0: MAX_TRAVERSAL_STEPS
+	int32_t sortBits = 12;        // "Ray sort bits": coherence binning of queued rays (0: off, <= 16)
+	int32_t sortDirBits = 3;      // "Ray sort direction bits": 0, 3 (octant) or 6
 	std::vector<unsigned char> planKey;
 	int32_t plannedTail = -1;
 	cudaGraphExec_t graphExec = nullptr;

@@ -267,6 +267,17 @@ MBD bool better(float tw, int inst, int prim, const HitRec& h) {
 struct LocalCounters {
 	unsigned int nodes = 0, prims = 0, instances = 0, rays = 0, shadow = 0, errors = 0;
 };
+// Counters of a traversal that keeps no statistics: the increments of node
+// visits, primitive tests, instance entries and rays compile to nothing (and
+// take no registers); abandoned rays are still counted.
+struct NullCount {
+	MBD NullCount& operator++() { return *this; }
+	MBD operator unsigned() const { return 0u; }
+};
+struct NoCounters {
+	NullCount nodes, prims, instances, rays, shadow;
+	unsigned int errors = 0;
+};
 
 // Reads the child pair of internal node `node` as four 128-bit loads.
 struct NodePair { float4 a, b, c, d; };

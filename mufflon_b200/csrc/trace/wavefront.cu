@@ -61,6 +61,115 @@ MBD unsigned warp_reserve(unsigned* counter, unsigned want) {
 	return base + g.thread_rank() * want;
 }
 
+// ---------------------------------------------------------------- ray binning
+// Rays queued by a shade stage are traced in an order that groups similar
+// rays: the shade gives every extension ray and every shadow-ray group a key
+// (direction cell above the Morton code of the origin's cell in the scene
+// box) and counts the keys; k_bin_scan turns the counts into bin offsets and
+// k_bin_scatter writes each ray's slot at its bin's next position. A warp of
+// the next trace launch then takes 32 rays of one or a few bins: similar
+// origins and directions, so similar node visits and step counts. Only the
+// order changes; each ray's result is written to its own slot, and a
+// closest hit does not depend on when the ray is traced.
+
+// Octahedral cell (3 bits per coordinate) of a unit direction.
+MBD unsigned octa_cell(f3 d) {
+	const float s = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+	float u = __fdividef(d.x, s), v = __fdividef(d.y, s);
+	if(d.z < 0.0f) {
+		const float uu = (1.0f - fabsf(v)) * (u < 0.0f ? -1.0f : 1.0f);
+		v = (1.0f - fabsf(u)) * (v < 0.0f ? -1.0f : 1.0f);
+		u = uu;
+	}
+	const unsigned cu = min(7u, unsigned(fmaxf(0.0f, (u + 1.0f) * 4.0f)));
+	const unsigned cv = min(7u, unsigned(fmaxf(0.0f, (v + 1.0f) * 4.0f)));
+	return cu << 3 | cv;
+}
+
+// Coherence key of a ray: W.sortDirBits of direction above a Morton code of
+// the origin's cell in the scene box with the remaining bits (x gets the
+// extra bit when they do not divide by three, then y).
+MBD unsigned ray_key(const WfState& W, const DScene& S, f3 o, f3 d) {
+	const int mb = W.sortBits - W.sortDirBits;
+	const int bb[3] = { (mb + 2) / 3, (mb + 1) / 3, mb / 3 };
+	const float oc[3] = { o.x, o.y, o.z };
+	unsigned cell[3];
+	for(int a = 0; a < 3; ++a) {
+		const float ext = S.aabbMax[a] - S.aabbMin[a];
+		const float f = ext > 0.0f ? __fdividef(oc[a] - S.aabbMin[a], ext) : 0.0f;
+		const unsigned cells = 1u << bb[a];
+		cell[a] = min(cells - 1u, unsigned(fmaxf(0.0f, f * float(cells))));
+	}
+	unsigned key = 0;
+	for(int level = bb[0] - 1; level >= 0; --level)
+		for(int a = 0; a < 3; ++a)
+			if(level < bb[a]) key = key << 1 | ((cell[a] >> level) & 1u);
+	unsigned dir = 0;
+	if(W.sortDirBits == 3) dir = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+	else if(W.sortDirBits == 6) dir = octa_cell(d);
+	return dir << mb | key;
+}
+
+// Records `key` for entry i and counts it (one atomic per key per warp).
+MBD void bin_append(unsigned* keys, unsigned* hist, unsigned i, unsigned key) {
+	keys[i] = key;
+	const unsigned peers = __match_any_sync(__activemask(), key);
+	if((threadIdx.x & 31u) == unsigned(__ffs(int(peers)) - 1)) atomicAdd(hist + key, unsigned(__popc(peers)));
+}
+
+// Exclusive offsets of the extension bins (block 0) and the shadow bins
+// (block 1), 1 << bits each; the counts are cleared for the next shade.
+__global__ void __launch_bounds__(1024) k_bin_scan(unsigned* hist, unsigned* cursor, int bits) {
+	__shared__ unsigned part[1024];
+	const unsigned nb = 1u << bits;
+	unsigned* h = hist + blockIdx.x * nb;
+	unsigned* c = cursor + blockIdx.x * nb;
+	const unsigned per = (nb + 1023u) / 1024u;
+	const unsigned t = threadIdx.x, b0 = t * per;
+	unsigned sum = 0;
+	for(unsigned k = 0; k < per && b0 + k < nb; ++k) sum += h[b0 + k];
+	part[t] = sum;
+	__syncthreads();
+	for(unsigned off = 1; off < 1024u; off <<= 1) {
+		const unsigned v = t >= off ? part[t - off] : 0u;
+		__syncthreads();
+		part[t] += v;
+		__syncthreads();
+	}
+	unsigned run = part[t] - sum;
+	for(unsigned k = 0; k < per && b0 + k < nb; ++k) {
+		const unsigned x = h[b0 + k];
+		c[b0 + k] = run;
+		run += x;
+		h[b0 + k] = 0u;
+	}
+}
+
+// Writes the trace order of the queues the last shade filled: extension
+// queue qNext and the shadow groups of shadow counter C_SHADOW0 + (qNext ^ 1).
+__global__ void k_bin_scatter(WfState W, int qNext, int neeCount, unsigned capacity) {
+	const unsigned nb = 1u << W.sortBits;
+	const unsigned nExt = W.counters[qNext];
+	const unsigned nGroups = W.counters[C_SHADOW0 + (qNext ^ 1)] / unsigned(neeCount);
+	const unsigned lane = threadIdx.x & 31u;
+	for(unsigned i0 = blockIdx.x * blockDim.x; i0 < nExt + nGroups; i0 += gridDim.x * blockDim.x) {
+		const unsigned i = i0 + threadIdx.x;
+		const bool ext = i < nExt;
+		const bool valid = i < nExt + nGroups;
+		const unsigned key = !valid ? 0xFFFFFFFFu : ext ? W.extKey[i] : nb + W.shKey[i - nExt];
+		const unsigned peers = __match_any_sync(0xffffffffu, key);
+		const int leader = __ffs(int(peers)) - 1;
+		unsigned base = 0;
+		if(valid && int(lane) == leader) base = atomicAdd(W.binCursor + key, unsigned(__popc(peers)));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if(!valid) continue;
+		const unsigned pos = base + unsigned(__popc(peers & ((1u << lane) - 1u)));
+		if(pos >= capacity) continue; // unreachable while the counts match the queues
+		if(ext) W.extOrder[pos] = i;
+		else W.shOrder[pos] = i - nExt;
+	}
+}
+
 // Where a path's scene and path-tracer parameters come from: the kernel
 // argument for a plain render, or the device job table of a batch, whose jobs
 // share the queues (path p belongs to job pathJob[p]).
@@ -165,7 +274,8 @@ __global__ void k_camera(const DScene S, const PtParams P, WfState W, uint32_t n
 
 // Block-wide traversal statistics in shared memory, one set per ray kind.
 struct BlockStats { unsigned long long v[2][6]; };
-MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
+template < class C >
+MBD void stats_add(BlockStats& b, int kind, const C& c) {
 	if(c.nodes) atomicAdd(&b.v[kind][0], (unsigned long long)c.nodes);
 	if(c.prims) atomicAdd(&b.v[kind][1], (unsigned long long)c.prims);
 	if(c.instances) atomicAdd(&b.v[kind][2], (unsigned long long)c.instances);
@@ -183,7 +293,7 @@ MBD void stats_add(BlockStats& b, int kind, const LocalCounters& c) {
 // Every loop iteration runs one traversal step in every busy lane.
 // Queue entries are read and written with streaming (evict-first) accesses so
 // that they do not displace the hierarchies from L2.
-template < int MINB, class SP >
+template < int MINB, class SP, class C >
 __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int q, int neeCount, int workIdx,
                                                      TraceCounters* counters, int refillLanes, int bounce) {
 	__shared__ BlockStats stats;
@@ -196,13 +306,14 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 		if(bounce < int(WF_BOUNCE_STATS)) W.counters[WF_COUNTERS - WF_BOUNCE_STATS + bounce] = W.counters[q];
 	}
 	LocalStack stack;
-	LocalCounters cnt;
+	C cnt;
 	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW0 + (q ^ 1)) / unsigned(neeCount);
 	const unsigned total = nExt + nGroups;
 	WideTracer t;
 	bool active = false, exhausted = false;
 	unsigned item = 0;
+	unsigned ent = 0;      // the item's extension-queue slot or shadow-ray group
 	int path = 0, ray = 0; // path of the current item
 	f3 radiance = make3(0.0f, 0.0f, 0.0f);
 	float radW = 0.0f;
@@ -214,6 +325,11 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 		const unsigned busy = __ballot_sync(0xffffffffu, active);
 		const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
 		if(idle && (__popc(idle) >= refillLanes || !busy)) {
+			// One atomic per refill: the items a warp takes at a time are the
+			// next ones of the queue. (Taking larger chunks per warp, to refill
+			// lanes one by one without the atomic, measured 12-100 % slower:
+			// the warps of an SM then trace rays from a wider window of the
+			// queue and share fewer hierarchy nodes in L1.)
 			unsigned base = 0;
 			if(lane == unsigned(__ffs(int(idle)) - 1)) base = atomicAdd(W.counters + C_WORK + workIdx, unsigned(__popc(idle)));
 			base = __shfl_sync(0xffffffffu, base, __ffs(int(idle)) - 1);
@@ -222,13 +338,15 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 				if(item >= total) {
 					exhausted = true;
 				} else if(item < nExt) {
-					const float4 o = __ldcs(W.qOrg[q] + item), d = __ldcs(W.qDir[q] + item);
-					path = W.qPath[q][item];
-					cnt = LocalCounters();
+					ent = W.ordered ? __ldcs(W.extOrder + item) : item;
+					const float4 o = __ldcs(W.qOrg[q] + ent), d = __ldcs(W.qDir[q] + ent);
+					path = W.qPath[q][ent];
+					cnt = C();
 					t.init(sp.scene(path), f4to3(o), f4to3(d), MAX_SCENE_SIZE, false, cnt);
 					active = true;
 				} else {
-					path = __ldcs(W.sPath + (item - nExt) * unsigned(neeCount));
+					ent = W.ordered ? __ldcs(W.shOrder + (item - nExt)) : item - nExt;
+					path = __ldcs(W.sPath + ent * unsigned(neeCount));
 					const float4 acc = W.rad[path];
 					radiance = f4to3(acc);
 					radW = acc.w;
@@ -242,12 +360,12 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 			if(item < nExt) {
 				stats_add(stats, 0, cnt);
 				const HitRec& h = t.best;
-				__stcs(W.qHit[q] + item, make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x));
-				__stcs(W.qHitSpy[q] + item, h.sp.y);
+				__stcs(W.qHit[q] + ent, make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x));
+				__stcs(W.qHitSpy[q] + ent, h.sp.y);
 				active = false;
 			} else {
 				stats_add(stats, 1, cnt);
-				const unsigned slot = (item - nExt) * unsigned(neeCount) + unsigned(ray);
+				const unsigned slot = ent * unsigned(neeCount) + unsigned(ray);
 				if(!t.occluded) {
 					const f3 c = f4to3(__ldcs(W.sContrib + slot));
 					radiance = contribute(radiance, c);
@@ -260,12 +378,12 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 		if(seek) {
 			// next non-empty slot of the group, or write the group's radiance
 			active = false;
-			const unsigned g0 = (item - nExt) * unsigned(neeCount);
+			const unsigned g0 = ent * unsigned(neeCount);
 			for(; ray < neeCount; ++ray) {
 				const float4 o = __ldcs(W.sOrg + g0 + unsigned(ray));
 				if(!(o.w > 0.0f)) continue;
 				const float4 d = __ldcs(W.sDir + g0 + unsigned(ray));
-				cnt = LocalCounters();
+				cnt = C();
 				t.init(sp.scene(path), f4to3(o), f4to3(d), o.w, true, cnt);
 				active = true;
 				break;
@@ -475,6 +593,8 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 			if(base == 0xFFFFFFFFu) {
 				base = atomicAdd(W.counters + C_SHADOW0 + q, unsigned(P.neeCount));
 				for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
+				if(W.sortBits)
+					bin_append(W.shKey, W.binHist + (1u << W.sortBits), base / unsigned(P.neeCount), ray_key(W, S, so, sd));
 			}
 			W.sOrg[base + i] = pack(so, stmax);
 			W.sDir[base + i] = pack(sd, 0.0f);
@@ -491,6 +611,7 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	W.qPath[out][nslot] = p;
 	W.qOrg[out][nslot] = pack(nextO, 0.0f);
 	W.qDir[out][nslot] = pack(nextD, 0.0f);
+	if(W.sortBits) bin_append(W.extKey, W.binHist, nslot, ray_key(W, S, nextO, nextD));
 }
 
 // Shade stage of the wavefront over queue q, grid-stride over its entries
@@ -524,7 +645,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(const SP sp, WfState W, int q,
 // of the loop traces at most one ray per lane (a shadow ray or the next
 // extension ray) in one traversal loop shared by the warp. A path's random
 // numbers, terms and their order are those of shade_vertex.
-template < int MINB, class SP >
+template < int MINB, class SP, class C >
 __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int q, int bounce,
                                                     int workIdx, TraceCounters* counters, unsigned tailMax) {
 	__shared__ BlockStats stats;
@@ -611,7 +732,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 		}
 		if(!trace) continue;
 		const DScene& S = sp.scene(p);
-		LocalCounters cnt;
+		C cnt;
 		WideTracer t;
 		t.init(S, ro, rd, tmax, shadow, cnt);
 		while(!t.step(S, cnt, stack)) {}
@@ -846,15 +967,21 @@ template < class SP > struct TraceKernel {
 	int blocks;
 };
 // The trace kernel compiled for `perSm` resident blocks of 128 threads
-// (register budget 65536 / (128 * perSm)); other values pick 6.
-template < class SP > TraceKernel<SP> trace_kernel(int perSm) {
-	static TraceKernel<SP> table[4] = {};
-	static const typename TraceKernel<SP>::Fn fns[4] = { k_trace<4, SP>, k_trace<5, SP>, k_trace<6, SP>, k_trace<8, SP> };
+// (register budget 65536 / (128 * perSm)); other values pick 6. With
+// `counting`, the variant that counts node visits, primitive tests and
+// instance entries per ray kind.
+template < class SP > TraceKernel<SP> trace_kernel(int perSm, bool counting) {
+	static TraceKernel<SP> table[2][4] = {};
+	static const typename TraceKernel<SP>::Fn fns[2][4] = {
+		{ k_trace<4, SP, NoCounters>, k_trace<5, SP, NoCounters>, k_trace<6, SP, NoCounters>, k_trace<8, SP, NoCounters> },
+		{ k_trace<4, SP, LocalCounters>, k_trace<5, SP, LocalCounters>, k_trace<6, SP, LocalCounters>, k_trace<8, SP, LocalCounters> } };
 	static const int occ[4] = { 4, 5, 6, 8 };
 	int idx = 2;
 	for(int i = 0; i < 4; ++i) if(occ[i] == perSm) idx = i;
-	if(!table[idx].fn) table[idx] = { fns[idx], persistent_blocks(reinterpret_cast<const void*>(fns[idx]), int(WF_BLOCK)) };
-	return table[idx];
+	const int c = counting ? 1 : 0;
+	if(!table[c][idx].fn)
+		table[c][idx] = { fns[c][idx], persistent_blocks(reinterpret_cast<const void*>(fns[c][idx]), int(WF_BLOCK)) };
+	return table[c][idx];
 }
 
 template < class SP > struct TailKernel {
@@ -862,10 +989,12 @@ template < class SP > struct TailKernel {
 	Fn fn;
 	int blocks;
 };
-template < class SP > TailKernel<SP> tail_kernel() {
-	static TailKernel<SP> k = {};
-	if(!k.fn) k = { k_tail<4, SP>, persistent_blocks(reinterpret_cast<const void*>(k_tail<4, SP>), int(WF_BLOCK)) };
-	return k;
+template < class SP > TailKernel<SP> tail_kernel(bool counting) {
+	static TailKernel<SP> k[2] = {};
+	const typename TailKernel<SP>::Fn fn = counting ? k_tail<4, SP, LocalCounters> : k_tail<4, SP, NoCounters>;
+	const int c = counting ? 1 : 0;
+	if(!k[c].fn) k[c] = { fn, persistent_blocks(reinterpret_cast<const void*>(fn), int(WF_BLOCK)) };
+	return k[c];
 }
 
 // Stage timing and launch counting of one iteration.
@@ -891,12 +1020,28 @@ template < class SP >
 void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numPaths, int maxBounces, int neeCount,
                  const WfTuning& tuning, LaunchLog& log, cudaStream_t stream) {
 	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
-	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm);
+	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm, tuning.counters);
 	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
 	static int sms = 0;
 	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
 	const unsigned shadeGrid = std::max(1u, std::min((numPaths + 127) / 128, unsigned(sms) * 16u));
 	const unsigned tailMax = unsigned(tuning.tailPaths < 0 ? 0 : tuning.tailPaths);
+	const bool binning = tuning.sortBits > 0 && W.extKey != nullptr;
+	W.sortBits = binning ? std::min(tuning.sortBits, WF_SORT_MAX_BITS) : 0;
+	W.sortDirBits = std::min(tuning.sortDirBits == 3 || tuning.sortDirBits == 6 ? tuning.sortDirBits : 0, W.sortBits);
+	// After the shade of bounce b, the rays it queued are binned for the
+	// trace launch of bounce b + 1.
+	// every shade's counts are consumed by the scan that follows it, except
+	// those of an iteration's last shade: start each iteration from zero
+	if(binning) cudaMemsetAsync(W.binHist, 0, (size_t(2) << W.sortBits) * sizeof(unsigned), stream);
+	auto bin = [&](int b) {
+		if(!binning || b + 1 >= maxBounces) return;
+		log.begin(WF_BIN);
+		k_bin_scan<<<2, 1024, 0, stream>>>(W.binHist, W.binCursor, W.sortBits);
+		++log.L.launches; // the scatter: two launches in one timed stage
+		k_bin_scatter<<<unsigned(sms) * 8u, 256, 0, stream>>>(W, (b & 1) ^ 1, neeCount, numPaths);
+		log.end();
+	};
 	unsigned work = 0;
 	for(int b = 0; b < maxBounces; ++b) {
 		const int q = b & 1;
@@ -904,13 +1049,15 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 			cudaMemsetAsync(W.counters + C_WORK, 0, sizeof(unsigned) * workSlots, stream);
 			work = 0;
 		}
+		WfState Wt = W;
+		Wt.ordered = binning && b >= 1 ? 1 : 0;
 		log.begin(WF_EXTEND);
-		tk.fn<<<tk.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, neeCount, int(work++), counters, refillLanes, b);
+		tk.fn<<<tk.blocks, WF_BLOCK, 0, stream>>>(sp, Wt, q, neeCount, int(work++), counters, refillLanes, b);
 		log.end();
 		if(tuning.tailBounce >= 0) {
 			// planned schedule: the tail takes over at tailBounce, nothing follows
 			if(b == tuning.tailBounce && b + 1 < maxBounces) {
-				const TailKernel<SP> tl = tail_kernel<SP>();
+				const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters);
 				log.begin(WF_TAIL);
 				tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, 0xFFFFFFFFu);
 				log.end();
@@ -919,6 +1066,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 			log.begin(WF_SHADE);
 			k_shade<SP><<<(numPaths + 127) / 128, 128, 0, stream>>>(sp, W, q, b, 0u, 0); // one thread per entry
 			log.end();
+			bin(b);
 			continue;
 		}
 		// From bounce wavefrontBounces on, the first bounce whose queue holds
@@ -926,7 +1074,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 		// device from the queue length); the later launches return at once.
 		const bool tailAllowed = b >= tuning.wavefrontBounces && b + 1 < maxBounces;
 		if(tailAllowed) {
-			const TailKernel<SP> tl = tail_kernel<SP>();
+			const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters);
 			log.begin(WF_TAIL);
 			tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, tailMax);
 			log.end();
@@ -936,6 +1084,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 		log.begin(WF_SHADE);
 		k_shade<SP><<<shadeGrid, 128, 0, stream>>>(sp, W, q, b, tailMax, tailAllowed ? 1 : 0);
 		log.end();
+		bin(b);
 	}
 }
 
@@ -957,7 +1106,8 @@ size_t wf_align(size_t b) { return (b + WF_ALIGN - 1) / WF_ALIGN * WF_ALIGN; }
 size_t wavefront_bytes(size_t n, int nee) {
 	if(nee < 1) nee = 1;
 	return wf_align(n * 16) * 2 + wf_align(n * 8) + 2 * (wf_align(n * 4) + 3 * wf_align(n * 16) + wf_align(n * 4)) +
-	       wf_align(n * nee * 4) + 3 * wf_align(n * nee * 16) + wf_align(WF_COUNTERS * 4);
+	       wf_align(n * nee * 4) + 3 * wf_align(n * nee * 16) + wf_align(WF_COUNTERS * 4) +
+	       4 * wf_align(n * 4) + 2 * wf_align((size_t(2) << WF_SORT_MAX_BITS) * 4);
 }
 
 void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
@@ -979,6 +1129,15 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
 	W.sDir = reinterpret_cast<float4*>(take(n * nee * 16));
 	W.sContrib = reinterpret_cast<float4*>(take(n * nee * 16));
 	W.counters = reinterpret_cast<unsigned*>(take(WF_COUNTERS * 4));
+	W.extKey = reinterpret_cast<unsigned*>(take(n * 4));
+	W.shKey = reinterpret_cast<unsigned*>(take(n * 4));
+	W.extOrder = reinterpret_cast<unsigned*>(take(n * 4));
+	W.shOrder = reinterpret_cast<unsigned*>(take(n * 4));
+	W.binHist = reinterpret_cast<unsigned*>(take((size_t(2) << WF_SORT_MAX_BITS) * 4));
+	W.binCursor = reinterpret_cast<unsigned*>(take((size_t(2) << WF_SORT_MAX_BITS) * 4));
+	W.sortBits = 0;
+	W.sortDirBits = 0;
+	W.ordered = 0;
 }
 
 cudaError_t launch_adjoint_albedo(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
@@ -1041,10 +1200,10 @@ cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_
 }
 
 void prepare_batch_kernels(const WfTuning& tuning) {
-	(void)trace_kernel<JobScenes>(tuning.traceBlocksPerSm);
-	(void)tail_kernel<JobScenes>();
-	(void)trace_kernel<OneScene>(tuning.traceBlocksPerSm);
-	(void)tail_kernel<OneScene>();
+	(void)trace_kernel<JobScenes>(tuning.traceBlocksPerSm, tuning.counters);
+	(void)tail_kernel<JobScenes>(tuning.counters);
+	(void)trace_kernel<OneScene>(tuning.traceBlocksPerSm, tuning.counters);
+	(void)tail_kernel<OneScene>(tuning.counters);
 }
 
 cudaError_t launch_trace_rays_wide(const DScene& S, const float* rays, const float* geoNormals, float tmax, uint32_t n,

@@ -22,7 +22,21 @@ struct WfState {
 	float4* sDir;         // direction
 	float4* sContrib;     // contribution if unoccluded
 	unsigned* counters;   // queue sizes and per-launch work counters (WF_COUNTERS)
+	// Coherence binning of the rays a shade stage queues (see wavefront.cu):
+	// the shade writes a key per queued extension ray and per shadow-ray
+	// group and counts the keys; a scan and a scatter then build the order in
+	// which the next trace launch takes them.
+	unsigned* extKey;     // per extension-queue slot
+	unsigned* shKey;      // per shadow-ray group
+	unsigned* extOrder;   // trace order: the slot of the i-th extension ray
+	unsigned* shOrder;    // trace order: the i-th shadow-ray group
+	unsigned* binHist;    // 2 << WF_SORT_MAX_BITS key counts (extension, then shadow)
+	unsigned* binCursor;  // 2 << WF_SORT_MAX_BITS scatter cursors
+	int sortBits;         // key bits (0: no binning; at most WF_SORT_MAX_BITS)
+	int sortDirBits;      // of those, direction bits: 0, 3 (octant) or 6 (octahedral 8 x 8)
+	int ordered;          // set for a trace launch whose queues were binned
 };
+constexpr int WF_SORT_MAX_BITS = 16;
 
 // Size of WfState::counters: queue sizes, flags and one work counter per
 // persistent launch (two per bounce; longer paths recycle them), then the
@@ -32,7 +46,8 @@ constexpr unsigned WF_BOUNCE_STATS = 64;
 
 // WF_EXTEND: the trace launches of the wavefront bounces (extension and
 // shadow rays); WF_TAIL: the launch that finishes the remaining paths.
-enum WfStage { WF_CAMERA = 0, WF_EXTEND = 1, WF_TAIL = 2, WF_SHADE = 3, WF_FINALIZE = 4, WF_STAGES = 5 };
+// WF_BIN: the scan and scatter launches that order queued rays by coherence.
+enum WfStage { WF_CAMERA = 0, WF_EXTEND = 1, WF_TAIL = 2, WF_SHADE = 3, WF_FINALIZE = 4, WF_BIN = 5, WF_STAGES = 6 };
 
 // Host-side launch record of one iteration. With `events` set, a pair of
 // events is recorded around each stage launch (while capacity lasts) and
@@ -57,6 +72,9 @@ struct WfTuning {
 	int tailBounce = -1;       // >= 0: planned schedule, the tail launch takes over at this bounce and
 	                           // nothing is launched after it; -1: decided on the device per bounce
 	int refillLanes = 32;      // idle lanes of a trace warp are refilled together once this many are idle (1..32)
+	int sortBits = 0;          // coherence binning of the queued rays before each trace launch of bounce >= 1
+	int sortDirBits = 3;       // (key bits in all, of them direction bits); 0 bits: trace in queue order
+	bool counters = true;      // count node visits, primitive tests and instance entries (a slower kernel variant)
 };
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
                                 TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info,

@@ -124,8 +124,7 @@ MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, u
 // lanes as soon as their ray finishes call step() from one loop shared by the
 // whole warp.
 struct WideTracer {
-	f3 wo, wd;            // world ray
-	FastRay wr;           // world ray, prepared
+	FastRay wr;           // world ray, prepared (wr.o, wr.d: the ray as given)
 	FastRay r;            // ray of the current level
 	float scale;          // object-space length of a world-space unit
 	float tmaxW;          // shadow rays: world-space segment length
@@ -136,8 +135,8 @@ struct WideTracer {
 	int inst, sp, instSp, steps; // steps: what is left of the scene's step limit
 	bool any, single, occluded, done;
 
-	MBD void init(const DScene& S, f3 o, f3 d, float tmax, bool anyHit, LocalCounters& cnt) {
-		wo = o; wd = d;
+	template < class C >
+	MBD void init(const DScene& S, f3 o, f3 d, float tmax, bool anyHit, C& cnt) {
 		tmaxW = tmax;
 		any = anyHit;
 		occluded = false;
@@ -156,11 +155,12 @@ struct WideTracer {
 		else ngHits = S.tlasNumWide > 0 ? (1u << flip) : 0u;
 	}
 
-	MBD void enter(const DScene& S, uint32_t i, LocalCounters& cnt) {
+	template < class C >
+	MBD void enter(const DScene& S, uint32_t i, C& cnt) {
 		++cnt.instances;
 		inst = int(i);
 		lod = S.lods + __ldg(S.instanceLod + i);
-		const InstRay ir = instance_ray_ool(S, i, wo, wd);
+		const InstRay ir = instance_ray_ool(S, i, wr.o, wr.d);
 		r = ir.ray;
 		scale = ir.scale;
 		flip = octant_flip(r.d);
@@ -172,8 +172,8 @@ struct WideTracer {
 		instSp = sp;
 	}
 
-	template < class Stack >
-	MBD bool step(const DScene& S, LocalCounters& cnt, Stack& stack) {
+	template < class Stack, class C >
+	MBD bool step(const DScene& S, C& cnt, Stack& stack) {
 		if(done) return true;
 		if(--steps < 0) { ++cnt.errors; done = true; return true; }
 		if(ngHits) {
@@ -235,7 +235,7 @@ struct WideTracer {
 			if(instSp >= 0 && sp == instSp) {
 				if(single) { done = true; return true; }
 				r = wr;
-				flip = octant_flip(wd);
+				flip = octant_flip(wr.d);
 				scale = 1.0f;
 				nodes = S.tlasWide;
 				instSp = -1;
@@ -251,8 +251,8 @@ struct WideTracer {
 };
 
 // Closest hit of a world-space ray whose origin is already offset.
-template < class Stack >
-MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCounters& cnt, Stack& stack) {
+template < class Stack, class C >
+MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, C& cnt, Stack& stack) {
 	++cnt.rays;
 	WideTracer t;
 	t.init(S, o, dir, tmax, false, cnt);
@@ -261,8 +261,8 @@ MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, LocalCoun
 }
 
 // Occlusion of a prepared shadow ray (origin offset, unit direction, length tmax).
-template < class Stack >
-MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, LocalCounters& cnt, Stack& stack) {
+template < class Stack, class C >
+MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, C& cnt, Stack& stack) {
 	++cnt.rays; ++cnt.shadow;
 	WideTracer t;
 	t.init(S, a, dir, tmax, true, cnt);

@@ -106,7 +106,7 @@ def test_lbvh_bit_exact_full_icosphere(dll, oracle):
 KERNELS = {"wavefront": 0, "megakernel": 1}
 DEFAULT_PARAMS = {"Seed": 0, "Min. path length": 0, "Max. path length": 16, "NEE count": 1,
                   "RR start depth": 0, "Megakernel": 0, "Wavefront bounces": 2, "Tail paths": 98304, "Iteration graph": 1,
-                  "Planned tail": 1}
+                  "Planned tail": 1, "Ray sort bits": 12, "Ray sort direction bits": 3}
 
 
 def _load(dll, spec):
@@ -313,6 +313,39 @@ def test_pt_schedule_parity(dll, oracle, wavefront_bounces, tail_paths):
         pt.iterate()
     assert np.array_equal(dll.get_target_image("Hit ID"), pt.target("Hit ID"))
     assert rel_rmse(dll.get_target_image("Radiance"), pt.target("Radiance")) <= RMSE_TOL
+
+
+@pytest.mark.parametrize("bits,dir_bits", [(3, 3), (12, 6), (16, 3), (16, 0), (6, 6)])
+@pytest.mark.parametrize("scene", ["cornell_nee2", "instanced"])
+def test_pt_ray_binning_parity(dll, oracle, scene, bits, dir_bits):
+    """Rays traced in coherence-binned order (extension rays and shadow-ray groups of every bounce >= 1)
+    give the oracle's bits: only the order of the trace launch's work changes."""
+    if scene == "cornell_nee2":
+        spec, kw = scenes.cornell_box(5, 80, 80), dict(nee=2, max_path=9, rr_start=2, min_path=1)
+    else:
+        spec, kw = _small_instanced(2), dict(nee=1, max_path=12, rr_start=3, min_path=0)
+    _load(dll, spec)
+    dll.render_enable_render_target("Radiance", False)
+    dll.render_enable_render_target("Hit ID", False)
+    for name, value in {"Ray sort bits": bits, "Ray sort direction bits": dir_bits, "NEE count": kw["nee"],
+                        "Max. path length": kw["max_path"], "RR start depth": kw["rr_start"],
+                        "Min. path length": kw["min_path"]}.items():
+        assert dll.renderer_set_parameter_int(name, value)
+    pt = oracle.OraclePathTracer(oracle.OracleScene(spec), seed=0, min_path=kw["min_path"], max_path=kw["max_path"],
+                                 nee_count=kw["nee"], rr_start=kw["rr_start"])
+    for _ in range(2):
+        dll.render_iterate()
+        pt.iterate()
+    assert dll.stage_stats()["launches"] > 0
+    assert np.array_equal(dll.get_target_image("Hit ID"), pt.target("Hit ID"))
+    assert np.array_equal(dll.get_target_image("Radiance").view(np.uint32), pt.target("Radiance").view(np.uint32))
+
+
+def test_ray_binning_parameters_are_checked(dll):
+    _load(dll, scenes.cornell_box(0, 16, 16))
+    assert not dll.renderer_set_parameter_int("Ray sort bits", 17)
+    assert not dll.renderer_set_parameter_int("Ray sort direction bits", 4)
+    assert dll.renderer_set_parameter_int("Ray sort bits", 0)
 
 
 def test_graph_replay_equals_plain_launches(dll):
