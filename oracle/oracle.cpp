@@ -230,7 +230,40 @@ inline u64 percentage_of(u64 num, float p) {
 	return ((pfix * (num & 0x7fffffff)) >> 31) + (pfix * (num >> 31));
 }
 
+// rng.hpp:119-140: GoldenRatio2D::next, the state advanced by the golden
+// ratio in 64-bit fixed point and turned from a Hilbert index into two 32-bit
+// coordinates (gray code, then the Morton bits separated)
+inline u64 golden_ratio2d_next(u64& state) {
+	u64 s = state;
+	state += 11400714819323198485ull;
+	s = s ^ (s >> 1);
+	s = ((s >> 1) & 0x2222222222222222ull) | ((s << 1) & 0x4444444444444444ull) | (s & 0x9999999999999999ull);
+	s = ((s >> 2) & 0x0c0c0c0c0c0c0c0cull) | ((s << 2) & 0x3030303030303030ull) | (s & 0xc3c3c3c3c3c3c3c3ull);
+	s = ((s >> 4) & 0x00f000f000f000f0ull) | ((s << 4) & 0x0f000f000f000f00ull) | (s & 0xf00ff00ff00ff00full);
+	s = ((s >> 8) & 0x0000ff000000ff00ull) | ((s << 8) & 0x00ff000000ff0000ull) | (s & 0xff0000ffff0000ffull);
+	s = ((s >> 16) & 0x00000000ffff0000ull) | ((s << 16) & 0x0000ffff00000000ull) | (s & 0xffff00000000ffffull);
+	return s;
+}
+
 // ---------------------------------------------------------------- morton
+// sfcurves.hpp:12-19: 16 bits spread 3 ways
+inline u64 part_by_two16(u32 x) {
+	u64 r = x & 0xFFFF;
+	r = (r | (r << 16)) & 0x0000ff0000ffull;
+	r = (r | (r << 8)) & 0x00f00f00f00full;
+	r = (r | (r << 4)) & 0x0c30c30c30c3ull;
+	r = (r | (r << 2)) & 0x249249249249ull;
+	return r;
+}
+// sfcurves.hpp:58-77: Morton code of three 16-bit values, and its Hilbert
+// index (the gray-code inverse of the Morton code)
+inline u64 morton_code16(u32 a, u32 b, u32 c) { return part_by_two16(a) | (part_by_two16(b) << 1u) | (part_by_two16(c) << 2u); }
+inline u64 hilbert_code16(u32 a, u32 b, u32 c) {
+	u64 num = morton_code16(a, b, c);
+	num = num ^ (num >> 32); num = num ^ (num >> 16); num = num ^ (num >> 8);
+	num = num ^ (num >> 4); num = num ^ (num >> 2); num = num ^ (num >> 1);
+	return num;
+}
 // sfcurves.hpp:35-44
 inline u64 part_by_two21(u32 x) {
 	u64 r = x;
@@ -1437,17 +1470,10 @@ inline float light_flux(const Scene& S, const PosLight& l) {
 	const V3 rad = m.radiance * m.scale;
 	// GoldenRatio2D seeded from the light's address in the reference; here
 	// seeded from its index in the light list (deterministic).
-	u64 state = scramble_seed(u32(l.primId) * 2654435761u + u32(l.primInst));
+	u64 state = scramble_seed(u32(l.primId) * 2654435761u + u32(l.primInst)); // GoldenRatio2D(seed)
 	V3 sum = { 0, 0, 0 };
 	for(int i = 0; i < 128; ++i) {
-		u64 s = state;
-		state += 11400714819323198485ull;
-		s = s ^ (s >> 1);
-		s = ((s >> 1) & 0x2222222222222222ull) | ((s << 1) & 0x4444444444444444ull) | (s & 0x9999999999999999ull);
-		s = ((s >> 2) & 0x0c0c0c0c0c0c0c0cull) | ((s << 2) & 0x3030303030303030ull) | (s & 0xc3c3c3c3c3c3c3c3ull);
-		s = ((s >> 4) & 0x00f000f000f000f0ull) | ((s << 4) & 0x0f000f000f000f00ull) | (s & 0xf00ff00ff00ff00full);
-		s = ((s >> 8) & 0x0000ff000000ff00ull) | ((s << 8) & 0x00ff000000ff0000ull) | (s & 0xff0000ffff0000ffull);
-		s = ((s >> 16) & 0x00000000ffff0000ull) | ((s << 16) & 0x0000ffff00000000ull) | (s & 0xffff00000000ffffull);
+		const u64 s = golden_ratio2d_next(state);
 		const float ux = sample_uniform(u32(s & 0xffffffffull));
 		const float uy = sample_uniform(u32(s >> 32ull));
 		const V3 tx = l.posV[1] + ux * l.posV[3];
@@ -2954,20 +2980,7 @@ Scene* create_scene(const OrSceneDesc* d) {
 	if(T.lights.size() > 1) {
 		const V3 scale = sceneBox.mx - sceneBox.mn;
 		auto conv = [](float v) { return v <= 0.0f ? 0u : (v >= 4294967040.0f ? 0xFFFFFF00u : u32(v)); };
-		auto p16 = [](u32 x) {
-			u64 r = x & 0xFFFF;
-			r = (r | (r << 16)) & 0x0000ff0000ffull;
-			r = (r | (r << 8)) & 0x00f00f00f00full;
-			r = (r | (r << 4)) & 0x0c30c30c30c3ull;
-			r = (r | (r << 2)) & 0x249249249249ull;
-			return r;
-		};
-		auto hilbert = [&](u32 a, u32 b, u32 c) {
-			u64 num = p16(a) | (p16(b) << 1u) | (p16(c) << 2u);
-			num = num ^ (num >> 32); num = num ^ (num >> 16); num = num ^ (num >> 8);
-			num = num ^ (num >> 4); num = num ^ (num >> 2); num = num ^ (num >> 1);
-			return num;
-		};
+		auto hilbert = [](u32 a, u32 b, u32 c) { return hilbert_code16(a, b, c); };
 		std::stable_sort(T.lights.begin(), T.lights.end(), [&](const PosLight& a, const PosLight& b) {
 			const V3 ca = light_center(a) * scale, cb = light_center(b) * scale;
 			const u32 ax = conv(ca.x), ay = conv(ca.y), az = conv(ca.z);
@@ -3344,6 +3357,14 @@ int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents) {
 uint64_t oracle_pcg64_seed(uint32_t seed) { return Pcg64::seeded(seed).state; }
 uint64_t oracle_pcg64_next(uint64_t* state) { Pcg64 r; r.state = *state; u64 v = r.next(); *state = r.state; return v; }
 uint64_t oracle_part_by_two21(uint32_t x) { return part_by_two21(x); }
+uint64_t oracle_scramble_seed(uint32_t x) { return scramble_seed(x); }
+void oracle_golden_ratio2d(uint32_t seed, uint32_t n, uint64_t* out) {
+	u64 state = scramble_seed(seed);
+	for(uint32_t i = 0; i < n; ++i) out[i] = golden_ratio2d_next(state);
+}
+uint64_t oracle_part_by_two16(uint32_t x) { return part_by_two16(x); }
+uint64_t oracle_morton_code16(uint32_t a, uint32_t b, uint32_t c) { return morton_code16(a, b, c); }
+uint64_t oracle_hilbert_code16(uint32_t a, uint32_t b, uint32_t c) { return hilbert_code16(a, b, c); }
 void oracle_sincos(float x, float* s, float* c) { mbmath::sincos(x, *s, *c); }
 float oracle_atan2(float y, float x) { return mbmath::atan2(y, x); }
 float oracle_acos(float x) { return mbmath::acos(x); }

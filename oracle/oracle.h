@@ -177,6 +177,12 @@ int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);
 uint64_t oracle_pcg64_seed(uint32_t seed);
 uint64_t oracle_part_by_two21(uint32_t x);
+uint64_t oracle_scramble_seed(uint32_t x);
+/* The first n outputs of GoldenRatio2D(seed) (rng.hpp:119-140). */
+void oracle_golden_ratio2d(uint32_t seed, uint32_t n, uint64_t* out);
+uint64_t oracle_part_by_two16(uint32_t x);
+uint64_t oracle_morton_code16(uint32_t a, uint32_t b, uint32_t c);
+uint64_t oracle_hilbert_code16(uint32_t a, uint32_t b, uint32_t c);
 void oracle_sincos(float x, float* s, float* c);
 float oracle_atan2(float y, float x);
 float oracle_acos(float x);

@@ -119,6 +119,15 @@ def lib():
         L.oracle_pcg64_next.argtypes = [C.POINTER(C.c_uint64)]
         L.oracle_part_by_two21.restype = C.c_uint64
         L.oracle_part_by_two21.argtypes = [C.c_uint32]
+        L.oracle_scramble_seed.restype = C.c_uint64
+        L.oracle_scramble_seed.argtypes = [C.c_uint32]
+        L.oracle_golden_ratio2d.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p]
+        for f in ("oracle_part_by_two16",):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_uint32]
+        for f in ("oracle_morton_code16", "oracle_hilbert_code16"):
+            getattr(L, f).restype = C.c_uint64
+            getattr(L, f).argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
         L.oracle_karras.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.oracle_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.oracle_atan2.restype = C.c_float
