@@ -578,6 +578,39 @@ def run_adjoint(args):
         ora = {"max_abs_err_over_max": float(np.abs(g - ref).max() / scale),
                "max_rel_err_significant": float(np.max(np.abs(g[big] - ref[big]) / np.abs(ref[big]))),
                "cpu_seconds": round(cpu_s, 2), "cpu_cores": os.cpu_count()}
+    # the emission adjoint of the ceiling light on the same scene (Russian
+    # roulette on, as a plain render): its replay against its forward pass,
+    # checked against the FP64 oracle gradient and central differences
+    from mufflon_b200.adjoint import EmissionRenderer
+    li = [i for i, m in enumerate(spec.materials) if m.type == scenes.MAT_EMISSIVE][0]
+    d.texture_update(d.textures[0], tex)
+    e = EmissionRenderer(d, d.materials[li], spp=spp, seed=0, max_path=depth, rr_start=0)
+    L0 = np.array([15.0, 15.0, 15.0], np.float32)
+    efwd, eadj = [], []
+    for _ in range(3 + args.steps):
+        eimg = e.render(L0)
+        edldi = 2.0 * (eimg - target)
+        eg = e.gradient(edldi)
+        efwd.append(e.last_forward_ms)
+        eadj.append(e.last_adjoint_ms)
+    efwd_ms, eadj_ms = float(np.median(efwd[3:])), float(np.median(eadj[3:]))
+    eloss = lambda L: float(np.sum((e.render(L).astype(np.float64) - target) ** 2))
+    efd = []
+    for c in range(3):
+        lp, lm = L0.copy(), L0.copy()
+        lp[c] += 1e-3
+        lm[c] -= 1e-3
+        efd.append(abs((eloss(lp) - eloss(lm)) / 2e-3 - eg[c]) / abs(eg[c]))
+    eora = None
+    if not args.no_cpu_baseline:
+        import dataclasses
+        mats = list(spec.materials)
+        mats[li] = scenes.MaterialSpec(scenes.MAT_EMISSIVE, radiance=tuple(float(x) for x in L0), name="light")
+        pte = pyoracle.OraclePathTracer(pyoracle.OracleScene(dataclasses.replace(dataclasses_replace_texture(spec, tex),
+                                                                                 materials=mats)),
+                                        seed=0, max_path=depth, rr_start=0)
+        eref = pte.emission_gradient(li, spp, edldi)
+        eora = {"max_rel_err": float(np.max(np.abs(eg - eref) / np.abs(eref)))}
     line = {"metric": "adjoint/forward time (512^2, 16 spp, depth 6, 512^2 albedo texture)",
             "value": round(adj_ms / fwd_ms, 3), "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
             "data": "synthetic", "dtype": "f32",
@@ -585,7 +618,11 @@ def run_adjoint(args):
                        "texture": [tsz, tsz, 3], "russian_roulette": "off"},
             "forward_ms": round(fwd_ms, 3), "adjoint_ms": round(adj_ms, 3),
             "fd_check": {"texels": len(fd_err), "step": 0.1, "max_rel_err": float(np.max(fd_err))},
-            "fp64_oracle_check": ora}
+            "fp64_oracle_check": ora,
+            "emission": {"ratio": round(eadj_ms / efwd_ms, 3), "forward_ms": round(efwd_ms, 3),
+                         "adjoint_ms": round(eadj_ms, 3), "russian_roulette": "on",
+                         "fd_check": {"step": 1e-3, "max_rel_err": float(np.max(efd))},
+                         "fp64_oracle_check": eora}}
     print(json.dumps(line), flush=True)
     d.close()
 

@@ -374,6 +374,20 @@ CORE_API Boolean CDECL mufflon_render_batch(const MufflonBatchJob* jobs, uint32_
 CORE_API Boolean CDECL mufflon_texture_update(MufflonInstanceHdl instHdl, TextureHdl texture, const float* rgba);
 CORE_API Boolean CDECL mufflon_albedo_gradient(MufflonInstanceHdl instHdl, TextureHdl texture, uint32_t spp,
                                                const float* imageGrad, float* textureGrad, float* deviceMs);
+/* mufflon_emission_gradient: the same path replay for the emitted radiance
+ * L = radiance x scale of an emissive material (EmissiveParams,
+ * core_interface.h:263-266; the CUDA renderer takes a constant radiance, a
+ * 1x1 value texture, so L is that texel times the scale): radianceGrad
+ * receives dLoss/dL (3 floats, RGB), summed over every material slot of the
+ * scenario that uses the material. Each term the material emits (hits of its
+ * surfaces and next-event samples of its area lights) is linear in L, and the
+ * sampling probabilities and MIS weights are held fixed; Russian roulette may
+ * be on. Channels with L = 0 get 0. mufflon_set_emitted_radiance replaces L
+ * (3 floats) of an emissive material; the scene, whose light fluxes depend
+ * on it, is rebuilt before the next render, and the accumulation is reset. */
+CORE_API Boolean CDECL mufflon_emission_gradient(MufflonInstanceHdl instHdl, MaterialHdl material, uint32_t spp,
+                                                 const float* imageGrad, float* radianceGrad, float* deviceMs);
+CORE_API Boolean CDECL mufflon_set_emitted_radiance(MufflonInstanceHdl instHdl, MaterialHdl material, const float* rgb);
 
 /* Host-side times (ms) of the last scene load (world_load_scenario or the
  * implicit load of the first render_iterate): the whole load, the geometry

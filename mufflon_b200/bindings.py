@@ -334,6 +334,8 @@ class DllHolder:
             "mufflon_get_lt_records": (c_uint32, [c_void_p, c_void_p, c_void_p, c_uint64]),
             "mufflon_texture_update": (c_uint32, [c_void_p, c_void_p, c_void_p]),
             "mufflon_albedo_gradient": (c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_float)]),
+            "mufflon_emission_gradient": (c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, POINTER(c_float)]),
+            "mufflon_set_emitted_radiance": (c_uint32, [c_void_p, c_void_p, c_void_p]),
             "mufflon_render_batch": (c_uint32, [POINTER(MufflonBatchJob), c_uint32, c_int32, c_void_p, c_void_p,
                                                 POINTER(c_float), POINTER(MufflonBatchStats)]),
             "mufflon_trace_rays": (c_uint32, [c_void_p, c_void_p, c_void_p, c_float, c_uint32, c_void_p, c_void_p,
@@ -624,6 +626,23 @@ class DllInterface:
                                                       byref(ms)), "mufflon_albedo_gradient")
         return out, ms.value
 
+    def emission_gradient(self, material, spp, image_grad):
+        """dLoss/dL (3,) for the emitted radiance L (radiance x scale) of an emissive material, for
+        imageGrad = dLoss/dImage (H, W, 3) of the spp-sample image; returns (gradient, device ms)."""
+        g = np.ascontiguousarray(image_grad, np.float32)
+        out = np.zeros(3, np.float32)
+        ms = c_float(0.0)
+        self._check(self.core.mufflon_emission_gradient(self.muffInst, material, int(spp), g.ctypes.data,
+                                                        out.ctypes.data, byref(ms)), "mufflon_emission_gradient")
+        return out, ms.value
+
+    def set_emitted_radiance(self, material, rgb):
+        """Replaces the emitted radiance (radiance x scale) of an emissive material; the scene is rebuilt
+        before the next render."""
+        a = np.ascontiguousarray(rgb, np.float32).reshape(3)
+        self._check(self.core.mufflon_set_emitted_radiance(self.muffInst, material, a.ctypes.data),
+                    "mufflon_set_emitted_radiance")
+
     def trace_rays(self, rays, tmax=1048576.0, geo_normals=None):
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
@@ -731,6 +750,7 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
         dll._check(t, "world_add_texture_rgba32f")
         textures.append(t)
     dll.textures = textures
+    dll.materials = []  # material handles in the spec's order (its slot indices)
     for i, m in enumerate(spec.materials):
         name = f"mat{i}".encode()
         slot = core.scenario_declare_material_slot(sc, name, len(name))
@@ -751,6 +771,7 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
             p.inner.emissive.scale = Vec3(*m.scale)
         mh = core.world_add_material(I, name, byref(p))
         dll._check(mh, "world_add_material")
+        dll.materials.append(mh)
         dll._check(core.scenario_assign_material(sc, slot, mh), "scenario_assign_material")
     objs = []
     for li, lod in enumerate(spec.lods):

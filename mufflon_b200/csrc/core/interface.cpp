@@ -1573,6 +1573,7 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 		CHECK((in.neeCount > 0 ? in.neeCount : 1) == nee, "all jobs of a batch must use the same NEE count");
 		DJob& d = hj[j];
 		d.scene = I.scene.desc;
+		d.sceneGroup = uint32_t(std::lower_bound(uniq.begin(), uniq.end(), insts[j]) - uniq.begin());
 		d.scene.maxSteps = step_limit(I.renderer);
 		d.scene.camera.resX = uint16_t(w);
 		d.scene.camera.resY = uint16_t(h);
@@ -1638,6 +1639,8 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	tune.sortBits = r0.sortBits;
 	tune.sortDirBits = r0.sortDirBits;
 	tune.counters = false;
+	// binning keeps the rays of different scenes apart: the scene's index among the batch's instances
+	while((size_t(1) << tune.sortGroupBits) < uniq.size()) ++tune.sortGroupBits;
 	prepare_batch_kernels(tune);
 	while(B.events.size() < size_t(maxSpp) + 1) {
 		cudaEvent_t e;
@@ -1724,35 +1727,29 @@ Boolean mufflon_texture_update(MufflonInstanceHdl h, TextureHdl texHdl, const fl
 	CATCH_ALL(false)
 }
 
-Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_t spp, const float* imageGrad,
-                                float* textureGrad, float* deviceMs) {
-	TRY
-	MufflonInstance& I = minst(h);
-	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
-	CHECK(texHdl && imageGrad && textureGrad && spp >= 1, "invalid arguments");
-	CHECK(I.current != nullptr, "no scenario loaded");
-	load_scene_if_needed(I);
+// The path-replay adjoint of the loaded scenario: spp samples of every pixel,
+// replayed from generators seeded as for a reset render, differentiating an
+// albedo texture (texIndex >= 0, gradient texGradOut of nt texels) and/or the
+// emitted radiance of the material slots flagged in emitTarget (3 floats to
+// emisGradOut).
+static void run_adjoint(MufflonInstance& I, uint32_t spp, const float* imageGrad, int texIndex, size_t nt,
+                        float* texGradOut, const std::vector<unsigned char>* emitTarget, float* emisGradOut,
+                        float* deviceMs) {
 	const RendererState& r = I.renderer;
-	CHECK(r.params.rrStartDepth >= r.params.maxPathLength,
-	      "the albedo adjoint needs Russian roulette off: RR start depth >= Max. path length");
-	CHECK(r.params.maxPathLength <= ADJOINT_MAX_PATH, "the albedo adjoint supports paths of at most 32 vertices");
-	const HostTexture* t = static_cast<const HostTexture*>(texHdl);
-	int texIndex = -1;
-	for(size_t k = 0; k < I.scene.textureSources.size(); ++k)
-		if(I.scene.textureSources[k] == t) texIndex = int(k);
-	CHECK(texIndex >= 0, "the texture is not an albedo texture of the loaded scenario");
+	CHECK(r.params.maxPathLength <= ADJOINT_MAX_PATH, "the adjoint supports paths of at most 32 vertices");
 	const uint32_t w = I.current->width, hgt = I.current->height;
-	const size_t n = size_t(w) * hgt, nt = size_t(t->width) * t->height;
+	const size_t n = size_t(w) * hgt;
 	DScene desc = I.scene.desc;
 	desc.maxSteps = step_limit(r);
 	desc.camera.resX = uint16_t(w);
 	desc.camera.resY = uint16_t(hgt);
 	uint64_t* rng = nullptr;
-	float *dImg = nullptr, *dGrad = nullptr;
+	float *dImg = nullptr, *dGrad = nullptr, *dEmis = nullptr;
+	unsigned char* dTarget = nullptr;
 	void* adjMem = nullptr;
 	cudaEvent_t a = nullptr, b = nullptr;
 	auto cleanup = [&]() {
-		cudaFree(rng); cudaFree(dImg); cudaFree(dGrad); cudaFree(adjMem);
+		cudaFree(rng); cudaFree(dImg); cudaFree(dGrad); cudaFree(dEmis); cudaFree(dTarget); cudaFree(adjMem);
 		if(a) cudaEventDestroy(a);
 		if(b) cudaEventDestroy(b);
 	};
@@ -1765,11 +1762,24 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		if(wavefront) CHECK_CUDA(cudaMalloc(&adjMem, adjoint_bytes(n, r.params.maxPathLength)));
 		CHECK_CUDA(cudaMalloc(&rng, n * 8));
 		CHECK_CUDA(cudaMalloc(&dImg, n * 12));
-		CHECK_CUDA(cudaMalloc(&dGrad, nt * 12));
+		AdjointTargets T;
+		if(texIndex >= 0) {
+			CHECK_CUDA(cudaMalloc(&dGrad, nt * 12));
+			CHECK_CUDA(cudaMemsetAsync(dGrad, 0, nt * 12, I.stream));
+			T.texIndex = texIndex;
+			T.texGrad = dGrad;
+		}
+		if(emitTarget) {
+			CHECK_CUDA(cudaMalloc(&dEmis, 12));
+			CHECK_CUDA(cudaMalloc(&dTarget, emitTarget->size()));
+			CHECK_CUDA(cudaMemsetAsync(dEmis, 0, 12, I.stream));
+			CHECK_CUDA(cudaMemcpyAsync(dTarget, emitTarget->data(), emitTarget->size(), cudaMemcpyHostToDevice, I.stream));
+			T.emitTarget = dTarget;
+			T.emisGrad = dEmis;
+		}
 		CHECK_CUDA(cudaEventCreate(&a));
 		CHECK_CUDA(cudaEventCreate(&b));
 		CHECK_CUDA(cudaMemcpyAsync(dImg, imageGrad, n * 12, cudaMemcpyHostToDevice, I.stream));
-		CHECK_CUDA(cudaMemsetAsync(dGrad, 0, nt * 12, I.stream));
 		CHECK_CUDA(launch_seed_rng(rng, uint32_t(n), r.params.seed, I.stream));
 		CHECK_CUDA(cudaEventRecord(a, I.stream));
 		WfTuning tune;
@@ -1783,13 +1793,14 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		if(wavefront) CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 		for(uint32_t s = 0; s < spp; ++s) {
 			if(wavefront)
-				CHECK_CUDA(launch_adjoint_wavefront(desc, r.params, rng, w, hgt, r.wf, adjMem, r.params.maxPathLength, texIndex,
-				                                    dImg, 1.0f / float(spp), dGrad, r.counters, I.stream, tune));
+				CHECK_CUDA(launch_adjoint_wavefront(desc, r.params, rng, w, hgt, r.wf, adjMem, r.params.maxPathLength, T,
+				                                    dImg, 1.0f / float(spp), r.counters, I.stream, tune));
 			else
-				CHECK_CUDA(launch_adjoint_albedo(desc, r.params, rng, w, hgt, texIndex, dImg, 1.0f / float(spp), dGrad, I.stream));
+				CHECK_CUDA(launch_adjoint_albedo(desc, r.params, rng, w, hgt, T, dImg, 1.0f / float(spp), I.stream));
 		}
 		CHECK_CUDA(cudaEventRecord(b, I.stream));
-		CHECK_CUDA(cudaMemcpyAsync(textureGrad, dGrad, nt * 12, cudaMemcpyDeviceToHost, I.stream));
+		if(texIndex >= 0) CHECK_CUDA(cudaMemcpyAsync(texGradOut, dGrad, nt * 12, cudaMemcpyDeviceToHost, I.stream));
+		if(emitTarget) CHECK_CUDA(cudaMemcpyAsync(emisGradOut, dEmis, 12, cudaMemcpyDeviceToHost, I.stream));
 		TraceCounters tc[2] = {};
 		if(wavefront) CHECK_CUDA(cudaMemcpyAsync(tc, r.counters, sizeof(tc), cudaMemcpyDeviceToHost, I.stream));
 		CHECK_CUDA(cudaStreamSynchronize(I.stream));
@@ -1800,6 +1811,66 @@ Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_
 		throw;
 	}
 	cleanup();
+}
+
+Boolean mufflon_albedo_gradient(MufflonInstanceHdl h, TextureHdl texHdl, uint32_t spp, const float* imageGrad,
+                                float* textureGrad, float* deviceMs) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(texHdl && imageGrad && textureGrad && spp >= 1, "invalid arguments");
+	CHECK(I.current != nullptr, "no scenario loaded");
+	load_scene_if_needed(I);
+	const RendererState& r = I.renderer;
+	CHECK(r.params.rrStartDepth >= r.params.maxPathLength,
+	      "the albedo adjoint needs Russian roulette off: RR start depth >= Max. path length");
+	const HostTexture* t = static_cast<const HostTexture*>(texHdl);
+	int texIndex = -1;
+	for(size_t k = 0; k < I.scene.textureSources.size(); ++k)
+		if(I.scene.textureSources[k] == t) texIndex = int(k);
+	CHECK(texIndex >= 0, "the texture is not an albedo texture of the loaded scenario");
+	run_adjoint(I, spp, imageGrad, texIndex, size_t(t->width) * t->height, textureGrad, nullptr, nullptr, deviceMs);
+	return true;
+	CATCH_ALL(false)
+}
+
+// dLoss/dL for the emitted radiance L = radiance x scale of an emissive
+// material, over every material slot of the loaded scenario that uses it.
+Boolean mufflon_emission_gradient(MufflonInstanceHdl h, MaterialHdl material, uint32_t spp, const float* imageGrad,
+                                  float* radianceGrad, float* deviceMs) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(material && imageGrad && radianceGrad && spp >= 1, "invalid arguments");
+	CHECK(I.current != nullptr, "no scenario loaded");
+	const HostMaterial* m = static_cast<const HostMaterial*>(material);
+	CHECK(m->type == MAT_EMISSIVE, "the material is not emissive");
+	load_scene_if_needed(I);
+	const auto& slots = I.current->slotMaterials;
+	std::vector<unsigned char> target(std::max<size_t>(slots.size(), 1), 0);
+	bool used = false;
+	for(size_t k = 0; k < slots.size(); ++k)
+		if(slots[k] == m) { target[k] = 1; used = true; }
+	CHECK(used, "the material is not used by the loaded scenario");
+	run_adjoint(I, spp, imageGrad, -1, 0, nullptr, &target, radianceGrad, deviceMs);
+	return true;
+	CATCH_ALL(false)
+}
+
+// Replaces the emitted radiance (radiance x scale) of an emissive material;
+// the scene (its light list and tree, whose fluxes depend on it) is rebuilt
+// before the next render.
+Boolean mufflon_set_emitted_radiance(MufflonInstanceHdl h, MaterialHdl material, const float* rgb) {
+	TRY
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	CHECK(material && rgb, "invalid arguments");
+	HostMaterial* m = static_cast<HostMaterial*>(material);
+	CHECK(m->type == MAT_EMISSIVE, "the material is not emissive");
+	m->emissionOverride = true;
+	for(int c = 0; c < 3; ++c) m->emission[c] = rgb[c];
+	I.sceneDirty = true;
+	I.renderer.needsReset = true;
 	return true;
 	CATCH_ALL(false)
 }

@@ -233,8 +233,8 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 			d.roughness[1] = m->roughness->channels > 1 ? m->roughness->texels[1] : m->roughness->texels[0];
 		} else { d.roughness[0] = d.roughness[1] = 0.5f; }
 		if(m->type == MAT_EMISSIVE) {
-			const V3 rad = tex_value(m->radiance, V3{ 0, 0, 0 });
-			st3(d.radiance, rad * ld3(m->scale));
+			if(m->emissionOverride) st3(d.radiance, ld3(m->emission));
+			else st3(d.radiance, tex_value(m->radiance, V3{ 0, 0, 0 }) * ld3(m->scale));
 		}
 	}
 

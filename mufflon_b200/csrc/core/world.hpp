@@ -95,6 +95,8 @@ struct HostMaterial {
 	float scale[3] = { 1, 1, 1 };
 	int32_t shadowing = 1, ndf = 1;
 	bool supported = true;
+	bool emissionOverride = false; // mufflon_set_emitted_radiance: emission replaces radiance x scale
+	float emission[3] = { 0, 0, 0 };
 };
 
 struct HostCamera {

@@ -301,6 +301,7 @@ struct Nee {
 	f3 geoNormal;
 	float distSq;
 	bool valid;
+	int emitMat;      // material of the sampled area light; -1 for point lights and the background
 };
 
 MBD f3 lv(const float* p) { return make3(p[0], p[1], p[2]); }
@@ -326,6 +327,7 @@ MBD Nee connect_quad(const DScene& S, const DLight& l, f3 pos, float u0, float u
 	Nee n;
 	n.position = position; n.creationPdf = pdf; n.dir = direction; n.cosOut = vcos;
 	n.diffIrradiance = value / distSq; n.geoNormal = normal; n.distSq = distSq; n.valid = true;
+	n.emitMat = int(l.material);
 	return n;
 }
 
@@ -352,6 +354,7 @@ MBD Nee connect_tri(const DScene& S, const DLight& l, f3 pos, float u0, float u1
 	Nee n;
 	n.position = position; n.creationPdf = pdf; n.dir = direction; n.cosOut = vcos;
 	n.diffIrradiance = value / distSq; n.geoNormal = normal; n.distSq = distSq; n.valid = true;
+	n.emitMat = int(l.material);
 	return n;
 }
 
@@ -363,6 +366,7 @@ MBD Nee connect_point(const DLight& l, f3 pos) {
 	Nee n;
 	n.position = lv(l.position); n.creationPdf = INF_PDF; n.dir = direction; n.cosOut = 0.0f;
 	n.diffIrradiance = lv(l.intensity) / distSq; n.geoNormal = make3(0, 0, 0); n.distSq = distSq; n.valid = true;
+	n.emitMat = -1;
 	return n;
 }
 
@@ -376,6 +380,7 @@ MBD Nee connect_background(const DScene& S, f3 pos, float u0, float u1) {
 	Nee n;
 	n.position = pos + dir * len(diag); n.creationPdf = creation; n.dir = dir; n.cosOut = 1.0f;
 	n.diffIrradiance = diff; n.geoNormal = make3(0, 0, 0); n.distSq = MAX_SCENE_SIZE * MAX_SCENE_SIZE; n.valid = true;
+	n.emitMat = -1;
 	return n;
 }
 

@@ -86,11 +86,12 @@ MBD unsigned octa_cell(f3 d) {
 	return cu << 3 | cv;
 }
 
-// Coherence key of a ray: W.sortDirBits of direction above a Morton code of
-// the origin's cell in the scene box with the remaining bits (x gets the
-// extra bit when they do not divide by three, then y).
-MBD unsigned ray_key(const WfState& W, const DScene& S, f3 o, f3 d) {
-	const int mb = W.sortBits - W.sortDirBits;
+// Coherence key of a ray: its group (W.sortGroupBits: the scene of a batch
+// job) above W.sortDirBits of direction above a Morton code of the origin's
+// cell in the scene box with the remaining bits (x gets the extra bit when
+// they do not divide by three, then y).
+MBD unsigned ray_key(const WfState& W, const DScene& S, unsigned group, f3 o, f3 d) {
+	const int mb = W.sortBits - W.sortGroupBits - W.sortDirBits;
 	const int bb[3] = { (mb + 2) / 3, (mb + 1) / 3, mb / 3 };
 	const float oc[3] = { o.x, o.y, o.z };
 	unsigned cell[3];
@@ -107,7 +108,7 @@ MBD unsigned ray_key(const WfState& W, const DScene& S, f3 o, f3 d) {
 	unsigned dir = 0;
 	if(W.sortDirBits == 3) dir = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
 	else if(W.sortDirBits == 6) dir = octa_cell(d);
-	return dir << mb | key;
+	return (group << (W.sortBits - W.sortGroupBits)) | dir << mb | key;
 }
 
 // Records `key` for entry i and counts it (one atomic per key per warp).
@@ -179,14 +180,21 @@ struct OneScene {
 	PtParams P;
 	MBD const DScene& scene(int) const { return S; }
 	MBD const PtParams& params(int) const { return P; }
+	MBD unsigned group(int) const { return 0u; } // binning group of a path's rays
 };
 
 // Per-path bookkeeping of the albedo adjoint (path replay through the
 // wavefront kernels): for every Lambert vertex that looked up albedo texture
 // texIndex, its texel and albedo and the sum of the radiance terms added
 // after it. Entry k of path p lives at k * numPaths + p.
+//
+// The same replay gives the derivative with respect to the emitted radiance
+// L (radiance x scale) of the emissive materials flagged in emitTarget: each
+// term such a material emits (an emitter hit, or a next-event sample of one
+// of its area lights) is linear in L, so it adds term / L to the path's
+// emisAcc, which k_adjoint_scatter weights by dL/dI and sums.
 struct AdjointState {
-	int texIndex;
+	int texIndex;      // albedo texture, or -1: no albedo gradient
 	uint32_t numPaths, maxEntries;
 	DTexture tex;
 	int* count;        // entries per path
@@ -195,6 +203,9 @@ struct AdjointState {
 	const float* imageGrad;
 	float scale;
 	float* texGrad;
+	const unsigned char* emitTarget; // per material slot: 1 if its emission is differentiated; null: none
+	float4* emisAcc;   // per path: sum of term / L over the target's terms
+	float* emisGrad;   // 3 floats: dLoss/dL
 };
 MBD void adjoint_add(const AdjointState& A, int p, f3 c) {
 	const int n = A.count[p];
@@ -202,6 +213,15 @@ MBD void adjoint_add(const AdjointState& A, int p, f3 c) {
 		float4& s = A.suffix[size_t(k) * A.numPaths + p];
 		s.x += c.x; s.y += c.y; s.z += c.z;
 	}
+}
+// A term c emitted by material slot `mat` (-1: not an emissive material).
+MBD void adjoint_emitted(const AdjointState& A, const DScene& S, int p, f3 c, int mat) {
+	if(!A.emitTarget || mat < 0 || !__ldg(A.emitTarget + mat)) return;
+	const f3 L = load3(S.materials[mat].radiance);
+	float4& a = A.emisAcc[p];
+	if(L.x > 0.0f) a.x += __fdiv_rn(c.x, L.x);
+	if(L.y > 0.0f) a.y += __fdiv_rn(c.y, L.y);
+	if(L.z > 0.0f) a.z += __fdiv_rn(c.z, L.z);
 }
 struct VertexInfo;
 MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, bool surface, int type, int mat, f2 uv,
@@ -215,6 +235,7 @@ struct OneSceneAdjoint {
 	AdjointState A;
 	MBD const DScene& scene(int) const { return S; }
 	MBD const PtParams& params(int) const { return P; }
+	MBD unsigned group(int) const { return 0u; }
 };
 struct JobScenes {
 	static constexpr bool adjoint = false;
@@ -222,6 +243,8 @@ struct JobScenes {
 	const uint16_t* pathJob;
 	MBD const DScene& scene(int p) const { return jobs[pathJob[p]].scene; }
 	MBD const PtParams& params(int p) const { return jobs[pathJob[p]].params; }
+	// rays of jobs on the same scene are binned together, apart from other scenes'
+	MBD unsigned group(int p) const { return jobs[pathJob[p]].sceneGroup; }
 };
 
 // Primary ray of one path (pinhole_ray, the camera's and the first walk's
@@ -367,9 +390,14 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 				stats_add(stats, 1, cnt);
 				const unsigned slot = ent * unsigned(neeCount) + unsigned(ray);
 				if(!t.occluded) {
-					const f3 c = f4to3(__ldcs(W.sContrib + slot));
+					const float4 c4 = __ldcs(W.sContrib + slot);
+					const f3 c = f4to3(c4);
 					radiance = contribute(radiance, c);
-					if constexpr(SP::adjoint) adjoint_add(sp.A, path, contribute(make3(0.0f, 0.0f, 0.0f), c));
+					if constexpr(SP::adjoint) {
+						const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
+						adjoint_add(sp.A, path, cc);
+						adjoint_emitted(sp.A, sp.scene(path), path, cc, __float_as_int(c4.w));
+					}
 				}
 				++ray;
 				seek = true;
@@ -508,7 +536,7 @@ MBD bool shade_has_nee(const PtParams& P, const ShadeState& v) {
 // Next-event sample i at v (pt_common.hpp:105-124): draws its number; true
 // with the shadow ray and the term it adds when it can contribute.
 MBD bool shade_nee(const DScene& S, const PtParams& P, const ShadeState& v, const f3& throughput, u64& rng, u64 neeSeed,
-                   int i, f3& so, f3& sd, float& stmax, f3& c) {
+                   int i, f3& so, f3& sd, float& stmax, f3& c, int& emitMat) {
 	const u64 r = pcg_next(rng);
 	const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
 	const Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, v.position, nu0, nu1);
@@ -520,6 +548,7 @@ MBD bool shade_nee(const DScene& S, const PtParams& P, const ShadeState& v, cons
 	const float hitPdf = __fdiv_rn(val.pdfF * fabsf(nee.cosOut), nee.distSq);
 	const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
 	c = ((throughput * val.cosOut) * rad) * mis;
+	emitMat = nee.emitMat;
 	shadow_ray(v.position, nee.position, v.ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
 	return true;
 }
@@ -558,7 +587,8 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 		for(int i = 0; i < P.neeCount; ++i) {
 			f3 so, sd, c;
 			float stmax;
-			if(shade_nee(S, P, v, throughput, rng, neeSeed, i, so, sd, stmax, c)) shadow(i, so, sd, stmax, c);
+			int emitMat = -1;
+			if(shade_nee(S, P, v, throughput, rng, neeSeed, i, so, sd, stmax, c, emitMat)) shadow(i, so, sd, stmax, c, emitMat);
 		}
 	}
 	return shade_walk(P, v, throughput, pdfF, rng, nextO, nextD);
@@ -589,16 +619,16 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	unsigned base = 0xFFFFFFFFu;
 	f3 nextO, nextD;
 	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
-		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c) {
+		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c, int emitMat) {
 			if(base == 0xFFFFFFFFu) {
 				base = atomicAdd(W.counters + C_SHADOW0 + q, unsigned(P.neeCount));
 				for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
 				if(W.sortBits)
-					bin_append(W.shKey, W.binHist + (1u << W.sortBits), base / unsigned(P.neeCount), ray_key(W, S, so, sd));
+					bin_append(W.shKey, W.binHist + (1u << W.sortBits), base / unsigned(P.neeCount), ray_key(W, S, sp.group(p), so, sd));
 			}
 			W.sOrg[base + i] = pack(so, stmax);
 			W.sDir[base + i] = pack(sd, 0.0f);
-			W.sContrib[base + i] = pack(c, 0.0f);
+			W.sContrib[base + i] = pack(c, __int_as_float(emitMat)); // w: the emitter's material (adjoint)
 		}, [&](f3 e, const VertexInfo& v) {
 			if constexpr(SP::adjoint) adjoint_vertex(sp.A, S, p, e, v.surface, v.materialType, v.materialIndex, v.uv, v.albedo);
 		});
@@ -611,7 +641,7 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	W.qPath[out][nslot] = p;
 	W.qOrg[out][nslot] = pack(nextO, 0.0f);
 	W.qDir[out][nslot] = pack(nextD, 0.0f);
-	if(W.sortBits) bin_append(W.extKey, W.binHist, nslot, ray_key(W, S, nextO, nextD));
+	if(W.sortBits) bin_append(W.extKey, W.binHist, nslot, ray_key(W, S, sp.group(p), nextO, nextD));
 }
 
 // Shade stage of the wavefront over queue q, grid-stride over its entries
@@ -659,6 +689,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 	const unsigned lane = threadIdx.x & 31u;
 	int phase = T_IDLE;
 	int p = 0, b = 0, i = 0;
+	int emitMat = -1; // emitter material of the current shadow ray (adjoint)
 	f3 throughput = make3(0.0f, 0.0f, 0.0f), radiance = make3(0.0f, 0.0f, 0.0f), c = make3(0.0f, 0.0f, 0.0f);
 	float pdfF = 0.0f, radW = 0.0f;
 	u64 rng = 0, neeSeed = 0;
@@ -717,7 +748,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 			const DScene& S = sp.scene(p);
 			const PtParams& P = sp.params(p);
 			while(i < P.neeCount) {
-				if(shade_nee(S, P, v, throughput, rng, neeSeed, i, ro, rd, tmax, c)) { trace = shadow = true; break; }
+				if(shade_nee(S, P, v, throughput, rng, neeSeed, i, ro, rd, tmax, c, emitMat)) { trace = shadow = true; break; }
 				++i;
 			}
 			if(!trace) phase = T_WALK;
@@ -740,7 +771,11 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 		if(shadow) {
 			if(!t.occluded) {
 				radiance = contribute(radiance, c);
-				if constexpr(SP::adjoint) adjoint_add(sp.A, p, contribute(make3(0.0f, 0.0f, 0.0f), c));
+				if constexpr(SP::adjoint) {
+					const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
+					adjoint_add(sp.A, p, cc);
+					adjoint_emitted(sp.A, S, p, cc, emitMat);
+				}
 			}
 			++i;
 		} else {
@@ -790,7 +825,8 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, bool surface, int type, int mat, f2 uv,
                         f3 albedo) {
 	adjoint_add(A, p, e);
-	if(!surface || type != MAT_LAMBERT || __ldg(&S.materials[mat].albedoTex) != A.texIndex) return;
+	if(surface && type == MAT_EMISSIVE) adjoint_emitted(A, S, p, e, mat);
+	if(A.texIndex < 0 || !surface || type != MAT_LAMBERT || __ldg(&S.materials[mat].albedoTex) != A.texIndex) return;
 	const int k = A.count[p];
 	if(k >= int(A.maxEntries)) return;
 	const float fx = uv.x - floorf(uv.x), fy = uv.y - floorf(uv.y);
@@ -804,8 +840,28 @@ MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, boo
 
 // End of an adjoint sample: d(sample)/d(a_k) = suffix_k / a_k, weighted by
 // scale * dL/dI of the pixel, added to the texel gradient.
+// The emission derivative: sum over paths of scale * dL/dI * emisAcc, reduced
+// per warp before the atomics.
 __global__ void k_adjoint_scatter(AdjointState A) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(A.emitTarget) {
+		float3 e = make_float3(0.0f, 0.0f, 0.0f);
+		if(p < A.numPaths) {
+			const float4 a = A.emisAcc[p];
+			e = make_float3(A.imageGrad[3 * size_t(p)] * A.scale * a.x, A.imageGrad[3 * size_t(p) + 1] * A.scale * a.y,
+			                A.imageGrad[3 * size_t(p) + 2] * A.scale * a.z);
+		}
+		for(int off = 16; off > 0; off >>= 1) {
+			e.x += __shfl_down_sync(0xffffffffu, e.x, off);
+			e.y += __shfl_down_sync(0xffffffffu, e.y, off);
+			e.z += __shfl_down_sync(0xffffffffu, e.z, off);
+		}
+		if((threadIdx.x & 31u) == 0) {
+			if(e.x != 0.0f) atomicAdd(A.emisGrad, e.x);
+			if(e.y != 0.0f) atomicAdd(A.emisGrad + 1, e.y);
+			if(e.z != 0.0f) atomicAdd(A.emisGrad + 2, e.z);
+		}
+	}
 	if(p >= A.numPaths) return;
 	const int n = A.count[p];
 	if(n == 0) return;
@@ -832,15 +888,25 @@ __global__ void k_adjoint_scatter(AdjointState A) {
 // terms added after vertex k, its own next-event terms included) / a_k. The
 // suffix sums are kept per textured vertex (no subtraction of running sums),
 // and `scale * imageGrad[p] * suffix / a_k` is added to the gradient of the
-// texel the vertex looked up (nearest texel, as sample_texture).
+// texel the vertex looked up (nearest texel, as sample_texture). With
+// emission targets, each term emitted by a flagged material adds term / L to
+// d(radiance)/dL, weighted the same way and reduced per warp at the end.
 constexpr int ADJOINT_MAX_VERTICES = 32;
 
 __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const PtParams P, uint64_t* rng,
-                                                            uint32_t numPixels, uint32_t width, int texIndex,
-                                                            const float* __restrict__ imageGrad, float scale,
-                                                            float* texGrad) {
+                                                            uint32_t numPixels, uint32_t width, AdjointTargets T,
+                                                            const float* __restrict__ imageGrad, float scale) {
 	LocalStack stack;
-	const DTexture tex = S.textures[texIndex];
+	const int texIndex = T.texIndex;
+	const DTexture tex = texIndex >= 0 ? S.textures[texIndex] : DTexture{ 0, 0, nullptr };
+	f3 emisSum = make3(0.0f, 0.0f, 0.0f); // this thread's share of dLoss/dL
+	auto emitted = [&](f3 c, int mat, f3& acc) {
+		if(!T.emitTarget || mat < 0 || !__ldg(T.emitTarget + mat)) return;
+		const f3 L = load3(S.materials[mat].radiance);
+		if(L.x > 0.0f) acc.x += __fdiv_rn(c.x, L.x);
+		if(L.y > 0.0f) acc.y += __fdiv_rn(c.y, L.y);
+		if(L.z > 0.0f) acc.z += __fdiv_rn(c.z, L.z);
+	};
 	for(uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < numPixels; p += gridDim.x * blockDim.x) {
 		u64 r = rng[p];
 		(void)pcg_next(r); // create_camera
@@ -860,6 +926,7 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
 		int texel[ADJOINT_MAX_VERTICES];
 		f3 alb[ADJOINT_MAX_VERTICES], suf[ADJOINT_MAX_VERTICES];
 		int n = 0;
+		f3 em = make3(0.0f, 0.0f, 0.0f);
 		f3 radiance = make3(0.0f, 0.0f, 0.0f);
 		f3 origin = lv(S.camera.position);
 		add_epsilon(origin, dir, make3(0.0f, 0.0f, 0.0f));
@@ -868,16 +935,18 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
 			const HitRec hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
 			f3 nextO, nextD;
 			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, r, nullptr, nextO, nextD,
-				[&](int, f3 so, f3 sd, float stmax, f3 c) {
+				[&](int, f3 so, f3 sd, float stmax, f3 c, int emitMat) {
 					LocalCounters sc;
 					if(occluded_wide(S, so, sd, stmax, sc, stack)) return;
 					const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
 					radiance = radiance + cc;
 					for(int k = 0; k < n; ++k) suf[k] = suf[k] + cc;
+					emitted(cc, emitMat, em);
 				},
 				[&](f3 e, const VertexInfo& v) {
 					for(int k = 0; k < n; ++k) suf[k] = suf[k] + e;
-					if(v.surface && v.materialType == MAT_LAMBERT && n < ADJOINT_MAX_VERTICES &&
+					if(v.surface && v.materialType == MAT_EMISSIVE) emitted(e, v.materialIndex, em);
+					if(texIndex >= 0 && v.surface && v.materialType == MAT_LAMBERT && n < ADJOINT_MAX_VERTICES &&
 					   __ldg(&S.materials[v.materialIndex].albedoTex) == texIndex) {
 						const float fx = v.uv.x - floorf(v.uv.x), fy = v.uv.y - floorf(v.uv.y);
 						int x = int(fx * float(tex.width)), y = int(fy * float(tex.height));
@@ -897,10 +966,23 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
 		const f3 g = make3(imageGrad[3 * size_t(p)] * scale, imageGrad[3 * size_t(p) + 1] * scale,
 		                   imageGrad[3 * size_t(p) + 2] * scale);
 		for(int k = 0; k < n; ++k) {
-			float* t = texGrad + 3 * size_t(texel[k]);
+			float* t = T.texGrad + 3 * size_t(texel[k]);
 			if(alb[k].x > 0.0f && suf[k].x != 0.0f) atomicAdd(t, g.x * __fdiv_rn(suf[k].x, alb[k].x));
 			if(alb[k].y > 0.0f && suf[k].y != 0.0f) atomicAdd(t + 1, g.y * __fdiv_rn(suf[k].y, alb[k].y));
 			if(alb[k].z > 0.0f && suf[k].z != 0.0f) atomicAdd(t + 2, g.z * __fdiv_rn(suf[k].z, alb[k].z));
+		}
+		emisSum = emisSum + make3(g.x * em.x, g.y * em.y, g.z * em.z);
+	}
+	if(T.emitTarget) {
+		for(int off = 16; off > 0; off >>= 1) {
+			emisSum.x += __shfl_down_sync(0xffffffffu, emisSum.x, off);
+			emisSum.y += __shfl_down_sync(0xffffffffu, emisSum.y, off);
+			emisSum.z += __shfl_down_sync(0xffffffffu, emisSum.z, off);
+		}
+		if((threadIdx.x & 31u) == 0) {
+			if(emisSum.x != 0.0f) atomicAdd(T.emisGrad, emisSum.x);
+			if(emisSum.y != 0.0f) atomicAdd(T.emisGrad + 1, emisSum.y);
+			if(emisSum.z != 0.0f) atomicAdd(T.emisGrad + 2, emisSum.z);
 		}
 	}
 }
@@ -1027,8 +1109,11 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 	const unsigned shadeGrid = std::max(1u, std::min((numPaths + 127) / 128, unsigned(sms) * 16u));
 	const unsigned tailMax = unsigned(tuning.tailPaths < 0 ? 0 : tuning.tailPaths);
 	const bool binning = tuning.sortBits > 0 && W.extKey != nullptr;
-	W.sortBits = binning ? std::min(tuning.sortBits, WF_SORT_MAX_BITS) : 0;
-	W.sortDirBits = std::min(tuning.sortDirBits == 3 || tuning.sortDirBits == 6 ? tuning.sortDirBits : 0, W.sortBits);
+	// key bits: the group's above the direction and origin bits, at most WF_SORT_MAX_BITS in all
+	W.sortGroupBits = binning ? std::min(tuning.sortGroupBits, WF_SORT_MAX_BITS - 1) : 0;
+	W.sortBits = binning ? std::min(tuning.sortBits + W.sortGroupBits, WF_SORT_MAX_BITS) : 0;
+	W.sortDirBits = std::min(tuning.sortDirBits == 3 || tuning.sortDirBits == 6 ? tuning.sortDirBits : 0,
+	                         W.sortBits - W.sortGroupBits);
 	// After the shade of bounce b, the rays it queued are binned for the
 	// trace launch of bounce b + 1.
 	// every shade's counts are consumed by the scan that follows it, except
@@ -1137,32 +1222,33 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
 	W.binCursor = reinterpret_cast<unsigned*>(take((size_t(2) << WF_SORT_MAX_BITS) * 4));
 	W.sortBits = 0;
 	W.sortDirBits = 0;
+	W.sortGroupBits = 0;
 	W.ordered = 0;
 }
 
 cudaError_t launch_adjoint_albedo(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
-                                  int texIndex, const float* imageGrad, float scale, float* texGrad, cudaStream_t stream) {
+                                  const AdjointTargets& T, const float* imageGrad, float scale, cudaStream_t stream) {
 	const uint32_t n = width * height;
 	if(n == 0) return cudaSuccess;
 	static int sms = 0;
 	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
 	const unsigned blocks = std::min<unsigned>((n + 127) / 128, unsigned(sms) * 8u);
-	k_adjoint_albedo<<<blocks, 128, 0, stream>>>(S, P, rng, n, width, texIndex, imageGrad, scale, texGrad);
+	k_adjoint_albedo<<<blocks, 128, 0, stream>>>(S, P, rng, n, width, T, imageGrad, scale);
 	return cudaGetLastError();
 }
 
 size_t adjoint_bytes(size_t numPaths, int maxEntries) {
-	return wf_align(numPaths * 4) + 2 * wf_align(numPaths * size_t(maxEntries) * 16);
+	return wf_align(numPaths * 4) + 2 * wf_align(numPaths * size_t(maxEntries) * 16) + wf_align(numPaths * 16);
 }
 
 cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
-                                     WfState W, void* adjointMemory, int maxEntries, int texIndex, const float* imageGrad,
-                                     float scale, float* texGrad, TraceCounters* counters, cudaStream_t stream,
+                                     WfState W, void* adjointMemory, int maxEntries, const AdjointTargets& T,
+                                     const float* imageGrad, float scale, TraceCounters* counters, cudaStream_t stream,
                                      const WfTuning& tuning) {
 	const uint32_t n = width * height;
 	if(n == 0) return cudaSuccess;
 	AdjointState A;
-	A.texIndex = texIndex;
+	A.texIndex = T.texIndex;
 	A.numPaths = n;
 	A.maxEntries = uint32_t(maxEntries);
 	char* m = static_cast<char*>(adjointMemory);
@@ -1171,12 +1257,21 @@ cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_
 	A.entry = reinterpret_cast<float4*>(m);
 	m += wf_align(size_t(n) * maxEntries * 16);
 	A.suffix = reinterpret_cast<float4*>(m);
+	m += wf_align(size_t(n) * maxEntries * 16);
+	A.emisAcc = reinterpret_cast<float4*>(m);
 	A.imageGrad = imageGrad;
 	A.scale = scale;
-	A.texGrad = texGrad;
-	cudaError_t e = cudaMemcpyAsync(&A.tex, S.textures + texIndex, sizeof(DTexture), cudaMemcpyDeviceToHost, stream);
-	if(e == cudaSuccess) e = cudaStreamSynchronize(stream);
+	A.texGrad = T.texGrad;
+	A.emitTarget = T.emitTarget;
+	A.emisGrad = T.emisGrad;
+	A.tex = DTexture{ 0, 0, nullptr };
+	cudaError_t e = cudaSuccess;
+	if(T.texIndex >= 0) {
+		e = cudaMemcpyAsync(&A.tex, S.textures + T.texIndex, sizeof(DTexture), cudaMemcpyDeviceToHost, stream);
+		if(e == cudaSuccess) e = cudaStreamSynchronize(stream);
+	}
 	if(e == cudaSuccess) e = cudaMemsetAsync(A.count, 0, size_t(n) * 4, stream);
+	if(e == cudaSuccess && T.emitTarget) e = cudaMemsetAsync(A.emisAcc, 0, size_t(n) * 16, stream);
 	if(e != cudaSuccess) return e;
 	const int neeCount = P.neeCount > 0 ? P.neeCount : 1;
 	const int maxBounces = P.maxPathLength < 1 ? 1 : P.maxPathLength;

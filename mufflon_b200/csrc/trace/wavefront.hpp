@@ -34,6 +34,7 @@ struct WfState {
 	unsigned* binCursor;  // 2 << WF_SORT_MAX_BITS scatter cursors
 	int sortBits;         // key bits (0: no binning; at most WF_SORT_MAX_BITS)
 	int sortDirBits;      // of those, direction bits: 0, 3 (octant) or 6 (octahedral 8 x 8)
+	int sortGroupBits;    // of those, the top bits: the path's group (the scene of a batch job)
 	int ordered;          // set for a trace launch whose queues were binned
 };
 constexpr int WF_SORT_MAX_BITS = 16;
@@ -74,6 +75,7 @@ struct WfTuning {
 	int refillLanes = 32;      // idle lanes of a trace warp are refilled together once this many are idle (1..32)
 	int sortBits = 0;          // coherence binning of the queued rays before each trace launch of bounce >= 1
 	int sortDirBits = 3;       // (key bits in all, of them direction bits); 0 bits: trace in queue order
+	int sortGroupBits = 0;     // extra key bits above those for the path's group (batches: the job's scene)
 	bool counters = true;      // count node visits, primitive tests and instance entries (a slower kernel variant)
 };
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
@@ -96,14 +98,24 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W);
 // that a later stream capture does not have to.
 void prepare_batch_kernels(const WfTuning& tuning);
 
+// What a path-replay adjoint sample differentiates: an albedo texture
+// (Lambert vertices that look it up; requires Russian roulette off) and/or
+// the emitted radiance (radiance x scale) of flagged emissive material slots.
+// Both gradients are accumulated: texGrad w * h * 3 floats, emisGrad 3 floats.
+struct AdjointTargets {
+	int texIndex = -1;                         // -1: no albedo gradient
+	float* texGrad = nullptr;
+	const unsigned char* emitTarget = nullptr; // per material slot, 1: differentiate; null: no emission gradient
+	float* emisGrad = nullptr;
+};
+
 // One sample of the path-replay adjoint for every pixel: adds
-// scale * dL/dI(p) * d(sample radiance)/d(texel) to texGrad (w * h * 3 floats)
-// for the albedo texture texIndex of the scene (Lambert vertices). `rng` is
-// the replay's per-pixel generator state, seeded as for a reset render and
-// advanced one sample per launch. Requires Russian roulette off.
+// scale * dL/dI(p) * d(sample radiance)/d(parameter) to the targets'
+// gradients. `rng` is the replay's per-pixel generator state, seeded as for
+// a reset render and advanced one sample per launch.
 constexpr int ADJOINT_MAX_PATH = 32;
 cudaError_t launch_adjoint_albedo(const DScene& scene, const PtParams& params, uint64_t* rng, uint32_t width,
-                                  uint32_t height, int texIndex, const float* imageGrad, float scale, float* texGrad,
+                                  uint32_t height, const AdjointTargets& targets, const float* imageGrad, float scale,
                                   cudaStream_t stream);
 
 // The same adjoint sample through the wavefront kernels (one sample for
@@ -111,9 +123,9 @@ cudaError_t launch_adjoint_albedo(const DScene& scene, const PtParams& params, u
 // maxEntries) bytes of per-path bookkeeping, maxEntries >= the max path length.
 size_t adjoint_bytes(size_t numPaths, int maxEntries);
 cudaError_t launch_adjoint_wavefront(const DScene& scene, const PtParams& params, uint64_t* rng, uint32_t width,
-                                     uint32_t height, WfState W, void* adjointMemory, int maxEntries, int texIndex,
-                                     const float* imageGrad, float scale, float* texGrad, TraceCounters* counters,
-                                     cudaStream_t stream, const WfTuning& tuning);
+                                     uint32_t height, WfState W, void* adjointMemory, int maxEntries,
+                                     const AdjointTargets& targets, const float* imageGrad, float scale,
+                                     TraceCounters* counters, cudaStream_t stream, const WfTuning& tuning);
 
 // One job of a batch: its scene (a loaded scene of some library instance),
 // path-tracer parameters, resolution, sample count, its pixels' place in the
@@ -124,6 +136,7 @@ struct DJob {
 	uint32_t width, height, pixelOffset, spp;
 	float* radiance;  // width * height * 3, cumulative mean
 	float* hitId;     // width * height * 2, or null
+	uint32_t sceneGroup; // jobs that render the same loaded scene share it (ray binning)
 };
 
 // One iteration (sample) of every job with spp > iteration, all jobs' paths

@@ -57,6 +57,7 @@
 #include "../mufflon_b200/csrc/common/fmath.hpp"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <atomic>
 #include <cfloat>
@@ -1579,6 +1580,7 @@ struct Nee {
 	V3 geoNormal;
 	float distSq;
 	bool valid;
+	i32 emitMat = -1; // material of the sampled area light (-1: point light, background)
 };
 
 // light_sampling.hpp:143-171 + 369-390
@@ -1604,7 +1606,7 @@ Nee connect_quad(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) 
 	V3 value = { 0, 0, 0 }; float vcos = 0.0f, vpdf = 0.0f;
 	if(cosOut > 0.0f) { value = intensity; vcos = cosOut; vpdf = cosOut / PI; }
 	const V3 diff = value / distSq;
-	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true };
+	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true, i32(l.material) };
 }
 
 // light_sampling.hpp:117-140 + 347-368; sampling.hpp:123-128 (barycentric sample)
@@ -1628,7 +1630,7 @@ Nee connect_tri(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
 	V3 value = { 0, 0, 0 }; float vcos = 0.0f, vpdf = 0.0f;
 	if(cosOut > 0.0f) { value = intensity; vcos = cosOut; vpdf = cosOut / PI; }
 	const V3 diff = value / distSq;
-	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true };
+	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true, i32(l.material) };
 }
 
 // light_sampling.hpp:308-325
@@ -1816,13 +1818,26 @@ inline V3 pinhole_ray(const Camera& c, i32 px, i32 py, float u0, float u1, float
 // those terms contains the vertex's albedo once, so the derivative of the
 // sample with respect to that albedo is suffix / albedo. This is the CPU
 // reference of the GPU path-replay adjoint (test infrastructure).
+// The same replay also gives the derivative of the sample with respect to
+// the emitted radiance L (radiance x scale) of one emissive material
+// (emissionMat >= 0): every term that material emits, at an emitter hit or
+// through next-event estimation, is linear in L, so it adds term / L
+// (Russian roulette may stay on: its probabilities do not depend on L).
 struct AlbedoAdjoint {
 	i32 texIndex = -1;
 	int n = 0;
 	i32 texel[64];
 	double alb[64][3], suf[64][3];
+	i32 emissionMat = -1;
+	V3 emissionL = { 0, 0, 0 };
+	double emis[3] = { 0, 0, 0 };
 	void add_all(const V3& c) {
 		for(int k = 0; k < n; ++k) { suf[k][0] += c.x; suf[k][1] += c.y; suf[k][2] += c.z; }
+	}
+	void emitted(const V3& c, i32 mat) {
+		if(emissionMat < 0 || mat != emissionMat) return;
+		const float L[3] = { emissionL.x, emissionL.y, emissionL.z }, t[3] = { c.x, c.y, c.z };
+		for(int k = 0; k < 3; ++k) if(L[k] > 0.0f) emis[k] += double(t[k]) / double(L[k]);
 	}
 	void vertex(const Scene& S, const V3& e, bool surface, i32 type, i32 mat, V2 uv, V3 albedo);
 };
@@ -1861,7 +1876,11 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 						const float hitPdf = val.pdfF * std::fabs(nee.cosOut) / nee.distSq;
 						const float mis = 1.0f / (float(P.neeCount) + hitPdf / nee.creationPdf);
 						radiance = contribute(radiance, ((throughput * val.cosOut) * rad) * mis);
-						if(adj) adj->add_all(contribute(V3{ 0, 0, 0 }, ((throughput * val.cosOut) * rad) * mis));
+						if(adj) {
+							const V3 term = contribute(V3{ 0, 0, 0 }, ((throughput * val.cosOut) * rad) * mis);
+							adj->add_all(term);
+							adj->emitted(term, nee.emitMat);
+						}
 					}
 				}
 			}
@@ -1955,7 +1974,8 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 
 void AlbedoAdjoint::vertex(const Scene& S, const V3& e, bool surface, i32 type, i32 mat, V2 uv, V3 albedo) {
 	add_all(e);
-	if(!surface || type != OR_MAT_LAMBERT || n >= 64 || mat < 0 || S.materials[size_t(mat)].albedoTex != texIndex) return;
+	if(surface && type == OR_MAT_EMISSIVE) emitted(e, mat);
+	if(texIndex < 0 || !surface || type != OR_MAT_LAMBERT || n >= 64 || mat < 0 || S.materials[size_t(mat)].albedoTex != texIndex) return;
 	const Texture& t = S.textures[size_t(texIndex)];
 	const float fx = uv.x - std::floor(uv.x), fy = uv.y - std::floor(uv.y);
 	i32 x = i32(fx * float(t.w)), y = i32(fy * float(t.h));
@@ -3180,6 +3200,48 @@ int oracle_albedo_gradient(void* p, int32_t texIndex, uint32_t spp, const float*
 		double acc = 0.0;
 		for(auto& g : part) acc += g[i];
 		gradOut[i] = acc;
+	}
+	return 1;
+}
+
+int oracle_emission_gradient(void* p, int32_t matIndex, uint32_t spp, const float* imageGrad, double* gradOut, int32_t nt) {
+	PtState& st = *static_cast<PtState*>(p);
+	const Scene& S = *st.scene;
+	if(matIndex < 0 || size_t(matIndex) >= S.materials.size() || spp == 0) return 0;
+	const Material& m = S.materials[size_t(matIndex)];
+	if(m.type != OR_MAT_EMISSIVE) return 0;
+	const i32 num = i32(S.width * S.height);
+	const i32 seed = i32(u32(st.params.seed) * u32(num + 1));
+	if(nt <= 0) nt = 1;
+	std::vector<std::array<double, 3>> part(size_t(nt), std::array<double, 3>{ 0.0, 0.0, 0.0 });
+#pragma omp parallel num_threads(nt)
+	{
+		int tid = 0;
+#ifdef _OPENMP
+		tid = omp_get_thread_num();
+#endif
+		Counters cnt;
+		AlbedoAdjoint adj;
+		adj.emissionMat = matIndex;
+		adj.emissionL = m.radiance * m.scale;
+#pragma omp for schedule(static, 64)
+		for(i32 pixel = 0; pixel < num; ++pixel) {
+			Pcg64 rng = Pcg64::seeded(u32(i32(u32(pixel) + u32(seed))));
+			const double w[3] = { double(imageGrad[3 * size_t(pixel)]) / spp, double(imageGrad[3 * size_t(pixel) + 1]) / spp,
+			                      double(imageGrad[3 * size_t(pixel) + 2]) / spp };
+			for(u32 s = 0; s < spp; ++s) {
+				adj.n = 0;
+				adj.emis[0] = adj.emis[1] = adj.emis[2] = 0.0;
+				V3 rad; V2 hid;
+				pt_sample(st, pixel % i32(S.width), pixel / i32(S.width), rng, rad, hid, cnt, &adj);
+				for(int c = 0; c < 3; ++c) part[size_t(tid)][size_t(c)] += w[c] * adj.emis[c];
+			}
+		}
+	}
+	for(int c = 0; c < 3; ++c) {
+		double acc = 0.0;
+		for(auto& g : part) acc += g[size_t(c)];
+		gradOut[c] = acc;
 	}
 	return 1;
 }

@@ -127,6 +127,12 @@ void oracle_pt_destroy(void* pt);
  * Returns 0 on invalid arguments. */
 int oracle_albedo_gradient(void* pt, int32_t texIndex, uint32_t spp, const float* imageGrad, double* gradOut,
                            int32_t threads);
+/* dLoss/dL (3 doubles) for the emitted radiance L = radiance x scale of
+ * emissive material matIndex: the same replay of spp samples per pixel, each
+ * term that material emits (emitter hits and next-event samples) adding
+ * term / L. Russian roulette may be on. Returns 0 on invalid arguments. */
+int oracle_emission_gradient(void* pt, int32_t matIndex, uint32_t spp, const float* imageGrad, double* gradOut,
+                             int32_t threads);
 int oracle_pt_iterate(void* pt, int32_t numThreads);
 /* Cumulative target: 0 radiance (3 ch), 1 hit id (2 ch) */
 int oracle_pt_get_target(void* pt, int32_t target, float* out);

@@ -89,6 +89,8 @@ def lib():
         L.oracle_pt_destroy.argtypes = [C.c_void_p]
         L.oracle_albedo_gradient.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int32]
         L.oracle_albedo_gradient.restype = C.c_int
+        L.oracle_emission_gradient.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int32]
+        L.oracle_emission_gradient.restype = C.c_int
         L.oracle_pt_iterate.argtypes = [C.c_void_p, C.c_int32]
         L.oracle_pt_iterate_rows.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_uint32]
         L.oracle_pt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
@@ -307,6 +309,18 @@ class OraclePathTracer:
         out = np.zeros((tex.shape[0], tex.shape[1], 3), np.float64)
         if not lib().oracle_albedo_gradient(self.handle, texture_index, spp, _ptr(g), _ptr(out), threads):
             raise ValueError("oracle_albedo_gradient: invalid arguments (is Russian roulette off?)")
+        return out
+
+    def emission_gradient(self, material_index: int, spp: int, image_grad, threads: int = 0) -> np.ndarray:
+        """dLoss/dL (3,) in float64 for the emitted radiance L = radiance x scale of emissive material
+        `material_index` (index into the scene's material list), for imageGrad = dLoss/dImage (H, W, 3),
+        replaying spp samples per pixel from the seed (test reference of the GPU emission adjoint)."""
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        g = np.ascontiguousarray(image_grad, np.float32)
+        out = np.zeros(3, np.float64)
+        if not lib().oracle_emission_gradient(self.handle, material_index, spp, _ptr(g), _ptr(out), threads):
+            raise ValueError("oracle_emission_gradient: invalid arguments (not an emissive material?)")
         return out
 
     def stats(self):

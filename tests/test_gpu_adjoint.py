@@ -103,3 +103,94 @@ def test_gradient_requires_roulette_off(world):
     assert d.renderer_set_parameter_int("RR start depth", 0)
     with pytest.raises(bindings.MufflonError):
         d.albedo_gradient(d.textures[0], 1, np.zeros((W, W, 3), np.float32), (TEX, TEX))
+
+
+# ---------------------------------------------------------------- emission
+# The gradient with respect to the emitted radiance L (radiance x scale) of
+# the Cornell box's ceiling light. The scene has one area light, so its
+# selection probability does not depend on L and the image is linear in L,
+# with Russian roulette on or off: a central difference is exact for any
+# step up to the FP32 rounding of the rendered image.
+L0 = np.array([15.0, 12.0, 9.0], np.float32)
+
+
+@pytest.fixture(scope="module")
+def emitter_world():
+    spec = scenes.cornell_box(4, W, W)
+    li = [i for i, m in enumerate(spec.materials) if m.type == scenes.MAT_EMISSIVE][0]
+    d = bindings.DllInterface()
+    bindings.load_scene_spec(d, spec)
+    assert d.render_enable_renderer(0, 0)
+    yield d, spec, li
+    d.close()
+
+
+def _emission_renderer(d, li, rr_start):
+    from mufflon_b200.adjoint import EmissionRenderer
+    return EmissionRenderer(d, d.materials[li], spp=SPP, seed=2, max_path=DEPTH + 1, rr_start=rr_start)
+
+
+def _oracle_with_emission(oracle, spec, li, L, rr_start):
+    import dataclasses
+    mats = list(spec.materials)
+    mats[li] = scenes.MaterialSpec(scenes.MAT_EMISSIVE, radiance=tuple(float(x) for x in L), name="light")
+    spec = dataclasses.replace(spec, materials=mats)
+    return oracle.OraclePathTracer(oracle.OracleScene(spec), seed=2, max_path=DEPTH + 1, rr_start=rr_start)
+
+
+@pytest.mark.parametrize("rr_start", [0, DEPTH + 1], ids=["roulette", "no_roulette"])
+@pytest.mark.parametrize("megakernel", [0, 1], ids=["wavefront", "megakernel"])
+def test_emission_gradient_matches_fp64_oracle(emitter_world, oracle, megakernel, rr_start):
+    d, spec, li = emitter_world
+    assert d.renderer_set_parameter_int("Megakernel", megakernel)
+    e = _emission_renderer(d, li, rr_start)
+    img = e.render(L0)
+    pt = _oracle_with_emission(oracle, spec, li, L0, rr_start)
+    for _ in range(SPP):
+        pt.iterate()
+    ref_img = pt.target("Radiance")
+    assert np.sqrt(np.mean((img - ref_img) ** 2)) <= 1e-4 * np.sqrt(np.mean(ref_img ** 2))
+    dldi = 2.0 * (img - _target())
+    g = e.gradient(dldi)
+    ref = pt.emission_gradient(li, SPP, dldi)
+    assert np.all(np.abs(ref) > 0)
+    assert np.all(np.abs(g - ref) <= 1e-4 * np.abs(ref)), (g, ref)
+    assert d.renderer_set_parameter_int("Megakernel", 0)
+
+
+@pytest.mark.parametrize("h", [1e-3, 1.0])
+def test_emission_gradient_matches_central_differences(emitter_world, h):
+    d, spec, li = emitter_world
+    e = _emission_renderer(d, li, 0)
+    target = _target()
+    g = e.gradient(2.0 * (e.render(L0) - target))
+    loss = lambda L: float(np.sum((e.render(L).astype(np.float64) - target) ** 2))
+    for c in range(3):
+        lp, lm = L0.copy(), L0.copy()
+        lp[c] += h
+        lm[c] -= h
+        fd = (loss(lp) - loss(lm)) / (2 * h)
+        # h = 1e-3 changes the image by ~1e-4 of itself, so its FP32 rounding (~1e-7) bounds the
+        # quotient's accuracy near 1e-3; with h = 1 the quotient is exact to ~1e-6
+        tol = 2e-3 if h < 0.01 else 1e-4
+        assert abs(fd - g[c]) <= tol * abs(g[c]), (c, h, fd, g[c])
+
+
+def test_emission_torch_autograd(emitter_world):
+    import torch
+    from mufflon_b200.adjoint import render_emission
+    d, spec, li = emitter_world
+    e = _emission_renderer(d, li, 0)
+    target = torch.from_numpy(_target())
+    L = torch.tensor(L0, requires_grad=True)
+    loss = ((render_emission(L, e) - target) ** 2).sum()
+    loss.backward()
+    direct = e.gradient(2.0 * (e.render(L0) - target.numpy()))
+    assert np.allclose(L.grad.numpy(), direct, rtol=1e-5)
+    assert e.last_adjoint_ms > 0
+
+
+def test_emission_gradient_rejects_non_emitters(emitter_world):
+    d, spec, li = emitter_world
+    with pytest.raises(bindings.MufflonError, match="not emissive"):
+        d.emission_gradient(d.materials[0], 1, np.zeros((W, W, 3), np.float32))
