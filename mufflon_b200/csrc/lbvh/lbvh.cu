@@ -184,6 +184,13 @@ __global__ void k_karras(int n, const u64* __restrict__ keys, int32_t* parents, 
 // ---------------------------------------------------------------- merge
 // build_lbvh.cu:326-411: one thread per leaf climbs while it is the second
 // child to arrive at a node.
+// Arrival counter of the bottom-up passes: an acquire-release atomic add.
+MBD unsigned arrive(unsigned int* flag) {
+	unsigned prev;
+	asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(flag) : "memory");
+	return prev;
+}
+
 __global__ void k_bbox(int mode, LodBuildInput lod, SceneBuildInput scene, int used, int numInternal,
                        const int32_t* __restrict__ primIds, const int32_t* __restrict__ parents,
                        const int32_t* __restrict__ children, float4* nodeData, unsigned int* flags) {
@@ -211,10 +218,11 @@ __global__ void k_bbox(int mode, LodBuildInput lod, SceneBuildInput scene, int u
 	if(cur < 0) cur = ~cur;
 	const float nodeCost = mode == MODE_SCENE ? 1.0f : 2.0f;
 	for(int depth = 0; depth < MAX_DEPTH; ++depth) {
-		__threadfence();
-		const unsigned prev = atomicAdd(&flags[cur], 1u);
-		if(prev == 0) return; // first arrival: the sibling's thread continues
-		__threadfence();
+		// first arrival: the sibling's thread continues; acquire-release on the
+		// flag orders this thread's node writes before it and the sibling's
+		// reads after it (two full fences per level measured 20 % slower)
+		const unsigned prev = arrive(flags + cur);
+		if(prev == 0) return;
 		const int L = children[2 * cur], R = children[2 * cur + 1];
 		const float4 l0 = __ldcg(&nodeData[2 * L]), l1 = __ldcg(&nodeData[2 * L + 1]);
 		const float4 r0 = __ldcg(&nodeData[2 * R]), r1 = __ldcg(&nodeData[2 * R + 1]);
@@ -251,10 +259,8 @@ __global__ void k_refit_boxes(int used, int numInternal, const int32_t* __restri
 	int cur = parents[leaf];
 	if(cur < 0) cur = ~cur;
 	for(int depth = 0; depth < MAX_DEPTH; ++depth) {
-		__threadfence();
-		const unsigned prev = atomicAdd(&flags[cur], 1u);
+		const unsigned prev = arrive(flags + cur);
 		if(prev == 0) return;
-		__threadfence();
 		const int L = children[2 * cur], R = children[2 * cur + 1];
 		const float4 l0 = __ldcg(&nodeData[2 * L]), l1 = __ldcg(&nodeData[2 * L + 1]);
 		const float4 r0 = __ldcg(&nodeData[2 * R]), r1 = __ldcg(&nodeData[2 * R + 1]);

@@ -49,8 +49,14 @@ __global__ void __launch_bounds__(128) k_wide_level(WideBuildArgs A, const int2*
 	if(blockIdx.x == 0 && threadIdx.x == 0) *zeroCount = 0;
 	const uint32_t count = *inCount;
 	const int nI = A.numInternal;
-	for(uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < count; item += gridDim.x * blockDim.x) {
-		const int2 e = qin[item];
+	const uint32_t lane = threadIdx.x & 31u;
+	// Warp-uniform loop: the node, primitive and queue allocations of a warp's
+	// nodes are one atomic each per warp (per-node atomics on these three
+	// counters serialised in L2 at the wide levels).
+	for(uint32_t first0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; first0 < count; first0 += gridDim.x * blockDim.x) {
+		const uint32_t item = first0 + lane;
+		const bool valid = item < count;
+		const int2 e = valid ? qin[item] : make_int2(0, 0);
 		const int b = e.x;
 		const uint32_t w = uint32_t(e.y);
 		// 1. gather
@@ -89,8 +95,25 @@ __global__ void __launch_bounds__(128) k_wide_level(WideBuildArgs A, const int2*
 			inner[i] = cnt[i] > A.leafMax;
 			if(inner[i]) ++nInner; else nPrims += cnt[i];
 		}
-		const uint32_t childBase = nInner ? atomicAdd(A.counters + CNT_NODES, uint32_t(nInner)) : 0u;
-		const uint32_t primBase = nPrims ? atomicAdd(A.counters + CNT_PRIMS, uint32_t(nPrims)) : 0u;
+		if(!valid) { nInner = 0; nPrims = 0; }
+		uint32_t incN = uint32_t(nInner), incP = uint32_t(nPrims);
+		for(int off = 1; off < 32; off <<= 1) {
+			const uint32_t tn = __shfl_up_sync(0xffffffffu, incN, off), tp = __shfl_up_sync(0xffffffffu, incP, off);
+			if(lane >= uint32_t(off)) { incN += tn; incP += tp; }
+		}
+		const uint32_t totN = __shfl_sync(0xffffffffu, incN, 31), totP = __shfl_sync(0xffffffffu, incP, 31);
+		uint32_t bn = 0, bp = 0, bq = 0;
+		if(lane == 0) {
+			if(totN) { bn = atomicAdd(A.counters + CNT_NODES, totN); bq = atomicAdd(outCount, totN); }
+			if(totP) bp = atomicAdd(A.counters + CNT_PRIMS, totP);
+		}
+		bn = __shfl_sync(0xffffffffu, bn, 0);
+		bp = __shfl_sync(0xffffffffu, bp, 0);
+		bq = __shfl_sync(0xffffffffu, bq, 0);
+		if(!valid) continue;
+		const uint32_t childBase = bn + incN - uint32_t(nInner);
+		const uint32_t primBase = bp + incP - uint32_t(nPrims);
+		const uint32_t queueBase = bq + incN - uint32_t(nInner);
 		if(childBase + nInner > A.nodeCapacity || primBase + nPrims > uint32_t(A.n) || w >= A.nodeCapacity) {
 			atomicOr(A.counters + CNT_ERROR, 1u);
 			continue;
@@ -156,8 +179,8 @@ __global__ void __launch_bounds__(128) k_wide_level(WideBuildArgs A, const int2*
 			}
 			if(inner[i]) {
 				imask |= 1u << s;
+				const uint32_t q = queueBase + uint32_t(innerRank);
 				const uint32_t idx = childBase + uint32_t(innerRank++);
-				const uint32_t q = atomicAdd(outCount, 1u);
 				if(q < A.nodeCapacity) qout[q] = make_int2(ch[i], int(idx));
 				else bad = true;
 			} else {
