@@ -69,7 +69,7 @@ const ParamDesc LT_PARAMS[] = {
 const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT },
                                   { "Traversal step limit", PARAM_INT } };
 // Render targets of the path tracer (pt_params.hpp:16-26). The CUDA path
-// implements Radiance and Hit ID; the others are recognised names.
+// implements all eight (the six auxiliary ones: aux_targets.cuh).
 const char* TARGETS[] = { "Radiance", "Position", "Depth", "Normal", "UV", "Albedo", "Lightness", "Hit ID" };
 // Render targets of the light tracer (lt_params.hpp:14-17) and of the
 // bidirectional path tracer (bpt_params.hpp:14-17, its first two), all implemented.
@@ -161,6 +161,40 @@ void ensure_variance_buffers(MufflonInstance& I) {
 	need(r.hitIdVar, r.varHitId, 2);
 	need(r.lightnessVar, r.varLightness, 1);
 	need(r.densityMean, r.varDensity, 1);
+}
+
+// The path tracer's auxiliary-target buffers (cumulative, variance and, for
+// the wavefront schedule, the per-path iteration state) of the enabled
+// targets; "Lightness" uses the light tracer's buffers. Cleared at every reset.
+constexpr int AUX_CH[5] = { 3, 1, 3, 2, 3 };
+bool aux_wanted(const RendererState& r) {
+	bool any = r.targetLightness;
+	for(int a = 0; a < 5; ++a) any = any || r.auxTarget[a];
+	return any;
+}
+void ensure_aux_buffers(MufflonInstance& I) {
+	RendererState& r = I.renderer;
+	const size_t n = size_t(r.width) * r.height;
+	for(int a = 0; a < 5; ++a) {
+		if(r.auxTarget[a] && !r.auxCum[a]) {
+			CHECK_CUDA(cudaMalloc(&r.auxCum[a], n * AUX_CH[a] * sizeof(float)));
+			CHECK_CUDA(cudaMemsetAsync(r.auxCum[a], 0, n * AUX_CH[a] * sizeof(float), I.stream));
+		}
+		if(r.auxTarget[a] && r.auxVarOn[a] && !r.auxVarBuf[a]) {
+			CHECK_CUDA(cudaMalloc(&r.auxVarBuf[a], n * AUX_CH[a] * sizeof(float)));
+			CHECK_CUDA(cudaMemsetAsync(r.auxVarBuf[a], 0, n * AUX_CH[a] * sizeof(float), I.stream));
+		}
+	}
+	if(r.targetLightness && !r.lightness) {
+		CHECK_CUDA(cudaMalloc(&r.lightness, n * sizeof(float)));
+		CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, n * sizeof(float), I.stream));
+	}
+	if(aux_wanted(r) && r.auxMemPixels != n) {
+		cudaFree(r.auxMem);
+		r.auxMem = nullptr; r.auxMemPixels = 0;
+		CHECK_CUDA(cudaMalloc(&r.auxMem, n * (sizeof(float2) + AUX_CHANNELS * sizeof(float))));
+		r.auxMemPixels = n;
+	}
 }
 
 // Wavefront state for the current resolution and NEE count (one slab).
@@ -321,6 +355,9 @@ void RendererState::release() {
 	bptScratch = nullptr; bptScratchBytes = 0;
 	cudaFree(radianceVar); cudaFree(hitIdVar); cudaFree(lightnessVar); cudaFree(densityMean);
 	radianceVar = nullptr; hitIdVar = nullptr; lightnessVar = nullptr; densityMean = nullptr;
+	for(int a = 0; a < 5; ++a) { cudaFree(auxCum[a]); cudaFree(auxVarBuf[a]); auxCum[a] = nullptr; auxVarBuf[a] = nullptr; }
+	cudaFree(auxMem);
+	auxMem = nullptr; auxMemPixels = 0;
 	if(screen) cudaFreeHost(screen);
 	screen = nullptr; screenCap = 0;
 	if(evStart) cudaEventDestroy(evStart);
@@ -441,6 +478,14 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 		read("Border", r.targetBorder, r.varBorder, r.radiance, r.radianceVar, 3);
 	} else if(r.kind == 0 && !std::strcmp(name, "Hit ID")) {
 		read("Hit ID", r.targetHitId, r.varHitId, r.hitId, r.hitIdVar, 2);
+	} else if(r.kind == 0 && !std::strcmp(name, "Lightness")) {
+		read("Lightness", r.targetLightness, r.varLightness, r.lightness, r.lightnessVar, 1);
+	} else if(r.kind == 0 && (!std::strcmp(name, "Position") || !std::strcmp(name, "Depth") || !std::strcmp(name, "Normal") ||
+	                          !std::strcmp(name, "UV") || !std::strcmp(name, "Albedo"))) {
+		static const char* AUX_NAMES[5] = { "Position", "Depth", "Normal", "UV", "Albedo" };
+		int a = 0;
+		while(std::strcmp(name, AUX_NAMES[a])) ++a;
+		read(AUX_NAMES[a], r.auxTarget[a], r.auxVarOn[a], r.auxCum[a], r.auxVarBuf[a], AUX_CH[a]);
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
 		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "wireframe renderer" : r.kind == 3 ? "bidirectional path tracer" : "path tracer"));
@@ -1131,6 +1176,7 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	I.scene.desc.maxSteps = step_limit(r);
 	const uint32_t n = r.width * r.height;
 	if(r.kind != 0) ensure_lt_buffers(I);
+	else ensure_aux_buffers(I);
 	ensure_variance_buffers(I);
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
@@ -1145,6 +1191,10 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 		if(r.hitIdVar) CHECK_CUDA(cudaMemsetAsync(r.hitIdVar, 0, size_t(n) * 2 * sizeof(float), I.stream));
 		if(r.lightnessVar) CHECK_CUDA(cudaMemsetAsync(r.lightnessVar, 0, size_t(n) * sizeof(float), I.stream));
 		if(r.densityMean) CHECK_CUDA(cudaMemsetAsync(r.densityMean, 0, size_t(n) * sizeof(float), I.stream));
+		for(int a = 0; a < 5; ++a) {
+			if(r.auxCum[a]) CHECK_CUDA(cudaMemsetAsync(r.auxCum[a], 0, size_t(n) * AUX_CH[a] * sizeof(float), I.stream));
+			if(r.auxVarBuf[a]) CHECK_CUDA(cudaMemsetAsync(r.auxVarBuf[a], 0, size_t(n) * AUX_CH[a] * sizeof(float), I.stream));
+		}
 		r.iteration = 0;
 		r.needsReset = false;
 	} else {
@@ -1166,12 +1216,26 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	rs.hitId = r.targetHitId ? r.hitId : nullptr;
 	rs.radianceVar = r.targetRadiance && r.varRadiance ? r.radianceVar : nullptr;
 	rs.hitIdVar = r.targetHitId && r.varHitId ? r.hitIdVar : nullptr;
+	for(int a = 0; a < 5; ++a) {
+		rs.aux[a] = r.auxTarget[a] ? r.auxCum[a] : nullptr;
+		rs.auxVar[a] = r.auxTarget[a] && r.auxVarOn[a] ? r.auxVarBuf[a] : nullptr;
+	}
+	rs.aux[5] = r.targetLightness ? r.lightness : nullptr;
+	rs.auxVar[5] = r.targetLightness && r.varLightness ? r.lightnessVar : nullptr;
+	rs.auxOn = aux_wanted(r) ? 1 : 0;
+	// the wavefront's per-path auxiliary state (in the graph key through r.wf)
+	r.wf.guide = nullptr; r.wf.auxIter = nullptr; r.wf.auxStride = 0;
 	rs.width = r.width; rs.height = r.height;
 	rs.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 	WfLaunchInfo info;
 	if(!r.megakernel) {
 		ensure_wavefront_buffers(I);
+		if(rs.auxOn) {
+			r.wf.guide = static_cast<float2*>(r.auxMem);
+			r.wf.auxIter = reinterpret_cast<float*>(static_cast<char*>(r.auxMem) + size_t(n) * sizeof(float2));
+			r.wf.auxStride = n;
+		}
 		if(r.stageTiming) {
 			const int pairs = 3 * std::max(1, r.params.maxPathLength) + 2;
 			while(int(r.stageEvents.size()) < 2 * pairs) {
@@ -1331,6 +1395,9 @@ const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) 
 // The record / record-variance flags of a target implemented by the CUDA
 // renderers (null for other names).
 static std::pair<bool*, bool*> target_flags(RendererState& r, const char* name) {
+	static const char* AUX_NAMES[5] = { "Position", "Depth", "Normal", "UV", "Albedo" };
+	for(int a = 0; a < 5; ++a)
+		if(!std::strcmp(name, AUX_NAMES[a])) return { &r.auxTarget[a], &r.auxVarOn[a] };
 	if(!std::strcmp(name, "Radiance")) return { &r.targetRadiance, &r.varRadiance };
 	if(!std::strcmp(name, "Hit ID")) return { &r.targetHitId, &r.varHitId };
 	if(!std::strcmp(name, "Lightness")) return { &r.targetLightness, &r.varLightness };

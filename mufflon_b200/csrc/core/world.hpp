@@ -245,6 +245,15 @@ struct RendererState {
 	float* hitIdVar = nullptr;     // 2 per pixel
 	float* lightnessVar = nullptr; // 1 per pixel
 	float* densityMean = nullptr;  // 1 per pixel
+	// The path tracer's auxiliary targets Position, Depth, Normal, UV, Albedo
+	// (3, 1, 3, 2, 3 channels; "Lightness" uses the light tracer's flags and
+	// buffers above): record / record-variance flags, cumulative and variance
+	// buffers, and the per-path iteration state of the wavefront schedule.
+	bool auxTarget[5] = {}, auxVarOn[5] = {};
+	float* auxCum[5] = {};
+	float* auxVarBuf[5] = {};
+	void* auxMem = nullptr;
+	size_t auxMemPixels = 0;
 	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
 	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
 	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters

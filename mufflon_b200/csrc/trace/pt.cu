@@ -10,6 +10,7 @@
 // mean of output_handler_variance.hpp:7-31 is updated in place, without
 // atomics and without a separate accumulation kernel.
 #include "accumulate.cuh"
+#include "aux_targets.cuh"
 #include "shading.cuh"
 #include "pt_api.hpp"
 
@@ -44,7 +45,7 @@ MBD f3 contribute(f3 acc, f3 c) {
 
 // pt_common.hpp:75-156
 MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng, f3& radianceOut, f2& hitOut,
-                   LocalCounters& cnt, int2* bstack, int2* tstack) {
+                   LocalCounters& cnt, int2* bstack, int2* tstack, float* aux) {
 	f3 throughput = make3(1.0f, 1.0f, 1.0f);
 	f3 radiance = make3(0.0f, 0.0f, 0.0f);
 	f2 hitAcc = make2(0.0f, 0.0f);
@@ -56,6 +57,8 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 	v.inst = v.prim = -1;
 	(void)pcg_next(rng); // create_camera consumes one number
 	int pathLen = 0;
+	float guideA = 0.0f, guideWeight = 1.0f;
+	auto aux_add = [&](int c, float x) { aux[c] += nan_to_zero(x); };
 	do {
 		if(pathLen > 0 && pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
 			const u64 neeSeed = pcg_next(rng);
@@ -73,6 +76,7 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 						const float hitPdf = __fdiv_rn(val.pdfF * fabsf(nee.cosOut), nee.distSq);
 						const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
 						radiance = contribute(radiance, ((throughput * val.cosOut) * rad) * mis);
+						if(aux) aux_add(AUX_LIGHT, __fmul_rn(guideWeight, val.cosOut));
 					}
 				}
 			}
@@ -122,6 +126,7 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 		}
 		if(pathLen == 0)
 			hitAcc = make2(float(v.type == V_SURFACE ? v.inst : -1), float(v.type == V_SURFACE ? v.prim : -1));
+		if(aux) guideWeight = guide_after_segment(guideA, pdfF);
 		++pathLen;
 		if(pathLen >= P.minPathLength) {
 			f3 emission = make3(0.0f, 0.0f, 0.0f);
@@ -148,6 +153,13 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 				emission = emission * misWeight;
 			}
 			radiance = contribute(radiance, throughput * emission);
+			if(aux) {
+				const bool surf = v.type == V_SURFACE;
+				const f3 zero = make3(0.0f, 0.0f, 0.0f);
+				aux_vertex(aux_add, guideWeight, surf ? v.position : zero, surf ? fabsf(v.incidentEncoded.z) : 0.0f,
+				           surf ? v.ts.shadingN : zero, surf ? hit.uv : make2(0.0f, 0.0f),
+				           surf && v.mat.type != MAT_EMISSIVE ? v.mat.albedo : zero, emission);
+			}
 		}
 		if(v.type != V_SURFACE) break;
 	} while(pathLen < P.maxPathLength);
@@ -180,8 +192,18 @@ __global__ void pt_megakernel(const DScene S, const PtParams P, RenderState R, u
 			const int px = int(pixel % R.width), py = int(pixel / R.width);
 			u64 rng = R.rngState[pixel];
 			f3 rad; f2 hid;
-			pt_sample(S, P, px, py, rng, rad, hid, cnt, bstack, tstack);
+			float aux[AUX_CHANNELS];
+			for(int c = 0; c < AUX_CHANNELS; ++c) aux[c] = 0.0f;
+			pt_sample(S, P, px, py, rng, rad, hid, cnt, bstack, tstack, R.auxOn ? aux : nullptr);
 			R.rngState[pixel] = rng;
+			if(R.auxOn)
+				for(int a = 0; a < AUX_TARGETS; ++a) {
+					if(!R.aux[a]) continue;
+					float* cum = R.aux[a] + size_t(aux_count(a)) * pixel;
+					float* var = R.auxVar[a] ? R.auxVar[a] + size_t(aux_count(a)) * pixel : nullptr;
+					for(int c = 0; c < aux_count(a); ++c)
+						update_moments(aux[aux_first(a) + c], cum + c, var ? var + c : nullptr, R.iteration);
+				}
 			if(R.radiance) {
 				float* cr = R.radiance + 3 * size_t(pixel);
 				float* vr = R.radianceVar ? R.radianceVar + 3 * size_t(pixel) : nullptr;

@@ -88,6 +88,10 @@ struct DCamera {
 	uint16_t resX, resY;
 };
 
+// Per-pixel iteration channels of the path tracer's auxiliary targets
+// (Position 3, Depth 1, Normal 3, UV 2, Albedo 3, Lightness 1).
+constexpr int AUX_CHANNELS = 13;
+
 // Default traversal step limit of a ray (DScene::maxSteps).
 constexpr int32_t MAX_TRAVERSAL_STEPS = 1 << 22;
 
@@ -145,6 +149,12 @@ struct RenderState {
 	float* iterRadiance;    // optional per-iteration radiance (may be null)
 	float* radianceVar;     // running variances of the two targets (null: not recorded)
 	float* hitIdVar;
+	// the auxiliary targets Position, Depth, Normal, UV, Albedo, Lightness
+	// (3, 1, 3, 2, 3, 1 channels per pixel): cumulative means and variances,
+	// null where not recorded; auxOn: any of them is recorded
+	float* aux[6];
+	float* auxVar[6];
+	int32_t auxOn;
 	uint32_t width, height;
 	int32_t iteration;      // 0 for the first iteration after a reset
 	const int32_t* dIteration; // if set: the iteration number is read here (a replayed CUDA graph)

@@ -20,6 +20,7 @@
 // shade k+1, so a next-event contribution is added between the emission terms
 // that surround it, exactly as the sequential loop adds them.
 #include "accumulate.cuh"
+#include "aux_targets.cuh"
 #include "shading.cuh"
 #include "wide_traverse.cuh"
 #include "wavefront.hpp"
@@ -269,6 +270,10 @@ MBD void camera_path(const DScene& S, const PtParams& P, WfState& W, uint32_t p,
 	W.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 	W.hit0[p] = make_float2(-1.0f, -1.0f);
 	W.thrPdf[p] = pack(thr, pdfF);
+	if(W.auxIter) {
+		W.guide[p] = make_float2(0.0f, 1.0f); // the camera vertex's footprint (pChoice 1)
+		for(int c = 0; c < AUX_CHANNELS; ++c) W.auxIter[size_t(c) * W.auxStride + p] = 0.0f;
+	}
 	if(!alive) return;
 	f3 o = lv(S.camera.position);
 	add_epsilon(o, dir, make3(0.0f, 0.0f, 0.0f));
@@ -393,6 +398,10 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 					const float4 c4 = __ldcs(W.sContrib + slot);
 					const f3 c = f4to3(c4);
 					radiance = contribute(radiance, c);
+					if(W.auxIter) {
+						float* a = W.auxIter + size_t(AUX_LIGHT) * W.auxStride + size_t(path);
+						*a = *a + nan_to_zero(__ldcs(W.sDir + slot).w);
+					}
 					if constexpr(SP::adjoint) {
 						const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
 						adjoint_add(sp.A, path, cc);
@@ -448,7 +457,24 @@ struct VertexInfo {
 	int materialType;
 	f2 uv;
 	f3 albedo;
+	// for the auxiliary targets: whether the vertex contributes (path length
+	// >= the minimum), its position, incident distance and shading normal (0
+	// for a miss), and its emission after the MIS weight, before the throughput
+	bool counts;
+	f3 position;
+	float depth;
+	f3 normal;
+	f3 emission;
 };
+
+// A vertex's auxiliary-target contributions, added to path p's iteration
+// values (channel-major, W.auxStride paths per channel).
+MBD void aux_vertex_path(const WfState& W, int p, float gw, const VertexInfo& v) {
+	const f3 zero = make3(0.0f, 0.0f, 0.0f);
+	aux_vertex([&](int c, float x) { float* a = W.auxIter + size_t(c) * W.auxStride + size_t(p); *a = *a + nan_to_zero(x); },
+	           gw, v.position, v.depth, v.normal, v.surface ? v.uv : make2(0.0f, 0.0f),
+	           v.surface && v.materialType != MAT_EMISSIVE ? v.albedo : zero, v.emission);
+}
 
 // The state of a shaded path vertex between the parts of shade_vertex.
 struct ShadeState {
@@ -514,10 +540,13 @@ MBD bool shade_begin(const DScene& S, const PtParams& P, int bounce, f3 origin, 
 		const f3 eterm = throughput * emission;
 		radiance = contribute(radiance, eterm);
 		onVertex(contribute(make3(0.0f, 0.0f, 0.0f), eterm), VertexInfo{ surface, matIndex, surface ? mat.type : -1, hit.uv,
-		                                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f) });
+		                                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f),
+		                                                            true, position, surface ? hit.distance : 0.0f,
+		                                                            surface ? ts.shadingN : make3(0.0f, 0.0f, 0.0f), emission });
 	} else {
 		onVertex(make3(0.0f, 0.0f, 0.0f), VertexInfo{ surface, matIndex, surface ? mat.type : -1, hit.uv,
-		                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f) });
+		                                            surface ? mat.albedo : make3(0.0f, 0.0f, 0.0f),
+		                                            false, position, 0.0f, make3(0.0f, 0.0f, 0.0f), make3(0.0f, 0.0f, 0.0f) });
 	}
 	if(!surface || !(pathLen < P.maxPathLength)) return false;
 	v.position = position;
@@ -536,7 +565,7 @@ MBD bool shade_has_nee(const PtParams& P, const ShadeState& v) {
 // Next-event sample i at v (pt_common.hpp:105-124): draws its number; true
 // with the shadow ray and the term it adds when it can contribute.
 MBD bool shade_nee(const DScene& S, const PtParams& P, const ShadeState& v, const f3& throughput, u64& rng, u64 neeSeed,
-                   int i, f3& so, f3& sd, float& stmax, f3& c, int& emitMat) {
+                   int i, f3& so, f3& sd, float& stmax, f3& c, int& emitMat, float& cosOut) {
 	const u64 r = pcg_next(rng);
 	const float nu0 = sample_uniform(uint32_t(r)), nu1 = sample_uniform(uint32_t(r >> 32));
 	const Nee nee = lights_connect(S, u64(i), u64(P.neeCount), neeSeed, v.position, nu0, nu1);
@@ -549,6 +578,7 @@ MBD bool shade_nee(const DScene& S, const PtParams& P, const ShadeState& v, cons
 	const float mis = __fdiv_rn(1.0f, float(P.neeCount) + __fdiv_rn(hitPdf, nee.creationPdf));
 	c = ((throughput * val.cosOut) * rad) * mis;
 	emitMat = nee.emitMat;
+	cosOut = val.cosOut;
 	shadow_ray(v.position, nee.position, v.ts.geoN, nee.geoNormal, nee.dir, so, sd, stmax);
 	return true;
 }
@@ -588,7 +618,9 @@ MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin,
 			f3 so, sd, c;
 			float stmax;
 			int emitMat = -1;
-			if(shade_nee(S, P, v, throughput, rng, neeSeed, i, so, sd, stmax, c, emitMat)) shadow(i, so, sd, stmax, c, emitMat);
+			float cosOut = 0.0f;
+			if(shade_nee(S, P, v, throughput, rng, neeSeed, i, so, sd, stmax, c, emitMat, cosOut))
+				shadow(i, so, sd, stmax, c, emitMat, cosOut);
 		}
 	}
 	return shade_walk(P, v, throughput, pdfF, rng, nextO, nextD);
@@ -617,9 +649,10 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	u64 rng = W.rng[p];
 	const u64 rng0 = rng;
 	unsigned base = 0xFFFFFFFFu;
+	float gw = 0.0f; // the vertex's guide weight (auxiliary targets)
 	f3 nextO, nextD;
 	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
-		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c, int emitMat) {
+		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c, int emitMat, float cosOut) {
 			if(base == 0xFFFFFFFFu) {
 				base = atomicAdd(W.counters + C_SHADOW0 + q, unsigned(P.neeCount));
 				for(int k = 0; k < P.neeCount; ++k) { W.sPath[base + k] = p; W.sOrg[base + k] = make_float4(0, 0, 0, -1.0f); }
@@ -627,10 +660,16 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 					bin_append(W.shKey, W.binHist + (1u << W.sortBits), base / unsigned(P.neeCount), ray_key(W, S, sp.group(p), so, sd));
 			}
 			W.sOrg[base + i] = pack(so, stmax);
-			W.sDir[base + i] = pack(sd, 0.0f);
+			W.sDir[base + i] = pack(sd, W.auxIter ? __fmul_rn(gw, cosOut) : 0.0f); // w: its Lightness term
 			W.sContrib[base + i] = pack(c, __int_as_float(emitMat)); // w: the emitter's material (adjoint)
 		}, [&](f3 e, const VertexInfo& v) {
 			if constexpr(SP::adjoint) adjoint_vertex(sp.A, S, p, e, v.surface, v.materialType, v.materialIndex, v.uv, v.albedo);
+			if(W.auxIter) {
+				float ma = W.guide[p].x;
+				gw = guide_after_segment(ma, pdfF); // pdfF: the pdf of the segment that reached this vertex
+				W.guide[p] = make_float2(ma, gw);
+				if(v.counts) aux_vertex_path(W, p, gw, v);
+			}
 		});
 	W.rad[p] = pack(radiance, ra.w);
 	if(rng != rng0) W.rng[p] = rng;
@@ -690,12 +729,17 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 	int phase = T_IDLE;
 	int p = 0, b = 0, i = 0;
 	int emitMat = -1; // emitter material of the current shadow ray (adjoint)
+	float guideA = 0.0f, gw = 0.0f, lightTerm = 0.0f; // auxiliary targets: footprint, guide weight, shadow ray's term
 	f3 throughput = make3(0.0f, 0.0f, 0.0f), radiance = make3(0.0f, 0.0f, 0.0f), c = make3(0.0f, 0.0f, 0.0f);
 	float pdfF = 0.0f, radW = 0.0f;
 	u64 rng = 0, neeSeed = 0;
 	ShadeState v;
 	auto on_vertex = [&](f3 e, const VertexInfo& vi) {
 		if constexpr(SP::adjoint) adjoint_vertex(sp.A, sp.scene(p), p, e, vi.surface, vi.materialType, vi.materialIndex, vi.uv, vi.albedo);
+		if(W.auxIter) {
+			gw = guide_after_segment(guideA, pdfF); // pdfF: the pdf of the segment that reached this vertex
+			if(vi.counts) aux_vertex_path(W, p, gw, vi);
+		}
 	};
 	// shades the vertex a traced extension ray reached; sets the next phase
 	auto begin_vertex = [&](f3 origin, f3 dir, const HitRec& hr) {
@@ -735,6 +779,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 					radiance = f4to3(ra);
 					radW = ra.w;
 					rng = W.rng[p];
+					if(W.auxIter) guideA = W.guide[p].x;
 					b = bounce;
 					begin_vertex(f4to3(W.qOrg[q][item]), f4to3(W.qDir[q][item]), hr);
 				}
@@ -748,7 +793,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 			const DScene& S = sp.scene(p);
 			const PtParams& P = sp.params(p);
 			while(i < P.neeCount) {
-				if(shade_nee(S, P, v, throughput, rng, neeSeed, i, ro, rd, tmax, c, emitMat)) { trace = shadow = true; break; }
+				if(shade_nee(S, P, v, throughput, rng, neeSeed, i, ro, rd, tmax, c, emitMat, lightTerm)) { trace = shadow = true; break; }
 				++i;
 			}
 			if(!trace) phase = T_WALK;
@@ -775,6 +820,10 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 					const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
 					adjoint_add(sp.A, p, cc);
 					adjoint_emitted(sp.A, S, p, cc, emitMat);
+				}
+				if(W.auxIter) {
+					float* a = W.auxIter + size_t(AUX_LIGHT) * W.auxStride + size_t(p);
+					*a = *a + nan_to_zero(__fmul_rn(gw, lightTerm));
 				}
 			}
 			++i;
@@ -820,6 +869,14 @@ __global__ void k_finalize(WfState W, RenderState R, uint32_t numPixels) {
 		float* o = R.iterRadiance + 3 * size_t(p);
 		o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
 	}
+	if(R.auxOn && W.auxIter)
+		for(int a = 0; a < AUX_TARGETS; ++a) {
+			if(!R.aux[a]) continue;
+			float* cum = R.aux[a] + size_t(aux_count(a)) * p;
+			float* var = R.auxVar[a] ? R.auxVar[a] + size_t(aux_count(a)) * p : nullptr;
+			for(int c = 0; c < aux_count(a); ++c)
+				update_moments(W.auxIter[size_t(aux_first(a) + c) * W.auxStride + p], cum + c, var ? var + c : nullptr, iteration);
+		}
 }
 
 MBD void adjoint_vertex(const AdjointState& A, const DScene& S, int p, f3 e, bool surface, int type, int mat, f2 uv,
@@ -935,7 +992,7 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
 			const HitRec hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
 			f3 nextO, nextD;
 			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, r, nullptr, nextO, nextD,
-				[&](int, f3 so, f3 sd, float stmax, f3 c, int emitMat) {
+				[&](int, f3 so, f3 sd, float stmax, f3 c, int emitMat, float) {
 					LocalCounters sc;
 					if(occluded_wide(S, so, sd, stmax, sc, stack)) return;
 					const f3 cc = contribute(make3(0.0f, 0.0f, 0.0f), c);
@@ -1224,6 +1281,9 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
 	W.sortDirBits = 0;
 	W.sortGroupBits = 0;
 	W.ordered = 0;
+	W.guide = nullptr;
+	W.auxIter = nullptr;
+	W.auxStride = 0;
 }
 
 cudaError_t launch_adjoint_albedo(const DScene& S, const PtParams& P, uint64_t* rng, uint32_t width, uint32_t height,
@@ -1265,6 +1325,8 @@ cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_
 	A.emitTarget = T.emitTarget;
 	A.emisGrad = T.emisGrad;
 	A.tex = DTexture{ 0, 0, nullptr };
+	W.auxIter = nullptr; // no auxiliary targets in a replay
+	W.guide = nullptr;
 	cudaError_t e = cudaSuccess;
 	if(T.texIndex >= 0) {
 		e = cudaMemcpyAsync(&A.tex, S.textures + T.texIndex, sizeof(DTexture), cudaMemcpyDeviceToHost, stream);
@@ -1360,6 +1422,8 @@ cudaError_t launch_pt_batch(const DJob* jobs, const uint16_t* pathJob, uint32_t 
 	if(numPixels == 0) return cudaSuccess;
 	if(neeCount < 1) neeCount = 1;
 	if(maxBounces < 1) maxBounces = 1;
+	W.auxIter = nullptr; // batches render Radiance and Hit ID only
+	W.guide = nullptr;
 	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
 	const unsigned firstClear = unsigned(2 * maxBounces) < workSlots ? unsigned(2 * maxBounces) : workSlots;
 	cudaError_t e = cudaMemsetAsync(W.counters, 0, sizeof(unsigned) * (C_WORK + firstClear), stream);

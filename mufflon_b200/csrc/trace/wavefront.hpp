@@ -36,6 +36,12 @@ struct WfState {
 	int sortDirBits;      // of those, direction bits: 0, 3 (octant) or 6 (octahedral 8 x 8)
 	int sortGroupBits;    // of those, the top bits: the path's group (the scene of a batch job)
 	int ordered;          // set for a trace launch whose queues were binned
+	// The auxiliary targets of the path tracer (null: none recorded): per path
+	// the footprint's m_a and the last vertex's guide weight, and the
+	// iteration's AUX_CHANNELS values, channel-major with auxStride paths per channel.
+	float2* guide;
+	float* auxIter;
+	uint32_t auxStride;
 };
 constexpr int WF_SORT_MAX_BITS = 16;
 

@@ -1766,12 +1766,18 @@ inline V3 incident_direction(const Vertex& v) {
 	return { e.x, e.y, sgn(e.z) * mbmath::sqrt(t) };
 }
 
+// The path tracer's auxiliary targets (pt_params.hpp:16-26, pt_common.hpp:
+// 146-152): per pixel and iteration 13 channels, position 3, depth 1, normal 3,
+// uv 2, albedo 3, lightness 1.
+enum { AUX_POS = 0, AUX_DEPTH = 3, AUX_NORMAL = 4, AUX_UV = 7, AUX_ALBEDO = 9, AUX_LIGHT = 12, AUX_CHANNELS = 13 };
+
 struct PtState {
 	const Scene* scene;
 	OrPtParams params;
 	std::vector<Pcg64> rngs;
 	std::vector<float> radiance, hitId;       // cumulative
 	std::vector<float> radianceVar, hitIdVar; // their variances
+	std::vector<float> aux, auxVar;           // AUX_CHANNELS per pixel: cumulative means, variances
 	i32 iteration = -1;
 	Counters stats;
 };
@@ -1842,9 +1848,21 @@ struct AlbedoAdjoint {
 	void vertex(const Scene& S, const V3& e, bool surface, i32 type, i32 mat, V2 uv, V3 albedo);
 };
 
+// FootprintV0::add_segment (footprint.hpp:137-165) of a camera path: the
+// camera vertex starts with m_a = 0 and pChoice 1 (path_util.hpp:553), every
+// sampled direction adds 1 / sqrt(its pdf), roulette passes 1; the guide
+// weight of the vertex reached is 1 / (1 + solid angle), solid angle = m_a^2
+// (pt_common.hpp:49-61).
+inline float guide_after_segment(float& ma, float pdf) {
+	ma = ma + 1.0f / mbmath::sqrt(pdf);
+	return 1.0f / (1.0f + ma * ma);
+}
+// ei::avg of the emission (the mean of the three channels)
+inline float avg3(V3 v) { return ((v.x + v.y) + v.z) / 3.0f; }
+
 // pt_common.hpp:75-156
 void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hitOut, Counters& cnt,
-               AlbedoAdjoint* adj = nullptr) {
+               AlbedoAdjoint* adj = nullptr, float* aux = nullptr) {
 	const Scene& S = *st.scene;
 	const OrPtParams& P = st.params;
 	V3 throughput = { 1, 1, 1 };
@@ -1859,6 +1877,8 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 	v.inst = v.prim = -1;
 	(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
 	int pathLen = 0;
+	float guideA = 0.0f, guideWeight = 1.0f;
+	auto aux_add = [&](int c, float x) { if(aux) aux[c] += nan_to_zero(x); };
 	do {
 		if(pathLen > 0 && pathLen + 1 >= P.minPathLength && pathLen + 1 <= P.maxPathLength) {
 			const u64 neeSeed = rng.next();
@@ -1881,6 +1901,7 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 							adj->add_all(term);
 							adj->emitted(term, nee.emitMat);
 						}
+						aux_add(AUX_LIGHT, guideWeight * val.cosOut);
 					}
 				}
 			}
@@ -1935,6 +1956,7 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 			v.incidentPdf = pdfF * std::fabs(inCosAbs) / (hit.distance * hit.distance);
 		}
 		if(pathLen == 0) hitAcc = { float(v.type == V_SURFACE ? v.inst : -1), float(v.type == V_SURFACE ? v.prim : -1) };
+		guideWeight = guide_after_segment(guideA, pdfF);
 		++pathLen;
 		if(pathLen >= P.minPathLength) {
 			V3 emission = { 0, 0, 0 };
@@ -1963,6 +1985,22 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 			}
 			radiance = contribute(radiance, throughput * emission);
 			if(adj) adj->vertex(S, contribute(V3{ 0, 0, 0 }, throughput * emission), v.type == V_SURFACE, v.mat.type, vMat, vUv, v.mat.albedo);
+			if(aux) {
+				// pt_common.hpp:146-152: position, incident distance, shading normal, uv, albedo
+				// (Lambert and Torrance; 0 for emitters) and lightness, each times the guide weight
+				const bool surf = v.type == V_SURFACE;
+				const V3 pos = surf ? v.position : V3{ 0, 0, 0 };
+				const V3 nrm = surf ? v.ts.shadingN : V3{ 0, 0, 0 };
+				const V3 alb = surf && v.mat.type != OR_MAT_EMISSIVE ? v.mat.albedo : V3{ 0, 0, 0 };
+				const float depth = surf ? std::fabs(v.incidentEncoded.z) : 0.0f;
+				const V2 uv = surf ? vUv : V2{ 0, 0 };
+				aux_add(AUX_POS, guideWeight * pos.x); aux_add(AUX_POS + 1, guideWeight * pos.y); aux_add(AUX_POS + 2, guideWeight * pos.z);
+				aux_add(AUX_DEPTH, guideWeight * depth);
+				aux_add(AUX_NORMAL, guideWeight * nrm.x); aux_add(AUX_NORMAL + 1, guideWeight * nrm.y); aux_add(AUX_NORMAL + 2, guideWeight * nrm.z);
+				aux_add(AUX_UV, guideWeight * uv.x); aux_add(AUX_UV + 1, guideWeight * uv.y);
+				aux_add(AUX_ALBEDO, guideWeight * alb.x); aux_add(AUX_ALBEDO + 1, guideWeight * alb.y); aux_add(AUX_ALBEDO + 2, guideWeight * alb.z);
+				aux_add(AUX_LIGHT, guideWeight * avg3(emission));
+			}
 		} else if(adj) {
 			adj->vertex(S, V3{ 0, 0, 0 }, v.type == V_SURFACE, v.mat.type, vMat, vUv, v.mat.albedo);
 		}
@@ -2001,13 +2039,17 @@ void pt_iterate(PtState& st, int numThreads, u32 y0, u32 y1, bool accumulate) {
 #pragma omp for schedule(static, 1000)
 		for(i32 pixel = p0; pixel < p1; ++pixel) {
 			V3 rad; V2 hid;
-			pt_sample(st, pixel % W, pixel / W, st.rngs[pixel], rad, hid, local);
+			float aux[AUX_CHANNELS] = {};
+			pt_sample(st, pixel % W, pixel / W, st.rngs[pixel], rad, hid, local, nullptr, aux);
 			if(accumulate) {
 				const float iter[5] = { rad.x, rad.y, rad.z, hid.x, hid.y };
 				for(int c = 0; c < 3; ++c)
 					update_moments(iter[c], st.radiance[size_t(pixel) * 3 + size_t(c)], st.radianceVar[size_t(pixel) * 3 + size_t(c)], it);
 				for(int c = 0; c < 2; ++c)
 					update_moments(iter[3 + c], st.hitId[size_t(pixel) * 2 + size_t(c)], st.hitIdVar[size_t(pixel) * 2 + size_t(c)], it);
+				for(int c = 0; c < AUX_CHANNELS; ++c)
+					update_moments(aux[c], st.aux[size_t(pixel) * AUX_CHANNELS + size_t(c)],
+					               st.auxVar[size_t(pixel) * AUX_CHANNELS + size_t(c)], it);
 			}
 		}
 #pragma omp critical
@@ -3155,6 +3197,8 @@ void* oracle_pt_create(void* s, const OrPtParams* params) {
 	st->hitId.assign(size_t(num) * 2, 0.0f);
 	st->radianceVar.assign(size_t(num) * 3, 0.0f);
 	st->hitIdVar.assign(size_t(num) * 2, 0.0f);
+	st->aux.assign(size_t(num) * AUX_CHANNELS, 0.0f);
+	st->auxVar.assign(size_t(num) * AUX_CHANNELS, 0.0f);
 	return st;
 }
 
@@ -3262,11 +3306,19 @@ int oracle_pt_iterate_rows(void* p, int32_t nt, uint32_t y0, uint32_t y1) {
 
 int oracle_pt_get_target(void* p, int32_t target, float* out) {
 	PtState* st = static_cast<PtState*>(p);
-	// 0 Radiance, 1 Hit ID; 2 and 3 their variances
+	// 0 Radiance, 1 Hit ID; 2 and 3 their variances; 4..9 Position, Depth,
+	// Normal, UV, Albedo, Lightness and 10..15 their variances
 	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->hitId
 	                            : target == 2 ? &st->radianceVar : target == 3 ? &st->hitIdVar : nullptr;
-	if(!v) return 0;
-	std::memcpy(out, v->data(), v->size() * 4);
+	if(v) { std::memcpy(out, v->data(), v->size() * 4); return 1; }
+	if(target < 4 || target > 15) return 0;
+	static const int first[6] = { AUX_POS, AUX_DEPTH, AUX_NORMAL, AUX_UV, AUX_ALBEDO, AUX_LIGHT };
+	static const int count[6] = { 3, 1, 3, 2, 3, 1 };
+	const int a = (target - 4) % 6;
+	const std::vector<float>& src = target < 10 ? st->aux : st->auxVar;
+	const size_t num = src.size() / AUX_CHANNELS;
+	for(size_t p = 0; p < num; ++p)
+		for(int c = 0; c < count[a]; ++c) out[p * size_t(count[a]) + size_t(c)] = src[p * AUX_CHANNELS + size_t(first[a] + c)];
 	return 1;
 }
 

@@ -286,6 +286,9 @@ class OraclePathTracer:
             threads = os.cpu_count() or 1
         lib().oracle_pt_iterate_rows(self.handle, threads, y0, y1)
 
+    # the auxiliary targets (pt_params.hpp:16-26): oracle target index, channels
+    AUX = {"Position": (4, 3), "Depth": (5, 1), "Normal": (6, 3), "UV": (7, 2), "Albedo": (8, 3), "Lightness": (9, 1)}
+
     def target(self, name: str, variance: bool = False):
         """Cumulative target, or with variance=True its running variance."""
         w, h = self.scene.spec.width, self.scene.spec.height
@@ -295,6 +298,10 @@ class OraclePathTracer:
         elif name == "Hit ID":
             out = np.zeros((h, w, 2), np.float32)
             lib().oracle_pt_get_target(self.handle, 3 if variance else 1, _ptr(out))
+        elif name in self.AUX:
+            k, ch = self.AUX[name]
+            out = np.zeros((h, w, ch), np.float32)
+            lib().oracle_pt_get_target(self.handle, k + (6 if variance else 0), _ptr(out))
         else:
             raise KeyError(name)
         return out
