@@ -65,8 +65,25 @@ static __device__ __noinline__ PrimHit other_prim_test(const DLod* l, FastRay r,
 	return h;
 }
 
+// Three-operand minimum and maximum of sm_100 (one instruction each; a NaN
+// operand is dropped like fminf/fmaxf drop it).
+MBD float min3_(float a, float b, float c) {
+	float d;
+	asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+	return d;
+}
+MBD float max3_(float a, float b, float c) {
+	float d;
+	asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+	return d;
+}
+
 // Tests the eight child boxes of node `idx`; returns the child's node group
-// and primitive group.
+// and primitive group. A child is hit when
+//   max(near planes, 0) <= min(far planes * (1 + 2^-20), tmaxBox).
+// The far-plane tolerance is applied to the per-node scale and offset, not per
+// child; that moves a far plane by a few ulp of its t, far less than the grid
+// step of margin every quantised box carries, so the test stays conservative.
 MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, uint32_t flip, float tmaxBox,
                         uint32_t& ngBase, uint32_t& ngImask, uint32_t& ngHits, uint32_t& pgBase, uint32_t& pgHits) {
 	const float4* q = reinterpret_cast<const float4*>(nodes + idx);
@@ -78,6 +95,8 @@ MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, u
 	const float ox = __fmul_rn(__fsub_rn(n0.x, r.o.x), r.inv.x);
 	const float oy = __fmul_rn(__fsub_rn(n0.y, r.o.y), r.inv.y);
 	const float oz = __fmul_rn(__fsub_rn(n0.z, r.o.z), r.inv.z);
+	const float fsx = __fmul_rn(sx, BOX_FAR_SLACK), fsy = __fmul_rn(sy, BOX_FAR_SLACK), fsz = __fmul_rn(sz, BOX_FAR_SLACK);
+	const float fox = __fmul_rn(ox, BOX_FAR_SLACK), foy = __fmul_rn(oy, BOX_FAR_SLACK), foz = __fmul_rn(oz, BOX_FAR_SLACK);
 	const uint32_t imask = eim >> 24;
 	const bool fx = r.inv.x < 0.0f, fy = r.inv.y < 0.0f, fz = r.inv.z < 0.0f;
 	const uint32_t lx0 = __float_as_uint(n2.x), lx1 = __float_as_uint(n2.y);
@@ -97,12 +116,12 @@ MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, u
 		const float tnx = __fmaf_rn(qbyte(nx[w], b), sx, ox);
 		const float tny = __fmaf_rn(qbyte(ny[w], b), sy, oy);
 		const float tnz = __fmaf_rn(qbyte(nz[w], b), sz, oz);
-		const float tfx = __fmaf_rn(qbyte(fxw[w], b), sx, ox);
-		const float tfy = __fmaf_rn(qbyte(fyw[w], b), sy, oy);
-		const float tfz = __fmaf_rn(qbyte(fzw[w], b), sz, oz);
-		const float tnear = fmax_(fmax_(tnx, tny), fmax_(tnz, 0.0f));
-		const float tfar = fmin_(fmin_(tfx, tfy), tfz);
-		if(tnear <= tmaxBox && tnear <= __fmul_rn(tfar, BOX_FAR_SLACK)) {
+		const float tfx = __fmaf_rn(qbyte(fxw[w], b), fsx, fox);
+		const float tfy = __fmaf_rn(qbyte(fyw[w], b), fsy, foy);
+		const float tfz = __fmaf_rn(qbyte(fzw[w], b), fsz, foz);
+		const float tnear = max3_(tnx, tny, fmax_(tnz, 0.0f));
+		const float tfar = min3_(tfx, tfy, fmin_(tfz, tmaxBox));
+		if(tnear <= tfar) {
 			if(imask & (1u << i)) {
 				nh |= 1u << (uint32_t(i) ^ flip);
 			} else {
@@ -196,15 +215,16 @@ struct WideTracer {
 				do {
 					const uint32_t j = uint32_t(__ffs(int(pgHits)) - 1);
 					pgHits &= pgHits - 1u;
+					// all three rows at once (every primitive has them), so a
+					// triangle costs one round trip to memory, not two
 					const float4* s4 = soup + 3 * size_t(pgBase + j);
-					const float4 a = __ldg(s4);
+					const float4 a = __ldg(s4), b = __ldg(s4 + 1), c = __ldg(s4 + 2);
 					const int p = __float_as_int(a.w);
 					++cnt.prims;
 					float t;
 					f2 uv;
 					bool hit;
 					if(uint32_t(p) < ntri) {
-						const float4 b = __ldg(s4 + 1), c = __ldg(s4 + 2);
 						hit = tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, uv) && t > 0.0f;
 					} else {
 						const PrimHit ph = other_prim_test(lod, r, p);
