@@ -52,6 +52,13 @@ typedef enum {
 	MATERIAL_BLEND, MATERIAL_FRESNEL, MATERIAL_MICROFACET, MATERIAL_NUM
 } MaterialParamType;
 typedef enum { MEDIUM_NONE, MEDIUM_DIELECTRIC, MEDIUM_CONDUCTOR } OuterMediumType;
+typedef enum { MIPMAP_NONE, MIPMAP_AVG, MIPMAP_MIN, MIPMAP_MAX } MipmapType;
+/* texture_data.h:10-31 */
+typedef enum {
+	FORMAT_R8U, FORMAT_RG8U, FORMAT_RGBA8U, FORMAT_R16U, FORMAT_RG16U, FORMAT_RGBA16U, FORMAT_R16F, FORMAT_RG16F,
+	FORMAT_RGBA16F, FORMAT_R32F, FORMAT_RG32F, FORMAT_RGBA32F, FORMAT_RGB8U, FORMAT_RGB16U, FORMAT_RGB16F,
+	FORMAT_RGB32F, FORMAT_NUM
+} TextureFormat;
 typedef enum { LOG_PEDANTIC, LOG_INFO, LOG_WARNING, LOG_ERROR, LOG_FATAL_ERROR } LogLevel;
 typedef enum { NONE = 0, OBJ_EMISSIVE = 1 } ObjectFlags;
 typedef enum { PARAM_INT, PARAM_FLOAT, PARAM_BOOL, PARAM_ENUM } ParameterType;
@@ -76,6 +83,8 @@ typedef void* SceneHdl;
 typedef void* MaterialHdl;
 typedef void* CameraHdl;
 typedef void* TextureHdl;
+/* core_interface.h:237-239 */
+typedef Vec4 (*TextureCallback)(uint32_t x, uint32_t y, uint32_t layer, TextureFormat format, Vec4 value, void* userParams);
 typedef const void* ConstCameraHdl;
 typedef void* MufflonInstanceHdl;
 typedef const void* ConstMufflonInstanceHdl;
@@ -200,6 +209,15 @@ CORE_API Boolean CDECL world_get_frame_count(MufflonInstanceHdl instHdl, uint32_
 CORE_API MaterialHdl CDECL world_add_material(MufflonInstanceHdl instHdl, const char* name, const MaterialParams* mat);
 CORE_API IndexType CDECL world_get_material_count(MufflonInstanceHdl instHdl);
 CORE_API TextureHdl CDECL world_add_texture_value(MufflonInstanceHdl instHdl, const float* value, int num, TextureSampling sampling);
+/* core_interface.h:469-477. world_add_texture reads a texture file: the core
+ * reads PFM ("PF" RGB, "Pf" one channel) itself, any other format fails (the
+ * reference's texture plugins). The callback, if given, rewrites each texel
+ * once. Textures are sampled with the nearest texel and have no mipmaps. */
+CORE_API TextureHdl CDECL world_get_texture(MufflonInstanceHdl instHdl, const char* path);
+CORE_API TextureHdl CDECL world_add_texture(MufflonInstanceHdl instHdl, const char* path, TextureSampling sampling, MipmapType type,
+                                            TextureCallback callback, void* userParams);
+CORE_API const char* CDECL world_get_texture_name(TextureHdl hdl);
+CORE_API Boolean CDECL world_get_texture_size(TextureHdl hdl, IVec2* size);
 /* EXTENSION: an RGBA float texture from memory (width * height * 4 floats, row 0 first). */
 CORE_API TextureHdl CDECL world_add_texture_rgba32f(MufflonInstanceHdl instHdl, const char* name, uint32_t width, uint32_t height, const float* texels, TextureSampling sampling);
 
@@ -433,6 +451,16 @@ CORE_API Boolean CDECL mufflon_lbvh_build(const float* vertices, uint32_t numVer
                                           uint32_t numTriangles, uint32_t numQuads, const float* spheres,
                                           uint32_t numSpheres, uint64_t* mortonSorted, int32_t* parents,
                                           void* nodes, int32_t* primIds, int32_t* numInternal, float* stageMs);
+/* The same build with the Morton code width chosen: 63 bits (what
+ * mufflon_lbvh_build and every scene load use, the reference's choice for LoD
+ * and instance hierarchies, build_lbvh.cu:35-48) or the reference's unused
+ * 30-bit code (build_lbvh.cu:59-69: 10 bits per axis). mortonSorted then holds
+ * the 30-bit codes, zero-extended. */
+CORE_API Boolean CDECL mufflon_lbvh_build_ex(const float* vertices, uint32_t numVertices, const uint32_t* indices,
+                                             uint32_t numTriangles, uint32_t numQuads, const float* spheres,
+                                             uint32_t numSpheres, int32_t mortonBits, uint64_t* mortonSorted,
+                                             int32_t* parents, void* nodes, int32_t* primIds, int32_t* numInternal,
+                                             float* stageMs);
 /* Same build on device-resident inputs; outputs stay on the device. Times
  * the whole build with CUDA events (ms), 8-wide conversion included. Returns
  * the node count after collapse; stageMs as above (9 floats). */

@@ -39,6 +39,18 @@ class UVec3(Structure):
     _fields_ = [("x", c_uint32), ("y", c_uint32), ("z", c_uint32)]
 
 
+class Vec4(Structure):
+    _fields_ = [("x", c_float), ("y", c_float), ("z", c_float), ("w", c_float)]
+
+
+class IVec2(Structure):
+    _fields_ = [("x", c_int32), ("y", c_int32)]
+
+
+# Vec4 (*TextureCallback)(x, y, layer, TextureFormat, Vec4 value, void* userParams), core_interface.h:237-239
+TextureCallback = ctypes.CFUNCTYPE(Vec4, c_uint32, c_uint32, c_uint32, c_int, Vec4, c_void_p)
+
+
 class UVec4(Structure):
     _fields_ = [("x", c_uint32), ("y", c_uint32), ("z", c_uint32), ("w", c_uint32)]
 
@@ -284,6 +296,13 @@ class DllHolder:
             "world_add_material": (c_void_p, [c_void_p, c_char_p, POINTER(MaterialParams)]),
             "world_add_texture_value": (c_void_p, [c_void_p, POINTER(c_float), c_int, c_int]),
             "world_add_texture_rgba32f": (c_void_p, [c_void_p, c_char_p, c_uint32, c_uint32, c_void_p, c_int]),
+            "mufflon_lbvh_build_ex": (c_uint32, [c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_void_p, c_uint32,
+                                                 c_int32, c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int32),
+                                                 c_void_p]),
+            "world_add_texture": (c_void_p, [c_void_p, c_char_p, c_int, c_int, TextureCallback, c_void_p]),
+            "world_get_texture": (c_void_p, [c_void_p, c_char_p]),
+            "world_get_texture_name": (c_char_p, [c_void_p]),
+            "world_get_texture_size": (c_uint32, [c_void_p, POINTER(IVec2)]),
             "world_add_pinhole_camera": (c_void_p, [c_void_p, c_char_p, POINTER(Vec3), POINTER(Vec3), POINTER(Vec3),
                                                     c_uint32, c_float, c_float, c_float]),
             "world_get_camera": (c_void_p, [c_void_p, c_char_p]),
@@ -673,8 +692,9 @@ class DllInterface:
         return nodes, prim, ni.value
 
 
-def lbvh_build(dll: DllInterface, lod):
-    """GPU LBVH build of one LodSpec: (morton_sorted, parents, nodes, prim_ids, num_internal, stage_ms)."""
+def lbvh_build(dll: DllInterface, lod, morton_bits: int = 63):
+    """GPU LBVH build of one LodSpec with 63- or 30-bit Morton codes:
+    (morton_sorted, parents, nodes, prim_ids, num_internal, stage_ms)."""
     idx = np.concatenate([lod.triangles.reshape(-1), lod.quads.reshape(-1)]).astype(np.uint32)
     v = np.ascontiguousarray(lod.vertices, np.float32)
     s = np.ascontiguousarray(lod.spheres, np.float32)
@@ -685,9 +705,10 @@ def lbvh_build(dll: DllInterface, lod):
     prim = np.zeros(max(n, 1), np.int32)
     ni = c_int32(0)
     ms = np.zeros(9, np.float32)
-    ok = dll.core.mufflon_lbvh_build(_ptr(v), len(v), _ptr(idx), len(lod.triangles), len(lod.quads), _ptr(s), len(s),
-                                     _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim), byref(ni), _ptr(ms))
-    dll._check(ok, "mufflon_lbvh_build")
+    ok = dll.core.mufflon_lbvh_build_ex(_ptr(v), len(v), _ptr(idx), len(lod.triangles), len(lod.quads), _ptr(s),
+                                        len(s), morton_bits, _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim),
+                                        byref(ni), _ptr(ms))
+    dll._check(ok, "mufflon_lbvh_build_ex")
     return morton[:n], parents[:max(2 * n - 1, 0)], nodes[:2 * ni.value], prim[:n], ni.value, ms
 
 
@@ -729,8 +750,10 @@ def render_batch(jobs, use_graph=True, hit_ids=False):
     return imgs, (hits if hit_ids else None), list(done), {k: getattr(st, k) for k, _ in MufflonBatchStats._fields_}
 
 
-def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
-    """Builds a SceneSpec through the world-building C API and loads it."""
+def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None, texture_files=None, texture_callback=None):
+    """Builds a SceneSpec through the world-building C API and loads it. With `texture_files`
+    (a path per texture of the spec), the textures are read from those files with world_add_texture,
+    passing `texture_callback` (a TextureCallback or None), instead of from the spec's arrays."""
     core, I = dll.core, dll.muffInst
     keep = []
     sc = core.world_create_scenario(I, (scenario_name or spec.name).encode())
@@ -744,6 +767,12 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
 
     textures = []
     for k, tex in enumerate(spec.textures):
+        if texture_files is not None:
+            t = core.world_add_texture(I, str(texture_files[k]).encode(), 0, 0,
+                                       texture_callback or TextureCallback(), None)
+            dll._check(t, "world_add_texture")
+            textures.append(t)
+            continue
         a = np.ascontiguousarray(tex, np.float32)
         keep.append(a)
         t = core.world_add_texture_rgba32f(I, f"texture{k}".encode(), a.shape[1], a.shape[0], _ptr(a), 0)
@@ -769,6 +798,8 @@ def load_scene_spec(dll: DllInterface, spec, scenario_name: str = None):
             p.innerType = MaterialParamType.EMISSIVE
             p.inner.emissive.radiance = tex_value(m.radiance)
             p.inner.emissive.scale = Vec3(*m.scale)
+        if getattr(m, "alpha_texture", -1) >= 0:
+            p.alpha = textures[m.alpha_texture]
         mh = core.world_add_material(I, name, byref(p))
         dll._check(mh, "world_add_material")
         dll.materials.append(mh)

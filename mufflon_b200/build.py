@@ -33,7 +33,7 @@ CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
 # the scene-file loader: its own library on top of the core's C API
 LOADER_SOURCES = ["loader/json.cpp", "loader/mff_binary.cpp", "loader/scene_loader.cpp", "loader/interface.cpp"]
 LOADER_HEADERS = ["loader/json.hpp", "loader/mff_binary.hpp", "loader/scene_loader.hpp"]
-HEADERS = ["common/fmath.hpp", "trace/dmath.cuh", "trace/intersect.cuh", "trace/shading.cuh",
+HEADERS = ["common/fmath.hpp", "common/pfm.hpp", "trace/dmath.cuh", "trace/intersect.cuh", "trace/shading.cuh",
            "trace/scene_types.hpp", "trace/pt_api.hpp", "lbvh/lbvh.hpp", "lbvh/radix_sort.cuh",
            "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "trace/wide_traverse.cuh", "lbvh/wide.hpp", "core/world.hpp",
            "core/light_build.hpp", "core/instance_boxes.hpp", "trace/lt_api.hpp",

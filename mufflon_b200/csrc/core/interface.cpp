@@ -7,6 +7,7 @@
 #include "world.hpp"
 #include "../trace/pt_api.hpp"
 #include "../lbvh/sort_noalloc.hpp"
+#include "../common/pfm.hpp"
 
 #include <algorithm>
 #include <cstdio>
@@ -14,6 +15,8 @@
 #include <cstdarg>
 #include <cstring>
 #include <exception>
+#include <fstream>
+#include <iterator>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -852,6 +855,7 @@ MaterialHdl world_add_material(MufflonInstanceHdl h, const char* name, const Mat
 		default:
 			throw ApiError("material type not implemented by the CUDA path tracer");
 	}
+	m->alpha = static_cast<HostTexture*>(p->alpha); // interface.cpp:1350-1351
 	I.materials.push_back(std::move(m));
 	I.sceneDirty = true;
 	return I.materials.back().get();
@@ -885,6 +889,83 @@ TextureHdl world_add_texture_rgba32f(MufflonInstanceHdl h, const char* name, uin
 	I.sceneDirty = true;
 	return I.textures.back().get();
 	CATCH_ALL(nullptr)
+}
+
+// core_interface.h:469-477. The core reads texture files itself (it has no
+// plugin system): PFM files ("PF" RGB, "Pf" one channel) as the reference's
+// PFM plugin reads them (src/pfmloader/interface.cpp:74-160); any other
+// format fails with a message, as a path no plugin can load does
+// (interface.cpp:1831-1835). A path that is already loaded returns the same
+// texture. A callback rewrites every texel once (interface.cpp:1843-1856).
+// Textures are sampled with the nearest texel whatever the sampling mode, and
+// carry no mipmaps.
+TextureHdl world_add_texture(MufflonInstanceHdl h, const char* path, TextureSampling, MipmapType,
+                             TextureCallback callback, void* userParams) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(path, "texture path is null");
+	for(auto& t : I.textures)
+		if(t->name == path) return t.get();
+	const std::string p(path);
+	const size_t dot = p.find_last_of('.');
+	std::string ext = dot == std::string::npos ? std::string() : p.substr(dot);
+	for(char& c : ext) c = char(std::tolower(static_cast<unsigned char>(c)));
+	CHECK(ext == ".pfm", "no texture reader for '" + p + "' (the core reads PFM files)");
+	std::ifstream f(p, std::ios::binary);
+	CHECK(f.good(), "cannot open texture file '" + p + "'");
+	const std::string bytes((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+	PfmImage img;
+	try {
+		img = parse_pfm(bytes);
+	} catch(const std::runtime_error& e) {
+		throw ApiError("texture '" + p + "': " + e.what());
+	}
+	auto t = std::make_unique<HostTexture>();
+	t->name = p;
+	t->width = img.width; t->height = img.height;
+	t->channels = img.channels == 1 ? 1u : 4u;
+	t->texels = std::move(img.rgba);
+	if(callback) {
+		const TextureFormat fmt = img.channels == 1 ? FORMAT_R32F : FORMAT_RGBA32F;
+		for(uint32_t y = 0; y < t->height; ++y)
+			for(uint32_t x = 0; x < t->width; ++x) {
+				float* v = &t->texels[(size_t(y) * t->width + x) * 4];
+				const Vec4 out = callback(x, y, 0u, fmt, Vec4{ v[0], v[1], v[2], v[3] }, userParams);
+				v[0] = out.x;
+				if(t->channels == 4) { v[1] = out.y; v[2] = out.z; v[3] = out.w; }
+			}
+	}
+	I.textures.push_back(std::move(t));
+	I.sceneDirty = true;
+	return I.textures.back().get();
+	CATCH_ALL(nullptr)
+}
+
+TextureHdl world_get_texture(MufflonInstanceHdl h, const char* path) {
+	TRY
+	MufflonInstance& I = minst(h);
+	CHECK(path, "texture path is null");
+	for(auto& t : I.textures)
+		if(t->name == path) return t.get();
+	throw ApiError(std::string("could not find texture ") + path);
+	CATCH_ALL(nullptr)
+}
+
+const char* world_get_texture_name(TextureHdl hdl) {
+	TRY
+	CHECK(hdl, "texture handle is null");
+	return static_cast<HostTexture*>(hdl)->name.c_str();
+	CATCH_ALL(nullptr)
+}
+
+Boolean world_get_texture_size(TextureHdl hdl, IVec2* size) {
+	TRY
+	CHECK(hdl && size, "texture handle or size is null");
+	const HostTexture* t = static_cast<HostTexture*>(hdl);
+	size->x = int32_t(t->width);
+	size->y = int32_t(t->height);
+	return true;
+	CATCH_ALL(false)
 }
 
 // ---------------------------------------------------------------- cameras
@@ -1288,7 +1369,9 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 			if(r.graphExec) cudaGraphExecDestroy(r.graphExec);
 			r.graphExec = nullptr;
 			r.graphKey.clear();
-			prepare_batch_kernels(tune);
+			WfTuning warm = tune;
+			warm.alpha = I.scene.desc.hasAlpha != 0;
+			prepare_batch_kernels(warm);
 			cudaGraph_t g = nullptr;
 			CHECK_CUDA(cudaStreamBeginCapture(I.stream, cudaStreamCaptureModeThreadLocal));
 			const cudaError_t e = launch_pt_wavefront(I.scene.desc, r.params, rs, r.wf, r.counters, I.stream, &info, tune);
@@ -1708,6 +1791,7 @@ Boolean mufflon_render_batch(const MufflonBatchJob* jobs, uint32_t count, int32_
 	tune.counters = false;
 	// binning keeps the rays of different scenes apart: the scene's index among the batch's instances
 	while((size_t(1) << tune.sortGroupBits) < uniq.size()) ++tune.sortGroupBits;
+	for(const auto* u : uniq) tune.alpha = tune.alpha || u->scene.desc.hasAlpha != 0;
 	prepare_batch_kernels(tune);
 	while(B.events.size() < size_t(maxSpp) + 1) {
 		cudaEvent_t e;
@@ -2048,8 +2132,17 @@ Boolean mufflon_get_bvh(MufflonInstanceHdl h, int32_t which, int32_t* numPrims, 
 Boolean mufflon_lbvh_build(const float* vertices, uint32_t numVertices, const uint32_t* indices, uint32_t numTriangles,
                            uint32_t numQuads, const float* spheres, uint32_t numSpheres, uint64_t* mortonSorted,
                            int32_t* parents, void* nodes, int32_t* primIds, int32_t* numInternal, float* stageMs) {
+	return mufflon_lbvh_build_ex(vertices, numVertices, indices, numTriangles, numQuads, spheres, numSpheres, 63,
+	                             mortonSorted, parents, nodes, primIds, numInternal, stageMs);
+}
+
+Boolean mufflon_lbvh_build_ex(const float* vertices, uint32_t numVertices, const uint32_t* indices, uint32_t numTriangles,
+                              uint32_t numQuads, const float* spheres, uint32_t numSpheres, int32_t mortonBits,
+                              uint64_t* mortonSorted, int32_t* parents, void* nodes, int32_t* primIds,
+                              int32_t* numInternal, float* stageMs) {
 	TRY
 	CHECK(mufflon_is_cuda_available(), "no CUDA device");
+	CHECK(mortonBits == 63 || mortonBits == 30, "Morton codes have 63 or 30 bits");
 	HostLod L;
 	L.vertices.assign(vertices, vertices + 3 * size_t(numVertices));
 	L.triIdx.assign(indices, indices + 3 * size_t(numTriangles));
@@ -2071,6 +2164,7 @@ Boolean mufflon_lbvh_build(const float* vertices, uint32_t numVertices, const ui
 	L.bounds(in.aabbMin, in.aabbMax);
 	LbvhBuilder builder;
 	builder.enable_timing(stageMs != nullptr);
+	builder.set_morton_bits(mortonBits);
 	BvhBuffers out;
 	cudaStream_t s;
 	CHECK_CUDA(cudaStreamCreate(&s));

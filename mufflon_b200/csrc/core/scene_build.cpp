@@ -214,12 +214,19 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	// --- materials per slot (scene.cpp load_materials)
 	std::vector<DMaterial> mats(std::max<size_t>(sc->slotMaterials.size(), 1));
 	std::vector<const HostTexture*> texList;
+	bool hasAlpha = false;
 	for(size_t i = 0; i < sc->slotMaterials.size(); ++i) {
 		const HostMaterial* m = sc->slotMaterials[i];
 		DMaterial& d = mats[i];
 		d = DMaterial{};
 		d.albedoTex = -1;
+		d.alphaTex = -1;
 		if(!m) { d.type = MAT_LAMBERT; continue; }
+		if(m->alpha) {
+			d.alphaTex = int32_t(texList.size());
+			texList.push_back(m->alpha);
+			hasAlpha = true;
+		}
 		d.type = m->type;
 		d.shadowing = m->shadowing;
 		const V3 alb = tex_value(m->albedo, V3{ 0.5f, 0.5f, 0.5f });
@@ -469,6 +476,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	S.worldToInstance = D.dW2I; S.instanceLod = D.dInstLod; S.numInstances = numInst;
 	S.activeInstances = active; S.validInstance = valid;
 	S.maxSteps = MAX_TRAVERSAL_STEPS;
+	S.hasAlpha = hasAlpha ? 1 : 0;
 	S.tlasNodes = D.tlas.nodes; S.tlasPrimIds = D.tlas.primIds; S.tlasNumInternal = D.tlas.numInternal;
 	S.tlasWide = D.tlas.wnodes; S.tlasWidePrims = D.tlas.wprims; S.tlasNumWide = D.tlas.numWide;
 	S.materials = D.dMaterials; S.textures = D.dTextures;

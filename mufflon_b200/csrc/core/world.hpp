@@ -92,6 +92,7 @@ struct HostMaterial {
 	HostTexture* albedo = nullptr;
 	HostTexture* roughness = nullptr;
 	HostTexture* radiance = nullptr;
+	HostTexture* alpha = nullptr;   // MaterialParams::alpha: cut-out where its first channel < 0.5
 	float scale[3] = { 1, 1, 1 };
 	int32_t shadowing = 1, ndf = 1;
 	bool supported = true;

@@ -115,24 +115,54 @@ MBD bool count_limit(int mode, Counts c) {
 	if(mode == MODE_SCENE) return c.c0 >= 1023;
 	return c.c0 >= 1023 || c.c1 >= 1023 || c.c2 >= 1023;
 }
+// sfcurves.hpp:37-46 (10 bits to every third bit) and build_lbvh.cu:59-69:
+// the 30-bit code, kept in the low bits of the 64-bit key. The hierarchy the
+// Karras emit builds on it equals the one on 32-bit keys: every common-prefix
+// length of two keys (and of two equal keys' indices) grows by the same 32
+// bits, and the emit only compares such lengths.
+MBD uint32_t part_by_two10(uint32_t x) {
+	uint32_t r = x;
+	r = (r * 0x00010001u) & 0xFF0000FFu;
+	r = (r * 0x00000101u) & 0x0F00F00Fu;
+	r = (r * 0x00000011u) & 0xC30C30C3u;
+	r = (r * 0x00000005u) & 0x49249249u;
+	return r;
+}
+MBD uint32_t disc10(float v) {
+	float x = v * 1024.0f;
+	x = fminf(fmaxf(x, 0.0f), 1023.0f);
+	return uint32_t(x);
+}
+MBD u64 morton30(f3 p, const float* mn, const float* mx) {
+	const f3 lo = make3(mn[0], mn[1], mn[2]);
+	const f3 span = make3(mx[0], mx[1], mx[2]) - lo;
+	const f3 d = p - lo;
+	const f3 n = make3(sdiv(d.x, span.x), sdiv(d.y, span.y), sdiv(d.z, span.z));
+	return u64(part_by_two10(disc10(n.x)) * 4u + part_by_two10(disc10(n.y)) * 2u + part_by_two10(disc10(n.z)));
+}
+
 MBD float surface(f3 mn, f3 mx) {
 	const f3 d = mx - mn;
 	return 2.0f * (d.x * d.y + d.x * d.z + d.y * d.z);
 }
 
 // ---------------------------------------------------------------- Morton
-__global__ void k_morton_lod(LodBuildInput in, uint32_t n, u64* keys, int32_t* vals) {
+__global__ void k_morton_lod(LodBuildInput in, uint32_t n, u64* keys, int32_t* vals, int bits) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= n) return;
-	keys[i] = morton63(lod_centroid(in, int(i)), in.aabbMin, in.aabbMax);
+	const f3 c = lod_centroid(in, int(i));
+	keys[i] = bits == 30 ? morton30(c, in.aabbMin, in.aabbMax) : morton63(c, in.aabbMin, in.aabbMax);
 	vals[i] = int32_t(i);
 }
 
-__global__ void k_morton_scene(SceneBuildInput in, uint32_t n, u64* keys, int32_t* vals) {
+__global__ void k_morton_scene(SceneBuildInput in, uint32_t n, u64* keys, int32_t* vals, int bits) {
 	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= n) return;
-	if(in.instanceLod[i] == 0xFFFFFFFFu) keys[i] = ~0ull;
-	else keys[i] = morton63(v3(in.instCentroids, i), in.aabbMin, in.aabbMax);
+	if(in.instanceLod[i] == 0xFFFFFFFFu) keys[i] = bits == 30 ? u64(0xFFFFFFFFu) : ~0ull;
+	else {
+		const f3 c = v3(in.instCentroids, i);
+		keys[i] = bits == 30 ? morton30(c, in.aabbMin, in.aabbMax) : morton63(c, in.aabbMin, in.aabbMax);
+	}
 	vals[i] = int32_t(i);
 }
 
@@ -509,7 +539,7 @@ cudaError_t LbvhBuilder::reserve(uint32_t n) {
 	return cudaSuccess;
 }
 
-cudaError_t LbvhBuilder::sort_pairs(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream) {
+cudaError_t LbvhBuilder::sort_pairs(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream, int passes) {
 	cudaError_t e = reserve(n);
 	if(e != cudaSuccess || n <= 1) return e;
 	const uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
@@ -522,14 +552,14 @@ cudaError_t LbvhBuilder::sort_pairs(uint64_t* keys, int32_t* values, uint32_t n,
 	u64* kin = keys; u64* kout = (keys == m_keysA) ? m_keysB : m_keysA;
 	int32_t* vin = values; int32_t* vout = (values == m_valsA) ? m_valsB : m_valsA;
 	// ping-pong between the caller's buffers and the builder's spare ones
-	for(int pass = 0; pass < 8; ++pass) {
+	for(int pass = 0; pass < passes; ++pass) {
 		cudaMemsetAsync(m_status, 0, size_t(tiles) * 256 * sizeof(uint32_t), stream);
 		k_onesweep<<<tiles, SORT_THREADS, SORT_SMEM, stream>>>(kin, vin, kout, vout, n, 8 * pass,
 			m_hist + 256 * pass, m_status, m_tileCounter + pass, m_error);
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}
-	// after 8 passes the data is back in (keys, values)
+	// after an even number of passes the data is back in (keys, values)
 	return cudaGetLastError();
 }
 
@@ -596,10 +626,11 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	const int numInternal = n - 1;
 	const int numNodes = numInternal + n;
 	if(m_timing) cudaEventRecord(m_ev[0], stream);
-	if(mode == MODE_LOD) k_morton_lod<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*lod, numPrimitives, m_keysA, m_valsA);
-	else k_morton_scene<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*scene, numPrimitives, m_keysA, m_valsA);
+	if(mode == MODE_LOD) k_morton_lod<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*lod, numPrimitives, m_keysA, m_valsA, m_mortonBits);
+	else k_morton_scene<<<blocks_for(numPrimitives, 256), 256, 0, stream>>>(*scene, numPrimitives, m_keysA, m_valsA, m_mortonBits);
 	if(m_timing) cudaEventRecord(m_ev[1], stream);
-	if((e = sort_pairs(m_keysA, m_valsA, numPrimitives, stream)) != cudaSuccess) return e;
+	// 30-bit codes: their four low bytes are the whole key
+	if((e = sort_pairs(m_keysA, m_valsA, numPrimitives, stream, m_mortonBits == 30 ? 4 : 8)) != cudaSuccess) return e;
 	if(m_timing) cudaEventRecord(m_ev[2], stream);
 	cudaMemsetAsync(m_parents, 0, sizeof(int32_t) * numNodes, stream);
 	k_karras<<<blocks_for(numInternal, 256), 256, 0, stream>>>(n, m_keysA, m_parents, m_children, m_marks, m_ranges);

@@ -91,7 +91,10 @@ public:
 
 	// Standalone stable sort of (u64 key, i32 value) pairs; used by the
 	// builder and exposed for tests. Results land in keys/values.
-	cudaError_t sort_pairs(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream);
+	// Stable sort by the low 8 * passes key bits (passes even, at most 8).
+	cudaError_t sort_pairs(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream, int passes = 8);
+	// Morton code width of the hierarchies: 63 (the reference's, default) or 30.
+	void set_morton_bits(int bits) { m_mortonBits = bits == 30 ? 30 : 63; }
 
 private:
 	cudaError_t reserve(uint32_t n);
@@ -123,6 +126,7 @@ private:
 	int32_t* m_hostCount = nullptr;   // pinned
 	int32_t m_lastN = 0;
 	bool m_timing = false;
+	int m_mortonBits = 63;
 	StageTimes m_times{};
 	cudaEvent_t m_ev[10] = {};
 };

@@ -14,6 +14,7 @@
 // still loads as long as no scenario uses them; a scenario that does use one
 // fails with the core's message.
 #include "scene_loader.hpp"
+#include "../common/pfm.hpp"
 
 #include <cctype>
 #include <cmath>
@@ -149,46 +150,18 @@ FileVersion parse_version(const std::string& s, const Reader& r) {
 // rows as stored, alpha 0 (src/pfmloader/interface.cpp:80-150).
 std::vector<float> read_pfm_rgb(const fs::path& p, uint32_t& w, uint32_t& h) {
 	const std::string data = read_text_file(p);
-	size_t pos = 0;
-	auto fail = [&](const std::string& m) -> void { throw LoaderError("texture '" + p.string() + "': " + m); };
-	auto skip_ws = [&]() { while(pos < data.size() && std::isspace(static_cast<unsigned char>(data[pos]))) ++pos; };
-	auto token = [&]() {
-		skip_ws();
-		const size_t s = pos;
-		while(pos < data.size() && !std::isspace(static_cast<unsigned char>(data[pos]))) ++pos;
-		return data.substr(s, pos - s);
-	};
-	if(data.size() < 2) fail("not a PFM file");
-	const std::string bands = data.substr(0, 2);
-	pos = 2;
-	if(bands == "Pf") fail("single-channel PFM textures are not supported for colours");
-	if(bands != "PF") fail("only PFM (\"PF\") textures are read by this loader");
-	long long wi = 0, hi = 0;
-	double scale = 0.0;
+	if(data.size() >= 2 && data.compare(0, 2, "Pf") == 0)
+		throw LoaderError("texture '" + p.string() + "': single-channel PFM textures are not supported for colours");
+	if(data.size() >= 2 && data.compare(0, 2, "PF") != 0)
+		throw LoaderError("texture '" + p.string() + "': only PFM (\"PF\") textures are read by this loader");
 	try {
-		wi = std::stoll(token());
-		hi = std::stoll(token());
-		scale = std::stod(token());
-	} catch(const std::logic_error&) { fail("malformed PFM header"); }
-	if(wi <= 0 || hi <= 0 || wi > 65536 || hi > 65536) fail("invalid PFM size");
-	if(pos < data.size() && data[pos] == '\r') ++pos;
-	if(pos >= data.size() || data[pos] != '\n') fail("expected a newline after the PFM header");
-	++pos;
-	const size_t count = size_t(wi) * size_t(hi) * 3u;
-	if(data.size() - pos < count * 4u) fail("PFM data shorter than its header says");
-	const bool swap = scale > 0.0; // big-endian data on a little-endian host
-	std::vector<float> rgba(size_t(wi) * size_t(hi) * 4u, 0.0f);
-	for(size_t i = 0; i < size_t(wi) * size_t(hi); ++i) {
-		for(int c = 0; c < 3; ++c) {
-			unsigned char b[4];
-			std::memcpy(b, data.data() + pos + (3 * i + c) * 4, 4);
-			if(swap) { std::swap(b[0], b[3]); std::swap(b[1], b[2]); }
-			std::memcpy(&rgba[4 * i + c], b, 4);
-		}
+		mb::PfmImage img = mb::parse_pfm(data);
+		w = img.width;
+		h = img.height;
+		return std::move(img.rgba);
+	} catch(const std::runtime_error& e) {
+		throw LoaderError("texture '" + p.string() + "': " + e.what());
 	}
-	w = uint32_t(wi);
-	h = uint32_t(hi);
-	return rgba;
 }
 
 void transform_box(const float* m, const float* mn, const float* mx, float* outMin, float* outMax) {
@@ -468,8 +441,6 @@ private:
 			p.outerMedium.refractionIndex = Vec2{ 1.0f, 0.0f };
 		}
 		const std::string type = r.text(r.req(m, "type"), "type");
-		if(r.opt(m, "alpha") && type != "emissive")
-			r.fail("alpha textures are not supported by the CUDA path tracer");
 		if(r.opt(m, "displacement")) r.fail("displacement maps are not supported by the CUDA path tracer");
 		if(type == "lambert") {
 			p.innerType = MATERIAL_LAMBERT;
@@ -521,6 +492,13 @@ private:
 		} else {
 			r.fail("material type '" + type + "' is not supported");
 		}
+		// the alpha texture comes last so that emissive materials drop it
+		// (json_loader.cpp:232-233, 326-329, 401-407)
+		if(type != "emissive")
+			if(const JsonValue* a = r.opt(m, "alpha")) {
+				if(!a->is_string()) r.fail("alpha: expected a texture path");
+				p.alpha = texture_file(a->string);
+			}
 	}
 
 	MaterialHdl material(const std::string& name) {

@@ -221,6 +221,7 @@ MBD void bpt_add(const LtTargets& T, uint32_t pix, float4 v) {
 }
 
 // cpu_bpt.cpp:170-232 as a per-lane state machine
+template < int AM >
 __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P, const LtTargets T, BV* lightVerts,
                                                 unsigned int* workCounter, TraceCounters* counters) {
 	LocalStack stack;
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 		if(!trace) continue;
 		++cnt.rays;
 		if(shadow) ++cnt.shadow;
-		WideTracer t;
+		WideTracerT<AM> t;
 		t.init(S, ro, rd, tmax, shadow, cnt);
 		while(!t.step(S, cnt, stack)) {}
 		if(shadow) {
@@ -480,7 +481,11 @@ int bpt_blocks() {
 		int dev = 0, sms = 148, perSm = 0;
 		cudaGetDevice(&dev);
 		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_bpt, 128, 0);
+		// both variants (scenes with and without alpha textures) fit as many blocks
+		int perSmAlpha = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_bpt<ALPHA_NEVER>, 128, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmAlpha, k_bpt<ALPHA_ALWAYS>, 128, 0);
+		if(perSmAlpha > perSm) perSm = perSmAlpha;
 		blocks = sms * (perSm > 0 ? perSm : 1);
 	}
 	return blocks;
@@ -505,7 +510,9 @@ cudaError_t launch_bpt(const DScene& S, const LtParams& P, const LtTargets& T, v
 		if((e = cudaMemsetAsync(T.recValue, 0, slots * 4 * sizeof(float), stream)) != cudaSuccess) return e;
 	}
 	if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-	k_bpt<<<bpt_blocks(), 128, 0, stream>>>(S, P, T, static_cast<BV*>(scratch), workCounter, counters);
+	// the variant for the scene: alpha textures or none (no alpha code in the loop)
+	if(S.hasAlpha) k_bpt<ALPHA_ALWAYS><<<bpt_blocks(), 128, 0, stream>>>(S, P, T, static_cast<BV*>(scratch), workCounter, counters);
+	else k_bpt<ALPHA_NEVER><<<bpt_blocks(), 128, 0, stream>>>(S, P, T, static_cast<BV*>(scratch), workCounter, counters);
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_bpt_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
 	return cudaGetLastError();

@@ -139,7 +139,9 @@ MBD float computeU(float v, float A1, float A2, float B1, float B2, float C1, fl
 }
 
 // intersection.cu:99-179
-MBD bool quad_test(f3 p00, f3 p10, f3 p11, f3 p01, const FastRay& ray, float& resT1, f2& uv1) {
+// Both roots: (resT1, uv1) is the nearer positive one, (resT2, uv2) the other
+// (t <= 0: none), which the alpha test falls back to.
+MBD bool quad_test(f3 p00, f3 p10, f3 p11, f3 p01, const FastRay& ray, float& resT1, f2& uv1, float& resT2, f2& uv2) {
 	int d0 = 0, d1 = 1, d2 = 2;
 	if(pabs(ray.d.x) < pabs(ray.d.y) || pabs(ray.d.x) < pabs(ray.d.z)) {
 		if(pabs(ray.d.y) >= pabs(ray.d.z)) { d0 = 1; d1 = 0; d2 = 2; }
@@ -169,6 +171,7 @@ MBD bool quad_test(f3 p00, f3 p10, f3 p11, f3 p01, const FastRay& ray, float& re
 		if(v1 == v0) {
 			uv1 = make2(u0, v0);
 			resT1 = t0;
+			resT2 = -1.0f;
 		} else {
 			if(v1 >= 0.0f && v1 <= 1.0f) {
 				u1 = computeU(v1, A1, A2, B1, B2, C1, C2, D1, D2);
@@ -176,10 +179,10 @@ MBD bool quad_test(f3 p00, f3 p10, f3 p11, f3 p01, const FastRay& ray, float& re
 					t1 = ((((u1 * v1) * a[d0] + u1 * b[d0]) + v1 * c[d0]) + d[d0]) * ray.inv[d0];
 			}
 			if(t0 > 0.0f) {
-				if(t1 > 0.0f && t1 < t0) { uv1 = make2(u1, v1); resT1 = t1; }
-				else { uv1 = make2(u0, v0); resT1 = t0; }
+				if(t1 > 0.0f && t1 < t0) { uv1 = make2(u1, v1); uv2 = make2(u0, v0); resT1 = t1; resT2 = t0; }
+				else { uv1 = make2(u0, v0); uv2 = make2(u1, v1); resT1 = t0; resT2 = t1; }
 			} else {
-				uv1 = make2(u1, v1); resT1 = t1;
+				uv1 = make2(u1, v1); uv2 = make2(u0, v0); resT1 = t1; resT2 = t0;
 			}
 		}
 		return resT1 > 0.0f;
@@ -187,7 +190,9 @@ MBD bool quad_test(f3 p00, f3 p10, f3 p11, f3 p01, const FastRay& ray, float& re
 	return false;
 }
 
-MBD bool sphere_test(const FastRay& r, f3 c, float rad, float& t) {
+// Nearest positive root t; t2 is the far root when t is the near one (the
+// alpha test's fallback), else -1.
+MBD bool sphere_test(const FastRay& r, f3 c, float rad, float& t, float& t2) {
 	const f3 oc = r.o - c;
 	const float b = dot(oc, r.d);
 	const float cc = dot(oc, oc) - rad * rad;
@@ -197,31 +202,115 @@ MBD bool sphere_test(const FastRay& r, f3 c, float rad, float& t) {
 	float x0, x1;
 	if(q == 0.0f) { x0 = x1 = 0.0f; }
 	else { x0 = q; x1 = __fdiv_rn(cc, q); if(x0 > x1) { const float tt = x0; x0 = x1; x1 = tt; } }
-	if(x0 > 0.0f) { t = x0; return true; }
-	if(x1 > 0.0f) { t = x1; return true; }
+	if(x0 > 0.0f) { t = x0; t2 = x1; return true; }
+	if(x1 > 0.0f) { t = x1; t2 = -1.0f; return true; }
 	return false;
+}
+MBD bool sphere_test(const FastRay& r, f3 c, float rad, float& t) {
+	float t2;
+	return sphere_test(r, c, rad, t, t2);
 }
 
 MBD f3 vert(const DLod& l, uint32_t i) { return ldg3(l.vertices + 3 * size_t(i)); }
 
+// Nearest-texel lookup with wrap-around (the CPU textures' nearest sampling).
+MBD f3 sample_texture(const DTexture& t, f2 uv) {
+	const float fx = uv.x - floorf(uv.x), fy = uv.y - floorf(uv.y);
+	int x = int(fx * float(t.width)), y = int(fy * float(t.height));
+	if(x >= int(t.width)) x = int(t.width) - 1;
+	if(y >= int(t.height)) y = int(t.height) - 1;
+	const float4 v = __ldg(t.texels + size_t(y) * t.width + x);
+	return make3(v.x, v.y, v.z);
+}
+
+MBD f2 uvat(const DLod& l, uint32_t i) { return ldg2(l.uvs + 2 * size_t(i)); }
+MBD f2 bilerp2(f2 x00, f2 x10, f2 x01, f2 x11, float s, float t) {
+	const f2 a = (1.0f - s) * x00 + s * x10;
+	const f2 b = (1.0f - s) * x01 + s * x11;
+	return (1.0f - t) * a + t * b;
+}
+
+// Alpha test of intersection.cu:205-216, 235-262 and 276-302: the alpha
+// texture of primitive p's material, if it has one, cuts the surface where
+// its first channel is below 0.5. `sp` is the hit's barycentric (triangles)
+// or bilinear (quads) parametrisation; spheres take the object-space hit
+// point (o + t d) instead.
+// The scene's materials and textures when the alpha test applies, else
+// materials == nullptr. (Passed instead of the scene itself: taking the
+// address of a kernel-parameter scene would copy it to local memory.)
+struct AlphaCtx {
+	const DMaterial* materials;
+	const DTexture* textures;
+	MBD bool on() const { return materials != nullptr; }
+};
+MBD AlphaCtx alpha_ctx(const DScene& S, bool enable = true) {
+	AlphaCtx a;
+	a.materials = enable && S.hasAlpha ? S.materials : nullptr;
+	a.textures = S.textures;
+	return a;
+}
+MBD int alpha_texture(const AlphaCtx& A, const DLod& l, int p) {
+	const uint32_t faces = l.numTriangles + l.numQuads;
+	const uint16_t m = uint32_t(p) < faces ? __ldg(l.faceMaterials + p) : __ldg(l.sphereMaterials + (uint32_t(p) - faces));
+	return A.materials[m].alphaTex;
+}
+MBD bool alpha_cut_at(const AlphaCtx& A, int tex, f2 uv) { return sample_texture(A.textures[tex], uv).x < 0.5f; }
+MBD f2 tri_uv(const DLod& l, int p, f2 b) {
+	const uint32_t o3 = uint32_t(p) * 3;
+	const f2 t0 = uvat(l, __ldg(l.indices + o3)), t1 = uvat(l, __ldg(l.indices + o3 + 1)), t2 = uvat(l, __ldg(l.indices + o3 + 2));
+	return (t0 * b.x + t1 * b.y) + t2 * ((1.0f - b.x) - b.y);
+}
+MBD f2 quad_uv(const DLod& l, int p, f2 b) {
+	const uint32_t o4 = uint32_t(p - int(l.numTriangles)) * 4 + l.numTriangles * 3;
+	const f2 t0 = uvat(l, __ldg(l.indices + o4)), t1 = uvat(l, __ldg(l.indices + o4 + 1));
+	const f2 t2 = uvat(l, __ldg(l.indices + o4 + 2)), t3 = uvat(l, __ldg(l.indices + o4 + 3));
+	return bilerp2(t0, t1, t3, t2, b.x, b.y);
+}
+MBD f2 sphere_uv(f3 center, const FastRay& r, float t) {
+	const f3 n = normalize((r.o + t * r.d) - center);
+	return make2(__fdiv_rn(mbmath::atan2(n.z, n.x), 2.0f * PI) + 0.5f, __fdiv_rn(mbmath::acos(-n.y), PI));
+}
+// Triangle hits: true when the alpha texture cuts the hit (kept out of line;
+// only scenes with alpha textures call it).
+static __device__ __noinline__ bool alpha_cuts_triangle(AlphaCtx A, const DLod& l, int p, f2 bary) {
+	const int tex = alpha_texture(A, l, p);
+	return tex >= 0 && alpha_cut_at(A, tex, tri_uv(l, p, bary));
+}
+
 // Primitive test for leaf slot `slot` holding primitive `p` (object space).
-MBD bool prim_test(const DLod& l, const FastRay& r, int slot, int p, float& t, f2& sp) {
+// With alpha.on(), the alpha textures of its materials apply.
+MBD bool prim_test(const DLod& l, const FastRay& r, int slot, int p, float& t, f2& sp, AlphaCtx alpha = AlphaCtx{ nullptr, nullptr }) {
 	if(p < int(l.numTriangles)) {
 		const float4* s = l.triSoup + 3 * size_t(slot);
 		const float4 a = __ldg(s), b = __ldg(s + 1), c = __ldg(s + 2);
-		return tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, sp) && t > 0.0f;
+		if(!(tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, sp) && t > 0.0f)) return false;
+		return !(alpha.on() && alpha_cuts_triangle(alpha, l, p, sp));
 	}
+	const int tex = alpha.on() ? alpha_texture(alpha, l, p) : -1;
 	if(p < int(l.numTriangles + l.numQuads)) {
 		const uint32_t o = uint32_t(p - int(l.numTriangles)) * 4 + l.numTriangles * 3;
 		const uint32_t i0 = __ldg(l.indices + o), i1 = __ldg(l.indices + o + 1), i2 = __ldg(l.indices + o + 2), i3 = __ldg(l.indices + o + 3);
-		float t1;
-		f2 uv;
-		if(quad_test(vert(l, i0), vert(l, i1), vert(l, i2), vert(l, i3), r, t1, uv)) { t = t1; sp = uv; return true; }
-		return false;
+		float t1, t2;
+		f2 uv, uv2 = make2(0.0f, 0.0f);
+		if(!quad_test(vert(l, i0), vert(l, i1), vert(l, i2), vert(l, i3), r, t1, uv, t2, uv2)) return false;
+		if(tex >= 0 && alpha_cut_at(alpha, tex, quad_uv(l, p, uv))) {
+			// a cut-out first root: the other part of a non-planar quad
+			if(!(t2 > 0.0f) || alpha_cut_at(alpha, tex, quad_uv(l, p, uv2))) return false;
+			t1 = t2; uv = uv2;
+		}
+		t = t1; sp = uv;
+		return true;
 	}
 	const float4 s = __ldg(l.spheres + (p - int(l.numTriangles + l.numQuads)));
-	if(sphere_test(r, f4to3(s), s.w, t)) { sp = make2(0.0f, 0.0f); return true; }
-	return false;
+	float t2;
+	if(!sphere_test(r, f4to3(s), s.w, t, t2)) return false;
+	if(tex >= 0 && alpha_cut_at(alpha, tex, sphere_uv(f4to3(s), r, t))) {
+		// a cut-out near side: the far side seen through it
+		if(!(t2 > 0.0f) || alpha_cut_at(alpha, tex, sphere_uv(f4to3(s), r, t2))) return false;
+		t = t2;
+	}
+	sp = make2(0.0f, 0.0f);
+	return true;
 }
 
 MBD void add_epsilon(f3& o, f3 dir, f3 n) {
@@ -358,7 +447,7 @@ MBD void blas_closest(const DScene& S, uint32_t inst, f3 o, f3 d, HitRec& best, 
 		const int p = __ldg(l.primIds + slot);
 		float t; f2 sp;
 		++cnt.prims;
-		if(prim_test(l, ir.ray, slot, p, t, sp)) {
+		if(prim_test(l, ir.ray, slot, p, t, sp, alpha_ctx(S))) {
 			const float tw = __fdiv_rn(t, ir.scale);
 			if(better(tw, int(inst), p, best)) { best.t = tw; best.inst = int(inst); best.prim = p; best.sp = sp; best.has = true; }
 		}
@@ -387,7 +476,7 @@ MBD bool blas_any(const DScene& S, uint32_t inst, f3 o, f3 d, float tmaxWorld, L
 		const int p = __ldg(l.primIds + slot);
 		float t; f2 sp;
 		++cnt.prims;
-		return prim_test(l, ir.ray, slot, p, t, sp) && t < tmaxObj;
+		return prim_test(l, ir.ray, slot, p, t, sp, alpha_ctx(S)) && t < tmaxObj;
 	};
 	if(l.numPrims == 1) return test(0);
 	traverse(l.nodes, l.numInternal, ir.ray,
@@ -408,18 +497,12 @@ struct Intersection {
 	f2 sp;
 };
 
-MBD f2 bilerp2(f2 x00, f2 x10, f2 x01, f2 x11, float s, float t) {
-	const f2 a = (1.0f - s) * x00 + s * x10;
-	const f2 b = (1.0f - s) * x01 + s * x11;
-	return (1.0f - t) * a + t * b;
-}
 MBD f3 bilerp3(f3 x00, f3 x10, f3 x01, f3 x11, float s, float t) {
 	const f3 a = (1.0f - s) * x00 + s * x10;
 	const f3 b = (1.0f - s) * x01 + s * x11;
 	return (1.0f - t) * a + t * b;
 }
 
-MBD f2 uvat(const DLod& l, uint32_t i) { return ldg2(l.uvs + 2 * size_t(i)); }
 MBD f3 nrmat(const DLod& l, uint32_t i) { return ldg3(l.normals + 3 * size_t(i)); }
 
 // Closest hit of a world-space ray whose origin is already offset

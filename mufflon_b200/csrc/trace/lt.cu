@@ -159,6 +159,7 @@ static __device__ __noinline__ bool lt_walk(const DScene& S, Photon& ph, f3& ori
 // threads (80 registers, some spilled to L1) measured fastest on the 1080p
 // headline scene: 616 Mrays/s against 588 with 5 blocks, 559 with 4, and 3
 // blocks without spills slower still.
+template < int AM >
 __global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P, const LtTargets T,
                                             unsigned int* workCounter, TraceCounters* counters) {
 	LocalStack stack;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P,
 		if(trace) {
 			++cnt.rays;
 			if(shadow) ++cnt.shadow;
-			WideTracer t;
+			WideTracerT<AM> t;
 			t.init(S, ro, rd, tmax, shadow, cnt);
 			while(!t.step(S, cnt, stack)) {}
 			if(shadow) {
@@ -280,7 +281,11 @@ int lt_blocks() {
 		int dev = 0, sms = 148, perSm = 0;
 		cudaGetDevice(&dev);
 		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_lt, 128, 0);
+		// both variants (scenes with and without alpha textures) fit as many blocks
+		int perSmAlpha = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_lt<ALPHA_NEVER>, 128, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmAlpha, k_lt<ALPHA_ALWAYS>, 128, 0);
+		if(perSmAlpha > perSm) perSm = perSmAlpha;
 		blocks = sms * (perSm > 0 ? perSm : 1);
 	}
 	return blocks;
@@ -301,7 +306,9 @@ cudaError_t launch_lt(const DScene& S, const LtParams& P, const LtTargets& T, un
 		if((e = cudaMemsetAsync(T.recValue, 0, slots * 5 * sizeof(float), stream)) != cudaSuccess) return e;
 	}
 	if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-	k_lt<<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
+	// the variant for the scene: alpha textures or none (no alpha code in the loop)
+	if(S.hasAlpha) k_lt<ALPHA_ALWAYS><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
+	else k_lt<ALPHA_NEVER><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_lt_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
 	return cudaGetLastError();

@@ -58,6 +58,7 @@ struct DMaterial {
 	float radiance[3];            // emission * scale
 	int32_t albedoTex;            // -1: constant albedo
 	int32_t shadowing;            // Torrance: SHADOW_VCAVITY or SHADOW_SMITH
+	int32_t alphaTex;             // -1: opaque; else the alpha texture (first channel < 0.5 cuts)
 };
 
 struct DTexture {
@@ -126,6 +127,7 @@ struct DScene {
 	float bgColor[3], bgScale[3];
 	float aabbMin[3], aabbMax[3];
 	DCamera camera;
+	int32_t hasAlpha;             // some material has an alpha texture
 	// Traversal steps a ray may take (per traversal loop of the binary
 	// hierarchies, per ray of the 8-wide ones) before it is abandoned and
 	// counted as an error; MAX_TRAVERSAL_STEPS unless the renderer parameter

@@ -14,15 +14,6 @@ namespace mb {
 
 struct Params { int type; f3 albedo; f2 roughness; f3 radiance; int shadowing; };
 
-MBD f3 sample_texture(const DTexture& t, f2 uv) {
-	const float fx = uv.x - floorf(uv.x), fy = uv.y - floorf(uv.y);
-	int x = int(fx * float(t.width)), y = int(fy * float(t.height));
-	if(x >= int(t.width)) x = int(t.width) - 1;
-	if(y >= int(t.height)) y = int(t.height) - 1;
-	const float4 v = __ldg(t.texels + size_t(y) * t.width + x);
-	return make3(v.x, v.y, v.z);
-}
-
 MBD Params fetch_material(const DScene& S, uint16_t idx, f2 uv) {
 	const DMaterial& m = S.materials[idx];
 	Params p;

@@ -321,7 +321,7 @@ MBD void stats_add(BlockStats& b, int kind, const C& c) {
 // Every loop iteration runs one traversal step in every busy lane.
 // Queue entries are read and written with streaming (evict-first) accesses so
 // that they do not displace the hierarchies from L2.
-template < int MINB, class SP, class C >
+template < int MINB, class SP, class C, int AM >
 __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int q, int neeCount, int workIdx,
                                                      TraceCounters* counters, int refillLanes, int bounce) {
 	__shared__ BlockStats stats;
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(128, MINB) k_trace(const SP sp, WfState W, int
 	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + q);
 	const unsigned nGroups = *reinterpret_cast<volatile unsigned*>(W.counters + C_SHADOW0 + (q ^ 1)) / unsigned(neeCount);
 	const unsigned total = nExt + nGroups;
-	WideTracer t;
+	WideTracerT<AM> t;
 	bool active = false, exhausted = false;
 	unsigned item = 0;
 	unsigned ent = 0;      // the item's extension-queue slot or shadow-ray group
@@ -714,7 +714,7 @@ __global__ void __launch_bounds__(128, 8) k_shade(const SP sp, WfState W, int q,
 // of the loop traces at most one ray per lane (a shadow ray or the next
 // extension ray) in one traversal loop shared by the warp. A path's random
 // numbers, terms and their order are those of shade_vertex.
-template < int MINB, class SP, class C >
+template < int MINB, class SP, class C, int AM >
 __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int q, int bounce,
                                                     int workIdx, TraceCounters* counters, unsigned tailMax) {
 	__shared__ BlockStats stats;
@@ -809,7 +809,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 		if(!trace) continue;
 		const DScene& S = sp.scene(p);
 		C cnt;
-		WideTracer t;
+		WideTracerT<AM> t;
 		t.init(S, ro, rd, tmax, shadow, cnt);
 		while(!t.step(S, cnt, stack)) {}
 		stats_add(stats, shadow ? 1 : 0, cnt);
@@ -1108,16 +1108,21 @@ template < class SP > struct TraceKernel {
 // The trace kernel compiled for `perSm` resident blocks of 128 threads
 // (register budget 65536 / (128 * perSm)); other values pick 6. With
 // `counting`, the variant that counts node visits, primitive tests and
-// instance entries per ray kind.
-template < class SP > TraceKernel<SP> trace_kernel(int perSm, bool counting) {
-	static TraceKernel<SP> table[2][4] = {};
-	static const typename TraceKernel<SP>::Fn fns[2][4] = {
-		{ k_trace<4, SP, NoCounters>, k_trace<5, SP, NoCounters>, k_trace<6, SP, NoCounters>, k_trace<8, SP, NoCounters> },
-		{ k_trace<4, SP, LocalCounters>, k_trace<5, SP, LocalCounters>, k_trace<6, SP, LocalCounters>, k_trace<8, SP, LocalCounters> } };
+// instance entries per ray kind (it decides on alpha textures per step);
+// otherwise the variant for scenes with (`alpha`) or without alpha textures.
+template < class SP > TraceKernel<SP> trace_kernel(int perSm, bool counting, bool alpha) {
+	static TraceKernel<SP> table[3][4] = {};
+	static const typename TraceKernel<SP>::Fn fns[3][4] = {
+		{ k_trace<4, SP, NoCounters, ALPHA_NEVER>, k_trace<5, SP, NoCounters, ALPHA_NEVER>,
+		  k_trace<6, SP, NoCounters, ALPHA_NEVER>, k_trace<8, SP, NoCounters, ALPHA_NEVER> },
+		{ k_trace<4, SP, NoCounters, ALPHA_ALWAYS>, k_trace<5, SP, NoCounters, ALPHA_ALWAYS>,
+		  k_trace<6, SP, NoCounters, ALPHA_ALWAYS>, k_trace<8, SP, NoCounters, ALPHA_ALWAYS> },
+		{ k_trace<4, SP, LocalCounters, ALPHA_SCENE>, k_trace<5, SP, LocalCounters, ALPHA_SCENE>,
+		  k_trace<6, SP, LocalCounters, ALPHA_SCENE>, k_trace<8, SP, LocalCounters, ALPHA_SCENE> } };
 	static const int occ[4] = { 4, 5, 6, 8 };
 	int idx = 2;
 	for(int i = 0; i < 4; ++i) if(occ[i] == perSm) idx = i;
-	const int c = counting ? 1 : 0;
+	const int c = counting ? 2 : (alpha ? 1 : 0);
 	if(!table[c][idx].fn)
 		table[c][idx] = { fns[c][idx], persistent_blocks(reinterpret_cast<const void*>(fns[c][idx]), int(WF_BLOCK)) };
 	return table[c][idx];
@@ -1128,10 +1133,11 @@ template < class SP > struct TailKernel {
 	Fn fn;
 	int blocks;
 };
-template < class SP > TailKernel<SP> tail_kernel(bool counting) {
-	static TailKernel<SP> k[2] = {};
-	const typename TailKernel<SP>::Fn fn = counting ? k_tail<4, SP, LocalCounters> : k_tail<4, SP, NoCounters>;
-	const int c = counting ? 1 : 0;
+template < class SP > TailKernel<SP> tail_kernel(bool counting, bool alpha) {
+	static TailKernel<SP> k[3] = {};
+	const typename TailKernel<SP>::Fn fn = counting ? k_tail<4, SP, LocalCounters, ALPHA_SCENE>
+	                                     : alpha ? k_tail<4, SP, NoCounters, ALPHA_ALWAYS> : k_tail<4, SP, NoCounters, ALPHA_NEVER>;
+	const int c = counting ? 2 : (alpha ? 1 : 0);
 	if(!k[c].fn) k[c] = { fn, persistent_blocks(reinterpret_cast<const void*>(fn), int(WF_BLOCK)) };
 	return k[c];
 }
@@ -1159,7 +1165,7 @@ template < class SP >
 void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numPaths, int maxBounces, int neeCount,
                  const WfTuning& tuning, LaunchLog& log, cudaStream_t stream) {
 	const int refillLanes = tuning.refillLanes < 1 ? 1 : (tuning.refillLanes > 32 ? 32 : tuning.refillLanes);
-	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm, tuning.counters);
+	const TraceKernel<SP> tk = trace_kernel<SP>(tuning.traceBlocksPerSm, tuning.counters, tuning.alpha);
 	const unsigned workSlots = WF_COUNTERS - WF_BOUNCE_STATS - C_WORK;
 	static int sms = 0;
 	if(!sms) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev); }
@@ -1199,7 +1205,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 		if(tuning.tailBounce >= 0) {
 			// planned schedule: the tail takes over at tailBounce, nothing follows
 			if(b == tuning.tailBounce && b + 1 < maxBounces) {
-				const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters);
+				const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters, tuning.alpha);
 				log.begin(WF_TAIL);
 				tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, 0xFFFFFFFFu);
 				log.end();
@@ -1216,7 +1222,7 @@ void run_bounces(const SP& sp, WfState W, TraceCounters* counters, uint32_t numP
 		// device from the queue length); the later launches return at once.
 		const bool tailAllowed = b >= tuning.wavefrontBounces && b + 1 < maxBounces;
 		if(tailAllowed) {
-			const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters);
+			const TailKernel<SP> tl = tail_kernel<SP>(tuning.counters, tuning.alpha);
 			log.begin(WF_TAIL);
 			tl.fn<<<tl.blocks, WF_BLOCK, 0, stream>>>(sp, W, q, b, int(work++), counters, tailMax);
 			log.end();
@@ -1351,16 +1357,17 @@ cudaError_t launch_adjoint_wavefront(const DScene& S, const PtParams& P, uint64_
 	LaunchLog log{ none, stream };
 	WfTuning t = tuning;
 	t.tailBounce = -1;
+	t.alpha = S.hasAlpha != 0;
 	run_bounces(one, W, counters, n, maxBounces, neeCount, t, log, stream);
 	k_adjoint_scatter<<<grid, 128, 0, stream>>>(A);
 	return cudaGetLastError();
 }
 
 void prepare_batch_kernels(const WfTuning& tuning) {
-	(void)trace_kernel<JobScenes>(tuning.traceBlocksPerSm, tuning.counters);
-	(void)tail_kernel<JobScenes>(tuning.counters);
-	(void)trace_kernel<OneScene>(tuning.traceBlocksPerSm, tuning.counters);
-	(void)tail_kernel<OneScene>(tuning.counters);
+	(void)trace_kernel<JobScenes>(tuning.traceBlocksPerSm, tuning.counters, tuning.alpha);
+	(void)tail_kernel<JobScenes>(tuning.counters, tuning.alpha);
+	(void)trace_kernel<OneScene>(tuning.traceBlocksPerSm, tuning.counters, tuning.alpha);
+	(void)tail_kernel<OneScene>(tuning.counters, tuning.alpha);
 }
 
 cudaError_t launch_trace_rays_wide(const DScene& S, const float* rays, const float* geoNormals, float tmax, uint32_t n,
@@ -1404,7 +1411,9 @@ cudaError_t launch_pt_wavefront(const DScene& S, const PtParams& P, const Render
 	OneScene one;
 	one.S = S;
 	one.P = P;
-	run_bounces(one, W, counters, n, maxBounces, neeCount, tuning, log, stream);
+	WfTuning t = tuning;
+	t.alpha = S.hasAlpha != 0;
+	run_bounces(one, W, counters, n, maxBounces, neeCount, t, log, stream);
 	log.begin(WF_FINALIZE);
 	k_finalize<<<grid, 128, 0, stream>>>(W, R, n);
 	log.end();

@@ -83,6 +83,7 @@ struct WfTuning {
 	int sortDirBits = 3;       // (key bits in all, of them direction bits); 0 bits: trace in queue order
 	int sortGroupBits = 0;     // extra key bits above those for the path's group (batches: the job's scene)
 	bool counters = true;      // count node visits, primitive tests and instance entries (a slower kernel variant)
+	bool alpha = false;        // batches: some job's scene has alpha textures (single renders take it from the scene)
 };
 cudaError_t launch_pt_wavefront(const DScene& scene, const PtParams& params, const RenderState& state, WfState W,
                                 TraceCounters* counters, cudaStream_t stream, WfLaunchInfo* info,

@@ -64,6 +64,11 @@ static __device__ __noinline__ PrimHit other_prim_test(const DLod* l, FastRay r,
 	h.hit = prim_test(*l, r, 0, p, h.t, h.uv);
 	return h;
 }
+static __device__ __noinline__ PrimHit other_prim_test_alpha(const DLod* l, FastRay r, int p, AlphaCtx alpha) {
+	PrimHit h;
+	h.hit = prim_test(*l, r, 0, p, h.t, h.uv, alpha);
+	return h;
+}
 
 // Three-operand minimum and maximum of sm_100 (one instruction each; a NaN
 // operand is dropped like fminf/fmaxf drop it).
@@ -141,8 +146,14 @@ MBD void wide_node_test(const WideNode* nodes, uint32_t idx, const FastRay& r, u
 // most one node and that node's hit primitives (or enters / leaves an
 // instance), and returns true once the ray is finished. Kernels that refill
 // lanes as soon as their ray finishes call step() from one loop shared by the
-// whole warp.
-struct WideTracer {
+// whole warp. Alpha mode AM: ALPHA_NEVER, every surface is opaque (scenes
+// without alpha textures, and the wireframe renderer's
+// first_intersection<CURRENT_DEV, false>, wireframe_common.hpp:108);
+// ALPHA_ALWAYS, the materials' alpha textures apply (kernels launched for
+// scenes with alpha textures); ALPHA_SCENE, decided per step by the scene.
+enum AlphaMode { ALPHA_NEVER = 0, ALPHA_ALWAYS = 1, ALPHA_SCENE = 2 };
+template < int AM >
+struct WideTracerT {
 	FastRay wr;           // world ray, prepared (wr.o, wr.d: the ray as given)
 	FastRay r;            // ray of the current level
 	float scale;          // object-space length of a world-space unit
@@ -191,8 +202,22 @@ struct WideTracer {
 		instSp = sp;
 	}
 
+	// One step. The hot kernels are compiled once per alpha mode and launched
+	// with ALPHA_NEVER for scenes without alpha textures, so their step carries
+	// no alpha code (any alpha check in a step shared by both kinds of scenes
+	// made the trace stage 5-7 % slower: more registers spilled).
 	template < class Stack, class C >
 	MBD bool step(const DScene& S, C& cnt, Stack& stack) {
+		if constexpr(AM == ALPHA_SCENE) {
+			if(S.hasAlpha) return step_impl<true>(S, cnt, stack);
+			return step_impl<false>(S, cnt, stack);
+		} else {
+			return step_impl<AM == ALPHA_ALWAYS>(S, cnt, stack);
+		}
+	}
+
+	template < bool ALPHA, class Stack, class C >
+	MBD bool step_impl(const DScene& S, C& cnt, Stack& stack) {
 		if(done) return true;
 		if(--steps < 0) { ++cnt.errors; done = true; return true; }
 		if(ngHits) {
@@ -226,8 +251,9 @@ struct WideTracer {
 					bool hit;
 					if(uint32_t(p) < ntri) {
 						hit = tri_test(r, f4to3(a), f4to3(b), f4to3(c), t, uv) && t > 0.0f;
+						if(ALPHA && hit) hit = !alpha_cuts_triangle(alpha_ctx(S), *lod, p, uv);
 					} else {
-						const PrimHit ph = other_prim_test(lod, r, p);
+						const PrimHit ph = ALPHA ? other_prim_test_alpha(lod, r, p, alpha_ctx(S)) : other_prim_test(lod, r, p);
 						hit = ph.hit; t = ph.t; uv = ph.uv;
 					}
 					if(hit) {
@@ -270,11 +296,13 @@ struct WideTracer {
 
 };
 
+using WideTracer = WideTracerT<ALPHA_SCENE>;
+
 // Closest hit of a world-space ray whose origin is already offset.
-template < class Stack, class C >
+template < int AM = ALPHA_SCENE, class Stack, class C >
 MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, C& cnt, Stack& stack) {
 	++cnt.rays;
-	WideTracer t;
+	WideTracerT<AM> t;
 	t.init(S, o, dir, tmax, false, cnt);
 	while(!t.step(S, cnt, stack)) {}
 	return t.best;
@@ -284,7 +312,7 @@ MBD HitRec closest_hit_wide(const DScene& S, f3 o, f3 dir, float tmax, C& cnt, S
 template < class Stack, class C >
 MBD bool occluded_wide(const DScene& S, f3 a, f3 dir, float tmax, C& cnt, Stack& stack) {
 	++cnt.rays; ++cnt.shadow;
-	WideTracer t;
+	WideTracerT<ALPHA_SCENE> t;
 	t.init(S, a, dir, tmax, true, cnt);
 	while(!t.step(S, cnt, stack)) {}
 	return t.occluded;

@@ -64,7 +64,7 @@ __global__ void k_wireframe(const DScene S, const float* instToWorld, WireParams
 		float total = 0.0f;
 		float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 		for(int i = 0; i < P.maxTraceDepth; ++i) {
-			const HitRec hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
+			const HitRec hr = closest_hit_wide<ALPHA_NEVER>(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
 			if(!hr.has) {
 				// evaluate_background (light_sampling.hpp:467-471)
 				if(S.hasBackground) {

@@ -216,15 +216,20 @@ def write_pfm(path: str, rgb: np.ndarray) -> None:
         f.write(a.tobytes())
 
 
-def material_json(m, texture_file: Optional[str] = None) -> dict:
-    """JSON material of a MaterialSpec (types 0 Lambert, 1 Torrance GGX/Smith, 2 emissive)."""
+def material_json(m, texture_file: Optional[str] = None, alpha_file: Optional[str] = None) -> dict:
+    """JSON material of a MaterialSpec (types 0 Lambert, 1 Torrance GGX/Smith, 2 emissive), with its
+    alpha texture file if it has one."""
     if m.type == 0:
-        return {"type": "lambert", "albedo": texture_file or _floats(m.albedo)}
-    if m.type == 1:
-        return {"type": "torrance", "ndf": "GGX", "shadowingModel": "smith" if m.shadowing == 1 else "vcavity",
-                "roughness": _floats(m.roughness),
-                "albedo": texture_file or _floats(m.albedo)}
-    return {"type": "emissive", "radiance": _floats(m.radiance), "scale": _floats(m.scale)}
+        out = {"type": "lambert", "albedo": texture_file or _floats(m.albedo)}
+    elif m.type == 1:
+        out = {"type": "torrance", "ndf": "GGX", "shadowingModel": "smith" if m.shadowing == 1 else "vcavity",
+               "roughness": _floats(m.roughness),
+               "albedo": texture_file or _floats(m.albedo)}
+    else:
+        return {"type": "emissive", "radiance": _floats(m.radiance), "scale": _floats(m.scale)}
+    if alpha_file:
+        out["alpha"] = alpha_file
+    return out
 
 
 def write_json(path: str, document: dict) -> None:
@@ -262,7 +267,8 @@ def write_scene(spec, json_path: str, *, deflate: bool = False, compressed_norma
         name = f"{os.path.basename(base)}_tex{k}.pfm"
         write_pfm(os.path.join(directory, name), tex)
         tex_files[k] = name
-    materials = {mat_names[i]: material_json(m, tex_files.get(m.albedo_texture) if m.albedo_texture >= 0 else None)
+    materials = {mat_names[i]: material_json(m, tex_files.get(m.albedo_texture) if m.albedo_texture >= 0 else None,
+                                             tex_files.get(getattr(m, "alpha_texture", -1)))
                  for i, m in enumerate(spec.materials)}
     deg = math.degrees(spec.vfov)
     lights = {f"point{k}": {"type": "point", "position": _floats(pl[:3]), "intensity": _floats(pl[3:])}

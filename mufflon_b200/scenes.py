@@ -62,6 +62,7 @@ class MaterialSpec:
     albedo_texture: int = -1
     name: str = "material"
     shadowing: int = 1                  # Torrance: 1 Smith, 0 V-cavity (core_interface.h ShadowingModel)
+    alpha_texture: int = -1             # cut-out texture (first channel < 0.5 is transparent), -1: opaque
 
 
 @dataclasses.dataclass
@@ -414,6 +415,61 @@ def displaced_plane(seed: int = 0, n: int = 224, width: int = 512, height: int =
     return SceneSpec([lod], np.array([identity34()], np.float32), np.array([0], np.uint32), mats, lights,
                      ((0.2, 0.2, 0.25), (1.0, 1.0, 1.0)), (0.0, 4.0, 8.0), (0.0, -0.5, -1.0), (0.0, 1.0, 0.0),
                      math.radians(50.0), width, height, name="displaced_plane")
+
+
+def alpha_cutouts(seed: int = 0, width: int = 128, height: int = 128, background: bool = True) -> SceneSpec:
+    """The Cornell box with cut-out surfaces (materials with an alpha texture, MaterialParams.alpha): a
+    checkerboard quad panel, a strongly twisted (non-planar) quad, a triangle fence with stripes, and
+    striped spheres in two instances (one rotated and scaled). Every cut-out kind of the reference's
+    alpha test (intersection.cu:181-316) is hit, including the second root of quads and spheres."""
+    spec = cornell_box(seed, width, height)
+    rng = np.random.default_rng(seed + 101)
+    checker = np.zeros((8, 8, 4), np.float32)
+    checker[..., 0] = (np.add.outer(np.arange(8), np.arange(8)) % 2).astype(np.float32)
+    stripes = np.zeros((1, 12, 4), np.float32)
+    stripes[0, :, 0] = (np.arange(12) % 3 != 0).astype(np.float32) * 0.9
+    spec.textures = [checker, stripes]
+    base = len(spec.materials)
+    spec.materials += [
+        MaterialSpec(MAT_LAMBERT, albedo=tuple(float(x) for x in rng.uniform(0.3, 0.9, 3)), alpha_texture=0, name="panel"),
+        MaterialSpec(MAT_TORRANCE, albedo=(0.8, 0.7, 0.5), roughness=(0.3, 0.3), alpha_texture=1, name="striped_glossy"),
+        MaterialSpec(MAT_LAMBERT, albedo=(0.3, 0.6, 0.8), alpha_texture=1, name="fence"),
+    ]
+    uv4 = np.array([(0, 0), (1, 0), (1, 1), (0, 1)], np.float32)
+    # checkerboard panel and a twisted quad
+    pp, pn = _quad((-0.6, -0.7, 0.1), (0.6, -0.7, 0.1), (0.6, 0.5, 0.1), (-0.6, 0.5, 0.1))
+    tw = np.array([(-0.9, 0.55, -0.6), (-0.1, 0.55, -0.2), (-0.1, 0.95, -0.9), (-0.9, 0.95, 0.2)], np.float32)
+    tn = np.tile(np.array([0, 0, 1], np.float32), (4, 1))
+    spec.lods.append(_lod(np.concatenate([pp, tw]), np.concatenate([pn, tn]), np.concatenate([uv4, uv4 * 3.0]),
+                          quads=np.arange(8, dtype=np.uint32).reshape(2, 4),
+                          mats=np.array([base, base], np.uint16), name="panels"))
+    # triangle fence: 4 x 3 cells, two triangles each, uv along x
+    nx, ny = 4, 3
+    xs, ys = np.linspace(-0.9, 0.9, nx + 1), np.linspace(-1.0, -0.2, ny + 1)
+    gv = np.array([(x, y, 0.55) for y in ys for x in xs], np.float32)
+    guv = np.array([(4.0 * i / nx, j / ny) for j in range(ny + 1) for i in range(nx + 1)], np.float32)
+    tris = []
+    for j in range(ny):
+        for i in range(nx):
+            a0 = j * (nx + 1) + i
+            tris += [(a0, a0 + 1, a0 + nx + 2), (a0, a0 + nx + 2, a0 + nx + 1)]
+    spec.lods.append(_lod(gv, np.tile(np.array([0, 0, 1], np.float32), (len(gv), 1)), guv, tris=tris,
+                          mats=np.full(len(tris), base + 2, np.uint16), name="fence"))
+    # striped spheres, the object in two instances
+    sph = np.array([(0.45, -0.55, -0.2, 0.3), (-0.5, -0.6, 0.35, 0.22), (0.2, 0.3, -0.4, 0.18)], np.float32)
+    spec.lods.append(_lod(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros((0, 2), np.float32),
+                          spheres=sph, sphere_mats=np.full(3, base + 1, np.uint16), name="spheres"))
+    yaw = 0.7
+    rot = np.array([[math.cos(yaw), 0, math.sin(yaw)], [0, 1, 0], [-math.sin(yaw), 0, math.cos(yaw)]])
+    spec.world_to_instance = np.concatenate([spec.world_to_instance,
+                                             np.array([identity34(), identity34(), identity34(),
+                                                       _w2i_from_rt(rot, (0.1, 0.35, 0.3), 0.6)], np.float32)])
+    n = len(spec.lods)
+    spec.instance_lod = np.concatenate([spec.instance_lod, np.array([n - 3, n - 2, n - 1, n - 1], np.uint32)])
+    if background:
+        spec.background = ((0.2, 0.25, 0.3), (1.0, 1.0, 1.0))
+    spec.name = "alpha_cutouts"
+    return spec
 
 
 def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: int = 16, num_point_lights: int = 1,

@@ -290,6 +290,28 @@ inline u64 morton63(V3 p, Box bb) {
 	return part_by_two21(disc(n.x)) * 4 + part_by_two21(disc(n.y)) * 2 + part_by_two21(disc(n.z));
 }
 
+// sfcurves.hpp:37-46: spreads 10 bits to every third bit (multiply-and-mask form)
+inline u32 part_by_two10(u32 x) {
+	u32 r = x;
+	r = (r * 0x00010001u) & 0xFF0000FFu;
+	r = (r * 0x00000101u) & 0x0F00F00Fu;
+	r = (r * 0x00000011u) & 0xC30C30C3u;
+	r = (r * 0x00000005u) & 0x49249249u;
+	return r;
+}
+// build_lbvh.cu:59-69, 81-86: the 30-bit code of a point (the reference builds
+// every hierarchy with the 63-bit code; this one is kept as its alternative)
+inline u32 morton30(V3 p, Box bb) {
+	V3 span = bb.mx - bb.mn;
+	V3 n = sdiv(p - bb.mn, span);
+	auto disc = [](float v) {
+		float x = v * 1024.0f;
+		x = std::fmin(std::fmax(x, 0.0f), 1023.0f);
+		return u32(x);
+	};
+	return part_by_two10(disc(n.x)) * 4u + part_by_two10(disc(n.y)) * 2u + part_by_two10(disc(n.z));
+}
+
 // ---------------------------------------------------------------- scene
 struct Lod {
 	u32 nV = 0, nT = 0, nQ = 0, nS = 0;
@@ -321,6 +343,7 @@ struct Material {
 	i32 shadowing, ndf;
 	V3 radiance, scale;
 	i32 albedoTex;
+	i32 alphaTex = -1; // cut-out texture (intersection.cu:205-216), -1: opaque
 };
 
 struct Texture { u32 w, h; std::vector<float> texels; };
@@ -370,6 +393,7 @@ struct Counters {
 };
 
 struct Scene {
+	bool hasAlpha = false; // some material has an alpha texture
 	std::vector<Lod> lods;
 	std::vector<Bvh> lodBvh;
 	std::vector<Mat34> w2i;
@@ -429,6 +453,7 @@ struct BuildDesc {
 	const Lod* lod;
 	i32 numPrims;
 	Box bb;
+	i32 mortonBits = 63;        // 63 (u64 keys, the reference's choice) or 30 (u32 keys)
 	std::vector<Box> instBoxes; // scene only
 	std::vector<V3> instCentroids;
 };
@@ -456,17 +481,22 @@ inline bool count_limit(const BuildDesc& d, Counts c) {
 	return c.c[0] >= 1023 || c.c[1] >= 1023 || c.c[2] >= 1023;
 }
 
-// build_lbvh.cu:164-178
-inline i32 lcp(const std::vector<u64>& k, i32 n, i32 i1, i32 i2, u64 key1) {
+// build_lbvh.cu:164-178, for u64 and u32 keys (sizeof(Key) * 8 + clz of the
+// index difference for equal keys)
+inline int clz_key(u64 v) { return clz64(v); }
+inline int clz_key(u32 v) { return clz32(v); }
+template < class Key >
+inline i32 lcp(const std::vector<Key>& k, i32 n, i32 i1, i32 i2, Key key1) {
 	if(i2 < 0 || i2 >= n) return -1;
-	const u64 key2 = k[i2];
-	if(key1 == key2) return 64 + clz32(u32(i1 ^ i2));
-	return clz64(key1 ^ key2);
+	const Key key2 = k[i2];
+	if(key1 == key2) return i32(sizeof(Key) * 8) + clz32(u32(i1 ^ i2));
+	return clz_key(Key(key1 ^ key2));
 }
 
 // build_lbvh.cu:180-245
-void karras_node(const std::vector<u64>& keys, i32 n, std::vector<i32>& parents, i32 idx) {
-	const u64 key1 = keys[idx];
+template < class Key >
+void karras_node(const std::vector<Key>& keys, i32 n, std::vector<i32>& parents, i32 idx) {
+	const Key key1 = keys[idx];
 	const i32 lcp1 = lcp(keys, n, idx, idx + 1, key1);
 	const i32 lcp2 = lcp(keys, n, idx, idx - 1, key1);
 	const i32 direction = (lcp1 - lcp2) < 0 ? -1 : 1;
@@ -511,25 +541,39 @@ void build_lbvh(const BuildDesc& d, i32 numPrimitives, i32 actualPrimCount, Bvh&
 	const i32 numNodes = numInternal + used;
 
 	// Morton codes (build_lbvh.cu:96-108)
-	std::vector<std::pair<u64, i32>> kv(numPrimitives);
-	for(i32 i = 0; i < numPrimitives; ++i) {
-		u64 code;
-		if(d.isScene) {
-			if(d.scene->instLod[i] == 0xFFFFFFFFu) code = ~0ull;
-			else code = morton63(d.instCentroids[i], d.bb);
-		} else {
-			code = morton63(lod_centroid(*d.lod, i), d.bb);
-		}
-		kv[i] = { code, i };
-	}
-	std::stable_sort(kv.begin(), kv.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
 	out.mortonSorted.resize(numPrimitives);
 	out.primIds.resize(numPrimitives);
-	for(i32 i = 0; i < numPrimitives; ++i) { out.mortonSorted[i] = kv[i].first; out.primIds[i] = kv[i].second; }
-
-	// Karras hierarchy
 	out.parents.assign(numNodes, 0);
-	for(i32 i = 0; i < numInternal; ++i) karras_node(out.mortonSorted, used, out.parents, i);
+	if(d.mortonBits == 30) {
+		// 30-bit codes in u32 keys: sorted, then the Karras hierarchy on u32 keys
+		std::vector<std::pair<u32, i32>> kv(numPrimitives);
+		for(i32 i = 0; i < numPrimitives; ++i) {
+			u32 code;
+			if(d.isScene) code = d.scene->instLod[i] == 0xFFFFFFFFu ? ~0u : morton30(d.instCentroids[i], d.bb);
+			else code = morton30(lod_centroid(*d.lod, i), d.bb);
+			kv[i] = { code, i };
+		}
+		std::stable_sort(kv.begin(), kv.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+		std::vector<u32> keys(numPrimitives);
+		for(i32 i = 0; i < numPrimitives; ++i) { keys[i] = kv[i].first; out.mortonSorted[i] = kv[i].first; out.primIds[i] = kv[i].second; }
+		for(i32 i = 0; i < numInternal; ++i) karras_node(keys, used, out.parents, i);
+	} else {
+		std::vector<std::pair<u64, i32>> kv(numPrimitives);
+		for(i32 i = 0; i < numPrimitives; ++i) {
+			u64 code;
+			if(d.isScene) {
+				if(d.scene->instLod[i] == 0xFFFFFFFFu) code = ~0ull;
+				else code = morton63(d.instCentroids[i], d.bb);
+			} else {
+				code = morton63(lod_centroid(*d.lod, i), d.bb);
+			}
+			kv[i] = { code, i };
+		}
+		std::stable_sort(kv.begin(), kv.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+		for(i32 i = 0; i < numPrimitives; ++i) { out.mortonSorted[i] = kv[i].first; out.primIds[i] = kv[i].second; }
+		// Karras hierarchy
+		for(i32 i = 0; i < numInternal; ++i) karras_node(out.mortonSorted, used, out.parents, i);
+	}
 
 	// Children from the parent links (root: node 0)
 	std::vector<i32> leftChild(numInternal, -1), rightChild(numInternal, -1);
@@ -786,8 +830,9 @@ bool quad_test(V3 p00, V3 p10, V3 p11, V3 p01, const FastRay& ray, float& resT1,
 	return false;
 }
 
-// Ray/sphere: nearest root with t > 0.
-inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t) {
+// Ray/sphere: nearest root with t > 0; t2 is the far root when t is the near
+// one (the alpha test's fallback), else -1.
+inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t, float& t2) {
 	const V3 oc = r.o - c;
 	const float b = dot(oc, r.d);
 	const float cc = dot(oc, oc) - rad * rad;
@@ -797,34 +842,92 @@ inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t) {
 	float x0, x1;
 	if(q == 0.0f) { x0 = x1 = 0.0f; }
 	else { x0 = q; x1 = cc / q; if(x0 > x1) std::swap(x0, x1); }
-	if(x0 > 0.0f) { t = x0; return true; }
-	if(x1 > 0.0f) { t = x1; return true; }
+	if(x0 > 0.0f) { t = x0; t2 = x1; return true; }
+	if(x1 > 0.0f) { t = x1; t2 = -1.0f; return true; }
 	return false;
+}
+inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t) {
+	float t2;
+	return sphere_test(r, c, rad, t, t2);
+}
+
+inline V3 sample_texture(const Texture& t, V2 uv) {
+	// nearest sampling with wrap-around
+	float fx = uv.x - std::floor(uv.x), fy = uv.y - std::floor(uv.y);
+	i32 x = i32(fx * float(t.w)), y = i32(fy * float(t.h));
+	if(x >= i32(t.w)) x = i32(t.w) - 1;
+	if(y >= i32(t.h)) y = i32(t.h) - 1;
+	const float* p = &t.texels[(size_t(y) * t.w + x) * 4];
+	return { p[0], p[1], p[2] };
+}
+
+inline V2 bilerp2(V2 x00, V2 x10, V2 x01, V2 x11, float s, float t) {
+	const V2 a = (1.0f - s) * x00 + s * x10;
+	const V2 b = (1.0f - s) * x01 + s * x11;
+	return (1.0f - t) * a + t * b;
+}
+
+// Alpha test (intersection.cu:205-216, 235-262, 276-302): the alpha texture of
+// primitive p's material, if any, cuts the surface where its first channel is
+// below 0.5; uv from the hit's barycentric / bilinear parametrisation, for
+// spheres from the object-space hit point.
+inline i32 alpha_texture(const Scene& S, const Lod& l, i32 p) {
+	const u32 faces = l.nT + l.nQ;
+	const u16 m = u32(p) < faces ? l.faceMat[size_t(p)] : l.sphereMat[size_t(u32(p) - faces)];
+	return S.materials[m].alphaTex;
+}
+inline bool alpha_cut_at(const Scene& S, i32 tex, V2 uv) { return sample_texture(S.textures[size_t(tex)], uv).x < 0.5f; }
+inline V2 quad_uv(const Lod& l, i32 p, V2 b) {
+	const u32 o = u32(p - i32(l.nT)) * 4 + l.nT * 3;
+	return bilerp2(l.uvs[l.idx[o]], l.uvs[l.idx[o + 1]], l.uvs[l.idx[o + 3]], l.uvs[l.idx[o + 2]], b.x, b.y);
+}
+inline V2 sphere_uv(V3 center, const FastRay& r, float t) {
+	const V3 n = normalize((r.o + t * r.d) - center);
+	return { mbmath::atan2(n.z, n.x) / (2.0f * PI) + 0.5f, mbmath::acos(-n.y) / PI };
 }
 
 // Primitive test in object space: returns the object-space t (> 0) and the
-// surface parametrisation. intersection.cu:181-316 without the alpha test.
-inline bool prim_test(const Lod& l, const FastRay& r, i32 p, float& t, V2& sp, Counters& cnt) {
+// surface parametrisation (intersection.cu:181-316); with `alphaS`, the alpha
+// textures of its materials apply, falling back to the second root of a quad
+// or sphere whose first root is cut out.
+inline bool prim_test(const Lod& l, const FastRay& r, i32 p, float& t, V2& sp, Counters& cnt, const Scene* alphaS = nullptr) {
 	if(p < i32(l.nT)) {
 		++cnt.tri;
 		const u32 o = u32(p) * 3;
-		if(tri_test(r, l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], t, sp)) return t > 0.0f;
-		return false;
+		if(!(tri_test(r, l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], t, sp) && t > 0.0f)) return false;
+		if(alphaS) {
+			const i32 tex = alpha_texture(*alphaS, l, p);
+			if(tex >= 0) {
+				const V2 uv = (l.uvs[l.idx[o]] * sp.x + l.uvs[l.idx[o + 1]] * sp.y) + l.uvs[l.idx[o + 2]] * ((1.0f - sp.x) - sp.y);
+				if(alpha_cut_at(*alphaS, tex, uv)) return false;
+			}
+		}
+		return true;
 	}
+	const i32 tex = alphaS ? alpha_texture(*alphaS, l, p) : -1;
 	if(p < i32(l.nT + l.nQ)) {
 		++cnt.quad;
 		const u32 o = u32(p - i32(l.nT)) * 4 + l.nT * 3;
-		float t1, t2; V2 b1, b2;
-		if(quad_test(l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], l.verts[l.idx[o + 3]], r, t1, t2, b1, b2)) {
-			t = t1; sp = b1;
-			return true;
+		float t1, t2; V2 b1, b2 = { 0, 0 };
+		if(!quad_test(l.verts[l.idx[o]], l.verts[l.idx[o + 1]], l.verts[l.idx[o + 2]], l.verts[l.idx[o + 3]], r, t1, t2, b1, b2))
+			return false;
+		if(tex >= 0 && alpha_cut_at(*alphaS, tex, quad_uv(l, p, b1))) {
+			if(!(t2 > 0.0f) || alpha_cut_at(*alphaS, tex, quad_uv(l, p, b2))) return false;
+			t1 = t2; b1 = b2;
 		}
-		return false;
+		t = t1; sp = b1;
+		return true;
 	}
 	++cnt.sphere;
 	const i32 s = p - i32(l.nT + l.nQ);
-	if(sphere_test(r, sphere_center(l, s), sphere_radius(l, s), t)) { sp = { 0, 0 }; return true; }
-	return false;
+	float t2;
+	if(!sphere_test(r, sphere_center(l, s), sphere_radius(l, s), t, t2)) return false;
+	if(tex >= 0 && alpha_cut_at(*alphaS, tex, sphere_uv(sphere_center(l, s), r, t))) {
+		if(!(t2 > 0.0f) || alpha_cut_at(*alphaS, tex, sphere_uv(sphere_center(l, s), r, t2))) return false;
+		t = t2;
+	}
+	sp = { 0, 0 };
+	return true;
 }
 
 inline void add_epsilon(V3& o, V3 dir, V3 n) {
@@ -860,12 +963,13 @@ inline bool better(float tw, i32 inst, i32 prim, const HitRec& h) {
 // BVH traversal inside one instance (closest hit). The stack discipline is
 // the reference's (near child first, far child pushed); the result is order
 // independent because of the (t, inst, prim) ordering.
-void blas_closest(const Scene& S, u32 inst, const InstRay& ir, HitRec& best, Counters& cnt) {
+void blas_closest(const Scene& S, u32 inst, const InstRay& ir, HitRec& best, Counters& cnt, bool alphaTest = true) {
 	const Lod& l = S.lods[S.instLod[inst]];
 	const Bvh& bvh = S.lodBvh[S.instLod[inst]];
+	const Scene* alphaS = alphaTest && S.hasAlpha ? &S : nullptr;
 	auto consider = [&](i32 p) {
 		float t; V2 sp;
-		if(prim_test(l, ir.ray, p, t, sp, cnt)) {
+		if(prim_test(l, ir.ray, p, t, sp, cnt, alphaS)) {
 			const float tw = t / ir.scale;
 			if(better(tw, i32(inst), p, best)) best = { tw, i32(inst), p, sp, true };
 		}
@@ -920,7 +1024,7 @@ bool blas_any(const Scene& S, u32 inst, const InstRay& ir, float tmaxObj, Counte
 	const Bvh& bvh = S.lodBvh[S.instLod[inst]];
 	auto hits = [&](i32 p) {
 		float t; V2 sp;
-		return prim_test(l, ir.ray, p, t, sp, cnt) && t < tmaxObj;
+		return prim_test(l, ir.ray, p, t, sp, cnt, S.hasAlpha ? &S : nullptr) && t < tmaxObj;
 	};
 	if(l.numPrims <= 0) return false;
 	if(l.numPrims == 1) return hits(0);
@@ -1023,19 +1127,15 @@ struct Intersection {
 	V2 sp;
 };
 
-inline V2 bilerp2(V2 x00, V2 x10, V2 x01, V2 x11, float s, float t) {
-	const V2 a = (1.0f - s) * x00 + s * x10;
-	const V2 b = (1.0f - s) * x01 + s * x11;
-	return (1.0f - t) * a + t * b;
-}
 inline V3 bilerp3(V3 x00, V3 x10, V3 x01, V3 x11, float s, float t) {
 	const V3 a = (1.0f - s) * x00 + s * x10;
 	const V3 b = (1.0f - s) * x01 + s * x11;
 	return (1.0f - t) * a + t * b;
 }
 
-// intersection.cu:366-621
-Intersection first_intersection(const Scene& S, V3& origin, V3 dir, V3 geoN, float tmax, Counters& cnt) {
+// intersection.cu:366-621; alphaTest false: every surface opaque
+// (first_intersection<dev, false> of wireframe_common.hpp:108)
+Intersection first_intersection(const Scene& S, V3& origin, V3 dir, V3 geoN, float tmax, Counters& cnt, bool alphaTest = true) {
 	add_epsilon(origin, dir, geoN);
 	++cnt.rays;
 	const FastRay wr = make_ray(origin, dir);
@@ -1043,7 +1143,7 @@ Intersection first_intersection(const Scene& S, V3& origin, V3 dir, V3 geoN, flo
 	bool stop;
 	tlas_visit(S, wr, &best.t, [&](u32 inst) {
 		InstRay ir;
-		if(enter_instance(S, inst, origin, dir, best.t, ir, cnt)) blas_closest(S, inst, ir, best, cnt);
+		if(enter_instance(S, inst, origin, dir, best.t, ir, cnt)) blas_closest(S, inst, ir, best, cnt, alphaTest);
 	}, cnt, stop);
 	Intersection res;
 	res.distance = best.t;
@@ -1155,15 +1255,6 @@ TangentSpace tangent_space(const Scene& S, const Intersection& h) {
 // ---------------------------------------------------------------- materials
 struct Params { i32 type; V3 albedo; V2 roughness; V3 radiance; i32 shadowing; };
 
-inline V3 sample_texture(const Texture& t, V2 uv) {
-	// nearest sampling with wrap-around
-	float fx = uv.x - std::floor(uv.x), fy = uv.y - std::floor(uv.y);
-	i32 x = i32(fx * float(t.w)), y = i32(fy * float(t.h));
-	if(x >= i32(t.w)) x = i32(t.w) - 1;
-	if(y >= i32(t.h)) y = i32(t.h) - 1;
-	const float* p = &t.texels[(size_t(y) * t.w + x) * 4];
-	return { p[0], p[1], p[2] };
-}
 
 inline Params fetch_material(const Scene& S, u16 matIdx, V2 uv) {
 	const Material& m = S.materials[matIdx];
@@ -2816,7 +2907,7 @@ V3 wireframe_sample(const WireState& st, i32 px, i32 py, Pcg64& rng, Counters& c
 	V3 origin = cam;
 	float total = 0.0f;
 	for(i32 i = 0; i < st.maxTraceDepth; ++i) {
-		const Intersection hit = first_intersection(S, origin, dir, V3{ 0, 0, 0 }, MAX_SCENE_SIZE, cnt);
+		const Intersection hit = first_intersection(S, origin, dir, V3{ 0, 0, 0 }, MAX_SCENE_SIZE, cnt, false);
 		if(hit.inst < 0) {
 			const LightTree& T = S.lightTree;
 			if(T.hasBackground) {
@@ -2897,6 +2988,8 @@ Scene* create_scene(const OrSceneDesc* d) {
 		mm.radiance = { m.radiance[0], m.radiance[1], m.radiance[2] };
 		mm.scale = { m.scale[0], m.scale[1], m.scale[2] };
 		mm.albedoTex = m.albedoTexture;
+		mm.alphaTex = m.alphaTexture;
+		S->hasAlpha = S->hasAlpha || m.alphaTexture >= 0;
 		S->materials.push_back(mm);
 	}
 	for(u32 i = 0; i < d->numTextures; ++i) {
@@ -3101,6 +3194,21 @@ int oracle_bvh_get(void* s, int32_t which, uint64_t* morton, int32_t* parents, f
 	if(parents && !b->parents.empty()) std::memcpy(parents, b->parents.data(), b->parents.size() * 4);
 	if(nodes && !b->nodes.empty()) std::memcpy(nodes, b->nodes.data(), b->nodes.size() * sizeof(BvhNode));
 	if(primIds && !b->primIds.empty()) std::memcpy(primIds, b->primIds.data(), b->primIds.size() * 4);
+	return 1;
+}
+
+// Rebuilds every LoD hierarchy of the scene with 63- or 30-bit Morton codes
+// (build_lbvh.cu:59-86); bvh(which) then returns those.
+int oracle_scene_rebuild_lod_bvhs(void* s, int32_t mortonBits) {
+	Scene* S = static_cast<Scene*>(s);
+	if(mortonBits != 63 && mortonBits != 30) return 0;
+	for(size_t i = 0; i < S->lods.size(); ++i) {
+		BuildDesc bd;
+		bd.isScene = false; bd.scene = S; bd.lod = &S->lods[i];
+		bd.numPrims = S->lods[i].numPrims; bd.bb = S->lods[i].aabb;
+		bd.mortonBits = mortonBits;
+		build_lbvh(bd, bd.numPrims, bd.numPrims, S->lodBvh[i]);
+	}
 	return 1;
 }
 
@@ -3471,6 +3579,7 @@ int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents) {
 uint64_t oracle_pcg64_seed(uint32_t seed) { return Pcg64::seeded(seed).state; }
 uint64_t oracle_pcg64_next(uint64_t* state) { Pcg64 r; r.state = *state; u64 v = r.next(); *state = r.state; return v; }
 uint64_t oracle_part_by_two21(uint32_t x) { return part_by_two21(x); }
+uint32_t oracle_part_by_two10(uint32_t x) { return part_by_two10(x); }
 uint64_t oracle_scramble_seed(uint32_t x) { return scramble_seed(x); }
 void oracle_golden_ratio2d(uint32_t seed, uint32_t n, uint64_t* out) {
 	u64 state = scramble_seed(seed);

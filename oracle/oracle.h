@@ -48,6 +48,7 @@ typedef struct {
 	float radiance[3];
 	float scale[3];
 	int32_t albedoTexture; /* index into the texture table or -1 */
+	int32_t alphaTexture;  /* cut-out texture (first channel < 0.5 is transparent) or -1 */
 } OrMaterial;
 
 typedef struct {
@@ -183,6 +184,9 @@ int oracle_karras(const uint64_t* keys, int32_t n, int32_t* parents);
 uint64_t oracle_pcg64_next(uint64_t* state);
 uint64_t oracle_pcg64_seed(uint32_t seed);
 uint64_t oracle_part_by_two21(uint32_t x);
+uint32_t oracle_part_by_two10(uint32_t x);
+/* Rebuilds the scene's LoD hierarchies with 63- or 30-bit Morton codes. */
+int oracle_scene_rebuild_lod_bvhs(void* scene, int32_t mortonBits);
 uint64_t oracle_scramble_seed(uint32_t x);
 /* The first n outputs of GoldenRatio2D(seed) (rng.hpp:119-140). */
 void oracle_golden_ratio2d(uint32_t seed, uint32_t n, uint64_t* out);

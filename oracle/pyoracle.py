@@ -26,7 +26,7 @@ class OrLod(C.Structure):
 class OrMaterial(C.Structure):
     _fields_ = [("type", C.c_int32), ("albedo", C.c_float * 3), ("roughness", C.c_float * 2),
                 ("shadowing", C.c_int32), ("ndf", C.c_int32), ("radiance", C.c_float * 3),
-                ("scale", C.c_float * 3), ("albedoTexture", C.c_int32)]
+                ("scale", C.c_float * 3), ("albedoTexture", C.c_int32), ("alphaTexture", C.c_int32)]
 
 
 class OrTexture(C.Structure):
@@ -121,6 +121,10 @@ def lib():
         L.oracle_pcg64_next.argtypes = [C.POINTER(C.c_uint64)]
         L.oracle_part_by_two21.restype = C.c_uint64
         L.oracle_part_by_two21.argtypes = [C.c_uint32]
+        L.oracle_part_by_two10.restype = C.c_uint32
+        L.oracle_part_by_two10.argtypes = [C.c_uint32]
+        L.oracle_scene_rebuild_lod_bvhs.restype = C.c_int
+        L.oracle_scene_rebuild_lod_bvhs.argtypes = [C.c_void_p, C.c_int32]
         L.oracle_scramble_seed.restype = C.c_uint64
         L.oracle_scramble_seed.argtypes = [C.c_uint32]
         L.oracle_golden_ratio2d.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p]
@@ -164,7 +168,8 @@ class OracleScene:
         for i, m in enumerate(spec.materials):
             mats[i] = OrMaterial(m.type, (C.c_float * 3)(*m.albedo), (C.c_float * 2)(*m.roughness),
                                  int(m.shadowing), 0,
-                                 (C.c_float * 3)(*m.radiance), (C.c_float * 3)(*m.scale), m.albedo_texture)
+                                 (C.c_float * 3)(*m.radiance), (C.c_float * 3)(*m.scale), m.albedo_texture,
+                                 getattr(m, "alpha_texture", -1))
         texs = (OrTexture * max(1, len(spec.textures)))()
         for i, t in enumerate(spec.textures):
             a = np.ascontiguousarray(t, np.float32)
@@ -226,6 +231,11 @@ class OracleScene:
         prim = np.zeros(max(n, 0), np.int32)
         L.oracle_bvh_get(self.handle, which, _ptr(morton), _ptr(parents), _ptr(nodes), _ptr(prim))
         return morton, parents, nodes, prim, ni.value
+
+    def rebuild_lod_bvhs(self, morton_bits: int):
+        """Rebuilds the LoD hierarchies with 63- or 30-bit Morton codes."""
+        if not lib().oracle_scene_rebuild_lod_bvhs(self.handle, morton_bits):
+            raise ValueError(f"Morton codes have 63 or 30 bits, not {morton_bits}")
 
     def aabb(self):
         a = np.zeros(6, np.float32)

@@ -113,7 +113,7 @@ def failure_files(tmp_path):
     yield variant(lambda x: x["materials"]["mat1"].update(type="torrance", ndf="BS", roughness=0.3)), ("GGX",)
     yield variant(lambda x: x["materials"]["mat0"].update(type="blend")), ("factorA",)
     yield variant(lambda x: x["materials"]["mat0"].update(type="glass")), ("'glass' is not supported",)
-    yield variant(lambda x: x["materials"]["mat0"].update(alpha="a.pfm")), ("alpha",)
+    yield variant(lambda x: x["materials"]["mat0"].update(alpha=[1, 2, 3])), ("alpha", "texture path")
     yield variant(lambda x: (x["lights"].update(spot={"type": "spot", "position": [0, 1, 0], "direction": [0, -1, 0],
                                                       "intensity": [1, 1, 1], "width": 0.5}),
                             x["scenarios"][scen]["lights"].append("spot"))), ("spot",)

@@ -65,6 +65,7 @@ def _specs():
                                        width=48, height=27),
         "tex": scenes.cornell_box_textured(2, 40, 40, texture=tex),
         "vcavity": _vcavity(scenes.displaced_icosphere(4, subdiv=3, width=40, height=24)),
+        "alpha": scenes.alpha_cutouts(2, 40, 40),
     }
 
 
@@ -74,7 +75,7 @@ def _vcavity(spec):
                                                 else m for m in spec.materials])
 
 
-@pytest.mark.parametrize("name", ["cornell", "ico", "inst", "tex", "vcavity"])
+@pytest.mark.parametrize("name", ["cornell", "ico", "inst", "tex", "vcavity", "alpha"])
 @pytest.mark.parametrize("deflate,packed", [(False, False), (True, False), (True, True)])
 def test_loaded_file_equals_api_built_scene(tmp_path, loader_dll, name, deflate, packed):
     spec = _specs()[name]

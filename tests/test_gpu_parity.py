@@ -95,6 +95,34 @@ def test_lbvh_bit_exact(dll, oracle, which):
     _compare_bvh(dll, oracle, lod)
 
 
+@pytest.mark.parametrize("which", ["walls", "random_5000", "mixed", "ico7", "ico8"])
+def test_lbvh_30bit_morton_bit_exact(dll, oracle, which):
+    """The reference's alternative 30-bit Morton code (build_lbvh.cu:59-69),
+    mufflon_lbvh_build_ex(mortonBits = 30): sorted codes, Karras parents,
+    collapsed nodes and primitive order equal to the oracle's build on 32-bit
+    keys, though the GPU keeps the codes in 64-bit keys and sorts 4 bytes."""
+    if which == "walls":
+        lod = scenes.cornell_box(0).lods[0]
+    elif which.startswith("random"):
+        lod = _random_tri_lod(int(which.split("_")[1]), 12)
+    elif which == "mixed":
+        lod = _mixed_lod(6)
+    else:
+        v, f = scenes.displaced_sphere_mesh(int(which[3:]), 2)
+        lod = scenes._lod(v, scenes.vertex_normals(v, f), scenes.spherical_uv(v), tris=f)
+    spec = scenes.SceneSpec([lod], np.array([scenes.identity34()]), np.array([0], np.uint32),
+                            [scenes.MaterialSpec(0)], np.zeros((0, 6), np.float32), None,
+                            (0, 0, 3), (0, 0, -1), (0, 1, 0), 0.8, 8, 8)
+    sc = oracle.OracleScene(spec)
+    sc.rebuild_lod_bvhs(30)
+    om, op, onodes, oprim, oni = sc.bvh(0)
+    gm, gp, gnodes, gprim, gni, _ = bindings.lbvh_build(dll, lod, morton_bits=30)
+    assert gm.max() < (1 << 30)
+    assert np.array_equal(gm, om) and np.array_equal(gp, op)
+    assert gni == oni and np.array_equal(gprim, oprim)
+    assert np.array_equal(gnodes.view(np.uint32), onodes.view(np.uint32))
+
+
 def test_lbvh_bit_exact_full_icosphere(dll, oracle):
     """The 1 310 720-triangle mesh of the 1080p workload."""
     spec = scenes.displaced_icosphere(0, subdiv=8, width=16, height=16)

@@ -94,3 +94,39 @@ def test_golden_cornell_regression(oracle):
     for _ in range(3):
         pt.iterate(2)
     assert np.array_equal(pt.target("Radiance"), g["radiance"])
+
+
+def _spread10(x):
+    """Bits of x (10 bits) moved to every third bit, computed bit by bit."""
+    return sum(((int(x) >> b) & 1) << (3 * b) for b in range(10))
+
+
+def test_thirty_bit_morton_codes_and_hierarchy(oracle):
+    """The reference's 30-bit code (build_lbvh.cu:59-69: 1024 cells per axis,
+    part_by_two10 of sfcurves.hpp:37-46), restated in the oracle: the sorted
+    codes are the codes computed here from the centroids, and the hierarchy
+    built on them (Karras emit on 32-bit keys) is valid."""
+    L = oracle.lib()
+    for x in (0, 1, 2, 5, 341, 682, 512, 777, 1023):
+        assert L.oracle_part_by_two10(x) == _spread10(x)
+    v, f = scenes.displaced_sphere_mesh(4, 3)
+    lod = scenes._lod(v, scenes.vertex_normals(v, f), scenes.spherical_uv(v), tris=f)
+    spec = scenes.SceneSpec([lod], np.array([scenes.identity34()]), np.array([0], np.uint32),
+                            [scenes.MaterialSpec(0)], np.zeros((0, 6), np.float32), None,
+                            (0, 0, 3), (0, 0, -1), (0, 1, 0), 0.8, 16, 16)
+    sc = oracle.OracleScene(spec)
+    m63 = sc.bvh(0)[0]
+    sc.rebuild_lod_bvhs(30)
+    morton, parents, nodes, prim, ni = sc.bvh(0)
+    assert morton.max() < (1 << 30) and np.all(np.diff(morton.astype(np.int64)) >= 0)
+    c = v[f].astype(np.float32).sum(1, dtype=np.float32) / np.float32(3.0)
+    lo, hi = v.min(0), v.max(0)
+    q = np.clip(np.floor((c - lo) / (hi - lo) * 1024.0), 0, 1023).astype(np.int64)
+    codes = np.array([_spread10(a) * 4 + _spread10(b) * 2 + _spread10(cz) for a, b, cz in q], np.uint64)
+    # the oracle's float path (sdiv, centroid order) may round a cell boundary differently: allow a few
+    assert np.mean(np.sort(codes) == morton) > 0.99
+    assert np.array_equal(np.sort(morton), morton)
+    assert not np.array_equal(morton, m63)
+    _check_bvh_invariants(nodes, prim, ni, lod.num_prims, _tri_boxes(lod))
+    with pytest.raises(ValueError):
+        sc.rebuild_lod_bvhs(32)

@@ -55,6 +55,7 @@ def test_golden_ratio2d(oracle, kat):
 def test_morton_spreads(oracle, kat):
     L = oracle.lib()
     assert [L.oracle_part_by_two21(x) for x in kat["x21"]] == kat["part_by_two21"]
+    assert [L.oracle_part_by_two10(x) for x in kat["x10"]] == kat["part_by_two10"]
     tri = np.array(kat["triples16"]).reshape(-1, 3)
     assert [L.oracle_part_by_two16(int(t[0])) for t in tri] == kat["part_by_two16"]
 
