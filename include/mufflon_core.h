@@ -417,8 +417,9 @@ typedef struct {
 	uint64_t h2dBytes;
 } MufflonLoadStats;
 CORE_API Boolean CDECL mufflon_get_load_stats(MufflonInstanceHdl instHdl, MufflonLoadStats* stats);
-/* EXTENSION: the loaded scene's light list (108 bytes per light: u16 type,
- * u16 material, position[3], intensity[3], quad vectors[4][3], uv vectors[4][2])
+/* EXTENSION: the loaded scene's light list (112 bytes per light: u16 type,
+ * u16 material, position[3], intensity[3], quad vectors[4][3], uv vectors[4][2],
+ * sphere radius)
  * and light tree (20 bytes per node: left/right flux, left/right index,
  * left/right type), as built on the GPU, plus the sorted
  * (instance << 32 | primitive) -> node-path code map of the area lights.

@@ -608,13 +608,13 @@ class DllInterface:
         return pix, val
 
     def light_tree(self):
-        """The GPU-built light list and tree: (lights (n, 108) uint8, nodes (m, 20) uint8,
+        """The GPU-built light list and tree: (lights (n, 112) uint8, nodes (m, 20) uint8,
         area-light keys uint64, codes uint32, root flux); layout in include/mufflon_core.h."""
         nl, nn, na = c_uint32(), c_uint32(), c_uint32()
         rf = c_float()
         self._check(self.core.mufflon_get_light_tree(self.muffInst, byref(nl), byref(nn), byref(na), None, None, None,
                                                      None, byref(rf)), "mufflon_get_light_tree")
-        lights = np.zeros((nl.value, 108), np.uint8)
+        lights = np.zeros((nl.value, 112), np.uint8)
         nodes = np.zeros((nn.value, 20), np.uint8)
         keys = np.zeros(na.value, np.uint64)
         codes = np.zeros(na.value, np.uint32)

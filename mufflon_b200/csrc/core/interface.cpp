@@ -2038,7 +2038,7 @@ Boolean mufflon_get_light_tree(MufflonInstanceHdl h, uint32_t* numLights, uint32
 	if(numNodes) *numNodes = D.numLightNodes;
 	if(numAreaLights) *numAreaLights = nArea;
 	if(rootFlux) *rootFlux = D.desc.rootFlux;
-	static_assert(sizeof(DLight) == 108 && sizeof(DLightNode) == 20, "light layouts");
+	static_assert(sizeof(DLight) == 112 && sizeof(DLightNode) == 20, "light layouts");
 	if(lights && D.numLights) CHECK_CUDA(cudaMemcpy(lights, D.dLights, sizeof(DLight) * D.numLights, cudaMemcpyDeviceToHost));
 	if(nodes && D.numLightNodes) CHECK_CUDA(cudaMemcpy(nodes, D.dLightNodes, sizeof(DLightNode) * D.numLightNodes, cudaMemcpyDeviceToHost));
 	if(primKeys && nArea) CHECK_CUDA(cudaMemcpy(primKeys, D.dLightKeys, sizeof(uint64_t) * nArea, cudaMemcpyDeviceToHost));

@@ -67,15 +67,25 @@ __device__ __forceinline__ uint64_t scramble_seed(uint32_t x) {
 }
 __device__ __forceinline__ float sample_uniform(uint32_t u) { return __fdiv_rn(float(u), 4294967810.0f); }
 
-// lights.cpp:16-62: a point light's flux from its intensity; a triangle's
-// from its area and the mean emitted radiance; a quad's from 128
-// low-discrepancy samples of its area times the emitted radiance.
+// lights.cpp:16-80: a point light's flux from its intensity; a triangle's
+// and a sphere's from the area and the mean emitted radiance; a quad's from
+// 128 low-discrepancy samples of its area times the emitted radiance.
 __device__ float light_flux(const DLight& l, int32_t primInst, int32_t primId, const DMaterial* mats) {
 	if(l.type == LT_POINT) {
 		const F3 f = ld(l.intensity) * 4.0f * LB_PI;
 		return (f.x + f.y) + f.z;
 	}
 	const F3 rad = ld(mats[l.material].radiance);
+	if(l.type == LT_SPHERE) {
+		// lights.cpp:63-80: the mean of 128 samples of the (constant) radiance,
+		// times the sphere's area times 2 pi
+		const float area = ((4.0f * LB_PI) * l.radius) * l.radius;
+		F3 sum = f3(0, 0, 0);
+		for(int i = 0; i < 128; ++i) sum = sum + rad;
+		sum = sum / 128.0f;
+		const F3 f = sum * area * 2.0f * LB_PI;
+		return (f.x + f.y) + f.z;
+	}
 	if(l.type == LT_TRI) {
 		// lights.cpp:24-40: the mean of 128 samples of the (constant) radiance,
 		// times area times 2 pi
@@ -128,6 +138,25 @@ __global__ void k_make_lights(const LightBuildInput in, uint32_t n, DLight* ligh
 		const uint32_t entry = lod.faceListStart + (t - in.instFirstLight[i]);
 		const uint32_t f = in.emissiveFaces[entry];
 		const float* m = in.instToWorld + 12 * size_t(i);
+		if(f >= lod.numTriangles + lod.numQuads) {
+			// world_container.cpp:966-990: the centre transformed, the radius
+			// scaled by the length of the instance's first axis
+			const float4 sp = lod.spheres[f - lod.numTriangles - lod.numQuads];
+			const F3 col0 = f3(m[0], m[4], m[8]);
+			L.type = LT_SPHERE;
+			L.material = in.faceMaterial[entry];
+			st(L.position, xform_point(m, f3(sp.x, sp.y, sp.z)));
+			L.radius = len(col0) * sp.w;
+			lights[t] = L;
+			primInst[t] = int32_t(i);
+			primId[t] = int32_t(f);
+			const F3 c = light_center(L) * f3(in.sceneScale[0], in.sceneScale[1], in.sceneScale[2]);
+			const uint32_t ax = to_u32(c.x), ay = to_u32(c.y), az = to_u32(c.z);
+			keyHi[t] = hilbert3(ax >> 16, ay >> 16, az >> 16);
+			keyLo[t] = hilbert3(ax & 0xffff, ay & 0xffff, az & 0xffff);
+			order[t] = int32_t(t);
+			return;
+		}
 		const bool tri = f < lod.numTriangles;
 		const int corners = tri ? 3 : 4;
 		const uint32_t base = tri ? 3u * f : 3u * lod.numTriangles + 4u * (f - lod.numTriangles);

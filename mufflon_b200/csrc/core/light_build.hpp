@@ -27,6 +27,8 @@ struct LightLodInfo {
 	const uint32_t* indices;      // 3 per triangle, then 4 per quad
 	uint32_t numTriangles;
 	uint32_t faceListStart;       // into LightBuildInput::emissiveFaces
+	uint32_t numQuads;
+	const float4* spheres;        // centre, radius
 };
 
 struct LightBuildInput {
@@ -36,7 +38,7 @@ struct LightBuildInput {
 	const uint8_t* mirroring;     // device: per instance, det of the 3x3 part < 0
 	const uint32_t* instFirstLight; // device: numInstances + 1 prefix sums of emissive faces
 	const LightLodInfo* lods;     // device: per used LoD
-	const uint32_t* emissiveFaces;// device: per LoD, its emissive faces (triangles first, then quads; index in the LoD's faces)
+	const uint32_t* emissiveFaces;// device: per LoD, its emissive primitives (triangles, quads, then spheres; primitive index)
 	const uint16_t* faceMaterial; // device: material slot of each entry of emissiveFaces
 	uint32_t numArea;             // area lights (emissive faces over all instances)
 	const float* pointLights;     // device: 6 floats (position, intensity) per point light

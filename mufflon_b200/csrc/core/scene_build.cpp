@@ -375,12 +375,11 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 
 	// --- lights (world_container.cpp:869-990), list and tree built on the GPU (light_build.cu)
 	if(!upload(D.dMaterials, D.cap[9], mats.data(), mats.size(), s, err)) return false;
-	// world_container.cpp:929-988: emissive triangles and quads become area
-	// lights (triangles first, then quads, per instance). Emissive spheres are
-	// area lights there too; this path tracer does not sample them, so a
-	// scenario with emissive spheres is refused rather than rendered without
-	// their next-event estimation. Emissive faces are listed once per LoD.
+	// world_container.cpp:929-990: emissive triangles, quads and spheres
+	// become area lights (in that order, per instance). Emissive primitives
+	// are listed once per LoD.
 	std::vector<uint32_t> lodQuadStart(D.lodSources.size(), 0), lodQuadCount(D.lodSources.size(), 0);
+	std::vector<uint32_t> lodSphereCount(D.lodSources.size(), 0);
 	std::vector<uint32_t> emissiveQuads;
 	std::vector<uint16_t> quadMaterial;
 	// Scenes without emissive materials (only point lights or the background)
@@ -391,22 +390,24 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	for(size_t li = 0; li < D.lodSources.size() && anyEmissive; ++li) {
 		const HostLod& h = *D.lodSources[li];
 		auto emissive = [&](uint16_t m) { return m < mats.size() && mats[m].type == MAT_EMISSIVE; };
-		for(uint16_t m : h.sphereMat)
-			if(emissive(m)) { err = "emissive spheres are not area lights in the CUDA path tracer; emitters must be triangles or quads"; return false; }
 		lodQuadStart[li] = uint32_t(emissiveQuads.size());
 		for(uint32_t t = 0; t < h.num_triangles(); ++t)
 			if(emissive(h.triMat[t])) { emissiveQuads.push_back(t); quadMaterial.push_back(h.triMat[t]); }
 		for(uint32_t q = 0; q < h.num_quads(); ++q)
 			if(emissive(h.quadMat[q])) { emissiveQuads.push_back(h.num_triangles() + q); quadMaterial.push_back(h.quadMat[q]); }
+		const uint32_t faces = h.num_triangles() + h.num_quads();
+		for(uint32_t k = 0; k < h.num_spheres(); ++k)
+			if(emissive(h.sphereMat[k])) { emissiveQuads.push_back(faces + k); quadMaterial.push_back(h.sphereMat[k]); ++lodSphereCount[li]; }
 		lodQuadCount[li] = uint32_t(emissiveQuads.size()) - lodQuadStart[li];
 	}
 	// per instance: instance-to-world, mirroring, first light index (area lights in instance order)
 	std::vector<uint8_t> lightMirror(std::max<uint32_t>(numInst, 1), 0);
 	std::vector<uint32_t> firstLight(size_t(numInst) + 1, 0);
-	uint64_t numArea64 = 0;
+	uint64_t numArea64 = 0, numSphere64 = 0;
 	for(uint32_t i = 0; i < numInst; ++i) {
 		firstLight[i] = uint32_t(numArea64);
 		if(instLod[i] == 0xFFFFFFFFu || lodQuadCount[instLod[i]] == 0) continue;
+		numSphere64 += lodSphereCount[instLod[i]];
 		const float* m = &i2wAll[12 * size_t(i)];
 		const float det3 = m[0] * (m[5] * m[10] - m[9] * m[6]) - m[1] * (m[4] * m[10] - m[8] * m[6]) + m[2] * (m[4] * m[9] - m[8] * m[5]);
 		lightMirror[i] = det3 < 0.0f ? 1 : 0;
@@ -426,7 +427,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	for(size_t li = 0; li < D.lodSources.size(); ++li) {
 		const HostLod& h = *D.lodSources[li];
 		lodInfo[li] = LightLodInfo{ D.lods[li].vertices, h.uvs.empty() ? nullptr : D.lods[li].uvs, D.lods[li].indices,
-		                            h.num_triangles(), lodQuadStart[li] };
+		                            h.num_triangles(), lodQuadStart[li], h.num_quads(), D.lods[li].spheres };
 	}
 	if(!upload(D.dLightMirror, D.lightCap[1], lightMirror.data(), numArea ? lightMirror.size() : 0, s, err)) return false;
 	if(!upload(D.dLightFirst, D.lightCap[2], firstLight.data(), numArea ? firstLight.size() : 0, s, err)) return false;
@@ -477,6 +478,7 @@ bool build_device_scene(MufflonInstance& inst, std::string& err) {
 	S.activeInstances = active; S.validInstance = valid;
 	S.maxSteps = MAX_TRAVERSAL_STEPS;
 	S.hasAlpha = hasAlpha ? 1 : 0;
+	S.sphereLights = numSphere64 > 0 ? 1 : 0;
 	S.tlasNodes = D.tlas.nodes; S.tlasPrimIds = D.tlas.primIds; S.tlasNumInternal = D.tlas.numInternal;
 	S.tlasWide = D.tlas.wnodes; S.tlasWidePrims = D.tlas.wprims; S.tlasNumWide = D.tlas.numWide;
 	S.materials = D.dMaterials; S.textures = D.dTextures;

@@ -420,7 +420,8 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 					if(cosOut > 0.0f) {
 						value = h.mat.radiance;
 						backPdf = __fdiv_rn(cosOut, PI);
-						if(nonzero(value)) startPdf = light_connect_pdf(S, h.inst, h.prim, h.sp);
+						// the bidirectional weight counts the light's emission pdf (cpu_bpt.cpp:228)
+						if(nonzero(value)) startPdf = light_pdfs(S, h.inst, h.prim, h.sp, vp[1 - cur].position).emit;
 					}
 				}
 				if(nonzero(value)) {

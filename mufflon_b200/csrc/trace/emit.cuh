@@ -22,19 +22,7 @@ struct Emitter { f3 position, intensity, normal; int kind; bool valid; float pCh
 // render_target.hpp:64-75: a NaN channel of a contribution is added as 0
 MBD float nan_to_zero(float x) { return isnan(x) ? 0.0f : x; }
 
-// A vector perpendicular to n (not normalised): n crossed with the coordinate
-// axis of n's smallest component. The reference takes `perpendicular` from
-// its math library (epsilon, absent); the emission lobe it orients is
-// rotationally symmetric about n, so the choice of axis changes which
-// direction a random number pair maps to, not the image's expectation.
-MBD f3 perpendicular(f3 n) {
-	const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
-	if(ax <= ay && ax <= az) return make3(0.0f, n.z, -n.y);
-	if(ay <= az) return make3(-n.z, 0.0f, n.x);
-	return make3(n.y, -n.x, 0.0f);
-}
-
-// light_sampling.hpp:80-84 (point), 117-140 (triangle), 143-171 (quad)
+// light_sampling.hpp:80-84 (point), 117-140 (triangle), 143-171 (quad), 173-194 (sphere)
 MBD Emitter sample_light_pos(const DScene& S, const DLight& l, float u0, float u1, float lightProb) {
 	Emitter e;
 	e.valid = true;
@@ -49,6 +37,20 @@ MBD Emitter sample_light_pos(const DScene& S, const DLight& l, float u0, float u
 	}
 	const DMaterial& m = S.materials[l.material];
 	const f3 radiance = m.type == MAT_EMISSIVE ? load3(m.radiance) : make3(0, 0, 0);
+	if(l.type == LT_SPHERE) {
+		// light_sampling.hpp:173-194: a uniformly chosen point of the sphere,
+		// its area pdf the direction pdf 1 / (4 pi) over r^2
+		const float r = l.radius;
+		const f3 normal = sample_dir_sphere_uniform(u0, u1);
+		const float area = ((4.0f * PI) * r) * r;
+		e.position = lv(l.position) + normal * r;
+		e.intensity = (radiance * area) / lightProb;
+		e.normal = normal;
+		e.kind = LV_AREA;
+		e.pChoice = lightProb;
+		e.pdf = __fdiv_rn(__fdiv_rn(1.0f, 4.0f * PI) * 1.0f, r * r);
+		return e;
+	}
 	f3 normal, position;
 	float area;
 	if(l.type == LT_TRI) {

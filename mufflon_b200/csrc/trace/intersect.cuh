@@ -196,7 +196,13 @@ MBD bool sphere_test(const FastRay& r, f3 c, float rad, float& t, float& t2) {
 	const f3 oc = r.o - c;
 	const float b = dot(oc, r.d);
 	const float cc = dot(oc, oc) - rad * rad;
-	const float disc = b * b - cc;
+	// The discriminant from the ray's closest approach to the centre (Haines,
+	// Guenther and Akenine-Moeller, Ray Tracing Gems ch. 7): b * b - cc cancels
+	// for a small sphere far from the origin, and its error then exceeds the
+	// shadow rays' 1e-4 origin offset (light paths to a sphere light 15 units
+	// away were occluded by the light itself).
+	const f3 perp = oc - r.d * b;
+	const float disc = rad * rad - dot(perp, perp);
 	if(disc < 0.0f) return false;
 	const float q = -(b + sgn(b) * sqrt_(disc));
 	float x0, x1;

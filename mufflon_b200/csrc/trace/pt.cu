@@ -105,6 +105,7 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 			throughput = throughput / cp;
 		}
 		const f3 geoN = (v.type == V_SURFACE) ? v.ts.geoN : make3(0.0f, 0.0f, 0.0f);
+		const f3 lastPosition = v.position; // pt_common.hpp:126
 		const Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt, bstack, tstack);
 		if(hit.inst < 0) {
 			v.type = V_VOID;
@@ -145,7 +146,7 @@ MBD void pt_sample(const DScene& S, const PtParams& P, int px, int py, u64& rng,
 				const float cosOut = dot(v.ts.geoN, ex);
 				if(cosOut > 0.0f) {
 					emission = v.mat.radiance;
-					if(nonzero(emission)) connectPdf = light_connect_pdf(S, v.inst, v.prim, v.surfaceParams);
+					if(nonzero(emission)) connectPdf = light_pdfs(S, v.inst, v.prim, v.surfaceParams, lastPosition).connect;
 				}
 			}
 			if(nonzero(emission) && pathLen > 1) {

@@ -17,7 +17,7 @@ struct WideNode; // lbvh/wide.hpp
 enum : int32_t { MAT_LAMBERT = 0, MAT_TORRANCE = 1, MAT_EMISSIVE = 2 };
 // Torrance shadowing models, numbered as core_interface.h ShadowingModel
 enum : int32_t { SHADOW_VCAVITY = 0, SHADOW_SMITH = 1 };
-enum : uint16_t { LT_POINT = 0, LT_TRI = 2, LT_QUAD = 3, LT_INTERNAL = 0xFFFF };
+enum : uint16_t { LT_POINT = 0, LT_TRI = 2, LT_QUAD = 3, LT_SPHERE = 4, LT_INTERNAL = 0xFFFF };
 
 // Reference binary node (src/core/scene/accel_structs/lbvh.hpp:14-18):
 // 32 bytes, two per internal node.
@@ -73,6 +73,7 @@ struct DLight {
 	float intensity[3];
 	float posV[4][3];             // quad: v0, v3-v0, v1-v0, v2-v3-(v1-v0); triangle: v0, v1-v0, v2-v0
 	float uvV[4][2];
+	float radius;                 // sphere (centre in position)
 };
 
 struct DLightNode {
@@ -128,6 +129,7 @@ struct DScene {
 	float aabbMin[3], aabbMax[3];
 	DCamera camera;
 	int32_t hasAlpha;             // some material has an alpha texture
+	int32_t sphereLights;         // emissive spheres in the light list (their hit pdf needs the previous vertex)
 	// Traversal steps a ray may take (per traversal loop of the binary
 	// hierarchies, per ray of the 8-wide ones) before it is abandoned and
 	// counted as an error; MAX_TRAVERSAL_STEPS unless the renderer parameter

@@ -349,6 +349,69 @@ MBD Nee connect_tri(const DScene& S, const DLight& l, f3 pos, float u0, float u1
 	return n;
 }
 
+// A vector perpendicular to n (not normalised): n crossed with the coordinate
+// axis of n's smallest component. The reference takes `perpendicular` from
+// its math library (epsilon, absent); the lobes and cones it orients are
+// rotationally symmetric about n, so the choice of axis changes which
+// direction a random number pair maps to, not the image's expectation.
+MBD f3 perpendicular(f3 n) {
+	const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+	if(ax <= ay && ax <= az) return make3(0.0f, n.z, -n.y);
+	if(ay <= az) return make3(-n.z, 0.0f, n.x);
+	return make3(n.y, -n.x, 0.0f);
+}
+
+// sampling.hpp:112-119: a direction in the cone cos theta >= maxCos about +z
+MBD f3 sample_cone_uniform(float maxCos, float u0, float u1, float& pdf) {
+	const float cosTheta = (1.0f - u0) + u0 * maxCos;
+	const float sinTheta = sqrt_(1.0f - cosTheta * cosTheta);
+	const float phi = (2.0f * u1) * PI;
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	pdf = __fdiv_rn(1.0f, (2.0f * PI) * (1.0f - maxCos));
+	return make3(c * sinTheta, s * sinTheta, cosTheta);
+}
+
+// light_sampling.hpp:389-430: the cap of the sphere seen from pos, sampled
+// uniformly by solid angle; no sample from inside the sphere (an empty NEE,
+// valid but without irradiance)
+MBD Nee connect_sphere(const DScene& S, const DLight& l, f3 pos, float u0, float u1) {
+	Nee n;
+	n.valid = true;
+	n.emitMat = int(l.material);
+	n.position = make3(0.0f, 0.0f, 0.0f); n.creationPdf = 0.0f; n.dir = make3(0.0f, 0.0f, 0.0f); n.cosOut = 0.0f;
+	n.diffIrradiance = make3(0.0f, 0.0f, 0.0f); n.geoNormal = make3(0.0f, 0.0f, 0.0f); n.distSq = 0.0f;
+	const f3 center = lv(l.position);
+	const float r = l.radius;
+	f3 centerDir = pos - center;
+	const float dist = len(centerDir);
+	if(dist <= r) return n;
+	centerDir = centerDir / dist;
+	const float cosSphere = __fdiv_rn(r, dist);
+	float conePdf;
+	const f3 d = sample_cone_uniform(cosSphere, u0, u1, conePdf);
+	const f3 tx = normalize(perpendicular(centerDir));
+	const f3 ty = cross(centerDir, tx);
+	const f3 globalDir = (tx * d.x + ty * d.y) + centerDir * d.z;
+	const f3 surfPos = center + globalDir * r;
+	f3 connection = surfPos - pos;
+	const float cDistSq = lensq(connection) + DISTANCESQ_EPSILON;
+	const float cDist = sqrt_(cDistSq);
+	connection = connection / cDist;
+	const DMaterial& m = S.materials[l.material];
+	const f3 radiance = m.type == MAT_EMISSIVE ? load3(m.radiance) : make3(0, 0, 0);
+	const float sampleArea = __fdiv_rn(r * r, conePdf);
+	const float cosOut = fmax_(0.0f, -dot(globalDir, connection));
+	n.position = surfPos;
+	n.creationPdf = __fdiv_rn(1.0f, sampleArea);
+	n.dir = connection;
+	n.cosOut = cosOut;
+	n.diffIrradiance = radiance * __fdiv_rn(sampleArea, cDistSq);
+	n.geoNormal = globalDir;
+	n.distSq = cDistSq;
+	return n;
+}
+
 MBD Nee connect_point(const DLight& l, f3 pos) {
 	f3 direction = lv(l.position) - pos;
 	const float distSq = lensq(direction) + DISTANCESQ_EPSILON;
@@ -412,11 +475,18 @@ MBD Nee lights_connect(const DScene& S, u64 index, u64 numIndices, u64 seed, f3 
 	const DLight& l = S.lights[idx];
 	if(l.type == LT_QUAD) return adjust(connect_quad(S, l, position, u0, u1), lightProb);
 	if(l.type == LT_TRI) return adjust(connect_tri(S, l, position, u0, u1), lightProb);
+	if(l.type == LT_SPHERE) return adjust(connect_sphere(S, l, position, u0, u1), lightProb);
 	return adjust(connect_point(l, position), lightProb);
 }
 
-// light_tree_sampling.hpp:340-412 (triangle and quad area lights)
-MBD float light_connect_pdf(const DScene& S, int inst, int prim, f2 sp) {
+// light_tree_sampling.hpp:340-412: the area pdfs of a hit on an area light,
+// for starting a light path there (emit: what the bidirectional path tracer
+// weighs) and for a next-event sample of it from refPos (connect: what the
+// path tracer weighs); they differ for spheres, whose next-event samples
+// cover only the cap seen from refPos.
+struct LightPdfs { float emit, connect; };
+MBD LightPdfs light_pdfs(const DScene& S, int inst, int prim, f2 sp, f3 refPos) {
+	LightPdfs out; out.emit = 0.0f; out.connect = 0.0f;
 	const float bgSum = (S.bgFlux[0] + S.bgFlux[1]) + S.bgFlux[2];
 	float p = __fdiv_rn(S.rootFlux, (S.dirFlux + S.rootFlux) + bgSum);
 	const u64 key = (u64(uint32_t(inst)) << 32) | uint32_t(prim);
@@ -427,7 +497,7 @@ MBD float light_connect_pdf(const DScene& S, int inst, int prim, f2 sp) {
 		if(k == key) { found = mid; break; }
 		if(k < key) lo = mid + 1; else hi = mid - 1;
 	}
-	if(found < 0) return 0.0f;
+	if(found < 0) return out;
 	uint32_t code = S.lightPrimCodes[found];
 	uint16_t type = S.rootType;
 	int idx = S.rootIndex;
@@ -444,10 +514,17 @@ MBD float light_connect_pdf(const DScene& S, int inst, int prim, f2 sp) {
 	if(l.type == LT_QUAD) {
 		const f3 tx = lv(l.posV[1]) + sp.x * lv(l.posV[3]);
 		const f3 ty = lv(l.posV[2]) + sp.y * lv(l.posV[3]);
-		return __fdiv_rn(p, len(cross(ty, tx)));
+		out.emit = out.connect = __fdiv_rn(p, len(cross(ty, tx)));
+	} else if(l.type == LT_TRI) {
+		out.emit = out.connect = __fdiv_rn(p, __fdiv_rn(len(cross(lv(l.posV[1]), lv(l.posV[2]))), 2.0f));
+	} else if(l.type == LT_SPHERE) {
+		const float cosSphere = __fdiv_rn(l.radius, len(refPos - lv(l.position)));
+		const float solidAngle = (2.0f * PI) * (1.0f - cosSphere);
+		const float rsq = l.radius * l.radius;
+		out.connect = __fdiv_rn(p, solidAngle * rsq);
+		out.emit = __fdiv_rn(p, (4.0f * PI) * rsq);
 	}
-	if(l.type == LT_TRI) return __fdiv_rn(p, __fdiv_rn(len(cross(lv(l.posV[1]), lv(l.posV[2]))), 2.0f));
-	return 0.0f;
+	return out;
 }
 
 MBD f3 pinhole_ray(const DCamera& c, int px, int py, float u0, float u1, float& pdf) {

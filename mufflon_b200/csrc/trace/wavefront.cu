@@ -276,6 +276,7 @@ MBD void camera_path(const DScene& S, const PtParams& P, WfState& W, uint32_t p,
 	}
 	if(!alive) return;
 	f3 o = lv(S.camera.position);
+	if(S.sphereLights) W.prevPos[p] = pack(o, 0.0f);
 	add_epsilon(o, dir, make3(0.0f, 0.0f, 0.0f));
 	const unsigned slot = warp_reserve(W.counters + C_QUEUE0, 1u);
 	W.qPath[0][slot] = int(p);
@@ -485,10 +486,11 @@ struct ShadeState {
 };
 
 // shade_vertex, first part: hit attributes, the first-hit id, the emission
-// term (pt_common.hpp:139-153). False when the path ends at this vertex (a
-// miss, or the maximum path length).
+// term (pt_common.hpp:139-153; prevPos: the previous vertex, whose distance
+// to an emissive sphere sets the sphere's next-event pdf). False when the path
+// ends at this vertex (a miss, or the maximum path length).
 template < class VertexFn >
-MBD bool shade_begin(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
+MBD bool shade_begin(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr, f3 prevPos,
                      const f3& throughput, float pdfF, f3& radiance, float2* hit0, ShadeState& v, VertexFn&& onVertex) {
 	bool surface = false;
 	int matIndex = -1;
@@ -530,7 +532,7 @@ MBD bool shade_begin(const DScene& S, const PtParams& P, int bounce, f3 origin, 
 			const float cosOut = dot(ts.geoN, ex);
 			if(cosOut > 0.0f) {
 				emission = mat.radiance;
-				if(nonzero(emission)) connectPdf = light_connect_pdf(S, hit.inst, hit.prim, hit.sp);
+				if(nonzero(emission)) connectPdf = light_pdfs(S, hit.inst, hit.prim, hit.sp, prevPos).connect;
 			}
 		}
 		if(nonzero(emission) && pathLen > 1) {
@@ -605,13 +607,15 @@ MBD bool shade_walk(const PtParams& P, const ShadeState& v, f3& throughput, floa
 }
 
 // One vertex of pt_sample: emission, next-event estimation (each shadow ray
-// handed to `shadow` in order) and the walk to the next ray.
+// handed to `shadow` in order) and the walk to the next ray. prevPos: the
+// previous vertex's position on entry, this vertex's on return.
 template < class ShadowFn, class VertexFn >
-MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr,
+MBD bool shade_vertex(const DScene& S, const PtParams& P, int bounce, f3 origin, f3 dir, const HitRec& hr, f3& prevPos,
                       f3& throughput, float& pdfF, f3& radiance, u64& rng, float2* hit0, f3& nextO, f3& nextD,
                       ShadowFn&& shadow, VertexFn&& onVertex) {
 	ShadeState v;
-	if(!shade_begin(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, hit0, v, onVertex)) return false;
+	if(!shade_begin(S, P, bounce, origin, dir, hr, prevPos, throughput, pdfF, radiance, hit0, v, onVertex)) return false;
+	prevPos = v.position; // the previous vertex of the next one
 	if(shade_has_nee(P, v)) {
 		const u64 neeSeed = pcg_next(rng);
 		for(int i = 0; i < P.neeCount; ++i) {
@@ -651,7 +655,8 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	unsigned base = 0xFFFFFFFFu;
 	float gw = 0.0f; // the vertex's guide weight (auxiliary targets)
 	f3 nextO, nextD;
-	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, throughput, pdfF, radiance, rng, W.hit0 + p,
+	f3 prevPos = S.sphereLights ? f4to3(W.prevPos[p]) : origin;
+	const bool cont = shade_vertex(S, P, bounce, origin, dir, hr, prevPos, throughput, pdfF, radiance, rng, W.hit0 + p,
 		nextO, nextD, [&](int i, f3 so, f3 sd, float stmax, f3 c, int emitMat, float cosOut) {
 			if(base == 0xFFFFFFFFu) {
 				base = atomicAdd(W.counters + C_SHADOW0 + q, unsigned(P.neeCount));
@@ -675,6 +680,7 @@ MBD void shade_slot(const SP& sp, WfState& W, int q, int bounce, unsigned slot) 
 	if(rng != rng0) W.rng[p] = rng;
 	if(!cont) return;
 	W.thrPdf[p] = pack(throughput, pdfF);
+	if(S.sphereLights) W.prevPos[p] = pack(prevPos, 0.0f);
 	const int out = q ^ 1;
 	const unsigned nslot = warp_reserve(W.counters + out, 1u);
 	W.qPath[out][nslot] = p;
@@ -742,10 +748,10 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 		}
 	};
 	// shades the vertex a traced extension ray reached; sets the next phase
-	auto begin_vertex = [&](f3 origin, f3 dir, const HitRec& hr) {
+	auto begin_vertex = [&](f3 origin, f3 dir, const HitRec& hr, f3 prevPos) {
 		const DScene& S = sp.scene(p);
 		const PtParams& P = sp.params(p);
-		if(!shade_begin(S, P, b, origin, dir, hr, throughput, pdfF, radiance, W.hit0 + p, v, on_vertex)) {
+		if(!shade_begin(S, P, b, origin, dir, hr, prevPos, throughput, pdfF, radiance, W.hit0 + p, v, on_vertex)) {
 			W.rad[p] = pack(radiance, radW);
 			W.rng[p] = rng;
 			phase = T_IDLE;
@@ -781,7 +787,8 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 					rng = W.rng[p];
 					if(W.auxIter) guideA = W.guide[p].x;
 					b = bounce;
-					begin_vertex(f4to3(W.qOrg[q][item]), f4to3(W.qDir[q][item]), hr);
+					const f3 o = f4to3(W.qOrg[q][item]);
+					begin_vertex(o, f4to3(W.qDir[q][item]), hr, sp.scene(p).sphereLights ? f4to3(W.prevPos[p]) : o);
 				}
 			}
 		}
@@ -829,7 +836,7 @@ __global__ void __launch_bounds__(128, MINB) k_tail(const SP sp, WfState W, int 
 			++i;
 		} else {
 			++b;
-			begin_vertex(ro, rd, t.best);
+			begin_vertex(ro, rd, t.best, v.position);
 		}
 	}
 	__syncthreads();
@@ -986,12 +993,13 @@ __global__ void __launch_bounds__(128, 4) k_adjoint_albedo(const DScene S, const
 		f3 em = make3(0.0f, 0.0f, 0.0f);
 		f3 radiance = make3(0.0f, 0.0f, 0.0f);
 		f3 origin = lv(S.camera.position);
+		f3 prevPos = origin;
 		add_epsilon(origin, dir, make3(0.0f, 0.0f, 0.0f));
 		for(int b = 0; alive; ++b) {
 			LocalCounters cnt;
 			const HitRec hr = closest_hit_wide(S, origin, dir, MAX_SCENE_SIZE, cnt, stack);
 			f3 nextO, nextD;
-			const bool cont = shade_vertex(S, P, b, origin, dir, hr, throughput, pdfF, radiance, r, nullptr, nextO, nextD,
+			const bool cont = shade_vertex(S, P, b, origin, dir, hr, prevPos, throughput, pdfF, radiance, r, nullptr, nextO, nextD,
 				[&](int, f3 so, f3 sd, float stmax, f3 c, int emitMat, float) {
 					LocalCounters sc;
 					if(occluded_wide(S, so, sd, stmax, sc, stack)) return;
@@ -1253,7 +1261,7 @@ size_t wf_align(size_t b) { return (b + WF_ALIGN - 1) / WF_ALIGN * WF_ALIGN; }
 
 size_t wavefront_bytes(size_t n, int nee) {
 	if(nee < 1) nee = 1;
-	return wf_align(n * 16) * 2 + wf_align(n * 8) + 2 * (wf_align(n * 4) + 3 * wf_align(n * 16) + wf_align(n * 4)) +
+	return wf_align(n * 16) * 3 + wf_align(n * 8) + 2 * (wf_align(n * 4) + 3 * wf_align(n * 16) + wf_align(n * 4)) +
 	       wf_align(n * nee * 4) + 3 * wf_align(n * nee * 16) + wf_align(WF_COUNTERS * 4) +
 	       4 * wf_align(n * 4) + 2 * wf_align((size_t(2) << WF_SORT_MAX_BITS) * 4);
 }
@@ -1264,6 +1272,7 @@ void wavefront_carve(void* memory, size_t n, int nee, WfState& W) {
 	auto take = [&](size_t b) { char* p = m; m += wf_align(b); return p; };
 	W.thrPdf = reinterpret_cast<float4*>(take(n * 16));
 	W.rad = reinterpret_cast<float4*>(take(n * 16));
+	W.prevPos = reinterpret_cast<float4*>(take(n * 16));
 	W.hit0 = reinterpret_cast<float2*>(take(n * 8));
 	for(int q = 0; q < 2; ++q) {
 		W.qPath[q] = reinterpret_cast<int*>(take(n * 4));

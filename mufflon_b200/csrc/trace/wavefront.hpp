@@ -11,6 +11,7 @@ struct WfState {
 	uint64_t* rng;        // per pixel (the renderer's generator state)
 	float4* thrPdf;       // per path: throughput xyz, pdf of the sampled direction
 	float4* rad;          // per path: radiance of this iteration
+	float4* prevPos;      // per path: position of the vertex that sent its ray (scenes with sphere lights only)
 	float2* hit0;         // per path: first hit (instance, primitive)
 	int* qPath[2];        // extension queues (double buffered)
 	float4* qOrg[2];      // ray origin (epsilon offset applied)

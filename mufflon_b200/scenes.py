@@ -473,14 +473,16 @@ def alpha_cutouts(seed: int = 0, width: int = 128, height: int = 128, background
 
 
 def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: int = 16, num_point_lights: int = 1,
-                    width: int = 96, height: int = 64, emissive_triangles: int = 0) -> SceneSpec:
+                    width: int = 96, height: int = 64, emissive_triangles: int = 0,
+                    emissive_spheres: int = 0) -> SceneSpec:
     """Many small emissive quads: a ground quad, and `num_instances` instances
     (one of them mirrored) of a panel set holding non-emissive triangles,
     `quads_per_instance` emissive quads of three radiances and some
     non-emissive quads; plus point lights. With `emissive_triangles` > 0 the
-    panel set also holds that many emissive triangles. The light tree then has
-    num_instances * (quads_per_instance + emissive_triangles) + num_point_lights
-    leaves."""
+    panel set also holds that many emissive triangles, and with `emissive_spheres` > 0
+    that many emissive spheres (next to two spheres that do not emit). The light tree
+    then has num_instances * (quads_per_instance + emissive_triangles + emissive_spheres)
+    + num_point_lights leaves."""
     rng = np.random.default_rng(seed)
     mats = [MaterialSpec(MAT_LAMBERT, albedo=(0.6, 0.6, 0.55), name="ground"),
             MaterialSpec(MAT_LAMBERT, albedo=(0.3, 0.5, 0.7), name="frame")]
@@ -521,10 +523,16 @@ def emissive_panels(seed: int = 0, num_instances: int = 4, quads_per_instance: i
         uvs += [(0, 0), (1, 0), (1, 1), (0, 1)]
         quads.append((base, base + 1, base + 2, base + 3))
         qmats.append(kind)
+    sph, smats = _empty_spheres()
+    if emissive_spheres:
+        c = rng.uniform(-1.8, 1.8, (emissive_spheres + 2, 3)) + np.array([0.0, 2.2, 0.0])
+        r = rng.uniform(0.08, 0.35, (emissive_spheres + 2, 1))
+        sph = np.concatenate([c, r], 1).astype(np.float32)
+        smats = np.array([1] + [2 + k % 3 for k in range(emissive_spheres)] + [1], np.uint16)
     panel = _lod(np.array(verts, np.float32), np.array(norms, np.float32), np.array(uvs, np.float32),
                  tris=np.array(tris, np.uint32), quads=np.array(quads, np.uint32),
                  mats=np.array([1] * 3 + [2 + t % 3 for t in range(emissive_triangles)] + qmats, np.uint16),
-                 name="panels")
+                 spheres=sph, sphere_mats=smats, name="panels")
     w2i, inst_lod = [identity34()], [0]
     for i in range(num_instances):
         rot = _random_rotation(rng)

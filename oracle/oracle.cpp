@@ -360,6 +360,7 @@ struct PosLight {
 	V2 uvV[4];
 	u16 material;
 	i32 primInst = -1, primId = -1;
+	float radius = 0.0f; // sphere (centre in position)
 };
 
 struct LightNodeRef { float flux; i32 index; u16 type; }; // index: light index or node index
@@ -836,7 +837,13 @@ inline bool sphere_test(const FastRay& r, V3 c, float rad, float& t, float& t2) 
 	const V3 oc = r.o - c;
 	const float b = dot(oc, r.d);
 	const float cc = dot(oc, oc) - rad * rad;
-	const float disc = b * b - cc;
+	// The discriminant from the ray's closest approach to the centre (Haines,
+	// Guenther and Akenine-Moeller, Ray Tracing Gems ch. 7): b * b - cc cancels
+	// for a small sphere far from the origin, and its error then exceeds the
+	// shadow rays' 1e-4 origin offset (light paths to a sphere light 15 units
+	// away were occluded by the light itself).
+	const V3 perp = oc - r.d * b;
+	const float disc = rad * rad - dot(perp, perp);
 	if(disc < 0.0f) return false;
 	const float q = -(b + sgn(b) * mbmath::sqrt(disc));
 	float x0, x1;
@@ -1543,6 +1550,18 @@ inline float light_flux(const Scene& S, const PosLight& l) {
 		const V3 f = l.intensity * 4.0f * PI;
 		return (f.x + f.y) + f.z;
 	}
+	if(l.type == LT_SPHERE) {
+		// lights.cpp:63-80: the mean of 128 radiance samples (constant here)
+		// times the sphere's area times 2 pi
+		const Material& m = S.materials[l.material];
+		const V3 rad = m.radiance * m.scale;
+		const float area = ((4.0f * PI) * l.radius) * l.radius;
+		V3 sum = { 0, 0, 0 };
+		for(int i = 0; i < 128; ++i) sum = sum + rad;
+		sum = sum / 128.0f;
+		const V3 f = sum * area * 2.0f * PI;
+		return (f.x + f.y) + f.z;
+	}
 	if(l.type == LT_TRI) {
 		// lights.cpp:24-40: the mean of 128 radiance samples (a constant emission
 		// adds the same value every time) times area times 2 pi
@@ -1724,6 +1743,49 @@ Nee connect_tri(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
 	return { position, pdf, direction, vpdf, vcos, diff, dist, normal, distSq, true, i32(l.material) };
 }
 
+inline V3 perpendicular(V3 n);
+
+// sampling.hpp:112-119: a direction in the cone cos theta >= maxCos about +z
+inline V3 sample_cone_uniform(float maxCos, float u0, float u1, float& pdf) {
+	const float cosTheta = (1.0f - u0) + u0 * maxCos;
+	const float sinTheta = mbmath::sqrt(1.0f - cosTheta * cosTheta);
+	const float phi = (2.0f * u1) * PI;
+	float s, c;
+	mbmath::sincos(phi, s, c);
+	pdf = 1.0f / ((2.0f * PI) * (1.0f - maxCos));
+	return { c * sinTheta, s * sinTheta, cosTheta };
+}
+
+// light_sampling.hpp:389-430: the cap of the sphere seen from pos, sampled
+// uniformly by solid angle; from inside the sphere an empty sample (valid,
+// without irradiance)
+Nee connect_sphere(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
+	Nee n{};
+	n.valid = true;
+	n.emitMat = i32(l.material);
+	V3 centerDir = pos - l.position;
+	const float dist = len(centerDir);
+	if(dist <= l.radius) return n;
+	centerDir = centerDir / dist;
+	const float cosSphere = l.radius / dist;
+	float conePdf;
+	const V3 d = sample_cone_uniform(cosSphere, u0, u1, conePdf);
+	const V3 tx = normalize(perpendicular(centerDir));
+	const V3 ty = cross(centerDir, tx);
+	const V3 globalDir = (tx * d.x + ty * d.y) + centerDir * d.z;
+	const V3 surfPos = l.position + globalDir * l.radius;
+	V3 connection = surfPos - pos;
+	const float cDistSq = lensq(connection) + DISTANCESQ_EPSILON;
+	const float cDist = mbmath::sqrt(cDistSq);
+	connection = connection / cDist;
+	const Material& m = S.materials[l.material];
+	const V3 radiance = m.type == OR_MAT_EMISSIVE ? m.radiance * m.scale : V3{ 0, 0, 0 };
+	const float sampleArea = (l.radius * l.radius) / conePdf;
+	const float cosOut = std::fmax(0.0f, -dot(globalDir, connection));
+	return { surfPos, 1.0f / sampleArea, connection, cosOut / PI, cosOut, radiance * (sampleArea / cDistSq), cDist,
+	         globalDir, cDistSq, true, i32(l.material) };
+}
+
 // light_sampling.hpp:308-325
 Nee connect_point(const PosLight& l, V3 pos) {
 	V3 direction = l.position - pos;
@@ -1755,6 +1817,7 @@ inline Nee adjust(Nee n, float chance) {
 Nee connect_pos_light(const Scene& S, const PosLight& l, V3 pos, float u0, float u1) {
 	if(l.type == LT_QUAD) return connect_quad(S, l, pos, u0, u1);
 	if(l.type == LT_TRI) return connect_tri(S, l, pos, u0, u1);
+	if(l.type == LT_SPHERE) return connect_sphere(S, l, pos, u0, u1);
 	return connect_point(l, pos);
 }
 
@@ -1802,13 +1865,16 @@ Nee lights_connect(const Scene& S, u64 index, u64 numIndices, u64 seed, V3 posit
 	return adjust(connect_pos_light(S, T.lights[index2], position, u0, u1), lightProb);
 }
 
-// light_tree_sampling.hpp:340-412 (quad area lights)
-float light_connect_pdf(const Scene& S, i32 inst, i32 prim, V2 sp) {
+// light_tree_sampling.hpp:340-412: the area pdfs of a hit on an area light,
+// for starting a light path there (emit) and for a next-event sample of it
+// from refPos (connect); they differ for spheres.
+struct LightPdfs { float emit, connect; };
+LightPdfs light_pdfs(const Scene& S, i32 inst, i32 prim, V2 sp, V3 refPos) {
 	const LightTree& T = S.lightTree;
 	const float bgSum = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
 	float p = T.rootFlux / ((T.dirFlux + T.rootFlux) + bgSum);
 	auto it = T.primToNodePath.find({ inst, prim });
-	if(it == T.primToNodePath.end()) return 0.0f;
+	if(it == T.primToNodePath.end()) return { 0.0f, 0.0f };
 	u32 code = it->second;
 	u16 type = T.rootType;
 	i32 idx = T.rootIndex;
@@ -1825,10 +1891,20 @@ float light_connect_pdf(const Scene& S, i32 inst, i32 prim, V2 sp) {
 	if(l.type == LT_QUAD) {
 		const V3 tx = l.posV[1] + sp.x * l.posV[3];
 		const V3 ty = l.posV[2] + sp.y * l.posV[3];
-		return p / len(cross(ty, tx));
+		const float a = p / len(cross(ty, tx));
+		return { a, a };
 	}
-	if(l.type == LT_TRI) return p / (len(cross(l.posV[1], l.posV[2])) / 2.0f);
-	return 0.0f;
+	if(l.type == LT_TRI) {
+		const float a = p / (len(cross(l.posV[1], l.posV[2])) / 2.0f);
+		return { a, a };
+	}
+	if(l.type == LT_SPHERE) {
+		const float cosSphere = l.radius / len(refPos - l.position);
+		const float solidAngle = (2.0f * PI) * (1.0f - cosSphere);
+		const float rsq = l.radius * l.radius;
+		return { p / ((4.0f * PI) * rsq), p / (solidAngle * rsq) };
+	}
+	return { 0.0f, 0.0f };
 }
 
 // ---------------------------------------------------------------- path tracer
@@ -2023,6 +2099,7 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 			throughput = throughput / cp;
 		}
 		const V3 geoN = (v.type == V_SURFACE) ? v.ts.geoN : V3{ 0, 0, 0 };
+		const V3 lastPosition = v.position; // pt_common.hpp:126
 		Intersection hit = first_intersection(S, origin, excident, geoN, MAX_SCENE_SIZE, cnt);
 		i32 vMat = -1;
 		const V2 vUv = hit.uv;
@@ -2067,7 +2144,7 @@ void pt_sample(PtState& st, i32 px, i32 py, Pcg64& rng, V3& radianceOut, V2& hit
 				const float cosOut = dot(v.ts.geoN, ex);
 				if(cosOut > 0.0f) {
 					emission = v.mat.radiance;
-					if(nonzero(emission)) connectPdf = light_connect_pdf(S, v.inst, v.prim, v.surfaceParams);
+					if(nonzero(emission)) connectPdf = light_pdfs(S, v.inst, v.prim, v.surfaceParams, lastPosition).connect;
 				}
 			}
 			if(nonzero(emission) && pathLen > 1) {
@@ -2171,7 +2248,7 @@ inline V3 perpendicular(V3 n) {
 	return { n.y, -n.x, 0.0f };
 }
 
-// light_sampling.hpp:80-84 (point), 117-140 (triangle), 143-171 (quad)
+// light_sampling.hpp:80-84 (point), 117-140 (triangle), 143-171 (quad), 173-194 (sphere)
 Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, float lightProb) {
 	Emitter e{};
 	e.valid = true;
@@ -2186,6 +2263,20 @@ Emitter sample_light_pos(const Scene& S, const PosLight& l, float u0, float u1, 
 	}
 	const Material& m = S.materials[l.material];
 	const V3 radiance = m.type == OR_MAT_EMISSIVE ? m.radiance * m.scale : V3{ 0, 0, 0 };
+	if(l.type == LT_SPHERE) {
+		// light_sampling.hpp:173-194: a uniformly chosen point of the sphere,
+		// its area pdf the direction pdf 1 / (4 pi) over r^2
+		const float r = l.radius;
+		const V3 normal = sample_dir_sphere_uniform(u0, u1);
+		const float area = ((4.0f * PI) * r) * r;
+		e.position = l.position + normal * r;
+		e.intensity = (radiance * area) / lightProb;
+		e.normal = normal;
+		e.kind = LV_AREA;
+		e.pChoice = lightProb;
+		e.pdf = ((1.0f / (4.0f * PI)) * 1.0f) / (r * r);
+		return e;
+	}
 	V3 normal, position;
 	float area;
 	if(l.type == LT_TRI) {
@@ -2805,7 +2896,8 @@ void bpt_sample(const BptState& st, i32 px, i32 py, u32 idx, u32 numPixels, Pcg6
 				if(cosOut > 0.0f) {
 					value = h.mat.radiance;
 					backPdf = cosOut / PI;
-					if(nonzero(value)) startPdf = light_connect_pdf(S, h.inst, h.prim, h.sp);
+					// the bidirectional weight counts the light's emission pdf (cpu_bpt.cpp:228)
+					if(nonzero(value)) startPdf = light_pdfs(S, h.inst, h.prim, h.sp, V3{ 0, 0, 0 }).emit;
 				}
 			}
 			if(nonzero(value)) {
@@ -3124,6 +3216,20 @@ Scene* create_scene(const OrSceneDesc* d) {
 			pl.primId = i32(l.nT + q);
 			T.lights.push_back(pl);
 		}
+		// world_container.cpp:966-990: then spheres, the centre transformed and
+		// the radius scaled by the length of the instance's first axis
+		for(u32 k = 0; k < l.nS; ++k) {
+			const u16 mi = l.sphereMat[k];
+			if(S->materials[mi].type != OR_MAT_EMISSIVE) continue;
+			PosLight pl{};
+			pl.type = LT_SPHERE;
+			pl.position = xform_point(i2w, sphere_center(l, k));
+			pl.radius = len(V3{ m[0], m[4], m[8] }) * sphere_radius(l, k);
+			pl.material = mi;
+			pl.primInst = i32(inst);
+			pl.primId = i32(l.nT + l.nQ + k);
+			T.lights.push_back(pl);
+		}
 	}
 	for(u32 i = 0; i < d->numPointLights; ++i) {
 		PosLight pl{};
@@ -3234,13 +3340,14 @@ int oracle_light_tree(void* s, uint32_t* numLights, uint32_t* numNodes, uint32_t
 	if(lightsOut) {
 		unsigned char* o = static_cast<unsigned char*>(lightsOut);
 		for(const PosLight& l : T.lights) {
-			float f[26] = { l.position.x, l.position.y, l.position.z, l.intensity.x, l.intensity.y, l.intensity.z };
+			float f[27] = { l.position.x, l.position.y, l.position.z, l.intensity.x, l.intensity.y, l.intensity.z };
 			for(int k = 0; k < 4; ++k) { f[6 + 3 * k] = l.posV[k].x; f[7 + 3 * k] = l.posV[k].y; f[8 + 3 * k] = l.posV[k].z; }
 			for(int k = 0; k < 4; ++k) { f[18 + 2 * k] = l.uvV[k].x; f[19 + 2 * k] = l.uvV[k].y; }
+			f[26] = l.radius;
 			std::memcpy(o, &l.type, 2);
 			std::memcpy(o + 2, &l.material, 2);
 			std::memcpy(o + 4, f, sizeof(f));
-			o += 108;
+			o += 112;
 		}
 	}
 	if(nodesOut) {

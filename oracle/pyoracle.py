@@ -247,12 +247,12 @@ class OracleScene:
         return lib().oracle_light_build_ms(self.handle)
 
     def light_tree(self):
-        """(lights (n, 108) uint8, nodes (m, 20) uint8, keys uint64, codes uint32, root flux) in the
+        """(lights (n, 112) uint8, nodes (m, 20) uint8, keys uint64, codes uint32, root flux) in the
         core's device layout."""
         nl, nn, nc = C.c_uint32(), C.c_uint32(), C.c_uint32()
         rf = C.c_float()
         lib().oracle_light_tree(self.handle, C.byref(nl), C.byref(nn), C.byref(nc), None, None, None, None, None)
-        lights = np.zeros((nl.value, 108), np.uint8)
+        lights = np.zeros((nl.value, 112), np.uint8)
         nodes = np.zeros((nn.value, 20), np.uint8)
         keys = np.zeros(nc.value, np.uint64)
         codes = np.zeros(nc.value, np.uint32)

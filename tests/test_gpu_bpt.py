@@ -36,6 +36,8 @@ def _instanced():
 
 CASES = {
     "panels": lambda: scenes.emissive_panels(5, 6, 40, 2, width=48, height=32, emissive_triangles=12),
+    "sphere_lights": lambda: scenes.emissive_panels(7, 4, 10, 1, width=48, height=32, emissive_triangles=2,
+                                                    emissive_spheres=6),
     "cornell": lambda: scenes.cornell_box(1, width=40, height=40),
     "icosphere_smith": lambda: _glossy_icosphere(1),
     "icosphere_vcavity_env": lambda: _glossy_icosphere(0, background=True),

@@ -38,6 +38,8 @@ def _instanced():
 
 CASES = {
     "panels": lambda: scenes.emissive_panels(5, 6, 40, 2, width=64, height=48, emissive_triangles=12),
+    "sphere_lights": lambda: scenes.emissive_panels(7, 4, 10, 1, width=64, height=48, emissive_triangles=2,
+                                                    emissive_spheres=6),
     "cornell": lambda: scenes.cornell_box(1, width=64, height=64),
     "icosphere_smith": lambda: _glossy_icosphere(1),
     "icosphere_vcavity": lambda: _glossy_icosphere(0),
