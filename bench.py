@@ -204,7 +204,7 @@ def run_reference(args):
 
 # DRAM bytes per algorithmic byte of the traversal launches, from an ncu
 # capture of the bounce-1 k_trace launch of this workload.
-TRACE_DRAM_PER_ALG_BYTE = 0.33  # 390.4 MB of DRAM traffic for 1.194 GB of algorithmic bytes
+TRACE_DRAM_PER_ALG_BYTE = 0.33  # 395.2 MB of DRAM traffic for 1.194 GB of algorithmic bytes
 LBVH_STAGES = ["morton", "sort", "emit", "merge", "mark", "scan", "compact", "soup", "wide"]
 # Algorithmic bytes per triangle of the reference's build stages (Morton 60,
 # sort 200, emit 32, merge 148, mark 32, scan 8, compact 68, soup 96), and of
