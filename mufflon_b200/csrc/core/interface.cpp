@@ -66,7 +66,7 @@ const ParamDesc PT_PARAMS[] = {
 // lt_params.hpp:8-12, plus the recording switch of the parity tests
 const ParamDesc LT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
-	{ "Record connections", PARAM_INT }, { "Traversal step limit", PARAM_INT },
+	{ "Record connections", PARAM_INT }, { "Traversal step limit", PARAM_INT }, { "Megakernel", PARAM_INT },
 };
 // wireframe_params.hpp:6-26
 const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT },
@@ -92,6 +92,7 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 		if(!std::strcmp(name, "Min. path length")) return &p.minPathLength;
 		if(!std::strcmp(name, "Max. path length")) return &p.maxPathLength;
 		if(!std::strcmp(name, "Record connections")) return r.kind == 1 ? &r.ltRecord : &r.bptRecord;
+		if(r.kind == 1 && !std::strcmp(name, "Megakernel")) return &r.ltMegakernel;
 		return nullptr;
 	}
 	if(!std::strcmp(name, "Seed")) return &r.params.seed;
@@ -247,6 +248,16 @@ void ensure_lt_buffers(MufflonInstance& I) {
 			r.ltRecFloats = floats;
 		}
 	}
+	if(r.kind == 1 && !r.ltMegakernel) {
+		const size_t bytes = ltw_bytes(n);
+		if(bytes > r.ltWavefrontBytes) {
+			cudaFree(r.ltWavefront);
+			r.ltWavefront = nullptr;
+			r.ltWavefrontBytes = 0;
+			CHECK_CUDA(cudaMalloc(&r.ltWavefront, bytes));
+			r.ltWavefrontBytes = bytes;
+		}
+	}
 	if(r.kind == 3) {
 		const size_t bytes = bpt_scratch_bytes(r.bptParams.maxPathLength);
 		if(bytes > r.bptScratchBytes) {
@@ -291,7 +302,11 @@ void iterate_lt(MufflonInstance& I) {
 		t.lightness = nullptr; t.density = nullptr; t.recPixel = nullptr; t.recValue = nullptr;
 		t.lightnessVar = nullptr; t.densityMean = nullptr;
 		CHECK_CUDA(launch_wireframe(S, I.scene.dInstI2W, r.wireParams, t, r.counters, I.stream));
-	} else CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream));
+	} else {
+		CHECK(r.ltMegakernel || r.ltParams.maxPathLength <= LTW_MAX_LAUNCHES,
+		      "the light tracer's stages take at most 64 path lengths (set \"Megakernel\" to 1 for longer paths)");
+		CHECK_CUDA(launch_lt(S, r.ltParams, t, r.workCounter, r.counters, I.stream, r.ltMegakernel ? nullptr : r.ltWavefront));
+	}
 	CHECK_CUDA(cudaEventRecord(r.evStop, I.stream));
 	TraceCounters c{};
 	CHECK_CUDA(cudaMemcpyAsync(&c, r.counters, sizeof(TraceCounters), cudaMemcpyDeviceToHost, I.stream));
@@ -356,6 +371,8 @@ void RendererState::release() {
 	ltRecPixel = nullptr; ltRecValue = nullptr; ltRecSlots = 0; ltRecFloats = 0;
 	cudaFree(bptScratch);
 	bptScratch = nullptr; bptScratchBytes = 0;
+	cudaFree(ltWavefront);
+	ltWavefront = nullptr; ltWavefrontBytes = 0;
 	cudaFree(radianceVar); cudaFree(hitIdVar); cudaFree(lightnessVar); cudaFree(densityMean);
 	radianceVar = nullptr; hitIdVar = nullptr; lightnessVar = nullptr; densityMean = nullptr;
 	for(int a = 0; a < 5; ++a) { cudaFree(auxCum[a]); cudaFree(auxVarBuf[a]); auxCum[a] = nullptr; auxVarBuf[a] = nullptr; }

@@ -257,6 +257,9 @@ struct RendererState {
 	size_t auxMemPixels = 0;
 	LtParams ltParams{ 0, 0, 16 }; // the light tracer's own Seed / Min. / Max. path length
 	int32_t ltRecord = 0;          // keep the light tracer's camera connections of the last iteration
+	int32_t ltMegakernel = 0;      // light tracer: 0 stages per path length (default), 1 one persistent kernel
+	void* ltWavefront = nullptr;   // its stage queues
+	size_t ltWavefrontBytes = 0;
 	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters
 	int32_t bptRecord = 0;         // keep its contributions of the last iteration
 	void* bptScratch = nullptr;    // its per-lane light subpaths

@@ -18,6 +18,9 @@
 #include "emit.cuh"
 #include "lt_api.hpp"
 
+#include <algorithm>
+#include <cooperative_groups.h>
+
 namespace mb {
 namespace {
 
@@ -258,6 +261,257 @@ __global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P,
 	}
 }
 
+// ---------------------------------------------------------------- wavefront schedule
+// The light tracer in stages, like the path tracer's wavefront: a start
+// launch emits every photon, connects its light vertex to the camera and
+// queues the first segment of its walk; then, per path length, a trace launch
+// runs the queued segments (closest hit) and camera connections (any hit,
+// adding visible ones to their pixels) and a shade launch turns each hit into
+// the next vertex: its camera connection and the next segment. Every photon
+// draws its random numbers in lt_sample's order, so the connections (their
+// pixels and values, and the records) are the single kernel's bit for bit;
+// only the order of the atomic additions into the image differs.
+//
+// Queue state (LtwState) lives in one device allocation carved by ltw_carve.
+enum { LTW_EXT0 = 0, LTW_SH0 = 2, LTW_WORK = 4 };
+constexpr int LTW_COUNTERS = 4 + 2 * LTW_MAX_LAUNCHES;
+
+struct LtwState {
+	float4* thr;        // per photon: throughput xyz, path length (int bits) in w
+	int* qPhoton[2];    // segment queues (double buffered by path length)
+	float4* qOrg[2];    // origin (offset)
+	float4* qDir[2];    // direction
+	float4* qHit[2];    // t, instance bits, primitive bits, surface u
+	float* qHitV[2];    // surface v
+	float4* sOrg;       // camera connections: origin, length
+	float4* sDir;       // direction, density
+	float4* sAdd;       // radiance rgb, lightness
+	uint2* sMeta;       // pixel, record slot
+	unsigned* counters; // LTW_COUNTERS
+};
+
+MBD unsigned ltw_reserve(unsigned* counter) {
+	namespace cg = cooperative_groups;
+	cg::coalesced_group g = cg::coalesced_threads();
+	unsigned base = 0;
+	if(g.thread_rank() == 0) base = atomicAdd(counter, g.size());
+	base = g.shfl(base, 0);
+	return base + g.thread_rank();
+}
+
+MBD void ltw_queue_connection(const LtwState& W, int gen, f3 so, f3 sd, float stmax, uint32_t pix, float4 add, float dens,
+                              uint32_t slot) {
+	const unsigned i = ltw_reserve(W.counters + LTW_SH0 + (gen & 1));
+	W.sOrg[i] = make_float4(so.x, so.y, so.z, stmax);
+	W.sDir[i] = make_float4(sd.x, sd.y, sd.z, dens);
+	W.sAdd[i] = add;
+	W.sMeta[i] = make_uint2(pix, slot);
+}
+
+MBD void ltw_queue_segment(const LtwState& W, int gen, uint32_t photon, f3 o, f3 d) {
+	const int q = gen & 1;
+	const unsigned i = ltw_reserve(W.counters + LTW_EXT0 + q);
+	W.qPhoton[q][i] = int(photon);
+	W.qOrg[q][i] = make_float4(o.x, o.y, o.z, 0.0f);
+	W.qDir[q][i] = make_float4(d.x, d.y, d.z, 0.0f);
+}
+
+// connection and walk of vertex ph (generation gen: the queues its rays go to)
+MBD void ltw_vertex(const DScene& S, const LtParams& P, const LtTargets& T, const LtwState& W, Photon& ph, int gen,
+                    uint32_t maxL) {
+	if(ph.pathLen + 1 >= P.minPathLength && ph.pathLen + 1 <= P.maxPathLength) {
+		f3 so, sd;
+		float stmax, dens;
+		uint32_t pix;
+		float4 add;
+		if(lt_connect(S, T, ph, so, sd, stmax, pix, add, dens))
+			ltw_queue_connection(W, gen, so, sd, stmax, pix, add, dens, ph.photon * maxL + uint32_t(ph.pathLen));
+	}
+	f3 o, d;
+	if(lt_walk(S, ph, o, d)) {
+		ltw_queue_segment(W, gen, ph.photon, o, d);
+		W.thr[ph.photon] = make_float4(ph.throughput.x, ph.throughput.y, ph.throughput.z, __int_as_float(ph.pathLen));
+	}
+	T.rngState[ph.photon] = ph.rng;
+}
+
+// Every photon: emission, the light vertex's connection and first segment
+// (generation 0).
+__global__ void k_ltw_start(const DScene S, const LtParams P, const LtTargets T, LtwState W) {
+	const uint32_t n = T.width * T.height;
+	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+	if(p >= n) return;
+	const uint32_t maxL = uint32_t(P.maxPathLength > 0 ? P.maxPathLength : 1);
+	Photon ph;
+	ph.photon = p;
+	ph.rng = T.rngState[p];
+	if(!lt_emit(S, ph, n)) { T.rngState[p] = ph.rng; return; }
+	ltw_vertex(S, P, T, W, ph, 0, maxL);
+}
+
+// Generation gen: the segments of queue gen & 1 (closest hit) and the camera
+// connections counted in LTW_SH0 + (gen & 1) (any hit), taken by persistent
+// warps 32 items at a time once all their lanes are idle.
+template < int AM >
+__global__ void __launch_bounds__(128, 6) k_ltw_trace(const DScene S, const LtParams P, const LtTargets T, LtwState W,
+                                                   int gen, TraceCounters* counters) {
+	const int q = gen & 1;
+	if(blockIdx.x == 0 && threadIdx.x == 0) {
+		W.counters[LTW_EXT0 + (q ^ 1)] = 0u; // filled by this generation's shade
+		W.counters[LTW_SH0 + (q ^ 1)] = 0u;
+	}
+	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_EXT0 + q);
+	const unsigned nSh = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_SH0 + q);
+	const unsigned total = nExt + nSh;
+	if(total == 0) return;
+	unsigned* work = W.counters + LTW_WORK + gen;
+	LocalStack stack;
+	LocalCounters cnt;
+	const unsigned lane = threadIdx.x & 31u;
+	WideTracerT<AM> t;
+	bool active = false, exhausted = false;
+	unsigned item = 0;
+	for(;;) {
+		const unsigned busy = __ballot_sync(0xffffffffu, active);
+		const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+		if(idle && !busy) {
+			unsigned base = 0;
+			if(lane == unsigned(__ffs(int(idle)) - 1)) base = atomicAdd(work, unsigned(__popc(idle)));
+			base = __shfl_sync(0xffffffffu, base, __ffs(int(idle)) - 1);
+			if(idle & (1u << lane)) {
+				item = base + unsigned(__popc(idle & ((1u << lane) - 1u)));
+				if(item >= total) exhausted = true;
+				else {
+					++cnt.rays;
+					if(item < nExt) {
+						t.init(S, f4to3(__ldcs(W.qOrg[q] + item)), f4to3(__ldcs(W.qDir[q] + item)), MAX_SCENE_SIZE, false, cnt);
+					} else {
+						++cnt.shadow;
+						const float4 o = __ldcs(W.sOrg + (item - nExt));
+						t.init(S, f4to3(o), f4to3(__ldcs(W.sDir + (item - nExt))), o.w, true, cnt);
+					}
+					active = true;
+				}
+			}
+		}
+		if(__all_sync(0xffffffffu, exhausted)) break;
+		if(active && t.step(S, cnt, stack)) {
+			active = false;
+			if(item < nExt) {
+				const HitRec& h = t.best;
+				__stcs(W.qHit[q] + item, make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x));
+				__stcs(W.qHitV[q] + item, h.sp.y);
+			} else if(!t.occluded) {
+				const unsigned s = item - nExt;
+				const float4 add = __ldcs(W.sAdd + s);
+				const uint2 meta = __ldcs(W.sMeta + s);
+				atomicAdd(T.iter + meta.x, add);
+				const float dens = __ldcs(W.sDir + s).w;
+				if(T.density) atomicAdd(T.iterDensity + meta.x, dens);
+				if(T.recPixel) {
+					T.recPixel[meta.y] = int(meta.x);
+					float* o = T.recValue + 5 * size_t(meta.y);
+					o[0] = add.x; o[1] = add.y; o[2] = add.z; o[3] = add.w; o[4] = dens;
+				}
+			}
+		}
+	}
+	unsigned long long rays = cnt.rays, shadowRays = cnt.shadow, nodes = cnt.nodes, prims = cnt.prims, inst = cnt.instances;
+	unsigned errs = cnt.errors;
+	for(int o = 16; o > 0; o >>= 1) {
+		rays += __shfl_down_sync(0xffffffffu, rays, o);
+		shadowRays += __shfl_down_sync(0xffffffffu, shadowRays, o);
+		nodes += __shfl_down_sync(0xffffffffu, nodes, o);
+		prims += __shfl_down_sync(0xffffffffu, prims, o);
+		inst += __shfl_down_sync(0xffffffffu, inst, o);
+		errs += __shfl_down_sync(0xffffffffu, errs, o);
+	}
+	if(lane == 0 && rays) {
+		atomicAdd(&counters->rays, rays);
+		atomicAdd(&counters->shadowRays, shadowRays);
+		atomicAdd(&counters->nodeVisits, nodes);
+		atomicAdd(&counters->primTests, prims);
+		atomicAdd(&counters->instanceVisits, inst);
+		if(errs) atomicAdd(&counters->errors, errs);
+	}
+}
+
+// Generation gen: each traced segment of queue gen & 1 that hit a surface
+// becomes the photon's next vertex (lt_sample's loop body); its connection
+// and next segment go to generation gen + 1.
+__global__ void __launch_bounds__(128, 8) k_ltw_shade(const DScene S, const LtParams P, const LtTargets T, LtwState W, int gen) {
+	const int q = gen & 1;
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_EXT0 + q);
+	const uint32_t maxL = uint32_t(P.maxPathLength > 0 ? P.maxPathLength : 1);
+	for(unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+		const float4 hh = __ldcs(W.qHit[q] + i);
+		const int hitInst = __float_as_int(hh.y);
+		if(hitInst < 0) continue; // the photon left the scene (its generator is stored)
+		const uint32_t p = uint32_t(__ldcs(W.qPhoton[q] + i));
+		const f3 ro = f4to3(__ldcs(W.qOrg[q] + i)), rd = f4to3(__ldcs(W.qDir[q] + i));
+		HitRec hr;
+		hr.t = hh.x; hr.inst = hitInst; hr.prim = __float_as_int(hh.z);
+		hr.sp = make2(hh.w, __ldcs(W.qHitV[q] + i));
+		hr.has = true;
+		const float4 tp = W.thr[p];
+		Photon ph;
+		ph.photon = p;
+		ph.rng = T.rngState[p];
+		ph.throughput = f4to3(tp);
+		ph.pathLen = __float_as_int(tp.w);
+		const Intersection hit = hit_attributes(S, ro, rd, hr);
+		ph.position = ro + rd * hit.distance;
+		ph.ts = tangent_space(S, hit);
+		ph.mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
+		ph.incEnc = make3(rd.x, rd.y, hit.distance * sgn(rd.z));
+		ph.kind = LV_SURFACE;
+		ph.normal = make3(0.0f, 0.0f, 0.0f);
+		ph.intensity = make3(0.0f, 0.0f, 0.0f);
+		++ph.pathLen;
+		if(ph.pathLen < P.maxPathLength) ltw_vertex(S, P, T, W, ph, gen + 1, maxL);
+	}
+}
+
+int ltw_trace_blocks() {
+	static int blocks = 0;
+	if(blocks == 0) {
+		int dev = 0, sms = 148, a = 0, b = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_ltw_trace<ALPHA_NEVER>, 128, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ltw_trace<ALPHA_ALWAYS>, 128, 0);
+		blocks = sms * std::max(1, std::min(a, b));
+	}
+	return blocks;
+}
+
+size_t ltw_size(size_t n) {
+	auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+	return al(n * 16) + 2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) + 3 * al(n * 16) + al(n * 8) +
+	       al(LTW_COUNTERS * sizeof(unsigned));
+}
+
+LtwState ltw_carve(void* memory, size_t n) {
+	auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+	char* m = static_cast<char*>(memory);
+	auto take = [&](size_t b) { char* r = m; m += al(b); return r; };
+	LtwState W;
+	W.thr = reinterpret_cast<float4*>(take(n * 16));
+	for(int q = 0; q < 2; ++q) {
+		W.qPhoton[q] = reinterpret_cast<int*>(take(n * 4));
+		W.qOrg[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qDir[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHit[q] = reinterpret_cast<float4*>(take(n * 16));
+		W.qHitV[q] = reinterpret_cast<float*>(take(n * 4));
+	}
+	W.sOrg = reinterpret_cast<float4*>(take(n * 16));
+	W.sDir = reinterpret_cast<float4*>(take(n * 16));
+	W.sAdd = reinterpret_cast<float4*>(take(n * 16));
+	W.sMeta = reinterpret_cast<uint2*>(take(n * 8));
+	W.counters = reinterpret_cast<unsigned*>(take(LTW_COUNTERS * sizeof(unsigned)));
+	return W;
+}
+
 // output_handler_variance.hpp:7-31: running means and variances; Density
 // reduces moments (render_targets.hpp:68-74): its target holds the
 // iteration's value and its variance slot the running mean.
@@ -293,8 +547,10 @@ int lt_blocks() {
 
 } // namespace
 
+size_t ltw_bytes(size_t numPhotons) { return ltw_size(numPhotons); }
+
 cudaError_t launch_lt(const DScene& S, const LtParams& P, const LtTargets& T, unsigned int* workCounter,
-                      TraceCounters* counters, cudaStream_t stream) {
+                      TraceCounters* counters, cudaStream_t stream, void* wavefront) {
 	const uint32_t n = T.width * T.height;
 	if(n == 0) return cudaSuccess;
 	cudaError_t e;
@@ -305,10 +561,28 @@ cudaError_t launch_lt(const DScene& S, const LtParams& P, const LtTargets& T, un
 		if((e = cudaMemsetAsync(T.recPixel, 0xFF, slots * sizeof(int32_t), stream)) != cudaSuccess) return e;
 		if((e = cudaMemsetAsync(T.recValue, 0, slots * 5 * sizeof(float), stream)) != cudaSuccess) return e;
 	}
-	if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-	// the variant for the scene: alpha textures or none (no alpha code in the loop)
-	if(S.hasAlpha) k_lt<ALPHA_ALWAYS><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
-	else k_lt<ALPHA_NEVER><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
+	if(wavefront) {
+		const LtwState W = ltw_carve(wavefront, n);
+		const int gens = P.maxPathLength > 0 ? P.maxPathLength : 1;
+		if(gens > LTW_MAX_LAUNCHES) return cudaErrorInvalidValue;
+		if((e = cudaMemsetAsync(W.counters, 0, LTW_COUNTERS * sizeof(unsigned), stream)) != cudaSuccess) return e;
+		k_ltw_start<<<(n + 127) / 128, 128, 0, stream>>>(S, P, T, W);
+		const int tb = ltw_trace_blocks();
+		int dev = 0, sms = 148;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		// generation g: the connections of path length g and the segments reaching path length g + 1
+		for(int g = 0; g < gens; ++g) {
+			if(S.hasAlpha) k_ltw_trace<ALPHA_ALWAYS><<<tb, 128, 0, stream>>>(S, P, T, W, g, counters);
+			else k_ltw_trace<ALPHA_NEVER><<<tb, 128, 0, stream>>>(S, P, T, W, g, counters);
+			if(g + 1 < gens) k_ltw_shade<<<sms * 8, 128, 0, stream>>>(S, P, T, W, g);
+		}
+	} else {
+		if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+		// the variant for the scene: alpha textures or none (no alpha code in the loop)
+		if(S.hasAlpha) k_lt<ALPHA_ALWAYS><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
+		else k_lt<ALPHA_NEVER><<<lt_blocks(), 128, 0, stream>>>(S, P, T, workCounter, counters);
+	}
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_lt_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
 	return cudaGetLastError();

@@ -34,9 +34,14 @@ struct LtTargets {
 };
 
 // One light-tracing iteration (width * height photons): clears the iteration
-// buffers and records, traces the photons, updates the running means.
+// buffers and records, traces the photons, updates the running means. With
+// `wavefront` (ltw_bytes(width * height) bytes of device memory) in stages
+// per path length; without, in one persistent kernel. Both give the same
+// connections; the wavefront takes at most LTW_MAX_LAUNCHES path lengths.
+constexpr int LTW_MAX_LAUNCHES = 64;
+size_t ltw_bytes(size_t numPhotons);
 cudaError_t launch_lt(const DScene& scene, const LtParams& params, const LtTargets& targets,
-                      unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
+                      unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream, void* wavefront);
 
 // Bytes of the bidirectional path tracer's per-lane light-subpath storage
 // (one slice of max. path length vertices per resident thread).

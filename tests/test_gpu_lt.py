@@ -78,9 +78,12 @@ def _rel_rmse(a, b):
 
 @pytest.mark.parametrize("case", list(CASES))
 @pytest.mark.parametrize("density", [False, True], ids=["plain", "density"])
-def test_lt_connections_and_image_match_oracle(oracle, case, density):
+@pytest.mark.parametrize("megakernel", [0, 1], ids=["stages", "single_kernel"])
+def test_lt_connections_and_image_match_oracle(oracle, case, density, megakernel):
+    """Both schedules: the stages per path length (default) and the single
+    persistent kernel ("Megakernel" 1)."""
     spec = CASES[case]()
-    params = {"Seed": 4, "Min. path length": 0, "Max. path length": 6}
+    params = {"Seed": 4, "Min. path length": 0, "Max. path length": 6, "Megakernel": megakernel}
     lt = oracle.OracleLightTracer(oracle.OracleScene(spec), seed=4, min_path=0, max_path=6, density=density)
     seen = []
 
