@@ -56,6 +56,8 @@ def parse():
                         "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
                         "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; instanced: config 2 (4 096 instances) at 1080p")
     p.add_argument("--jobs", type=int, default=64)
+    p.add_argument("--megakernel", action="store_true",
+                   help="lt / bpt: the single persistent kernel instead of the stages per path length")
     return p.parse_args()
 
 
@@ -739,6 +741,7 @@ def run_lt(args):
     bindings.load_scene_spec(d, spec)
     assert d.render_enable_renderer(1, 0)
     assert d.renderer_set_parameter_int("Max. path length", MAX_PATH)
+    assert d.renderer_set_parameter_int("Megakernel", int(args.megakernel))
     d.render_enable_render_target("Radiance", False)
     iters = SPP_PER_FRAME
     for _ in range(args.warmup * iters):
@@ -771,6 +774,7 @@ def run_lt(args):
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
             "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
             "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_1920x1080_lt_16it_depth{MAX_PATH}",
+                       "schedule": "single kernel" if args.megakernel else "stages per path length",
                        "photons_per_step": iters * WIDTH * HEIGHT,
                        "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
             "photons_per_s": round(photons / (ms / 1e3), 1), "rays_per_step": int(rays / args.steps),
@@ -799,6 +803,7 @@ def run_bpt(args):
     bindings.load_scene_spec(d, spec)
     assert d.render_enable_renderer(3, 0)
     assert d.renderer_set_parameter_int("Max. path length", MAX_PATH)
+    assert d.renderer_set_parameter_int("Megakernel", int(args.megakernel))
     d.render_enable_render_target("Radiance", False)
     iters = SPP_PER_FRAME
     for _ in range(args.warmup * iters):
@@ -831,6 +836,7 @@ def run_bpt(args):
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
             "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
             "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_1920x1080_bpt_16it_depth{MAX_PATH}",
+                       "schedule": "single kernel" if args.megakernel else "stages per path length",
                        "samples_per_step": iters * WIDTH * HEIGHT,
                        "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
             "samples_per_s": round(args.steps * iters * WIDTH * HEIGHT / (ms / 1e3), 1),

@@ -92,7 +92,7 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 		if(!std::strcmp(name, "Min. path length")) return &p.minPathLength;
 		if(!std::strcmp(name, "Max. path length")) return &p.maxPathLength;
 		if(!std::strcmp(name, "Record connections")) return r.kind == 1 ? &r.ltRecord : &r.bptRecord;
-		if(r.kind == 1 && !std::strcmp(name, "Megakernel")) return &r.ltMegakernel;
+		if(!std::strcmp(name, "Megakernel")) return r.kind == 1 ? &r.ltMegakernel : &r.bptMegakernel;
 		return nullptr;
 	}
 	if(!std::strcmp(name, "Seed")) return &r.params.seed;
@@ -258,7 +258,7 @@ void ensure_lt_buffers(MufflonInstance& I) {
 			r.ltWavefrontBytes = bytes;
 		}
 	}
-	if(r.kind == 3) {
+	if(r.kind == 3 && r.bptMegakernel) {
 		const size_t bytes = bpt_scratch_bytes(r.bptParams.maxPathLength);
 		if(bytes > r.bptScratchBytes) {
 			cudaFree(r.bptScratch);
@@ -266,6 +266,16 @@ void ensure_lt_buffers(MufflonInstance& I) {
 			r.bptScratchBytes = 0;
 			CHECK_CUDA(cudaMalloc(&r.bptScratch, bytes));
 			r.bptScratchBytes = bytes;
+		}
+	}
+	if(r.kind == 3 && !r.bptMegakernel) {
+		const size_t bytes = bptw_bytes(n, r.bptParams.maxPathLength);
+		if(bytes > r.bptWavefrontBytes) {
+			cudaFree(r.bptWavefront);
+			r.bptWavefront = nullptr;
+			r.bptWavefrontBytes = 0;
+			CHECK_CUDA(cudaMalloc(&r.bptWavefront, bytes));
+			r.bptWavefrontBytes = bytes;
 		}
 	}
 }
@@ -295,7 +305,10 @@ void iterate_lt(MufflonInstance& I) {
 	if(r.kind == 3) {
 		t.density = nullptr;
 		t.densityMean = nullptr;
-		CHECK_CUDA(launch_bpt(S, r.bptParams, t, r.bptScratch, r.workCounter, r.counters, I.stream));
+		CHECK(r.bptMegakernel || r.bptParams.maxPathLength <= BPTW_MAX_PATH,
+		      "the bidirectional path tracer's stages take at most 64 path lengths (set \"Megakernel\" to 1 for longer paths)");
+		CHECK_CUDA(launch_bpt(S, r.bptParams, t, r.bptScratch, r.workCounter, r.counters, I.stream,
+		                      r.bptMegakernel ? nullptr : r.bptWavefront));
 	} else if(r.kind == 2) {
 		t.radiance = r.radiance; // the "Border" target
 		t.radianceVar = r.varBorder ? r.radianceVar : nullptr;
@@ -373,6 +386,8 @@ void RendererState::release() {
 	bptScratch = nullptr; bptScratchBytes = 0;
 	cudaFree(ltWavefront);
 	ltWavefront = nullptr; ltWavefrontBytes = 0;
+	cudaFree(bptWavefront);
+	bptWavefront = nullptr; bptWavefrontBytes = 0;
 	cudaFree(radianceVar); cudaFree(hitIdVar); cudaFree(lightnessVar); cudaFree(densityMean);
 	radianceVar = nullptr; hitIdVar = nullptr; lightnessVar = nullptr; densityMean = nullptr;
 	for(int a = 0; a < 5; ++a) { cudaFree(auxCum[a]); cudaFree(auxVarBuf[a]); auxCum[a] = nullptr; auxVarBuf[a] = nullptr; }

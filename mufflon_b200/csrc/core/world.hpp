@@ -262,8 +262,11 @@ struct RendererState {
 	size_t ltWavefrontBytes = 0;
 	LtParams bptParams{ 0, 0, 16 }; // the bidirectional path tracer's own parameters
 	int32_t bptRecord = 0;         // keep its contributions of the last iteration
-	void* bptScratch = nullptr;    // its per-lane light subpaths
+	int32_t bptMegakernel = 0;     // 0 stages per path length (default), 1 one persistent kernel
+	void* bptScratch = nullptr;    // the persistent kernel's per-lane light subpaths
 	size_t bptScratchBytes = 0;
+	void* bptWavefront = nullptr;  // the stages' subpaths and queues
+	size_t bptWavefrontBytes = 0;
 	size_t ltRecFloats = 0;        // floats allocated at ltRecValue
 	float4* ltIter = nullptr;      // light tracer iteration buffers (radiance rgb + lightness, density)
 	float* ltIterDensity = nullptr;

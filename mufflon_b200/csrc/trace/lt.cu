@@ -15,11 +15,11 @@
 #include "accumulate.cuh"
 #include "shading.cuh"
 #include "wide_traverse.cuh"
+#include "ray_queue.cuh"
 #include "emit.cuh"
 #include "lt_api.hpp"
 
 #include <algorithm>
-#include <cooperative_groups.h>
 
 namespace mb {
 namespace {
@@ -290,18 +290,9 @@ struct LtwState {
 	unsigned* counters; // LTW_COUNTERS
 };
 
-MBD unsigned ltw_reserve(unsigned* counter) {
-	namespace cg = cooperative_groups;
-	cg::coalesced_group g = cg::coalesced_threads();
-	unsigned base = 0;
-	if(g.thread_rank() == 0) base = atomicAdd(counter, g.size());
-	base = g.shfl(base, 0);
-	return base + g.thread_rank();
-}
-
 MBD void ltw_queue_connection(const LtwState& W, int gen, f3 so, f3 sd, float stmax, uint32_t pix, float4 add, float dens,
                               uint32_t slot) {
-	const unsigned i = ltw_reserve(W.counters + LTW_SH0 + (gen & 1));
+	const unsigned i = queue_reserve(W.counters + LTW_SH0 + (gen & 1));
 	W.sOrg[i] = make_float4(so.x, so.y, so.z, stmax);
 	W.sDir[i] = make_float4(sd.x, sd.y, sd.z, dens);
 	W.sAdd[i] = add;
@@ -310,7 +301,7 @@ MBD void ltw_queue_connection(const LtwState& W, int gen, f3 so, f3 sd, float st
 
 MBD void ltw_queue_segment(const LtwState& W, int gen, uint32_t photon, f3 o, f3 d) {
 	const int q = gen & 1;
-	const unsigned i = ltw_reserve(W.counters + LTW_EXT0 + q);
+	const unsigned i = queue_reserve(W.counters + LTW_EXT0 + q);
 	W.qPhoton[q][i] = int(photon);
 	W.qOrg[q][i] = make_float4(o.x, o.y, o.z, 0.0f);
 	W.qDir[q][i] = make_float4(d.x, d.y, d.z, 0.0f);
@@ -360,80 +351,25 @@ __global__ void __launch_bounds__(128, 6) k_ltw_trace(const DScene S, const LtPa
 		W.counters[LTW_EXT0 + (q ^ 1)] = 0u; // filled by this generation's shade
 		W.counters[LTW_SH0 + (q ^ 1)] = 0u;
 	}
-	const unsigned nExt = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_EXT0 + q);
-	const unsigned nSh = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_SH0 + q);
-	const unsigned total = nExt + nSh;
-	if(total == 0) return;
-	unsigned* work = W.counters + LTW_WORK + gen;
-	LocalStack stack;
-	LocalCounters cnt;
-	const unsigned lane = threadIdx.x & 31u;
-	WideTracerT<AM> t;
-	bool active = false, exhausted = false;
-	unsigned item = 0;
-	for(;;) {
-		const unsigned busy = __ballot_sync(0xffffffffu, active);
-		const unsigned idle = __ballot_sync(0xffffffffu, !active && !exhausted);
-		if(idle && !busy) {
-			unsigned base = 0;
-			if(lane == unsigned(__ffs(int(idle)) - 1)) base = atomicAdd(work, unsigned(__popc(idle)));
-			base = __shfl_sync(0xffffffffu, base, __ffs(int(idle)) - 1);
-			if(idle & (1u << lane)) {
-				item = base + unsigned(__popc(idle & ((1u << lane) - 1u)));
-				if(item >= total) exhausted = true;
-				else {
-					++cnt.rays;
-					if(item < nExt) {
-						t.init(S, f4to3(__ldcs(W.qOrg[q] + item)), f4to3(__ldcs(W.qDir[q] + item)), MAX_SCENE_SIZE, false, cnt);
-					} else {
-						++cnt.shadow;
-						const float4 o = __ldcs(W.sOrg + (item - nExt));
-						t.init(S, f4to3(o), f4to3(__ldcs(W.sDir + (item - nExt))), o.w, true, cnt);
-					}
-					active = true;
-				}
-			}
+	RayQueue Q;
+	Q.org = W.qOrg[q]; Q.dir = W.qDir[q]; Q.hit = W.qHit[q]; Q.hitV = W.qHitV[q];
+	Q.sOrg = W.sOrg; Q.sDir = W.sDir;
+	Q.nExt = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_EXT0 + q);
+	Q.nSh = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_SH0 + q);
+	Q.work = W.counters + LTW_WORK + gen;
+	trace_ray_queue<AM>(S, Q, counters, [&](unsigned s, bool occluded) {
+		if(occluded) return;
+		const float4 add = __ldcs(W.sAdd + s);
+		const uint2 meta = __ldcs(W.sMeta + s);
+		atomicAdd(T.iter + meta.x, add);
+		const float dens = __ldcs(W.sDir + s).w;
+		if(T.density) atomicAdd(T.iterDensity + meta.x, dens);
+		if(T.recPixel) {
+			T.recPixel[meta.y] = int(meta.x);
+			float* o = T.recValue + 5 * size_t(meta.y);
+			o[0] = add.x; o[1] = add.y; o[2] = add.z; o[3] = add.w; o[4] = dens;
 		}
-		if(__all_sync(0xffffffffu, exhausted)) break;
-		if(active && t.step(S, cnt, stack)) {
-			active = false;
-			if(item < nExt) {
-				const HitRec& h = t.best;
-				__stcs(W.qHit[q] + item, make_float4(h.t, __int_as_float(h.has ? h.inst : -1), __int_as_float(h.has ? h.prim : -1), h.sp.x));
-				__stcs(W.qHitV[q] + item, h.sp.y);
-			} else if(!t.occluded) {
-				const unsigned s = item - nExt;
-				const float4 add = __ldcs(W.sAdd + s);
-				const uint2 meta = __ldcs(W.sMeta + s);
-				atomicAdd(T.iter + meta.x, add);
-				const float dens = __ldcs(W.sDir + s).w;
-				if(T.density) atomicAdd(T.iterDensity + meta.x, dens);
-				if(T.recPixel) {
-					T.recPixel[meta.y] = int(meta.x);
-					float* o = T.recValue + 5 * size_t(meta.y);
-					o[0] = add.x; o[1] = add.y; o[2] = add.z; o[3] = add.w; o[4] = dens;
-				}
-			}
-		}
-	}
-	unsigned long long rays = cnt.rays, shadowRays = cnt.shadow, nodes = cnt.nodes, prims = cnt.prims, inst = cnt.instances;
-	unsigned errs = cnt.errors;
-	for(int o = 16; o > 0; o >>= 1) {
-		rays += __shfl_down_sync(0xffffffffu, rays, o);
-		shadowRays += __shfl_down_sync(0xffffffffu, shadowRays, o);
-		nodes += __shfl_down_sync(0xffffffffu, nodes, o);
-		prims += __shfl_down_sync(0xffffffffu, prims, o);
-		inst += __shfl_down_sync(0xffffffffu, inst, o);
-		errs += __shfl_down_sync(0xffffffffu, errs, o);
-	}
-	if(lane == 0 && rays) {
-		atomicAdd(&counters->rays, rays);
-		atomicAdd(&counters->shadowRays, shadowRays);
-		atomicAdd(&counters->nodeVisits, nodes);
-		atomicAdd(&counters->primTests, prims);
-		atomicAdd(&counters->instanceVisits, inst);
-		if(errs) atomicAdd(&counters->errors, errs);
-	}
+	});
 }
 
 // Generation gen: each traced segment of queue gen & 1 that hit a surface

@@ -44,15 +44,25 @@ cudaError_t launch_lt(const DScene& scene, const LtParams& params, const LtTarge
                       unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream, void* wavefront);
 
 // Bytes of the bidirectional path tracer's per-lane light-subpath storage
-// (one slice of max. path length vertices per resident thread).
+// (one slice of max. path length vertices per resident thread), used by the
+// single-kernel schedule.
 size_t bpt_scratch_bytes(int maxPathLength);
+
+// Bytes of the staged schedule's device memory for numPixels pixels: every
+// pixel's light subpath, its last two view vertices, the segment queues and
+// up to max. path length connections per pixel and path length.
+constexpr int BPTW_MAX_PATH = 64;
+size_t bptw_bytes(size_t numPixels, int maxPathLength);
 
 // One bidirectional path-tracing iteration (one light and one view subpath
 // per pixel) into the same targets as the light tracer (radiance and
 // lightness; no density); records hold 4 floats per slot, M*M + M slots per
-// pixel for maximum path length M.
+// pixel for maximum path length M. With `wavefront` (bptw_bytes bytes) in
+// stages per path length (at most BPTW_MAX_PATH); without, in one persistent
+// kernel with `scratch` (bpt_scratch_bytes bytes). Both give the same
+// contributions.
 cudaError_t launch_bpt(const DScene& scene, const LtParams& params, const LtTargets& targets, void* scratch,
-                       unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream);
+                       unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream, void* wavefront);
 
 // wireframe_params.hpp:6-26
 struct WireParams {

@@ -68,10 +68,16 @@ def _rel_rmse(a, b):
     return float(np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) / max(np.sqrt(np.mean(b.astype(np.float64) ** 2)), 1e-30))
 
 
+SCHEDULES = pytest.mark.parametrize("megakernel", [0, 1], ids=["stages", "single_kernel"])
+
+
+@SCHEDULES
 @pytest.mark.parametrize("case", list(CASES))
-def test_bpt_contributions_and_image_match_oracle(oracle, case):
+def test_bpt_contributions_and_image_match_oracle(oracle, case, megakernel):
+    """Both schedules: stages per path length (the default) and the persistent
+    kernel ("Megakernel" 1)."""
     spec = CASES[case]()
-    params = {"Seed": 6, "Min. path length": 0, "Max. path length": 5}
+    params = {"Seed": 6, "Min. path length": 0, "Max. path length": 5, "Megakernel": megakernel}
     ob = oracle.OracleBidirPathTracer(oracle.OracleScene(spec), seed=6, min_path=0, max_path=5)
     seen = []
 
@@ -91,9 +97,10 @@ def test_bpt_contributions_and_image_match_oracle(oracle, case):
         assert _rel_rmse(img, ob.target(name)) <= 1e-5, (name, _rel_rmse(img, ob.target(name)))
 
 
-def test_bpt_min_path_length(oracle):
+@SCHEDULES
+def test_bpt_min_path_length(oracle, megakernel):
     spec = CASES["cornell"]()
-    params = {"Seed": 2, "Min. path length": 3, "Max. path length": 4}
+    params = {"Seed": 2, "Min. path length": 3, "Max. path length": 4, "Megakernel": megakernel}
     ob = oracle.OracleBidirPathTracer(oracle.OracleScene(spec), seed=2, min_path=3, max_path=4)
 
     def check(it, rec):
@@ -129,12 +136,13 @@ def _dark_icosphere():
     return dataclasses.replace(spec, background=None, point_lights=np.zeros((0, 6), np.float32))
 
 
+@SCHEDULES
 @pytest.mark.parametrize("case,max_path", [("panels", 1), ("cornell", 2), ("dark", 4)])
-def test_bpt_edge_cases_match_oracle(oracle, case, max_path):
+def test_bpt_edge_cases_match_oracle(oracle, case, max_path, megakernel):
     """Path length 1 (no light-subpath walk), 2, and a scene without lights
     (no light subpath; only the view subpath runs and the image stays black)."""
     spec = _dark_icosphere() if case == "dark" else CASES[case]()
-    params = {"Seed": 1, "Min. path length": 0, "Max. path length": max_path}
+    params = {"Seed": 1, "Min. path length": 0, "Max. path length": max_path, "Megakernel": megakernel}
     ob = oracle.OracleBidirPathTracer(oracle.OracleScene(spec), seed=1, min_path=0, max_path=max_path)
 
     def check(it, rec):
@@ -148,3 +156,23 @@ def test_bpt_edge_cases_match_oracle(oracle, case, max_path):
     else:
         assert out["Radiance"].any()
         assert _rel_rmse(out["Radiance"], ob.target("Radiance")) <= 1e-5
+
+
+@pytest.mark.parametrize("renderer", [1, 3], ids=["lt", "bpt"])
+def test_stages_refuse_paths_beyond_their_launch_count(renderer):
+    """The staged schedules launch a fixed number of generations; a longer
+    max. path length fails the iteration with a message naming the switch to
+    the persistent kernel, and "Megakernel" 1 renders it."""
+    spec = scenes.cornell_box(1, width=8, height=8)
+    d = bindings.DllInterface()
+    try:
+        bindings.load_scene_spec(d, spec)
+        assert d.render_enable_renderer(renderer, 0)
+        assert d.renderer_set_parameter_int("Max. path length", 65)
+        with pytest.raises(bindings.MufflonError, match="at most 64 path lengths"):
+            d.render_iterate()
+        assert d.renderer_set_parameter_int("Megakernel", 1)
+        d.render_iterate()
+        assert d.render_stats()["rays"] > 0
+    finally:
+        d.close()
