@@ -56,6 +56,8 @@ def parse():
                         "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
                         "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; instanced: config 2 (4 096 instances) at 1080p")
     p.add_argument("--jobs", type=int, default=64)
+    p.add_argument("--resolution", type=lambda v: tuple(int(x) for x in v.split("x")), default=(WIDTH, HEIGHT),
+                   help="lt / bpt: image size WxH (default 1920x1080; smaller for profiler captures)")
     p.add_argument("--megakernel", action="store_true",
                    help="lt / bpt: the single persistent kernel instead of the stages per path length")
     return p.parse_args()
@@ -733,10 +735,11 @@ def run_lt(args):
     camera-connection shadow rays. The CPU baseline is one iteration of the
     oracle's light tracer on all host cores."""
     import torch
+    W, H = args.resolution
     torch.cuda.set_device(0)
     from mufflon_b200 import bindings, build, scenes
     build.build()
-    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=W, height=H)
     d = bindings.DllInterface()
     bindings.load_scene_spec(d, spec)
     assert d.render_enable_renderer(1, 0)
@@ -758,7 +761,7 @@ def run_lt(args):
     wall = time.perf_counter() - t0
     img = d.get_target_image("Radiance")
     d.close()
-    photons = args.steps * iters * WIDTH * HEIGHT
+    photons = args.steps * iters * W * H
     cpu = None
     if not args.no_cpu_baseline:
         from oracle import pyoracle
@@ -769,13 +772,13 @@ def run_lt(args):
         el = time.perf_counter() - t1
         r = lt.stats()["rays"]
         cpu = {"value": round(r / el / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
-               "sample": f"one iteration: {WIDTH * HEIGHT} photons, {r} rays, {el:.1f} s"}
+               "sample": f"one iteration: {W * H} photons, {r} rays, {el:.1f} s"}
     line = {"metric": "light tracer Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
             "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
-            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_1920x1080_lt_16it_depth{MAX_PATH}",
+            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_{W}x{H}_lt_16it_depth{MAX_PATH}",
                        "schedule": "single kernel" if args.megakernel else "stages per path length",
-                       "photons_per_step": iters * WIDTH * HEIGHT,
+                       "photons_per_step": iters * W * H,
                        "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
             "photons_per_s": round(photons / (ms / 1e3), 1), "rays_per_step": int(rays / args.steps),
             "shadow_rays_per_step": int(shadow / args.steps),
@@ -795,10 +798,11 @@ def run_bpt(args):
     and camera)."""
     import dataclasses
     import torch
+    W, H = args.resolution
     torch.cuda.set_device(0)
     from mufflon_b200 import bindings, build, scenes
     build.build()
-    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=W, height=H)
     d = bindings.DllInterface()
     bindings.load_scene_spec(d, spec)
     assert d.render_enable_renderer(3, 0)
@@ -824,7 +828,7 @@ def run_bpt(args):
     if not args.no_cpu_baseline:
         from oracle import pyoracle
         threads = os.cpu_count() or 1
-        small = dataclasses.replace(spec, width=WIDTH // 4, height=HEIGHT // 4)
+        small = dataclasses.replace(spec, width=W // 4, height=H // 4)
         ob = pyoracle.OracleBidirPathTracer(pyoracle.OracleScene(small), seed=0, max_path=MAX_PATH)
         t1 = time.perf_counter()
         ob.iterate(threads)
@@ -835,11 +839,11 @@ def run_bpt(args):
     line = {"metric": "bidirectional path tracer Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
             "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
-            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_1920x1080_bpt_16it_depth{MAX_PATH}",
+            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_{W}x{H}_bpt_16it_depth{MAX_PATH}",
                        "schedule": "single kernel" if args.megakernel else "stages per path length",
-                       "samples_per_step": iters * WIDTH * HEIGHT,
+                       "samples_per_step": iters * W * H,
                        "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
-            "samples_per_s": round(args.steps * iters * WIDTH * HEIGHT / (ms / 1e3), 1),
+            "samples_per_s": round(args.steps * iters * W * H / (ms / 1e3), 1),
             "rays_per_step": int(rays / args.steps), "shadow_rays_per_step": int(shadow / args.steps),
             "e2e": {"value": round(rays / wall / 1e6, 2), "unit": "Mrays/s", "note": "wall clock around render_iterate + stats"},
             "image_mean": [round(float(x), 5) for x in img.reshape(-1, 3).mean(0)],

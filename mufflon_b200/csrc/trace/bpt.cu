@@ -10,11 +10,15 @@
 // have been built, evaluated recursively from the MIS data each vertex keeps
 // (BptVertexExt, cpu_bpt.cpp:18-60 and 68-115).
 //
-// Schedule: one persistent kernel whose lanes run a state machine (as the
-// light tracer's): a lane takes a new pixel as soon as its own finishes, and
-// every pass of the loop traces at most one ray per lane (a light-subpath
+// Two schedules with the same contributions. The default runs in stages per
+// path length (k_bptw_*: the light subpaths of all pixels, then the view
+// subpaths, each generation one trace launch over its queued segments and
+// connections and one shade launch over the vertices they reach). The other
+// ("Megakernel") is one persistent kernel whose lanes run a state machine (as
+// the light tracer's): a lane takes a new pixel as soon as its own finishes,
+// and every pass of the loop traces at most one ray per lane (a light-subpath
 // segment, a connection's shadow ray or a view-subpath segment) in one
-// traversal loop shared by the warp. A lane keeps its light subpath in its
+// traversal loop shared by the warp; a lane keeps its light subpath in its
 // own slice of a scratch array (max. path length vertices) and the last two
 // view vertices in local memory. Connections from the camera land in other
 // pixels, so all contributions go to an iteration buffer with vector atomics.
