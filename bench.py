@@ -51,13 +51,15 @@ def parse():
     p.add_argument("--subdiv", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt", "bpt", "instanced"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batch", "adjoint", "load", "lights", "lt", "bpt", "vcm", "instanced"],
                    help="frame: the 1080p headline; batch: 64 mixed jobs in one batched launch vs one by one; "
                         "adjoint: albedo gradient vs forward time; load: scene-file import of the headline scene; "
-                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; instanced: config 2 (4 096 instances) at 1080p")
+                        "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; vcm: vertex connection and merging at 1080p; instanced: config 2 (4 096 instances) at 1080p")
     p.add_argument("--jobs", type=int, default=64)
     p.add_argument("--resolution", type=lambda v: tuple(int(x) for x in v.split("x")), default=(WIDTH, HEIGHT),
                    help="lt / bpt: image size WxH (default 1920x1080; smaller for profiler captures)")
+    p.add_argument("--merge-radius", type=float, default=0.001,
+                   help="vcm: \"Relative merge radius\" (of the scene's diagonal; the reference's default 0.001)")
     p.add_argument("--megakernel", action="store_true",
                    help="lt / bpt: the single persistent kernel instead of the stages per path length")
     return p.parse_args()
@@ -788,14 +790,15 @@ def run_lt(args):
     print(json.dumps(line), flush=True)
 
 
-def run_bpt(args):
-    """The bidirectional path tracer ("Bidirectional Pathtracer", bpt.cu) on
-    the headline scene (1080p icosphere, point light, colored background):
-    16 iterations of one light and one view subpath per pixel per step, path
+def run_bpt(args, vcm=False):
+    """The bidirectional path tracer ("Bidirectional Pathtracer", bpt.cu), or
+    with vcm vertex connection and merging ("Vertex Connection and Merging",
+    vcm.cu, merge radius --merge-radius of the scene's diagonal), on the
+    headline scene (1080p icosphere, point light, colored background): 16
+    iterations of one light and one view subpath per pixel per step, path
     length up to 10. Device time from CUDA events; rays = subpath segments +
     connection shadow rays. The CPU baseline is one iteration of the oracle's
-    bidirectional path tracer on all host cores at 480 x 270 (the same scene
-    and camera)."""
+    renderer on all host cores at 480 x 270 (the same scene and camera)."""
     import dataclasses
     import torch
     W, H = args.resolution
@@ -805,9 +808,12 @@ def run_bpt(args):
     spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=W, height=H)
     d = bindings.DllInterface()
     bindings.load_scene_spec(d, spec)
-    assert d.render_enable_renderer(3, 0)
+    assert d.render_enable_renderer(4 if vcm else 3, 0)
     assert d.renderer_set_parameter_int("Max. path length", MAX_PATH)
-    assert d.renderer_set_parameter_int("Megakernel", int(args.megakernel))
+    if vcm:
+        assert d.renderer_set_parameter_float("Relative merge radius", args.merge_radius)
+    else:
+        assert d.renderer_set_parameter_int("Megakernel", int(args.megakernel))
     d.render_enable_render_target("Radiance", False)
     iters = SPP_PER_FRAME
     for _ in range(args.warmup * iters):
@@ -829,20 +835,26 @@ def run_bpt(args):
         from oracle import pyoracle
         threads = os.cpu_count() or 1
         small = dataclasses.replace(spec, width=W // 4, height=H // 4)
-        ob = pyoracle.OracleBidirPathTracer(pyoracle.OracleScene(small), seed=0, max_path=MAX_PATH)
+        if vcm:
+            ob = pyoracle.OracleVcm(pyoracle.OracleScene(small), seed=0, max_path=MAX_PATH, merge_radius=args.merge_radius)
+        else:
+            ob = pyoracle.OracleBidirPathTracer(pyoracle.OracleScene(small), seed=0, max_path=MAX_PATH)
         t1 = time.perf_counter()
         ob.iterate(threads)
         el = time.perf_counter() - t1
         r = ob.stats()["rays"]
         cpu = {"value": round(r / el / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
                "sample": f"one iteration at {small.width}x{small.height}: {r} rays, {el:.1f} s"}
-    line = {"metric": "bidirectional path tracer Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
+    name = "vertex connection and merging" if vcm else "bidirectional path tracer"
+    config = {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_{W}x{H}_{'vcm' if vcm else 'bpt'}_16it_depth{MAX_PATH}",
+              "schedule": "single kernel" if args.megakernel and not vcm else "stages per path length",
+              "samples_per_step": iters * W * H,
+              "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"}
+    if vcm:
+        config["relative_merge_radius"] = args.merge_radius
+    line = {"metric": f"{name} Mrays/s at 1080p", "value": round(rays / ms / 1e3, 2), "unit": "Mrays/s",
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
-            "dtype": "f32", "ms_per_step": round(ms / args.steps, 3),
-            "config": {"workload": f"displaced_icosphere_{spec.num_prims - 1}tri_{W}x{H}_bpt_16it_depth{MAX_PATH}",
-                       "schedule": "single kernel" if args.megakernel else "stages per path length",
-                       "samples_per_step": iters * W * H,
-                       "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)"},
+            "dtype": "f32", "ms_per_step": round(ms / args.steps, 3), "config": config,
             "samples_per_s": round(args.steps * iters * W * H / (ms / 1e3), 1),
             "rays_per_step": int(rays / args.steps), "shadow_rays_per_step": int(shadow / args.steps),
             "e2e": {"value": round(rays / wall / 1e6, 2), "unit": "Mrays/s", "note": "wall clock around render_iterate + stats"},
@@ -923,6 +935,9 @@ def main():
         return
     if args.workload == "bpt":
         run_bpt(args)
+        return
+    if args.workload == "vcm":
+        run_bpt(args, vcm=True)
         return
     if args.workload == "instanced":
         run_instanced(args)

@@ -345,6 +345,7 @@ class DllHolder:
             "renderer_set_parameter_float": (c_uint32, [c_void_p, c_char_p, c_float]),
             "renderer_get_parameter_float": (c_uint32, [c_void_p, c_char_p, POINTER(c_float)]),
             "renderer_set_parameter_bool": (c_uint32, [c_void_p, c_char_p, c_uint32]),
+            "renderer_get_parameter_bool": (c_uint32, [c_void_p, c_char_p, POINTER(c_uint32)]),
             "renderer_set_parameter_enum": (c_uint32, [c_void_p, c_char_p, c_int32]),
             "mufflon_get_render_stats": (c_uint32, [c_void_p, POINTER(MufflonRenderStats)]),
             "mufflon_get_stage_stats": (c_uint32, [c_void_p, POINTER(MufflonStageStats)]),
@@ -461,6 +462,12 @@ class DllInterface:
 
     def renderer_set_parameter_bool(self, parameterName, value):
         return self.core.renderer_set_parameter_bool(self.muffInst, parameterName.encode(), 1 if value else 0) != 0
+
+    def renderer_get_parameter_bool(self, parameterName):
+        v = c_uint32(0)
+        self._check(self.core.renderer_get_parameter_bool(self.muffInst, parameterName.encode(), byref(v)),
+                    "renderer_get_parameter_bool")
+        return v.value != 0
 
     def renderer_set_parameter_float(self, parameterName, value):
         return self.core.renderer_set_parameter_float(self.muffInst, parameterName.encode(), value) != 0
@@ -602,6 +609,19 @@ class DllInterface:
         w, h = self.current_resolution()
         m = max(1, max_path_length)
         n = w * h * (m * m + m)
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 4), np.float32)
+        self._check(self.core.mufflon_get_lt_records(self.muffInst, _ptr(pix), _ptr(val), n), "mufflon_get_lt_records")
+        return pix, val
+
+    def vcm_records(self, max_path_length: int):
+        """Vertex connection and merging's contributions of the last iteration (integer parameter
+        "Record connections" set): per pixel M*M connection slots [view length][light vertex], then M
+        emitter-hit and M merge slots [view length - 1] (M = max. path length); pixel index (-1: none)
+        and (radiance rgb, lightness)."""
+        w, h = self.current_resolution()
+        m = max(1, max_path_length)
+        n = w * h * (m * m + 2 * m)
         pix = np.zeros(n, np.int32)
         val = np.zeros((n, 4), np.float32)
         self._check(self.core.mufflon_get_lt_records(self.muffInst, _ptr(pix), _ptr(val), n), "mufflon_get_lt_records")

@@ -28,7 +28,7 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["lbvh/lbvh.cu", "lbvh/wide.cu", "lbvh/sort_noalloc.cu", "trace/pt.cu", "trace/wavefront.cu",
               "core/light_build.cu", "core/instance_boxes.cu", "trace/lt.cu",
-              "trace/bpt.cu", "trace/wireframe.cu"]
+              "trace/bpt.cu", "trace/vcm.cu", "trace/wireframe.cu"]
 CPP_SOURCES = ["core/interface.cpp", "core/scene_build.cpp"]
 # the scene-file loader: its own library on top of the core's C API
 LOADER_SOURCES = ["loader/json.cpp", "loader/mff_binary.cpp", "loader/scene_loader.cpp", "loader/interface.cpp"]
@@ -37,7 +37,7 @@ HEADERS = ["common/fmath.hpp", "common/pfm.hpp", "trace/dmath.cuh", "trace/inter
            "trace/scene_types.hpp", "trace/pt_api.hpp", "lbvh/lbvh.hpp", "lbvh/radix_sort.cuh",
            "lbvh/sort_noalloc.hpp", "trace/wavefront.hpp", "trace/wide_traverse.cuh", "lbvh/wide.hpp", "core/world.hpp",
            "core/light_build.hpp", "core/instance_boxes.hpp", "trace/lt_api.hpp",
-           "trace/emit.cuh", "trace/accumulate.cuh"]
+           "trace/emit.cuh", "trace/accumulate.cuh", "trace/ray_queue.cuh", "trace/bidir.cuh", "trace/aux_targets.cuh"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-Xptxas", "-v",

@@ -68,6 +68,12 @@ const ParamDesc LT_PARAMS[] = {
 	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
 	{ "Record connections", PARAM_INT }, { "Traversal step limit", PARAM_INT }, { "Megakernel", PARAM_INT },
 };
+// vcm_params.hpp:8-14, plus the recording switch of the parity tests
+const ParamDesc VCM_PARAMS[] = {
+	{ "Seed", PARAM_INT }, { "Min. path length", PARAM_INT }, { "Max. path length", PARAM_INT },
+	{ "Relative merge radius", PARAM_FLOAT }, { "Progressive", PARAM_BOOL }, { "Record connections", PARAM_INT },
+	{ "Traversal step limit", PARAM_INT },
+};
 // wireframe_params.hpp:6-26
 const ParamDesc WIRE_PARAMS[] = { { "Line width", PARAM_FLOAT }, { "Maximum trace depth", PARAM_INT },
                                   { "Traversal step limit", PARAM_INT } };
@@ -86,13 +92,13 @@ int32_t* param_ptr(RendererState& r, const char* name) {
 		if(!std::strcmp(name, "Maximum trace depth")) return &r.wireParams.maxTraceDepth;
 		return nullptr;
 	}
-	if(r.kind == 1 || r.kind == 3) {
-		LtParams& p = r.kind == 1 ? r.ltParams : r.bptParams;
+	if(r.kind == 1 || r.kind == 3 || r.kind == 4) {
+		LtParams& p = r.kind == 1 ? r.ltParams : r.kind == 3 ? r.bptParams : r.vcmParams;
 		if(!std::strcmp(name, "Seed")) return &p.seed;
 		if(!std::strcmp(name, "Min. path length")) return &p.minPathLength;
 		if(!std::strcmp(name, "Max. path length")) return &p.maxPathLength;
-		if(!std::strcmp(name, "Record connections")) return r.kind == 1 ? &r.ltRecord : &r.bptRecord;
-		if(!std::strcmp(name, "Megakernel")) return r.kind == 1 ? &r.ltMegakernel : &r.bptMegakernel;
+		if(!std::strcmp(name, "Record connections")) return r.kind == 1 ? &r.ltRecord : r.kind == 3 ? &r.bptRecord : &r.vcmRecord;
+		if(r.kind != 4 && !std::strcmp(name, "Megakernel")) return r.kind == 1 ? &r.ltMegakernel : &r.bptMegakernel;
 		return nullptr;
 	}
 	if(!std::strcmp(name, "Seed")) return &r.params.seed;
@@ -230,12 +236,14 @@ void ensure_lt_buffers(MufflonInstance& I) {
 		CHECK_CUDA(cudaMemsetAsync(r.lightness, 0, n * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.density, 0, n * sizeof(float), I.stream));
 	}
-	// records: light tracer M slots of 5 floats per photon, bidirectional
-	// path tracer M*M + M slots of 4 floats per pixel (M = max. path length)
-	const size_t m = size_t(std::max(1, r.kind == 3 ? r.bptParams.maxPathLength : r.ltParams.maxPathLength));
-	const bool record = r.kind == 3 ? r.bptRecord != 0 : r.kind == 1 ? r.ltRecord != 0 : false;
-	const size_t slots = record ? (r.kind == 3 ? n * (m * m + m) : n * m) : 0;
-	const size_t floats = slots * (r.kind == 3 ? 4 : 5);
+	// records: light tracer M slots of 5 floats per photon; bidirectional path
+	// tracer M*M + M, vertex connection and merging M*M + 2M slots of 4 floats
+	// per pixel (M = max. path length)
+	const size_t m = size_t(std::max(1, r.kind == 3 ? r.bptParams.maxPathLength : r.kind == 4 ? r.vcmParams.maxPathLength
+	                                                                            : r.ltParams.maxPathLength));
+	const bool record = r.kind == 3 ? r.bptRecord != 0 : r.kind == 4 ? r.vcmRecord != 0 : r.kind == 1 ? r.ltRecord != 0 : false;
+	const size_t slots = record ? (r.kind == 3 ? n * (m * m + m) : r.kind == 4 ? n * (m * m + 2 * m) : n * m) : 0;
+	const size_t floats = slots * (r.kind == 3 || r.kind == 4 ? 4 : 5);
 	if(slots != r.ltRecSlots || floats != r.ltRecFloats) {
 		cudaFree(r.ltRecPixel); cudaFree(r.ltRecValue);
 		r.ltRecPixel = nullptr; r.ltRecValue = nullptr; r.ltRecSlots = 0; r.ltRecFloats = 0;
@@ -266,6 +274,17 @@ void ensure_lt_buffers(MufflonInstance& I) {
 			r.bptScratchBytes = 0;
 			CHECK_CUDA(cudaMalloc(&r.bptScratch, bytes));
 			r.bptScratchBytes = bytes;
+		}
+	}
+	if(r.kind == 4) {
+		CHECK(r.vcmParams.maxPathLength <= BPTW_MAX_PATH, "vertex connection and merging takes at most 64 path lengths");
+		const size_t bytes = vcm_bytes(n, r.vcmParams.maxPathLength);
+		if(bytes > r.vcmMemoryBytes) {
+			cudaFree(r.vcmMemory);
+			r.vcmMemory = nullptr;
+			r.vcmMemoryBytes = 0;
+			CHECK_CUDA(cudaMalloc(&r.vcmMemory, bytes));
+			r.vcmMemoryBytes = bytes;
 		}
 	}
 	if(r.kind == 3 && !r.bptMegakernel) {
@@ -302,7 +321,12 @@ void iterate_lt(MufflonInstance& I) {
 	t.iteration = r.iteration;
 	CHECK_CUDA(cudaMemsetAsync(r.counters, 0, 2 * sizeof(TraceCounters), I.stream));
 	CHECK_CUDA(cudaEventRecord(r.evStart, I.stream));
-	if(r.kind == 3) {
+	if(r.kind == 4) {
+		t.density = nullptr;
+		t.densityMean = nullptr;
+		const VcmSettings v{ r.vcmMergeRadius, r.vcmProgressive };
+		CHECK_CUDA(launch_vcm(S, r.vcmParams, v, t, r.counters, I.stream, r.vcmMemory));
+	} else if(r.kind == 3) {
 		t.density = nullptr;
 		t.densityMean = nullptr;
 		CHECK(r.bptMegakernel || r.bptParams.maxPathLength <= BPTW_MAX_PATH,
@@ -388,6 +412,8 @@ void RendererState::release() {
 	ltWavefront = nullptr; ltWavefrontBytes = 0;
 	cudaFree(bptWavefront);
 	bptWavefront = nullptr; bptWavefrontBytes = 0;
+	cudaFree(vcmMemory);
+	vcmMemory = nullptr; vcmMemoryBytes = 0;
 	cudaFree(radianceVar); cudaFree(hitIdVar); cudaFree(lightnessVar); cudaFree(densityMean);
 	radianceVar = nullptr; hitIdVar = nullptr; lightnessVar = nullptr; densityMean = nullptr;
 	for(int a = 0; a < 5; ++a) { cudaFree(auxCum[a]); cudaFree(auxVarBuf[a]); auxCum[a] = nullptr; auxVarBuf[a] = nullptr; }
@@ -506,7 +532,7 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 	if(!std::strcmp(name, "Radiance") && r.kind != 2) {
 		read("Radiance", r.targetRadiance, r.varRadiance, r.radiance, r.radianceVar, 3);
 	} else if((r.kind == 1 && (!std::strcmp(name, "Lightness") || !std::strcmp(name, "Density"))) ||
-	          (r.kind == 3 && !std::strcmp(name, "Lightness"))) {
+	          ((r.kind == 3 || r.kind == 4) && !std::strcmp(name, "Lightness"))) {
 		if(!std::strcmp(name, "Lightness")) read("Lightness", r.targetLightness, r.varLightness, r.lightness, r.lightnessVar, 1);
 		else read("Density", r.targetDensity, r.varDensity, r.density, r.densityMean, 1);
 	} else if(r.kind == 2 && !std::strcmp(name, "Border")) {
@@ -523,7 +549,8 @@ Boolean mufflon_get_target_image(MufflonInstanceHdl h, const char* name, Boolean
 		read(AUX_NAMES[a], r.auxTarget[a], r.auxVarOn[a], r.auxCum[a], r.auxVarBuf[a], AUX_CH[a]);
 	} else {
 		throw ApiError(std::string("render target '") + name + "' is not produced by the CUDA " +
-		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "wireframe renderer" : r.kind == 3 ? "bidirectional path tracer" : "path tracer"));
+		               (r.kind == 1 ? "light tracer" : r.kind == 2 ? "wireframe renderer" : r.kind == 3 ? "bidirectional path tracer"
+		                : r.kind == 4 ? "vertex connection and merging renderer" : "path tracer"));
 	}
 	CHECK_CUDA(cudaStreamSynchronize(I.stream));
 	if(ptr) *ptr = r.screen;
@@ -1243,12 +1270,12 @@ Boolean world_set_env_light_scale(MufflonInstanceHdl h, LightHdl l, Vec3 c) {
 
 // ---------------------------------------------------------------- renderers
 // Renderers grouped by name in the reference's registry order (renderers.hpp:23-31,
-// interface.cpp:126-154): the path tracer, the light tracer and the
-// wireframe renderer and the bidirectional path tracer (CPU-only in the
-// reference), each with a CUDA variation.
-const char* RENDERER_NAMES[4][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" }, { "Wireframe", "WF" },
-                                     { "Bidirectional Pathtracer", "BPT" } };
-constexpr uint32_t NUM_RENDERERS = 4u;
+// interface.cpp:126-154): the path tracer, the light tracer, the wireframe
+// renderer, the bidirectional path tracer and vertex connection and merging
+// (the last two CPU-only in the reference), each with a CUDA variation.
+const char* RENDERER_NAMES[5][2] = { { "Pathtracer", "PT" }, { "Lighttracer", "LT" }, { "Wireframe", "WF" },
+                                     { "Bidirectional Pathtracer", "BPT" }, { "Vertex Connection and Merging", "VCM" } };
+constexpr uint32_t NUM_RENDERERS = 5u;
 uint32_t render_get_renderer_count(MufflonInstanceHdl h) { TRY (void)minst(h); return NUM_RENDERERS; CATCH_ALL(0u) }
 uint32_t render_get_renderer_variations(MufflonInstanceHdl h, uint32_t index) {
 	TRY (void)minst(h); CHECK(index < NUM_RENDERERS, "renderer index out of bounds"); return 1u; CATCH_ALL(0u)
@@ -1294,7 +1321,8 @@ Boolean render_iterate(MufflonInstanceHdl h, ProcessTime* iterTime, ProcessTime*
 	if(r.needsReset) {
 		// cpu_pt.cpp:40-45, cpu_lt.cpp:33-38: one generator per pixel index
 		// the wireframe renderer's generators are seeded with the pixel index (cpu_wireframe.cpp:31-36)
-		const int32_t seed = r.kind == 1 ? r.ltParams.seed : r.kind == 3 ? r.bptParams.seed : r.kind == 2 ? 0 : r.params.seed;
+		const int32_t seed = r.kind == 1 ? r.ltParams.seed : r.kind == 3 ? r.bptParams.seed : r.kind == 4 ? r.vcmParams.seed
+		                   : r.kind == 2 ? 0 : r.params.seed;
 		CHECK_CUDA(launch_seed_rng(r.rng, n, seed, I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.radiance, 0, size_t(n) * 3 * sizeof(float), I.stream));
 		CHECK_CUDA(cudaMemsetAsync(r.hitId, 0, size_t(n) * 2 * sizeof(float), I.stream));
@@ -1498,7 +1526,7 @@ Boolean render_save_screenshot(MufflonInstanceHdl h, const char* filename, const
 	CATCH_ALL(false)
 }
 
-static uint32_t target_count(int32_t kind) { return kind == 1 ? 3u : kind == 3 ? 2u : kind == 2 ? 1u : 8u; }
+static uint32_t target_count(int32_t kind) { return kind == 1 ? 3u : kind == 3 || kind == 4 ? 2u : kind == 2 ? 1u : 8u; }
 uint32_t render_get_render_target_count(MufflonInstanceHdl h) { TRY return target_count(minst(h).renderer.kind); CATCH_ALL(0u) }
 const char* render_get_render_target_name(MufflonInstanceHdl h, uint32_t index) {
 	TRY
@@ -1565,14 +1593,16 @@ uint32_t renderer_get_num_parameters(MufflonInstanceHdl h) {
 	TRY
 	const int32_t kind = minst(h).renderer.kind;
 	if(kind == 2) return uint32_t(sizeof(WIRE_PARAMS) / sizeof(WIRE_PARAMS[0]));
+	if(kind == 4) return uint32_t(sizeof(VCM_PARAMS) / sizeof(VCM_PARAMS[0]));
 	return kind != 0 ? uint32_t(sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0])) : uint32_t(sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]));
 	CATCH_ALL(0u)
 }
 const char* renderer_get_parameter_desc(MufflonInstanceHdl h, uint32_t idx, ParameterType* type) {
 	TRY
 	const int32_t kind = minst(h).renderer.kind;
-	const ParamDesc* table = kind == 2 ? WIRE_PARAMS : kind != 0 ? LT_PARAMS : PT_PARAMS;
+	const ParamDesc* table = kind == 2 ? WIRE_PARAMS : kind == 4 ? VCM_PARAMS : kind != 0 ? LT_PARAMS : PT_PARAMS;
 	const size_t count = kind == 2 ? sizeof(WIRE_PARAMS) / sizeof(WIRE_PARAMS[0])
+	                   : kind == 4 ? sizeof(VCM_PARAMS) / sizeof(VCM_PARAMS[0])
 	                   : kind != 0 ? sizeof(LT_PARAMS) / sizeof(LT_PARAMS[0]) : sizeof(PT_PARAMS) / sizeof(PT_PARAMS[0]);
 	CHECK(idx < count, "parameter index out of bounds");
 	if(type) *type = table[idx].type;
@@ -1609,7 +1639,14 @@ Boolean renderer_set_parameter_float(MufflonInstanceHdl h, const char* name, flo
 	TRY
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
-	CHECK(I.renderer.kind == 2 && name && !std::strcmp(name, "Line width"), std::string("unknown float parameter '") + (name ? name : "") + "'");
+	CHECK(name, "parameter name is null");
+	if(I.renderer.kind == 4 && !std::strcmp(name, "Relative merge radius")) {
+		CHECK(value > 0.0f, "Relative merge radius must be positive");
+		I.renderer.vcmMergeRadius = value;
+		I.renderer.needsReset = true;
+		return true;
+	}
+	CHECK(I.renderer.kind == 2 && !std::strcmp(name, "Line width"), std::string("unknown float parameter '") + name + "'");
 	I.renderer.wireParams.lineWidth = value;
 	I.renderer.needsReset = true;
 	return true;
@@ -1618,14 +1655,25 @@ Boolean renderer_set_parameter_float(MufflonInstanceHdl h, const char* name, flo
 Boolean renderer_get_parameter_float(MufflonInstanceHdl h, const char* name, float* value) {
 	TRY
 	MufflonInstance& I = minst(h);
-	CHECK(I.renderer.kind == 2 && name && !std::strcmp(name, "Line width") && value, std::string("unknown float parameter '") + (name ? name : "") + "'");
+	CHECK(name && value, "invalid arguments");
+	if(I.renderer.kind == 4 && !std::strcmp(name, "Relative merge radius")) {
+		*value = I.renderer.vcmMergeRadius;
+		return true;
+	}
+	CHECK(I.renderer.kind == 2 && !std::strcmp(name, "Line width"), std::string("unknown float parameter '") + name + "'");
 	*value = I.renderer.wireParams.lineWidth;
 	return true;
 	CATCH_ALL(false)
 }
 Boolean renderer_set_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean value) {
 	TRY
-	(void)minst(h);
+	MufflonInstance& I = minst(h);
+	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
+	if(name && I.renderer.kind == 4 && !std::strcmp(name, "Progressive")) {
+		I.renderer.vcmProgressive = value ? 1 : 0;
+		I.renderer.needsReset = true;
+		return true;
+	}
 	CHECK(name && !std::strcmp(name, "NEE position guide"), std::string("unknown bool parameter '") + (name ? name : "") + "'");
 	CHECK(!value, "NEE position guide is not implemented by the CUDA path tracer");
 	return true;
@@ -1633,7 +1681,11 @@ Boolean renderer_set_parameter_bool(MufflonInstanceHdl h, const char* name, Bool
 }
 Boolean renderer_get_parameter_bool(MufflonInstanceHdl h, const char* name, Boolean* value) {
 	TRY
-	(void)minst(h);
+	MufflonInstance& I = minst(h);
+	if(name && value && I.renderer.kind == 4 && !std::strcmp(name, "Progressive")) {
+		*value = I.renderer.vcmProgressive ? 1 : 0;
+		return true;
+	}
 	CHECK(name && !std::strcmp(name, "NEE position guide") && value, "unknown bool parameter");
 	*value = 0;
 	return true;
@@ -1681,7 +1733,8 @@ Boolean mufflon_get_lt_records(MufflonInstanceHdl h, int32_t* pixels, float* val
 	MufflonInstance& I = minst(h);
 	std::lock_guard<std::recursive_mutex> lock(I.iterationMutex);
 	const RendererState& r = I.renderer;
-	CHECK((r.kind == 1 || r.kind == 3) && r.ltRecSlots > 0 && r.iteration >= 0, "no recorded light-tracer or bidirectional iteration");
+	CHECK((r.kind == 1 || r.kind == 3 || r.kind == 4) && r.ltRecSlots > 0 && r.iteration >= 0,
+	      "no recorded light-tracer, bidirectional or vertex connection and merging iteration");
 	CHECK(pixels && values && slots == r.ltRecSlots, "the record buffers must hold the renderer's number of slots");
 	CHECK_CUDA(cudaMemcpyAsync(pixels, r.ltRecPixel, slots * sizeof(int32_t), cudaMemcpyDeviceToHost, I.stream));
 	CHECK_CUDA(cudaMemcpyAsync(values, r.ltRecValue, r.ltRecFloats * sizeof(float), cudaMemcpyDeviceToHost, I.stream));

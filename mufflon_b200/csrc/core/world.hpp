@@ -267,6 +267,12 @@ struct RendererState {
 	size_t bptScratchBytes = 0;
 	void* bptWavefront = nullptr;  // the stages' subpaths and queues
 	size_t bptWavefrontBytes = 0;
+	LtParams vcmParams{ 0, 0, 16 }; // vertex connection and merging: its own Seed / Min. / Max. path length
+	float vcmMergeRadius = 0.001f; // "Relative merge radius" (of the scene's diagonal)
+	int32_t vcmProgressive = 0;    // "Progressive"
+	int32_t vcmRecord = 0;         // keep its contributions of the last iteration
+	void* vcmMemory = nullptr;     // its stages' state and photon grid
+	size_t vcmMemoryBytes = 0;
 	size_t ltRecFloats = 0;        // floats allocated at ltRecValue
 	float4* ltIter = nullptr;      // light tracer iteration buffers (radiance rgb + lightness, density)
 	float* ltIterDensity = nullptr;

@@ -22,202 +22,10 @@
 // own slice of a scratch array (max. path length vertices) and the last two
 // view vertices in local memory. Connections from the camera land in other
 // pixels, so all contributions go to an iteration buffer with vector atomics.
-#include "accumulate.cuh"
-#include "wide_traverse.cuh"
-#include "ray_queue.cuh"
-#include "emit.cuh"
-#include "lt_api.hpp"
-
-#include <algorithm>
+#include "bidir.cuh"
 
 namespace mb {
 namespace {
-
-enum BKind { BV_VIRTUAL = 0, BV_CAMERA, BV_SURFACE, BV_VOID, BV_POINT, BV_AREA, BV_ENV };
-
-// A path vertex with the reference's PathVertex<BptVertexExt> contents:
-// incEnc is the encoded incident direction (surfaces: x, y of the direction
-// and the distance with the sign of z; a miss: the direction; an area light:
-// its normal; a point light: its intensity; the environment: the photon's
-// direction).
-struct BV {
-	int kind;
-	f3 position, incEnc, intensity;
-	float projSceneArea;
-	TangentSpace ts;
-	Params mat;
-	int inst, prim;
-	f2 sp;
-	float incidentPdf;  // BptVertexExt::incidentPdf
-	float prevRelSum;   // BptVertexExt::prevRelativeProbabilitySum
-	f3 throughput;      // BptVertexExt::throughput
-};
-
-MBD bool bv_ortho(int k) { return k == BV_VOID || k == BV_ENV; } // path_util.hpp:41-46
-MBD bool bv_end(int k) { return k != BV_SURFACE; }               // path_util.hpp:33-35
-
-// path_util.hpp:160-176
-MBD float bv_geo_factor(const BV& v, f3 dir) {
-	if(v.kind == BV_AREA) return dot(dir, v.incEnc);
-	if(v.kind == BV_SURFACE) return dot(dir, v.ts.shadingN);
-	if(v.kind == BV_ENV || v.kind == BV_VOID) return 1.0f;
-	return 0.0f;
-}
-MBD f3 bv_geo_normal(const BV& v) {
-	if(v.kind == BV_AREA) return v.incEnc;
-	if(v.kind == BV_SURFACE) return v.ts.geoN;
-	return make3(0.0f, 0.0f, 0.0f);
-}
-MBD f3 bv_incident_dir(const BV& v) { return decode_incident(v.incEnc); }
-MBD float bv_incident_dist_sq(const BV& v) { return bv_end(v.kind) ? 0.0f : v.incEnc.z * v.incEnc.z; }
-// path_util.hpp:130-137
-MBD f3 bv_position(const BV& v, f3 ref) {
-	return v.kind == BV_ENV ? ref - bv_incident_dir(v) * MAX_SCENE_SIZE : v.position;
-}
-// path_util.hpp:208-221: a sampling pdf converted into an area pdf at v
-MBD float bv_convert_pdf(const BV& v, int source, float samplePdf, f3 dir, float distSq) {
-	if(source == BV_VIRTUAL) return samplePdf;
-	const float geo = bv_geo_factor(v, dir);
-	if(bv_ortho(source) || bv_ortho(v.kind)) return samplePdf * fabsf(geo);
-	return __fdiv_rn(samplePdf * fabsf(geo), distSq);
-}
-
-// path_util.hpp:245-293: value, cosine and pdfs of leaving v along excident;
-// a camera also yields the pixel (px = -1 off the image)
-MBD EvalValue bv_evaluate(const DScene& S, const BV& v, f3 excident, bool adjoint, int& px, int& py) {
-	EvalValue r;
-	r.value = make3(0.0f, 0.0f, 0.0f); r.cosOut = 0.0f; r.pdfF = 0.0f; r.pdfB = 0.0f;
-	if(v.kind == BV_POINT) { r.value = v.incEnc; r.cosOut = 1.0f; r.pdfF = __fdiv_rn(1.0f, 4.0f * PI); }
-	else if(v.kind == BV_AREA) {
-		const float cosOut = dot(v.incEnc, excident);
-		if(cosOut > 0.0f) { r.value = v.intensity; r.cosOut = cosOut; r.pdfF = __fdiv_rn(cosOut, PI); }
-	} else if(v.kind == BV_ENV) { r.value = v.intensity; r.cosOut = 1.0f; r.pdfF = __fdiv_rn(1.0f, v.projSceneArea); }
-	else if(v.kind == BV_CAMERA) {
-		float w = 0.0f;
-		r.cosOut = 1.0f;
-		if(!pinhole_project(S.camera, excident, px, py, w)) { px = -1; py = -1; }
-		else { r.value = make3(w, w, w); r.pdfF = w; }
-	} else if(v.kind == BV_SURFACE) r = material_evaluate(v.ts, v.mat, bv_incident_dir(v), excident, adjoint);
-	return r;
-}
-
-// cpu_bpt.cpp:68-88: the relative probabilities of the events before v
-MBD float bpt_mis_part(const BV& v, const BV* prev, float vertexPdfBack, float nextPdfBack, int nextType, f3 dir,
-                       float distSq) {
-	float reversePdf = bv_convert_pdf(v, nextType, nextPdfBack, dir, distSq);
-	const float relPdf = __fdiv_rn(reversePdf, v.incidentPdf);
-	if(prev) {
-		reversePdf = bv_convert_pdf(*prev, v.kind, vertexPdfBack, bv_incident_dir(v), bv_incident_dist_sq(v));
-		const float prevRelPdf = __fdiv_rn(reversePdf, prev->incidentPdf);
-		return relPdf + relPdf * (prevRelPdf + prevRelPdf * prev->prevRelSum);
-	}
-	return relPdf;
-}
-
-// random_walk.hpp:38-75 for a BPT vertex: samples v, updates its MIS data
-// (cpu_bpt.cpp:49-58) and applies Russian roulette; false: cancelled.
-static __device__ __noinline__ bool bpt_sample(const DScene& S, BV& v, const BV* prev, int px, int py, u64& rng,
-                                               bool adjoint, f3& throughput, f3& origin, f3& excident, float& pdfF) {
-	const u64 x0 = pcg_next(rng), x1 = pcg_next(rng);
-	const float ru0 = sample_uniform(uint32_t(x0)), ru1 = sample_uniform(uint32_t(x0 >> 32));
-	const float rr = sample_uniform(uint32_t(pcg_next(rng)));
-	f3 sThroughput;
-	float pdfB = 0.0f;
-	origin = v.position;
-	if(v.kind == BV_POINT) {
-		excident = sample_dir_sphere_uniform(ru0, ru1);
-		sThroughput = (v.incEnc * 4.0f) * PI;
-		pdfF = __fdiv_rn(1.0f, 4.0f * PI);
-	} else if(v.kind == BV_AREA) {
-		const f3 d = sample_dir_cosine(ru0, ru1);
-		const f3 tx = normalize(perpendicular(v.incEnc));
-		const f3 ty = cross(v.incEnc, tx);
-		excident = (d.x * tx + d.y * ty) + d.z * v.incEnc;
-		sThroughput = v.intensity * PI;
-		pdfF = __fdiv_rn(d.z, PI);
-	} else if(v.kind == BV_ENV) {
-		float pdf;
-		origin = sample_position(S, v.incEnc, ru0, ru1, pdf);
-		excident = v.incEnc;
-		sThroughput = v.intensity / pdf;
-		pdfF = pdf;
-	} else if(v.kind == BV_CAMERA) {
-		excident = pinhole_ray(S.camera, px, py, ru0, ru1, pdfF);
-		sThroughput = make3(1.0f, 1.0f, 1.0f);
-	} else {
-		const PathSample smp = material_sample(v.ts, v.mat, bv_incident_dir(v), ru0, ru1, x1, adjoint);
-		if(!smp.valid) return false;
-		excident = smp.excident;
-		sThroughput = smp.throughput;
-		pdfF = smp.pdfF;
-		pdfB = smp.pdfB;
-	}
-	if(prev) {
-		const float prevReversePdf = bv_convert_pdf(*prev, v.kind, pdfB, bv_incident_dir(v), bv_incident_dist_sq(v));
-		const float relToPrev = __fdiv_rn(prevReversePdf, prev->incidentPdf);
-		v.prevRelSum = relToPrev + relToPrev * prev->prevRelSum;
-	}
-	throughput = throughput * sThroughput;
-	const float cp = fmin_(maxc(throughput) + 0.1f, 1.0f);
-	if(rr >= cp) return false;
-	throughput = throughput / cp;
-	add_epsilon(origin, excident, bv_geo_normal(v));
-	return true;
-}
-
-// random_walk.hpp:77-113 and cpu_bpt.cpp:36-47: the vertex a segment from
-// `from` ends in (a surface or a miss), with its incident pdf and throughput.
-static __device__ __noinline__ void bpt_new_vertex(const DScene& S, const BV& from, f3 ro, f3 rd, const HitRec& best,
-                                                   float pdfF, f3 throughput, BV& out) {
-	out.inst = -1; out.prim = -1;
-	out.prevRelSum = 0.0f;
-	float dist = best.t;
-	if(!best.has) {
-		out.kind = BV_VOID;
-		out.position = make3(0.0f, 0.0f, 0.0f);
-		out.incEnc = rd;
-	} else {
-		const Intersection hit = hit_attributes(S, ro, rd, best);
-		dist = hit.distance;
-		out.kind = BV_SURFACE;
-		out.position = ro + rd * hit.distance;
-		out.incEnc = make3(rd.x, rd.y, hit.distance * sgn(rd.z));
-		out.ts = tangent_space(S, hit);
-		out.inst = hit.inst;
-		out.prim = hit.prim;
-		out.sp = hit.sp;
-		out.mat = fetch_material(S, material_index(S, hit.inst, hit.prim), hit.uv);
-	}
-	const float inCosAbs = fabsf(bv_geo_factor(out, rd));
-	const bool ortho = bv_ortho(from.kind) || bv_ortho(out.kind);
-	out.incidentPdf = ortho ? pdfF * inCosAbs : __fdiv_rn(pdfF * fabsf(inCosAbs), dist * dist);
-	out.throughput = throughput;
-}
-
-// The start vertex of the light subpath (path_util.hpp:568-625 create_light with
-// BptVertexExt::init and mis_start_pdf, :763-771).
-MBD void bpt_light_vertex(const DScene& S, const Emitter& em, BV& v) {
-	v.position = em.position;
-	v.throughput = make3(1.0f, 1.0f, 1.0f);
-	v.prevRelSum = 0.0f;
-	v.inst = -1; v.prim = -1;
-	if(em.kind == LV_POINT) { v.kind = BV_POINT; v.incEnc = em.intensity; v.incidentPdf = em.pChoice; }
-	else if(em.kind == LV_AREA) { v.kind = BV_AREA; v.incEnc = em.normal; v.intensity = em.intensity; v.incidentPdf = em.pdf * em.pChoice; }
-	else {
-		v.kind = BV_ENV; v.incEnc = em.normal; v.intensity = em.intensity; v.incidentPdf = em.pdf * em.pChoice;
-		v.position = make3(0.0f, 0.0f, 0.0f);
-		v.projSceneArea = projected_area(-em.normal, S.aabbMin, S.aabbMax);
-	}
-}
-
-// A connection's shadow ray and what it adds.
-struct BptConn {
-	f3 ro, rd;
-	float tmax;
-	uint32_t pix;       // the pixel it adds to
-	float4 add;         // radiance rgb, lightness when the shadow ray is unoccluded
-	unsigned zeroSigns; // sign bits of the zeros an occluded one records (bit c: component c)
-};
 
 // cpu_bpt.cpp:120-148: the connection of view vertex v (its predecessor pv)
 // with light vertex w (its predecessor pw) for view throughput thr. 1: it
@@ -257,23 +65,16 @@ MBD int bpt_connect(const DScene& S, uint32_t width, const BV& v, const BV* pv, 
 				const f3 rad = (full * cosProd) * bxdfs;
 				const float light = __fdiv_rn((full.x + full.y) + full.z, 3.0f) * cosProd;
 				c.add = make_float4(nan_to_zero(rad.x), nan_to_zero(rad.y), nan_to_zero(rad.z), nan_to_zero(light));
-				// an occluded connection adds (throughput * 0) * 0
-				const f3 zr = (full * 0.0f) * make3(0.0f, 0.0f, 0.0f);
-				const float zl = __fdiv_rn((full.x + full.y) + full.z, 3.0f) * 0.0f;
-				c.zeroSigns = (__float_as_uint(nan_to_zero(zr.x)) >> 31) | ((__float_as_uint(nan_to_zero(zr.y)) >> 31) << 1) |
-				              ((__float_as_uint(nan_to_zero(zr.z)) >> 31) << 2) | ((__float_as_uint(nan_to_zero(zl)) >> 31) << 3);
+				c.zeroSigns = zero_signs(full, __fdiv_rn((full.x + full.y) + full.z, 3.0f));
 				return 1;
 			}
 		}
 	}
 	if(ox == -1) return -1;
 	c.pix = uint32_t(oy) * width + uint32_t(ox);
+	const f3 full = thr * w.throughput;
+	c.zeroSigns = zero_signs(full, __fdiv_rn((full.x + full.y) + full.z, 3.0f));
 	return 0;
-}
-
-MBD float4 bpt_zeros(unsigned signs) {
-	return make_float4(__uint_as_float((signs & 1u) << 31), __uint_as_float(((signs >> 1) & 1u) << 31),
-	                   __uint_as_float(((signs >> 2) & 1u) << 31), __uint_as_float(((signs >> 3) & 1u) << 31));
 }
 
 // get_emission (path_util.hpp:410-458) and the random-hit weight
@@ -323,10 +124,6 @@ struct BptRec {
 	}
 };
 
-MBD void bpt_add(const LtTargets& T, uint32_t pix, float4 v) {
-	if(v.x != 0.0f || v.y != 0.0f || v.z != 0.0f || v.w != 0.0f) atomicAdd(T.iter + pix, v);
-}
-
 // cpu_bpt.cpp:170-232 as a per-lane state machine
 template < int AM >
 __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P, const LtTargets T, BV* lightVerts,
@@ -350,13 +147,7 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 	// the segment being traced
 	float segPdf = 0.0f;
 	auto start_view = [&]() {
-		BV& c = vp[0];
-		c.kind = BV_CAMERA;
-		c.position = lv(S.camera.position);
-		c.incEnc = make3(float(px), float(py), 0.0f);
-		c.incidentPdf = 1.0f;
-		c.prevRelSum = 0.0f;
-		c.throughput = make3(1.0f, 1.0f, 1.0f);
+		bpt_camera_vertex(S, px, py, vp[0]);
 		(void)pcg_next(rng); // create_camera consumes one number (unused by the pinhole camera)
 		thr = make3(1.0f, 1.0f, 1.0f);
 		viewLen = 0;
@@ -416,7 +207,7 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 		const bool mine = phase == pick;
 		if(mine && phase == BP_LWALK) {
 			BV& v = lp[lightLen];
-			if(bpt_sample(S, v, lightLen > 0 ? &lp[lightLen - 1] : nullptr, px, py, rng, true, lthr, ro, rd, segPdf)) trace = true;
+			if(bpt_sample<false>(S, v, lightLen > 0 ? &lp[lightLen - 1] : nullptr, px, py, rng, true, lthr, ro, rd, segPdf)) trace = true;
 			else start_view();
 		}
 		if(mine && !trace && phase == BP_VCONNECT) {
@@ -429,14 +220,14 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 					trace = shadow = true;
 					break;
 				}
-				if(k == 0) rec.put(size_t(viewLen) * size_t(maxP) + size_t(l), conn.pix, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+				if(k == 0) rec.put(size_t(viewLen) * size_t(maxP) + size_t(l), conn.pix, bpt_zeros(conn.zeroSigns));
 				++l;
 			}
 			if(!trace) phase = BP_VWALK;
 		}
 		if(mine && pick == BP_VWALK && !trace && phase == BP_VWALK) {
 			BV& v = vp[cur];
-			if(bpt_sample(S, v, viewLen > 0 ? &vp[1 - cur] : nullptr, px, py, rng, false, thr, ro, rd, segPdf)) {
+			if(bpt_sample<false>(S, v, viewLen > 0 ? &vp[1 - cur] : nullptr, px, py, rng, false, thr, ro, rd, segPdf)) {
 				trace = true;
 				tmax = MAX_SCENE_SIZE;
 			} else finish();
@@ -455,13 +246,13 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 		} else if(phase == BP_LWALK) {
 			if(!t.best.has) start_view();
 			else {
-				bpt_new_vertex(S, lp[lightLen], ro, rd, t.best, segPdf, lthr, lp[lightLen + 1]);
+				bpt_new_vertex<false>(S, lp[lightLen], ro, rd, t.best, segPdf, lthr, lp[lightLen + 1]);
 				++lightLen;
 				if(lightLen >= maxP - 1) start_view();
 			}
 		} else {
 			const int nxt = 1 - cur;
-			bpt_new_vertex(S, vp[cur], ro, rd, t.best, segPdf, thr, vp[nxt]);
+			bpt_new_vertex<false>(S, vp[cur], ro, rd, t.best, segPdf, thr, vp[nxt]);
 			++viewLen;
 			cur = nxt;
 			const BV& h = vp[cur];
@@ -511,36 +302,6 @@ __global__ void __launch_bounds__(128, 4) k_bpt(const DScene S, const LtParams P
 // generation maxPathLength - 1 + k of the view phase those from view vertex
 // k and the connections of view vertex k. Queue state (BptwState) lives in
 // one device allocation carved by bptw_carve.
-enum { BPTW_EXT0 = 0, BPTW_SH0 = 2, BPTW_WORK = 4 };
-constexpr int BPTW_COUNTERS = 4 + 2 * BPTW_MAX_PATH;
-
-struct BptwState {
-	BV* lv;             // light subpath vertices: vertex l of pixel p at l * n + p
-	BV* vp[2];          // the view vertex with path length k of pixel p at vp[k & 1][p]
-	float4* thr;        // per pixel: throughput of the subpath being walked, the pdf of its segment in w
-	int* lightLen;      // per pixel: index of the light subpath's last vertex (-1: no light)
-	int* qPixel[2];     // segment queues (double buffered by generation)
-	float4* qOrg[2];    // origin (offset)
-	float4* qDir[2];    // direction
-	float4* qHit[2];    // t, instance bits, primitive bits, surface u
-	float* qHitV[2];    // surface v
-	float4* sOrg;       // connections: origin, length
-	float4* sDir;       // direction
-	float4* sAdd;       // radiance rgb, lightness if unoccluded
-	uint4* sMeta;       // pixel, record slot (low, high word), sign bits of the occluded zeros
-	unsigned* counters; // BPTW_COUNTERS
-	uint32_t n;
-};
-
-MBD void bptw_queue_segment(const BptwState& W, int gen, uint32_t p, f3 o, f3 d, f3 thr, float pdf) {
-	const int q = gen & 1;
-	const unsigned i = queue_reserve(W.counters + BPTW_EXT0 + q);
-	W.qPixel[q][i] = int(p);
-	W.qOrg[q][i] = make_float4(o.x, o.y, o.z, 0.0f);
-	W.qDir[q][i] = make_float4(d.x, d.y, d.z, 0.0f);
-	W.thr[p] = make_float4(thr.x, thr.y, thr.z, pdf);
-}
-
 // The connections of view vertex v (path length viewLen, predecessor pv) with
 // light vertices lo .. hi-1 of pixel p: shadow rays of generation gen, or
 // the zero records of those that carry nothing.
@@ -561,8 +322,9 @@ MBD void bptw_connect(const DScene& S, const LtParams& P, const LtTargets& T, co
 			W.sMeta[i] = make_uint4(c.pix, uint32_t(slot), uint32_t(slot >> 32), c.zeroSigns);
 		} else if(k == 0 && T.recPixel) {
 			T.recPixel[slot] = int(c.pix);
+			const float4 z = bpt_zeros(c.zeroSigns);
 			float* o = T.recValue + 4 * slot;
-			o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f; o[3] = 0.0f;
+			o[0] = z.x; o[1] = z.y; o[2] = z.z; o[3] = z.w;
 		}
 	}
 }
@@ -585,86 +347,12 @@ __global__ void __launch_bounds__(128) k_bptw_light_start(const DScene S, const 
 		if(maxP > 1) {
 			f3 thr = make3(1.0f, 1.0f, 1.0f), o, d;
 			float pdf;
-			if(bpt_sample(S, v, nullptr, 0, 0, rng, true, thr, o, d, pdf)) bptw_queue_segment(W, 0, p, o, d, thr, pdf);
+			if(bpt_sample<false>(S, v, nullptr, 0, 0, rng, true, thr, o, d, pdf)) bptw_queue_segment(W, 0, p, o, d, thr, pdf);
 		}
 		W.lv[p] = v;
 	}
 	W.lightLen[p] = lightLen;
 	T.rngState[p] = rng;
-}
-
-// The trace stage of generation gen: segments (closest hit) and connections
-// (any hit; a visible one adds its value, each one records what it added).
-template < int AM >
-__global__ void __launch_bounds__(128, 6) k_bptw_trace(const DScene S, const LtTargets T, BptwState W, int gen,
-                                                    TraceCounters* counters) {
-	const int q = gen & 1;
-	if(blockIdx.x == 0 && threadIdx.x == 0) {
-		W.counters[BPTW_EXT0 + (q ^ 1)] = 0u; // filled by this generation's shade
-		W.counters[BPTW_SH0 + (q ^ 1)] = 0u;
-	}
-	RayQueue Q;
-	Q.org = W.qOrg[q]; Q.dir = W.qDir[q]; Q.hit = W.qHit[q]; Q.hitV = W.qHitV[q];
-	Q.sOrg = W.sOrg; Q.sDir = W.sDir;
-	Q.nExt = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
-	Q.nSh = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_SH0 + q);
-	Q.work = W.counters + BPTW_WORK + gen;
-	trace_ray_queue<AM>(S, Q, counters, [&](unsigned s, bool occluded) {
-		const uint4 meta = __ldcs(W.sMeta + s);
-		float4 add;
-		if(occluded) add = bpt_zeros(meta.w);
-		else {
-			add = __ldcs(W.sAdd + s);
-			bpt_add(T, meta.x, add);
-		}
-		if(T.recPixel) {
-			const size_t slot = size_t(meta.y) | (size_t(meta.z) << 32);
-			T.recPixel[slot] = int(meta.x);
-			float* o = T.recValue + 4 * slot;
-			o[0] = add.x; o[1] = add.y; o[2] = add.z; o[3] = add.w;
-		}
-	});
-}
-
-MBD HitRec bptw_hit(const BptwState& W, int q, unsigned i) {
-	const float4 hh = __ldcs(W.qHit[q] + i);
-	HitRec hr;
-	hr.t = hh.x;
-	hr.inst = __float_as_int(hh.y);
-	hr.prim = __float_as_int(hh.z);
-	hr.sp = make2(hh.w, __ldcs(W.qHitV[q] + i));
-	hr.has = hr.inst >= 0;
-	return hr;
-}
-
-// Light phase, generation g: a segment from light vertex g that hit a surface
-// becomes vertex g + 1, which takes the next segment unless it is the last
-// one the path length allows.
-__global__ void __launch_bounds__(128, 4) k_bptw_light_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
-                                                          int g) {
-	const int q = g & 1;
-	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
-	const int maxP = P.maxPathLength > 0 ? P.maxPathLength : 1;
-	for(unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-		const HitRec hr = bptw_hit(W, q, i);
-		if(!hr.has) continue; // the light subpath ends with vertex g
-		const uint32_t p = uint32_t(__ldcs(W.qPixel[q] + i));
-		const f3 ro = f4to3(__ldcs(W.qOrg[q] + i)), rd = f4to3(__ldcs(W.qDir[q] + i));
-		const float4 tp = W.thr[p];
-		f3 thr = f4to3(tp);
-		const BV* from = W.lv + size_t(g) * W.n + p;
-		BV v;
-		bpt_new_vertex(S, *from, ro, rd, hr, tp.w, thr, v);
-		W.lightLen[p] = g + 1;
-		if(g + 1 < maxP - 1) {
-			u64 rng = T.rngState[p];
-			f3 o, d;
-			float pdf;
-			if(bpt_sample(S, v, from, 0, 0, rng, true, thr, o, d, pdf)) bptw_queue_segment(W, g + 1, p, o, d, thr, pdf);
-			T.rngState[p] = rng;
-		}
-		W.lv[size_t(g + 1) * W.n + p] = v;
-	}
 }
 
 // View phase, first generation (gen): every pixel's camera vertex, its
@@ -677,19 +365,14 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_start(const DScene S, cons
 	const int px = int(p % T.width), py = int(p / T.width);
 	u64 rng = T.rngState[p];
 	BV c;
-	c.kind = BV_CAMERA;
-	c.position = lv(S.camera.position);
-	c.incEnc = make3(float(px), float(py), 0.0f);
-	c.incidentPdf = 1.0f;
-	c.prevRelSum = 0.0f;
-	c.throughput = make3(1.0f, 1.0f, 1.0f);
+	bpt_camera_vertex(S, px, py, c);
 	(void)pcg_next(rng); // create_camera consumes one number (unused by the pinhole camera)
 	f3 thr = make3(1.0f, 1.0f, 1.0f);
 	const int lightLen = W.lightLen[p];
 	bptw_connect(S, P, T, W, c, nullptr, 0, p, px, py, thr, max(0, P.minPathLength - 1), min(lightLen + 1, maxP), gen);
 	f3 o, d;
 	float pdf;
-	if(bpt_sample(S, c, nullptr, px, py, rng, false, thr, o, d, pdf)) {
+	if(bpt_sample<false>(S, c, nullptr, px, py, rng, false, thr, o, d, pdf)) {
 		bptw_queue_segment(W, gen, p, o, d, thr, pdf);
 		W.vp[0][p] = c;
 	}
@@ -714,7 +397,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_shade(const DScene S, cons
 		f3 thr = f4to3(tp);
 		const BV pv = W.vp[k & 1][p];
 		BV h;
-		bpt_new_vertex(S, pv, ro, rd, hr, tp.w, thr, h);
+		bpt_new_vertex<false>(S, pv, ro, rd, hr, tp.w, thr, h);
 		if(viewLen >= P.minPathLength) {
 			const float4 add = bpt_emission(S, h, pv, thr);
 			bpt_add(T, p, add);
@@ -733,58 +416,12 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_shade(const DScene S, cons
 		u64 rng = T.rngState[p];
 		f3 o, d;
 		float pdf;
-		if(bpt_sample(S, h, &pv, px, py, rng, false, thr, o, d, pdf)) {
+		if(bpt_sample<false>(S, h, &pv, px, py, rng, false, thr, o, d, pdf)) {
 			bptw_queue_segment(W, gen + 1, p, o, d, thr, pdf);
 			W.vp[viewLen & 1][p] = h;
 		}
 		T.rngState[p] = rng;
 	}
-}
-
-int bptw_trace_blocks() {
-	static int blocks = 0;
-	if(blocks == 0) {
-		int dev = 0, sms = 148, a = 0, b = 0;
-		cudaGetDevice(&dev);
-		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_bptw_trace<ALPHA_NEVER>, 128, 0);
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bptw_trace<ALPHA_ALWAYS>, 128, 0);
-		blocks = sms * std::max(1, std::min(a, b));
-	}
-	return blocks;
-}
-
-size_t bptw_size(size_t n, size_t m) {
-	auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-	return al(n * m * sizeof(BV)) + 2 * al(n * sizeof(BV)) + al(n * 16) + al(n * 4) +
-	       2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) + 4 * al(n * m * 16) + al(BPTW_COUNTERS * sizeof(unsigned));
-}
-
-BptwState bptw_carve(void* memory, size_t n, size_t m) {
-	auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-	char* mem = static_cast<char*>(memory);
-	auto take = [&](size_t b) { char* r = mem; mem += al(b); return r; };
-	BptwState W;
-	W.n = uint32_t(n);
-	W.lv = reinterpret_cast<BV*>(take(n * m * sizeof(BV)));
-	W.vp[0] = reinterpret_cast<BV*>(take(n * sizeof(BV)));
-	W.vp[1] = reinterpret_cast<BV*>(take(n * sizeof(BV)));
-	W.thr = reinterpret_cast<float4*>(take(n * 16));
-	W.lightLen = reinterpret_cast<int*>(take(n * 4));
-	for(int q = 0; q < 2; ++q) {
-		W.qPixel[q] = reinterpret_cast<int*>(take(n * 4));
-		W.qOrg[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qDir[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qHit[q] = reinterpret_cast<float4*>(take(n * 16));
-		W.qHitV[q] = reinterpret_cast<float*>(take(n * 4));
-	}
-	// a view vertex has at most max. path length connections
-	W.sOrg = reinterpret_cast<float4*>(take(n * m * 16));
-	W.sDir = reinterpret_cast<float4*>(take(n * m * 16));
-	W.sAdd = reinterpret_cast<float4*>(take(n * m * 16));
-	W.sMeta = reinterpret_cast<uint4*>(take(n * m * 16));
-	W.counters = reinterpret_cast<unsigned*>(take(BPTW_COUNTERS * sizeof(unsigned)));
-	return W;
 }
 
 // output_handler_variance.hpp:7-31: running means and variances
@@ -857,7 +494,7 @@ cudaError_t launch_bpt(const DScene& S, const LtParams& P, const LtTargets& T, v
 		const int lightGens = maxP - 1;
 		for(int g = 0; g < lightGens; ++g) {
 			trace(g);
-			k_bptw_light_shade<<<sms * 4, 128, 0, stream>>>(S, P, T, W, g);
+			k_bptw_light_shade<false><<<sms * 4, 128, 0, stream>>>(S, P, T, W, g);
 		}
 		k_bptw_view_start<<<(n + 127) / 128, 128, 0, stream>>>(S, P, T, W, lightGens);
 		for(int k = 0; k < maxP; ++k) {

@@ -64,6 +64,30 @@ size_t bptw_bytes(size_t numPixels, int maxPathLength);
 cudaError_t launch_bpt(const DScene& scene, const LtParams& params, const LtTargets& targets, void* scratch,
                        unsigned int* workCounter, TraceCounters* counters, cudaStream_t stream, void* wavefront);
 
+// vcm_params.hpp:8-14 beyond the light tracer's three: "Relative merge
+// radius" (of the scene's diagonal, default 0.001) and "Progressive" (the
+// radius shrinks as iteration^(-1/6)).
+struct VcmSettings {
+	float mergeRadius;
+	int32_t progressive;
+};
+
+// The photon map's bucket count for `capacity` photon slots
+// (photon_map.hpp:216-229), and the device memory of one vertex connection
+// and merging iteration over numPixels pixels: the bidirectional stages'
+// state plus the photon grid (keys, sort buffers, bucket ranges, 80 B of merge
+// data per photon slot).
+uint32_t vcm_map_size(uint32_t capacity);
+size_t vcm_bytes(size_t numPixels, int maxPathLength);
+
+// One vertex connection and merging iteration (cpu_vcm.cpp:148-290) in stages
+// per path length, into the light tracer's targets (radiance, lightness);
+// records hold 4 floats per slot, M*M + 2M slots per pixel for max. path
+// length M (connections [view length][light vertex], emitter hits and merges
+// [view length - 1]). memory: vcm_bytes bytes.
+cudaError_t launch_vcm(const DScene& scene, const LtParams& params, const VcmSettings& vcm, const LtTargets& targets,
+                       TraceCounters* counters, cudaStream_t stream, void* memory);
+
 // wireframe_params.hpp:6-26
 struct WireParams {
 	float lineWidth;        // "Line width" in pixels (default 1)

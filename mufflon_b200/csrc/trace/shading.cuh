@@ -229,8 +229,11 @@ MBD PathSample material_sample(const TangentSpace& ts, const Params& p, f3 incid
 // material_sampling.hpp:156-237 (no merge normal). adjoint: a light sub-path
 // vertex; the tangent-space directions are swapped for the BSDF, the value
 // gets the shading-normal correction and the pdfs are swapped back.
+// lightNormal (material_sampling.hpp:173, 217-220): a merge evaluates the view
+// vertex's material with the photon's geometric normal in the shadow-masking
+// test and corrects the value by |cos| at the shading over the geometric normal.
 MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 incident, f3 excident,
-                                bool adjoint = false) {
+                                bool adjoint = false, const f3* lightNormal = nullptr) {
 	EvalValue none; none.value = make3(0, 0, 0); none.cosOut = 0.0f; none.pdfF = none.pdfB = 0.0f;
 	const float iDotN = -dot(incident, ts.shadingN);
 	const float eDotN = dot(excident, ts.shadingN);
@@ -240,8 +243,9 @@ MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 inci
 	} else {
 		if(iDotN * eDotN < 0.0f) return none;
 	}
-	const float iDotG = -dot(incident, ts.geoN);
-	const float eDotG = dot(excident, ts.geoN);
+	const f3 geoN = lightNormal ? *lightNormal : ts.geoN;
+	const float iDotG = -dot(incident, geoN);
+	const float eDotG = dot(excident, geoN);
 	if(eDotG * eDotN <= 0.0f || iDotG * iDotN <= 0.0f) return none;
 	f3 inTS = make3(-dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN);
 	f3 exTS = make3(dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN);
@@ -276,7 +280,9 @@ MBD EvalValue material_evaluate(const TangentSpace& ts, const Params& p, f3 inci
 	}
 	if(!nonzero(value)) return none;
 	EvalValue r; r.value = value; r.cosOut = fabsf(eDotN); r.pdfF = fmin_(pf, 1e9f); r.pdfB = fmin_(pb, 1e9f);
-	if(adjoint) {
+	if(lightNormal) {
+		r.value = value * __fdiv_rn(SHADING_NORMAL_EPS + fabsf(eDotN), SHADING_NORMAL_EPS + fabsf(eDotG));
+	} else if(adjoint) {
 		r.value = value * __fdiv_rn(SHADING_NORMAL_EPS + fabsf(iDotN * eDotG), SHADING_NORMAL_EPS + fabsf(iDotG * eDotN));
 		r.pdfF = fmin_(pb, 1e9f); r.pdfB = fmin_(pf, 1e9f);
 	}

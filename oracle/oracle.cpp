@@ -1480,10 +1480,14 @@ PathSample material_sample(const TangentSpace& ts, const Params& p, V3 incident,
 	return res;
 }
 
-// material_sampling.hpp:156-237 (no merge normal). adjoint: a light sub-path
-// vertex; the tangent-space directions are swapped for the BSDF, the value
-// gets the shading-normal correction and the pdfs are swapped back.
-EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident, V3 excident, bool adjoint = false) {
+// material_sampling.hpp:156-237. adjoint: a light sub-path vertex; the
+// tangent-space directions are swapped for the BSDF, the value gets the
+// shading-normal correction and the pdfs are swapped back. lightNormal: a
+// merge; the photon's geometric normal replaces the vertex's in the
+// shadow-masking test and the value gets |cos| at the shading over the
+// geometric normal (:173, 217-220).
+EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident, V3 excident, bool adjoint = false,
+                            const V3* lightNormal = nullptr) {
 	EvalValue none = { { 0, 0, 0 }, 0, 0, 0 };
 	const float iDotN = -dot(incident, ts.shadingN);
 	const float eDotN = dot(excident, ts.shadingN);
@@ -1494,8 +1498,9 @@ EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident
 	} else {
 		if(iDotN * eDotN < 0.0f) return none; // not refractive
 	}
-	const float iDotG = -dot(incident, ts.geoN);
-	const float eDotG = dot(excident, ts.geoN);
+	const V3 geoN = lightNormal ? *lightNormal : ts.geoN;
+	const float iDotG = -dot(incident, geoN);
+	const float eDotG = dot(excident, geoN);
 	if(eDotG * eDotN <= 0.0f || iDotG * iDotN <= 0.0f) return none;
 	V3 inTS = { -dot(incident, ts.shadingTX), -dot(incident, ts.shadingTY), iDotN };
 	V3 exTS = { dot(excident, ts.shadingTX), dot(excident, ts.shadingTY), eDotN };
@@ -1529,6 +1534,10 @@ EvalValue material_evaluate(const TangentSpace& ts, const Params& p, V3 incident
 		return none;
 	}
 	if(!nonzero(value)) return none;
+	if(lightNormal) {
+		value = value * ((SHADING_NORMAL_EPS + std::fabs(eDotN)) / (SHADING_NORMAL_EPS + std::fabs(eDotG)));
+		return { value, std::fabs(eDotN), fmin_(pf, 1e9f), fmin_(pb, 1e9f) };
+	}
 	if(adjoint) {
 		value = value * ((SHADING_NORMAL_EPS + std::fabs(iDotN * eDotG)) / (SHADING_NORMAL_EPS + std::fabs(iDotG * eDotN)));
 		return { value, std::fabs(eDotN), fmin_(pb, 1e9f), fmin_(pf, 1e9f) };
@@ -2602,6 +2611,8 @@ struct BVertex {
 	float incidentPdf;  // BptVertexExt::incidentPdf
 	float prevRelSum;   // BptVertexExt::prevRelativeProbabilitySum
 	V3 throughput;      // BptVertexExt::throughput
+	i32 pathLen;        // PathVertex::m_pathLen
+	float prevConv;     // VcmVertexExt::prevConversionFactor
 };
 
 inline bool bv_ortho(BKind k) { return k == BV_VOID || k == BV_ENV; }           // path_util.hpp:41-46
@@ -2685,11 +2696,27 @@ struct BptState {
 
 inline size_t bpt_slots(i32 maxPath) { return size_t(maxPath) * size_t(maxPath) + size_t(maxPath); }
 
+inline bool bv_hitable(BKind k) { return k == BV_SURFACE || k == BV_AREA || k == BV_ENV || k == BV_VOID; } // path_util.hpp:53-58
+
+// cpu_vcm.cpp:21-32: the relative probabilities of the events before v
+// (connections and merges) for the reverse sampling pdf pdfBack at v.
+float vcm_prev_rel_sum(const std::vector<BVertex>& path, const BVertex& v, float pdfBack, float nPhotons, float area) {
+	if(v.prev < 0) return 0.0f;
+	const BVertex& p = path[size_t(v.prev)];
+	const float pdfBackA = pdfBack * v.prevConv;
+	const float relMerge = p.prev >= 0 ? pdfBackA * nPhotons * area : 0.0f; // no merges at start points
+	const float relConn = pdfBackA / p.incidentPdf;
+	return relConn + relMerge + relConn * p.prevRelSum;
+}
+
 // random_walk.hpp:38-113 for a BPT vertex: samples v (updating its MIS
 // extension), applies Russian roulette and traces; out gets the next vertex.
 // Returns 0: cancelled, 1: hit, 2: miss (out is a void vertex).
+// vcm: null for the bidirectional path tracer; for vertex connection and
+// merging the number of light subpaths and the merge area (VcmVertexExt's
+// updates, cpu_vcm.cpp:117-146).
 int bpt_walk(const Scene& S, std::vector<BVertex>& path, i32 vi, const OrLtParams& P, i32 px, i32 py, Pcg64& rng,
-             bool adjoint, V3& throughput, BVertex& out, Counters& cnt) {
+             bool adjoint, V3& throughput, BVertex& out, Counters& cnt, const float* vcm = nullptr) {
 	BVertex& v = path[size_t(vi)];
 	const u64 x0 = rng.next(), x1 = rng.next();
 	const float ru0 = sample_uniform(u32(x0)), ru1 = sample_uniform(u32(x0 >> 32));
@@ -2736,8 +2763,9 @@ int bpt_walk(const Scene& S, std::vector<BVertex>& path, i32 vi, const OrLtParam
 		}
 		default: return 0;
 	}
-	// BptVertexExt::update after sampling (cpu_bpt.cpp:49-58)
-	if(v.prev >= 0) {
+	// BptVertexExt::update after sampling (cpu_bpt.cpp:49-58), or VcmVertexExt's
+	if(vcm) v.prevRelSum = vcm_prev_rel_sum(path, v, pdfB, vcm[0], vcm[1]);
+	else if(v.prev >= 0) {
 		const BVertex& p = path[size_t(v.prev)];
 		const float prevReversePdf = bv_convert_pdf(p, v.kind, pdfB, bv_incident_dir(v), bv_incident_dist_sq(v));
 		const float relToPrev = prevReversePdf / p.incidentPdf;
@@ -2750,6 +2778,7 @@ int bpt_walk(const Scene& S, std::vector<BVertex>& path, i32 vi, const OrLtParam
 	const Intersection hit = first_intersection(S, origin, excident, bv_geo_normal(v), MAX_SCENE_SIZE, cnt);
 	out = BVertex{};
 	out.prev = vi;
+	out.pathLen = v.pathLen + 1;
 	out.prevRelSum = 0.0f;
 	out.inst = out.prim = -1;
 	if(hit.inst < 0) {
@@ -2771,6 +2800,10 @@ int bpt_walk(const Scene& S, std::vector<BVertex>& path, i32 vi, const OrLtParam
 	const bool ortho = bv_ortho(v.kind) || bv_ortho(out.kind);
 	out.incidentPdf = ortho ? pdfF * inCosAbs : pdfF * std::fabs(inCosAbs) / (hit.distance * hit.distance);
 	out.throughput = throughput;
+	if(vcm && bv_hitable(v.kind)) {
+		const float outCosAbs = std::fabs(bv_geo_factor(v, excident));
+		out.prevConv = ortho ? outCosAbs : outCosAbs / (hit.distance * hit.distance);
+	}
 	return hit.inst < 0 ? 2 : 1;
 }
 
@@ -2944,6 +2977,346 @@ void bpt_iterate(BptState& st, int numThreads) {
 	const float itf = float(st.iteration);
 	for(size_t p = 0; p < n; ++p) {
 		for(int c = 0; c < 3; ++c) update_moments(iter[4 * p + size_t(c)], st.radiance[3 * p + size_t(c)], st.radianceVar[3 * p + size_t(c)], itf);
+		update_moments(iter[4 * p + 3], st.lightness[p], st.lightnessVar[p], itf);
+	}
+}
+
+// ---------------------------------------------------------------- vertex connection and merging
+// cpu_vcm.cpp:1-298: one light subpath per pixel, all of them stored as
+// photons in a hash grid (data_structs/photon_map.hpp); then per pixel a view
+// subpath whose vertices connect to every vertex of one light subpath (chosen
+// by a hash of the pixel index), count the emitters they hit, and merge with
+// the photons within the merge radius. All estimates share one balance
+// heuristic over connections and merges (VcmVertexExt, cpu_vcm.cpp:17-146).
+//
+// The hash grid here is deterministic: the reference inserts photons from
+// parallel threads at the head of each bucket's list, so its buckets hold
+// them in reverse insertion order; this restatement visits a bucket's photons
+// in descending (light subpath, vertex) order, the reference's order for a
+// single thread.
+
+// photon_map.hpp:29-52: the cell of a position and the hash of a cell
+constexpr u32 VCM_MAGIC[3] = { 0xb286aff7u, 0x35e4a487u, 0x75a9c18fu };
+// An integral float as the grid's unsigned coordinate (two's complement wrap
+// for negative cells, as the conversion does on the reference's x86 hosts).
+inline u32 vcm_cell_coord(float x) { return u32(int64_t(x)); }
+inline u32 vcm_cell_hash(u32 x, u32 y, u32 z) { return x * VCM_MAGIC[0] + y * VCM_MAGIC[1] + z * VCM_MAGIC[2]; }
+// HashGrid::insert: the cell is ceil(position / cell edge)
+inline u32 vcm_insert_hash(V3 p, float density) {
+	return vcm_cell_hash(vcm_cell_coord(std::ceil(p.x * density)), vcm_cell_coord(std::ceil(p.y * density)),
+	                     vcm_cell_coord(std::ceil(p.z * density)));
+}
+// HashGrid::find_first: the query's base cell is round(position / cell edge);
+// the 8 cells base + {0, 1}^3 cover a disc of half the cell edge
+inline u32 vcm_query_hash(V3 p, float density) {
+	return vcm_cell_hash(vcm_cell_coord(std::round(p.x * density)), vcm_cell_coord(std::round(p.y * density)),
+	                     vcm_cell_coord(std::round(p.z * density)));
+}
+inline u32 vcm_query_bucket(u32 baseHash, int cell, u32 mapSize) {
+	u32 h = baseHash;
+	if(cell & 1) h += VCM_MAGIC[0];
+	if(cell & 2) h += VCM_MAGIC[1];
+	if(cell & 4) h += VCM_MAGIC[2];
+	return h % mapSize;
+}
+// HashGridManager::resize (photon_map.hpp:216-229): the next prime above
+// 1.15 x the capacity that is 3 mod 4
+u32 vcm_map_size(u32 capacity) {
+	auto prime = [](u32 v) {
+		if(v < 2) return false;
+		for(u32 d = 2; u64(d) * d <= v; ++d) if(v % d == 0) return false;
+		return true;
+	};
+	u32 v = u32(float(capacity) * 1.15f);
+	do { ++v; while(!prime(v)) ++v; } while((v & 3u) != 3u);
+	return v;
+}
+// Thomas Wang's 32-bit integer hash (cn::WangHash of the reference's
+// cn/rnd.hpp, a dependency the reference does not vendor)
+inline u32 wang_hash(u32 x) {
+	x = (x ^ 61u) ^ (x >> 16);
+	x = x * 9u;
+	x = x ^ (x >> 4);
+	x = x * 0x27d4eb2du;
+	x = x ^ (x >> 15);
+	return x;
+}
+
+struct VcmState {
+	const Scene* scene;
+	OrLtParams params;
+	float mergeRadius;      // "Relative merge radius": of the scene's diagonal
+	bool progressive;       // "Progressive": the radius shrinks with iteration^(-1/6)
+	std::vector<Pcg64> rngs;
+	std::vector<float> radiance, lightness, radianceVar, lightnessVar;
+	std::vector<i32> recPixel; // per pixel: connections [view length][light vertex], hits [view length - 1], merges [view length - 1]
+	std::vector<float> recValue;
+	i32 iteration = -1;
+	Counters stats;
+};
+
+inline size_t vcm_slots(i32 maxPath) { return size_t(maxPath) * size_t(maxPath) + 2 * size_t(maxPath); }
+
+// path_util.hpp:568-625 create_light and mis_start_pdf (:763-771)
+BVertex vcm_light_vertex(const Scene& S, const Emitter& em) {
+	BVertex l0 = BVertex{};
+	l0.prev = -1;
+	l0.position = em.position;
+	l0.throughput = { 1, 1, 1 };
+	if(em.kind == LV_POINT) { l0.kind = BV_POINT; l0.incEnc = em.intensity; l0.incidentPdf = em.pChoice; }
+	else if(em.kind == LV_AREA) { l0.kind = BV_AREA; l0.incEnc = em.normal; l0.intensity = em.intensity; l0.incidentPdf = em.pdf * em.pChoice; }
+	else {
+		l0.kind = BV_ENV; l0.incEnc = em.normal; l0.intensity = em.intensity; l0.incidentPdf = em.pdf * em.pChoice;
+		l0.position = { 0, 0, 0 };
+		l0.projSceneArea = projected_area(-em.normal, S.aabb);
+	}
+	return l0;
+}
+
+// cpu_vcm.cpp:50-68: the weight of a connection of view vertex v with light vertex w
+float vcm_connection_weight(const std::vector<BVertex>& vpath, const BVertex& v, const EvalValue& vPdf,
+                            const std::vector<BVertex>& lpath, const BVertex& w, const EvalValue& lPdf, V3 dir,
+                            float distSq, float nPhotons, float area) {
+	float relSumV = 1.0f + vcm_prev_rel_sum(vpath, v, vPdf.pdfB, nPhotons, area);
+	float relSumL = 1.0f + vcm_prev_rel_sum(lpath, w, lPdf.pdfB, nPhotons, area);
+	const float lightToView = bv_convert_pdf(v, w.kind, lPdf.pdfF, dir, distSq);
+	relSumV *= lightToView / v.incidentPdf;
+	if(v.prev >= 0) relSumV += lightToView * nPhotons * area;
+	const float viewToLight = bv_convert_pdf(w, v.kind, vPdf.pdfF, dir, distSq);
+	relSumL *= viewToLight / w.incidentPdf;
+	if(w.prev >= 0) relSumL += viewToLight * nPhotons * area;
+	return 1.0f / (1.0f + relSumV + relSumL);
+}
+
+// cpu_vcm.cpp:35-47: the weight of a merge of view vertex v with photon w
+float vcm_merge_weight(const std::vector<BVertex>& vpath, const BVertex& v, const EvalValue& pdf,
+                       const std::vector<BVertex>& lpath, const BVertex& w, float nPhotons, float area) {
+	float relSumV = 1.0f + vcm_prev_rel_sum(vpath, v, pdf.pdfB, nPhotons, area);
+	float relSumL = 1.0f + vcm_prev_rel_sum(lpath, w, pdf.pdfF, nPhotons, area);
+	relSumV /= v.incidentPdf * nPhotons * area;
+	relSumL /= w.incidentPdf * nPhotons * area;
+	return 1.0f / (1.0f + relSumV + relSumL);
+}
+
+// cpu_vcm.cpp:71-78: the weight of an emitter or the background hit at v
+float vcm_hit_weight(const std::vector<BVertex>& vpath, const BVertex& v, float pdfBack, float startPdf, float nPhotons,
+                     float area) {
+	float relSum = 1.0f + vcm_prev_rel_sum(vpath, v, pdfBack, nPhotons, area);
+	const float relRndHit = startPdf / v.incidentPdf;
+	relSum *= relRndHit;
+	return 1.0f / (1.0f + relSum);
+}
+
+struct VcmGrid {
+	float density = 1.0f;        // 1 / cell edge
+	u32 mapSize = 1;
+	std::vector<u32> start, end; // per bucket: range in keys
+	std::vector<u32> keys;       // light subpath * max. path length + vertex, by bucket then ascending
+};
+
+void vcm_iterate(VcmState& st, int numThreads) {
+	const Scene& S = *st.scene;
+	const OrLtParams& P = st.params;
+	const u32 n = S.width * S.height;
+	const i32 maxP = std::max(1, P.maxPathLength);
+	const size_t slots = vcm_slots(maxP);
+	++st.iteration;
+	st.recPixel.assign(size_t(n) * slots, -1);
+	st.recValue.assign(size_t(n) * slots * 4, 0.0f);
+	// CpuVcm::iterate (cpu_vcm.cpp:148-172)
+	const float diag = len(S.aabb.mx - S.aabb.mn); // SceneDescriptor::diagSize (scene.cpp:377)
+	float radius = st.mergeRadius * diag;
+	if(st.progressive) radius *= std::pow(float(st.iteration + 1), -1.0f / 6.0f);
+	const float nPhotons = float(n);
+	const float lightArea[2] = { nPhotons, PI * radius * radius };     // trace_photon's merge area
+	const float radiusSq = radius * radius;
+	const float viewArea[2] = { nPhotons, PI * radiusSq };             // sample's merge area
+	const u64 photonSeed = st.rngs[0].next();
+	std::vector<std::vector<BVertex>> lpaths(n);
+	std::vector<i32> lightLen(n, -1);
+	Counters total;
+	// first pass: one light subpath per pixel (CpuVcm::trace_photon, :191-218)
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(dynamic, 256)
+		for(i32 i = 0; i < i32(n); ++i) {
+			Pcg64& rng = st.rngs[size_t(i)];
+			const u64 r0 = rng.next();
+			const Emitter em = lights_emit(S, u64(i), n, photonSeed, sample_uniform(u32(r0)), sample_uniform(u32(r0 >> 32)));
+			if(!em.valid) continue; // no light in the scene at all
+			std::vector<BVertex>& lp = lpaths[size_t(i)];
+			lp.assign(size_t(maxP) + 1, BVertex{});
+			lp[0] = vcm_light_vertex(S, em);
+			V3 thr = { 1, 1, 1 };
+			i32 len = 0;
+			while(len < maxP - 1) {
+				if(bpt_walk(S, lp, len, P, 0, 0, rng, true, thr, lp[size_t(len) + 1], local, lightArea) != 1) break;
+				++len;
+			}
+			lightLen[size_t(i)] = len;
+		}
+#pragma omp critical
+		total.add(local);
+	}
+	// the photon map: every light vertex after the start (vertex 0 is never merged)
+	VcmGrid G;
+	G.density = 1.0f / (radius * 2.0001f);
+	G.mapSize = vcm_map_size(n * u32(maxP));
+	{
+		std::vector<std::pair<u32, u32>> e;
+		for(u32 i = 0; i < n; ++i)
+			for(i32 l = 1; l <= lightLen[i]; ++l)
+				e.push_back({ vcm_insert_hash(lpaths[i][size_t(l)].position, G.density) % G.mapSize, i * u32(maxP) + u32(l) });
+		std::sort(e.begin(), e.end());
+		G.start.assign(G.mapSize, 0);
+		G.end.assign(G.mapSize, 0);
+		G.keys.resize(e.size());
+		for(size_t k = 0; k < e.size(); ++k) {
+			G.keys[k] = e[k].second;
+			if(k == 0 || e[k - 1].first != e[k].first) G.start[e[k].first] = u32(k);
+			G.end[e[k].first] = u32(k + 1);
+		}
+	}
+	// second pass: view subpaths (CpuVcm::sample, :220-290)
+#pragma omp parallel num_threads(numThreads)
+	{
+		Counters local;
+#pragma omp for schedule(dynamic, 256)
+		for(i32 pixel = 0; pixel < i32(n); ++pixel) {
+			const i32 px = pixel % i32(S.width), py = pixel / i32(S.width);
+			Pcg64& rng = st.rngs[size_t(pixel)];
+			i32* recPixel = &st.recPixel[size_t(pixel) * slots];
+			float* recValue = &st.recValue[size_t(pixel) * slots * 4];
+			auto put = [&](size_t slot, i32 pix, V3 rad, float light) {
+				recPixel[slot] = pix;
+				float* o = recValue + 4 * slot;
+				o[0] = nan_to_zero(rad.x); o[1] = nan_to_zero(rad.y); o[2] = nan_to_zero(rad.z); o[3] = nan_to_zero(light);
+			};
+			const u32 lightPath = wang_hash(u32(pixel)) % n;
+			const std::vector<BVertex>& lp = lpaths[lightPath];
+			const i32 lLen = lightLen[lightPath];
+			std::vector<BVertex> vpath(size_t(maxP) + 1);
+			BVertex& c = vpath[0];
+			c = BVertex{};
+			c.kind = BV_CAMERA;
+			c.prev = -1;
+			c.position = S.cam.position;
+			c.incEnc = { float(px), float(py), 0.0f };
+			c.incidentPdf = 1.0f;
+			c.throughput = { 1, 1, 1 };
+			(void)rng.next(); // create_camera consumes one number (unused by the pinhole camera)
+			V3 throughput = { 1, 1, 1 };
+			i32 viewLen = 0;
+			do {
+				// connections to every vertex of the light subpath, from its end (:232-246)
+				const BVertex& v = vpath[size_t(viewLen)];
+				for(i32 l = lLen; l >= 0; --l) {
+					const i32 pathLen = l + 1 + viewLen;
+					if(pathLen < P.minPathLength || pathLen > P.maxPathLength) continue;
+					const BVertex& w = lp[size_t(l)];
+					i32 ox = px, oy = py;
+					V3 bxdfs = { 0, 0, 0 };
+					float cosines = 0.0f;
+					if(!((bv_ortho(v.kind) && bv_ortho(w.kind)) || (bv_ortho(v.kind) && bv_camera(w.kind)) ||
+					     (bv_camera(v.kind) && bv_ortho(w.kind)))) {
+						V3 dir;
+						float distSq;
+						if(bv_ortho(w.kind)) { dir = -w.incEnc; distSq = 1.0f; }
+						else {
+							const V3 cv = w.position - v.position;
+							distSq = lensq(cv);
+							const float dist = mbmath::sqrt(distSq);
+							dir = { sdiv(cv.x, dist), sdiv(cv.y, dist), sdiv(cv.z, dist) };
+						}
+						const EvalValue val0 = bv_evaluate(S, v, dir, false, ox, oy);
+						const EvalValue val1 = bv_evaluate(S, w, -dir, true, ox, oy);
+						if(ox != -1) {
+							const V3 bxdfProd = val0.value * val1.value;
+							const float cosProd = val0.cosOut * val1.cosOut;
+							if(any_pos(bxdfProd) && cosProd > 0.0f &&
+							   !any_intersection(S, v.position, bv_position(w, v.position), bv_geo_normal(v), bv_geo_normal(w), dir, local)) {
+								const float mis = vcm_connection_weight(vpath, v, val0, lp, w, val1, dir, distSq, viewArea[0], viewArea[1]);
+								bxdfs = bxdfProd * (mis / distSq);
+								cosines = cosProd;
+							}
+						}
+					}
+					if(ox != -1)
+						put(size_t(viewLen) * size_t(maxP) + size_t(l), oy * i32(S.width) + ox,
+						    ((throughput * w.throughput) * cosines) * bxdfs, (((throughput.x + throughput.y) + throughput.z) / 3.0f) * cosines);
+				}
+				// walk (:249-256)
+				if(bpt_walk(S, vpath, viewLen, P, px, py, rng, false, throughput, vpath[size_t(viewLen) + 1], local, viewArea) == 0) break;
+				++viewLen;
+				const BVertex& h = vpath[size_t(viewLen)];
+				// emitters and the background (:259-268)
+				if(viewLen >= P.minPathLength) {
+					V3 value = { 0, 0, 0 };
+					float backPdf = 0.0f, startPdf = 0.0f;
+					if(h.kind == BV_VOID) {
+						const LightTree& T = S.lightTree;
+						if(T.hasBackground) {
+							value = T.bgColor * T.bgScale;
+							if(nonzero(value)) {
+								backPdf = 1.0f / projected_area(h.incEnc, S.aabb);
+								const float bgFlux = (T.bgFlux.x + T.bgFlux.y) + T.bgFlux.z;
+								const float p = bgFlux / ((T.dirFlux + T.rootFlux) + bgFlux);
+								startPdf = (1.0f / (4.0f * PI)) * p;
+							}
+						}
+					} else if(h.mat.type == OR_MAT_EMISSIVE) {
+						const float cosOut = dot(h.ts.geoN, -bv_incident_dir(h));
+						if(cosOut > 0.0f) {
+							value = h.mat.radiance;
+							backPdf = cosOut / PI;
+							if(nonzero(value)) startPdf = light_pdfs(S, h.inst, h.prim, h.sp, V3{ 0, 0, 0 }).emit;
+						}
+					}
+					if(nonzero(value)) value = value * vcm_hit_weight(vpath, h, backPdf, startPdf, viewArea[0], viewArea[1]);
+					put(size_t(maxP) * size_t(maxP) + size_t(viewLen - 1), pixel, throughput * value,
+					    (((throughput.x + throughput.y) + throughput.z) / 3.0f) * (((value.x + value.y) + value.z) / 3.0f));
+				}
+				if(bv_end(h.kind)) break;
+				// merges with the photons within the radius (:271-288)
+				V3 rad = { 0, 0, 0 };
+				const u32 base = vcm_query_hash(h.position, G.density);
+				for(int cell = 0; cell < 8; ++cell) {
+					const u32 b = vcm_query_bucket(base, cell, G.mapSize);
+					for(u32 k = G.end[b]; k > G.start[b];) {
+						--k;
+						const u32 key = G.keys[k];
+						const std::vector<BVertex>& ph = lpaths[key / u32(maxP)];
+						const i32 l = i32(key % u32(maxP));
+						const BVertex& w = ph[size_t(l)];
+						const i32 pathLen = viewLen + l;
+						if(l > 0 && pathLen >= P.minPathLength && pathLen <= P.maxPathLength && lensq(w.position - h.position) < radiusSq) {
+							const V3 geoN = w.ts.geoN;
+							const EvalValue bsdf = material_evaluate(h.ts, h.mat, bv_incident_dir(h), -bv_incident_dir(w), false, &geoN);
+							const float mis = vcm_merge_weight(vpath, h, bsdf, ph, w, viewArea[0], viewArea[1]);
+							rad = rad + (bsdf.value * w.throughput) * mis;
+						}
+					}
+				}
+				const float norm = viewArea[1] * viewArea[0];
+				rad = { rad.x / norm, rad.y / norm, rad.z / norm };
+				put(size_t(maxP) * size_t(maxP) + size_t(maxP) + size_t(viewLen - 1), pixel, throughput * rad,
+				    (((throughput.x + throughput.y) + throughput.z) / 3.0f) * (((rad.x + rad.y) + rad.z) / 3.0f));
+			} while(viewLen < maxP);
+		}
+#pragma omp critical
+		total.add(local);
+	}
+	st.stats.add(total);
+	std::vector<float> iter(size_t(n) * 4, 0.0f);
+	for(size_t k = 0; k < st.recPixel.size(); ++k) {
+		if(st.recPixel[k] < 0) continue;
+		float* dd = &iter[size_t(st.recPixel[k]) * 4];
+		for(int ch = 0; ch < 4; ++ch) dd[ch] += st.recValue[4 * k + size_t(ch)];
+	}
+	const float itf = float(st.iteration);
+	for(size_t p = 0; p < n; ++p) {
+		for(int ch = 0; ch < 3; ++ch) update_moments(iter[4 * p + size_t(ch)], st.radiance[3 * p + size_t(ch)], st.radianceVar[3 * p + size_t(ch)], itf);
 		update_moments(iter[4 * p + 3], st.lightness[p], st.lightnessVar[p], itf);
 	}
 }
@@ -3647,6 +4020,60 @@ int oracle_bpt_stats(void* p, OrStats* o) {
 	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
 	return 1;
 }
+
+void* oracle_vcm_create(void* s, const OrLtParams* params, float mergeRadius, int32_t progressive) {
+	Scene* S = static_cast<Scene*>(s);
+	auto* st = new VcmState();
+	st->scene = S;
+	st->params = *params;
+	st->mergeRadius = mergeRadius;
+	st->progressive = progressive != 0;
+	const i32 num = i32(S->width * S->height);
+	st->rngs.resize(size_t(num));
+	// cpu_vcm.cpp:292-297
+	const i32 seed = i32(u32(params->seed) * u32(num + 1));
+	for(i32 i = 0; i < num; ++i) st->rngs[size_t(i)] = Pcg64::seeded(u32(i32(u32(i) + u32(seed))));
+	st->radiance.assign(size_t(num) * 3, 0.0f);
+	st->lightness.assign(size_t(num), 0.0f);
+	st->radianceVar.assign(size_t(num) * 3, 0.0f);
+	st->lightnessVar.assign(size_t(num), 0.0f);
+	return st;
+}
+
+void oracle_vcm_destroy(void* p) { delete static_cast<VcmState*>(p); }
+
+int oracle_vcm_iterate(void* p, int32_t nt) {
+	vcm_iterate(*static_cast<VcmState*>(p), nt > 0 ? nt : 1);
+	return 1;
+}
+
+int oracle_vcm_get_target(void* p, int32_t target, float* out) {
+	const VcmState* st = static_cast<const VcmState*>(p);
+	const std::vector<float>* v = target == 0 ? &st->radiance : target == 1 ? &st->lightness
+	                            : target == 2 ? &st->radianceVar : target == 3 ? &st->lightnessVar : nullptr;
+	if(!v) return 0;
+	std::memcpy(out, v->data(), v->size() * 4);
+	return 1;
+}
+
+int oracle_vcm_records(void* p, int32_t* pixels, float* values) {
+	const VcmState* st = static_cast<const VcmState*>(p);
+	if(st->iteration < 0) return 0;
+	std::memcpy(pixels, st->recPixel.data(), st->recPixel.size() * 4);
+	std::memcpy(values, st->recValue.data(), st->recValue.size() * 4);
+	return 1;
+}
+
+int oracle_vcm_stats(void* p, OrStats* o) {
+	const VcmState* st = static_cast<const VcmState*>(p);
+	o->rays = st->stats.rays; o->shadowRays = st->stats.shadowRays;
+	o->nodeVisits = st->stats.nodeVisits; o->instanceVisits = st->stats.instanceVisits;
+	o->triTests = st->stats.tri; o->quadTests = st->stats.quad; o->sphereTests = st->stats.sphere;
+	return 1;
+}
+
+uint32_t oracle_vcm_map_size(uint32_t capacity) { return vcm_map_size(capacity); }
+uint32_t oracle_wang_hash(uint32_t x) { return wang_hash(x); }
 
 void* oracle_wireframe_create(void* s, float lineWidth, int32_t maxTraceDepth) {
 	Scene* S = static_cast<Scene*>(s);

@@ -172,6 +172,24 @@ int oracle_bpt_get_target(void* bpt, int32_t target, float* out);
  * index or -1, values[4k..4k+3] = radiance rgb and lightness as added. */
 int oracle_bpt_records(void* bpt, int32_t* pixels, float* values);
 int oracle_bpt_stats(void* bpt, OrStats* stats);
+/* Vertex connection and merging (CpuVcm equivalent, cpu_vcm.cpp); the
+ * parameters are the light tracer's (density unused), the merge radius
+ * relative to the scene's diagonal and the progressive switch. */
+void* oracle_vcm_create(void* scene, const OrLtParams* params, float mergeRadius, int32_t progressive);
+void oracle_vcm_destroy(void* vcm);
+int oracle_vcm_iterate(void* vcm, int32_t numThreads);
+/* Cumulative target: 0 radiance (3 ch), 1 lightness (1 ch), 2, 3 their variances */
+int oracle_vcm_get_target(void* vcm, int32_t target, float* out);
+/* The last iteration's contributions, W*H*(M*M + 2M) slots for maximum path
+ * length M (pixel major): the connections [view path length][light vertex],
+ * the emitter hits [view path length - 1], the merges [view path length - 1];
+ * pixels[k] = pixel index or -1, values[4k..4k+3] = radiance rgb, lightness. */
+int oracle_vcm_records(void* vcm, int32_t* pixels, float* values);
+int oracle_vcm_stats(void* vcm, OrStats* stats);
+/* The photon map's bucket count for a capacity, and the Wang hash that picks
+ * a pixel's light subpath (for the tests of both). */
+uint32_t oracle_vcm_map_size(uint32_t capacity);
+uint32_t oracle_wang_hash(uint32_t x);
 /* Wireframe renderer (CpuWireframe equivalent, wireframe_common.hpp);
  * the target is the cumulative "Border" image (3 channels). */
 void* oracle_wireframe_create(void* scene, float lineWidth, int32_t maxTraceDepth);

@@ -109,6 +109,17 @@ def lib():
         L.oracle_bpt_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
         L.oracle_bpt_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_bpt_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_vcm_create.restype = C.c_void_p
+        L.oracle_vcm_create.argtypes = [C.c_void_p, C.POINTER(OrLtParams), C.c_float, C.c_int32]
+        L.oracle_vcm_destroy.argtypes = [C.c_void_p]
+        L.oracle_vcm_iterate.argtypes = [C.c_void_p, C.c_int32]
+        L.oracle_vcm_get_target.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        L.oracle_vcm_records.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_vcm_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
+        L.oracle_vcm_map_size.restype = C.c_uint32
+        L.oracle_vcm_map_size.argtypes = [C.c_uint32]
+        L.oracle_wang_hash.restype = C.c_uint32
+        L.oracle_wang_hash.argtypes = [C.c_uint32]
         L.oracle_wireframe_create.restype = C.c_void_p
         L.oracle_wireframe_create.argtypes = [C.c_void_p, C.c_float, C.c_int32]
         L.oracle_wireframe_destroy.argtypes = [C.c_void_p]
@@ -494,3 +505,67 @@ class OracleWireframe:
             self.close()
         except Exception:
             pass
+
+
+class OracleVcm:
+    """CPU restatement of vertex connection and merging (cpu_vcm.cpp): per pixel and iteration one light
+    subpath (all stored as photons in a hash grid) and one view subpath whose vertices connect to one
+    light subpath, count emitter hits and merge with the photons within the merge radius."""
+
+    TARGETS = {"Radiance": (0, 3), "Lightness": (1, 1)}
+
+    def __init__(self, scene: OracleScene, seed=0, min_path=0, max_path=16, merge_radius=0.001, progressive=False):
+        self.scene = scene
+        self.max_path = max(1, max_path)
+        p = OrLtParams(seed, min_path, max_path, 0)
+        self.handle = lib().oracle_vcm_create(scene.handle, C.byref(p), float(merge_radius), int(progressive))
+        if not self.handle:
+            raise ValueError("oracle_vcm_create failed")
+
+    def iterate(self, threads: int = 0):
+        if threads <= 0:
+            threads = os.cpu_count() or 1
+        lib().oracle_vcm_iterate(self.handle, threads)
+
+    def target(self, name: str, variance: bool = False):
+        w, h = self.scene.spec.width, self.scene.spec.height
+        idx, ch = self.TARGETS[name]
+        out = np.zeros((h, w, ch), np.float32)
+        lib().oracle_vcm_get_target(self.handle, idx + (2 if variance else 0), _ptr(out))
+        return out
+
+    def records(self):
+        """The last iteration's contributions per pixel: M*M connection slots [view length][light vertex],
+        M emitter-hit slots and M merge slots [view length - 1] (M = max. path length); pixel index (-1:
+        none) and (radiance rgb, lightness) as added."""
+        m = self.max_path
+        n = self.scene.spec.width * self.scene.spec.height * (m * m + 2 * m)
+        pix = np.zeros(n, np.int32)
+        val = np.zeros((n, 4), np.float32)
+        if not lib().oracle_vcm_records(self.handle, _ptr(pix), _ptr(val)):
+            raise RuntimeError("no iteration has run")
+        return pix, val
+
+    def stats(self):
+        s = OrStats()
+        lib().oracle_vcm_stats(self.handle, C.byref(s))
+        return {k: getattr(s, k) for k, _ in OrStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().oracle_vcm_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def vcm_map_size(capacity: int) -> int:
+    return int(lib().oracle_vcm_map_size(capacity))
+
+
+def wang_hash(x: int) -> int:
+    return int(lib().oracle_wang_hash(x))

@@ -116,7 +116,7 @@ def test_bpt_in_the_registry():
     d = bindings.DllInterface()
     try:
         core, I = d.core, d.muffInst
-        assert d.render_get_renderer_count() == 4
+        assert d.render_get_renderer_count() == 5
         assert d.render_get_renderer_name(3) == "Bidirectional Pathtracer"
         assert d.render_get_renderer_short_name(3) == "BPT"
         assert core.render_get_renderer_devices(I, 3, 0) == 2  # DEVICE_CUDA

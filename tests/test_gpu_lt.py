@@ -123,14 +123,14 @@ def test_lt_min_path_length(oracle):
 def test_renderer_registry_lists_the_light_tracer():
     d = bindings.DllInterface()
     try:
-        assert d.render_get_renderer_count() == 4
-        assert [d.render_get_renderer_name(i) for i in range(4)] == \
-            ["Pathtracer", "Lighttracer", "Wireframe", "Bidirectional Pathtracer"]
-        assert [d.render_get_renderer_short_name(i) for i in range(4)] == ["PT", "LT", "WF", "BPT"]
+        assert d.render_get_renderer_count() == 5
+        assert [d.render_get_renderer_name(i) for i in range(5)] == \
+            ["Pathtracer", "Lighttracer", "Wireframe", "Bidirectional Pathtracer", "Vertex Connection and Merging"]
+        assert [d.render_get_renderer_short_name(i) for i in range(5)] == ["PT", "LT", "WF", "BPT", "VCM"]
         core, I = d.core, d.muffInst
         assert core.render_get_renderer_variations(I, 1) == 1
         assert core.render_get_renderer_devices(I, 1, 0) == 2  # DEVICE_CUDA
-        assert not d.render_enable_renderer(4, 0)
+        assert not d.render_enable_renderer(5, 0)
         assert d.render_enable_renderer(1, 0)
         assert core.render_get_render_target_count(I) == 3
         assert [core.render_get_render_target_name(I, i).decode() for i in range(3)] == ["Radiance", "Lightness", "Density"]
