@@ -24,7 +24,7 @@ enum BKind { BV_VIRTUAL = 0, BV_CAMERA, BV_SURFACE, BV_VOID, BV_POINT, BV_AREA, 
 // and the distance with the sign of z; a miss: the direction; an area light:
 // its normal; a point light: its intensity; the environment: the photon's
 // direction).
-struct BV {
+struct alignas(16) BV {
 	int kind;
 	f3 position, incEnc, intensity;
 	float projSceneArea;
@@ -38,6 +38,24 @@ struct BV {
 	int pathLen;        // segments from the subpath's start (PathVertex::m_pathLen)
 	float prevConv;     // VcmVertexExt::prevConversionFactor: |cos| / d^2 towards the previous vertex
 };
+
+// The stages keep vertices in device arrays; a vertex moves as 11 16-byte
+// words (one vector load or store each) instead of 44 scalar ones.
+static_assert(sizeof(BV) == 176 && sizeof(BV) % 16 == 0, "BV moves as float4 words");
+MBD BV bv_load(const BV* p) {
+	BV v;
+	const float4* s = reinterpret_cast<const float4*>(p);
+	float4* d = reinterpret_cast<float4*>(&v);
+#pragma unroll
+	for(int i = 0; i < int(sizeof(BV) / 16); ++i) d[i] = s[i];
+	return v;
+}
+MBD void bv_store(BV* p, const BV& v) {
+	const float4* s = reinterpret_cast<const float4*>(&v);
+	float4* d = reinterpret_cast<float4*>(p);
+#pragma unroll
+	for(int i = 0; i < int(sizeof(BV) / 16); ++i) d[i] = s[i];
+}
 
 MBD bool bv_ortho(int k) { return k == BV_VOID || k == BV_ENV; } // path_util.hpp:41-46
 MBD bool bv_end(int k) { return k != BV_SURFACE; }               // path_util.hpp:33-35
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_light_shade(const DScene S, con
 				bptw_queue_segment(W, g + 1, p, o, d, thr, pdf);
 			T.rngState[p] = rng;
 		}
-		W.lv[size_t(g + 1) * W.n + p] = v;
+		bv_store(W.lv + size_t(g + 1) * W.n + p, v);
 	}
 }
 

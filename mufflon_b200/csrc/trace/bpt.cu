@@ -311,7 +311,7 @@ MBD void bptw_connect(const DScene& S, const LtParams& P, const LtTargets& T, co
 	const size_t base = size_t(p) * (maxP * maxP + maxP) + size_t(viewLen) * maxP;
 	for(int l = lo; l < hi; ++l) {
 		BptConn c;
-		const BV& w = W.lv[size_t(l) * W.n + p];
+		const BV w = bv_load(W.lv + size_t(l) * W.n + p);
 		const int k = bpt_connect(S, T.width, v, pv, w, l > 0 ? &W.lv[size_t(l - 1) * W.n + p] : nullptr, thr, px, py, c);
 		const size_t slot = base + size_t(l);
 		if(k > 0) {
@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(128) k_bptw_light_start(const DScene S, const 
 			float pdf;
 			if(bpt_sample<false>(S, v, nullptr, 0, 0, rng, true, thr, o, d, pdf)) bptw_queue_segment(W, 0, p, o, d, thr, pdf);
 		}
-		W.lv[p] = v;
+		bv_store(W.lv + p, v);
 	}
 	W.lightLen[p] = lightLen;
 	T.rngState[p] = rng;
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_start(const DScene S, cons
 	float pdf;
 	if(bpt_sample<false>(S, c, nullptr, px, py, rng, false, thr, o, d, pdf)) {
 		bptw_queue_segment(W, gen, p, o, d, thr, pdf);
-		W.vp[0][p] = c;
+		bv_store(W.vp[0] + p, c);
 	}
 	T.rngState[p] = rng;
 }
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_shade(const DScene S, cons
 		const f3 ro = f4to3(__ldcs(W.qOrg[q] + i)), rd = f4to3(__ldcs(W.qDir[q] + i));
 		const float4 tp = W.thr[p];
 		f3 thr = f4to3(tp);
-		const BV pv = W.vp[k & 1][p];
+		const BV pv = bv_load(W.vp[k & 1] + p);
 		BV h;
 		bpt_new_vertex<false>(S, pv, ro, rd, hr, tp.w, thr, h);
 		if(viewLen >= P.minPathLength) {
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_shade(const DScene S, cons
 		float pdf;
 		if(bpt_sample<false>(S, h, &pv, px, py, rng, false, thr, o, d, pdf)) {
 			bptw_queue_segment(W, gen + 1, p, o, d, thr, pdf);
-			W.vp[viewLen & 1][p] = h;
+			bv_store(W.vp[viewLen & 1] + p, h);
 		}
 		T.rngState[p] = rng;
 	}

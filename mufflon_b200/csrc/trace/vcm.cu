@@ -305,7 +305,7 @@ MBD void vcmw_connect(const DScene& S, const LtParams& P, const LtTargets& T, co
 		const int pathLen = l + 1 + viewLen;
 		if(pathLen < P.minPathLength || pathLen > P.maxPathLength) continue;
 		BptConn c;
-		const BV& w = W.lv[size_t(l) * W.n + lp];
+		const BV w = bv_load(W.lv + size_t(l) * W.n + lp);
 		const int k = vcm_connect(S, T.width, v, pv, w, l > 0 ? &W.lv[size_t(l - 1) * W.n + lp] : nullptr, thr, px, py, C, c);
 		const size_t slot = base + size_t(l);
 		if(k > 0) {
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(128) k_vcmw_light_start(const DScene S, const 
 			if(bpt_sample<true>(S, v, nullptr, 0, 0, rng, true, thr, o, d, pdf, C.nPhotons, C.lightArea))
 				bptw_queue_segment(W, 0, p, o, d, thr, pdf);
 		}
-		W.lv[p] = v;
+		bv_store(W.lv + p, v);
 	}
 	W.lightLen[p] = lightLen;
 	T.rngState[p] = rng;
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(128, 4) k_vcmw_view_start(const DScene S, cons
 	float pdf;
 	if(bpt_sample<true>(S, c, nullptr, px, py, rng, false, thr, o, d, pdf, C.nPhotons, C.viewArea)) {
 		bptw_queue_segment(W, gen, p, o, d, thr, pdf);
-		W.vp[0][p] = c;
+		bv_store(W.vp[0] + p, c);
 	}
 	T.rngState[p] = rng;
 }
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(128, 4) k_vcmw_view_shade(const DScene S, cons
 		const f3 ro = f4to3(__ldcs(W.qOrg[q] + i)), rd = f4to3(__ldcs(W.qDir[q] + i));
 		const float4 tp = W.thr[p];
 		f3 thr = f4to3(tp);
-		const BV pv = W.vp[k & 1][p];
+		const BV pv = bv_load(W.vp[k & 1] + p);
 		BV h;
 		bpt_new_vertex<true>(S, pv, ro, rd, hr, tp.w, thr, h);
 		const size_t base = size_t(p) * vcm_slots(maxP) + size_t(maxP) * size_t(maxP);
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(128, 4) k_vcmw_view_shade(const DScene S, cons
 		float pdf;
 		if(bpt_sample<true>(S, h, &pv, px, py, rng, false, thr, o, d, pdf, C.nPhotons, C.viewArea)) {
 			bptw_queue_segment(W, gen + 1, p, o, d, thr, pdf);
-			W.vp[viewLen & 1][p] = h;
+			bv_store(W.vp[viewLen & 1] + p, h);
 		}
 		T.rngState[p] = rng;
 	}
