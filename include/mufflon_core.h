@@ -480,7 +480,7 @@ CORE_API Boolean CDECL mufflon_sort_pairs(uint64_t* keys, int32_t* values, uint3
  * For callers that cannot call cudaMalloc: an engine that has reserved all
  * device memory for its own allocator, or a frame loop that must not stall in
  * cudaMalloc/cudaFree (they may synchronise the device). The scratch space is
- * a fixed array of about 12.3 MiB inside the library, held by every GPU that
+ * a fixed array of about 12.5 MiB inside the library, held by every GPU that
  * loads the library until the process exits; n above
  * MUFFLON_SORT_NOALLOC_MAX_PAIRS is rejected with an error. Set-up:
  * mufflon_initialize looks up the array's address on the device it selects

@@ -17,7 +17,7 @@ namespace mb {
 namespace {
 
 constexpr int SORT_THREADS = 256;
-constexpr int SORT_ITEMS = 16;
+constexpr int SORT_ITEMS = 8;
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr size_t SORT_SMEM = size_t(SORT_TILE) * 8 + size_t(SORT_TILE) * 4 + size_t(SORT_WARPS) * 256 * 4;

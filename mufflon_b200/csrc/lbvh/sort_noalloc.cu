@@ -10,7 +10,7 @@
 //
 // Limits and sharing:
 //   * at most NOALLOC_MAX_PAIRS pairs per call; larger sizes are rejected;
-//   * the array (about 12.3 MiB) is part of the library's device image: every
+//   * the array (about 12.5 MiB) is part of the library's device image: every
 //     GPU on which the library is loaded holds it until the process exits;
 //   * all calls share the array and it keeps the previous call's contents, so
 //     every region that must start at zero is cleared at the start of a call,
