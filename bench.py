@@ -57,7 +57,7 @@ def parse():
                         "lights: GPU light-tree build of 262 145 lights; lt: the light tracer at 1080p; bpt: the bidirectional path tracer at 1080p; vcm: vertex connection and merging at 1080p; instanced: config 2 (4 096 instances) at 1080p")
     p.add_argument("--jobs", type=int, default=64)
     p.add_argument("--resolution", type=lambda v: tuple(int(x) for x in v.split("x")), default=(WIDTH, HEIGHT),
-                   help="lt / bpt: image size WxH (default 1920x1080; smaller for profiler captures)")
+                   help="frame / lt / bpt / vcm: image size WxH (default 1920x1080; smaller for profiler captures)")
     p.add_argument("--merge-radius", type=float, default=0.001,
                    help="vcm: \"Relative merge radius\" (of the scene's diagonal; the reference's default 0.001)")
     p.add_argument("--megakernel", action="store_true",
@@ -262,7 +262,8 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from mufflon_b200 import bindings, build, distributed, scenes
     build.build()
-    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=WIDTH, height=HEIGHT)
+    W, H = args.resolution
+    spec = scenes.displaced_icosphere(0, subdiv=args.subdiv, width=W, height=H)
     dll = bindings.DllInterface()
     bindings.load_scene_spec(dll, spec)
     assert dll.render_enable_renderer(0, 0)
@@ -330,7 +331,7 @@ def run_b200(args):
     spp_s = SPP_PER_FRAME * args.steps * world / (kernel_ms_max * 1e-3)
 
     # e2e: scene upload + BVH build + 16 iterations + image readback per step
-    d2h = WIDTH * HEIGHT * 3 * 4
+    d2h = W * H * 3 * 4
     h2d = scene_bytes(spec)
     dll.get_target_image("Radiance", copy=False)  # warm-up: allocates the page-locked read-back buffer once
     barrier()
@@ -421,7 +422,7 @@ def run_b200(args):
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(kernel_ms_max / args.steps, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "triangles": int(spec.num_prims), "resolution": [WIDTH, HEIGHT],
+                "config": {"workload": WORKLOAD.replace("1920x1080", f"{W}x{H}"), "triangles": int(spec.num_prims), "resolution": [W, H],
                            "spp_per_step": SPP_PER_FRAME, "max_path_length": MAX_PATH,
                            "l2": "inputs larger than L2 (BVH + triangle soup + image > 126 MB)",
                            "parallelism": f"replicas x{world} (samples split by seed)"},
