@@ -153,6 +153,31 @@ def test_bpt_alpha_contributions_match_oracle(oracle):
     assert rel_rmse(img, ob.target("Radiance")) <= 1e-5
 
 
+def test_vcm_alpha_contributions_match_oracle(oracle):
+    """Connections, hits and merges with cut-out surfaces: the light walk,
+    the view walk and the connections' shadow rays all pass through the
+    alpha test."""
+    spec = scenes.alpha_cutouts(4, 48, 48)
+    ov_ = oracle.OracleVcm(oracle.OracleScene(spec), seed=7, min_path=0, max_path=5, merge_radius=0.02)
+    d = _session(spec, 4)
+    try:
+        for k, v in {"Seed": 7, "Max. path length": 5, "Record connections": 1}.items():
+            assert d.renderer_set_parameter_int(k, v)
+        assert d.renderer_set_parameter_float("Relative merge radius", 0.02)
+        d.render_enable_render_target("Radiance", False)
+        for it in range(2):
+            d.render_iterate()
+            ov_.iterate()
+            gp, gv = d.vcm_records(5)
+            op, ov = ov_.records()
+            assert np.array_equal(gp, op), f"iteration {it}"
+            assert np.array_equal(gv.view(np.uint32), ov.view(np.uint32)), f"iteration {it}"
+        img = d.get_target_image("Radiance").copy()
+    finally:
+        d.close()
+    assert rel_rmse(img, ov_.target("Radiance")) <= 1e-5
+
+
 def test_wireframe_ignores_alpha(oracle):
     spec = scenes.alpha_cutouts(5, 64, 64, background=False)
     imgs = []

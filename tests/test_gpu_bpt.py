@@ -158,11 +158,13 @@ def test_bpt_edge_cases_match_oracle(oracle, case, max_path, megakernel):
         assert _rel_rmse(out["Radiance"], ob.target("Radiance")) <= 1e-5
 
 
-@pytest.mark.parametrize("renderer", [1, 3], ids=["lt", "bpt"])
+@pytest.mark.parametrize("renderer", [1, 3, 4], ids=["lt", "bpt", "vcm"])
 def test_stages_refuse_paths_beyond_their_launch_count(renderer):
     """The staged schedules launch a fixed number of generations; a longer
-    max. path length fails the iteration with a message naming the switch to
-    the persistent kernel, and "Megakernel" 1 renders it."""
+    max. path length fails the iteration with a message (for the light and
+    bidirectional tracers naming the switch to the persistent kernel, and
+    "Megakernel" 1 renders it; vertex connection and merging has only the
+    stages)."""
     spec = scenes.cornell_box(1, width=8, height=8)
     d = bindings.DllInterface()
     try:
@@ -171,6 +173,8 @@ def test_stages_refuse_paths_beyond_their_launch_count(renderer):
         assert d.renderer_set_parameter_int("Max. path length", 65)
         with pytest.raises(bindings.MufflonError, match="at most 64 path lengths"):
             d.render_iterate()
+        if renderer == 4:
+            return
         assert d.renderer_set_parameter_int("Megakernel", 1)
         d.render_iterate()
         assert d.render_stats()["rays"] > 0

@@ -21,8 +21,11 @@ def _iterate_ok(d):
     return d.core.render_iterate(d.muffInst, None, None, None) != 0
 
 
-@pytest.mark.parametrize("renderer,extra", [(0, {"Megakernel": 0}), (0, {"Megakernel": 1}), (1, {}), (2, {}), (3, {})],
-                         ids=["pt-wavefront", "pt-megakernel", "lt", "wireframe", "bpt"])
+@pytest.mark.parametrize("renderer,extra", [(0, {"Megakernel": 0}), (0, {"Megakernel": 1}), (1, {"Megakernel": 0}),
+                                            (1, {"Megakernel": 1}), (2, {}), (3, {"Megakernel": 0}), (3, {"Megakernel": 1}),
+                                            (4, {})],
+                         ids=["pt-wavefront", "pt-megakernel", "lt-stages", "lt-single-kernel", "wireframe", "bpt-stages",
+                              "bpt-single-kernel", "vcm"])
 def test_step_limit_fails_the_iteration(renderer, extra):
     spec = scenes.displaced_icosphere(0, subdiv=4, width=48, height=27)
     d = bindings.DllInterface()

@@ -89,6 +89,30 @@ def test_bpt_variance_matches_oracle(oracle):
         assert _rel_rmse(var, bpt.target(name, variance=True)) <= 1e-5, name
 
 
+def test_vcm_variance_matches_oracle(oracle):
+    spec = scenes.cornell_box(2, 48, 48)
+    d = bindings.DllInterface()
+    try:
+        bindings.load_scene_spec(d, spec)
+        assert d.render_enable_renderer(4, 0)
+        for k, v in {"Max. path length": 5, "Seed": 1}.items():
+            assert d.renderer_set_parameter_int(k, v)
+        assert d.renderer_set_parameter_float("Relative merge radius", 0.02)
+        for t in ("Radiance", "Lightness"):
+            assert d.render_enable_render_target(t, True)
+        for _ in range(3):
+            d.render_iterate()
+        out = {t: (d.get_target_image(t), d.get_target_image(t, variance=True)) for t in ("Radiance", "Lightness")}
+    finally:
+        d.close()
+    vcm = oracle.OracleVcm(oracle.OracleScene(spec), seed=1, max_path=5, merge_radius=0.02)
+    for _ in range(3):
+        vcm.iterate()
+    for name, (cum, var) in out.items():
+        assert _rel_rmse(cum, vcm.target(name)) <= 1e-5, name
+        assert _rel_rmse(var, vcm.target(name, variance=True)) <= 1e-5, name
+
+
 def test_wireframe_border_variance_matches_oracle(oracle):
     spec = scenes.displaced_icosphere(2, subdiv=3, width=64, height=36)
     out = _render(spec, 2, {}, ["Border"], iterations=3)
