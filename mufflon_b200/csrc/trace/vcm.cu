@@ -507,7 +507,8 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	// queue and photon indices are 32-bit: max. path length slots per pixel
 	if(maxP > BPTW_MAX_PATH || size_t(n) * size_t(maxP) >= size_t(0xFFFFFFFFu)) return cudaErrorInvalidValue;
 	const uint32_t slots = n * uint32_t(maxP);
-	static uint32_t cachedSlots = 0, cachedMap = 0;
+	// the bucket count of the last size this thread launched (the prime search is cheap but not free)
+	thread_local uint32_t cachedSlots = 0, cachedMap = 0;
 	if(cachedSlots != slots) { cachedMap = vcm_map_size(slots); cachedSlots = slots; }
 	// CpuVcm::iterate (cpu_vcm.cpp:148-157) and the areas of trace_photon / sample
 	const float dx = S.aabbMax[0] - S.aabbMin[0], dy = S.aabbMax[1] - S.aabbMin[1], dz = S.aabbMax[2] - S.aabbMin[2];
