@@ -355,6 +355,7 @@ void iterate_lt(MufflonInstance& I) {
 	r.lastLaunches = 2;
 	for(float& m : r.stageMs) m = 0.0f;
 	check_traversal(c.errors, S.maxSteps);
+	CHECK(c.waitErrors == 0, "a bounded wait of the photon-grid sort expired; the result of this call is incomplete");
 }
 
 // Brings in, through the registered LoD loader, every LoD the current

@@ -172,7 +172,7 @@ struct TraceCounters {
 	unsigned long long primTests;
 	unsigned long long instanceVisits;
 	unsigned int errors;       // stack overflow or bounded-wait expiry
-	unsigned int pad;
+	unsigned int waitErrors;   // expired bounded waits outside traversal (the photon-grid sort)
 };
 
 } // namespace mb

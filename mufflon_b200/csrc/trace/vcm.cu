@@ -135,7 +135,7 @@ __global__ void k_vcm_gather(const BptwState W, VcmGrid G, uint32_t total, uint3
 }
 
 __global__ void k_vcm_sort_status(VcmGrid G, TraceCounters* counters) {
-	if(*G.error) atomicAdd(&counters->errors, 1u);
+	if(*G.error) atomicAdd(&counters->waitErrors, 1u);
 }
 
 // ---------------------------------------------------------------- weights
