@@ -285,6 +285,12 @@ MBD void bpt_add(const LtTargets& T, uint32_t pix, float4 v) {
 
 
 enum { BPTW_EXT0 = 0, BPTW_SH0 = 2, BPTW_WORK = 4 };
+// Resident blocks of 128 threads per SM that the shade-side stage kernels
+// (light shade, view start, view shade) are compiled for; their grids are
+// this many blocks per SM. They wait on scattered vertex loads, so occupancy
+// beats registers: 8 blocks (64 registers) measured fastest, bidirectional
+// path tracer 748 / 765 / 764 and VCM 468 / 479 / 490 Mrays/s at 4 / 6 / 8.
+constexpr int BPTW_SHADE_BLOCKS = 8;
 constexpr int BPTW_COUNTERS = 4 + 2 * BPTW_MAX_PATH;
 
 struct BptwState {
@@ -363,7 +369,7 @@ MBD HitRec bptw_hit(const BptwState& W, int q, unsigned i) {
 // one the path length allows. VCM: with its MIS data (nPhotons light
 // subpaths, merge area mergeArea).
 template < bool VCM >
-__global__ void __launch_bounds__(128, 4) k_bptw_light_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_light_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                           int g, float nPhotons = 0.0f, float mergeArea = 0.0f) {
 	const int q = g & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);

@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128) k_bptw_light_start(const DScene S, const 
 
 // View phase, first generation (gen): every pixel's camera vertex, its
 // connections with the light subpath and its first segment.
-__global__ void __launch_bounds__(128, 4) k_bptw_view_start(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_view_start(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                          int gen) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= W.n) return;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(128, 4) k_bptw_view_start(const DScene S, cons
 // length) becomes vertex k + 1 (a surface or a miss): what it adds by
 // reaching an emitter or the background, then, unless the path ends there,
 // its connections and its segment of generation gen + 1.
-__global__ void __launch_bounds__(128, 4) k_bptw_view_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_view_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                          int gen, int k) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
@@ -494,12 +494,12 @@ cudaError_t launch_bpt(const DScene& S, const LtParams& P, const LtTargets& T, v
 		const int lightGens = maxP - 1;
 		for(int g = 0; g < lightGens; ++g) {
 			trace(g);
-			k_bptw_light_shade<false><<<sms * 4, 128, 0, stream>>>(S, P, T, W, g);
+			k_bptw_light_shade<false><<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, g);
 		}
 		k_bptw_view_start<<<(n + 127) / 128, 128, 0, stream>>>(S, P, T, W, lightGens);
 		for(int k = 0; k < maxP; ++k) {
 			trace(lightGens + k);
-			k_bptw_view_shade<<<sms * 4, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
+			k_bptw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
 		}
 	} else {
 		if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;

@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(128) k_vcmw_light_start(const DScene S, const 
 
 // View phase, first generation (gen): every pixel's camera vertex, its
 // connections and its first segment.
-__global__ void __launch_bounds__(128, 4) k_vcmw_view_start(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_view_start(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                          VcmConsts C, int gen) {
 	const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
 	if(p >= W.n) return;
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(128, 4) k_vcmw_view_start(const DScene S, cons
 // View phase, generation gen: a segment from view vertex k becomes vertex
 // k + 1; its emitter term, then unless the path ends there its merges, and
 // below the max. path length its connections and next segment.
-__global__ void __launch_bounds__(128, 4) k_vcmw_view_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_view_shade(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                          VcmGrid G, VcmConsts C, int gen, int k) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
@@ -548,7 +548,7 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	const int lightGens = maxP - 1;
 	for(int g = 0; g < lightGens; ++g) {
 		trace(g);
-		k_bptw_light_shade<true><<<sms * 4, 128, 0, stream>>>(S, P, T, W, g, C.nPhotons, C.lightArea);
+		k_bptw_light_shade<true><<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, g, C.nPhotons, C.lightArea);
 	}
 	// photon grid
 	const unsigned gb = std::min<unsigned>((slots + 255) / 256, unsigned(sms) * 16u);
@@ -563,7 +563,7 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	k_vcmw_view_start<<<(n + 127) / 128, 128, 0, stream>>>(S, P, T, W, C, lightGens);
 	for(int k = 0; k < maxP; ++k) {
 		trace(lightGens + k);
-		k_vcmw_view_shade<<<sms * 4, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
+		k_vcmw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
 	}
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_vcm_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
