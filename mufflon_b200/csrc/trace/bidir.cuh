@@ -291,6 +291,8 @@ enum { BPTW_EXT0 = 0, BPTW_SH0 = 2, BPTW_WORK = 4 };
 // beats registers: 8 blocks (64 registers) measured fastest, bidirectional
 // path tracer 748 / 765 / 764 and VCM 468 / 479 / 490 Mrays/s at 4 / 6 / 8.
 constexpr int BPTW_SHADE_BLOCKS = 8;
+// ... and the trace stage (5 and 6 measured alike; 8 was 6 % slower).
+constexpr int BPTW_TRACE_BLOCKS = 6;
 constexpr int BPTW_COUNTERS = 4 + 2 * BPTW_MAX_PATH;
 
 struct BptwState {
@@ -323,7 +325,7 @@ MBD void bptw_queue_segment(const BptwState& W, int gen, uint32_t p, f3 o, f3 d,
 // The trace stage of generation gen: segments (closest hit) and connections
 // (any hit; a visible one adds its value, each one records what it added).
 template < int AM >
-__global__ void __launch_bounds__(128, 6) k_bptw_trace(const DScene S, const LtTargets T, BptwState W, int gen,
+__global__ void __launch_bounds__(128, BPTW_TRACE_BLOCKS) k_bptw_trace(const DScene S, const LtTargets T, BptwState W, int gen,
                                                     TraceCounters* counters) {
 	const int q = gen & 1;
 	if(blockIdx.x == 0 && threadIdx.x == 0) {

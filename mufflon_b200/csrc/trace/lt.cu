@@ -274,6 +274,10 @@ __global__ void __launch_bounds__(128, 6) k_lt(const DScene S, const LtParams P,
 //
 // Queue state (LtwState) lives in one device allocation carved by ltw_carve.
 enum { LTW_EXT0 = 0, LTW_SH0 = 2, LTW_WORK = 4 };
+// Resident blocks of 128 threads per SM the trace stage is compiled for: 5
+// measured fastest on the 1080p headline scene (1 063 Mrays/s; 6: 1 048,
+// 8: 975).
+constexpr int LTW_TRACE_BLOCKS = 5;
 constexpr int LTW_COUNTERS = 4 + 2 * LTW_MAX_LAUNCHES;
 
 struct LtwState {
@@ -344,7 +348,7 @@ __global__ void k_ltw_start(const DScene S, const LtParams P, const LtTargets T,
 // connections counted in LTW_SH0 + (gen & 1) (any hit), taken by persistent
 // warps 32 items at a time once all their lanes are idle.
 template < int AM >
-__global__ void __launch_bounds__(128, 6) k_ltw_trace(const DScene S, const LtParams P, const LtTargets T, LtwState W,
+__global__ void __launch_bounds__(128, LTW_TRACE_BLOCKS) k_ltw_trace(const DScene S, const LtParams P, const LtTargets T, LtwState W,
                                                    int gen, TraceCounters* counters) {
 	const int q = gen & 1;
 	if(blockIdx.x == 0 && threadIdx.x == 0) {
