@@ -503,6 +503,10 @@ LbvhBuilder::~LbvhBuilder() {
 	cudaFree(m_ranges); cudaFree(m_wideCounters); cudaFree(m_wideQueueA); cudaFree(m_wideQueueB);
 	if(m_hostCount) cudaFreeHost(m_hostCount);
 	for(auto& e : m_ev) if(e) cudaEventDestroy(e);
+	for(auto& e : m_wideEv) if(e) cudaEventDestroy(e);
+	if(m_fork) cudaEventDestroy(m_fork);
+	if(m_join) cudaEventDestroy(m_join);
+	if(m_side) cudaStreamDestroy(m_side);
 }
 
 cudaError_t LbvhBuilder::reserve(uint32_t n) {
@@ -515,6 +519,10 @@ cudaError_t LbvhBuilder::reserve(uint32_t n) {
 		if((e = cudaMallocHost(&m_hostCount, sizeof(int32_t))) != cudaSuccess) return e;
 		if((e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SORT_SMEM))) != cudaSuccess) return e;
 		for(auto& ev : m_ev) if((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+		for(auto& ev : m_wideEv) if((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+		if((e = cudaEventCreateWithFlags(&m_fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+		if((e = cudaEventCreateWithFlags(&m_join, cudaEventDisableTiming)) != cudaSuccess) return e;
+		if((e = cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking)) != cudaSuccess) return e;
 	}
 	if(n <= m_capacity) return cudaSuccess;
 	const size_t N = n;
@@ -641,6 +649,17 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	k_bbox<<<blocks_for(n, 128), 128, 0, stream>>>(mode, lodIn, sceneIn, n, numInternal, m_valsA, m_parents,
 	                                               m_children, m_nodeData, m_flags);
 	if(m_timing) cudaEventRecord(m_ev[4], stream);
+	// An object hierarchy's 8-wide conversion reads only the merged tree
+	// (children, ranges, boxes, sorted ids), as the collapse below does, so it
+	// runs beside it on the side stream; the instance level's conversion waits
+	// for its box refit after the collapse.
+	const bool sideWide = wide && mode == MODE_LOD;
+	cudaStream_t ws = stream;
+	if(sideWide) {
+		if((e = cudaEventRecord(m_fork, stream)) != cudaSuccess) return e;
+		if((e = cudaStreamWaitEvent(m_side, m_fork, 0)) != cudaSuccess) return e;
+		ws = m_side;
+	}
 	k_mark<<<blocks_for(n, 128), 128, 0, stream>>>(mode, n, numInternal, m_parents, m_nodeData, m_marks);
 	if(m_timing) cudaEventRecord(m_ev[5], stream);
 	const int scanBlocks = (numInternal + SCAN_TILE - 1) / SCAN_TILE;
@@ -678,10 +697,16 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 		wa.queueA = m_wideQueueA;
 		wa.queueB = m_wideQueueB;
 		int32_t numWide = 0;
-		if((e = build_wide(wa, &numWide, stream)) != cudaSuccess) return e;
+		if(m_timing) cudaEventRecord(m_wideEv[0], ws);
+		if((e = build_wide(wa, &numWide, ws)) != cudaSuccess) return e;
 		out.numWide = numWide;
 		if(mode == MODE_LOD)
-			k_wsoup<<<blocks_for(n, 256), 256, 0, stream>>>(*lod, n, out.wprims, out.wsoup);
+			k_wsoup<<<blocks_for(n, 256), 256, 0, ws>>>(*lod, n, out.wprims, out.wsoup);
+		if(m_timing) cudaEventRecord(m_wideEv[1], ws);
+	}
+	if(sideWide) {
+		if((e = cudaEventRecord(m_join, m_side)) != cudaSuccess) return e;
+		if((e = cudaStreamWaitEvent(stream, m_join, 0)) != cudaSuccess) return e;
 	}
 	if(m_timing) cudaEventRecord(m_ev[9], stream);
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -692,7 +717,10 @@ cudaError_t LbvhBuilder::build_common(int mode, const LodBuildInput* lod, const 
 	out.numInternal = *m_hostCount;
 	if(m_timing) {
 		float t[9];
-		for(int k = 0; k < 9; ++k) cudaEventElapsedTime(&t[k], m_ev[k], m_ev[k + 1]);
+		for(int k = 0; k < 8; ++k) cudaEventElapsedTime(&t[k], m_ev[k], m_ev[k + 1]);
+		// the conversion's own span (beside the collapse for object hierarchies)
+		t[8] = 0.0f;
+		if(wide) cudaEventElapsedTime(&t[8], m_wideEv[0], m_wideEv[1]);
 		m_times = { t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8] };
 	}
 	return cudaSuccess;

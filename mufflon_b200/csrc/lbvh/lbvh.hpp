@@ -129,6 +129,11 @@ private:
 	int m_mortonBits = 63;
 	StageTimes m_times{};
 	cudaEvent_t m_ev[10] = {};
+	// The 8-wide conversion of an object hierarchy runs on a stream of its own,
+	// beside the reference-layout collapse: both only read the merged tree.
+	cudaStream_t m_side = nullptr;
+	cudaEvent_t m_fork = nullptr, m_join = nullptr;
+	cudaEvent_t m_wideEv[2] = {};     // the conversion's start and end (timing)
 };
 
 } // namespace mb
