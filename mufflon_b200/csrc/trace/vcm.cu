@@ -13,11 +13,12 @@
 // Schedule: the bidirectional path tracer's stages (bidir.cuh). Light phase:
 // k_vcm_seed (the light tree's shared seed from pixel 0's generator),
 // k_vcmw_light_start, then per generation the shared trace kernel and
-// k_bptw_light_shade<true>. Photon grid (photon_map.hpp): k_vcm_keys gives
-// every light vertex its bucket, a 4-pass onesweep radix sort (stable, so a
-// bucket holds its photons in ascending (subpath, vertex) order), k_vcm_ranges
-// the bucket ranges and k_vcm_gather packs each photon's merge data (80 B) in
-// bucket order. View phase: k_vcmw_view_start, then per generation the trace
+// k_bptw_light_shade<true>. Photon grid (photon_map.hpp): k_vcm_keys appends
+// every light vertex after the start with the key (bucket, slot), a onesweep
+// radix sort over the photons (their count read back first) orders them by
+// bucket and, within a bucket, by ascending (subpath, vertex) slot,
+// k_vcm_ranges finds the bucket ranges and k_vcm_gather packs each photon's
+// merge data (80 B) in bucket order. View phase: k_vcmw_view_start, then per generation the trace
 // kernel and k_vcmw_view_shade (the vertex reached: its emitter term, its
 // merges, its connections and next segment). A bucket's photons are visited
 // from the last to the first, the order of the reference's head-inserted
@@ -36,7 +37,6 @@ namespace {
 // photon_map.hpp:29-52: a cell's hash; the insert's cell is ceil(p / edge),
 // a query's base cell round(p / edge) and its 8 cells base + {0, 1}^3
 constexpr uint32_t VCM_MAGIC_X = 0xb286aff7u, VCM_MAGIC_Y = 0x35e4a487u, VCM_MAGIC_Z = 0x75a9c18fu;
-constexpr uint32_t VCM_NO_BUCKET = 0xFFFFFFFFu;
 // an integral float as an unsigned grid coordinate (two's complement wrap
 // for negative cells, as the conversion does on the reference's x86 hosts)
 MBD uint32_t vcm_cell_coord(float x) { return uint32_t((long long)(x)); }
@@ -68,11 +68,12 @@ struct VcmConsts {
 	float radiusSq;
 	float density;    // 1 / cell edge (edge = 2.0001 r)
 	uint32_t mapSize; // buckets
+	int slotBits;     // bits of a light-vertex slot index p * M + l (the low part of a photon's sort key)
 };
 
 // The photon grid, carved after the stages' state.
 struct VcmGrid {
-	u64* keys;            // per light-vertex slot p * M + l: its bucket (VCM_NO_BUCKET: none), then sorted
+	u64* keys;            // per photon: its bucket << slotBits | its slot p * M + l, then sorted
 	int32_t* vals;        // the slot, sorted with the keys
 	u64* keysAlt;         // the sort's ping-pong buffers
 	int32_t* valsAlt;
@@ -86,6 +87,7 @@ struct VcmGrid {
 	                      // incident pdf; geometric normal, conversion factor; throughput, the previous
 	                      // vertex's incident pdf; the previous vertex's relative-probability sum
 	u64* seed;            // the light tree's seed of the iteration
+	unsigned* count;      // photons of the iteration (light vertices after the start)
 };
 
 __global__ void k_vcm_seed(const LtTargets T, VcmGrid G) {
@@ -95,31 +97,33 @@ __global__ void k_vcm_seed(const LtTargets T, VcmGrid G) {
 	T.rngState[0] = rng;
 }
 
-// Every slot p * M + l of the light subpaths: the bucket of light vertex l of
-// pixel p's subpath if it exists and is not the start (no photon otherwise).
+// Every light vertex l >= 1 of pixel p's subpath (slot s = p * M + l) is a
+// photon: key (bucket << slotBits) | s, value s, appended in any order. The
+// key makes the sorted order the same whatever the order of the appends: by
+// bucket, and within a bucket by ascending slot.
 __global__ void k_vcm_keys(const BptwState W, VcmGrid G, VcmConsts C, uint32_t maxP) {
 	const size_t total = size_t(W.n) * maxP;
 	for(size_t s = size_t(blockIdx.x) * blockDim.x + threadIdx.x; s < total; s += size_t(gridDim.x) * blockDim.x) {
 		const uint32_t p = uint32_t(s / maxP), l = uint32_t(s % maxP);
-		uint32_t b = VCM_NO_BUCKET;
-		if(l >= 1 && int(l) <= W.lightLen[p]) b = vcm_insert_hash(W.lv[size_t(l) * W.n + p].position, C.density) % C.mapSize;
-		G.keys[s] = b;
-		G.vals[s] = int32_t(s);
+		if(l >= 1 && int(l) <= W.lightLen[p]) {
+			const uint32_t b = vcm_insert_hash(W.lv[size_t(l) * W.n + p].position, C.density) % C.mapSize;
+			const unsigned i = queue_reserve(G.count);
+			G.keys[i] = (u64(b) << C.slotBits) | u64(s);
+			G.vals[i] = int32_t(s);
+		}
 	}
 }
 
-__global__ void k_vcm_ranges(VcmGrid G, uint32_t total) {
+__global__ void k_vcm_ranges(VcmGrid G, uint32_t total, int slotBits) {
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-		const uint32_t b = uint32_t(G.keys[i]);
-		if(b == VCM_NO_BUCKET) continue;
-		if(i == 0 || uint32_t(G.keys[i - 1]) != b) G.start[b] = i;
-		if(i + 1 == total || uint32_t(G.keys[i + 1]) != b) G.end[b] = i + 1;
+		const uint32_t b = uint32_t(G.keys[i] >> slotBits);
+		if(i == 0 || uint32_t(G.keys[i - 1] >> slotBits) != b) G.start[b] = i;
+		if(i + 1 == total || uint32_t(G.keys[i + 1] >> slotBits) != b) G.end[b] = i + 1;
 	}
 }
 
 __global__ void k_vcm_gather(const BptwState W, VcmGrid G, uint32_t total, uint32_t maxP) {
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-		if(uint32_t(G.keys[i]) == VCM_NO_BUCKET) continue;
 		const uint32_t s = uint32_t(G.vals[i]);
 		const uint32_t p = s / maxP, l = s % maxP;
 		const BV& w = W.lv[size_t(l) * W.n + p];
@@ -430,7 +434,7 @@ size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 size_t vcm_grid_size(size_t slots, uint32_t mapSize) {
 	const size_t tiles = (slots + SORT_TILE - 1) / SORT_TILE;
 	return 2 * al256(slots * 8) + 2 * al256(slots * 4) + al256(tiles * 256 * 4) + al256(8 * 256 * 4) + al256(8 * 4) +
-	       al256(4) + 2 * al256(size_t(mapSize) * 4) + al256(slots * 80) + al256(8);
+	       al256(4) + 2 * al256(size_t(mapSize) * 4) + al256(slots * 80) + al256(8) + al256(4);
 }
 
 VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize) {
@@ -449,11 +453,13 @@ VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize) {
 	G.end = reinterpret_cast<uint32_t*>(take(size_t(mapSize) * 4));
 	G.photons = reinterpret_cast<float4*>(take(slots * 80));
 	G.seed = reinterpret_cast<u64*>(take(8));
+	G.count = reinterpret_cast<unsigned*>(take(4));
 	return G;
 }
 
-// Stable sort of the grid's (bucket, slot) pairs by the low 32 key bits.
-cudaError_t vcm_sort(const VcmGrid& G, uint32_t n, cudaStream_t stream) {
+// Stable sort of the grid's photon keys by their low 8 * passes bits (passes
+// even, at most 8).
+cudaError_t vcm_sort(const VcmGrid& G, uint32_t n, int passes, cudaStream_t stream) {
 	if(n <= 1) return cudaSuccess;
 	static std::once_flag once;
 	static cudaError_t attr = cudaSuccess;
@@ -468,14 +474,14 @@ cudaError_t vcm_sort(const VcmGrid& G, uint32_t n, cudaStream_t stream) {
 	k_sort_scan<<<8, 256, 0, stream>>>(G.hist);
 	u64* kin = G.keys; u64* kout = G.keysAlt;
 	int32_t* vin = G.vals; int32_t* vout = G.valsAlt;
-	for(int pass = 0; pass < 4; ++pass) {
+	for(int pass = 0; pass < passes; ++pass) {
 		if((e = cudaMemsetAsync(G.status, 0, size_t(tiles) * 256 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
 		k_onesweep<<<tiles, SORT_THREADS, SORT_SMEM, stream>>>(kin, vin, kout, vout, n, 8 * pass, G.hist + 256 * pass,
 		                                                       G.status, G.tileCounter + pass, G.error);
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}
-	return cudaGetLastError(); // after 4 passes the pairs are back in keys / vals
+	return cudaGetLastError(); // after an even number of passes the pairs are back in keys / vals
 }
 
 } // namespace
@@ -522,6 +528,12 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	C.viewArea = PI * C.radiusSq;
 	C.density = 1.0f / (radius * 2.0001f);
 	C.mapSize = cachedMap;
+	auto bits = [](uint64_t v) { int b = 0; while(v) { ++b; v >>= 1; } return b; };
+	C.slotBits = bits(uint64_t(slots) - 1);
+	// key bits: bucket and slot, sorted 8 per pass in an even number of passes
+	const int keyBits = bits(uint64_t(C.mapSize) - 1) + C.slotBits;
+	if(keyBits > 64) return cudaErrorInvalidValue;
+	const int passes = std::max(2, ((keyBits + 15) / 16) * 2);
 
 	cudaError_t e;
 	if((e = cudaMemsetAsync(T.iter, 0, size_t(n) * sizeof(float4), stream)) != cudaSuccess) return e;
@@ -550,15 +562,23 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 		trace(g);
 		k_bptw_light_shade<true><<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, g, C.nPhotons, C.lightArea);
 	}
-	// photon grid
+	// photon grid: the photons' keys, their count (read back to size the
+	// sort), the sort, the bucket ranges and the packed merge data
 	const unsigned gb = std::min<unsigned>((slots + 255) / 256, unsigned(sms) * 16u);
+	if((e = cudaMemsetAsync(G.count, 0, sizeof(unsigned), stream)) != cudaSuccess) return e;
 	k_vcm_keys<<<gb, 256, 0, stream>>>(W, G, C, uint32_t(maxP));
-	if((e = vcm_sort(G, slots, stream)) != cudaSuccess) return e;
+	unsigned photons = 0;
+	if((e = cudaMemcpyAsync(&photons, G.count, sizeof(unsigned), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return e;
+	if((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+	if((e = vcm_sort(G, photons, passes, stream)) != cudaSuccess) return e;
 	k_vcm_sort_status<<<1, 1, 0, stream>>>(G, counters);
 	if((e = cudaMemsetAsync(G.start, 0, size_t(C.mapSize) * 4, stream)) != cudaSuccess) return e;
 	if((e = cudaMemsetAsync(G.end, 0, size_t(C.mapSize) * 4, stream)) != cudaSuccess) return e;
-	k_vcm_ranges<<<gb, 256, 0, stream>>>(G, slots);
-	k_vcm_gather<<<gb, 256, 0, stream>>>(W, G, slots, uint32_t(maxP));
+	if(photons > 0) {
+		const unsigned pb = std::min<unsigned>((photons + 255) / 256, unsigned(sms) * 16u);
+		k_vcm_ranges<<<pb, 256, 0, stream>>>(G, photons, C.slotBits);
+		k_vcm_gather<<<pb, 256, 0, stream>>>(W, G, photons, uint32_t(maxP));
+	}
 	// view phase
 	k_vcmw_view_start<<<(n + 127) / 128, 128, 0, stream>>>(S, P, T, W, C, lightGens);
 	for(int k = 0; k < maxP; ++k) {
