@@ -289,7 +289,8 @@ enum { BPTW_EXT0 = 0, BPTW_SH0 = 2, BPTW_WORK = 4 };
 // (light shade, view start, view shade) are compiled for; their grids are
 // this many blocks per SM. They wait on scattered vertex loads, so occupancy
 // beats registers: 8 blocks (64 registers) measured fastest, bidirectional
-// path tracer 748 / 765 / 764 and VCM 468 / 479 / 490 Mrays/s at 4 / 6 / 8.
+// path tracer 748 / 765 / 764 and VCM 468 / 479 / 490 Mrays/s at 4 / 6 / 8;
+// 12 blocks (42 registers, more spills) fell back to 715 and 497.
 constexpr int BPTW_SHADE_BLOCKS = 8;
 // ... and the trace stage (5 and 6 measured alike; 8 was 6 % slower).
 constexpr int BPTW_TRACE_BLOCKS = 6;

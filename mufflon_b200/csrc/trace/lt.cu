@@ -278,6 +278,9 @@ enum { LTW_EXT0 = 0, LTW_SH0 = 2, LTW_WORK = 4 };
 // measured fastest on the 1080p headline scene (1 063 Mrays/s; 6: 1 048,
 // 8: 975).
 constexpr int LTW_TRACE_BLOCKS = 5;
+// ... and the shade stage (its grid is this many blocks per SM): 8 (64
+// registers, no spills) measured 1 059 Mrays/s, 12 (42 registers) 992.
+constexpr int LTW_SHADE_BLOCKS = 8;
 constexpr int LTW_COUNTERS = 4 + 2 * LTW_MAX_LAUNCHES;
 
 struct LtwState {
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(128, LTW_TRACE_BLOCKS) k_ltw_trace(const DScen
 // Generation gen: each traced segment of queue gen & 1 that hit a surface
 // becomes the photon's next vertex (lt_sample's loop body); its connection
 // and next segment go to generation gen + 1.
-__global__ void __launch_bounds__(128, 8) k_ltw_shade(const DScene S, const LtParams P, const LtTargets T, LtwState W, int gen) {
+__global__ void __launch_bounds__(128, LTW_SHADE_BLOCKS) k_ltw_shade(const DScene S, const LtParams P, const LtTargets T, LtwState W, int gen) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + LTW_EXT0 + q);
 	const uint32_t maxL = uint32_t(P.maxPathLength > 0 ? P.maxPathLength : 1);
@@ -515,7 +518,7 @@ cudaError_t launch_lt(const DScene& S, const LtParams& P, const LtTargets& T, un
 		for(int g = 0; g < gens; ++g) {
 			if(S.hasAlpha) k_ltw_trace<ALPHA_ALWAYS><<<tb, 128, 0, stream>>>(S, P, T, W, g, counters);
 			else k_ltw_trace<ALPHA_NEVER><<<tb, 128, 0, stream>>>(S, P, T, W, g, counters);
-			if(g + 1 < gens) k_ltw_shade<<<sms * 8, 128, 0, stream>>>(S, P, T, W, g);
+			if(g + 1 < gens) k_ltw_shade<<<sms * LTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, g);
 		}
 	} else {
 		if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
