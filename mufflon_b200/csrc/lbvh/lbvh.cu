@@ -549,11 +549,13 @@ cudaError_t LbvhBuilder::reserve(uint32_t n) {
 
 cudaError_t LbvhBuilder::sort_pairs(uint64_t* keys, int32_t* values, uint32_t n, cudaStream_t stream, int passes) {
 	cudaError_t e = reserve(n);
-	if(e != cudaSuccess || n <= 1) return e;
+	if(e != cudaSuccess) return e;
+	// callers read the error word after the sort, also when there is nothing to sort
+	cudaMemsetAsync(m_error, 0, sizeof(unsigned int), stream);
+	if(n <= 1) return cudaSuccess;
 	const uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
 	cudaMemsetAsync(m_hist, 0, 8 * 256 * sizeof(uint32_t), stream);
 	cudaMemsetAsync(m_tileCounter, 0, 8 * sizeof(unsigned int), stream);
-	cudaMemsetAsync(m_error, 0, sizeof(unsigned int), stream);
 	const unsigned hb = std::min<unsigned>(blocks_for(n, 256), 148u * 8u);
 	k_sort_hist<<<hb, 256, 0, stream>>>(keys, n, m_hist);
 	k_sort_scan<<<8, 256, 0, stream>>>(m_hist);

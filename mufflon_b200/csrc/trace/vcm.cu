@@ -460,16 +460,17 @@ VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize) {
 // Stable sort of the grid's photon keys by their low 8 * passes bits (passes
 // even, at most 8).
 cudaError_t vcm_sort(const VcmGrid& G, uint32_t n, int passes, cudaStream_t stream) {
+	cudaError_t e;
+	// the error word is read after the sort even when there is nothing to sort
+	if((e = cudaMemsetAsync(G.error, 0, sizeof(unsigned), stream)) != cudaSuccess) return e;
 	if(n <= 1) return cudaSuccess;
 	static std::once_flag once;
 	static cudaError_t attr = cudaSuccess;
 	std::call_once(once, [] { attr = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SORT_SMEM)); });
 	if(attr != cudaSuccess) return attr;
-	cudaError_t e;
 	const uint32_t tiles = (n + SORT_TILE - 1) / SORT_TILE;
 	if((e = cudaMemsetAsync(G.hist, 0, 8 * 256 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
 	if((e = cudaMemsetAsync(G.tileCounter, 0, 8 * sizeof(unsigned), stream)) != cudaSuccess) return e;
-	if((e = cudaMemsetAsync(G.error, 0, sizeof(unsigned), stream)) != cudaSuccess) return e;
 	k_sort_hist<<<std::min<unsigned>((n + 255) / 256, 148u * 8u), 256, 0, stream>>>(G.keys, n, G.hist);
 	k_sort_scan<<<8, 256, 0, stream>>>(G.hist);
 	u64* kin = G.keys; u64* kout = G.keysAlt;
