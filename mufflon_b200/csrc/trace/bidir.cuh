@@ -310,6 +310,8 @@ struct BptwState {
 	float4* sDir;       // direction
 	float4* sAdd;       // radiance rgb, lightness if unoccluded
 	uint4* sMeta;       // pixel, record slot (low, high word), sign bits of the occluded zeros
+	BV* hv;             // per item of a view generation's segment queue: the vertex it reached
+	float4* hThr;       // its throughput, and its pixel + 1 (bits; 0: nothing more to do for it)
 	unsigned* counters; // BPTW_COUNTERS
 	uint32_t n;
 };
@@ -416,7 +418,8 @@ int bptw_trace_blocks() {
 size_t bptw_size(size_t n, size_t m) {
 	auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
 	return al(n * m * sizeof(BV)) + 2 * al(n * sizeof(BV)) + al(n * 16) + al(n * 4) +
-	       2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) + 4 * al(n * m * 16) + al(BPTW_COUNTERS * sizeof(unsigned));
+	       2 * (al(n * 4) + 3 * al(n * 16) + al(n * 4)) + 4 * al(n * m * 16) + al(n * sizeof(BV)) + al(n * 16) +
+	       al(BPTW_COUNTERS * sizeof(unsigned));
 }
 
 BptwState bptw_carve(void* memory, size_t n, size_t m) {
@@ -442,6 +445,8 @@ BptwState bptw_carve(void* memory, size_t n, size_t m) {
 	W.sDir = reinterpret_cast<float4*>(take(n * m * 16));
 	W.sAdd = reinterpret_cast<float4*>(take(n * m * 16));
 	W.sMeta = reinterpret_cast<uint4*>(take(n * m * 16));
+	W.hv = reinterpret_cast<BV*>(take(n * sizeof(BV)));
+	W.hThr = reinterpret_cast<float4*>(take(n * 16));
 	W.counters = reinterpret_cast<unsigned*>(take(BPTW_COUNTERS * sizeof(unsigned)));
 	return W;
 }

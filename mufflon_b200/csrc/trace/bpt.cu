@@ -408,11 +408,13 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_view_shade(cons
 				o[0] = add.x; o[1] = add.y; o[2] = add.z; o[3] = add.w;
 			}
 		}
-		if(bv_end(h.kind) || viewLen >= maxP) continue;
+		// the connections run in k_bptw_connect: with them this kernel waited
+		// on instruction fetches more than on memory
+		const bool more = !bv_end(h.kind) && viewLen < maxP;
+		__stcs(W.hThr + i, make_float4(thr.x, thr.y, thr.z, __uint_as_float(more ? p + 1u : 0u)));
+		if(!more) continue;
+		bv_store(W.hv + i, h);
 		const int px = int(p % T.width), py = int(p / T.width);
-		const int lightLen = W.lightLen[p];
-		bptw_connect(S, P, T, W, h, &pv, viewLen, p, px, py, thr, max(0, P.minPathLength - viewLen - 1),
-		             min(lightLen + 1, maxP - viewLen), gen + 1);
 		u64 rng = T.rngState[p];
 		f3 o, d;
 		float pdf;
@@ -421,6 +423,29 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_view_shade(cons
 			bv_store(W.vp[viewLen & 1] + p, h);
 		}
 		T.rngState[p] = rng;
+	}
+}
+
+// The connections of the vertices k_bptw_view_shade reached in generation gen
+// (view path length k + 1) with their pixels' light subpaths, item by item of
+// the same queue; the predecessors are still in vp[k & 1]. The shadow rays go
+// to generation gen + 1.
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+                                                      int gen, int k) {
+	const int q = gen & 1;
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
+	const int maxP = P.maxPathLength > 0 ? P.maxPathLength : 1;
+	const int viewLen = k + 1;
+	for(unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+		const float4 tm = __ldcs(W.hThr + i);
+		const uint32_t tag = __float_as_uint(tm.w);
+		if(tag == 0u) continue;
+		const uint32_t p = tag - 1u;
+		const BV h = bv_load(W.hv + i);
+		const BV pv = bv_load(W.vp[k & 1] + p);
+		const int lightLen = W.lightLen[p];
+		bptw_connect(S, P, T, W, h, &pv, viewLen, p, int(p % T.width), int(p / T.width), f4to3(tm),
+		             max(0, P.minPathLength - viewLen - 1), min(lightLen + 1, maxP - viewLen), gen + 1);
 	}
 }
 
@@ -500,6 +525,7 @@ cudaError_t launch_bpt(const DScene& S, const LtParams& P, const LtTargets& T, v
 		for(int k = 0; k < maxP; ++k) {
 			trace(lightGens + k);
 			k_bptw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
+			if(k + 1 < maxP) k_bptw_connect<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
 		}
 	} else {
 		if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;

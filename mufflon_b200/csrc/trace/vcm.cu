@@ -19,9 +19,9 @@
 // bucket and, within a bucket, by ascending (subpath, vertex) slot,
 // k_vcm_ranges finds the bucket ranges and k_vcm_gather packs each photon's
 // merge data (80 B) in bucket order. View phase: k_vcmw_view_start, then per generation the trace
-// kernel, k_vcmw_view_shade (the vertex reached: its emitter term, its
-// connections and next segment; it hands the vertex on) and k_vcmw_merge (the
-// vertex's merges). A bucket's photons are visited
+// kernel, k_vcmw_view_shade (the vertex reached: its emitter term and next
+// segment; it hands the vertex on), k_vcmw_merge (the vertex's merges) and
+// k_vcmw_connect (its connections). A bucket's photons are visited
 // from the last to the first, the order of the reference's head-inserted
 // lists when one thread fills them, so every contribution is the oracle's bit
 // for bit.
@@ -89,8 +89,6 @@ struct VcmGrid {
 	                      // vertex's incident pdf; the previous vertex's relative-probability sum
 	u64* seed;            // the light tree's seed of the iteration
 	unsigned* count;      // photons of the iteration (light vertices after the start)
-	BV* mergeV;           // per item of a view generation's queue: the vertex reached
-	float4* mergeThr;     // its throughput, and its pixel + 1 (bits; 0: no merge, the path ended)
 };
 
 __global__ void k_vcm_seed(const LtTargets T, VcmGrid G) {
@@ -400,14 +398,13 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_view_shade(cons
 			bpt_add(T, p, add);
 			vcm_record(T, base + size_t(viewLen - 1), p, add);
 		}
-		// the merges run in k_vcmw_merge: with them this kernel waited on
-		// instruction fetches more than on memory
-		__stcs(G.mergeThr + i, make_float4(thr.x, thr.y, thr.z, __uint_as_float(bv_end(h.kind) ? 0u : p + 1u)));
+		// the merges and connections run in k_vcmw_merge and k_vcmw_connect:
+		// with them this kernel waited on instruction fetches more than on memory
+		__stcs(W.hThr + i, make_float4(thr.x, thr.y, thr.z, __uint_as_float(bv_end(h.kind) ? 0u : p + 1u)));
 		if(bv_end(h.kind)) continue;
-		bv_store(G.mergeV + i, h);
+		bv_store(W.hv + i, h);
 		if(viewLen >= maxP) continue;
 		const int px = int(p % T.width), py = int(p / T.width);
-		vcmw_connect(S, P, T, W, C, h, &pv, viewLen, p, px, py, thr, gen + 1);
 		u64 rng = T.rngState[p];
 		f3 o, d;
 		float pdf;
@@ -429,15 +426,33 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_merge(const DSc
 	const int maxP = P.maxPathLength > 0 ? P.maxPathLength : 1;
 	const int viewLen = k + 1;
 	for(unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-		const float4 tm = __ldcs(G.mergeThr + i);
+		const float4 tm = W.hThr[i];
 		const uint32_t tag = __float_as_uint(tm.w);
 		if(tag == 0u) continue;
 		const uint32_t p = tag - 1u;
-		const BV h = bv_load(G.mergeV + i);
+		const BV h = bv_load(W.hv + i);
 		const BV pv = bv_load(W.vp[k & 1] + p);
 		const float4 merged = vcm_merge(S, P, G, C, h, pv, viewLen, f4to3(tm));
 		bpt_add(T, p, merged);
 		vcm_record(T, size_t(p) * vcm_slots(maxP) + size_t(maxP) * size_t(maxP) + size_t(maxP) + size_t(viewLen - 1), p, merged);
+	}
+}
+
+// The connections of the same vertices with the light subpath each pixel is
+// paired with; the shadow rays go to generation gen + 1.
+__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+                                                      VcmConsts C, int gen, int k) {
+	const int q = gen & 1;
+	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
+	const int viewLen = k + 1;
+	for(unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+		const float4 tm = __ldcs(W.hThr + i);
+		const uint32_t tag = __float_as_uint(tm.w);
+		if(tag == 0u) continue;
+		const uint32_t p = tag - 1u;
+		const BV h = bv_load(W.hv + i);
+		const BV pv = bv_load(W.vp[k & 1] + p);
+		vcmw_connect(S, P, T, W, C, h, &pv, viewLen, p, int(p % T.width), int(p / T.width), f4to3(tm), gen + 1);
 	}
 }
 
@@ -457,14 +472,13 @@ __global__ void k_vcm_finalize(LtTargets T) {
 // ---------------------------------------------------------------- memory
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
-size_t vcm_grid_size(size_t slots, uint32_t mapSize, size_t pixels) {
+size_t vcm_grid_size(size_t slots, uint32_t mapSize) {
 	const size_t tiles = (slots + SORT_TILE - 1) / SORT_TILE;
 	return 2 * al256(slots * 8) + 2 * al256(slots * 4) + al256(tiles * 256 * 4) + al256(8 * 256 * 4) + al256(8 * 4) +
-	       al256(4) + 2 * al256(size_t(mapSize) * 4) + al256(slots * 80) + al256(8) + al256(4) +
-	       al256(pixels * sizeof(BV)) + al256(pixels * 16);
+	       al256(4) + 2 * al256(size_t(mapSize) * 4) + al256(slots * 80) + al256(8) + al256(4);
 }
 
-VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize, size_t pixels) {
+VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize) {
 	auto take = [&](size_t b) { char* r = m; m += al256(b); return r; };
 	const size_t tiles = (slots + SORT_TILE - 1) / SORT_TILE;
 	VcmGrid G;
@@ -481,8 +495,6 @@ VcmGrid vcm_grid_carve(char* m, size_t slots, uint32_t mapSize, size_t pixels) {
 	G.photons = reinterpret_cast<float4*>(take(slots * 80));
 	G.seed = reinterpret_cast<u64*>(take(8));
 	G.count = reinterpret_cast<unsigned*>(take(4));
-	G.mergeV = reinterpret_cast<BV*>(take(pixels * sizeof(BV)));
-	G.mergeThr = reinterpret_cast<float4*>(take(pixels * 16));
 	return G;
 }
 
@@ -532,7 +544,7 @@ uint32_t vcm_map_size(uint32_t capacity) {
 size_t vcm_bytes(size_t numPixels, int maxPathLength) {
 	const size_t m = size_t(maxPathLength > 0 ? maxPathLength : 1);
 	const size_t slots = numPixels * m;
-	return al256(bptw_size(numPixels, m)) + vcm_grid_size(slots, vcm_map_size(uint32_t(slots)), numPixels);
+	return al256(bptw_size(numPixels, m)) + vcm_grid_size(slots, vcm_map_size(uint32_t(slots)));
 }
 
 cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V, const LtTargets& T, TraceCounters* counters,
@@ -574,7 +586,7 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	}
 	char* mem = static_cast<char*>(memory);
 	const BptwState W = bptw_carve(mem, n, size_t(maxP));
-	const VcmGrid G = vcm_grid_carve(mem + al256(bptw_size(n, size_t(maxP))), slots, C.mapSize, n);
+	const VcmGrid G = vcm_grid_carve(mem + al256(bptw_size(n, size_t(maxP))), slots, C.mapSize);
 	if((e = cudaMemsetAsync(W.counters, 0, BPTW_COUNTERS * sizeof(unsigned), stream)) != cudaSuccess) return e;
 	const int tb = bptw_trace_blocks();
 	int dev = 0, sms = 148;
@@ -615,6 +627,7 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 		trace(lightGens + k);
 		k_vcmw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
 		k_vcmw_merge<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
+		if(k + 1 < maxP) k_vcmw_connect<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, C, lightGens + k, k);
 	}
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_vcm_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
