@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_view_shade(cons
 // (view path length k + 1) with their pixels' light subpaths, item by item of
 // the same queue; the predecessors are still in vp[k & 1]. The shadow rays go
 // to generation gen + 1.
-__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_bptw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_CONNECT_BLOCKS) k_bptw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                       int gen, int k) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
@@ -525,7 +525,7 @@ cudaError_t launch_bpt(const DScene& S, const LtParams& P, const LtTargets& T, v
 		for(int k = 0; k < maxP; ++k) {
 			trace(lightGens + k);
 			k_bptw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
-			if(k + 1 < maxP) k_bptw_connect<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
+			if(k + 1 < maxP) k_bptw_connect<<<sms * BPTW_CONNECT_BLOCKS, 128, 0, stream>>>(S, P, T, W, lightGens + k, k);
 		}
 	} else {
 		if((e = cudaMemsetAsync(workCounter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;

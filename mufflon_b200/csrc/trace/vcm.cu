@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_view_shade(cons
 // The merges of the vertices k_vcmw_view_shade reached in generation gen
 // (view path length k + 1), item by item of the same queue; the predecessors
 // are still in vp[k & 1].
-__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_merge(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, VCM_MERGE_BLOCKS) k_vcmw_merge(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                     VcmGrid G, VcmConsts C, int gen, int k) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_merge(const DSc
 
 // The connections of the same vertices with the light subpath each pixel is
 // paired with; the shadow rays go to generation gen + 1.
-__global__ void __launch_bounds__(128, BPTW_SHADE_BLOCKS) k_vcmw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
+__global__ void __launch_bounds__(128, BPTW_CONNECT_BLOCKS) k_vcmw_connect(const DScene S, const LtParams P, const LtTargets T, BptwState W,
                                                       VcmConsts C, int gen, int k) {
 	const int q = gen & 1;
 	const unsigned count = *reinterpret_cast<volatile unsigned*>(W.counters + BPTW_EXT0 + q);
@@ -626,8 +626,8 @@ cudaError_t launch_vcm(const DScene& S, const LtParams& P, const VcmSettings& V,
 	for(int k = 0; k < maxP; ++k) {
 		trace(lightGens + k);
 		k_vcmw_view_shade<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
-		k_vcmw_merge<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
-		if(k + 1 < maxP) k_vcmw_connect<<<sms * BPTW_SHADE_BLOCKS, 128, 0, stream>>>(S, P, T, W, C, lightGens + k, k);
+		k_vcmw_merge<<<sms * VCM_MERGE_BLOCKS, 128, 0, stream>>>(S, P, T, W, G, C, lightGens + k, k);
+		if(k + 1 < maxP) k_vcmw_connect<<<sms * BPTW_CONNECT_BLOCKS, 128, 0, stream>>>(S, P, T, W, C, lightGens + k, k);
 	}
 	if((e = cudaGetLastError()) != cudaSuccess) return e;
 	k_vcm_finalize<<<(n + 255) / 256, 256, 0, stream>>>(T);
