@@ -297,7 +297,7 @@ constexpr int BPTW_TRACE_BLOCKS = 6;
 // Resident blocks per SM of the connection kernels (k_bptw_connect,
 // k_vcmw_connect) and of VCM's merge kernel. Measured at 1080p (Mrays/s,
 // connections at 8 / 6 / 4 blocks): BPT 778 / 780 / 785, VCM 569 / 569 / 571;
-// the merges at 6 blocks: VCM 567.
+// the merges at 6 / 8 / 10 / 12 blocks: VCM 567 / 569 / 560 / 560.
 constexpr int BPTW_CONNECT_BLOCKS = 4;
 constexpr int VCM_MERGE_BLOCKS = 8;
 constexpr int BPTW_COUNTERS = 4 + 2 * BPTW_MAX_PATH;
